@@ -1,0 +1,290 @@
+"""ORACLE — test infrastructure only.
+
+ctypes bindings for
+  liboracle.so              CPU restatement of the reference Krylov path
+                            (xs_oracle.cpp, every function cites the reference
+                            file:line it restates), and
+  _ref/libxsref_intel.so    the reference's own intel/ CPU solver compiled from
+  _ref/libxsref_ilu0.so     its sources, and its hip ilu0_simple (Makefile).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
+this package, as the checker or the timed CPU baseline.  The product path
+(xsolver_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF_INTEL = None
+_REF_ILU0 = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def build(ref: bool = True) -> None:
+    """Compile liboracle.so (and the reference libraries when the reference
+    sources are present)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    refdir = os.environ.get("XS_REFERENCE_DIR", "/root/reference")
+    if ref and os.path.isdir(os.path.join(refdir, "intel")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={refdir}"], check=True)
+
+
+def _p(a, t=np.float64):
+    if a is None:
+        return None
+    assert a.dtype == t and a.flags["C_CONTIGUOUS"], (a.dtype, t)
+    return a.ctypes.data_as(_dp if t == np.float64 else _ip)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(ref=False)
+        _LIB = C.CDLL(path)
+    return _LIB
+
+
+def ref_intel():
+    """The compiled reference intel/ solver, or None if it was not built."""
+    global _REF_INTEL
+    if _REF_INTEL is None:
+        path = os.path.join(HERE, "_ref", "libxsref_intel.so")
+        if not os.path.exists(path):
+            return None
+        _REF_INTEL = C.CDLL(path)
+    return _REF_INTEL
+
+
+def ref_ilu0():
+    global _REF_ILU0
+    if _REF_ILU0 is None:
+        path = os.path.join(HERE, "_ref", "libxsref_ilu0.so")
+        if not os.path.exists(path):
+            return None
+        _REF_ILU0 = C.CDLL(path)
+    return _REF_ILU0
+
+
+class LU:
+    """Factors in the seqilu0 layout: L strict lower (unit diagonal implied),
+    dinv = 1/u_ii, U' = dinv_i * u_ij strict upper (row-scaled)."""
+
+    def __init__(self, n, lrp, lci, lv, dinv, urp, uci, uv):
+        self.n = n
+        self.lrp, self.lci, self.lv = lrp, lci, lv
+        self.dinv = dinv
+        self.urp, self.uci, self.uv = urp, uci, uv
+
+    def args(self):
+        return (_p(self.lrp, np.int32), _p(self.lci, np.int32), _p(self.lv), _p(self.dinv),
+                _p(self.urp, np.int32), _p(self.uci, np.int32), _p(self.uv))
+
+
+def _counts(A):
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    nl = int((A.colidx < rows).sum())
+    nu = int((A.colidx > rows).sum())
+    return nl, nu
+
+
+def ilu0(A) -> LU:
+    nl, nu = _counts(A)
+    n = A.n
+    lrp = np.zeros(n + 1, np.int32); urp = np.zeros(n + 1, np.int32)
+    lci = np.zeros(max(nl, 1), np.int32); uci = np.zeros(max(nu, 1), np.int32)
+    lv = np.zeros(max(nl, 1)); uv = np.zeros(max(nu, 1)); dinv = np.zeros(n)
+    rc = lib().orc_ilu0(n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val),
+                        _p(lrp, np.int32), _p(lci, np.int32), _p(lv), _p(dinv),
+                        _p(urp, np.int32), _p(uci, np.int32), _p(uv))
+    if rc != 0:
+        raise ValueError("matrix has a row without a diagonal entry")
+    return LU(n, lrp, lci[:nl], lv[:nl], dinv, urp, uci[:nu], uv[:nu])
+
+
+def ilu0_values(A) -> np.ndarray:
+    out = np.zeros(A.nnz)
+    lib().orc_ilu0_values(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), _p(out))
+    return out
+
+
+def ref_ilu0_values(A):
+    """Combined ILU(0) values from the reference's own ilu0_simple."""
+    r = ref_ilu0()
+    if r is None:
+        return None
+    out = np.zeros(A.nnz)
+    uptr = np.zeros(A.n, np.int32)
+    val = A.val.copy()
+    rp = A.rowptr.copy(); ci = A.colidx.copy()
+    r.ref_ilu0_simple(_p(out), _p(val), _p(rp, np.int32), _p(ci, np.int32), C.c_int(A.n), _p(uptr, np.int32))
+    return out
+
+
+def split_lu(A, luv) -> LU:
+    nl, nu = _counts(A)
+    n = A.n
+    lrp = np.zeros(n + 1, np.int32); urp = np.zeros(n + 1, np.int32)
+    lci = np.zeros(max(nl, 1), np.int32); uci = np.zeros(max(nu, 1), np.int32)
+    lv = np.zeros(max(nl, 1)); uv = np.zeros(max(nu, 1)); dinv = np.zeros(n)
+    luv = np.ascontiguousarray(luv, dtype=np.float64)
+    rc = lib().orc_split_lu(n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(luv),
+                            _p(lrp, np.int32), _p(lci, np.int32), _p(lv), _p(dinv),
+                            _p(urp, np.int32), _p(uci, np.int32), _p(uv))
+    if rc != 0:
+        raise ValueError("matrix has a row without a diagonal entry")
+    return LU(n, lrp, lci[:nl], lv[:nl], dinv, urp, uci[:nu], uv[:nu])
+
+
+def parilu_values(A, sweeps=20) -> np.ndarray:
+    out = np.zeros(A.nnz)
+    rc = lib().orc_parilu(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), C.c_int(sweeps), _p(out))
+    if rc != 0:
+        raise ValueError("matrix has a row without a diagonal entry")
+    return out
+
+
+def parilu(A, sweeps=20) -> LU:
+    return split_lu(A, parilu_values(A, sweeps))
+
+
+def parilut(A, fill=2.0, sweeps=5, droptol=0.0) -> LU:
+    L = C.CDLL  # placeholder to keep linters quiet
+    ptrs = [C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)(), C.POINTER(C.c_double)(),
+            C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()]
+    f = lib().orc_parilut
+    rc = f(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), C.c_double(fill), C.c_int(sweeps),
+           C.c_double(droptol), *[C.byref(p) for p in ptrs])
+    if rc != 0:
+        raise ValueError("matrix has a row without a diagonal entry")
+    n = A.n
+    lrp = np.ctypeslib.as_array(ptrs[0], (n + 1,)).copy()
+    urp = np.ctypeslib.as_array(ptrs[4], (n + 1,)).copy()
+    nl, nu = int(lrp[-1]), int(urp[-1])
+    lci = np.ctypeslib.as_array(ptrs[1], (max(nl, 1),))[:nl].copy()
+    lv = np.ctypeslib.as_array(ptrs[2], (max(nl, 1),))[:nl].copy()
+    dinv = np.ctypeslib.as_array(ptrs[3], (n,)).copy()
+    uci = np.ctypeslib.as_array(ptrs[5], (max(nu, 1),))[:nu].copy()
+    uv = np.ctypeslib.as_array(ptrs[6], (max(nu, 1),))[:nu].copy()
+    for p in ptrs:
+        lib().orc_free(C.cast(p, C.c_void_p))
+    del L
+    return LU(n, lrp, lci, lv, dinv, urp, uci, uv)
+
+
+def lusolve(F: LU, x) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(F.n)
+    lib().orc_lusolve(F.n, *F.args()[:4], *F.args()[4:], _p(x), _p(y))
+    return y
+
+
+def lusolve_t(F: LU, x) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(F.n)
+    lib().orc_lusolve_t(F.n, *F.args(), _p(x), _p(y))
+    return y
+
+
+def spmv(A, x) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(A.n)
+    lib().orc_csr_spmv(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), _p(x), _p(y))
+    return y
+
+
+def spmv_t(A, x) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(A.n)
+    lib().orc_csr_spmv_t(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), _p(x), _p(y))
+    return y
+
+
+def levels_lower(n, rp, ci):
+    lev = np.zeros(n, np.int32)
+    nlev = lib().orc_levels_lower(n, _p(rp, np.int32), _p(ci, np.int32), _p(lev, np.int32))
+    return lev, nlev
+
+
+PC = {"none": 0, "jacobi": 1, "lu": 2}
+
+
+def solve(method, A, rhs, x0=None, tol=1e-8, maxiter=1000, restart=30, pc="jacobi", factors: LU | None = None,
+          quirk=1):
+    """Run a restated Krylov loop.  method: cg, cgm, bicgstab, gcr, igcr,
+    hip_igcr, gmres, fgmres.  pc: none / jacobi / lu (needs factors).
+
+    Returns (x, resvec, usediter).  resvec follows the restated loop's own
+    convention: intel loops give relative residuals indexed by iteration;
+    hip_igcr gives absolute residuals with resvec[0] = ||r0||."""
+    n = A.n
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+    x = np.zeros(n) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+    x0c = x.copy()
+    resvec = np.zeros(maxiter + 2)
+    used = C.c_int(0)
+    kind = PC[pc]
+    fargs = factors.args() if (kind == 2) else (None,) * 7
+    common = (n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), kind, *fargs)
+    L = lib()
+    if method in ("cg", "cgm", "bicgstab"):
+        f = {"cg": L.orc_cg, "cgm": L.orc_cgm, "bicgstab": L.orc_bicgstab}[method]
+        w = f(*common, _p(rhs), _p(x), C.c_double(tol), C.c_int(maxiter), _p(x0c), C.byref(used), _p(resvec))
+    elif method in ("gcr", "igcr"):
+        w = L.orc_gcr(*common, _p(rhs), _p(x), C.c_int(restart), C.c_double(tol), C.c_int(maxiter), _p(x0c),
+                      C.byref(used), _p(resvec), C.c_int(1 if method == "igcr" else 0))
+    elif method == "hip_igcr":
+        w = L.orc_hip_igcr(*common, _p(rhs), _p(x), C.c_int(restart), C.c_double(tol), C.c_int(maxiter), _p(x0c),
+                           C.byref(used), _p(resvec))
+    elif method in ("gmres", "fgmres"):
+        w = L.orc_gmres(*common, _p(rhs), _p(x), C.c_int(restart), C.c_double(tol), C.c_int(maxiter), _p(x0c),
+                        C.byref(used), _p(resvec), C.c_int(1 if method == "fgmres" else 0), C.c_int(quirk))
+    else:
+        raise ValueError(method)
+    return x, resvec[:w].copy(), used.value
+
+
+def ref_solve(method, A, rhs, x0=None, tol=1e-8, maxiter=1000, restart=30):
+    """Run the compiled reference intel/ solver with its Jacobi
+    preconditioner (the only one it supports).  Returns (x, resvec, usediter)
+    in the intel convention, or None when the reference was not built."""
+    R = ref_intel()
+    if R is None:
+        return None
+    n = A.n
+    rows = np.repeat(np.arange(n), np.diff(A.rowptr))
+    off = A.colidx != rows
+    diag = np.zeros(n)
+    diag[rows[~off]] = A.val[~off]
+    offval = np.ascontiguousarray(A.val[off])
+    offcol = np.ascontiguousarray(A.colidx[off])
+    offptr = np.zeros(n + 1, np.int32)
+    np.cumsum(np.bincount(rows[off], minlength=n), out=offptr[1:])
+    nI, nH, nS = C.c_int(n), C.c_int(0), C.c_int(int(off.sum()))
+    R.cpu_mat_setup(C.byref(nI), C.byref(nH), C.byref(nS), _p(diag), _p(offval), _p(offptr, np.int32),
+                    _p(offcol, np.int32))
+    R.cpu_preconditioner_setup(C.c_char_p(b"Jacobi"))
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64).copy()
+    x = np.zeros(n) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+    x0c = x.copy()
+    resvec = np.zeros(maxiter + 2)
+    used = C.c_int(-1)
+    t, mi, rs = C.c_double(tol), C.c_int(maxiter), C.c_int(restart)
+    if method in ("cg", "cgm", "bicgstab"):
+        f = {"cg": R.cpu_cg_solve, "cgm": R.cpu_cgm_solve, "bicgstab": R.cpu_bicgstab_solve}[method]
+        f(_p(rhs), _p(x), C.byref(t), C.byref(mi), _p(x0c), C.byref(used), _p(resvec))
+    else:
+        f = {"gcr": R.cpu_gcr_solve, "igcr": R.cpu_igcr_solve, "gmres": R.cpu_gmres_solve,
+             "fgmres": R.cpu_fgmres_solve}[method]
+        f(_p(rhs), _p(x), C.byref(rs), C.byref(t), C.byref(mi), _p(x0c), C.byref(used), _p(resvec))
+    R.cpu_preconditioner_free(C.c_char_p(b"Jacobi"))
+    return x, resvec, used.value

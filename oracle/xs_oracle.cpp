@@ -1,0 +1,1135 @@
+/*
+ * ORACLE — test infrastructure only.
+ *
+ * CPU restatement of the reference (tandongdong10/xsolver) preconditioned
+ * Krylov path.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg load this library, and only as the checker or the timed CPU
+ * baseline; the product path (libxsolver_b200.so) never calls it.
+ *
+ * What is restated, and from where (paths relative to the reference root):
+ *   - BLAS-1 in sequential order: the cblas_* calls of intel/mpisolver-C-v1.cpp,
+ *     with the natural left-to-right summation the sequential shim gives.
+ *   - SpMV / b-Ax in the intel "diag + off-diagonal" order:
+ *     intel/HostMatrix.h:83-125 (off-diagonal entries in row order, diagonal
+ *     term added last).
+ *   - Jacobi: intel/HostMatrix.h:127-147 (diag = 1/(a_ii + 1e-20)).
+ *   - ILU(0): hip/Precond/ilut_diag_in_csr.cpp:347-405 (ilu0_simple, IKJ,
+ *     pivot clamp 1e-20) + the split of hip/HostMatrix/HostMatrixCSR.cpp:164-197
+ *     (seqilu0: L strict lower, diag = 1/u_ii, U' = U_strict * diag row-scaled).
+ *   - LUsolve: hip/HostMatrix/HostMatrixCSR.cpp:385-409.
+ *   - Krylov loops: intel/mpisolver-C-v1.cpp  cg :26-102, cgm :193-272,
+ *     bicgstab :365-482, gcr :685-810, igcr :812-931, gmres :933-1087,
+ *     fgmres :1089-1247, Givens/updatec :1249-1301.  Right-preconditioned
+ *     GCR with modified Gram-Schmidt: hip/Solver/xsolver_igcr.cpp:29-108.
+ *   - ParILU: hip/Precond/gpuparilu.cpp:46-102 (ilu0_ij_aw), with the split of
+ *     hip/Precond/par_ilu_hip/Asplit_gpu.cpp:4-49; restated with SYNCHRONOUS
+ *     (Jacobi-style) sweeps so that it is deterministic.
+ *   - ParILUT: hip/Precond/parilut.cpp:621-1206 (parilut_clean) with the sweep
+ *     kernels :392-560, threshold removal :283-380 and k-th select
+ *     par_ilut_hip/select_kth.h:501; restated with synchronous sweeps.
+ *
+ * The only deliberate departure from the intel loops: intel's
+ * preconditionerCPU() is a no-op unless "Jacobi" was selected
+ * (intel/HostMatrix.h:170-176); here "no preconditioner" is an identity copy.
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+/* ---------------- BLAS-1, sequential order ---------------- */
+double o_dot(int n, const double *x, const double *y)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += x[i] * y[i];
+    return s;
+}
+void o_axpy(int n, double a, const double *x, double *y)
+{
+    for (int i = 0; i < n; i++) y[i] += a * x[i];
+}
+void o_copy(int n, const double *x, double *y)
+{
+    if (x != y) std::memcpy(y, x, sizeof(double) * (size_t)n);
+}
+void o_scal(int n, double a, double *x)
+{
+    for (int i = 0; i < n; i++) x[i] *= a;
+}
+
+/* ---------------- matrix in intel "diag + off-diagonal" form ---------------- */
+struct MCSR {
+    int n = 0;
+    std::vector<double> diag;
+    std::vector<int> rp, ci;
+    std::vector<double> v;
+    void from_csr(int n_, const int *rowptr, const int *colidx, const double *val)
+    {
+        n = n_;
+        diag.assign(n, 0.0);
+        rp.assign(n + 1, 0);
+        ci.clear();
+        v.clear();
+        int base = rowptr[0];
+        for (int i = 0; i < n; i++) {
+            for (int k = rowptr[i] - base; k < rowptr[i + 1] - base; k++) {
+                int j = colidx[k] - base;
+                if (j == i) diag[i] = val[k];
+                else { ci.push_back(j); v.push_back(val[k]); }
+            }
+            rp[i + 1] = (int)ci.size();
+        }
+    }
+    void spmv(const double *x, double *y) const
+    {
+        for (int i = 0; i < n; i++) {
+            double r = 0.0;
+            for (int k = rp[i]; k < rp[i + 1]; k++) r = r + v[k] * x[ci[k]];
+            y[i] = r + diag[i] * x[i];
+        }
+    }
+    void bmax(const double *b, const double *x, double *y) const
+    {
+        for (int i = 0; i < n; i++) {
+            double r = b[i];
+            for (int k = rp[i]; k < rp[i + 1]; k++) r = r - v[k] * x[ci[k]];
+            y[i] = r - diag[i] * x[i];
+        }
+    }
+};
+
+/* ---------------- preconditioners ---------------- */
+enum { PC_NONE = 0, PC_JACOBI = 1, PC_LU = 2 };
+
+struct LUFactors {
+    int n = 0;
+    std::vector<int> lrp, lci, urp, uci;
+    std::vector<double> lv, uv, dinv;
+};
+
+/* hip/HostMatrix/HostMatrixCSR.cpp:385-409 */
+void lusolve(const LUFactors &f, const double *x, double *y)
+{
+    int n = f.n;
+    for (int i = 0; i < n; i++) {
+        double sum = x[i];
+        for (int ii = f.lrp[i]; ii < f.lrp[i + 1]; ii++) sum -= y[f.lci[ii]] * f.lv[ii];
+        y[i] = sum;
+    }
+    for (int i = 0; i < n; i++) y[i] *= f.dinv[i];
+    for (int i = n - 1; i >= 0; i--) {
+        double sum = y[i];
+        for (int ii = f.urp[i + 1] - 1; ii >= f.urp[i]; ii--) sum -= y[f.uci[ii]] * f.uv[ii];
+        y[i] = sum;
+    }
+}
+
+struct Precond {
+    int kind = PC_NONE;
+    int n = 0;
+    std::vector<double> jdiag;
+    const LUFactors *lu = nullptr;
+    std::vector<double> tmp;
+    void apply(const double *x, double *y)
+    {
+        if (kind == PC_JACOBI) {
+            for (int i = 0; i < n; i++) y[i] = jdiag[i] * x[i];
+        } else if (kind == PC_LU) {
+            lusolve(*lu, x, y);
+        } else {
+            o_copy(n, x, y);
+        }
+    }
+};
+
+/* ---------------- ILU(0) ---------------- */
+/* hip/Precond/ilut_diag_in_csr.cpp:347-405 (ilu0_simple) */
+void ilu0_simple(double *luval, const double *val, const int *rows, const int *cols, int n, int *uptr)
+{
+    for (int i = 0; i < n; i++) uptr[i] = -1;
+    for (int i = 0; i < rows[n]; i++) luval[i] = val[i];
+    for (int i = 0; i < n; i++)
+        for (int j = rows[i]; j < rows[i + 1]; j++)
+            if (cols[j] == i) { uptr[i] = j; break; }
+    for (int i = 0; i < n; i++) {
+        int upart = uptr[i];
+        for (int j = rows[i]; j < upart; j++) {
+            int k = cols[j];
+            if (std::fabs(luval[uptr[k]]) < 1e-20) luval[uptr[k]] = 1e-20;
+            luval[j] = luval[j] / luval[uptr[k]];
+            int subptr = uptr[k];
+            for (int jj = j + 1; jj < rows[i + 1]; jj++) {
+                int kk = cols[jj];
+                while (cols[subptr] < kk && subptr < rows[k + 1]) subptr++;
+                if (subptr < rows[k + 1]) {
+                    if (cols[subptr] == kk) {
+                        double tmp = luval[j] * luval[subptr];
+                        luval[jj] = luval[jj] - tmp;
+                    }
+                } else
+                    break;
+            }
+        }
+        if (std::fabs(luval[uptr[i]]) < 1e-20) luval[uptr[i]] = 1e-20;
+    }
+}
+
+/* hip/HostMatrix/HostMatrixCSR.cpp:164-197 (seqilu0 split) applied to a
+ * combined LU value array over A's pattern. */
+void split_lu(int n, const int *rp, const int *ci, const double *luv, const int *uptr, LUFactors &f)
+{
+    f.n = n;
+    f.lrp.assign(n + 1, 0);
+    f.urp.assign(n + 1, 0);
+    f.lci.clear(); f.lv.clear(); f.uci.clear(); f.uv.clear();
+    f.dinv.assign(n, 0.0);
+    for (int i = 0; i < n; i++) {
+        for (int ii = rp[i]; ii < uptr[i]; ii++) { f.lv.push_back(luv[ii]); f.lci.push_back(ci[ii]); }
+        f.dinv[i] = 1 / luv[uptr[i]];
+        for (int ii = uptr[i] + 1; ii < rp[i + 1]; ii++) { f.uv.push_back(luv[ii] * f.dinv[i]); f.uci.push_back(ci[ii]); }
+        f.lrp[i + 1] = (int)f.lci.size();
+        f.urp[i + 1] = (int)f.uci.size();
+    }
+}
+
+/* ---------------- CSR helpers ---------------- */
+struct CSR {
+    int n = 0;
+    std::vector<int> rp, ci;
+    std::vector<double> v;
+};
+
+/* stable transpose (rows within each column stay in increasing order) */
+CSR transpose(const CSR &a)
+{
+    CSR t;
+    t.n = a.n;
+    t.rp.assign(a.n + 1, 0);
+    for (int k = 0; k < a.rp[a.n]; k++) t.rp[a.ci[k] + 1]++;
+    for (int i = 0; i < a.n; i++) t.rp[i + 1] += t.rp[i];
+    t.ci.resize(a.rp[a.n]);
+    t.v.resize(a.rp[a.n]);
+    std::vector<int> pos(t.rp.begin(), t.rp.end() - 1);
+    for (int i = 0; i < a.n; i++)
+        for (int k = a.rp[i]; k < a.rp[i + 1]; k++) {
+            int p = pos[a.ci[k]]++;
+            t.ci[p] = i;
+            t.v[p] = a.v[k];
+        }
+    return t;
+}
+
+double find_in_row(const CSR &a, int i, int j)
+{
+    /* binary search as in parilut.cpp:407-419 (first position with col >= j) */
+    int l = a.rp[i], r = a.rp[i + 1];
+    while (l < r) {
+        int mid = l + ((r - l) >> 1);
+        if (a.ci[mid] < j) l = mid + 1;
+        else r = mid;
+    }
+    return (l < a.rp[i + 1] && a.ci[l] == j) ? a.v[l] : 0.0;
+}
+
+/* ParILUT sweep value for entry (i,j): a_ij - sum_{k<min(i,j)} l_ik u_kj,
+ * merging L row i (CSR, unit diag stored last) with U column j (CSC, diag
+ * stored last); parilut.cpp:421-441.  Returns the sum; *l_div receives u_jj. */
+double sweep_value(const CSR &A, const CSR &L, const CSR &Uc, int i, int j)
+{
+    double t = find_in_row(A, i, j);
+    int il = L.rp[i], iu = Uc.rp[j];
+    int last = (i <= j) ? i : j;
+    while (true) {
+        int lj = L.ci[il], ui = Uc.ci[iu];
+        int check = (i <= j) ? ui : lj;
+        if (check >= last) break;
+        if (lj == ui) t = t - L.v[il] * Uc.v[iu];
+        il += (lj <= ui);
+        iu += (ui <= lj);
+    }
+    return t;
+}
+
+}  // namespace
+
+extern "C" {
+
+/* ========================= basic kernels ========================= */
+
+/* y = A x, CSR (0- or 1-based via rowptr[0]), sequential order per row. */
+void orc_csr_spmv(int n, const int *rp, const int *ci, const double *v, const double *x, double *y)
+{
+    int base = rp[0];
+    for (int i = 0; i < n; i++) {
+        double s = 0.0;
+        for (int k = rp[i] - base; k < rp[i + 1] - base; k++) s += v[k] * x[ci[k] - base];
+        y[i] = s;
+    }
+}
+
+/* y = A^T x, CSR input. */
+void orc_csr_spmv_t(int n, const int *rp, const int *ci, const double *v, const double *x, double *y)
+{
+    int base = rp[0];
+    for (int i = 0; i < n; i++) y[i] = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int k = rp[i] - base; k < rp[i + 1] - base; k++) y[ci[k] - base] += v[k] * x[i];
+}
+
+/* ILU(0) + seqilu0 split.  Outputs sized by the caller: L arrays hold
+ * nnz_strict_lower, U arrays nnz_strict_upper.  Returns 0 or -1 if a row
+ * has no diagonal entry. */
+int orc_ilu0(int n, const int *rp, const int *ci, const double *v,
+             int *lrp, int *lci, double *lv, double *dinv, int *urp, int *uci, double *uv)
+{
+    int nnz = rp[n];
+    std::vector<double> luv(nnz);
+    std::vector<int> uptr(n);
+    ilu0_simple(luv.data(), v, rp, ci, n, uptr.data());
+    for (int i = 0; i < n; i++)
+        if (uptr[i] < 0) return -1;
+    LUFactors f;
+    split_lu(n, rp, ci, luv.data(), uptr.data(), f);
+    std::memcpy(lrp, f.lrp.data(), sizeof(int) * (n + 1));
+    std::memcpy(urp, f.urp.data(), sizeof(int) * (n + 1));
+    std::memcpy(lci, f.lci.data(), sizeof(int) * f.lci.size());
+    std::memcpy(uci, f.uci.data(), sizeof(int) * f.uci.size());
+    std::memcpy(lv, f.lv.data(), sizeof(double) * f.lv.size());
+    std::memcpy(uv, f.uv.data(), sizeof(double) * f.uv.size());
+    std::memcpy(dinv, f.dinv.data(), sizeof(double) * n);
+    return 0;
+}
+
+/* Combined ILU(0) values over A's pattern (ilu0_simple output, before split). */
+void orc_ilu0_values(int n, const int *rp, const int *ci, const double *v, double *luv)
+{
+    std::vector<int> uptr(n);
+    ilu0_simple(luv, v, rp, ci, n, uptr.data());
+}
+
+void orc_lusolve(int n, const int *lrp, const int *lci, const double *lv, const double *dinv,
+                 const int *urp, const int *uci, const double *uv, const double *x, double *y)
+{
+    LUFactors f;
+    f.n = n;
+    f.lrp.assign(lrp, lrp + n + 1);
+    f.lci.assign(lci, lci + lrp[n]);
+    f.lv.assign(lv, lv + lrp[n]);
+    f.urp.assign(urp, urp + n + 1);
+    f.uci.assign(uci, uci + urp[n]);
+    f.uv.assign(uv, uv + urp[n]);
+    f.dinv.assign(dinv, dinv + n);
+    lusolve(f, x, y);
+}
+
+/* Transposed LU solve: y = (L D U')^{-T} x = L^{-T} D U'^{-T} x, in the
+ * order U'^T forward (unit), scale by dinv, L^T backward (unit).  Used by the
+ * adjoint checks.  Row sums accumulate in increasing source-row order. */
+void orc_lusolve_t(int n, const int *lrp, const int *lci, const double *lv, const double *dinv,
+                   const int *urp, const int *uci, const double *uv, const double *x, double *y)
+{
+    std::vector<double> w(x, x + n);
+    /* U'^T z = x : column-oriented forward (scatter) */
+    for (int i = 0; i < n; i++) {
+        double zi = w[i];
+        y[i] = zi;
+        for (int k = urp[i]; k < urp[i + 1]; k++) w[uci[k]] -= uv[k] * zi;
+    }
+    for (int i = 0; i < n; i++) y[i] *= dinv[i];
+    for (int i = 0; i < n; i++) w[i] = y[i];
+    for (int i = n - 1; i >= 0; i--) {
+        double yi = w[i];
+        y[i] = yi;
+        for (int k = lrp[i]; k < lrp[i + 1]; k++) w[lci[k]] -= lv[k] * yi;
+    }
+}
+
+/* ========================= ParILU ========================= */
+/* Synchronous restatement of hip/Precond/gpuparilu.cpp:46-102 (ilu0_ij_aw)
+ * over A's pattern.  luv (size nnz) receives L (strict lower, unit diag
+ * implicit) and U (upper incl. diagonal) values over A's pattern, in the same
+ * layout as ilu0_simple's output.  Initial guess: L = strict lower of A,
+ * U = upper of A (Asplit_gpu.cpp:28-49). */
+int orc_parilu(int n, const int *rp, const int *ci, const double *v, int sweeps, double *luv)
+{
+    int nnz = rp[n];
+    std::vector<int> uptr(n, -1), rowof(nnz);
+    for (int i = 0; i < n; i++)
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            rowof[k] = i;
+            if (ci[k] == i) uptr[i] = k;
+        }
+    for (int i = 0; i < n; i++)
+        if (uptr[i] < 0) return -1;
+    /* U column access: for column j, the positions k (in A order) of upper
+     * entries (row <= j), sorted by row */
+    std::vector<int> ucp(n + 1, 0), ucpos;
+    for (int k = 0; k < nnz; k++)
+        if (rowof[k] <= ci[k]) ucp[ci[k] + 1]++;
+    for (int j = 0; j < n; j++) ucp[j + 1] += ucp[j];
+    ucpos.resize(ucp[n]);
+    {
+        std::vector<int> pos(ucp.begin(), ucp.end() - 1);
+        for (int k = 0; k < nnz; k++)
+            if (rowof[k] <= ci[k]) ucpos[pos[ci[k]]++] = k;
+    }
+    std::vector<double> cur(v, v + nnz), nxt(nnz);
+    for (int s = 0; s < sweeps; s++) {
+        for (int k = 0; k < nnz; k++) {
+            int i = rowof[k], j = ci[k];
+            double sacc = v[k], sp = 0.0;
+            /* L row i: A entries with col < i, then the unit diagonal (col i) */
+            int il = rp[i], ilend = uptr[i] + 1; /* position uptr[i] stands for the unit diagonal */
+            int iu = ucp[j], iuend = ucp[j + 1];
+            while (il < ilend && iu < iuend) {
+                sp = 0.0;
+                int jl = ci[il];
+                int ju = rowof[ucpos[iu]];
+                double lval = (il == uptr[i]) ? 1.0 : cur[il];
+                double uval = cur[ucpos[iu]];
+                sp = (jl == ju) ? lval * uval : sp;
+                sacc = (jl == ju) ? sacc - sp : sacc;
+                il = (jl <= ju) ? il + 1 : il;
+                iu = (jl >= ju) ? iu + 1 : iu;
+            }
+            sacc += sp;
+            if (i > j) {
+                double t = cur[uptr[j]];
+                if (std::fabs(t) < 1e-10) t = (t >= 0 ? 1e-10 : -1e-10);
+                t = sacc / t;
+                nxt[k] = std::isfinite(t) ? t : cur[k];
+            } else {
+                if (i == j && std::fabs(sacc) < 1e-10) sacc = (sacc >= 0 ? 1e-10 : -1e-10);
+                nxt[k] = std::isfinite(sacc) ? sacc : cur[k];
+            }
+        }
+        cur.swap(nxt);
+    }
+    std::memcpy(luv, cur.data(), sizeof(double) * nnz);
+    return 0;
+}
+
+/* Split combined LU values over A's pattern into (L strict, dinv, U'), the
+ * seqilu0 layout.  Sizes as for orc_ilu0. */
+int orc_split_lu(int n, const int *rp, const int *ci, const double *luv,
+                 int *lrp, int *lci, double *lv, double *dinv, int *urp, int *uci, double *uv)
+{
+    std::vector<int> uptr(n, -1);
+    for (int i = 0; i < n; i++)
+        for (int k = rp[i]; k < rp[i + 1]; k++)
+            if (ci[k] == i) uptr[i] = k;
+    for (int i = 0; i < n; i++)
+        if (uptr[i] < 0) return -1;
+    LUFactors f;
+    split_lu(n, rp, ci, luv, uptr.data(), f);
+    std::memcpy(lrp, f.lrp.data(), sizeof(int) * (n + 1));
+    std::memcpy(urp, f.urp.data(), sizeof(int) * (n + 1));
+    std::memcpy(lci, f.lci.data(), sizeof(int) * f.lci.size());
+    std::memcpy(uci, f.uci.data(), sizeof(int) * f.uci.size());
+    std::memcpy(lv, f.lv.data(), sizeof(double) * f.lv.size());
+    std::memcpy(uv, f.uv.data(), sizeof(double) * f.uv.size());
+    std::memcpy(dinv, f.dinv.data(), sizeof(double) * n);
+    return 0;
+}
+
+/* ========================= ParILUT ========================= */
+/*
+ * Restatement of parilut_clean (hip/Precond/parilut.cpp:621-1206) with
+ * synchronous sweeps.  Per sweep s = 0..sweeps-1:
+ *   rate = (fill - 1)/sweeps*(s+1) + 1                          (:692)
+ *   R = A - L*U over pattern(A) u pattern(L*U); each entry formed as
+ *       c = -a_ij; c += l_ik*u_kj for k ascending; r = -c     (:730-744)
+ *   D: lower entries r_ij / u_jj, upper entries r_ij, then every entry in
+ *       A's pattern reset to a_ij                            (embedA_intoB_L2/U2)
+ *   L = strict lower(D) + unit diag (last), U = upper(D) (CSC, diag last)
+ *   one sweep over all L (off-diagonal) and U entries          (LU_sweep)
+ *   if nnz(D) - round(rate*nnz(A)) > 0: for L and for U separately keep
+ *       keep = (int)(rate*nnz0) entries: thr = remove-th smallest |v|
+ *       (remove = max(nnz - keep, 0), 1-based; entries incl. diagonal),
+ *       drop non-diagonal entries with |v| < thr                (:1000-1090)
+ *   optional drop tolerance (no reference counterpart): also drop
+ *       off-diagonal l_ij with |l_ij| < droptol and u_ij with
+ *       |u_ij| < droptol*|u_jj|
+ *   L sweep, then U sweep (using the new L)                    (:1110-1150)
+ * Result: L (CSR, strict lower, unit diag implicit), dinv = 1/u_ii, and
+ * U' = dinv_i * u_ij (CSR strict upper, row-scaled) — the seqilu0 layout.
+ * Output arrays are allocated with malloc; free with orc_free.
+ */
+int orc_parilut(int n, const int *arp, const int *aci, const double *av, double fill, int sweeps, double droptol,
+                int **lrp_o, int **lci_o, double **lv_o, double **dinv_o, int **urp_o, int **uci_o, double **uv_o)
+{
+    CSR A;
+    A.n = n;
+    A.rp.assign(arp, arp + n + 1);
+    A.ci.assign(aci, aci + arp[n]);
+    A.v.assign(av, av + arp[n]);
+    int nnzA = arp[n];
+    /* initial L (CSR, unit diag last), U (CSR, diag first) */
+    CSR L, U;
+    L.n = U.n = n;
+    L.rp.assign(n + 1, 0);
+    U.rp.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        bool hasdiag = false;
+        for (int k = arp[i]; k < arp[i + 1]; k++) {
+            if (aci[k] < i) { L.ci.push_back(aci[k]); L.v.push_back(av[k]); }
+            else { U.ci.push_back(aci[k]); U.v.push_back(av[k]); if (aci[k] == i) hasdiag = true; }
+        }
+        if (!hasdiag) return -1;
+        L.ci.push_back(i); L.v.push_back(1.0);
+        L.rp[i + 1] = (int)L.ci.size();
+        U.rp[i + 1] = (int)U.ci.size();
+    }
+    long l0nnz = L.rp[n], u0nnz = U.rp[n];
+
+    for (int s = 0; s < sweeps; s++) {
+        double rate = (fill - 1) / sweeps * (s + 1) + 1;
+        CSR Uc = transpose(U); /* CSC of U: column j, rows ascending, diag last */
+        /* u_jj from current U (CSR row j, first entry is the diagonal) */
+        std::vector<double> udiag(n);
+        for (int j = 0; j < n; j++) udiag[j] = U.v[U.rp[j]];
+        /* candidates D */
+        CSR D;
+        D.n = n;
+        D.rp.assign(n + 1, 0);
+        std::vector<int> cols;
+        for (int i = 0; i < n; i++) {
+            cols.clear();
+            for (int k = arp[i]; k < arp[i + 1]; k++) cols.push_back(aci[k]);
+            for (int kl = L.rp[i]; kl < L.rp[i + 1]; kl++) {
+                int k = L.ci[kl];
+                for (int ku = U.rp[k]; ku < U.rp[k + 1]; ku++) cols.push_back(U.ci[ku]);
+            }
+            std::sort(cols.begin(), cols.end());
+            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+            for (int j : cols) {
+                /* c = -a_ij + sum_k l_ik u_kj (k ascending, k <= min(i,j)) */
+                double c = -find_in_row(A, i, j);
+                int il = L.rp[i], iu = Uc.rp[j];
+                while (il < L.rp[i + 1] && iu < Uc.rp[j + 1]) {
+                    int lj = L.ci[il], ui = Uc.ci[iu];
+                    if (lj == ui) { c += L.v[il] * Uc.v[iu]; il++; iu++; }
+                    else if (lj < ui) il++;
+                    else iu++;
+                }
+                double r = -c;
+                double d;
+                if (j < i) d = r / udiag[j];
+                else d = r;
+                D.ci.push_back(j);
+                D.v.push_back(d);
+            }
+            /* reset A-pattern entries to a_ij */
+            int p = D.rp[i];
+            for (int k = arp[i]; k < arp[i + 1]; k++) {
+                while (D.ci[p] < aci[k]) p++;
+                D.v[p] = av[k];
+            }
+            D.rp[i + 1] = (int)D.ci.size();
+        }
+        long nnzD = D.rp[n];
+        /* split */
+        CSR L2, U2;
+        L2.n = U2.n = n;
+        L2.rp.assign(n + 1, 0);
+        U2.rp.assign(n + 1, 0);
+        for (int i = 0; i < n; i++) {
+            for (int k = D.rp[i]; k < D.rp[i + 1]; k++) {
+                if (D.ci[k] < i) { L2.ci.push_back(D.ci[k]); L2.v.push_back(D.v[k]); }
+                else { U2.ci.push_back(D.ci[k]); U2.v.push_back(D.v[k]); }
+            }
+            L2.ci.push_back(i); L2.v.push_back(1.0);
+            L2.rp[i + 1] = (int)L2.ci.size();
+            U2.rp[i + 1] = (int)U2.ci.size();
+        }
+        CSR U2c = transpose(U2);
+        /* LU sweep (synchronous): new values from the snapshot (L2, U2c) */
+        {
+            std::vector<double> lnew(L2.v), unew(U2c.v);
+            for (int i = 0; i < n; i++)
+                for (int k = L2.rp[i]; k < L2.rp[i + 1]; k++) {
+                    int j = L2.ci[k];
+                    if (j >= i) continue;
+                    double t = sweep_value(A, L2, U2c, i, j);
+                    lnew[k] = t / U2c.v[U2c.rp[j + 1] - 1];
+                }
+            for (int j = 0; j < n; j++)
+                for (int k = U2c.rp[j]; k < U2c.rp[j + 1]; k++) {
+                    int i = U2c.ci[k];
+                    unew[k] = sweep_value(A, L2, U2c, i, j);
+                }
+            L2.v.swap(lnew);
+            U2c.v.swap(unew);
+        }
+        /* threshold removal */
+        long keep_nnz = std::lround(rate * nnzA);
+        long remove_nnz = nnzD - keep_nnz;
+        CSR L3, U3c;
+        auto kth_smallest_abs = [](const std::vector<double> &vals, long k) -> double {
+            if (k <= 0) return 0.0;
+            std::vector<double> a(vals.size());
+            for (size_t q = 0; q < vals.size(); q++) a[q] = std::fabs(vals[q]);
+            std::nth_element(a.begin(), a.begin() + (k - 1), a.end());
+            return a[k - 1];
+        };
+        if (remove_nnz > 0 || droptol > 0) {
+            double lthr = 0.0, uthr = 0.0;
+            if (remove_nnz > 0) {
+                long lkeep = (long)(rate * l0nnz);
+                long lremove = std::max((long)L2.rp[n] - lkeep, 0L);
+                long ukeep = (long)(rate * u0nnz);
+                long uremove = std::max((long)U2c.rp[n] - ukeep, 0L);
+                lthr = kth_smallest_abs(L2.v, lremove);
+                uthr = kth_smallest_abs(U2c.v, uremove);
+            }
+            L3.n = U3c.n = n;
+            L3.rp.assign(n + 1, 0);
+            U3c.rp.assign(n + 1, 0);
+            for (int i = 0; i < n; i++) {
+                int last = L2.rp[i + 1] - 1;
+                for (int k = L2.rp[i]; k < L2.rp[i + 1]; k++) {
+                    double a = std::fabs(L2.v[k]);
+                    bool keep = (k == last) || (a >= lthr && !(droptol > 0 && a < droptol));
+                    if (keep) { L3.ci.push_back(L2.ci[k]); L3.v.push_back(L2.v[k]); }
+                }
+                L3.rp[i + 1] = (int)L3.ci.size();
+            }
+            for (int j = 0; j < n; j++) {
+                int last = U2c.rp[j + 1] - 1;
+                double ujj = std::fabs(U2c.v[last]);
+                for (int k = U2c.rp[j]; k < U2c.rp[j + 1]; k++) {
+                    double a = std::fabs(U2c.v[k]);
+                    bool keep = (k == last) || (a >= uthr && !(droptol > 0 && a < droptol * ujj));
+                    if (keep) { U3c.ci.push_back(U2c.ci[k]); U3c.v.push_back(U2c.v[k]); }
+                }
+                U3c.rp[j + 1] = (int)U3c.ci.size();
+            }
+        } else {
+            L3 = L2;
+            U3c = U2c;
+        }
+        /* L sweep, then U sweep with the new L */
+        {
+            std::vector<double> lnew(L3.v);
+            for (int i = 0; i < n; i++)
+                for (int k = L3.rp[i]; k < L3.rp[i + 1]; k++) {
+                    int j = L3.ci[k];
+                    if (j >= i) continue;
+                    double t = sweep_value(A, L3, U3c, i, j);
+                    lnew[k] = t / U3c.v[U3c.rp[j + 1] - 1];
+                }
+            L3.v.swap(lnew);
+            std::vector<double> unew(U3c.v);
+            for (int j = 0; j < n; j++)
+                for (int k = U3c.rp[j]; k < U3c.rp[j + 1]; k++) {
+                    int i = U3c.ci[k];
+                    unew[k] = sweep_value(A, L3, U3c, i, j);
+                }
+            U3c.v.swap(unew);
+        }
+        L = L3;
+        U = transpose(U3c); /* back to CSR, diag first in each row */
+    }
+    /* convert to (L strict, dinv, U' row-scaled) */
+    int *lrp = (int *)std::malloc(sizeof(int) * (n + 1));
+    int *urp = (int *)std::malloc(sizeof(int) * (n + 1));
+    double *dinv = (double *)std::malloc(sizeof(double) * n);
+    long nl = L.rp[n] - n, nu = U.rp[n] - n;
+    int *lci = (int *)std::malloc(sizeof(int) * std::max(nl, 1L));
+    double *lv = (double *)std::malloc(sizeof(double) * std::max(nl, 1L));
+    int *uci = (int *)std::malloc(sizeof(int) * std::max(nu, 1L));
+    double *uv = (double *)std::malloc(sizeof(double) * std::max(nu, 1L));
+    lrp[0] = urp[0] = 0;
+    long pl = 0, pu = 0;
+    for (int i = 0; i < n; i++) {
+        for (int k = L.rp[i]; k < L.rp[i + 1]; k++)
+            if (L.ci[k] < i) { lci[pl] = L.ci[k]; lv[pl] = L.v[k]; pl++; }
+        lrp[i + 1] = (int)pl;
+        double d = 0.0;
+        for (int k = U.rp[i]; k < U.rp[i + 1]; k++)
+            if (U.ci[k] == i) d = U.v[k];
+        dinv[i] = 1.0 / d;
+        for (int k = U.rp[i]; k < U.rp[i + 1]; k++)
+            if (U.ci[k] > i) { uci[pu] = U.ci[k]; uv[pu] = U.v[k] * dinv[i]; pu++; }
+        urp[i + 1] = (int)pu;
+    }
+    *lrp_o = lrp; *lci_o = lci; *lv_o = lv; *dinv_o = dinv; *urp_o = urp; *uci_o = uci; *uv_o = uv;
+    return 0;
+}
+
+void orc_free(void *p) { std::free(p); }
+
+/* ========================= Krylov loops ========================= */
+/*
+ * Common arguments:
+ *   n, rp/ci/v      A in CSR (0-based, sorted, diagonal present)
+ *   pc_kind         0 identity, 1 Jacobi, 2 LU factors (lrp..uv as orc_ilu0)
+ *   rhs, sol        sol receives the solution
+ *   sol_init        initial guess (may equal sol)
+ *   resvec          relative residual per iteration (intel convention:
+ *                   resvec[iiter] = ||r_iiter|| / ||r_0||), may be NULL
+ *   usediter        out: intel convention
+ * Returns the number of resvec entries written.
+ */
+struct OracleCtx {
+    MCSR A;
+    Precond M;
+    LUFactors lu;
+};
+
+static void ctx_init(OracleCtx &c, int n, const int *rp, const int *ci, const double *v, int pc_kind,
+                     const int *lrp, const int *lci, const double *lv, const double *dinv,
+                     const int *urp, const int *uci, const double *uv)
+{
+    c.A.from_csr(n, rp, ci, v);
+    c.M.kind = pc_kind;
+    c.M.n = n;
+    if (pc_kind == PC_JACOBI) {
+        c.M.jdiag.resize(n);
+        for (int i = 0; i < n; i++) {
+            double t = c.A.diag[i] + 1e-20;
+            c.M.jdiag[i] = 1.0 / t;
+        }
+    } else if (pc_kind == PC_LU) {
+        c.lu.n = n;
+        c.lu.lrp.assign(lrp, lrp + n + 1);
+        c.lu.lci.assign(lci, lci + lrp[n]);
+        c.lu.lv.assign(lv, lv + lrp[n]);
+        c.lu.urp.assign(urp, urp + n + 1);
+        c.lu.uci.assign(uci, uci + urp[n]);
+        c.lu.uv.assign(uv, uv + urp[n]);
+        c.lu.dinv.assign(dinv, dinv + n);
+        c.M.lu = &c.lu;
+    }
+}
+
+#define ORC_ARGS                                                                                  \
+    int n, const int *rp, const int *ci, const double *v, int pc_kind, const int *lrp, const int *lci, \
+        const double *lv, const double *dinv, const int *urp, const int *uci, const double *uv
+#define ORC_CTX                    \
+    OracleCtx ctx;                 \
+    ctx_init(ctx, n, rp, ci, v, pc_kind, lrp, lci, lv, dinv, urp, uci, uv); \
+    const MCSR &A = ctx.A;         \
+    Precond &M = ctx.M;
+
+/* intel/mpisolver-C-v1.cpp:26-102 (left-preconditioned CG on M^-1 A) */
+int orc_cg(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
+           int *usediter, double *resvec)
+{
+    ORC_CTX;
+    std::vector<double> pk(n), phi(n), res(n), Apk(n), qk(n);
+    double sigma, alpha, minalpha, taoo, tao, resl, rsm, beta;
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    M.apply(res.data(), res.data());
+    double res0 = o_dot(n, res.data(), res.data());
+    o_copy(n, res.data(), pk.data());
+    taoo = res0;
+    res0 = std::sqrt(res0);
+    for (int iiter = 0; iiter < maxiter; iiter++) {
+        *usediter = iiter;
+        A.spmv(pk.data(), Apk.data());
+        M.apply(Apk.data(), qk.data());
+        sigma = o_dot(n, pk.data(), qk.data());
+        alpha = taoo / (sigma + small);
+        minalpha = minone * alpha;
+        o_axpy(n, alpha, pk.data(), phi.data());
+        o_axpy(n, minalpha, qk.data(), res.data());
+        resl = o_dot(n, res.data(), res.data());
+        tao = resl;
+        resl = std::sqrt(resl);
+        rsm = resl / (res0 + small);
+        if (resvec) resvec[iiter] = rsm;
+        written = iiter + 1;
+        if (rsm < tol) {
+            *usediter = iiter;
+            o_copy(n, phi.data(), sol);
+            return written;
+        }
+        beta = tao / (taoo + small);
+        taoo = tao;
+        o_scal(n, beta, pk.data());
+        o_axpy(n, one, res.data(), pk.data());
+    }
+    o_copy(n, phi.data(), sol);
+    return written;
+}
+
+/* intel/mpisolver-C-v1.cpp:193-272 (standard PCG, "cgm") */
+int orc_cgm(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
+            int *usediter, double *resvec)
+{
+    ORC_CTX;
+    std::vector<double> pk(n), phi(n), res(n), zk(n), Apk(n);
+    double sigma, alpha, minalpha, taoo, tao, resl, rsm, beta;
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    M.apply(res.data(), zk.data());
+    double res0 = o_dot(n, res.data(), res.data());
+    tao = o_dot(n, res.data(), zk.data());
+    o_copy(n, zk.data(), pk.data());
+    res0 = std::sqrt(res0);
+    for (int iiter = 0; iiter < maxiter; iiter++) {
+        *usediter = iiter;
+        taoo = tao;
+        A.spmv(pk.data(), Apk.data());
+        sigma = o_dot(n, pk.data(), Apk.data());
+        alpha = tao / (sigma + small);
+        minalpha = minone * alpha;
+        o_axpy(n, alpha, pk.data(), phi.data());
+        o_axpy(n, minalpha, Apk.data(), res.data());
+        M.apply(res.data(), zk.data());
+        tao = o_dot(n, res.data(), zk.data());
+        beta = tao / (taoo + small);
+        o_scal(n, beta, pk.data());
+        o_axpy(n, one, zk.data(), pk.data());
+        resl = o_dot(n, res.data(), res.data());
+        resl = std::sqrt(resl);
+        rsm = resl / (res0 + small);
+        if (resvec) resvec[iiter] = rsm;
+        written = iiter + 1;
+        if (rsm < tol) {
+            *usediter = iiter;
+            o_copy(n, phi.data(), sol);
+            return written;
+        }
+    }
+    o_copy(n, phi.data(), sol);
+    return written;
+}
+
+/* intel/mpisolver-C-v1.cpp:365-482 (right-preconditioned BiCGSTAB; phi is
+ * kept in the preconditioned variable and sol = M^-1 phi at the end). */
+int orc_bicgstab(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
+                 int *usediter, double *resvec)
+{
+    ORC_CTX;
+    std::vector<double> zk(n, 0.0), phi(n), res(n), pk(n, 0.0), uk(n, 0.0), vk(n, 0.0), sk(n, 0.0), reso(n);
+    double alpha, minalpha, omega, resl, rsm, beta, beto, gama, mingama, tmp, t0, t1;
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    double res0 = o_dot(n, res.data(), res.data());
+    res0 = std::sqrt(res0);
+    o_copy(n, res.data(), reso.data());
+    alpha = 1.0;
+    beto = 1.0;
+    gama = 1.0;
+    for (int iiter = 0; iiter < maxiter; iiter++) {
+        *usediter = iiter;
+        beta = o_dot(n, res.data(), reso.data());
+        omega = (beta * gama) / (alpha * beto + small);
+        beto = beta;
+        minalpha = minone * alpha;
+        o_axpy(n, minalpha, uk.data(), pk.data());
+        o_scal(n, omega, pk.data());
+        o_axpy(n, one, res.data(), pk.data());
+        M.apply(pk.data(), zk.data());
+        A.spmv(zk.data(), uk.data());
+        tmp = o_dot(n, uk.data(), reso.data());
+        gama = beta / (tmp + small);
+        mingama = minone * gama;
+        o_copy(n, res.data(), sk.data());
+        o_axpy(n, mingama, uk.data(), sk.data());
+        M.apply(sk.data(), zk.data());
+        A.spmv(zk.data(), vk.data());
+        t0 = o_dot(n, vk.data(), sk.data());
+        t1 = o_dot(n, vk.data(), vk.data());
+        alpha = t0 / (t1 + small);
+        o_axpy(n, gama, pk.data(), phi.data());
+        o_axpy(n, alpha, sk.data(), phi.data());
+        minalpha = minone * alpha;
+        o_copy(n, sk.data(), res.data());
+        o_axpy(n, minalpha, vk.data(), res.data());
+        resl = o_dot(n, res.data(), res.data());
+        resl = std::sqrt(resl);
+        rsm = resl / (res0 + small);
+        if (resvec) resvec[iiter] = rsm;
+        written = iiter + 1;
+        if (rsm < tol) {
+            *usediter = iiter;
+            M.apply(phi.data(), sol);
+            return written;
+        }
+    }
+    M.apply(phi.data(), sol);
+    return written;
+}
+
+/* intel/mpisolver-C-v1.cpp:685-931: left-preconditioned GCR(restart),
+ * classical Gram-Schmidt (mgs = 0, cpu_gcr_solve) or modified (mgs = 1,
+ * cpu_igcr_solve). */
+int orc_gcr(ORC_ARGS, const double *rhs, double *sol, int restart, double tol, int maxiter,
+            const double *sol_init, int *usediter, double *resvec, int mgs)
+{
+    ORC_CTX;
+    std::vector<std::vector<double>> uk(restart, std::vector<double>(n, 0.0)), ck(restart, std::vector<double>(n, 0.0));
+    std::vector<double> res(n), phi(n), alpha(restart, 0.0);
+    double error, rnorm, tmp, mintmp, t0, t1;
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    M.apply(res.data(), res.data());
+    double res0 = o_dot(n, res.data(), res.data());
+    res0 = std::sqrt(res0);
+    int iiter = 0;
+    while (iiter < maxiter) {
+        int k = 0;
+        while (k < restart && iiter < maxiter) {
+            o_copy(n, res.data(), uk[k].data());
+            A.spmv(uk[k].data(), ck[k].data());
+            M.apply(ck[k].data(), ck[k].data());
+            if (!mgs) {
+                for (int i = 0; i < k; i++) alpha[i] = o_dot(n, ck[i].data(), ck[k].data());
+                for (int i = 0; i < k; i++) {
+                    tmp = minone * alpha[i];
+                    o_axpy(n, tmp, ck[i].data(), ck[k].data());
+                    o_axpy(n, tmp, uk[i].data(), uk[k].data());
+                }
+            } else {
+                for (int i = 0; i < k; i++) {
+                    double a = o_dot(n, ck[i].data(), ck[k].data());
+                    double ma = minone * a;
+                    o_axpy(n, ma, ck[i].data(), ck[k].data());
+                    o_axpy(n, ma, uk[i].data(), uk[k].data());
+                }
+            }
+            t0 = o_dot(n, ck[k].data(), ck[k].data());
+            t1 = o_dot(n, ck[k].data(), res.data());
+            t0 = std::sqrt(t0);
+            tmp = one / (t0 + small);
+            o_scal(n, tmp, uk[k].data());
+            o_scal(n, tmp, ck[k].data());
+            tmp = t1 / (t0 + small);
+            mintmp = minone * tmp;
+            o_axpy(n, tmp, uk[k].data(), phi.data());
+            o_axpy(n, mintmp, ck[k].data(), res.data());
+            tmp = o_dot(n, res.data(), res.data());
+            rnorm = std::sqrt(tmp);
+            error = rnorm / (res0 + small);
+            if (resvec) resvec[iiter] = error;
+            written = iiter + 1;
+            if (error < tol) {
+                *usediter = iiter;
+                o_copy(n, phi.data(), sol);
+                return written;
+            }
+            k = k + 1;
+            iiter = iiter + 1;
+        }
+    }
+    *usediter = iiter;
+    o_copy(n, phi.data(), sol);
+    return written;
+}
+
+/* hip/Solver/xsolver_igcr.cpp:29-108: right-preconditioned GCR(restart) with
+ * modified Gram-Schmidt; residual history is absolute with
+ * resvec[0] = ||r0|| and resvec[k+1] = ||r_k|| (hip convention);
+ * usediter = k+1 on convergence.  small = 1e-20 as in intel. */
+int orc_hip_igcr(ORC_ARGS, const double *rhs, double *sol, int restart, double tol, int maxiter,
+                 const double *sol_init, int *usediter, double *resvec)
+{
+    ORC_CTX;
+    std::vector<std::vector<double>> uk(restart, std::vector<double>(n, 0.0)), ck(restart, std::vector<double>(n, 0.0));
+    std::vector<double> res(n), phi(n);
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    double res0 = std::sqrt(o_dot(n, res.data(), res.data()));
+    if (resvec) resvec[0] = res0;
+    int written = 1;
+    *usediter = 0;
+    if (res0 == 0) { o_copy(n, phi.data(), sol); return written; }
+    int iiter = 0;
+    while (iiter < maxiter) {
+        int k = 0;
+        while (k < restart && iiter < maxiter) {
+            M.apply(res.data(), uk[k].data());
+            A.spmv(uk[k].data(), ck[k].data());
+            for (int i = 0; i < k; i++) {
+                double a = o_dot(n, ck[i].data(), ck[k].data());
+                double ma = minone * a;
+                o_axpy(n, ma, ck[i].data(), ck[k].data());
+                o_axpy(n, ma, uk[i].data(), uk[k].data());
+            }
+            double t0 = o_dot(n, ck[k].data(), ck[k].data());
+            double t1 = o_dot(n, ck[k].data(), res.data());
+            t0 = std::sqrt(t0);
+            double t = one / (t0 + small);
+            o_scal(n, t, uk[k].data());
+            o_scal(n, t, ck[k].data());
+            double tmp = t1 / (t0 + small);
+            o_axpy(n, tmp, uk[k].data(), phi.data());
+            o_axpy(n, minone * tmp, ck[k].data(), res.data());
+            double rnorm = std::sqrt(o_dot(n, res.data(), res.data()));
+            if (resvec) resvec[iiter + 1] = rnorm;
+            written = iiter + 2;
+            if (rnorm / (res0 + small) < tol) {
+                *usediter = iiter + 1;
+                o_copy(n, phi.data(), sol);
+                return written;
+            }
+            k++;
+            iiter++;
+        }
+    }
+    *usediter = iiter;
+    o_copy(n, phi.data(), sol);
+    return written;
+}
+
+/* intel/mpisolver-C-v1.cpp:1249-1279 */
+static void applyplanerotation(double &dx, double &dy, double csx, double snx)
+{
+    double t = csx * dx + snx * dy;
+    dy = -snx * dx + csx * dy;
+    dx = t;
+}
+static void generateplanerotation(double dx, double dy, double &csx, double &snx)
+{
+    if (dy == 0.0) { csx = 1.0; snx = 0.0; }
+    else if (std::fabs(dy) > std::fabs(dx)) {
+        double t = dx / dy;
+        snx = 1.0 / std::sqrt(1.0 + t * t);
+        csx = t * snx;
+    } else {
+        double t = dy / dx;
+        csx = 1.0 / std::sqrt(1.0 + t * t);
+        snx = t * csx;
+    }
+}
+/* intel/mpisolver-C-v1.cpp:1281-1301 (updatec) */
+static void updatec(double *phi, int k, const std::vector<std::vector<double>> &H, const double *s,
+                    const std::vector<std::vector<double>> &V, int n)
+{
+    std::vector<double> y(s, s + k);
+    double small = 1e-20;
+    for (int i = k - 1; i >= 0; i--) {
+        y[i] = y[i] / (H[i][i] + small);
+        for (int j = i - 1; j >= 0; j--) y[j] = y[j] - H[j][i] * y[i];
+    }
+    for (int i = 0; i < k; i++) o_axpy(n, y[i], V[i].data(), phi);
+}
+
+/*
+ * intel/mpisolver-C-v1.cpp:933-1087 (left-preconditioned GMRES(m), right = 0)
+ * and :1089-1247 (FGMRES(m), right-preconditioned, right = 1), both with
+ * modified Gram-Schmidt and Givens rotations.
+ * resvec is written with the GLOBAL iteration index j (relative residual
+ * estimate |s_{i+1}|/res0); the intel code writes it with the inner index i
+ * (so a later restart cycle overwrites it) — in the first cycle both agree.
+ * quirk = 1 reproduces the intel update with i instead of i+1 columns on
+ * convergence (:1043, :1209); quirk = 0 uses i+1.
+ */
+int orc_gmres(ORC_ARGS, const double *rhs, double *sol, int restart, double tol, int maxiter,
+              const double *sol_init, int *usediter, double *resvec, int right, int quirk)
+{
+    ORC_CTX;
+    int m = restart;
+    std::vector<std::vector<double>> V(m + 1, std::vector<double>(n, 0.0)), Z, H(m + 1, std::vector<double>(m, 0.0));
+    if (right) Z.assign(m + 1, std::vector<double>(n, 0.0));
+    std::vector<double> phi(n), res(n), w(n), s(m + 1), cs(m + 1), sn(m + 1);
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    if (!right) M.apply(res.data(), res.data());
+    double res0 = std::sqrt(o_dot(n, res.data(), res.data()));
+    double beta = res0;
+    int j = 0;
+    while (j < maxiter) {
+        for (int q = 0; q < m + 1; q++) {
+            std::fill(V[q].begin(), V[q].end(), 0.0);
+            std::fill(H[q].begin(), H[q].end(), 0.0);
+            if (right) std::fill(Z[q].begin(), Z[q].end(), 0.0);
+        }
+        std::fill(s.begin(), s.end(), 0.0);
+        std::fill(cs.begin(), cs.end(), 0.0);
+        std::fill(sn.begin(), sn.end(), 0.0);
+        double tmp = one / (beta + small);
+        o_scal(n, tmp, res.data());
+        o_copy(n, res.data(), V[0].data());
+        s[0] = beta;
+        int i = 0;
+        while (i < m && j < maxiter) {
+            if (right) {
+                M.apply(V[i].data(), Z[i].data());
+                A.spmv(Z[i].data(), w.data());
+            } else {
+                A.spmv(V[i].data(), w.data());
+                M.apply(w.data(), w.data());
+            }
+            for (int k = 0; k <= i; k++) {
+                tmp = o_dot(n, w.data(), V[k].data());
+                H[k][i] = tmp;
+                o_axpy(n, minone * tmp, V[k].data(), w.data());
+            }
+            tmp = std::sqrt(o_dot(n, w.data(), w.data()));
+            H[i + 1][i] = tmp;
+            tmp = one / (tmp + small);
+            o_scal(n, tmp, w.data());
+            o_copy(n, w.data(), V[i + 1].data());
+            for (int k = 0; k < i; k++) applyplanerotation(H[k][i], H[k + 1][i], cs[k], sn[k]);
+            generateplanerotation(H[i][i], H[i + 1][i], cs[i], sn[i]);
+            applyplanerotation(H[i][i], H[i + 1][i], cs[i], sn[i]);
+            applyplanerotation(s[i], s[i + 1], cs[i], sn[i]);
+            double error = std::fabs(s[i + 1]) / (res0 + small);
+            if (resvec) resvec[j] = error;
+            written = j + 1;
+            if (error < tol) {
+                updatec(phi.data(), quirk ? i : i + 1, H, s.data(), right ? Z : V, n);
+                *usediter = j;
+                o_copy(n, phi.data(), sol);
+                return written;
+            }
+            i = i + 1;
+            j = j + 1;
+        }
+        updatec(phi.data(), m, H, s.data(), right ? Z : V, n);
+        A.bmax(rhs, phi.data(), res.data());
+        if (!right) M.apply(res.data(), res.data());
+        beta = std::fabs(s[m]);
+        *usediter = j;
+    }
+    o_copy(n, phi.data(), sol);
+    return written;
+}
+
+/* Jacobi preconditioner vector (intel/HostMatrix.h:127-137) */
+void orc_jacobi_diag(int n, const int *rp, const int *ci, const double *v, double *dinv)
+{
+    MCSR a;
+    a.from_csr(n, rp, ci, v);
+    for (int i = 0; i < n; i++) {
+        double t = a.diag[i] + 1e-20;
+        dinv[i] = 1.0 / t;
+    }
+}
+
+/* Dependency depth (level) of each row of a strictly lower triangular
+ * pattern: level[i] = 1 + max(level[j]) over the row's columns (0 if none). */
+int orc_levels_lower(int n, const int *rp, const int *ci, int *level)
+{
+    int maxl = 0;
+    for (int i = 0; i < n; i++) {
+        int l = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) l = std::max(l, level[ci[k]] + 1);
+        level[i] = l;
+        maxl = std::max(maxl, l);
+    }
+    return maxl + 1;
+}
+
+}  // extern "C"
