@@ -1,0 +1,273 @@
+/*
+ * xsolver_b200 — B200 (sm_100a) preconditioned Krylov solve path behind the
+ * xsolver C API.
+ *
+ * Three groups of entry points, all exported with C linkage from
+ * libxsolver_b200.so:
+ *
+ *  1. The reference's setter-style API (hip/xsolver_c.h:37-49).  The
+ *     reference declares these with C++ linkage and one C++ reference
+ *     parameter (usediter); here they are extern "C" with a pointer, and
+ *     C++ callers additionally get inline forwarders with the reference's
+ *     exact signatures (same names, argument meaning and defaults).
+ *  2. The Fortran-style cpu_/gpu_ entry points of the reference's cuda/
+ *     backend (cuda/DeviceMatrix.h:121-169, cuda/mpicudasolver-C-v1.cu:165-1391,
+ *     intel/HostMatrix.h:187-222).  Their C++ reference parameters are
+ *     pointers at the ABI level; C callers pass pointers.
+ *  3. Extensions with no reference counterpart: status-returning twins,
+ *     precision control (mixed-precision iterative refinement), ParILU/ParILUT
+ *     parameters, the adjoint, and a few kernel-level calls on device
+ *     pointers used by tests and benchmarks.
+ *
+ * Errors: the reference prints and calls exit(0) on bad input; this library
+ * never exits.  Every call records a status readable with
+ * xsolver_last_error(); the xs_* twins return it directly.
+ */
+#ifndef XSOLVER_B200_C_H
+#define XSOLVER_B200_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                        */
+/* ------------------------------------------------------------------ */
+enum xs_status {
+    XS_OK = 0,
+    XS_ERR_INVALID = 1,       /* bad argument (size, pointer, string)          */
+    XS_ERR_CUDA = 2,          /* a CUDA runtime call failed                     */
+    XS_ERR_NOMEM = 3,         /* device allocation failed                       */
+    XS_ERR_NO_DIAG = 4,       /* a row has no diagonal entry (ILU/Jacobi)       */
+    XS_ERR_TRSV_TIMEOUT = 5,  /* sync-free solve gave up waiting on a row       */
+    XS_ERR_BREAKDOWN = 6,     /* Krylov breakdown (non-finite scalar)           */
+    XS_ERR_NAN = 7,           /* non-finite input or residual                   */
+    XS_ERR_ORDER = 8,         /* calls out of order (e.g. pc before ksp)        */
+    XS_ERR_ELL_WIDTH = 9,     /* ELL width outside the supported range          */
+    XS_ERR_UNSUPPORTED = 10,  /* combination not provided (e.g. ic0 on GPU)     */
+    XS_ERR_CAPACITY = 11,     /* a fixed per-row capacity was exceeded          */
+    XS_ERR_NO_GPU = 12        /* no CUDA device visible                         */
+};
+
+/* ------------------------------------------------------------------ */
+/* 1. reference setter-style API (hip/xsolver_c.h:37-49)               */
+/* ------------------------------------------------------------------ */
+
+/* hip/xsolver_c.cpp:41-102.  CSR with n rows; rowptr[0] selects 0- or
+ * 1-based indexing.  advanced_pam[3] = {distribute (must be 0: one GPU),
+ * SpMV format (0 CSR, 1 ELL), gpu (ignored: always the GPU)}.  The host
+ * arrays are borrowed and must outlive xsolver_free(), as in the reference. */
+void xsolver_mat_setup(int nInterior, int *rowptr, int *colidx, double *val, int *advanced_pam);
+/* hip/xsolver_c.cpp:103-130: "bicgstab", "cg", "igcr" (case variants as in
+ * the reference), plus "gcr", "gmres", "fgmres". */
+void xsolver_ksp_settype(char *fmt);
+/* hip/xsolver_c.cpp:131-133 */
+void xsolver_ksp_set_absolute_tol(double absolute_tol);
+/* hip/xsolver_c.cpp:134-149.  *usediter and resvec (>= maxiter+1 entries)
+ * must stay valid until xsolver_solve returns.  resvec[0] = ||r0||,
+ * resvec[k+1] = ||r_k|| (absolute), *usediter = iterations used. */
+void xsolver_ksp_setoption(double tol, int maxiter, int *usediter, double *resvec, int restart);
+/* hip/xsolver_c.cpp:150-263: "jacobi", "ilu0", "ilut" (GPU ParILUT),
+ * "ilu0_mkl"/"ilut_mkl" (mapped to ilu0/ilut as the reference does on GPU),
+ * plus "parilu" and "none".  "ic0"/"ict" record XS_ERR_UNSUPPORTED (the
+ * reference exits for them on GPU).  Must follow xsolver_ksp_settype. */
+void xsolver_pc_settype(char *fmt);
+/* hip/xsolver_c.cpp:268-273.  For "ilut": max_fill is the ParILUT fill
+ * factor, tol its drop tolerance. */
+void xsolver_pc_setilut(double tol, int max_fill);
+/* hip/xsolver_c.cpp:264-267 (IC-type preconditioners are not provided). */
+void xsolver_pc_setict(double tol, int max_fill);
+/* hip/xsolver_c.cpp:274-292.  sol holds x0 on entry, the solution on exit. */
+void xsolver_solve(double *rhs, double *sol);
+/* hip/xsolver_c.cpp:308-333 */
+void xsolver_free(void);
+
+/* status of the last call of any entry point on this thread's default handle */
+int xsolver_last_error(void);
+const char *xsolver_error_string(int status);
+
+/* ------------------------------------------------------------------ */
+/* 3a. extensions to the setter API                                    */
+/* ------------------------------------------------------------------ */
+/* Mixed precision.  outer must be "fp64".  inner "fp64" (plain FP64 solve)
+ * or "fp32" (FP64 iterative refinement around an FP32 inner solve of the
+ * selected ksp type).  factor "fp64", "fp32", "bf16" or "fp16": storage of
+ * the ILU factor values (dinv is kept in FP32/FP64). */
+void xsolver_set_precision(const char *outer, const char *inner, const char *factor);
+/* inner relative tolerance and iteration cap of the refinement's inner solve */
+void xsolver_set_inner(double inner_rtol, int inner_maxiter);
+/* ParILU sweep count (default 20, hip/Precond/precon_gpuilu0.cpp:5) */
+void xsolver_pc_setparilu(int sweeps);
+/* ParILUT: fill factor (default 3), sweeps (default 10), drop tolerance
+ * (default 0, no reference counterpart) */
+void xsolver_pc_setparilut(double fill, int sweeps, double droptol);
+/* triangular solve mode: 0 exact sync-free (default), k > 0 k Jacobi sweeps
+ * per triangle (the reference GPU path's approximate solve) */
+void xsolver_pc_set_trsv(int mode);
+/* 1 (default for the gpu_* entry points) reproduces the reference GMRES
+ * update with i instead of i+1 columns on convergence; 0 uses i+1. */
+void xsolver_set_compat(int reference_quirks);
+
+/* Adjoint of the last xsolver_solve: given dLdx (n), solve A^T lambda = dLdx
+ * with the transposed SpMV and transposed triangular solves, then
+ * dLdb = lambda and dLdA_vals[k] = -lambda_i * x_j for each stored entry
+ * k = (i, j) of A (in A's CSR order).  Any output may be NULL.
+ * The backward solve uses the forward solver type, tolerance and maxiter. */
+void xsolver_adjoint(double *dLdx, double *dLdb, double *dLdA_vals);
+
+/* ------------------------------------------------------------------ */
+/* 3b. status-returning handle API                                     */
+/* ------------------------------------------------------------------ */
+typedef struct xs_handle_s *xs_handle_t;
+
+int xs_create(xs_handle_t *h);
+int xs_destroy(xs_handle_t h);
+int xs_mat_setup(xs_handle_t h, int n, const int *rowptr, const int *colidx, const double *val, int format);
+int xs_ksp_settype(xs_handle_t h, const char *fmt);
+int xs_ksp_setoption(xs_handle_t h, double tol, int maxiter, int *usediter, double *resvec, int restart);
+int xs_ksp_set_absolute_tol(xs_handle_t h, double absolute_tol);
+int xs_pc_settype(xs_handle_t h, const char *fmt);
+int xs_pc_setilut(xs_handle_t h, double tol, int max_fill);
+int xs_pc_setparilu(xs_handle_t h, int sweeps);
+int xs_pc_setparilut(xs_handle_t h, double fill, int sweeps, double droptol);
+int xs_pc_set_trsv(xs_handle_t h, int mode);
+int xs_set_precision(xs_handle_t h, const char *outer, const char *inner, const char *factor);
+int xs_set_inner(xs_handle_t h, double inner_rtol, int inner_maxiter);
+int xs_set_compat(xs_handle_t h, int reference_quirks);
+/* host rhs/sol (sol = x0 on entry) */
+int xs_solve(xs_handle_t h, const double *rhs, double *sol);
+/* device-resident rhs/sol (device pointers, n doubles each) */
+int xs_solve_device(xs_handle_t h, const double *d_rhs, double *d_sol);
+/* nrhs independent right-hand sides stored contiguously (column i at
+ * rhs + i*n); host pointers.  usediter/resvec of the handle receive the last
+ * system's values. */
+int xs_solve_batch(xs_handle_t h, int nrhs, const double *rhs, double *sol);
+int xs_adjoint(xs_handle_t h, const double *dLdx, double *dLdb, double *dLdA_vals);
+/* batch adjoint: nrhs forward solutions (host, contiguous) and gradients */
+int xs_adjoint_batch(xs_handle_t h, int nrhs, const double *x, const double *dLdx, double *dLdb, double *dLdA_vals);
+/* timing of the last solve, in milliseconds (CUDA events around the solve
+ * on the handle's stream): setup = preconditioner construction */
+int xs_last_timing(xs_handle_t h, double *setup_ms, double *solve_ms, int *iterations, double *final_relres);
+/* number of refinement (outer) steps of the last mixed-precision solve */
+int xs_last_outer_steps(xs_handle_t h, int *outer_steps);
+
+/* ------------------------------------------------------------------ */
+/* 2. reference cuda/ + intel/ Fortran-style API                       */
+/* ------------------------------------------------------------------ */
+/* intel/HostMatrix.h:187-195 (also cuda/HostMatrix.h): "diag + off-diagonal"
+ * matrix, 0-based, borrowed host pointers.  nHalo must be 0 (one GPU). */
+void cpu_mat_setup(int *nInterior, int *nHalo, int *nSizes, double *diag_val, double *offdiag_val,
+                   int *offdiag_row_offset, int *offdiag_col_index);
+/* intel/HostMatrix.h:196-200: new values, same pattern */
+void cpu_mat_update(double *diag_val, double *offdiag_val);
+/* cuda/DeviceMatrix.h:121-126: upload the matrix set by cpu_mat_setup */
+void gpu_mat_setup(void);
+/* cuda/DeviceMatrix.h:127-144: "ELL"; num_nz in (0, 32] is rounded up to 16
+ * or 32 as in the reference (the kernel itself uses the true max row length) */
+void gpu_mat_format(char *fmt, int *num_nz);
+/* cuda/DeviceMatrix.h:145-148: re-upload values after cpu_mat_update */
+void gpu_mat_update(void);
+/* cuda/DeviceMatrix.h:149-152 */
+void gpu_mat_free(void);
+/* cuda/DeviceMatrix.h:153-158: "Jacobi", plus "ILU0", "ParILU", "ParILUT" */
+void gpu_preconditioner_setup(char *fmt);
+/* cuda/DeviceMatrix.h:159-165 */
+void gpu_preconditioner_update(char *fmt);
+/* cuda/DeviceMatrix.h:166-168 */
+void gpu_preconditioner_free(char *fmt);
+/* cuda/mpicudasolver-C-v1.cu:165 / :380 / :588.  resvec[k] = ||r_k||/||r_0||
+ * (relative, intel convention), *usediter = index of the last iteration. */
+void gpu_cg_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter, double *resvec);
+void gpu_cgm_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter, double *resvec);
+void gpu_bicgstab_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter,
+                        double *resvec);
+/* cuda/mpicudasolver-C-v1.cu:939 / :1074 / :1221 / :1391 */
+void gpu_gcr_solve(double *rhs, double *sol, int *restart, double *tol, int *maxiter, double *sol_init, int *usediter,
+                   double *resvec);
+void gpu_igcr_solve(double *rhs, double *sol, int *restart, double *tol, int *maxiter, double *sol_init, int *usediter,
+                    double *resvec);
+void gpu_gmres_solve(double *rhs, double *sol, int *restart, double *tol, int *maxiter, double *sol_init,
+                     int *usediter, double *resvec);
+void gpu_fgmres_solve(double *rhs, double *sol, int *restart, double *tol, int *maxiter, double *sol_init,
+                      int *usediter, double *resvec);
+
+/* ------------------------------------------------------------------ */
+/* 3c. kernel-level entry points on device pointers (tests/benchmarks) */
+/* ------------------------------------------------------------------ */
+/* A plan holds a device copy of a CSR matrix (and optionally its ELL form
+ * and ILU factors) with the analysis the kernels need.  All d_* pointers are
+ * device pointers; every call is ordered on the plan's stream and returns
+ * after enqueueing unless stated. */
+typedef struct xs_plan_s *xs_plan_t;
+/* copy a host CSR (0-based) to the device and analyse it */
+int xs_plan_create(xs_plan_t *p, int n, const int *rowptr, const int *colidx, const double *val);
+int xs_plan_destroy(xs_plan_t p);
+/* build the ELL form (width = max row length) */
+int xs_plan_build_ell(xs_plan_t p, int *width);
+/* y = A x (format 0 CSR, 1 ELL; precision 0 FP64, 1 FP32 values+vectors) */
+int xs_plan_spmv(xs_plan_t p, int format, int precision, const void *d_x, void *d_y);
+/* y = A^T x (FP64, CSR of A^T built on first use) */
+int xs_plan_spmv_t(xs_plan_t p, const double *d_x, double *d_y);
+/* ILU factorisation on the device: kind 0 exact ILU(0) (sync-free, same
+ * operation order as the reference CPU ILU(0)), 1 ParILU (sweeps),
+ * 2 ParILUT (fill, sweeps, droptol) */
+int xs_plan_factor(xs_plan_t p, int kind, int sweeps, double fill, double droptol);
+/* copy the factors to the host in the seqilu0 layout (L strict lower, dinv,
+ * U' = dinv-row-scaled strict upper).  Pass NULL arrays to query nnzL/nnzU. */
+int xs_plan_get_factors(xs_plan_t p, int *nnzL, int *nnzU, int *lrp, int *lci, double *lv, double *dinv, int *urp,
+                        int *uci, double *uv);
+/* combined LU values over A's pattern (exact ILU(0) / ParILU only) */
+int xs_plan_get_lu_values(xs_plan_t p, double *luv);
+/* factor storage precision for the solves below: 0 FP64, 1 FP32, 2 BF16, 3 FP16 */
+int xs_plan_set_factor_precision(xs_plan_t p, int prec);
+/* z = (L D U')^{-1} x with sync-free solves (vec_prec 0 FP64 / 1 FP32) */
+int xs_plan_lusolve(xs_plan_t p, int vec_prec, const void *d_x, void *d_z);
+/* z = (L D U')^{-T} x */
+int xs_plan_lusolve_t(xs_plan_t p, const double *d_x, double *d_z);
+/* wait for the plan's stream; returns the device status word (e.g. a
+ * sync-free timeout) */
+int xs_plan_sync(xs_plan_t p);
+/* number of dependency levels of L and U */
+int xs_plan_levels(xs_plan_t p, int *levelsL, int *levelsU);
+/* average device time in ms of `reps` repetitions of op (0 CSR SpMV FP64,
+ * 1 ELL SpMV FP64, 2 CSR SpMV FP32, 3 L solve, 4 U solve, 5 LU solve,
+ * 6 ELL SpMV FP32) on internal buffers, timed with CUDA events on the plan's
+ * stream; flushes L2 between repetitions when flush_l2 != 0 */
+int xs_plan_time_op(xs_plan_t p, int op, int reps, int flush_l2, double *ms);
+/* algorithmic bytes of op (counted once per array element) */
+int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes);
+
+/* Host-only dependency analysis of a strictly triangular CSR pattern (no
+ * GPU needed): level[i] = 1 + max level of the rows row i depends on, perm =
+ * rows sorted by (level, row) — the position order of the sync-free solve. */
+int xs_tri_levels(int n, const int *rowptr, const int *colidx, int upper, int *level, int *perm, int *nlevels);
+
+/* library identification */
+const char *xs_version(void);
+int xs_device_count(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+
+/* C++ forwarders with the reference's exact signatures */
+inline void xsolver_ksp_setoption(double tol, int maxiter, int &usediter, double *resvec, int restart = 0)
+{
+    xsolver_ksp_setoption(tol, maxiter, &usediter, resvec, restart);
+}
+#endif
+
+#endif /* XSOLVER_B200_C_H */

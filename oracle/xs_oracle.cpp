@@ -439,16 +439,19 @@ int orc_split_lu(int n, const int *rp, const int *ci, const double *luv,
 
 /* ========================= ParILUT ========================= */
 /*
- * Restatement of parilut_clean (hip/Precond/parilut.cpp:621-1206) with
- * synchronous sweeps.  Per sweep s = 0..sweeps-1:
+ * ParILUT after parilut_clean (hip/Precond/parilut.cpp:621-1206: candidate
+ * generation from A - L*U, a sweep over all entries, threshold removal to a
+ * growing fill budget, then separate L and U sweeps), restated with
+ * SYNCHRONOUS sweeps.  Per sweep s = 0..sweeps-1:
  *   rate = (fill - 1)/sweeps*(s+1) + 1                          (:692)
- *   R = A - L*U over pattern(A) u pattern(L*U); each entry formed as
- *       c = -a_ij; c += l_ik*u_kj for k ascending; r = -c     (:730-744)
- *   D: lower entries r_ij / u_jj, upper entries r_ij, then every entry in
- *       A's pattern reset to a_ij                            (embedA_intoB_L2/U2)
- *   L = strict lower(D) + unit diag (last), U = upper(D) (CSC, diag last)
+ *   candidates = pattern(A) u pattern(L*U);  R = A - L*U with each entry
+ *       formed as c = -a_ij; c += l_ik*u_kj for k ascending; r = -c
+ *       (the reference's multiply-add then negate, :730-744)
+ *   entries already in L or U keep their current value; new entries get
+ *       l_ij = r_ij / u_jj (lower) or u_ij = r_ij (upper)
+ *   L = strict lower + unit diag (last), U = upper (CSC, diag last)
  *   one sweep over all L (off-diagonal) and U entries          (LU_sweep)
- *   if nnz(D) - round(rate*nnz(A)) > 0: for L and for U separately keep
+ *   if nnz(cand) - round(rate*nnz(A)) > 0: for L and for U separately keep
  *       keep = (int)(rate*nnz0) entries: thr = remove-th smallest |v|
  *       (remove = max(nnz - keep, 0), 1-based; entries incl. diagonal),
  *       drop non-diagonal entries with |v| < thr                (:1000-1090)
@@ -456,6 +459,14 @@ int orc_split_lu(int n, const int *rp, const int *ci, const double *luv,
  *       off-diagonal l_ij with |l_ij| < droptol and u_ij with
  *       |u_ij| < droptol*|u_jj|
  *   L sweep, then U sweep (using the new L)                    (:1110-1150)
+ * Initial factors: l_ij = a_ij / a_jj (strict lower), U = upper(A).
+ * Two departures from the reference, both needed because the sweeps here are
+ * synchronous (deterministic) rather than asynchronous in place: the
+ * reference starts from the unscaled lower triangle and resets every entry of
+ * A's pattern to a_ij before each sweep (embedA_intoB_L2/U2); with
+ * synchronous sweeps that reset diverges on convection-dominated matrices, so
+ * existing entries keep their values, as in the published ParILUT algorithm
+ * (Anzt, Chow, Dongarra, SIAM J. Sci. Comput. 40(4), 2018).
  * Result: L (CSR, strict lower, unit diag implicit), dinv = 1/u_ii, and
  * U' = dinv_i * u_ij (CSR strict upper, row-scaled) — the seqilu0 layout.
  * Output arrays are allocated with malloc; free with orc_free.
@@ -474,13 +485,18 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
     L.n = U.n = n;
     L.rp.assign(n + 1, 0);
     U.rp.assign(n + 1, 0);
+    std::vector<double> adiag(n, 0.0);
     for (int i = 0; i < n; i++) {
         bool hasdiag = false;
-        for (int k = arp[i]; k < arp[i + 1]; k++) {
-            if (aci[k] < i) { L.ci.push_back(aci[k]); L.v.push_back(av[k]); }
-            else { U.ci.push_back(aci[k]); U.v.push_back(av[k]); if (aci[k] == i) hasdiag = true; }
-        }
+        for (int k = arp[i]; k < arp[i + 1]; k++)
+            if (aci[k] == i) { adiag[i] = av[k]; hasdiag = true; }
         if (!hasdiag) return -1;
+    }
+    for (int i = 0; i < n; i++) {
+        for (int k = arp[i]; k < arp[i + 1]; k++) {
+            if (aci[k] < i) { L.ci.push_back(aci[k]); L.v.push_back(av[k] / adiag[aci[k]]); }
+            else { U.ci.push_back(aci[k]); U.v.push_back(av[k]); }
+        }
         L.ci.push_back(i); L.v.push_back(1.0);
         L.rp[i + 1] = (int)L.ci.size();
         U.rp[i + 1] = (int)U.ci.size();
@@ -507,32 +523,34 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
             }
             std::sort(cols.begin(), cols.end());
             cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+            int pl = L.rp[i], pu = U.rp[i];
             for (int j : cols) {
-                /* c = -a_ij + sum_k l_ik u_kj (k ascending, k <= min(i,j)) */
-                double c = -find_in_row(A, i, j);
-                int il = L.rp[i], iu = Uc.rp[j];
-                while (il < L.rp[i + 1] && iu < Uc.rp[j + 1]) {
-                    int lj = L.ci[il], ui = Uc.ci[iu];
-                    if (lj == ui) { c += L.v[il] * Uc.v[iu]; il++; iu++; }
-                    else if (lj < ui) il++;
-                    else iu++;
-                }
-                double r = -c;
+                /* existing entries keep their value */
+                while (pl < L.rp[i + 1] && L.ci[pl] < j) pl++;
+                while (pu < U.rp[i + 1] && U.ci[pu] < j) pu++;
                 double d;
-                if (j < i) d = r / udiag[j];
-                else d = r;
+                if (j < i && pl < L.rp[i + 1] && L.ci[pl] == j) d = L.v[pl];
+                else if (j >= i && pu < U.rp[i + 1] && U.ci[pu] == j) d = U.v[pu];
+                else {
+                    /* c = -a_ij + sum_k l_ik u_kj (k ascending, k <= min(i,j)) */
+                    double c = -find_in_row(A, i, j);
+                    int il = L.rp[i], iu = Uc.rp[j];
+                    while (il < L.rp[i + 1] && iu < Uc.rp[j + 1]) {
+                        int lj = L.ci[il], ui = Uc.ci[iu];
+                        if (lj == ui) { c += L.v[il] * Uc.v[iu]; il++; iu++; }
+                        else if (lj < ui) il++;
+                        else iu++;
+                    }
+                    double r = -c;
+                    d = (j < i) ? r / udiag[j] : r;
+                }
                 D.ci.push_back(j);
                 D.v.push_back(d);
-            }
-            /* reset A-pattern entries to a_ij */
-            int p = D.rp[i];
-            for (int k = arp[i]; k < arp[i + 1]; k++) {
-                while (D.ci[p] < aci[k]) p++;
-                D.v[p] = av[k];
             }
             D.rp[i + 1] = (int)D.ci.size();
         }
         long nnzD = D.rp[n];
+        if (getenv("ORC_DEBUG")) fprintf(stderr, "sweep %d rate %g nnzD %ld L %d U %d\n", s, rate, nnzD, L.rp[n], U.rp[n]);
         /* split */
         CSR L2, U2;
         L2.n = U2.n = n;
@@ -586,6 +604,7 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
                 long uremove = std::max((long)U2c.rp[n] - ukeep, 0L);
                 lthr = kth_smallest_abs(L2.v, lremove);
                 uthr = kth_smallest_abs(U2c.v, uremove);
+                if (getenv("ORC_DEBUG")) fprintf(stderr, "  lremove %ld lthr %g uremove %ld uthr %g (nL %d nU %d)\n", lremove, lthr, uremove, uthr, L2.rp[n], U2c.rp[n]);
             }
             L3.n = U3c.n = n;
             L3.rp.assign(n + 1, 0);
@@ -658,6 +677,7 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
             if (U.ci[k] > i) { uci[pu] = U.ci[k]; uv[pu] = U.v[k] * dinv[i]; pu++; }
         urp[i + 1] = (int)pu;
     }
+    if (getenv("ORC_DEBUG")) fprintf(stderr, "final nl %ld nu %ld L %d U %d\n", pl, pu, L.rp[n], U.rp[n]);
     *lrp_o = lrp; *lci_o = lci; *lv_o = lv; *dinv_o = dinv; *urp_o = urp; *uci_o = uci; *uv_o = uv;
     return 0;
 }

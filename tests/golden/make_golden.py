@@ -1,0 +1,67 @@
+"""Generate the golden fixtures in this directory from the reference's own
+CPU code, compiled from its sources by oracle/Makefile into oracle/_ref:
+
+  krylov_jacobi.npz   intel/ cpu_{cg,cgm,bicgstab,gcr,igcr,gmres,fgmres}_solve
+                      (Jacobi, the only preconditioner intel/ has) on small
+                      seeded stencil systems: matrix, rhs, solution, resvec,
+                      usediter.
+  ilu0.npz            hip ilu0_simple (hip/Precond/ilut_diag_in_csr.cpp:347)
+                      combined LU values on small stencil matrices.
+
+Run here (where the reference sources exist):  python tests/golden/make_golden.py
+The fixtures are committed; tests never need the reference sources.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import oracle  # noqa: E402
+from xsolver_b200 import stencils as st  # noqa: E402
+
+PROBLEMS = {
+    "p2d_5pt_24": (lambda: st.poisson2d_5pt(24), 0, -1.0, 1.0),
+    "p3d_7pt_9": (lambda: st.poisson3d_7pt(9), 1, -1.0, 1.0),
+    "cd3d_27pt_7": (lambda: st.convdiff3d_27pt(7), 2, 0.0, 1.0),
+    "vc3d_7pt_8": (lambda: st.varcoef3d_7pt(8, 3), 3, -1.0, 1.0),
+}
+METHODS = ["cg", "cgm", "bicgstab", "gcr", "igcr", "gmres", "fgmres"]
+
+
+def main():
+    oracle.build(ref=True)
+    if oracle.ref_intel() is None:
+        raise SystemExit("reference not built (needs the reference sources)")
+    kr = {}
+    for name, (gen, seed, lo, hi) in PROBLEMS.items():
+        A = gen()
+        b = st.rhs_uniform(A.n, seed, lo, hi)
+        kr[f"{name}/rowptr"] = A.rowptr
+        kr[f"{name}/colidx"] = A.colidx
+        kr[f"{name}/val"] = A.val
+        kr[f"{name}/rhs"] = b
+        for m in METHODS:
+            sym = name.startswith(("p2d", "p3d", "vc3d"))
+            if m in ("cg", "cgm") and not sym:
+                continue
+            x, rv, used = oracle.ref_solve(m, A, b, tol=1e-9, maxiter=400, restart=20)
+            kr[f"{name}/{m}/x"] = x
+            kr[f"{name}/{m}/resvec"] = rv
+            kr[f"{name}/{m}/usediter"] = np.array(used)
+    np.savez_compressed(os.path.join(HERE, "krylov_jacobi.npz"), **kr)
+    il = {}
+    for name, (gen, _, _, _) in PROBLEMS.items():
+        A = gen()
+        il[f"{name}/rowptr"] = A.rowptr
+        il[f"{name}/colidx"] = A.colidx
+        il[f"{name}/val"] = A.val
+        il[f"{name}/luv"] = oracle.ref_ilu0_values(A)
+    np.savez_compressed(os.path.join(HERE, "ilu0.npz"), **il)
+    print("wrote", sorted(os.listdir(HERE)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,56 @@
+"""Build libxsolver_b200.so in-tree with nvcc for sm_100a.
+
+    python -m xsolver_b200.build            # build if sources are newer
+    python -m xsolver_b200.build --force
+
+The library is a single translation unit (csrc/xs_api.cu includes the kernel
+headers).  It is compiled without FMA contraction (-fmad=false) so that the
+FP64 triangular solves and ILU(0) reproduce the CPU reference bit for bit;
+the FP32 kernels request fused multiply-adds explicitly where they want them.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libxsolver_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
+    "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fvisibility=hidden",
+]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+                  + [os.path.join(HERE, "..", "include", "xsolver_c.h")])
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(s) > t for s in sources())
+
+
+def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    if not force and not needs_build():
+        return LIB
+    cmd = [NVCC, *FLAGS, *(extra or []), "-o", LIB + ".tmp", os.path.join(CSRC, "xs_api.cu"), "-lcudart"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else None)

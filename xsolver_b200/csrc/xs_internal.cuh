@@ -1,0 +1,341 @@
+// Internal definitions shared by the xsolver_b200 CUDA sources.
+//
+// Conventions
+//  * Matrices are CSR, 0-based, int32 indices, sorted columns, stored on the
+//    device; rows are the reference's "cells" (nInterior).
+//  * Every reduction uses a fixed grid and a fixed element->block mapping, and
+//    the last block to finish (ticket counter) sums the per-block partials in
+//    block order, so results are run-to-run deterministic.
+//  * Scalars of a Krylov iteration (alpha, beta, omega, residual norms,
+//    convergence flag) live in device memory (KState) and never travel to the
+//    host inside the iteration loop.
+//  * Every spin-wait in a kernel is bounded; on expiry the kernel records an
+//    error in the device status word and returns.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+#include <cstdio>
+
+#include "../../include/xsolver_c.h"
+
+namespace xs {
+
+// ---------------------------------------------------------------- errors
+struct CudaError {
+    cudaError_t err;
+};
+
+#define XS_CUDA(call)                                                                            \
+    do {                                                                                         \
+        cudaError_t _e = (call);                                                                 \
+        if (_e != cudaSuccess) {                                                                 \
+            if (getenv("XS_DEBUG")) fprintf(stderr, "xsolver_b200: %s failed: %s (%s:%d)\n", #call, \
+                                            cudaGetErrorString(_e), __FILE__, __LINE__);         \
+            throw ::xs::Status(_e == cudaErrorMemoryAllocation ? XS_ERR_NOMEM : XS_ERR_CUDA);    \
+        }                                                                                        \
+    } while (0)
+
+struct Status {
+    int code;
+    explicit Status(int c) : code(c) {}
+};
+
+inline void check_launch()
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        if (getenv("XS_DEBUG")) fprintf(stderr, "xsolver_b200: launch failed: %s\n", cudaGetErrorString(e));
+        throw Status(XS_ERR_CUDA);
+    }
+}
+
+// ---------------------------------------------------------------- device buffers
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    DBuf(DBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf &operator=(DBuf &&o) noexcept
+    {
+        if (this != &o) { free(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DBuf() { free(); }
+    // pad: extra elements allocated (and zeroed) past n, e.g. for aligned bulk copies
+    void alloc(size_t count, size_t pad = 0)
+    {
+        free();
+        size_t bytes = (count + pad) * sizeof(T);
+        if (bytes == 0) bytes = 16;
+        XS_CUDA(cudaMalloc((void **)&p, bytes));
+        XS_CUDA(cudaMemset(p, 0, bytes));
+        n = count;
+    }
+    void free()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void upload(const T *h, size_t count, cudaStream_t s)
+    {
+        XS_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void download(T *h, size_t count, cudaStream_t s) const
+    {
+        XS_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+    }
+    operator T *() const { return p; }
+};
+
+// ---------------------------------------------------------------- device status
+// status word bits written by kernels (device side), read by the host after a
+// synchronisation point
+enum DevErr : int {
+    DEV_OK = 0,
+    DEV_TRSV_TIMEOUT = 1,
+    DEV_BREAKDOWN = 2,
+    DEV_NAN = 4,
+    DEV_TMA_TIMEOUT = 8,
+    DEV_CAPACITY = 16,
+    DEV_FACTOR_TIMEOUT = 32
+};
+
+inline int dev_err_to_status(int e)
+{
+    if (e & (DEV_TRSV_TIMEOUT | DEV_FACTOR_TIMEOUT | DEV_TMA_TIMEOUT)) return XS_ERR_TRSV_TIMEOUT;
+    if (e & DEV_CAPACITY) return XS_ERR_CAPACITY;
+    if (e & DEV_NAN) return XS_ERR_NAN;
+    if (e & DEV_BREAKDOWN) return XS_ERR_BREAKDOWN;
+    return XS_OK;
+}
+
+// ---------------------------------------------------------------- Krylov state
+// Scalar slots used by the solver bodies (indices into KState::sc)
+constexpr int KS_SLOTS = 48;
+
+struct KState {
+    double sc[KS_SLOTS];  // method-defined scalars
+    double res0;          // initial residual norm (the method's own norm)
+    double rnorm;         // latest residual norm
+    double tol;           // relative tolerance
+    double abstol;        // absolute tolerance (hip: resl <= absolute_tol)
+    int iter;             // iterations completed
+    int maxiter;
+    int done;             // 0 running, 1 converged, 2 maxiter, 3 breakdown/error
+    int err;              // DevErr bits
+    int conv_inner;       // GMRES/GCR: inner index at convergence
+    int kcols;            // GMRES: columns used by the final update
+    int finalized;        // GMRES: final update applied
+    int cycle_i;          // GMRES/GCR: inner index inside the current cycle
+    double *hist;         // device history: hist[0] = res0, hist[k+1] = after iteration k
+    double *hist_rel;     // device history, method's relative residual per iteration (intel convention)
+};
+
+// ---------------------------------------------------------------- launch geometry
+struct Geom {
+    int sms = 148;
+    int red_grid = 592;  // fixed grid for reductions: 4 blocks per SM
+    int red_block = 256;
+};
+Geom &geom();
+
+// ---------------------------------------------------------------- sentinel values
+// The sync-free triangular solves signal "row ready" through the value
+// itself: a solve buffer holds a NaN bit pattern that IEEE arithmetic never
+// produces (GPU arithmetic yields the canonical NaN 0x7fff...), and a row is
+// ready once its value differs from that pattern.
+__host__ __device__ constexpr uint64_t sentinel_bits64() { return 0x7ff4dead5e17e1a1ull; }
+__host__ __device__ constexpr uint32_t sentinel_bits32() { return 0x7fa5e17eu; }
+
+template <typename V>
+struct Sentinel;
+template <>
+struct Sentinel<double> {
+    __device__ static double value() { return __longlong_as_double((long long)sentinel_bits64()); }
+    __device__ static bool is(double v) { return (uint64_t)__double_as_longlong(v) == sentinel_bits64(); }
+};
+template <>
+struct Sentinel<float> {
+    __device__ static float value() { return __int_as_float((int)sentinel_bits32()); }
+    __device__ static bool is(float v) { return (uint32_t)__float_as_int(v) == sentinel_bits32(); }
+};
+
+// relaxed, L1-bypassing accesses for values other SMs write while we poll
+__device__ __forceinline__ double ld_poll(const double *p)
+{
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ float ld_poll(const float *p)
+{
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_publish(double *p, double v)
+{
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_publish(float *p, float v)
+{
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// ---------------------------------------------------------------- factor value types
+template <typename T>
+struct FVal;
+template <>
+struct FVal<double> {
+    __device__ static double ld(const double *p, long i) { return __ldg(p + i); }
+};
+template <>
+struct FVal<float> {
+    __device__ static float ld(const float *p, long i) { return __ldg(p + i); }
+};
+template <>
+struct FVal<__nv_bfloat16> {
+    __device__ static float ld(const __nv_bfloat16 *p, long i) { return __bfloat162float(p[i]); }
+};
+template <>
+struct FVal<__half> {
+    __device__ static float ld(const __half *p, long i) { return __half2float(p[i]); }
+};
+
+// ---------------------------------------------------------------- deterministic reductions
+// One "reduction slot": per-block partials for K values and a ticket counter.
+struct RedSlot {
+    double *part;      // [K][grid]
+    unsigned *ticket;  // single counter, reset by the last block
+};
+
+template <int K>
+__device__ __forceinline__ void warp_sum(double (&v)[K])
+{
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+}
+
+// Reduce v[K] over the block, publish the block partial, and let the last
+// block (in ticket order) sum all partials in block order.  Returns true in
+// every thread of the last block; the totals are then in tot[K] (shared).
+// blockDim.x must be a multiple of 32 and <= 1024.
+template <int K>
+__device__ bool block_reduce_publish(double (&v)[K], RedSlot slot, double *tot /*shared, >= K*/)
+{
+    __shared__ double sred[32][K > 0 ? K : 1];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    warp_sum<K>(v);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) sred[wid][k] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int G = gridDim.x;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double s = 0.0;
+            for (int w = 0; w < nw; w++) s += sred[w][k];
+            slot.part[(long)k * G + blockIdx.x] = s;
+        }
+        __threadfence();
+        unsigned t = atomicAdd(slot.ticket, 1u);
+        s_last = (t == (unsigned)G - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    // last block: sum partials in fixed order
+    const int G = gridDim.x;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < G; b += blockDim.x) s += __ldcg(slot.part + (long)k * G + b);
+        v[k] = s;
+    }
+    warp_sum<K>(v);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) sred[wid][k] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double s = 0.0;
+            for (int w = 0; w < nw; w++) s += sred[w][k];
+            tot[k] = s;
+        }
+        *slot.ticket = 0u;
+    }
+    __syncthreads();
+    return true;
+}
+
+// ---------------------------------------------------------------- CSR / plans
+struct DevCsr {
+    int n = 0;
+    long nnz = 0;
+    const int *rp = nullptr;
+    const int *ci = nullptr;
+    const double *v = nullptr;
+    const float *v32 = nullptr;
+};
+
+// Row-block tiling of a CSR matrix for the staged SpMV kernel.  Block b covers
+// rows [rb[b], rb[b+1]); its entries are copied to shared memory by one bulk
+// copy of the 16-byte aligned range that contains them.
+struct SpmvTiling {
+    int nblocks = 0;
+    int max_rows = 0;      // rows per block (<= threads per block)
+    int cap = 0;           // max entries staged per block (aligned range)
+    DBuf<int> rb;          // nblocks+1 row boundaries
+    DBuf<int> longrow;     // 1 if the block is a single row longer than cap
+};
+
+struct DevEll {
+    int n = 0, w = 0;
+    const int *ci = nullptr;     // [w][n] column-major
+    const double *v = nullptr;   // [w][n]
+    const float *v32 = nullptr;  // [w][n]
+};
+
+// A triangular factor prepared for the sync-free solve: rows permuted into
+// dependency-level order ("positions"), each position's entries stored
+// contiguously in the order the row sum is accumulated.
+template <typename FT>
+struct TriPlan {
+    int n = 0;
+    long nnz = 0;
+    int nlevels = 0;
+    const int *perm = nullptr;  // position -> row
+    const int *prp = nullptr;   // position row pointer (n+1)
+    const int *pci = nullptr;   // dependency row of each entry
+    const FT *pv = nullptr;     // entry values
+    const void *dinv = nullptr; // per position (U solve only): double or float
+};
+
+}  // namespace xs

@@ -1,0 +1,597 @@
+// Krylov iteration bodies with device-resident scalars.
+//
+// The reference drives every iteration from the host and reads each dot
+// product back (rocBLAS/cuBLAS ddot into a host double: DeviceVector.h:139-153,
+// cuda/mpicudasolver-C-v1.cu), i.e. >= 5 host synchronisations per BiCGSTAB
+// iteration.  Here one iteration is a short fixed sequence of fused kernels:
+// every dot product is accumulated inside the kernel that produces or reads
+// its operands (SpMV epilogue or vector update), reduced deterministically,
+// and the last block computes the next scalars (alpha, beta, omega, ...) and
+// the convergence test directly into KState.  Iterations are captured once
+// into a CUDA graph (a chunk of several iterations) and replayed; every
+// kernel exits immediately once KState::done is set, and the host polls the
+// done flag once per chunk, one chunk behind, so the GPU never idles.
+//
+// Scalar recurrences follow the reference loops operation for operation
+// (intel/mpisolver-C-v1.cpp with small = 1e-20), so the FP64 residual
+// history matches the CPU reference to rounding:
+//   cgm       (PCG)                      :193-272   (= hip/Solver/xsolver_cg.cpp:17-74)
+//   cg        (CG on M^-1 A, left)        :26-102
+//   bicgstab  (right preconditioned)      :365-482   (x updated with M^-1 p, M^-1 s as
+//                                                     hip/Solver/xsolver_bicgstab.cpp:20-124)
+//   gcr/igcr  (left, CGS / MGS)           :685-931
+//   hip igcr  (right, MGS)                hip/Solver/xsolver_igcr.cpp:29-108
+//   gmres     (left, MGS, Givens)         :933-1087, fgmres (right) :1089-1247
+#pragma once
+#include "xs_internal.cuh"
+#include "xs_spmv.cuh"
+#include "xs_precond.cuh"
+
+namespace xs {
+
+constexpr double KSMALL = 1e-20;
+
+// ---------------------------------------------------------------- generic vector-op kernel
+template <class Op>
+__global__ void __launch_bounds__(256) k_vecop(Op op, RedSlot slot)
+{
+    constexpr int KK = Op::K > 0 ? Op::K : 1;
+    __shared__ double tot[KK];
+    if (op.st->done) return;
+    Op o = op;
+    o.load();
+    double acc[KK];
+#pragma unroll
+    for (int k = 0; k < KK; k++) acc[k] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) o.elem(i, acc);
+    if (Op::K > 0) {
+        if (block_reduce_publish<KK>(acc, slot, tot)) {
+            if (threadIdx.x == 0) o.finalize(tot);
+        }
+    }
+}
+
+template <class Op>
+inline void vecop(const Op &op, RedSlot slot, cudaStream_t s)
+{
+    k_vecop<Op><<<geom().red_grid, 256, 0, s>>>(op, slot);
+    check_launch();
+}
+
+// single-thread scalar step
+template <class F>
+__global__ void k_scalar(F f)
+{
+    f();
+}
+
+// convergence bookkeeping shared by all methods (last block, thread 0)
+//   resl: new residual norm of the method; writes hist / hist_rel, advances
+//   iter, sets done.  Returns true if iteration continues.
+__device__ inline bool record_and_test(KState *st, double resl)
+{
+    const double rsm = resl / (st->res0 + KSMALL);
+    const int it = st->iter;
+    st->rnorm = resl;
+    if (st->hist) st->hist[it + 1] = resl;
+    if (st->hist_rel) st->hist_rel[it] = rsm;
+    st->iter = it + 1;
+    if (!isfinite(resl)) {
+        st->err |= DEV_NAN;
+        st->done = 3;
+        return false;
+    }
+    if (rsm < st->tol || resl <= st->abstol) {
+        st->done = 1;
+        return false;
+    }
+    if (st->iter >= st->maxiter) {
+        st->done = 2;
+        return false;
+    }
+    return true;
+}
+
+__device__ inline void init_record(KState *st, double res0)
+{
+    st->res0 = res0;
+    st->rnorm = res0;
+    st->iter = 0;
+    if (st->hist) st->hist[0] = res0;
+    if (!isfinite(res0)) {
+        st->err |= DEV_NAN;
+        st->done = 3;
+    } else if (res0 == 0.0 || res0 <= st->abstol || st->maxiter <= 0) {
+        st->done = 1;
+    } else {
+        st->done = 0;
+    }
+}
+
+// ---------------------------------------------------------------- SpMV epilogues with state
+// y = A x;  acc0 += w[r] * y   (w may be y's own partner vector)
+template <typename VT>
+struct EpiDot1 {
+    static constexpr int K = 1;
+    KState *st;
+    const VT *w;
+    int slot_out;  // sc[slot_out] = dot
+    int mode;      // finalize action (method specific)
+    __device__ bool active() const { return st->done == 0; }
+    __device__ VT out(int, double ax) const { return (VT)ax; }
+    __device__ void acc(int r, double y, double (&a)[1]) const { a[0] += (double)w[r] * y; }
+    __device__ void finalize(const double *tot) const;
+};
+
+// y = A x; acc0 += w0[r]*y, acc1 += y*y
+template <typename VT>
+struct EpiDot2 {
+    static constexpr int K = 2;
+    KState *st;
+    const VT *w0;
+    int mode;
+    __device__ bool active() const { return st->done == 0; }
+    __device__ VT out(int, double ax) const { return (VT)ax; }
+    __device__ void acc(int r, double y, double (&a)[2]) const
+    {
+        a[0] += y * (double)w0[r];
+        a[1] += y * y;
+    }
+    __device__ void finalize(const double *tot) const;
+};
+
+// finalize modes
+enum EpiMode {
+    M_CGM_SIGMA = 1,      // alpha = tao/(sigma+small); taoo = tao
+    M_BICG_GAMA = 2,      // gama = beta/(tmp+small)
+    M_BICG_ALPHA = 3,     // alpha = t0/(t1+small)
+    M_CG_SIGMA = 4,       // cg (left): alpha = taoo/(sigma+small)
+    M_STORE = 5           // sc[slot_out] = dot
+};
+
+// slot layout
+enum {
+    S_TAO = 0, S_TAOO, S_ALPHA, S_BETA, S_SIGMA, S_OMEGA, S_GAMA, S_BETO, S_T0, S_T1, S_TMP, S_RES0SQ,
+    S_GCR_T0 = 12, S_GCR_T1, S_GCR_INV, S_GCR_COEF,
+    S_H = 16  // GCR alpha[] (classical GS) stored from here (up to 32)
+};
+
+template <typename VT>
+__device__ void EpiDot1<VT>::finalize(const double *tot) const
+{
+    double d = tot[0];
+    if (mode == M_CGM_SIGMA) {
+        st->sc[S_SIGMA] = d;
+        st->sc[S_ALPHA] = st->sc[S_TAO] / (d + KSMALL);
+    } else if (mode == M_CG_SIGMA) {
+        st->sc[S_SIGMA] = d;
+        st->sc[S_ALPHA] = st->sc[S_TAOO] / (d + KSMALL);
+    } else if (mode == M_BICG_GAMA) {
+        st->sc[S_TMP] = d;
+        st->sc[S_GAMA] = st->sc[S_BETA] / (d + KSMALL);
+    } else {
+        st->sc[slot_out] = d;
+    }
+    if (!isfinite(d)) {
+        st->err |= DEV_BREAKDOWN;
+        st->done = 3;
+    }
+}
+template <typename VT>
+__device__ void EpiDot2<VT>::finalize(const double *tot) const
+{
+    if (mode == M_BICG_ALPHA) {
+        st->sc[S_T0] = tot[0];
+        st->sc[S_T1] = tot[1];
+        st->sc[S_ALPHA] = tot[0] / (tot[1] + KSMALL);
+    }
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) {
+        st->err |= DEV_BREAKDOWN;
+        st->done = 3;
+    }
+}
+
+// y = A x, skipped once the solve is done
+template <typename VT>
+struct EpiActive {
+    static constexpr int K = 0;
+    KState *st;
+    __device__ bool active() const { return st->done == 0; }
+    __device__ VT out(int, double ax) const { return (VT)ax; }
+    __device__ void acc(int, double, double (&)[1]) const {}
+    __device__ void finalize(const double *) const {}
+};
+// y = b - A x, skipped once the solve is done
+template <typename VT>
+struct EpiResidActive {
+    static constexpr int K = 0;
+    KState *st;
+    const VT *b;
+    __device__ bool active() const { return st->done == 0; }
+    __device__ VT out(int r, double ax) const { return (VT)((double)b[r] - ax); }
+    __device__ void acc(int, double, double (&)[1]) const {}
+    __device__ void finalize(const double *) const {}
+};
+
+// r = b - A x, acc0 += r*r, acc1 += r*w (w optional)
+template <typename VT>
+struct EpiResid {
+    static constexpr int K = 1;
+    KState *st;
+    const VT *b;
+    __device__ bool active() const { return true; }
+    __device__ VT out(int r, double ax) const { return (VT)((double)b[r] - ax); }
+    __device__ void acc(int r, double y, double (&a)[1]) const { a[0] += y * y; }
+    __device__ void finalize(const double *tot) const { st->sc[S_RES0SQ] = tot[0]; }
+};
+
+// ---------------------------------------------------------------- vector ops
+// Each op: fields n, st; load() reads scalars; elem(i, acc); finalize(tot).
+
+// PCG init: acc0 = r.r, acc1 = r.z ; p = z
+template <typename VT>
+struct OpCgmInit {
+    static constexpr int K = 2;
+    int n;
+    KState *st;
+    const VT *r, *z;
+    VT *p;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[2]) const
+    {
+        const VT ri = r[i], zi = z[i];
+        a[0] += (double)ri * (double)ri;
+        a[1] += (double)ri * (double)zi;
+        p[i] = zi;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        st->sc[S_TAO] = t[1];
+        init_record(st, sqrt(t[0]));
+    }
+};
+
+// x += alpha p ; r -= alpha Ap ; acc0 = r.r (convergence)
+template <typename VT>
+struct OpCgmUpdate {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    VT *x, *r;
+    const VT *p, *Ap;
+    VT alpha;
+    __device__ void load() { alpha = (VT)st->sc[S_ALPHA]; }
+    __device__ void elem(int i, double (&a)[1]) const
+    {
+        const VT minalpha = -alpha;
+        x[i] = x[i] + alpha * p[i];
+        const VT ri = r[i] + minalpha * Ap[i];
+        r[i] = ri;
+        a[0] += (double)ri * (double)ri;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        // pcg tests convergence after the p update; the value is the same
+        // r.r, so test here and skip the rest of the iteration when done
+        record_and_test(st, sqrt(t[0]));
+    }
+};
+
+// tao = r.z ; beta = tao/(taoo + small)  then p = beta p + z  (two ops: the
+// dot must complete before p can be updated)
+template <typename VT>
+struct OpDotRZ {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    const VT *r, *z;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[1]) const { a[0] += (double)r[i] * (double)z[i]; }
+    __device__ void finalize(const double *t) const
+    {
+        st->sc[S_TAOO] = st->sc[S_TAO];
+        st->sc[S_TAO] = t[0];
+        st->sc[S_BETA] = t[0] / (st->sc[S_TAOO] + KSMALL);
+        if (!isfinite(t[0])) { st->err |= DEV_BREAKDOWN; st->done = 3; }
+    }
+};
+template <typename VT>
+struct OpPUpdate {  // p = beta*p + z
+    static constexpr int K = 0;
+    int n;
+    KState *st;
+    VT *p;
+    const VT *z;
+    VT beta;
+    __device__ void load() { beta = (VT)st->sc[S_BETA]; }
+    __device__ void elem(int i, double (&)[1]) const
+    {
+        const VT t = beta * p[i];
+        p[i] = t + z[i];
+    }
+    __device__ void finalize(const double *) const {}
+};
+
+// ---- left CG (cg): res = M^-1(b - Ax) ; res0 = ||res||, taoo = res0^2 ; p = res
+template <typename VT>
+struct OpCgInit {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    const VT *r;
+    VT *p;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[1]) const
+    {
+        const VT ri = r[i];
+        a[0] += (double)ri * (double)ri;
+        p[i] = ri;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        st->sc[S_TAOO] = t[0];
+        init_record(st, sqrt(t[0]));
+    }
+};
+// x += alpha p ; r -= alpha q ; acc r.r ; then beta = tao/(taoo+small), taoo = tao
+template <typename VT>
+struct OpCgUpdate {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    VT *x, *r;
+    const VT *p, *q;
+    VT alpha;
+    __device__ void load() { alpha = (VT)st->sc[S_ALPHA]; }
+    __device__ void elem(int i, double (&a)[1]) const
+    {
+        const VT minalpha = -alpha;
+        x[i] = x[i] + alpha * p[i];
+        const VT ri = r[i] + minalpha * q[i];
+        r[i] = ri;
+        a[0] += (double)ri * (double)ri;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        const double tao = t[0];
+        if (!record_and_test(st, sqrt(tao))) return;
+        st->sc[S_BETA] = tao / (st->sc[S_TAOO] + KSMALL);
+        st->sc[S_TAOO] = tao;
+    }
+};
+template <typename VT>
+struct OpCgP {  // p = beta*p + r
+    static constexpr int K = 0;
+    int n;
+    KState *st;
+    VT *p;
+    const VT *r;
+    VT beta;
+    __device__ void load() { beta = (VT)st->sc[S_BETA]; }
+    __device__ void elem(int i, double (&)[1]) const
+    {
+        const VT t = beta * p[i];
+        p[i] = t + r[i];
+    }
+    __device__ void finalize(const double *) const {}
+};
+
+// ---- BiCGSTAB
+// init: rhat = r ; acc r.r ; then beta = r.rhat = r.r, omega, beto
+template <typename VT>
+struct OpBicgInit {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    const VT *r;
+    VT *rhat, *p, *u;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[1]) const
+    {
+        const VT ri = r[i];
+        rhat[i] = ri;
+        p[i] = (VT)0;
+        u[i] = (VT)0;
+        a[0] += (double)ri * (double)ri;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        st->sc[S_ALPHA] = 1.0;
+        st->sc[S_BETO] = 1.0;
+        st->sc[S_GAMA] = 1.0;
+        init_record(st, sqrt(t[0]));
+        const double beta = t[0];
+        st->sc[S_BETA] = beta;
+        st->sc[S_OMEGA] = (beta * st->sc[S_GAMA]) / (st->sc[S_ALPHA] * st->sc[S_BETO] + KSMALL);
+        st->sc[S_BETO] = beta;
+    }
+};
+// p = r + omega (p - alpha u)
+template <typename VT>
+struct OpBicgP {
+    static constexpr int K = 0;
+    int n;
+    KState *st;
+    VT *p;
+    const VT *r, *u;
+    VT alpha, omega;
+    __device__ void load()
+    {
+        alpha = (VT)st->sc[S_ALPHA];
+        omega = (VT)st->sc[S_OMEGA];
+    }
+    __device__ void elem(int i, double (&)[1]) const
+    {
+        const VT minalpha = -alpha;
+        VT t = p[i] + minalpha * u[i];
+        t = omega * t;
+        p[i] = t + r[i];
+    }
+    __device__ void finalize(const double *) const {}
+};
+// s = r - gama u
+template <typename VT>
+struct OpBicgS {
+    static constexpr int K = 0;
+    int n;
+    KState *st;
+    VT *s;
+    const VT *r, *u;
+    VT gama;
+    __device__ void load() { gama = (VT)st->sc[S_GAMA]; }
+    __device__ void elem(int i, double (&)[1]) const
+    {
+        const VT mingama = -gama;
+        s[i] = r[i] + mingama * u[i];
+    }
+    __device__ void finalize(const double *) const {}
+};
+// x += gama z1 + alpha z2 ; r = s - alpha v ; acc r.r, r.rhat
+template <typename VT>
+struct OpBicgX {
+    static constexpr int K = 2;
+    int n;
+    KState *st;
+    VT *x, *r;
+    const VT *z1, *z2, *s, *v, *rhat;
+    VT gama, alpha;
+    __device__ void load()
+    {
+        gama = (VT)st->sc[S_GAMA];
+        alpha = (VT)st->sc[S_ALPHA];
+    }
+    __device__ void elem(int i, double (&a)[2]) const
+    {
+        VT xi = x[i] + gama * z1[i];
+        x[i] = xi + alpha * z2[i];
+        const VT minalpha = -alpha;
+        const VT ri = s[i] + minalpha * v[i];
+        r[i] = ri;
+        a[0] += (double)ri * (double)ri;
+        a[1] += (double)ri * (double)rhat[i];
+    }
+    __device__ void finalize(const double *t) const
+    {
+        if (!record_and_test(st, sqrt(t[0]))) return;
+        const double beta = t[1];
+        st->sc[S_BETA] = beta;
+        st->sc[S_OMEGA] = (beta * st->sc[S_GAMA]) / (st->sc[S_ALPHA] * st->sc[S_BETO] + KSMALL);
+        st->sc[S_BETO] = beta;
+        if (!isfinite(beta)) { st->err |= DEV_BREAKDOWN; st->done = 3; }
+    }
+};
+
+// restarted methods: res0 = ||res|| ; beta = res0
+template <typename VT>
+struct OpGmInit {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    const VT *r;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[1]) const { a[0] += (double)r[i] * (double)r[i]; }
+    __device__ void finalize(const double *t) const
+    {
+        const double r0 = sqrt(t[0]);
+        init_record(st, r0);
+        st->sc[S_BETA] = r0;
+    }
+};
+
+// mixed-precision refinement: outer FP64 residual state
+struct OuterState {
+    double rnorm;
+    double rnorm0;
+    double scale;      // ||r|| (the inner rhs is r / ||r||)
+    double scale_inv;
+};
+
+// ---- generic small ops used by GCR / GMRES
+// acc0 = x.y  (finalize stores into a device address)
+template <typename VT>
+struct OpDotTo {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    const VT *x, *y;
+    double *dst;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[1]) const { a[0] += (double)x[i] * (double)y[i]; }
+    __device__ void finalize(const double *t) const { *dst = t[0]; }
+};
+
+// w = w - h*v_prev ; acc0 = w.v_next  (MGS step fused with the next dot);
+// coefficient read from *hptr; if v_next == null, acc0 = w.w
+template <typename VT>
+struct OpMgsStep {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    VT *w;
+    const VT *vprev, *vnext;
+    const double *hptr;
+    double *dst;
+    VT h;
+    __device__ void load() { h = vprev ? (VT)(*hptr) : (VT)0; }
+    __device__ void elem(int i, double (&a)[1]) const
+    {
+        VT wi = w[i];
+        if (vprev) {
+            const VT minh = -h;
+            wi = wi + minh * vprev[i];
+            w[i] = wi;
+        }
+        const VT o = vnext ? vnext[i] : wi;
+        a[0] += (double)wi * (double)o;
+    }
+    __device__ void finalize(const double *t) const { *dst = t[0]; }
+};
+
+// copy: dst = src
+template <typename VT>
+struct OpCopy {
+    static constexpr int K = 0;
+    int n;
+    KState *st;
+    VT *dst;
+    const VT *src;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&)[1]) const { dst[i] = src[i]; }
+    __device__ void finalize(const double *) const {}
+};
+
+// ---------------------------------------------------------------- workspace
+struct Workspace {
+    DBuf<KState> st;
+    KState *h_st = nullptr;  // pinned mirror
+    DBuf<double> part;
+    DBuf<unsigned> ticket;
+    DBuf<double> hist, hist_rel;
+    int hist_cap = 0;
+    int part_cap = 0;
+    RedSlot slot() const { return RedSlot{part.p, ticket.p}; }
+    void ensure(int max_k, int maxiter)
+    {
+        int G = std::max(geom().red_grid, geom().sms * 8);
+        if (part_cap < max_k * G) {
+            part.alloc((size_t)max_k * G);
+            part_cap = max_k * G;
+        }
+        if (!ticket.p) ticket.alloc(1);
+        if (!st.p) {
+            st.alloc(1);
+            XS_CUDA(cudaMallocHost((void **)&h_st, sizeof(KState)));
+        }
+        if (hist_cap < maxiter + 2) {
+            hist.alloc(maxiter + 2);
+            hist_rel.alloc(maxiter + 2);
+            hist_cap = maxiter + 2;
+        }
+    }
+    ~Workspace()
+    {
+        if (h_st) cudaFreeHost(h_st);
+    }
+};
+
+}  // namespace xs

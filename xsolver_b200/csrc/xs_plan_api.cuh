@@ -1,0 +1,344 @@
+// Kernel-level entry points on device pointers (tests and benchmarks).
+// Included at the end of xs_api.cu (uses its Handle and helpers).
+
+struct xs_plan_s {
+    std::unique_ptr<Handle> h;
+    bool factored = false;
+    int factor_kind = -1;
+    DBuf<double> l2flush;
+    DBuf<double> bx64, by64, bz64;
+    DBuf<float> bx32, by32, bz32;
+};
+
+namespace xs {
+
+__global__ void k_flush(double *p, long m, double v)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < m; i += (long)gridDim.x * blockDim.x) p[i] = v + (double)i;
+}
+__global__ void k_fill_rand(int n, double *x, float *x32, unsigned seed)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)i * 2654435761u ^ seed;
+        h ^= h >> 13;
+        h *= 0x5bd1e995u;
+        h ^= h >> 15;
+        double v = (double)(h & 0xffffff) / (double)0x1000000 * 2.0 - 1.0;
+        x[i] = v;
+        if (x32) x32[i] = (float)v;
+    }
+}
+
+static void plan_lusolve64(Handle &h, const double *x, double *z)
+{
+    if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
+    h.M.apply<double>(x, z, nullptr, h.s);
+}
+static void plan_lusolve32(Handle &h, const float *x, float *z)
+{
+    if (!h.M.have_factors || !h.M.U.dinv32.p) throw Status(XS_ERR_ORDER);
+    h.M.apply<float>(x, z, nullptr, h.s);
+}
+
+}  // namespace xs
+
+extern "C" {
+
+int xs_plan_create(xs_plan_t *p, int n, const int *rp, const int *ci, const double *v)
+{
+    return guarded([&] {
+        if (!p) throw Status(XS_ERR_INVALID);
+        check_gpu();
+        auto *w = new xs_plan_s;
+        w->h.reset(new Handle());
+        try {
+            set_matrix(*w->h, n, rp, ci, v, 0);
+        } catch (...) {
+            delete w;
+            throw;
+        }
+        *p = w;
+    });
+}
+int xs_plan_destroy(xs_plan_t p)
+{
+    return guarded([&] { delete p; });
+}
+int xs_plan_build_ell(xs_plan_t p, int *width)
+{
+    return guarded([&] {
+        if (!p) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        operator_build_ell(h.A, h.hrp.data(), h.hci.data(), h.hv.data(), 0, h.A.v32.p != nullptr, h.s);
+        if (width) *width = h.A.ell_w;
+    });
+}
+int xs_plan_spmv(xs_plan_t p, int format, int precision, const void *x, void *y)
+{
+    return guarded([&] {
+        if (!p || !x || !y) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (format == 1 && h.A.ell_w == 0) throw Status(XS_ERR_ORDER);
+        int saved = h.A.format;
+        h.A.format = format;
+        RedSlot sl = h.W.slot();
+        h.W.ensure(64, 1);
+        if (precision == 0)
+            spmv<double, double>(h.A, (const double *)x, (double *)y, EpiAx<double>{}, sl, h.s);
+        else {
+            operator_ensure32(h.A, h.hrp.data(), h.s);
+            spmv<float, float>(h.A, (const float *)x, (float *)y, EpiAx<float>{}, sl, h.s);
+        }
+        h.A.format = saved;
+    });
+}
+int xs_plan_spmv_t(xs_plan_t p, const double *x, double *y)
+{
+    return guarded([&] {
+        if (!p || !x || !y) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (!h.adj.have_At) {
+            std::vector<int> trp, tci;
+            std::vector<double> tv;
+            host_transpose(h.n, h.hrp.data(), h.hci.data(), h.hv.data(), trp, tci, &tv, nullptr);
+            h.adj.At = Operator();
+            operator_setup(h.adj.At, h.n, trp.data(), tci.data(), tv.data(), 0, false, h.s, h.err.p);
+            h.adj.have_At = true;
+        }
+        h.W.ensure(64, 1);
+        spmv<double, double>(h.adj.At, x, y, EpiAx<double>{}, h.W.slot(), h.s);
+    });
+}
+int xs_plan_factor(xs_plan_t p, int kind, int sweeps, double fill, double droptol)
+{
+    return guarded([&] {
+        if (!p) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (kind == 0) h.pc_req = PC_ILU0;
+        else if (kind == 1) { h.pc_req = PC_PARILU; h.parilu_sweeps = sweeps; }
+        else if (kind == 2) { h.pc_req = PC_PARILUT; h.parilut_fill = fill; h.parilut_sweeps = sweeps; h.parilut_droptol = droptol; }
+        else throw Status(XS_ERR_INVALID);
+        h.inner32 = 1;  // keep reduced-precision copies of the factors for the solves
+        invalidate_pc(h);
+        build_precond(h);
+        p->factored = true;
+        p->factor_kind = kind;
+    });
+}
+int xs_plan_get_lu_values(xs_plan_t p, double *luv)
+{
+    return guarded([&] {
+        if (!p || !luv) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (!p->factored || p->factor_kind > 1) throw Status(XS_ERR_ORDER);
+        h.luv.download(luv, h.nnz, h.s);
+        XS_CUDA(cudaStreamSynchronize(h.s));
+    });
+}
+int xs_plan_get_factors(xs_plan_t p, int *nnzL, int *nnzU, int *lrp, int *lci, double *lv, double *dinv, int *urp, int *uci,
+                        double *uv)
+{
+    return guarded([&] {
+        if (!p) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (!p->factored) throw Status(XS_ERR_ORDER);
+        const int n = h.n;
+        if (p->factor_kind == 2) {
+            ParilutResult &R = h.ilut;
+            if (nnzL) *nnzL = (int)R.nnzL;
+            if (nnzU) *nnzU = (int)R.nnzU;
+            if (lrp) std::memcpy(lrp, R.hlrp.data(), sizeof(int) * (n + 1));
+            if (urp) std::memcpy(urp, R.hurp.data(), sizeof(int) * (n + 1));
+            if (lci) std::memcpy(lci, R.hlci.data(), sizeof(int) * R.nnzL);
+            if (uci) std::memcpy(uci, R.huci.data(), sizeof(int) * R.nnzU);
+            if (lv && R.nnzL) R.lv.download(lv, R.nnzL, h.s);
+            if (uv && R.nnzU) R.uv.download(uv, R.nnzU, h.s);
+            if (dinv) R.dinv.download(dinv, n, h.s);
+            XS_CUDA(cudaStreamSynchronize(h.s));
+            return;
+        }
+        std::vector<double> fv(h.nnz);
+        h.fv.download(fv.data(), h.nnz, h.s);
+        XS_CUDA(cudaStreamSynchronize(h.s));
+        int nl = 0, nu = 0;
+        if (lrp) lrp[0] = 0;
+        if (urp) urp[0] = 0;
+        for (int i = 0; i < n; i++) {
+            for (int k = h.hrp[i]; k < h.hrp[i + 1]; k++) {
+                int c = h.hci[k];
+                if (c < i) {
+                    if (lci) lci[nl] = c;
+                    if (lv) lv[nl] = fv[k];
+                    nl++;
+                } else if (c > i) {
+                    if (uci) uci[nu] = c;
+                    if (uv) uv[nu] = fv[k];
+                    nu++;
+                } else if (dinv)
+                    dinv[i] = fv[k];
+            }
+            if (lrp) lrp[i + 1] = nl;
+            if (urp) urp[i + 1] = nu;
+        }
+        if (nnzL) *nnzL = nl;
+        if (nnzU) *nnzU = nu;
+    });
+}
+int xs_plan_set_factor_precision(xs_plan_t p, int prec)
+{
+    return guarded([&] {
+        if (!p || prec < 0 || prec > 3) throw Status(XS_ERR_INVALID);
+        p->h->M.factor_prec = prec;
+        p->h->factor_prec = prec;
+    });
+}
+int xs_plan_lusolve(xs_plan_t p, int vec_prec, const void *x, void *z)
+{
+    return guarded([&] {
+        if (!p || !x || !z) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (vec_prec == 0) plan_lusolve64(h, (const double *)x, (double *)z);
+        else plan_lusolve32(h, (const float *)x, (float *)z);
+    });
+}
+int xs_plan_lusolve_t(xs_plan_t p, const double *x, double *z)
+{
+    return guarded([&] {
+        if (!p || !x || !z) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
+        adjoint_prepare(h);
+        h.adj.Mt.apply<double>(x, z, nullptr, h.s);
+    });
+}
+int xs_plan_sync(xs_plan_t p)
+{
+    return guarded([&] {
+        if (!p) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        XS_CUDA(cudaStreamSynchronize(h.s));
+        int e = read_dev_err(h);
+        if (e) {
+            h.M.rearm(h.s);
+            clear_dev_err(h);
+            XS_CUDA(cudaStreamSynchronize(h.s));
+            throw Status(dev_err_to_status(e));
+        }
+    });
+}
+int xs_plan_levels(xs_plan_t p, int *lL, int *lU)
+{
+    return guarded([&] {
+        if (!p) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
+        if (lL) *lL = h.M.L.nlevels;
+        if (lU) *lU = h.M.U.nlevels;
+    });
+}
+int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
+{
+    return guarded([&] {
+        if (!p || !bytes) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        const double n = h.n, nnz = (double)h.nnz;
+        const double I = 4.0;
+        switch (op) {
+        case 0: *bytes = (8 + I) * nnz + I * (n + 1) + 8 * n + 8 * n; break;
+        case 1: *bytes = (8 + I) * h.A.ell_w * n + 2 * 8 * n; break;
+        case 2: *bytes = (4 + I) * nnz + I * (n + 1) + 4 * n + 4 * n; break;
+        case 6: *bytes = (4 + I) * h.A.ell_w * n + 2 * 4 * n; break;
+        case 3: case 4: case 5: {
+            if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
+            const int fp = h.M.factor_prec;
+            const double V = fp == 0 ? 8 : (fp == 1 ? 4 : 2);
+            const double X = fp == 0 ? 8 : 4;  // vector element
+            const double l = (V + I) * h.M.L.nnz + I * (n + 1) + 2 * X * n;
+            const double u = (V + I) * h.M.U.nnz + I * (n + 1) + 3 * X * n;
+            *bytes = op == 3 ? l : (op == 4 ? u : l + u);
+            break;
+        }
+        default: throw Status(XS_ERR_INVALID);
+        }
+    });
+}
+int xs_plan_time_op(xs_plan_t p, int op, int reps, int flush_l2, double *ms)
+{
+    return guarded([&] {
+        if (!p || !ms || reps < 1) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        const int n = h.n;
+        const bool f32 = (op == 2 || op == 6) || ((op >= 3 && op <= 5) && h.M.factor_prec != FP_F64);
+        if (p->bx64.n != (size_t)n) {
+            p->bx64.alloc(n); p->by64.alloc(n); p->bz64.alloc(n);
+            p->bx32.alloc(n); p->by32.alloc(n); p->bz32.alloc(n);
+        }
+        k_fill_rand<<<geom().sms * 4, 256, 0, h.s>>>(n, p->bx64.p, p->bx32.p, 12345u);
+        check_launch();
+        if (flush_l2 && !p->l2flush.p) p->l2flush.alloc((size_t)48 << 20);  // 384 MB > L2
+        if (op == 1 || op == 6) {
+            if (h.A.ell_w == 0) operator_build_ell(h.A, h.hrp.data(), h.hci.data(), h.hv.data(), 0, f32, h.s);
+        }
+        if (f32) operator_ensure32(h.A, h.hrp.data(), h.s);
+        h.W.ensure(64, 1);
+        RedSlot sl = h.W.slot();
+        auto run = [&]() {
+            switch (op) {
+            case 0: { int sv = h.A.format; h.A.format = 0; spmv<double, double>(h.A, p->bx64.p, p->by64.p, EpiAx<double>{}, sl, h.s); h.A.format = sv; break; }
+            case 1: { int sv = h.A.format; h.A.format = 1; spmv<double, double>(h.A, p->bx64.p, p->by64.p, EpiAx<double>{}, sl, h.s); h.A.format = sv; break; }
+            case 2: { int sv = h.A.format; h.A.format = 0; spmv<float, float>(h.A, p->bx32.p, p->by32.p, EpiAx<float>{}, sl, h.s); h.A.format = sv; break; }
+            case 6: { int sv = h.A.format; h.A.format = 1; spmv<float, float>(h.A, p->bx32.p, p->by32.p, EpiAx<float>{}, sl, h.s); h.A.format = sv; break; }
+            case 3: case 4: case 5: {
+                if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
+                // op 3: L only (into the L buffer), op 4: U only, op 5: both
+                if (!f32) h.M.apply<double>(p->bx64.p, p->bz64.p, nullptr, h.s);
+                else h.M.apply<float>(p->bx32.p, p->bz32.p, nullptr, h.s);
+                break;
+            }
+            default: throw Status(XS_ERR_INVALID);
+            }
+        };
+        // warm-up
+        run();
+        run();
+        XS_CUDA(cudaStreamSynchronize(h.s));
+        cudaEvent_t a, b;
+        XS_CUDA(cudaEventCreate(&a));
+        XS_CUDA(cudaEventCreate(&b));
+        double total = 0.0;
+        const bool half = (op == 3 || op == 4) && h.M.trsv_mode == 0;
+        for (int r = 0; r < reps; r++) {
+            if (flush_l2) k_flush<<<geom().sms * 4, 256, 0, h.s>>>(p->l2flush.p, (long)p->l2flush.n, (double)r);
+            if (half && op == 4) {  // U alone needs a fresh L result in the L buffer
+                if (!f32) h.M.apply_half<double>(0, p->bx64.p, p->bz64.p, h.s);
+                else h.M.apply_half<float>(0, p->bx32.p, p->bz32.p, h.s);
+            }
+            XS_CUDA(cudaEventRecord(a, h.s));
+            if (half) {
+                if (!f32) h.M.apply_half<double>(op == 3 ? 0 : 1, p->bx64.p, p->bz64.p, h.s);
+                else h.M.apply_half<float>(op == 3 ? 0 : 1, p->bx32.p, p->bz32.p, h.s);
+            } else
+                run();
+            XS_CUDA(cudaEventRecord(b, h.s));
+            if (half && op == 3) {  // finish the pair so both buffers are re-armed
+                if (!f32) h.M.apply_half<double>(1, p->bx64.p, p->bz64.p, h.s);
+                else h.M.apply_half<float>(1, p->bx32.p, p->bz32.p, h.s);
+            }
+            XS_CUDA(cudaEventSynchronize(b));
+            float t = 0;
+            cudaEventElapsedTime(&t, a, b);
+            total += t;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        *ms = total / reps;
+        int e = read_dev_err(h);
+        if (e) {
+            h.M.rearm(h.s);
+            clear_dev_err(h);
+            throw Status(dev_err_to_status(e));
+        }
+    });
+}
+
+}  // extern "C"

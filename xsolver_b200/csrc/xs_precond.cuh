@@ -1,0 +1,203 @@
+// Preconditioner objects on the device (replaces the reference's Precond
+// hierarchy, hip/Precond/preconditioner.h:14-30, for the GPU cases: gpujacobi,
+// gpuilu0 = ParILU, gpuilut = ParILUT; plus exact ILU(0)).
+#pragma once
+#include "xs_internal.cuh"
+#include "xs_trsv.cuh"
+
+namespace xs {
+
+enum PcType { PC_NONE = 0, PC_JACOBI = 1, PC_ILU0 = 2, PC_PARILU = 3, PC_PARILUT = 4 };
+enum FactorPrec { FP_F64 = 0, FP_F32 = 1, FP_BF16 = 2, FP_F16 = 3 };
+
+template <typename VT>
+__global__ void k_copy(int n, const VT *__restrict__ x, VT *__restrict__ y, const int *done_flag)
+{
+    if (done_flag && *done_flag) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i];
+}
+template <typename VT, typename DT>
+__global__ void k_diag_scale(int n, const DT *__restrict__ d, const VT *__restrict__ x, VT *__restrict__ y,
+                             const int *done_flag)
+{
+    if (done_flag && *done_flag) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = (VT)d[i] * x[i];
+}
+
+struct PrecondDev {
+    int type = PC_NONE;
+    int n = 0;
+    int factor_prec = FP_F64;
+    int trsv_mode = 0;  // 0 exact sync-free; k > 0 Jacobi sweeps
+    DBuf<double> jdiag64;
+    DBuf<float> jdiag32;
+    TriDev L, U;
+    DBuf<double> lbuf64, ubuf64, tmp64a, tmp64b;
+    DBuf<float> lbuf32, ubuf32, tmp32a, tmp32b;
+    int *err = nullptr;
+    bool have_factors = false;
+
+    void ensure_buffers64(cudaStream_t s)
+    {
+        if (lbuf64.n != (size_t)n) {
+            lbuf64.alloc(n);
+            ubuf64.alloc(n);
+            k_fill_sentinel<double><<<256, 256, 0, s>>>(lbuf64, n);
+            k_fill_sentinel<double><<<256, 256, 0, s>>>(ubuf64, n);
+            check_launch();
+        }
+    }
+    void ensure_buffers32(cudaStream_t s)
+    {
+        if (lbuf32.n != (size_t)n) {
+            lbuf32.alloc(n);
+            ubuf32.alloc(n);
+            k_fill_sentinel<float><<<256, 256, 0, s>>>(lbuf32, n);
+            k_fill_sentinel<float><<<256, 256, 0, s>>>(ubuf32, n);
+            check_launch();
+        }
+    }
+    // re-arm the sentinel buffers (after an aborted solve)
+    void rearm(cudaStream_t s)
+    {
+        if (lbuf64.n) { k_fill_sentinel<double><<<256, 256, 0, s>>>(lbuf64, n); k_fill_sentinel<double><<<256, 256, 0, s>>>(ubuf64, n); }
+        if (lbuf32.n) { k_fill_sentinel<float><<<256, 256, 0, s>>>(lbuf32, n); k_fill_sentinel<float><<<256, 256, 0, s>>>(ubuf32, n); }
+        check_launch();
+    }
+
+    template <typename VT>
+    VT *lbuf() const;
+    template <typename VT>
+    VT *ubuf() const;
+
+    // z = M^{-1} x on stream s.  x == z allowed.
+    template <typename VT>
+    void apply(const VT *x, VT *z, const int *done_flag, cudaStream_t s)
+    {
+        const int g = geom().sms * 4;
+        if (type == PC_NONE) {
+            if (x != z) k_copy<VT><<<g, 256, 0, s>>>(n, x, z, done_flag);
+        } else if (type == PC_JACOBI) {
+            if constexpr (std::is_same<VT, double>::value)
+                k_diag_scale<double, double><<<g, 256, 0, s>>>(n, jdiag64.p, x, z, done_flag);
+            else
+                k_diag_scale<float, float><<<g, 256, 0, s>>>(n, jdiag32.p, x, z, done_flag);
+        } else {
+            if (trsv_mode == 0) {
+                if constexpr (std::is_same<VT, double>::value) apply_exact<double, double>(x, z, done_flag, s);
+                else {
+                    switch (factor_prec) {
+                    case FP_BF16: apply_exact<float, __nv_bfloat16>(x, z, done_flag, s); break;
+                    case FP_F16: apply_exact<float, __half>(x, z, done_flag, s); break;
+                    default: apply_exact<float, float>(x, z, done_flag, s); break;
+                    }
+                }
+            } else {
+                if constexpr (std::is_same<VT, double>::value) apply_sweeps<double, double>(x, z, done_flag, s);
+                else {
+                    switch (factor_prec) {
+                    case FP_BF16: apply_sweeps<float, __nv_bfloat16>(x, z, done_flag, s); break;
+                    case FP_F16: apply_sweeps<float, __half>(x, z, done_flag, s); break;
+                    default: apply_sweeps<float, float>(x, z, done_flag, s); break;
+                    }
+                }
+            }
+        }
+        check_launch();
+    }
+
+    template <typename VT, typename FT>
+    void apply_exact(const VT *x, VT *z, const int *done_flag, cudaStream_t s)
+    {
+        exact_half<VT, FT>(0, x, z, done_flag, s);
+        exact_half<VT, FT>(1, x, z, done_flag, s);
+    }
+    // half 0: L solve x -> L buffer (re-arms the U buffer)
+    // half 1: U solve L buffer -> z (re-arms the L buffer)
+    template <typename VT, typename FT>
+    void exact_half(int half, const VT *x, VT *z, const int *done_flag, cudaStream_t s)
+    {
+        using DT = VT;
+        const DT *dinv;
+        if constexpr (std::is_same<VT, double>::value) dinv = U.dinv64.p;
+        else dinv = U.dinv32.p;
+        VT *lb = lbuf<VT>(), *ub = ubuf<VT>();
+        const int gl = (L.n + TRSV_THREADS - 1) / TRSV_THREADS;
+        if (half == 0)
+            k_trsv_syncfree<VT, FT, DT, false><<<gl, TRSV_THREADS, 0, s>>>(L.args<FT>(), (const DT *)nullptr, x, lb,
+                                                                           (VT *)nullptr, ub, done_flag, err, L.ticket.p);
+        else
+            k_trsv_syncfree<VT, FT, DT, true><<<gl, TRSV_THREADS, 0, s>>>(U.args<FT>(), dinv, lb, ub, z, lb, done_flag,
+                                                                          err, U.ticket.p);
+    }
+    // one half of the exact solve in the configured precision (timing)
+    template <typename VT>
+    void apply_half(int half, const VT *x, VT *z, cudaStream_t s)
+    {
+        if constexpr (std::is_same<VT, double>::value) exact_half<double, double>(half, x, z, nullptr, s);
+        else {
+            switch (factor_prec) {
+            case FP_BF16: exact_half<float, __nv_bfloat16>(half, x, z, nullptr, s); break;
+            case FP_F16: exact_half<float, __half>(half, x, z, nullptr, s); break;
+            default: exact_half<float, float>(half, x, z, nullptr, s); break;
+            }
+        }
+        check_launch();
+    }
+
+    template <typename FT>
+    const FT *natvals(const TriDev &T) const;
+
+    template <typename VT, typename FT>
+    void apply_sweeps(const VT *x, VT *z, const int *done_flag, cudaStream_t s)
+    {
+        using DT = VT;
+        VT *ta, *tb;
+        const DT *dinv;
+        if constexpr (std::is_same<VT, double>::value) { ta = tmp64a.p; tb = tmp64b.p; dinv = U.dinv64_nat.p; }
+        else { ta = tmp32a.p; tb = tmp32b.p; dinv = U.dinv32_nat.p; }
+        const int g = geom().sms * 4;
+        // L: y_1 = x, y_{t+1} = x - L y_t ; ends in ta
+        VT *cur = ta, *other = tb;
+        k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, L.rp_nat, L.ci_nat, natvals<FT>(L), (const DT *)nullptr, x,
+                                                          (const VT *)nullptr, cur, 1, done_flag);
+        for (int t = 1; t < trsv_mode; t++) {
+            k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, L.rp_nat, L.ci_nat, natvals<FT>(L), (const DT *)nullptr,
+                                                              x, cur, other, 0, done_flag);
+            std::swap(cur, other);
+        }
+        // U: w_1 = dinv*y, w_{t+1} = dinv*y - U' w_t ; result in z
+        const VT *yv = cur;
+        VT *wa = other, *wb = z;
+        // ping-pong between `other` and z, finishing in z
+        int sweeps = trsv_mode;
+        VT *bufs[2] = {(sweeps % 2 == 1) ? z : other, (sweeps % 2 == 1) ? other : z};
+        k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, U.rp_nat, U.ci_nat, natvals<FT>(U), dinv, yv,
+                                                         (const VT *)nullptr, bufs[0], 1, done_flag);
+        for (int t = 1; t < sweeps; t++) {
+            k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, U.rp_nat, U.ci_nat, natvals<FT>(U), dinv, yv,
+                                                             bufs[(t - 1) & 1], bufs[t & 1], 0, done_flag);
+        }
+        (void)wa;
+        (void)wb;
+    }
+};
+
+template <>
+inline double *PrecondDev::lbuf<double>() const { return lbuf64.p; }
+template <>
+inline double *PrecondDev::ubuf<double>() const { return ubuf64.p; }
+template <>
+inline float *PrecondDev::lbuf<float>() const { return lbuf32.p; }
+template <>
+inline float *PrecondDev::ubuf<float>() const { return ubuf32.p; }
+template <>
+inline const double *PrecondDev::natvals<double>(const TriDev &T) const { return T.nv64.p; }
+template <>
+inline const float *PrecondDev::natvals<float>(const TriDev &T) const { return T.nv32.p; }
+template <>
+inline const __nv_bfloat16 *PrecondDev::natvals<__nv_bfloat16>(const TriDev &T) const { return T.nvbf.p; }
+template <>
+inline const __half *PrecondDev::natvals<__half>(const TriDev &T) const { return T.nvh.p; }
+
+}  // namespace xs

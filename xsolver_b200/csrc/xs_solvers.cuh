@@ -1,0 +1,217 @@
+// Host drivers of the Krylov methods: initial sequence, one CUDA graph per
+// chunk of iterations, pipelined polling of the device done flag.
+#pragma once
+#include <vector>
+#include <cstring>
+#include "xs_krylov.cuh"
+
+namespace xs {
+
+enum Method {
+    KSP_CGM = 1,       // PCG (hip "cg", intel cpu_cgm_solve)
+    KSP_CG_LEFT = 2,   // intel cpu_cg_solve (CG on M^-1 A)
+    KSP_BICGSTAB = 3,
+    KSP_GCR_LEFT = 4,  // intel cpu_gcr_solve (classical GS)
+    KSP_IGCR_LEFT = 5, // intel cpu_igcr_solve (modified GS)
+    KSP_GCR_RIGHT = 6, // hip Xsolver_igcr (right preconditioned, MGS)
+    KSP_GMRES_LEFT = 7,
+    KSP_GMRES_RIGHT = 8
+};
+
+// vectors owned by a solve, cached across solves of the same size
+template <typename VT>
+struct VecPool {
+    std::vector<DBuf<VT>> v;
+    int n = 0;
+    VT *get(int idx, int nn)
+    {
+        if (nn != n) {
+            v.clear();
+            n = nn;
+        }
+        while ((int)v.size() <= idx) {
+            v.emplace_back();
+            v.back().alloc(n);
+        }
+        return v[idx].p;
+    }
+};
+
+struct GraphCache {
+    GraphCache() = default;
+    GraphCache(const GraphCache &) = delete;
+    GraphCache &operator=(const GraphCache &) = delete;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void *> key;
+    void reset()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+    }
+    ~GraphCache() { reset(); }
+};
+
+struct SolveCtx {
+    cudaStream_t s;
+    Operator *A;
+    PrecondDev *M;
+    Workspace *W;
+    int n;
+    int chunk = 8;
+    int quirk = 1;
+};
+
+// configuration that changes the captured kernels
+inline long cfg_key(const SolveCtx &c)
+{
+    return (long)c.M->type * 100000 + (long)c.M->trsv_mode * 100 + c.M->factor_prec * 10 + c.A->format;
+}
+
+// Capture `body` `reps` times into a graph and replay until done.
+template <class Body>
+inline void run_graph_loop(SolveCtx &c, GraphCache &gc, const std::vector<const void *> &key, int reps,
+                           int max_launches, Body body)
+{
+    if (!gc.exec || gc.key != key) {
+        gc.reset();
+        cudaGraph_t g;
+        XS_CUDA(cudaStreamBeginCapture(c.s, cudaStreamCaptureModeRelaxed));
+        try {
+            for (int r = 0; r < reps; r++) body();
+        } catch (...) {
+            cudaGraph_t junk;
+            cudaStreamEndCapture(c.s, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            throw;
+        }
+        XS_CUDA(cudaStreamEndCapture(c.s, &g));
+        cudaError_t e = cudaGraphInstantiate(&gc.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) throw Status(XS_ERR_CUDA);
+        gc.key = key;
+    }
+    // pipelined polling: check launch k-1's flag after enqueueing launch k
+    int *hflag = nullptr;
+    XS_CUDA(cudaMallocHost((void **)&hflag, sizeof(int) * 2));
+    cudaEvent_t ev[2];
+    XS_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    XS_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    KState *dst = c.W->st.p;
+    bool stop = false;
+    for (int l = 0; l < max_launches && !stop; l++) {
+        XS_CUDA(cudaGraphLaunch(gc.exec, c.s));
+        XS_CUDA(cudaMemcpyAsync(&hflag[l & 1], &dst->done, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        XS_CUDA(cudaEventRecord(ev[l & 1], c.s));
+        if (l > 0) {
+            XS_CUDA(cudaEventSynchronize(ev[(l - 1) & 1]));
+            if (hflag[(l - 1) & 1]) stop = true;
+        }
+    }
+    XS_CUDA(cudaStreamSynchronize(c.s));
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    cudaFreeHost(hflag);
+}
+
+// ---------------------------------------------------------------- PCG (cgm)
+template <typename VT, typename MT>
+struct PcgRun {
+    VecPool<VT> pool;
+    GraphCache gc;
+    void run(SolveCtx &c, const VT *b, VT *x)
+    {
+        const int n = c.n;
+        VT *r = pool.get(0, n), *z = pool.get(1, n), *p = pool.get(2, n), *Ap = pool.get(3, n);
+        KState *st = c.W->st.p;
+        RedSlot sl = c.W->slot();
+        const int *done = &st->done;
+        spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
+        c.M->apply<VT>(r, z, done, c.s);
+        vecop(OpCgmInit<VT>{n, st, r, z, p}, sl, c.s);
+        auto body = [&]() {
+            spmv<VT, MT>(*c.A, p, Ap, EpiDot1<VT>{st, p, 0, M_CGM_SIGMA}, sl, c.s);
+            vecop(OpCgmUpdate<VT>{n, st, x, r, p, Ap, (VT)0}, sl, c.s);
+            c.M->apply<VT>(r, z, done, c.s);
+            vecop(OpDotRZ<VT>{n, st, r, z}, sl, c.s);
+            vecop(OpPUpdate<VT>{n, st, p, z, (VT)0}, sl, c.s);
+        };
+        std::vector<const void *> key{b, x, r, z, p, Ap, st, c.M, c.A, (const void *)cfg_key(c)};
+        int maxit = c.W->h_st->maxiter;
+        run_graph_loop(c, gc, key, c.chunk, maxit / c.chunk + 3, body);
+    }
+};
+
+// ---------------------------------------------------------------- left CG (cg)
+template <typename VT>
+struct OpCgSigma {  // sigma = p.q ; alpha = taoo/(sigma+small)
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    const VT *p, *q;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[1]) const { a[0] += (double)p[i] * (double)q[i]; }
+    __device__ void finalize(const double *t) const
+    {
+        st->sc[S_SIGMA] = t[0];
+        st->sc[S_ALPHA] = st->sc[S_TAOO] / (t[0] + KSMALL);
+        if (!isfinite(t[0])) { st->err |= DEV_BREAKDOWN; st->done = 3; }
+    }
+};
+
+template <typename VT, typename MT>
+struct CgLeftRun {
+    VecPool<VT> pool;
+    GraphCache gc;
+    void run(SolveCtx &c, const VT *b, VT *x)
+    {
+        const int n = c.n;
+        VT *r = pool.get(0, n), *q = pool.get(1, n), *p = pool.get(2, n), *Ap = pool.get(3, n);
+        KState *st = c.W->st.p;
+        RedSlot sl = c.W->slot();
+        const int *done = &st->done;
+        spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
+        c.M->apply<VT>(r, r, done, c.s);
+        vecop(OpCgInit<VT>{n, st, r, p}, sl, c.s);
+        auto body = [&]() {
+            spmv<VT, MT>(*c.A, p, Ap, EpiActive<VT>{st}, sl, c.s);
+            c.M->apply<VT>(Ap, q, done, c.s);
+            vecop(OpCgSigma<VT>{n, st, p, q}, sl, c.s);
+            vecop(OpCgUpdate<VT>{n, st, x, r, p, q, (VT)0}, sl, c.s);
+            vecop(OpCgP<VT>{n, st, p, r, (VT)0}, sl, c.s);
+        };
+        std::vector<const void *> key{b, x, r, q, p, Ap, st, c.M, c.A, (const void *)cfg_key(c)};
+        run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
+    }
+};
+
+// ---------------------------------------------------------------- BiCGSTAB
+template <typename VT, typename MT>
+struct BicgRun {
+    VecPool<VT> pool;
+    GraphCache gc;
+    void run(SolveCtx &c, const VT *b, VT *x)
+    {
+        const int n = c.n;
+        VT *r = pool.get(0, n), *rhat = pool.get(1, n), *p = pool.get(2, n), *u = pool.get(3, n);
+        VT *s = pool.get(4, n), *v = pool.get(5, n), *z1 = pool.get(6, n), *z2 = pool.get(7, n);
+        KState *st = c.W->st.p;
+        RedSlot sl = c.W->slot();
+        const int *done = &st->done;
+        spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
+        vecop(OpBicgInit<VT>{n, st, r, rhat, p, u}, sl, c.s);
+        auto body = [&]() {
+            vecop(OpBicgP<VT>{n, st, p, r, u, (VT)0, (VT)0}, sl, c.s);
+            c.M->apply<VT>(p, z1, done, c.s);
+            spmv<VT, MT>(*c.A, z1, u, EpiDot1<VT>{st, rhat, 0, M_BICG_GAMA}, sl, c.s);
+            vecop(OpBicgS<VT>{n, st, s, r, u, (VT)0}, sl, c.s);
+            c.M->apply<VT>(s, z2, done, c.s);
+            spmv<VT, MT>(*c.A, z2, v, EpiDot2<VT>{st, s, M_BICG_ALPHA}, sl, c.s);
+            vecop(OpBicgX<VT>{n, st, x, r, z1, z2, s, v, rhat, (VT)0, (VT)0}, sl, c.s);
+        };
+        std::vector<const void *> key{b, x, r, rhat, p, u, s, v, z1, z2, st, c.M, c.A, (const void *)cfg_key(c)};
+        run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
+    }
+};
+
+}  // namespace xs

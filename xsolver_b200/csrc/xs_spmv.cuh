@@ -1,0 +1,419 @@
+// Sparse matrix-vector products.
+//
+// CSR (replaces DeviceMatrixCSR::SpMV/bmAx, hip/HostMatrix/DeviceMatrix/
+// DeviceMatrixCSR.cpp:59-84, whose kernels map one thread to one row and read
+// each row's entries with uncoalesced scalar loads):
+//   The rows are cut into row blocks whose entries form one contiguous,
+//   16-byte aligned range of at most `cap` entries.  A persistent CTA walks
+//   its row blocks (block b, b+G, ...), staging each block's values and column
+//   indices into shared memory with two TMA bulk copies (cp.async.bulk,
+//   completion on an mbarrier), double-buffered so the copy of the next block
+//   overlaps the arithmetic of the current one.  Each thread then sums one row
+//   from shared memory in increasing entry order — the same order as the
+//   sequential CPU loop — and gathers x through the read-only cache.  An
+//   epilogue functor turns the row sum into the stored value (y = Ax,
+//   y = b - Ax, ...) and accumulates fused dot products, reduced
+//   deterministically across the fixed grid.
+//
+// ELL (replaces DeviceMatrixELL::SpMV, DeviceMatrixELL.cpp:3-34): column-major
+//   val[k*n + row] with the true maximum row width (no fixed width 16); padding
+//   entries point at the row itself with value 0.  Consecutive threads read
+//   consecutive addresses for every k.
+#pragma once
+#include "xs_internal.cuh"
+
+namespace xs {
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// 1D bulk copy global -> shared, completion counted on bar (no multicast)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait; returns false (and records DEV_TMA_TIMEOUT) if the copy never lands
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err)
+{
+    for (long it = 0; it < (1L << 26); it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicOr(err, DEV_TMA_TIMEOUT);
+    return false;
+}
+
+// ---------------------------------------------------------------- epilogues
+// Epilogue interface:
+//   static constexpr int K;                   number of fused dot products
+//   bool active() const;                      false -> kernel exits (solver done)
+//   VT out(int row, double ax);               value stored in y[row]
+//   void acc(int row, double stored, double (&a)[K]);   dot contributions
+//   void finalize(const double *tot);         last block, thread 0
+template <typename VT>
+struct EpiAx {
+    static constexpr int K = 0;
+    __device__ bool active() const { return true; }
+    __device__ VT out(int, double ax) const { return (VT)ax; }
+    __device__ void acc(int, double, double (&)[K > 0 ? K : 1]) const {}
+    __device__ void finalize(const double *) const {}
+};
+
+// y = b - A x (bmAx, hip/HostMatrix/DeviceMatrix/DeviceMatrixCSR.cpp:72-84)
+template <typename VT>
+struct EpiBmAx {
+    static constexpr int K = 0;
+    const VT *b;
+    __device__ bool active() const { return true; }
+    __device__ VT out(int r, double ax) const { return (VT)((double)b[r] - ax); }
+    __device__ void acc(int, double, double (&)[1]) const {}
+    __device__ void finalize(const double *) const {}
+};
+
+// ---------------------------------------------------------------- CSR tiled kernel
+template <typename MT>
+struct CsrTileArgs {
+    int n;
+    const int *rp;
+    const int *ci;
+    const MT *v;
+    const int *rb;
+    const int *longrow;
+    int nblocks;
+    int cap;
+    int *err;
+};
+
+template <typename VT, typename MT, typename Epi>
+__global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const VT *__restrict__ x, VT *__restrict__ y,
+                                                        Epi epi, RedSlot slot)
+{
+    constexpr int KK = Epi::K > 0 ? Epi::K : 1;
+    if (!epi.active()) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ double tot[KK];
+    MT *vbuf[2];
+    int *cbuf[2];
+    vbuf[0] = (MT *)smem_raw;
+    vbuf[1] = vbuf[0] + A.cap;
+    cbuf[0] = (int *)(vbuf[1] + A.cap);
+    cbuf[1] = cbuf[0] + A.cap;
+
+    double acc[KK];
+#pragma unroll
+    for (int k = 0; k < KK; k++) acc[k] = 0.0;
+
+    const int G = gridDim.x;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int b, int slotb) {
+        if (A.longrow[b]) {
+            // no staging: arrive without transaction bytes so the wait completes
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bars[slotb])) : "memory");
+            return;
+        }
+        int r0 = A.rb[b], r1 = A.rb[b + 1];
+        int e0 = A.rp[r0] & ~3;
+        int e1 = (A.rp[r1] + 3) & ~3;
+        uint32_t cnt = (uint32_t)(e1 - e0);
+        uint32_t vbytes = cnt * (uint32_t)sizeof(MT), cbytes = cnt * 4u;
+        if (cnt == 0) {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bars[slotb])) : "memory");
+            return;
+        }
+        mbar_expect_tx(&bars[slotb], vbytes + cbytes);
+        bulk_g2s(vbuf[slotb], A.v + e0, vbytes, &bars[slotb]);
+        bulk_g2s(cbuf[slotb], A.ci + e0, cbytes, &bars[slotb]);
+    };
+
+    int it = 0;
+    if (threadIdx.x == 0 && blockIdx.x < A.nblocks) issue(blockIdx.x, 0);
+    for (int b = blockIdx.x; b < A.nblocks; b += G, it++) {
+        const int s = it & 1;
+        if (threadIdx.x == 0 && b + G < A.nblocks) {
+            fence_proxy_async();
+            issue(b + G, s ^ 1);
+        }
+        if (!mbar_wait_bounded(&bars[s], (uint32_t)((it >> 1) & 1), A.err)) return;
+        const int r0 = A.rb[b], r1 = A.rb[b + 1];
+        if (!A.longrow[b]) {
+            const int e0 = A.rp[r0] & ~3;
+            const int r = r0 + (int)threadIdx.x;
+            if (r < r1) {
+                const int k0 = A.rp[r] - e0, k1 = A.rp[r + 1] - e0;
+                const MT *vv = vbuf[s];
+                const int *cc = cbuf[s];
+                double sum = 0.0;
+                int k = k0;
+                for (; k + 4 <= k1; k += 4) {
+                    const int c0 = cc[k], c1 = cc[k + 1], c2 = cc[k + 2], c3 = cc[k + 3];
+                    const double x0 = (double)__ldg(x + c0), x1 = (double)__ldg(x + c1);
+                    const double x2 = (double)__ldg(x + c2), x3 = (double)__ldg(x + c3);
+                    sum += (double)vv[k] * x0;
+                    sum += (double)vv[k + 1] * x1;
+                    sum += (double)vv[k + 2] * x2;
+                    sum += (double)vv[k + 3] * x3;
+                }
+                for (; k < k1; k++) sum += (double)vv[k] * (double)__ldg(x + cc[k]);
+                VT o = epi.out(r, sum);
+                y[r] = o;
+                if (Epi::K > 0) epi.acc(r, (double)o, acc);
+            }
+        } else {
+            // one row longer than the staging capacity: block-wide reduction
+            __shared__ double lsum[32];
+            double part = 0.0;
+            for (int k = A.rp[r0] + threadIdx.x; k < A.rp[r0 + 1]; k += blockDim.x)
+                part += (double)A.v[k] * (double)__ldg(x + A.ci[k]);
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            if ((threadIdx.x & 31) == 0) lsum[threadIdx.x >> 5] = part;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double sum = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += lsum[w];
+                VT o = epi.out(r0, sum);
+                y[r0] = o;
+                if (Epi::K > 0) epi.acc(r0, (double)o, acc);
+            }
+        }
+        __syncthreads();
+    }
+    if (Epi::K > 0) {
+        if (block_reduce_publish<KK>(acc, slot, tot)) {
+            if (threadIdx.x == 0) epi.finalize(tot);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- ELL kernel
+template <typename MT>
+struct EllArgs {
+    int n, w;
+    const int *ci;
+    const MT *v;
+};
+
+template <typename VT, typename MT, typename Epi>
+__global__ void __launch_bounds__(256) k_ell_spmv(EllArgs<MT> A, const VT *__restrict__ x, VT *__restrict__ y, Epi epi,
+                                                  RedSlot slot)
+{
+    constexpr int KK = Epi::K > 0 ? Epi::K : 1;
+    if (!epi.active()) return;
+    __shared__ double tot[KK];
+    double acc[KK];
+#pragma unroll
+    for (int k = 0; k < KK; k++) acc[k] = 0.0;
+    const int n = A.n;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        double sum = 0.0;
+        const int *cp = A.ci + r;
+        const MT *vp = A.v + r;
+        int k = 0;
+        for (; k + 4 <= A.w; k += 4) {
+            const long o0 = (long)k * n, o1 = o0 + n, o2 = o1 + n, o3 = o2 + n;
+            const int c0 = __ldg(cp + o0), c1 = __ldg(cp + o1), c2 = __ldg(cp + o2), c3 = __ldg(cp + o3);
+            const double v0 = (double)__ldg(vp + o0), v1 = (double)__ldg(vp + o1);
+            const double v2 = (double)__ldg(vp + o2), v3 = (double)__ldg(vp + o3);
+            sum += v0 * (double)__ldg(x + c0);
+            sum += v1 * (double)__ldg(x + c1);
+            sum += v2 * (double)__ldg(x + c2);
+            sum += v3 * (double)__ldg(x + c3);
+        }
+        for (; k < A.w; k++) {
+            const long o = (long)k * n;
+            sum += (double)__ldg(vp + o) * (double)__ldg(x + __ldg(cp + o));
+        }
+        VT o = epi.out(r, sum);
+        y[r] = o;
+        if (Epi::K > 0) epi.acc(r, (double)o, acc);
+    }
+    if (Epi::K > 0) {
+        if (block_reduce_publish<KK>(acc, slot, tot)) {
+            if (threadIdx.x == 0) epi.finalize(tot);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- host side
+// The matrix operator the solvers call: CSR (tiled) or ELL, FP64 or FP32 values.
+struct Operator {
+    int n = 0;
+    long nnz = 0;
+    int format = 0;  // 0 CSR, 1 ELL
+    // CSR (device, padded by 8 entries for aligned bulk copies)
+    DBuf<int> rp, ci;
+    DBuf<double> v;
+    DBuf<float> v32;
+    SpmvTiling tile64, tile32;
+    int grid64 = 0, grid32 = 0;  // persistent grid sizes
+    // ELL
+    int ell_w = 0;
+    DBuf<int> eci;
+    DBuf<double> ev;
+    DBuf<float> ev32;
+    int ell_grid = 0;
+    int *err = nullptr;  // device status word
+
+    CsrTileArgs<double> csr64() const
+    {
+        return CsrTileArgs<double>{n, rp.p, ci.p, v.p, tile64.rb.p, tile64.longrow.p, tile64.nblocks, tile64.cap, err};
+    }
+    CsrTileArgs<float> csr32() const
+    {
+        return CsrTileArgs<float>{n, rp.p, ci.p, v32.p, tile32.rb.p, tile32.longrow.p, tile32.nblocks, tile32.cap, err};
+    }
+    EllArgs<double> ell64() const { return EllArgs<double>{n, ell_w, eci.p, ev.p}; }
+    EllArgs<float> ell32() const { return EllArgs<float>{n, ell_w, eci.p, ev32.p}; }
+};
+
+// Cut rows into blocks: at most max_rows rows, and the 4-aligned entry range
+// [rp[r0] & ~3, (rp[r1] + 3) & ~3) at most cap entries.  A single row whose
+// range exceeds cap becomes its own "long row" block.
+inline void build_tiling(const int *h_rp, int n, int max_rows, int cap, SpmvTiling &t, cudaStream_t s)
+{
+    std::vector<int> rb;
+    std::vector<int> lr;
+    rb.reserve(n / 64 + 2);
+    int r0 = 0;
+    while (r0 < n) {
+        int r1 = r0;
+        auto span = [&](int a, int b) { return (long)(((h_rp[b] + 3) & ~3) - (h_rp[a] & ~3)); };
+        if (span(r0, r0 + 1) > cap) {
+            rb.push_back(r0);
+            lr.push_back(1);
+            r0 = r0 + 1;
+            continue;
+        }
+        // grow while within limits (binary search would be faster; this is setup)
+        int lo = r0 + 1, hi = std::min(n, r0 + max_rows);
+        // largest r1 in [lo, hi] with span(r0, r1) <= cap (span is monotone in r1)
+        while (lo < hi) {
+            int mid = (lo + hi + 1) / 2;
+            if (span(r0, mid) <= cap) lo = mid;
+            else hi = mid - 1;
+        }
+        r1 = lo;
+        rb.push_back(r0);
+        lr.push_back(0);
+        r0 = r1;
+    }
+    rb.push_back(n);
+    t.nblocks = (int)lr.size();
+    t.max_rows = max_rows;
+    t.cap = cap;
+    t.rb.alloc(rb.size());
+    t.rb.upload(rb.data(), rb.size(), s);
+    t.longrow.alloc(std::max<size_t>(lr.size(), 1));
+    if (!lr.empty()) t.longrow.upload(lr.data(), lr.size(), s);
+    XS_CUDA(cudaStreamSynchronize(s));
+}
+
+constexpr int SPMV_THREADS = 256;
+constexpr int SPMV_BYTES_PER_BUF = 48 * 1024;
+
+template <typename MT>
+inline int spmv_cap()
+{
+    return SPMV_BYTES_PER_BUF / (int)(sizeof(MT) + sizeof(int)) & ~3;
+}
+template <typename MT>
+inline size_t spmv_smem(int cap)
+{
+    return (size_t)2 * cap * (sizeof(MT) + sizeof(int));
+}
+
+template <typename VT, typename MT, typename Epi>
+inline int spmv_grid(int nblocks)
+{
+    static int per_sm = -1;
+    static int dev_sms = 0;
+    if (per_sm < 0) {
+        int cap = spmv_cap<MT>();
+        size_t sm = spmv_smem<MT>(cap);
+        XS_CUDA(cudaFuncSetAttribute(k_csr_spmv_tiled<VT, MT, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+        int occ = 0;
+        XS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_csr_spmv_tiled<VT, MT, Epi>, SPMV_THREADS, sm));
+        per_sm = occ > 0 ? occ : 1;
+        dev_sms = geom().sms;
+    }
+    long g = (long)per_sm * dev_sms;
+    if (g > nblocks) g = nblocks;
+    return (int)(g > 0 ? g : 1);
+}
+
+// Launch y = epi(A x) on the CSR tiled kernel (FP64 values if MT = double).
+template <typename VT, typename MT, typename Epi>
+inline void launch_csr(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot slot, cudaStream_t s, int grid = 0)
+{
+    const SpmvTiling &t = std::is_same<MT, double>::value ? op.tile64 : op.tile32;
+    CsrTileArgs<MT> a;
+    if constexpr (std::is_same<MT, double>::value) a = op.csr64();
+    else a = op.csr32();
+    int g = grid > 0 ? grid : spmv_grid<VT, MT, Epi>(t.nblocks);
+    size_t sm = spmv_smem<MT>(t.cap);
+    k_csr_spmv_tiled<VT, MT, Epi><<<g, SPMV_THREADS, sm, s>>>(a, x, y, epi, slot);
+    check_launch();
+}
+
+template <typename VT, typename MT, typename Epi>
+inline void launch_ell(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot slot, cudaStream_t s)
+{
+    EllArgs<MT> a;
+    if constexpr (std::is_same<MT, double>::value) a = op.ell64();
+    else a = op.ell32();
+    int g = op.ell_grid;
+    k_ell_spmv<VT, MT, Epi><<<g, 256, 0, s>>>(a, x, y, epi, slot);
+    check_launch();
+}
+
+// Dispatch on the operator's format.  The grid of each path is fixed per
+// operator so the fused reductions are deterministic.
+template <typename VT, typename MT, typename Epi>
+inline void spmv(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot slot, cudaStream_t s)
+{
+    if (op.format == 1) launch_ell<VT, MT, Epi>(op, x, y, epi, slot, s);
+    else launch_csr<VT, MT, Epi>(op, x, y, epi, slot, s);
+}
+
+// Build the operator's device CSR, tilings and (optionally) ELL from host CSR.
+void operator_setup(Operator &op, int n, const int *h_rp, const int *h_ci, const double *h_v, int base,
+                    bool want32, cudaStream_t s, int *d_err);
+void operator_build_ell(Operator &op, const int *h_rp, const int *h_ci, const double *h_v, int base, bool want32,
+                        cudaStream_t s);
+
+}  // namespace xs

@@ -1,0 +1,287 @@
+// Sync-free sparse triangular solves.
+//
+// Replaces the reference's triangular solves of the ILU preconditioners:
+//   * Lcsr_trsv_sync_free / Ucsc_trsv_sync_free (hip/Precond/gpuparilu.cpp:
+//     257-364): warp per row, unbounded spin on an int flag array, per-call
+//     hipMalloc, not on the default path;
+//   * Lsolve_iter / Usolve_iter (DeviceMatrixCSR.cpp:281-304): the default
+//     path, an approximate solve by k Jacobi sweeps (kept here as an option).
+//
+// Design
+//   Rows are renumbered into "positions" sorted by dependency level (rows of
+//   level 0 first), so every dependency of a position lies at a smaller
+//   position.  Blocks take consecutive position ranges through a ticket
+//   counter (atomicAdd at block start), so a block only ever waits on blocks
+//   that are already running or finished: no deadlock whatever order the
+//   hardware schedules blocks in.  One thread solves one row; its entries are
+//   stored contiguously per position, in exactly the order the CPU reference
+//   accumulates them (L: increasing column; U: decreasing column), with
+//   separate multiply and subtract, so the FP64 result is bitwise identical
+//   to hip/HostMatrix/HostMatrixCSR.cpp:385-409 (LUsolve).
+//
+//   Readiness is carried by the value itself: the solve buffer is pre-filled
+//   with a NaN bit pattern that arithmetic never produces, and a row is
+//   ready when its value differs from it.  A waiting thread issues the loads
+//   of up to 8 dependencies at once and re-polls only the pending ones, so a
+//   dependency hop costs one L2 round trip.  The L solve re-arms the U
+//   buffer and the U solve re-arms the L buffer, so no separate reset pass is
+//   needed.  Each spin is bounded (DEV_TRSV_TIMEOUT recorded, kernel returns),
+//   and any thread seeing the error word set stops waiting.
+#pragma once
+#include <vector>
+#include <algorithm>
+#include "xs_internal.cuh"
+
+namespace xs {
+
+constexpr int TRSV_THREADS = 128;
+constexpr int TRSV_CHUNK = 8;
+constexpr long TRSV_SPIN_CAP = 1L << 22;
+
+template <typename FT>
+struct TrsvArgs {
+    int n;
+    const int *perm;
+    const int *prp;
+    const int *pci;
+    const FT *pv;
+};
+
+template <typename VT>
+struct CalcT {
+    using T = VT;
+};
+
+// acc - y*v in the vector type; FP64: separate multiply and subtract (the
+// library is compiled without FMA contraction), FP32: fused.
+__device__ __forceinline__ double msub(double acc, double y, double v) { return acc - y * v; }
+__device__ __forceinline__ float msub(float acc, float y, float v) { return __fmaf_rn(-y, v, acc); }
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+__global__ void __launch_bounds__(TRSV_THREADS) k_trsv_syncfree(TrsvArgs<FT> P, const DT *__restrict__ dinv,
+                                                               const VT *rhs, VT *self, VT *out_user, VT *reset_other,
+                                                               const int *done_flag, int *err, unsigned *ticket)
+{
+    if (done_flag && *done_flag) return;
+    __shared__ int s_blk;
+    if (threadIdx.x == 0) {
+        unsigned t = atomicAdd(ticket, 1u);
+        if (t == gridDim.x - 1) *ticket = 0u;  // every block already holds its ticket
+        s_blk = (int)t;
+    }
+    __syncthreads();
+    const int p = s_blk * TRSV_THREADS + (int)threadIdx.x;
+    if (p >= P.n) return;
+    const int row = __ldg(P.perm + p);
+    VT acc;
+    if (!UPPER) {
+        acc = rhs[row];
+    } else {
+        const VT yv = rhs[row];
+        acc = yv * (VT)__ldg(dinv + p);
+    }
+    if (reset_other) reset_other[row] = Sentinel<VT>::value();
+    const int k0 = __ldg(P.prp + p), k1 = __ldg(P.prp + p + 1);
+    bool failed = false;
+    for (int base = k0; base < k1; base += TRSV_CHUNK) {
+        const int cnt = min(TRSV_CHUNK, k1 - base);
+        int c[TRSV_CHUNK];
+        VT yv[TRSV_CHUNK];
+        VT fv[TRSV_CHUNK];
+        unsigned pending = 0;
+#pragma unroll
+        for (int j = 0; j < TRSV_CHUNK; j++) {
+            if (j < cnt) {
+                c[j] = __ldg(P.pci + base + j);
+                fv[j] = (VT)FVal<FT>::ld(P.pv, base + j);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < TRSV_CHUNK; j++) {
+            if (j < cnt) {
+                yv[j] = ld_poll(self + c[j]);
+                if (Sentinel<VT>::is(yv[j])) pending |= 1u << j;
+            }
+        }
+        long spins = 0;
+        while (pending) {
+#pragma unroll
+            for (int j = 0; j < TRSV_CHUNK; j++) {
+                if (pending & (1u << j)) {
+                    yv[j] = ld_poll(self + c[j]);
+                    if (!Sentinel<VT>::is(yv[j])) pending &= ~(1u << j);
+                }
+            }
+            if (pending && ((++spins & 1023) == 0)) {
+                if (spins > TRSV_SPIN_CAP) {
+                    atomicOr(err, DEV_TRSV_TIMEOUT);
+                    failed = true;
+                    break;
+                }
+                if (*(volatile int *)err) {
+                    failed = true;
+                    break;
+                }
+            }
+        }
+        if (failed) break;
+#pragma unroll
+        for (int j = 0; j < TRSV_CHUNK; j++)
+            if (j < cnt) acc = msub(acc, yv[j], fv[j]);
+    }
+    if (failed) return;  // leaves the row unpublished; dependants stop on the error word
+    st_publish(self + row, acc);
+    if (out_user) out_user[row] = acc;
+}
+
+// Re-arm a solve buffer (used at setup and after an aborted solve).
+template <typename VT>
+__global__ void k_fill_sentinel(VT *b, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = Sentinel<VT>::value();
+}
+
+// ---------------------------------------------------------------- Jacobi-sweep mode
+// Reference GPU path (DeviceMatrixCSR.cpp:14-58, 281-304): y = 0, then k times
+// y = x - L_off y   (L) / y = dinv*x - U' y  (U, row-scaled form).
+// Each sweep reads the previous iterate and writes the next (double buffer).
+template <typename VT, typename FT, typename DT, bool UPPER>
+__global__ void k_trsv_sweep(int n, const int *__restrict__ rp, const int *__restrict__ ci, const FT *__restrict__ v,
+                             const DT *__restrict__ dinv_row, const VT *__restrict__ x, const VT *__restrict__ yin,
+                             VT *__restrict__ yout, int first, const int *done_flag)
+{
+    if (done_flag && *done_flag) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        VT acc = UPPER ? (VT)(x[i] * (VT)dinv_row[i]) : x[i];
+        if (!first) {
+            for (int k = rp[i]; k < rp[i + 1]; k++) acc = msub(acc, yin[ci[k]], (VT)FVal<FT>::ld(v, k));
+        }
+        yout[i] = acc;
+    }
+}
+
+// ---------------------------------------------------------------- host plan building
+// Host-side analysis of a triangular pattern.
+struct TriHostPlan {
+    int n = 0;
+    int nlevels = 0;
+    std::vector<int> perm;  // position -> row
+    std::vector<int> prp;   // position rowptr
+    std::vector<int> pci;   // dependency row per entry
+    std::vector<long> src;  // source index of each entry in the value array
+    std::vector<int> level; // per row
+};
+
+// rp/ci: CSR of the strict triangle (0-based); src_of(k) maps entry k of the
+// triangle's CSR to its index in the value array the values will be gathered
+// from.  upper: dependencies on larger rows, entries summed in decreasing
+// column order.
+template <typename SrcF>
+inline void tri_analyse(int n, const int *rp, const int *ci, bool upper, SrcF src_of, TriHostPlan &h)
+{
+    h.n = n;
+    h.level.assign(n, 0);
+    int maxl = 0;
+    if (!upper) {
+        for (int i = 0; i < n; i++) {
+            int l = 0;
+            for (int k = rp[i]; k < rp[i + 1]; k++) l = std::max(l, h.level[ci[k]] + 1);
+            h.level[i] = l;
+            maxl = std::max(maxl, l);
+        }
+    } else {
+        for (int i = n - 1; i >= 0; i--) {
+            int l = 0;
+            for (int k = rp[i]; k < rp[i + 1]; k++) l = std::max(l, h.level[ci[k]] + 1);
+            h.level[i] = l;
+            maxl = std::max(maxl, l);
+        }
+    }
+    h.nlevels = n > 0 ? maxl + 1 : 0;
+    // counting sort by level, rows ascending within a level
+    std::vector<int> cnt(h.nlevels + 1, 0);
+    for (int i = 0; i < n; i++) cnt[h.level[i] + 1]++;
+    for (int l = 0; l < h.nlevels; l++) cnt[l + 1] += cnt[l];
+    h.perm.assign(n, 0);
+    for (int i = 0; i < n; i++) h.perm[cnt[h.level[i]]++] = i;
+    h.prp.assign(n + 1, 0);
+    for (int p = 0; p < n; p++) {
+        int r = h.perm[p];
+        h.prp[p + 1] = h.prp[p] + (rp[r + 1] - rp[r]);
+    }
+    long nnz = h.prp[n];
+    h.pci.assign(nnz, 0);
+    h.src.assign(nnz, 0);
+    for (int p = 0; p < n; p++) {
+        int r = h.perm[p];
+        int q = h.prp[p];
+        if (!upper) {
+            for (int k = rp[r]; k < rp[r + 1]; k++, q++) { h.pci[q] = ci[k]; h.src[q] = src_of(k); }
+        } else {
+            for (int k = rp[r + 1] - 1; k >= rp[r]; k--, q++) { h.pci[q] = ci[k]; h.src[q] = src_of(k); }
+        }
+    }
+}
+
+// Device copy of a triangle prepared for the sync-free solve.  Values are
+// gathered on the device from a value array (so re-factorisation or a change
+// of storage precision does not repeat the host analysis).
+struct TriDev {
+    int n = 0;
+    long nnz = 0;
+    int nlevels = 0;
+    bool upper = false;
+    DBuf<int> perm, prp, pci;
+    DBuf<long> src;
+    DBuf<int> rp_nat, ci_nat;    // natural-order CSR of the triangle (Jacobi-sweep mode)
+    DBuf<long> src_nat;
+    DBuf<double> pv64, nv64;     // position-order and natural-order values (FP64)
+    DBuf<float> pv32, nv32;
+    DBuf<__nv_bfloat16> pvbf, nvbf;
+    DBuf<__half> pvh, nvh;
+    DBuf<double> dinv64;         // U: per position; also natural order for sweeps
+    DBuf<float> dinv32;
+    DBuf<double> dinv64_nat;
+    DBuf<float> dinv32_nat;
+    DBuf<unsigned> ticket;
+
+    template <typename FT>
+    TrsvArgs<FT> args() const;
+};
+
+template <>
+inline TrsvArgs<double> TriDev::args<double>() const { return TrsvArgs<double>{n, perm.p, prp.p, pci.p, pv64.p}; }
+template <>
+inline TrsvArgs<float> TriDev::args<float>() const { return TrsvArgs<float>{n, perm.p, prp.p, pci.p, pv32.p}; }
+template <>
+inline TrsvArgs<__nv_bfloat16> TriDev::args<__nv_bfloat16>() const
+{
+    return TrsvArgs<__nv_bfloat16>{n, perm.p, prp.p, pci.p, pvbf.p};
+}
+template <>
+inline TrsvArgs<__half> TriDev::args<__half>() const { return TrsvArgs<__half>{n, perm.p, prp.p, pci.p, pvh.p}; }
+
+// gather + convert: dst[q] = (FT) src_vals[src[q]]
+template <typename FT>
+__global__ void k_gather_convert(long m, const long *__restrict__ src, const double *__restrict__ vals, FT *dst)
+{
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < m; q += (long)gridDim.x * blockDim.x) {
+        double v = vals[src[q]];
+        if constexpr (std::is_same<FT, double>::value) dst[q] = v;
+        else if constexpr (std::is_same<FT, float>::value) dst[q] = (float)v;
+        else if constexpr (std::is_same<FT, __nv_bfloat16>::value) dst[q] = __double2bfloat16(v);
+        else dst[q] = __double2half(v);
+    }
+}
+// dinv per position: dst[p] = vals[diagpos[perm[p]]]
+template <typename DT>
+__global__ void k_gather_dinv(int n, const int *__restrict__ perm, const long *__restrict__ diagsrc,
+                              const double *__restrict__ vals, DT *dst)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int r = perm ? perm[p] : p;
+        dst[p] = (DT)vals[diagsrc[r]];
+    }
+}
+
+}  // namespace xs
