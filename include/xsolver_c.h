@@ -155,6 +155,11 @@ int xs_adjoint_batch(xs_handle_t h, int nrhs, const double *x, const double *dLd
 /* timing of the last solve, in milliseconds (CUDA events around the solve
  * on the handle's stream): setup = preconditioner construction */
 int xs_last_timing(xs_handle_t h, double *setup_ms, double *solve_ms, int *iterations, double *final_relres);
+/* the CUDA stream (cudaStream_t) all of the handle's work is ordered on */
+int xs_get_stream(xs_handle_t h, void **stream);
+/* kernels launched by the last solve (captured graph nodes replayed + direct
+ * launches) */
+int xs_last_launches(xs_handle_t h, long long *count);
 /* number of refinement (outer) steps of the last mixed-precision solve */
 int xs_last_outer_steps(xs_handle_t h, int *outer_steps);
 

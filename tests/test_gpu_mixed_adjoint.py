@@ -1,0 +1,131 @@
+"""Mixed-precision iterative refinement and the adjoint.
+
+Mixed: FP64 outer residual/update around an FP32 inner solve with FP32 /
+BF16 / FP16 ILU factors; the refined solution must reach relative residual
+1e-10 and agree with an FP64 solve converged to 1e-14.
+Adjoint: dL/db and dL/dA from the transposed solve against central finite
+differences (h = 1e-6, probe solves at 1e-14) and against the oracle's
+transposed solve."""
+import numpy as np
+import pytest
+
+import oracle
+from xsolver_b200 import stencils as st
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("ksp", ["bicgstab", "gmres"])
+@pytest.mark.parametrize("factor", ["fp32", "bf16", "fp16"])
+def test_mixed_refinement_reaches_1e10(cuda, ksp, factor):
+    from xsolver_b200.api import Solver
+
+    A = st.poisson3d_7pt(40) if ksp == "bicgstab" else st.convdiff3d_27pt(20)
+    b = st.rhs_uniform(A.n, 0, -1.0 if ksp == "bicgstab" else 0.0, 1.0)
+    S = Solver(A).ksp_settype(ksp).ksp_setoption(1e-10, 2000, 30).pc_settype("ilu0")
+    S.set_precision("fp64", "fp32", factor).set_inner(1e-4, 200)
+    x = S.solve(b)
+    r = b - A.to_scipy() @ x
+    relres = np.linalg.norm(r) / np.linalg.norm(b)
+    assert relres < 1e-10, relres
+    assert S.outer_steps() >= 2
+    ref = Solver(A).ksp_settype(ksp).ksp_setoption(1e-14, 4000, 30).pc_settype("ilu0").solve(b)
+    err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+    # the error is bounded by cond(A) * 1e-10; these systems are mildly conditioned
+    assert err < 1e-7, err
+
+
+def _loss_grad(x, xs):
+    return x - xs
+
+
+def test_adjoint_vs_finite_differences(cuda):
+    from xsolver_b200.api import Solver
+
+    A = st.varcoef3d_7pt(9, seed=4)
+    n = A.n
+    rng = np.random.default_rng(0)
+    b = st.rhs_uniform(n, 1)
+    xs = rng.uniform(-1, 1, n)
+
+    def solve(vals, rhs, tol=1e-14):
+        S = Solver(st.CSRMatrix(n, A.rowptr, A.colidx, vals)).ksp_settype("cg").ksp_setoption(tol, 4000).pc_settype(
+            "ilu0")
+        return S.solve(rhs), S
+
+    x, S = solve(A.val, b)
+    dLdb, dLdA = S.adjoint(_loss_grad(x, xs))
+    L = lambda xx: 0.5 * np.sum((xx - xs) ** 2)  # noqa: E731
+    h = 1e-6
+    picks = rng.choice(A.nnz, 8, replace=False)
+    for k in picks:
+        vp = A.val.copy(); vp[k] += h
+        vm = A.val.copy(); vm[k] -= h
+        fd = (L(solve(vp, b)[0]) - L(solve(vm, b)[0])) / (2 * h)
+        assert abs(fd - dLdA[k]) <= 1e-6 * max(abs(fd), 1e-3), (k, fd, dLdA[k])
+    for i in rng.choice(n, 8, replace=False):
+        bp = b.copy(); bp[i] += h
+        bm = b.copy(); bm[i] -= h
+        fd = (L(solve(A.val, bp)[0]) - L(solve(A.val, bm)[0])) / (2 * h)
+        assert abs(fd - dLdb[i]) <= 1e-6 * max(abs(fd), 1e-3), (i, fd, dLdb[i])
+
+
+def test_adjoint_nonsymmetric_vs_oracle_transposed_solve(cuda):
+    """On a nonsymmetric matrix, lambda must solve A^T lambda = g: compare
+    with the oracle solving the explicitly transposed system."""
+    from xsolver_b200.api import Solver
+
+    A = st.convdiff3d_27pt(10)
+    n = A.n
+    b = st.rhs_uniform(n, 2, 0.0, 1.0)
+    S = Solver(A).ksp_settype("gmres").ksp_setoption(1e-13, 2000, 30).pc_settype("ilu0")
+    x = S.solve(b)
+    g = st.rhs_uniform(n, 3)
+    dLdb, dLdA = S.adjoint(g)
+    At = A.to_scipy().T.tocsr()
+    At.sort_indices()
+    T = st.CSRMatrix(n, At.indptr, At.indices, At.data)
+    lam, _, _ = oracle.solve("fgmres", T, g, tol=1e-13, maxiter=2000, restart=30, pc="lu", factors=oracle.ilu0(T),
+                             quirk=0)
+    assert np.linalg.norm(dLdb - lam) / np.linalg.norm(lam) < 1e-9
+    rows = np.repeat(np.arange(n), np.diff(A.rowptr))
+    assert np.allclose(dLdA, -dLdb[rows] * x[A.colidx], rtol=1e-12, atol=1e-14)
+
+
+def test_adjoint_batch_matches_single(cuda):
+    from xsolver_b200.api import Solver
+
+    A = st.varcoef3d_7pt(8, seed=7)
+    n = A.n
+    S = Solver(A).ksp_settype("cg").ksp_setoption(1e-12, 2000).pc_settype("ilu0")
+    B = np.stack([st.rhs_uniform(n, s) for s in range(3)])
+    X = S.solve_batch(B)
+    G = X - 0.5
+    DB, DA = S.adjoint_batch(X, G)
+    for k in range(3):
+        S.solve(B[k])
+        db, da = S.adjoint(G[k])
+        assert np.allclose(DB[k], db, rtol=1e-12, atol=1e-15)
+        assert np.allclose(DA[k], da, rtol=1e-12, atol=1e-15)
+
+
+def test_autograd_function(cuda):
+    import torch
+    from xsolver_b200.autograd import SparseSolve, configured_solver
+
+    A = st.varcoef3d_7pt(6, seed=2)
+    S = configured_solver(A, ksp="cg", pc="ilu0", tol=1e-14)
+    vals = torch.tensor(A.val, dtype=torch.float64, requires_grad=True)
+    b = torch.tensor(st.rhs_uniform(A.n, 0), dtype=torch.float64, requires_grad=True)
+    x = SparseSolve.apply(vals, b, S)
+    loss = 0.5 * (x ** 2).sum()
+    loss.backward()
+    # check against a dense solve
+    Ad = torch.tensor(A.to_scipy().toarray(), dtype=torch.float64, requires_grad=True)
+    bd = b.detach().clone().requires_grad_(True)
+    xd = torch.linalg.solve(Ad, bd)
+    (0.5 * (xd ** 2).sum()).backward()
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    gA = Ad.grad.numpy()[rows, A.colidx]
+    assert np.allclose(b.grad.numpy(), bd.grad.numpy(), rtol=1e-8, atol=1e-12)
+    assert np.allclose(vals.grad.numpy(), gA, rtol=1e-8, atol=1e-12)

@@ -69,6 +69,8 @@ def _declare(L):
         "xs_adjoint_batch": [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp],
         "xs_last_timing": [C.c_void_p, _dp, _dp, _ip, _dp],
         "xs_last_outer_steps": [C.c_void_p, _ip],
+        "xs_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
+        "xs_last_launches": [C.c_void_p, C.POINTER(C.c_longlong)],
         "xs_plan_create": [C.POINTER(C.c_void_p), C.c_int, _ip, _ip, _dp],
         "xs_plan_destroy": [C.c_void_p],
         "xs_plan_build_ell": [C.c_void_p, _ip],

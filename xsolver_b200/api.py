@@ -143,6 +143,16 @@ class Solver:
         check(self._L.xs_last_timing(self.h, C.byref(s), C.byref(t), C.byref(it), C.byref(r)), "xs_last_timing")
         return {"setup_ms": s.value, "solve_ms": t.value, "iterations": it.value, "final_relres": r.value}
 
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        check(self._L.xs_get_stream(self.h, C.byref(p)), "xs_get_stream")
+        return p.value or 0
+
+    def launches(self) -> int:
+        c = C.c_longlong()
+        check(self._L.xs_last_launches(self.h, C.byref(c)), "xs_last_launches")
+        return c.value
+
     def outer_steps(self) -> int:
         o = C.c_int()
         check(self._L.xs_last_outer_steps(self.h, C.byref(o)), "xs_last_outer_steps")

@@ -25,6 +25,7 @@ class SparseSolve(torch.autograd.Function):
         if not np.array_equal(vals, A.val):
             # same pattern, new values: rebuild the handle's matrix
             newA = CSRMatrix(A.n, A.rowptr, A.colidx, vals, A.name)
+            solver.close()
             solver.__init__(newA)  # type: ignore[misc]
             for step in getattr(solver, "_config", []):
                 step()

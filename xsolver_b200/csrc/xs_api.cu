@@ -179,6 +179,7 @@ struct Handle {
     // results
     double setup_ms = 0, solve_ms = 0, final_relres = 0;
     int last_iters = 0;
+    long long launches = 0;  // kernels launched by the last solve (graph nodes + direct)
     // adjoint
     AdjointState adj;
     DBuf<OuterState> outer_st;
@@ -511,9 +512,9 @@ static void prepare_state(Handle &h, int maxiter, double tol, double abstol, boo
 // and preconditioner
 template <typename VT>
 static void run_method_on(RunSet<VT> &R, Operator &A, PrecondDev &M, Workspace &W, cudaStream_t s, int n, int quirk,
-                          int method, const VT *b, VT *x, int restart)
+                          int method, const VT *b, VT *x, int restart, long long *launches = nullptr)
 {
-    SolveCtx c{s, &A, &M, &W, n, 8, quirk};
+    SolveCtx c{s, &A, &M, &W, n, 8, quirk, launches};
     if (n < 200000) c.chunk = 16;
     switch (method) {
     case KSP_CGM: R.pcg.run(c, b, x); break;
@@ -534,9 +535,9 @@ template <typename VT>
 static void run_method(Handle &h, int method, const VT *b, VT *x, int restart)
 {
     if constexpr (std::is_same<VT, double>::value)
-        run_method_on<double>(h.r64, h.A, h.M, h.W, h.s, h.n, h.quirk, method, b, x, restart);
+        run_method_on<double>(h.r64, h.A, h.M, h.W, h.s, h.n, h.quirk, method, b, x, restart, &h.launches);
     else
-        run_method_on<float>(h.r32, h.A, h.M, h.W, h.s, h.n, h.quirk, method, b, x, restart);
+        run_method_on<float>(h.r32, h.A, h.M, h.W, h.s, h.n, h.quirk, method, b, x, restart, &h.launches);
 }
 
 static int effective_restart(const Handle &h)
@@ -593,6 +594,7 @@ static void solve_device(Handle &h, const double *d_b, double *d_x)
     int iters = 0;
     std::vector<double> hist;
     int done = 0, devflags = 0;
+    h.launches = 4;  // residual SpMV, preconditioner (<= 2 kernels), init reduction
     if (!h.inner32) {
         prepare_state(h, h.maxiter, h.tol, h.abstol, true);
         run_method<double>(h, h.method, b, x, restart);
@@ -661,6 +663,7 @@ static void solve_device(Handle &h, const double *d_b, double *d_x)
             XS_CUDA(cudaMemcpyAsync(&hos, os, sizeof(OuterState), cudaMemcpyDeviceToHost, h.s));
             XS_CUDA(cudaStreamSynchronize(h.s));
             iters += std::max(it_in, 1);
+            h.launches += 7;  // convert, refinement update, outer residual SpMV, inner init
             rn = hos.rnorm;
             hist.push_back(rn);
             outer++;
@@ -694,7 +697,10 @@ static void solve_device(Handle &h, const double *d_b, double *d_x)
     XS_CUDA(cudaStreamSynchronize(h.s));
     int e = read_dev_err(h) | devflags;
     if (e & (DEV_TRSV_TIMEOUT | DEV_TMA_TIMEOUT | DEV_FACTOR_TIMEOUT)) {
+        // an aborted kernel may leave solve buffers and reduction tickets
+        // mid-way: re-arm them so the handle stays usable
         h.M.rearm(h.s);
+        XS_CUDA(cudaMemsetAsync(h.W.ticket.p, 0, sizeof(unsigned), h.s));
         XS_CUDA(cudaStreamSynchronize(h.s));
     }
     h.have_solution = true;
@@ -1195,6 +1201,22 @@ int xs_last_timing(xs_handle_t h, double *setup_ms, double *solve_ms, int *itera
         if (solve_ms) *solve_ms = H.solve_ms;
         if (iterations) *iterations = H.last_iters;
         if (relres) *relres = H.final_relres;
+    });
+}
+int xs_get_stream(xs_handle_t h, void **stream)
+{
+    return guarded([&] {
+        HCHK(h);
+        if (!stream) throw Status(XS_ERR_INVALID);
+        *stream = (void *)h->h->s;
+    });
+}
+int xs_last_launches(xs_handle_t h, long long *count)
+{
+    return guarded([&] {
+        HCHK(h);
+        if (!count) throw Status(XS_ERR_INVALID);
+        *count = h->h->launches;
     });
 }
 int xs_last_outer_steps(xs_handle_t h, int *o)

@@ -23,7 +23,6 @@
 
 namespace xs {
 
-constexpr long FACTOR_SPIN_CAP = 1L << 24;
 
 // exact ILU(0), thread per row in level order (perm/level from the L analysis)
 __global__ void __launch_bounds__(128) k_ilu0_rows(int n, const int *__restrict__ rp, const int *__restrict__ ci,
@@ -44,9 +43,12 @@ __global__ void __launch_bounds__(128) k_ilu0_rows(int n, const int *__restrict_
     for (int j = rs; j < up; j++) {
         const int k = ci[j];
         long spins = 0;
+        unsigned long long t0 = 0;
         while (ld_acquire(flag + k) != epoch) {
-            if ((++spins & 1023) == 0) {
-                if (spins > FACTOR_SPIN_CAP) {
+            if ((++spins & 255) == 0) {
+                const unsigned long long t = gtimer();
+                if (t0 == 0) t0 = t;
+                else if (t - t0 > WAIT_LIMIT_NS) {
                     atomicOr(err, DEV_FACTOR_TIMEOUT);
                     return;
                 }

@@ -167,6 +167,15 @@ struct Sentinel<float> {
     __device__ static bool is(float v) { return (uint32_t)__float_as_int(v) == sentinel_bits32(); }
 };
 
+// nanosecond wall clock for bounding every spin-wait
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;  // 1 s
+
 // relaxed, L1-bypassing accesses for values other SMs write while we poll
 __device__ __forceinline__ double ld_poll(const double *p)
 {

@@ -38,6 +38,7 @@ struct VecPool {
 };
 
 struct GraphCache {
+    size_t nodes = 0;  // kernel nodes in the captured graph
     GraphCache() = default;
     GraphCache(const GraphCache &) = delete;
     GraphCache &operator=(const GraphCache &) = delete;
@@ -60,6 +61,7 @@ struct SolveCtx {
     int n;
     int chunk = 8;
     int quirk = 1;
+    long long *launches = nullptr;  // kernels launched (graph nodes), accumulated
 };
 
 // configuration that changes the captured kernels
@@ -86,6 +88,9 @@ inline void run_graph_loop(SolveCtx &c, GraphCache &gc, const std::vector<const 
             throw;
         }
         XS_CUDA(cudaStreamEndCapture(c.s, &g));
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        gc.nodes = nn;
         cudaError_t e = cudaGraphInstantiate(&gc.exec, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) throw Status(XS_ERR_CUDA);
@@ -101,6 +106,7 @@ inline void run_graph_loop(SolveCtx &c, GraphCache &gc, const std::vector<const 
     bool stop = false;
     for (int l = 0; l < max_launches && !stop; l++) {
         XS_CUDA(cudaGraphLaunch(gc.exec, c.s));
+        if (c.launches) *c.launches += (long long)gc.nodes;
         XS_CUDA(cudaMemcpyAsync(&hflag[l & 1], &dst->done, sizeof(int), cudaMemcpyDeviceToHost, c.s));
         XS_CUDA(cudaEventRecord(ev[l & 1], c.s));
         if (l > 0) {

@@ -65,8 +65,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 // bounded wait; returns false (and records DEV_TMA_TIMEOUT) if the copy never lands
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err)
 {
-    for (long it = 0; it < (1L << 26); it++)
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    for (long it = 1;; it++) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255) == 0 && gtimer() - t0 > 2 * WAIT_LIMIT_NS) break;
+    }
     if (err) atomicOr(err, DEV_TMA_TIMEOUT);
     return false;
 }

@@ -36,7 +36,6 @@ namespace xs {
 
 constexpr int TRSV_THREADS = 128;
 constexpr int TRSV_CHUNK = 8;
-constexpr long TRSV_SPIN_CAP = 1L << 22;
 
 template <typename FT>
 struct TrsvArgs {
@@ -104,6 +103,7 @@ __global__ void __launch_bounds__(TRSV_THREADS) k_trsv_syncfree(TrsvArgs<FT> P, 
             }
         }
         long spins = 0;
+        unsigned long long t0 = 0;
         while (pending) {
 #pragma unroll
             for (int j = 0; j < TRSV_CHUNK; j++) {
@@ -112,8 +112,10 @@ __global__ void __launch_bounds__(TRSV_THREADS) k_trsv_syncfree(TrsvArgs<FT> P, 
                     if (!Sentinel<VT>::is(yv[j])) pending &= ~(1u << j);
                 }
             }
-            if (pending && ((++spins & 1023) == 0)) {
-                if (spins > TRSV_SPIN_CAP) {
+            if (pending && ((++spins & 255) == 0)) {
+                const unsigned long long t = gtimer();
+                if (t0 == 0) t0 = t;
+                else if (t - t0 > WAIT_LIMIT_NS) {
                     atomicOr(err, DEV_TRSV_TIMEOUT);
                     failed = true;
                     break;
