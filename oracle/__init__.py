@@ -218,6 +218,11 @@ def levels_lower(n, rp, ci):
 PC = {"none": 0, "jacobi": 1, "lu": 2}
 
 
+def set_dot_mode(mode: str):
+    """'sequential' (the reference's order) or 'pairwise' (another valid order)."""
+    lib().orc_set_dot_mode({"sequential": 0, "pairwise": 1}[mode])
+
+
 def solve(method, A, rhs, x0=None, tol=1e-8, maxiter=1000, restart=30, pc="jacobi", factors: LU | None = None,
           quirk=1):
     """Run a restated Krylov loop.  method: cg, cgm, bicgstab, gcr, igcr,

@@ -43,8 +43,23 @@
 namespace {
 
 /* ---------------- BLAS-1, sequential order ---------------- */
+/* dot-product order: 0 = sequential (the reference's cblas_ddot through the
+ * sequential shim), 1 = pairwise (another valid order, used to measure how
+ * sensitive a reference solve is to the summation order of its dots) */
+int g_dot_mode = 0;
+double o_dot_pairwise(int n, const double *x, const double *y)
+{
+    if (n <= 8) {
+        double s = 0.0;
+        for (int i = 0; i < n; i++) s += x[i] * y[i];
+        return s;
+    }
+    int h = n / 2;
+    return o_dot_pairwise(h, x, y) + o_dot_pairwise(n - h, x + h, y + h);
+}
 double o_dot(int n, const double *x, const double *y)
 {
+    if (g_dot_mode == 1) return o_dot_pairwise(n, x, y);
     double s = 0.0;
     for (int i = 0; i < n; i++) s += x[i] * y[i];
     return s;
@@ -683,6 +698,9 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
 }
 
 void orc_free(void *p) { std::free(p); }
+
+/* select the dot-product summation order of the restated Krylov loops */
+void orc_set_dot_mode(int mode) { g_dot_mode = mode; }
 
 /* ========================= Krylov loops ========================= */
 /*

@@ -628,8 +628,8 @@ static void solve_device(Handle &h, const double *d_b, double *d_x)
         double *r = h.vpool64.get(2, n);
         float *r32 = h.vpool32.get(0, n), *d32 = h.vpool32.get(1, n);
         operator_ensure32(h.A, h.hrp.data(), h.s);
-        RedSlot sl = h.W.slot();
         prepare_state(h, std::max(h.inner_maxiter, 1), h.inner_rtol, 0.0, true);
+        const RedSlot sl = h.W.slot();  // after prepare_state: the workspace exists now
         spmv<double, double>(h.A, x, r, EpiOuterResid<double>{os, b}, sl, h.s);
         OuterState hos;
         XS_CUDA(cudaMemcpyAsync(&hos, os, sizeof(OuterState), cudaMemcpyDeviceToHost, h.s));

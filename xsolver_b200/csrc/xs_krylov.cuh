@@ -569,7 +569,11 @@ struct Workspace {
     DBuf<double> hist, hist_rel;
     int hist_cap = 0;
     int part_cap = 0;
-    RedSlot slot() const { return RedSlot{part.p, ticket.p}; }
+    RedSlot slot() const
+    {
+        if (!part.p || !ticket.p) throw Status(XS_ERR_ORDER);  // ensure() must run first
+        return RedSlot{part.p, ticket.p};
+    }
     void ensure(int max_k, int maxiter)
     {
         int G = std::max(geom().red_grid, geom().sms * 8);

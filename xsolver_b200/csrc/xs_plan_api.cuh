@@ -81,8 +81,8 @@ int xs_plan_spmv(xs_plan_t p, int format, int precision, const void *x, void *y)
         if (format == 1 && h.A.ell_w == 0) throw Status(XS_ERR_ORDER);
         int saved = h.A.format;
         h.A.format = format;
-        RedSlot sl = h.W.slot();
         h.W.ensure(64, 1);
+        const RedSlot sl = h.W.slot();
         if (precision == 0)
             spmv<double, double>(h.A, (const double *)x, (double *)y, EpiAx<double>{}, sl, h.s);
         else {
