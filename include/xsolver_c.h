@@ -239,6 +239,12 @@ int xs_plan_lusolve_t(xs_plan_t p, const double *d_x, double *d_z);
 /* wait for the plan's stream; returns the device status word (e.g. a
  * sync-free timeout) */
 int xs_plan_sync(xs_plan_t p);
+/* Testing hook for the bounded waits: with enable != 0, the first dependency
+ * of the L-solve row at `position` is redirected to the row itself, a value
+ * that no thread ever publishes, so the next L solve waits out its limit
+ * (about a second) and reports XS_ERR_TRSV_TIMEOUT through xs_plan_sync;
+ * enable = 0 restores the dependency. */
+int xs_plan_debug_break_dependency(xs_plan_t p, int position, int enable);
 /* number of dependency levels of L and U */
 int xs_plan_levels(xs_plan_t p, int *levelsL, int *levelsU);
 /* average device time in ms of `reps` repetitions of op (0 CSR SpMV FP64,

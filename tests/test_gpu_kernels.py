@@ -190,3 +190,40 @@ def test_levels_match_oracle(cuda):
     A = st.poisson3d_7pt(20)
     P = Plan(A).factor("ilu0")
     assert P.levels() == (3 * 20 - 2, 3 * 20 - 2)
+
+
+def test_parilut_bitwise_vs_oracle(cuda):
+    """GPU ParILUT (synchronous sweeps, radix-select thresholds) equals the
+    CPU restatement entry for entry."""
+    from xsolver_b200.api import Plan
+
+    for A, fill, sweeps, droptol in ((st.convdiff3d_27pt(9), 2.0, 5, 0.0), (st.poisson3d_7pt(12), 3.0, 4, 0.0),
+                                     (st.convdiff3d_27pt(8, pe=10.0), 2.0, 3, 1e-4)):
+        P = Plan(A).factor("parilut", sweeps=sweeps, fill=fill, droptol=droptol)
+        G = P.factors()
+        F = oracle.parilut(A, fill=fill, sweeps=sweeps, droptol=droptol)
+        for k in ("lrp", "lci", "lv", "dinv", "urp", "uci", "uv"):
+            assert np.array_equal(G[k], getattr(F, k)), (A.name, k)
+
+
+def test_syncfree_wait_times_out_and_recovers(cuda):
+    """A dependency nothing publishes: the bounded wait gives up (about 1 s),
+    the error is reported, and the plan works again after the dependency is
+    restored."""
+    import torch
+    from xsolver_b200.api import Plan, XsError
+
+    A = st.poisson3d_7pt(16)
+    P = Plan(A).factor("ilu0")
+    F = oracle.ilu0(A)
+    x = st.rhs_uniform(A.n, 1)
+    z = torch.zeros(A.n, dtype=torch.float64, device=cuda)
+    P.debug_break_dependency(A.n - 1, True)
+    P.lusolve(_dev(x, cuda), z)
+    with pytest.raises(XsError) as e:
+        P.sync()
+    assert e.value.code == 5  # XS_ERR_TRSV_TIMEOUT
+    P.debug_break_dependency(A.n - 1, False)
+    P.lusolve(_dev(x, cuda), z)
+    P.sync()
+    assert np.array_equal(z.cpu().numpy(), oracle.lusolve(F, x))

@@ -248,3 +248,22 @@ def test_one_based_input_and_warm_start(cuda):
     x2 = S.solve(b, x0=x)
     assert S.usediter <= 1 < it1
     assert np.allclose(x, x2, rtol=1e-10, atol=1e-12)
+
+
+def test_gmres_gcr_parilut_convdiff(cuda):
+    """27-point convection-diffusion, GMRES(30) and GCR(30) + ParILUT
+    (fill 2, 5 sweeps, drop tolerance 1e-4): converge to 1e-10 and agree with
+    the oracle using the same (bitwise-equal) ParILUT factors."""
+    A = st.convdiff3d_27pt(18)
+    b = st.rhs_uniform(A.n, 0, 0.0, 1.0)
+    F = oracle.parilut(A, fill=2.0, sweeps=5, droptol=1e-4)
+    for ksp, om in (("gmres", "fgmres"), ("gcr", "hip_igcr")):
+        S = _solver(A, ksp, "ilut", 1e-10, 600, restart=30)
+        S.pc_setparilut(2.0, 5, 1e-4)
+        x = S.solve(b)
+        r = b - A.to_scipy() @ x
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-9
+        xo, ro, uo, hb, xb = reference_with_bounds(om, A, b, tol=1e-10, maxiter=600, restart=30, pc="lu", factors=F,
+                                                   quirk=0)
+        assert abs(S.usediter - (uo + (0 if om == "hip_igcr" else 1))) <= 1
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb

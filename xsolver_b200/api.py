@@ -258,6 +258,9 @@ class Plan:
     def sync(self):
         check(self._L.xs_plan_sync(self.p), "plan sync")
 
+    def debug_break_dependency(self, position: int, enable: bool = True):
+        check(self._L.xs_plan_debug_break_dependency(self.p, position, 1 if enable else 0), "debug_break_dependency")
+
     def levels(self):
         a, b = C.c_int(), C.c_int()
         check(self._L.xs_plan_levels(self.p, C.byref(a), C.byref(b)), "levels")

@@ -211,6 +211,29 @@ int xs_plan_lusolve_t(xs_plan_t p, const double *x, double *z)
         h.adj.Mt.apply<double>(x, z, nullptr, h.s);
     });
 }
+int xs_plan_debug_break_dependency(xs_plan_t p, int position, int enable)
+{
+    return guarded([&] {
+        if (!p) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
+        TriDev &L = h.M.L;
+        if (position < 0 || position >= L.n) throw Status(XS_ERR_INVALID);
+        int k[2];
+        XS_CUDA(cudaMemcpy(k, L.prp.p + position, sizeof(int) * 2, cudaMemcpyDeviceToHost));
+        if (k[1] <= k[0]) throw Status(XS_ERR_INVALID);  // the row has no dependency to break
+        int row = 0;
+        XS_CUDA(cudaMemcpy(&row, L.perm.p + position, sizeof(int), cudaMemcpyDeviceToHost));
+        static thread_local int saved = -1;
+        if (enable) {
+            XS_CUDA(cudaMemcpy(&saved, L.pci.p + k[0], sizeof(int), cudaMemcpyDeviceToHost));
+            XS_CUDA(cudaMemcpy(L.pci.p + k[0], &row, sizeof(int), cudaMemcpyHostToDevice));  // waits on itself
+        } else if (saved >= 0) {
+            XS_CUDA(cudaMemcpy(L.pci.p + k[0], &saved, sizeof(int), cudaMemcpyHostToDevice));
+            saved = -1;
+        }
+    });
+}
 int xs_plan_sync(xs_plan_t p)
 {
     return guarded([&] {
