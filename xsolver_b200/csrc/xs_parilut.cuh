@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int *buf = sbuf[w];
     for (int i = blockIdx.x * PLT_WARPS + w; i < n; i += gridDim.x * PLT_WARPS) {
-        // total with duplicates
-        int tot = arp[i + 1] - arp[i];
+        // total with duplicates (A's row counted once, by lane 0)
+        int tot = lane == 0 ? arp[i + 1] - arp[i] : 0;
         for (int q = lrp[i] + lane; q < lrp[i + 1]; q += 32) {
             const int k = lci[q];
             tot += urp[k + 1] - urp[k];
@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int 
             for (int t = urp[k] + lane; t < urp[k + 1]; t += 32) buf[atomicAdd(&scount[w], 1)] = uci[t];
         }
         __syncwarp();
+        tot = scount[w];  // exactly the entries gathered
         int N = 1;
         while (N < tot) N <<= 1;
         for (int q = tot + lane; q < N; q += 32) buf[q] = INT_MAX;
