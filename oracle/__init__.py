@@ -218,9 +218,13 @@ def levels_lower(n, rp, ci):
 PC = {"none": 0, "jacobi": 1, "lu": 2}
 
 
+DOT_MODES = {"sequential": 0, "pairwise": 1, "reverse": 2, "simd8": 3, "blocked": 4}
+
+
 def set_dot_mode(mode: str):
-    """'sequential' (the reference's order) or 'pairwise' (another valid order)."""
-    lib().orc_set_dot_mode({"sequential": 0, "pairwise": 1}[mode])
+    """'sequential' (the reference's order) or another valid summation order:
+    'pairwise', 'reverse', 'simd8', 'blocked'."""
+    lib().orc_set_dot_mode(DOT_MODES[mode])
 
 
 def solve(method, A, rhs, x0=None, tol=1e-8, maxiter=1000, restart=30, pc="jacobi", factors: LU | None = None,

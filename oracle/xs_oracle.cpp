@@ -44,8 +44,9 @@ namespace {
 
 /* ---------------- BLAS-1, sequential order ---------------- */
 /* dot-product order: 0 = sequential (the reference's cblas_ddot through the
- * sequential shim), 1 = pairwise (another valid order, used to measure how
- * sensitive a reference solve is to the summation order of its dots) */
+ * sequential shim); 1 pairwise, 2 reverse, 3 eight interleaved partial sums,
+ * 4 blocked — other valid orders, used to measure how sensitive a reference
+ * solve is to the summation order of its dot products */
 int g_dot_mode = 0;
 double o_dot_pairwise(int n, const double *x, const double *y)
 {
@@ -60,6 +61,29 @@ double o_dot_pairwise(int n, const double *x, const double *y)
 double o_dot(int n, const double *x, const double *y)
 {
     if (g_dot_mode == 1) return o_dot_pairwise(n, x, y);
+    if (g_dot_mode == 2) { /* reverse sequential */
+        double s = 0.0;
+        for (int i = n - 1; i >= 0; i--) s += x[i] * y[i];
+        return s;
+    }
+    if (g_dot_mode == 3) { /* 8 interleaved partial sums, as a SIMD ddot */
+        double p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int i = 0;
+        for (; i + 8 <= n; i += 8)
+            for (int l = 0; l < 8; l++) p[l] += x[i + l] * y[i + l];
+        double s = ((p[0] + p[4]) + (p[2] + p[6])) + ((p[1] + p[5]) + (p[3] + p[7]));
+        for (; i < n; i++) s += x[i] * y[i];
+        return s;
+    }
+    if (g_dot_mode == 4) { /* blocks of 1024 summed sequentially, then combined */
+        double s = 0.0;
+        for (int b = 0; b < n; b += 1024) {
+            double t = 0.0;
+            for (int i = b; i < n && i < b + 1024; i++) t += x[i] * y[i];
+            s += t;
+        }
+        return s;
+    }
     double s = 0.0;
     for (int i = 0; i < n; i++) s += x[i] * y[i];
     return s;

@@ -74,7 +74,11 @@ struct DBuf {
         size_t bytes = (count + pad) * sizeof(T);
         if (bytes == 0) bytes = 16;
         XS_CUDA(cudaMalloc((void **)&p, bytes));
-        XS_CUDA(cudaMemset(p, 0, bytes));
+        // zero and wait: the handle's stream does not synchronise with the
+        // legacy default stream, so an asynchronous memset there could land
+        // after the handle's own first writes to this buffer
+        XS_CUDA(cudaMemsetAsync(p, 0, bytes, 0));
+        XS_CUDA(cudaStreamSynchronize(0));
         n = count;
     }
     void free()

@@ -219,6 +219,7 @@ int xs_plan_debug_break_dependency(xs_plan_t p, int position, int enable)
         if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
         TriDev &L = h.M.L;
         if (position < 0 || position >= L.n) throw Status(XS_ERR_INVALID);
+        XS_CUDA(cudaStreamSynchronize(h.s));
         int k[2];
         XS_CUDA(cudaMemcpy(k, L.prp.p + position, sizeof(int) * 2, cudaMemcpyDeviceToHost));
         if (k[1] <= k[0]) throw Status(XS_ERR_INVALID);  // the row has no dependency to break
