@@ -260,6 +260,22 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes);
  * rows sorted by (level, row) — the position order of the sync-free solve. */
 int xs_tri_levels(int n, const int *rowptr, const int *colidx, int upper, int *level, int *perm, int *nlevels);
 
+/* LU solve that allocates nothing (no counterpart in the reference).
+ * z = (L D U')^{-1} x with the factors in the seqilu0 layout (L strict lower
+ * CSR with unit diagonal implied, dinv = 1/u_ii, U' = dinv-row-scaled strict
+ * upper CSR; natural row order, columns sorted), all device pointers, FP64,
+ * enqueued on `stream` (a cudaStream_t, NULL = default stream) and waited
+ * for before returning.  For callers that cannot allocate device memory
+ * (a pool or allocator that owns all of it, a fixed memory budget after
+ * start-up, buffers handed in by the caller only): the scratch lives in a
+ * fixed 4 MiB __device__ array that every GPU loading the library holds
+ * until exit.  n must be <= 262144 (XS_ERR_CAPACITY otherwise).  Calls that
+ * overlap on the GPU share that array and race: serialise them.  The first
+ * call on a device looks up the array's address; make it before any stream
+ * capture.  Result bitwise equal to xs_plan_lusolve on the same factors. */
+int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, const double *dinv, const int *urp,
+                       const int *uci, const double *uv, const double *x, double *z, void *stream);
+
 /* library identification */
 const char *xs_version(void);
 int xs_device_count(void);

@@ -3,8 +3,8 @@
     python -m xsolver_b200.build            # build if sources are newer
     python -m xsolver_b200.build --force
 
-The library is a single translation unit (csrc/xs_api.cu includes the kernel
-headers).  It is compiled without FMA contraction (-fmad=false) so that the
+The library is built from csrc/*.cu (xs_api.cu includes the kernel headers;
+xs_noalloc.cu holds the allocation-free LU solve).  It is compiled without FMA contraction (-fmad=false) so that the
 FP64 triangular solves and ILU(0) reproduce the CPU reference bit for bit;
 the FP32 kernels request fused multiply-adds explicitly where they want them.
 """
@@ -44,7 +44,8 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     if not force and not needs_build():
         return LIB
-    cmd = [NVCC, *FLAGS, *(extra or []), "-o", LIB + ".tmp", os.path.join(CSRC, "xs_api.cu"), "-lcudart"]
+    units = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    cmd = [NVCC, *FLAGS, *(extra or []), "-o", LIB + ".tmp", *units, "-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
