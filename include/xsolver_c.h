@@ -276,6 +276,13 @@ int xs_tri_levels(int n, const int *rowptr, const int *colidx, int upper, int *l
 int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, const double *dinv, const int *urp,
                        const int *uci, const double *uv, const double *x, double *z, void *stream);
 
+/* Launch tuning of the sync-free triangular solves, process-wide:
+ * blocks_per_sm persistent blocks per SM (0 = one block per 128 rows) and
+ * the cap of the exponential back-off between polls of a pending row, in ns
+ * (0 = no sleep).  Defaults 4 and 128; environment XS_TRSV_BLOCKS_PER_SM /
+ * XS_TRSV_BACKOFF_NS override them at first use. */
+int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns);
+
 /* library identification */
 const char *xs_version(void);
 int xs_device_count(void);

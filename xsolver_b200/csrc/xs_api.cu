@@ -44,6 +44,18 @@ Geom &geom()
     return g;
 }
 
+TrsvTuning &trsv_tuning()
+{
+    static TrsvTuning t;
+    static bool init = false;
+    if (!init) {
+        if (const char *e = getenv("XS_TRSV_BLOCKS_PER_SM")) t.blocks_per_sm = atoi(e);
+        if (const char *e = getenv("XS_TRSV_BACKOFF_NS")) t.backoff_ns = atoi(e);
+        init = true;
+    }
+    return t;
+}
+
 // ---------------------------------------------------------------- operator setup
 __global__ void k_convert_f32(long m, const double *__restrict__ a, float *__restrict__ b)
 {
@@ -965,6 +977,15 @@ static int check_gpu()
 extern "C" {
 
 const char *xs_version(void) { return "xsolver_b200 1.0 (sm_100a)"; }
+
+int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns)
+{
+    return guarded([&] {
+        if (blocks_per_sm < 0 || blocks_per_sm > 64 || backoff_ns < 0 || backoff_ns > 100000) throw Status(XS_ERR_INVALID);
+        trsv_tuning().blocks_per_sm = blocks_per_sm;
+        trsv_tuning().backoff_ns = backoff_ns;
+    });
+}
 
 int xs_tri_levels(int n, const int *rp, const int *ci, int upper, int *level, int *perm, int *nlevels)
 {

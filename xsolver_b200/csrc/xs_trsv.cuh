@@ -56,21 +56,21 @@ struct CalcT {
 __device__ __forceinline__ double msub(double acc, double y, double v) { return acc - y * v; }
 __device__ __forceinline__ float msub(float acc, float y, float v) { return __fmaf_rn(-y, v, acc); }
 
+// Launch tuning of the sync-free solves (host side, process-wide):
+//   blocks_per_sm  persistent blocks per SM (0: one block per 128 positions,
+//                  no persistence)
+//   backoff_ns     upper bound of the exponential back-off between polls of a
+//                  pending dependency (0: spin without sleeping)
+struct TrsvTuning {
+    int blocks_per_sm = 4;
+    int backoff_ns = 128;
+};
+TrsvTuning &trsv_tuning();
+
 template <typename VT, typename FT, typename DT, bool UPPER>
-__global__ void __launch_bounds__(TRSV_THREADS) k_trsv_syncfree(TrsvArgs<FT> P, const DT *__restrict__ dinv,
-                                                               const VT *rhs, VT *self, VT *out_user, VT *reset_other,
-                                                               const int *done_flag, int *err, unsigned *ticket)
+__device__ __forceinline__ bool trsv_row(const TrsvArgs<FT> &P, const DT *__restrict__ dinv, const VT *rhs, VT *self,
+                                         VT *out_user, VT *reset_other, int *err, int p, int backoff_ns)
 {
-    if (done_flag && *done_flag) return;
-    __shared__ int s_blk;
-    if (threadIdx.x == 0) {
-        unsigned t = atomicAdd(ticket, 1u);
-        if (t == gridDim.x - 1) *ticket = 0u;  // every block already holds its ticket
-        s_blk = (int)t;
-    }
-    __syncthreads();
-    const int p = s_blk * TRSV_THREADS + (int)threadIdx.x;
-    if (p >= P.n) return;
     const int row = __ldg(P.perm + p);
     VT acc;
     if (!UPPER) {
@@ -81,7 +81,6 @@ __global__ void __launch_bounds__(TRSV_THREADS) k_trsv_syncfree(TrsvArgs<FT> P, 
     }
     if (reset_other) reset_other[row] = Sentinel<VT>::value();
     const int k0 = __ldg(P.prp + p), k1 = __ldg(P.prp + p + 1);
-    bool failed = false;
     for (int base = k0; base < k1; base += TRSV_CHUNK) {
         const int cnt = min(TRSV_CHUNK, k1 - base);
         int c[TRSV_CHUNK];
@@ -102,38 +101,78 @@ __global__ void __launch_bounds__(TRSV_THREADS) k_trsv_syncfree(TrsvArgs<FT> P, 
                 if (Sentinel<VT>::is(yv[j])) pending |= 1u << j;
             }
         }
-        long spins = 0;
-        unsigned long long t0 = 0;
-        while (pending) {
+        if (pending) {
+            const unsigned long long t0 = gtimer();
+            unsigned ns = 8;
+            long spins = 0;
+            while (pending) {
+                if (backoff_ns > 0) {
+                    __nanosleep(ns);
+                    if (ns < (unsigned)backoff_ns) ns <<= 1;
+                }
 #pragma unroll
-            for (int j = 0; j < TRSV_CHUNK; j++) {
-                if (pending & (1u << j)) {
-                    yv[j] = ld_poll(self + c[j]);
-                    if (!Sentinel<VT>::is(yv[j])) pending &= ~(1u << j);
+                for (int j = 0; j < TRSV_CHUNK; j++) {
+                    if (pending & (1u << j)) {
+                        yv[j] = ld_poll(self + c[j]);
+                        if (!Sentinel<VT>::is(yv[j])) pending &= ~(1u << j);
+                    }
                 }
-            }
-            if (pending && ((++spins & 255) == 0)) {
-                const unsigned long long t = gtimer();
-                if (t0 == 0) t0 = t;
-                else if (t - t0 > WAIT_LIMIT_NS) {
-                    atomicOr(err, DEV_TRSV_TIMEOUT);
-                    failed = true;
-                    break;
-                }
-                if (*(volatile int *)err) {
-                    failed = true;
-                    break;
+                if (pending && ((++spins & 63) == 0)) {
+                    if (gtimer() - t0 > WAIT_LIMIT_NS) {
+                        atomicOr(err, DEV_TRSV_TIMEOUT);
+                        return false;
+                    }
+                    if (*(volatile int *)err) return false;
                 }
             }
         }
-        if (failed) break;
 #pragma unroll
         for (int j = 0; j < TRSV_CHUNK; j++)
             if (j < cnt) acc = msub(acc, yv[j], fv[j]);
     }
-    if (failed) return;  // leaves the row unpublished; dependants stop on the error word
     st_publish(self + row, acc);
     if (out_user) out_user[row] = acc;
+    return true;
+}
+
+// Blocks take position ranges of TRSV_THREADS rows through a ticket counter
+// (so a block only waits on ranges taken earlier, by running blocks).  With a
+// persistent grid every block keeps taking tickets until the work runs out;
+// the block that draws the last ticket (work + grid - 1) resets the counter.
+template <typename VT, typename FT, typename DT, bool UPPER>
+__global__ void __launch_bounds__(TRSV_THREADS) k_trsv_syncfree(TrsvArgs<FT> P, const DT *__restrict__ dinv,
+                                                               const VT *rhs, VT *self, VT *out_user, VT *reset_other,
+                                                               const int *done_flag, int *err, unsigned *ticket,
+                                                               int backoff_ns)
+{
+    if (done_flag && *done_flag) return;
+    __shared__ int s_blk;
+    const unsigned work = (unsigned)((P.n + TRSV_THREADS - 1) / TRSV_THREADS);
+    const unsigned last = work + gridDim.x - 1;
+    bool ok = true;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            if (t == last) *ticket = 0u;  // every block has drawn its final ticket
+            s_blk = (int)t;
+        }
+        __syncthreads();
+        const int b = s_blk;
+        if ((unsigned)b >= work) break;
+        const int p = b * TRSV_THREADS + (int)threadIdx.x;
+        if (ok && p < P.n) ok = trsv_row<VT, FT, DT, UPPER>(P, dinv, rhs, self, out_user, reset_other, err, p, backoff_ns);
+    }
+}
+
+inline int trsv_grid(int n)
+{
+    const int work = (n + TRSV_THREADS - 1) / TRSV_THREADS;
+    const TrsvTuning &t = trsv_tuning();
+    if (t.blocks_per_sm <= 0) return work;
+    long g = (long)t.blocks_per_sm * geom().sms;
+    if (g > work) g = work;
+    return (int)(g > 0 ? g : 1);
 }
 
 // Re-arm a solve buffer (used at setup and after an aborted solve).
