@@ -89,7 +89,7 @@ def _declare(L):
         "xs_plan_op_bytes": [C.c_void_p, C.c_int, _dp],
         "xs_device_count": [],
         "xs_tri_levels": [C.c_int, _ip, _ip, C.c_int, _ip, _ip, _ip],
-        "xs_set_trsv_tuning": [C.c_int, C.c_int],
+        "xs_set_trsv_tuning": [C.c_int, C.c_int, C.c_int],
         "xs_lusolve_noalloc": [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         "xsolver_last_error": [],
     }

@@ -50,7 +50,8 @@ TrsvTuning &trsv_tuning()
     static bool init = false;
     if (!init) {
         if (const char *e = getenv("XS_TRSV_BLOCKS_PER_SM")) t.blocks_per_sm = atoi(e);
-        if (const char *e = getenv("XS_TRSV_BACKOFF_NS")) t.backoff_ns = atoi(e);
+        if (const char *e = getenv("XS_TRSV_BACKOFF_NS")) t.backoff_ns = std::max(8, atoi(e));
+        if (const char *e = getenv("XS_TRSV_CHUNK_ROWS")) t.chunk_rows = std::max(0, atoi(e));
         init = true;
     }
     return t;
@@ -315,27 +316,8 @@ static void analyse_pattern(Handle &h)
         lrp[i + 1] = (int)lci.size();
         urp[i + 1] = (int)uci.size();
     }
-    tri_analyse(n, lrp.data(), lci.data(), false, [&](int k) { return lsrc[k]; }, h.hL);
-    tri_analyse(n, urp.data(), uci.data(), true, [&](int k) { return usrc[k]; }, h.hU);
-    // device copies of the plans
-    auto upload_tri = [&](TriDev &T, const TriHostPlan &P, const std::vector<int> &nrp, const std::vector<int> &nci,
-                          const std::vector<long> &nsrc, bool upper) {
-        T.n = n;
-        T.nnz = P.prp[n];
-        T.nlevels = P.nlevels;
-        T.upper = upper;
-        T.perm.alloc(n); T.perm.upload(P.perm.data(), n, h.s);
-        T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, h.s);
-        T.pci.alloc(std::max<long>(T.nnz, 1)); if (T.nnz) T.pci.upload(P.pci.data(), T.nnz, h.s);
-        T.src.alloc(std::max<long>(T.nnz, 1)); if (T.nnz) T.src.upload(P.src.data(), T.nnz, h.s);
-        T.rp_nat.alloc(n + 1); T.rp_nat.upload(nrp.data(), n + 1, h.s);
-        T.ci_nat.alloc(std::max<size_t>(nci.size(), 1)); if (!nci.empty()) T.ci_nat.upload(nci.data(), nci.size(), h.s);
-        T.src_nat.alloc(std::max<size_t>(nsrc.size(), 1)); if (!nsrc.empty()) T.src_nat.upload(nsrc.data(), nsrc.size(), h.s);
-        T.ticket.alloc(1);
-        XS_CUDA(cudaStreamSynchronize(h.s));
-    };
-    upload_tri(h.M.L, h.hL, lrp, lci, lsrc, false);
-    upload_tri(h.M.U, h.hU, urp, uci, usrc, true);
+    build_tri_dev(h.M.L, n, lrp, lci, false, [&](int k) { return lsrc[k]; }, h.s);
+    build_tri_dev(h.M.U, n, urp, uci, true, [&](int k) { return usrc[k]; }, h.s);
     h.uptr.alloc(n);
     h.uptr.upload(h.huptr.data(), n, h.s);
     h.rowof.alloc(std::max<long>(h.nnz, 1));
@@ -810,26 +792,8 @@ static void adjoint_prepare(Handle &h)
         std::vector<double> dummy;
         host_transpose(n, urp.data(), uci.data(), nullptr, utrp, utci, nullptr, &utsrc_k);
         host_transpose(n, lrp.data(), lci.data(), nullptr, ltrp, ltci, nullptr, &ltsrc_k);
-        TriHostPlan PL, PU;
-        tri_analyse(n, utrp.data(), utci.data(), false, [&](int k) { return usrc[utsrc_k[k]]; }, PL);
-        tri_analyse(n, ltrp.data(), ltci.data(), true, [&](int k) { return lsrc[ltsrc_k[k]]; }, PU);
-        auto up = [&](TriDev &D, const TriHostPlan &P, const std::vector<int> &nrp, const std::vector<int> &nci,
-                      const std::vector<long> &srcmap, const std::vector<long> &orig, bool upper) {
-            D.n = n; D.nnz = P.prp[n]; D.nlevels = P.nlevels; D.upper = upper;
-            D.perm.alloc(n); D.perm.upload(P.perm.data(), n, h.s);
-            D.prp.alloc(n + 1); D.prp.upload(P.prp.data(), n + 1, h.s);
-            D.pci.alloc(std::max<long>(D.nnz, 1)); if (D.nnz) D.pci.upload(P.pci.data(), D.nnz, h.s);
-            D.src.alloc(std::max<long>(D.nnz, 1)); if (D.nnz) D.src.upload(P.src.data(), D.nnz, h.s);
-            D.rp_nat.alloc(n + 1); D.rp_nat.upload(nrp.data(), n + 1, h.s);
-            D.ci_nat.alloc(std::max<size_t>(nci.size(), 1)); if (!nci.empty()) D.ci_nat.upload(nci.data(), nci.size(), h.s);
-            std::vector<long> ns(srcmap.size());
-            for (size_t k = 0; k < ns.size(); k++) ns[k] = orig[srcmap[k]];
-            D.src_nat.alloc(std::max<size_t>(ns.size(), 1)); if (!ns.empty()) D.src_nat.upload(ns.data(), ns.size(), h.s);
-            D.ticket.alloc(1);
-            XS_CUDA(cudaStreamSynchronize(h.s));
-        };
-        up(T.L, PL, utrp, utci, utsrc_k, usrc, false);
-        up(T.U, PU, ltrp, ltci, ltsrc_k, lsrc, true);
+        build_tri_dev(T.L, n, utrp, utci, false, [&](int k) { return usrc[utsrc_k[k]]; }, h.s);
+        build_tri_dev(T.U, n, ltrp, ltci, true, [&](int k) { return lsrc[ltsrc_k[k]]; }, h.s);
         const int g = geom().sms * 4;
         for (TriDev *D : {&T.L, &T.U}) {
             long m = std::max<long>(D->nnz, 1);
@@ -978,12 +942,14 @@ extern "C" {
 
 const char *xs_version(void) { return "xsolver_b200 1.0 (sm_100a)"; }
 
-int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns)
+int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows)
 {
     return guarded([&] {
-        if (blocks_per_sm < 0 || blocks_per_sm > 64 || backoff_ns < 0 || backoff_ns > 100000) throw Status(XS_ERR_INVALID);
+        if (blocks_per_sm < 0 || blocks_per_sm > 64 || backoff_ns < 8 || backoff_ns > 100000) throw Status(XS_ERR_INVALID);
+        if (chunk_rows < 0 || chunk_rows > 24576) throw Status(XS_ERR_INVALID);  // 24576 doubles = 192 KiB shared
         trsv_tuning().blocks_per_sm = blocks_per_sm;
         trsv_tuning().backoff_ns = backoff_ns;
+        trsv_tuning().chunk_rows = chunk_rows;
     });
 }
 

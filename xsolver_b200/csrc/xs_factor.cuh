@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(128) k_ilu0_rows(int n, const int *__restrict_
         long spins = 0;
         unsigned long long t0 = 0;
         while (ld_acquire(flag + k) != epoch) {
+            __nanosleep(32);  // yield point: the producer may be a lane of this warp
             if ((++spins & 255) == 0) {
                 const unsigned long long t = gtimer();
                 if (t0 == 0) t0 = t;

@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(NA_THREADS) k_na_trsv(int n, const int *__rest
             const unsigned long long t0 = na_timer();
             long spins = 0;
             while (na_is_sentinel(y)) {
+                __nanosleep(64);  // yield point: the producer may be a lane of this warp
                 y = na_poll(self + c);
                 if ((++spins & 255) == 0) {
                     if (na_timer() - t0 > NA_LIMIT_NS) {

@@ -665,27 +665,10 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
 // prepare the sync-free solve plans for ParILUT factors (own pattern)
 inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriDev &U, bool need32)
 {
-    TriHostPlan PL, PU;
-    tri_analyse(n, R.hlrp.data(), R.hlci.data(), false, [](int k) { return (long)k; }, PL);
-    tri_analyse(n, R.hurp.data(), R.huci.data(), true, [](int k) { return (long)k; }, PU);
-    auto up = [&](TriDev &T, const TriHostPlan &P, const std::vector<int> &nrp, const std::vector<int> &nci, bool upper,
-                  const double *vals) {
+    auto up = [&](TriDev &T, const std::vector<int> &nrp, const std::vector<int> &nci, bool upper, const double *vals) {
         T = TriDev();
-        T.n = n;
-        T.nnz = P.prp[n];
-        T.nlevels = P.nlevels;
-        T.upper = upper;
-        T.perm.alloc(n); T.perm.upload(P.perm.data(), n, s);
-        T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
+        build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s);
         const long m = std::max<long>(T.nnz, 1);
-        T.pci.alloc(m); if (T.nnz) T.pci.upload(P.pci.data(), T.nnz, s);
-        T.src.alloc(m); if (T.nnz) T.src.upload(P.src.data(), T.nnz, s);
-        T.rp_nat.alloc(n + 1); T.rp_nat.upload(nrp.data(), n + 1, s);
-        T.ci_nat.alloc(m); if (T.nnz) T.ci_nat.upload(nci.data(), T.nnz, s);
-        std::vector<long> ns(T.nnz);
-        std::iota(ns.begin(), ns.end(), 0L);
-        T.src_nat.alloc(m); if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
-        T.ticket.alloc(1);
         const int g = geom().sms * 4;
         T.pv64.alloc(m); T.nv64.alloc(m);
         if (T.nnz) {
@@ -706,8 +689,8 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
         check_launch();
         XS_CUDA(cudaStreamSynchronize(s));
     };
-    up(L, PL, R.hlrp, R.hlci, false, R.lv.p);
-    up(U, PU, R.hurp, R.huci, true, R.uv.p);
+    up(L, R.hlrp, R.hlci, false, R.lv.p);
+    up(U, R.hurp, R.huci, true, R.uv.p);
     const int g = geom().sms * 4;
     U.dinv64.alloc(n); U.dinv64_nat.alloc(n);
     k_gather_dinv<double><<<g, 256, 0, s>>>(n, U.perm.p, R.diag_ident.p, R.dinv.p, U.dinv64.p);

@@ -122,15 +122,10 @@ struct PrecondDev {
         if constexpr (std::is_same<VT, double>::value) dinv = U.dinv64.p;
         else dinv = U.dinv32.p;
         VT *lb = lbuf<VT>(), *ub = ubuf<VT>();
-        const int gl = trsv_grid(L.n);
-        const int bo = trsv_tuning().backoff_ns;
         if (half == 0)
-            k_trsv_syncfree<VT, FT, DT, false><<<gl, TRSV_THREADS, 0, s>>>(L.args<FT>(), (const DT *)nullptr, x, lb,
-                                                                           (VT *)nullptr, ub, done_flag, err, L.ticket.p,
-                                                                           bo);
+            launch_trsv<VT, FT, DT, false>(L, (const DT *)nullptr, x, lb, (VT *)nullptr, ub, done_flag, err, s);
         else
-            k_trsv_syncfree<VT, FT, DT, true><<<gl, TRSV_THREADS, 0, s>>>(U.args<FT>(), dinv, lb, ub, z, lb, done_flag,
-                                                                          err, U.ticket.p, bo);
+            launch_trsv<VT, FT, DT, true>(U, dinv, lb, ub, z, lb, done_flag, err, s);
     }
     // one half of the exact solve in the configured precision (timing)
     template <typename VT>

@@ -64,6 +64,7 @@ __device__ __forceinline__ float msub(float acc, float y, float v) { return __fm
 struct TrsvTuning {
     int blocks_per_sm = 4;
     int backoff_ns = 128;
+    int chunk_rows = 24576;  // chunked kernel: rows per CTA chunk (0: level-ordered kernel)
 };
 TrsvTuning &trsv_tuning();
 
@@ -106,10 +107,11 @@ __device__ __forceinline__ bool trsv_row(const TrsvArgs<FT> &P, const DT *__rest
             unsigned ns = 8;
             long spins = 0;
             while (pending) {
-                if (backoff_ns > 0) {
-                    __nanosleep(ns);
-                    if (ns < (unsigned)backoff_ns) ns <<= 1;
-                }
+                // the sleep is also the yield point that lets a producer lane
+                // of the same warp run: a spin without it can starve the lane
+                // it waits for
+                __nanosleep(ns);
+                if (ns < (unsigned)backoff_ns) ns <<= 1;
 #pragma unroll
                 for (int j = 0; j < TRSV_CHUNK; j++) {
                     if (pending & (1u << j)) {
@@ -173,6 +175,152 @@ inline int trsv_grid(int n)
     long g = (long)t.blocks_per_sm * geom().sms;
     if (g > work) g = work;
     return (int)(g > 0 ? g : 1);
+}
+
+// ---------------------------------------------------------------- chunked variant
+// Rows are taken in "logical" order (L: row order; U: reverse row order, so a
+// dependency always has a smaller logical index) and cut into contiguous
+// chunks of at most CH rows, one CTA per chunk (chunks claimed through a
+// ticket in order).  Inside a chunk, rows are sorted by their local
+// dependency level (levels counted over dependencies inside the chunk only);
+// the CTA walks the local levels with __syncthreads between them and keeps
+// every result of the chunk in shared memory, so a dependency inside the
+// chunk is one shared-memory load.  A dependency on an earlier chunk is read
+// from the global solve buffer with the same sentinel polling as above; the
+// encoded dependency index carries the distinction (high bit set: local
+// shared-memory slot).  Each thread prefetches the row data of its row in the
+// next local level while it works on the current one.  The entry order and
+// arithmetic per row are those of the level-ordered kernel, so results are
+// bitwise identical.
+template <typename FT>
+struct ChunkArgs {
+    int n, nchunks, ch;
+    const int *lvl_off;  // per chunk: first level index (nchunks+1)
+    const int *lvl_ptr;  // per level: first position (total levels + 1)
+    const int *perm;
+    const int *prp;
+    const int *pci;      // encoded: >= 0 global row, < 0 local slot | 0x80000000
+    const FT *pv;
+};
+
+constexpr int CH_THREADS = 256;
+constexpr int CH_PF = 8;  // entries prefetched per row
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+struct ChunkRow {
+    int p = -1, row = 0, k0 = 0, k1 = 0;
+    VT rhsv = 0;
+    DT dv = 0;
+    int c[CH_PF];
+    VT f[CH_PF];
+    __device__ __forceinline__ void load(const ChunkArgs<FT> &P, const DT *dinv, const VT *rhs, int pos)
+    {
+        p = pos;
+        row = __ldg(P.perm + pos);
+        k0 = __ldg(P.prp + pos);
+        k1 = __ldg(P.prp + pos + 1);
+        rhsv = rhs[row];
+        if (UPPER) dv = __ldg(dinv + pos);
+#pragma unroll
+        for (int j = 0; j < CH_PF; j++)
+            if (k0 + j < k1) {
+                c[j] = __ldg(P.pci + k0 + j);
+                f[j] = (VT)FVal<FT>::ld(P.pv, k0 + j);
+            }
+    }
+};
+
+template <typename VT>
+__device__ __forceinline__ bool chunk_dep(int enc, const VT *ysh, const VT *self, int *err, int backoff_ns, VT &y)
+{
+    if (enc < 0) {
+        y = ysh[enc & 0x7fffffff];
+        return true;
+    }
+    y = ld_poll(self + enc);
+    if (!Sentinel<VT>::is(y)) return true;
+    const unsigned long long t0 = gtimer();
+    unsigned ns = 8;
+    long spins = 0;
+    while (Sentinel<VT>::is(y)) {
+        __nanosleep(ns);
+        if (ns < (unsigned)backoff_ns) ns <<= 1;
+        y = ld_poll(self + enc);
+        if ((++spins & 63) == 0) {
+            if (gtimer() - t0 > WAIT_LIMIT_NS) {
+                atomicOr(err, DEV_TRSV_TIMEOUT);
+                return false;
+            }
+            if (*(volatile int *)err) return false;
+        }
+    }
+    return true;
+}
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+__global__ void __launch_bounds__(CH_THREADS) k_trsv_chunked(ChunkArgs<FT> P, const DT *__restrict__ dinv, const VT *rhs,
+                                                             VT *self, VT *out_user, VT *reset_other,
+                                                             const int *done_flag, int *err, unsigned *ticket,
+                                                             int backoff_ns)
+{
+    if (done_flag && *done_flag) return;
+    extern __shared__ __align__(16) unsigned char ch_smem[];
+    VT *ysh = (VT *)ch_smem;
+    __shared__ int s_chunk;
+    const unsigned last = (unsigned)P.nchunks + gridDim.x - 1;
+    bool ok = true;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            if (t == last) *ticket = 0u;
+            s_chunk = (int)t;
+        }
+        __syncthreads();
+        const int c = s_chunk;
+        if (c >= P.nchunks) break;
+        const int c0 = c * P.ch;
+        const int l0 = P.lvl_off[c], l1 = P.lvl_off[c + 1];
+        ChunkRow<VT, FT, DT, UPPER> cur, nxt;
+        {
+            const int pos = P.lvl_ptr[l0] + (int)threadIdx.x;
+            if (pos < P.lvl_ptr[l0 + 1]) cur.load(P, dinv, rhs, pos);
+        }
+        for (int l = l0; l < l1; l++) {
+            const int pa = P.lvl_ptr[l], pb = P.lvl_ptr[l + 1];
+            // prefetch this thread's first row of the next level
+            nxt.p = -1;
+            if (l + 1 < l1) {
+                const int pos = pb + (int)threadIdx.x;
+                if (pos < P.lvl_ptr[l + 2]) nxt.load(P, dinv, rhs, pos);
+            }
+            for (int pos = pa + (int)threadIdx.x; pos < pb; pos += CH_THREADS) {
+                ChunkRow<VT, FT, DT, UPPER> r;
+                if (pos == cur.p) r = cur;
+                else r.load(P, dinv, rhs, pos);
+                if (!ok) continue;
+                VT acc = UPPER ? (VT)(r.rhsv * (VT)r.dv) : r.rhsv;
+                if (reset_other) reset_other[r.row] = Sentinel<VT>::value();
+                for (int k = r.k0; k < r.k1 && ok; k++) {
+                    const int j = k - r.k0;
+                    int enc;
+                    VT fv;
+                    if (j < CH_PF) { enc = r.c[j]; fv = r.f[j]; }
+                    else { enc = __ldg(P.pci + k); fv = (VT)FVal<FT>::ld(P.pv, k); }
+                    VT y;
+                    ok = chunk_dep<VT>(enc, ysh, self, err, backoff_ns, y);
+                    if (ok) acc = msub(acc, y, fv);
+                }
+                if (!ok) continue;
+                const int q = UPPER ? P.n - 1 - r.row : r.row;
+                ysh[q - c0] = acc;
+                st_publish(self + r.row, acc);
+                if (out_user) out_user[r.row] = acc;
+            }
+            cur = nxt;
+            __syncthreads();
+        }
+    }
 }
 
 // Re-arm a solve buffer (used at setup and after an aborted solve).
@@ -264,6 +412,80 @@ inline void tri_analyse(int n, const int *rp, const int *ci, bool upper, SrcF sr
     }
 }
 
+// Chunked layout (see k_trsv_chunked).  Produces perm/prp/src as
+// tri_analyse does plus the encoded dependency array, chunk level offsets
+// and level position pointers.
+struct TriChunkPlan {
+    int n = 0, ch = 0, nchunks = 0, maxlevels = 0;
+    std::vector<int> perm, prp, pci_enc, lvl_off, lvl_ptr;
+    std::vector<long> src;
+};
+
+template <typename SrcF>
+inline void tri_analyse_chunked(int n, const int *rp, const int *ci, bool upper, SrcF src_of, int ch, TriChunkPlan &h)
+{
+    h.n = n;
+    h.ch = ch;
+    h.nchunks = (n + ch - 1) / ch;
+    h.perm.assign(n, 0);
+    h.prp.assign(n + 1, 0);
+    h.lvl_off.assign(h.nchunks + 1, 0);
+    h.lvl_ptr.clear();
+    std::vector<int> lev(n, 0);  // by logical index
+    auto row_of = [&](int q) { return upper ? n - 1 - q : q; };
+    auto logical = [&](int r) { return upper ? n - 1 - r : r; };
+    int pos = 0;
+    for (int c = 0; c < h.nchunks; c++) {
+        const int c0 = c * ch, c1 = std::min(n, c0 + ch);
+        int maxl = 0;
+        for (int q = c0; q < c1; q++) {
+            const int r = row_of(q);
+            int l = 0;
+            for (int k = rp[r]; k < rp[r + 1]; k++) {
+                const int qd = logical(ci[k]);
+                if (qd >= c0) l = std::max(l, lev[qd] + 1);
+            }
+            lev[q] = l;
+            maxl = std::max(maxl, l);
+        }
+        const int nl = maxl + 1;
+        std::vector<int> cnt(nl + 1, 0);
+        for (int q = c0; q < c1; q++) cnt[lev[q] + 1]++;
+        for (int l = 0; l < nl; l++) cnt[l + 1] += cnt[l];
+        h.lvl_off[c] = (int)h.lvl_ptr.size();
+        for (int l = 0; l < nl; l++) h.lvl_ptr.push_back(pos + cnt[l]);
+        std::vector<int> fillp(cnt.begin(), cnt.end() - 1);
+        for (int q = c0; q < c1; q++) h.perm[pos + fillp[lev[q]]++] = row_of(q);
+        pos += c1 - c0;
+        h.maxlevels = std::max(h.maxlevels, nl);
+    }
+    h.lvl_off[h.nchunks] = (int)h.lvl_ptr.size();
+    h.lvl_ptr.push_back(n);
+    for (int p = 0; p < n; p++) {
+        const int r = h.perm[p];
+        h.prp[p + 1] = h.prp[p] + (rp[r + 1] - rp[r]);
+    }
+    const long nnz = h.prp[n];
+    h.pci_enc.assign(nnz, 0);
+    h.src.assign(nnz, 0);
+    for (int p = 0; p < n; p++) {
+        const int r = h.perm[p];
+        const int c0 = (logical(r) / ch) * ch;
+        int q = h.prp[p];
+        auto put = [&](int k) {
+            const int d = ci[k];
+            const int qd = logical(d);
+            h.pci_enc[q] = qd >= c0 ? (int)(0x80000000u | (unsigned)(qd - c0)) : d;
+            h.src[q] = src_of(k);
+            q++;
+        };
+        if (!upper)
+            for (int k = rp[r]; k < rp[r + 1]; k++) put(k);
+        else
+            for (int k = rp[r + 1] - 1; k >= rp[r]; k--) put(k);
+    }
+}
+
 // Device copy of a triangle prepared for the sync-free solve.  Values are
 // gathered on the device from a value array (so re-factorisation or a change
 // of storage precision does not repeat the host analysis).
@@ -285,10 +507,29 @@ struct TriDev {
     DBuf<double> dinv64_nat;
     DBuf<float> dinv32_nat;
     DBuf<unsigned> ticket;
+    // chunked layout (perm/prp/pci then hold the chunk-major order, pci encoded)
+    bool chunked = false;
+    int nchunks = 0, ch = 0;
+    DBuf<int> lvl_off, lvl_ptr;
 
     template <typename FT>
     TrsvArgs<FT> args() const;
+    template <typename FT>
+    ChunkArgs<FT> cargs() const
+    {
+        return ChunkArgs<FT>{n, nchunks, ch, lvl_off.p, lvl_ptr.p, perm.p, prp.p, pci.p, vals<FT>()};
+    }
+    template <typename FT>
+    const FT *vals() const;
 };
+template <>
+inline const double *TriDev::vals<double>() const { return pv64.p; }
+template <>
+inline const float *TriDev::vals<float>() const { return pv32.p; }
+template <>
+inline const __nv_bfloat16 *TriDev::vals<__nv_bfloat16>() const { return pvbf.p; }
+template <>
+inline const __half *TriDev::vals<__half>() const { return pvh.p; }
 
 template <>
 inline TrsvArgs<double> TriDev::args<double>() const { return TrsvArgs<double>{n, perm.p, prp.p, pci.p, pv64.p}; }
@@ -322,6 +563,74 @@ __global__ void k_gather_dinv(int n, const int *__restrict__ perm, const long *_
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         int r = perm ? perm[p] : p;
         dst[p] = (DT)vals[diagsrc[r]];
+    }
+}
+
+}  // namespace xs
+
+namespace xs {
+
+// Build the device plan of a strict triangle (natural CSR rp/ci, src_of maps
+// an entry to its index in the value array) in the layout the tuning selects,
+// plus the natural-order copy used by the Jacobi-sweep mode.
+template <typename SrcF>
+inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const std::vector<int> &ci, bool upper, SrcF src_of,
+                          cudaStream_t s)
+{
+    TriHostPlan P;  // level analysis (also gives the level count)
+    tri_analyse(n, rp.data(), ci.data(), upper, src_of, P);
+    T.n = n;
+    T.nnz = P.prp[n];
+    T.nlevels = P.nlevels;
+    T.upper = upper;
+    const long m = std::max<long>(T.nnz, 1);
+    const int chr = trsv_tuning().chunk_rows;
+    T.chunked = chr > 0;
+    if (!T.chunked) {
+        T.perm.alloc(n); T.perm.upload(P.perm.data(), n, s);
+        T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
+        T.pci.alloc(m); if (T.nnz) T.pci.upload(P.pci.data(), T.nnz, s);
+        T.src.alloc(m); if (T.nnz) T.src.upload(P.src.data(), T.nnz, s);
+    } else {
+        TriChunkPlan C;
+        tri_analyse_chunked(n, rp.data(), ci.data(), upper, src_of, chr, C);
+        T.nchunks = C.nchunks;
+        T.ch = C.ch;
+        T.perm.alloc(n); T.perm.upload(C.perm.data(), n, s);
+        T.prp.alloc(n + 1); T.prp.upload(C.prp.data(), n + 1, s);
+        T.pci.alloc(m); if (T.nnz) T.pci.upload(C.pci_enc.data(), T.nnz, s);
+        T.src.alloc(m); if (T.nnz) T.src.upload(C.src.data(), T.nnz, s);
+        T.lvl_off.alloc(C.lvl_off.size()); T.lvl_off.upload(C.lvl_off.data(), C.lvl_off.size(), s);
+        T.lvl_ptr.alloc(C.lvl_ptr.size()); T.lvl_ptr.upload(C.lvl_ptr.data(), C.lvl_ptr.size(), s);
+    }
+    T.rp_nat.alloc(n + 1); T.rp_nat.upload(rp.data(), n + 1, s);
+    T.ci_nat.alloc(m); if (T.nnz) T.ci_nat.upload(ci.data(), T.nnz, s);
+    std::vector<long> ns(T.nnz);
+    for (long k = 0; k < T.nnz; k++) ns[k] = src_of((int)k);
+    T.src_nat.alloc(m); if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
+    T.ticket.alloc(1);
+    XS_CUDA(cudaStreamSynchronize(s));
+}
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+inline void launch_trsv(const TriDev &T, const DT *dinv, const VT *rhs, VT *self, VT *out_user, VT *reset_other,
+                        const int *done_flag, int *err, cudaStream_t s)
+{
+    const int bo = trsv_tuning().backoff_ns;
+    if (T.chunked) {
+        static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
+        const size_t smem = (size_t)T.ch * sizeof(VT);
+        if (smem > attr) {
+            XS_CUDA(cudaFuncSetAttribute(k_trsv_chunked<VT, FT, DT, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+            attr = smem;
+        }
+        const int g = std::min(T.nchunks, geom().sms);
+        k_trsv_chunked<VT, FT, DT, UPPER><<<g, CH_THREADS, smem, s>>>(T.cargs<FT>(), dinv, rhs, self, out_user,
+                                                                     reset_other, done_flag, err, T.ticket.p, bo);
+    } else {
+        k_trsv_syncfree<VT, FT, DT, UPPER><<<trsv_grid(T.n), TRSV_THREADS, 0, s>>>(
+            T.args<FT>(), dinv, rhs, self, out_user, reset_other, done_flag, err, T.ticket.p, bo);
     }
 }
 
