@@ -277,14 +277,14 @@ int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, 
                        const int *uci, const double *uv, const double *x, double *z, void *stream);
 
 /* Launch tuning of the sync-free triangular solves, process-wide.
- * chunk_rows > 0 (default 24576) selects the chunked kernel: contiguous row
+ * chunk_rows > 0 selects the chunked kernel: contiguous row
  * chunks of that size, one block per chunk, dependencies inside a chunk
  * through shared memory (<= 24576 so the FP64 chunk fits in 192 KiB);
- * 0 selects the level-ordered kernel with blocks_per_sm persistent blocks
+ * 0 (default) selects the level-ordered kernel with blocks_per_sm persistent blocks
  * per SM (0 = one block per 128 rows).  backoff_ns caps the exponential
  * back-off between polls of a pending row (>= 8: the sleep is also the
  * yield point a waiting lane needs so that a producer lane of its own warp
- * runs).  Defaults 4 / 128 / 24576; environment XS_TRSV_BLOCKS_PER_SM,
+ * runs).  Defaults 2 / 128 / 0; environment XS_TRSV_BLOCKS_PER_SM,
  * XS_TRSV_BACKOFF_NS, XS_TRSV_CHUNK_ROWS override them at first use.  The
  * layout is fixed when a preconditioner is built: set before factorising. */
 int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);

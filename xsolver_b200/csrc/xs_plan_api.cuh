@@ -225,13 +225,16 @@ int xs_plan_debug_break_dependency(xs_plan_t p, int position, int enable)
         if (k[1] <= k[0]) throw Status(XS_ERR_INVALID);  // the row has no dependency to break
         int row = 0;
         XS_CUDA(cudaMemcpy(&row, L.perm.p + position, sizeof(int), cudaMemcpyDeviceToHost));
-        static thread_local int saved = -1;
+        // the saved entry may be an encoded (negative) chunk-local slot
+        static thread_local int saved = 0;
+        static thread_local bool have_saved = false;
         if (enable) {
-            XS_CUDA(cudaMemcpy(&saved, L.pci.p + k[0], sizeof(int), cudaMemcpyDeviceToHost));
+            if (!have_saved) XS_CUDA(cudaMemcpy(&saved, L.pci.p + k[0], sizeof(int), cudaMemcpyDeviceToHost));
+            have_saved = true;
             XS_CUDA(cudaMemcpy(L.pci.p + k[0], &row, sizeof(int), cudaMemcpyHostToDevice));  // waits on itself
-        } else if (saved >= 0) {
+        } else if (have_saved) {
             XS_CUDA(cudaMemcpy(L.pci.p + k[0], &saved, sizeof(int), cudaMemcpyHostToDevice));
-            saved = -1;
+            have_saved = false;
         }
     });
 }

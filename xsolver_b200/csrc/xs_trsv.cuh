@@ -62,9 +62,9 @@ __device__ __forceinline__ float msub(float acc, float y, float v) { return __fm
 //   backoff_ns     upper bound of the exponential back-off between polls of a
 //                  pending dependency (0: spin without sleeping)
 struct TrsvTuning {
-    int blocks_per_sm = 4;
+    int blocks_per_sm = 2;
     int backoff_ns = 128;
-    int chunk_rows = 24576;  // chunked kernel: rows per CTA chunk (0: level-ordered kernel)
+    int chunk_rows = 0;  // chunked kernel: rows per CTA chunk (0: level-ordered kernel)
 };
 TrsvTuning &trsv_tuning();
 
