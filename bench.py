@@ -2,12 +2,14 @@
 """Benchmark: time to relative residual 1e-10 on one B200.
 
 Workload (the configuration the headline metric is quoted on): 3D 7-point
-Poisson on a 128^3 grid (n = 2,097,152, nnz = 14,581,760), FP64 CSR,
-b ~ U(-1,1) from seed 0, x0 = 0, BiCGSTAB + exact ILU(0) with sync-free
-SpTRSV, rtol 1e-10.  One step = one complete solve of that system by the
-mixed-precision refinement (FP64 outer residual/update, FP32 inner BiCGSTAB,
-BF16 ILU factors, inner rtol 1e-4).  The FP64 GPU solve of the same system is
-timed alongside and reported as `fp64_ms`.
+Poisson on a 128^3 grid (n = 2,097,152, nnz = 14,581,760), FP64, stored as
+ELL (width 7) — CSR with --format csr — b ~ U(-1,1) from seed 0, x0 = 0,
+BiCGSTAB + ILU(0), rtol 1e-10.  One step = one complete solve of that system
+by the mixed-precision refinement (FP64 outer residual/update, FP32 inner
+BiCGSTAB, BF16 ILU(0) factors, inner rtol 1e-4, inner triangular solves by
+Jacobi sweeps).  The FP64 GPU path (exact sync-free SpTRSV) is timed
+alongside as `fp64_ms`, and the two cross-over variants (FP64 with sweeps,
+mixed with exact SpTRSV) under `variants`.
 
   value   device time per solve (ms), inputs resident in HBM, CUDA events on
           the solver's stream, max over ranks
@@ -199,15 +201,24 @@ def run_ours(args):
 
     A, b = make_problem()
     n = A.n
+    fmt = args.format
 
-    def make_solver(mixed: bool):
-        S = Solver(A).ksp_settype("bicgstab").ksp_setoption(1e-10, 2000).pc_settype("ilu0")
+    def make_solver(mixed: bool, trsv: int):
+        S = Solver(A, fmt=fmt).ksp_settype("bicgstab").ksp_setoption(1e-10, 3000).pc_settype("ilu0")
+        S.pc_set_trsv(trsv)
         if mixed:
             S.set_precision("fp64", "fp32", "bf16").set_inner(1e-4, 300)
         return S
 
-    S_mix = make_solver(True)
-    S_64 = make_solver(False)
+    # headline: mixed-precision refinement with BF16 ILU(0) factors and the
+    # Jacobi-sweep triangular solve in the inner FP32 solve; the FP64 GPU path
+    # (exact sync-free SpTRSV) and the two cross-over variants are timed too
+    variants = {
+        "mixed_sweeps": make_solver(True, args.sweeps),
+        "fp64_exact": make_solver(False, 0),
+        "fp64_sweeps": make_solver(False, args.sweeps),
+        "mixed_exact": make_solver(True, 0),
+    }
     db = torch.from_numpy(b).to(dev)
     x = torch.zeros(n, dtype=torch.float64, device=dev)
 
@@ -235,66 +246,81 @@ def run_ours(args):
 
     # warm-up (includes factorisation and graph capture)
     for _ in range(max(args.warmup, 3)):
-        x.zero_()
-        S_mix.solve_device(db, x)
-        x.zero_()
-        S_64.solve_device(db, x)
+        for S in variants.values():
+            x.zero_()
+            S.solve_device(db, x)
     clocks = Clocks(local)
     clocks.start()
-    ms_mix, launches = timed(S_mix, args.steps)
-    it_mix = S_mix.timing()["iterations"]
-    outer = S_mix.outer_steps()
-    ms_64, _ = timed(S_64, args.steps)
-    it_64 = S_64.timing()["iterations"]
+    res = {}
+    for name, S in variants.items():
+        steps = args.steps if name in ("mixed_sweeps", "fp64_exact") else max(1, args.steps // 2)
+        ms, launches = timed(S, steps)
+        t = S.timing()
+        res[name] = {"ms": ms, "iterations": t["iterations"], "outer_steps": S.outer_steps(),
+                     "launches_per_solve": launches // steps, "setup_ms": t["setup_ms"]}
     clk = clocks.stop()
-    # correctness of the timed solve (true residual in FP64 on the host)
-    x.zero_()
-    S_mix.solve_device(db, x)
-    xs = x.cpu().numpy()
-    relres = float(np.linalg.norm(b - A.to_scipy() @ xs) / np.linalg.norm(b))
+    Asp = A.to_scipy()
+    for name, S in variants.items():
+        x.zero_()
+        S.solve_device(db, x)
+        xs = x.cpu().numpy()
+        res[name]["true_relres"] = float(np.linalg.norm(b - Asp @ xs) / np.linalg.norm(b))
+    S_mix = variants["mixed_sweeps"]
+    ms_mix = res["mixed_sweeps"]["ms"]
     # e2e through the public API with host buffers
-    e2e_ms, _ = timed(S_mix, max(1, args.steps // 2 or 1), device_resident=False)
-    setup_ms = S_mix.timing()["setup_ms"]
+    e2e_ms, _ = timed(S_mix, max(1, args.steps // 2), device_resident=False)
 
     # kernel roofline, timed live with CUDA events (L2 flushed between reps)
     peak, peak_kind = _peaks()
     P = Plan(A).factor("ilu0")
     P.build_ell()
     kern = {}
-    for op, prec in [("csr64", "fp64"), ("ell64", "fp64"), ("csr32", "fp64"), ("lsolve", "fp64"), ("usolve", "fp64"),
-                     ("lsolve", "bf16"), ("usolve", "bf16"), ("lusolve", "bf16")]:
+
+    def tk(label, op, prec, trsv):
         P.set_factor_precision(prec)
+        P.set_trsv(trsv)
         t = P.time_op(op, reps=10, flush_l2=True)
         by = P.op_bytes(op)
-        kern[f"{op}_{prec}" if op not in ("csr64", "ell64", "csr32") else op] = {
-            "ms": t, "bytes": by, "GBs": by / t / 1e6, "frac": by / t / 1e6 / peak}
+        kern[label] = {"ms": t, "bytes": by, "GBs": by / t / 1e6, "frac": by / t / 1e6 / peak}
+
+    tk("spmv_csr_fp64", "csr64", "fp64", 0)
+    tk("spmv_ell_fp64", "ell64", "fp64", 0)
+    tk("spmv_csr_fp32", "csr32", "fp64", 0)
+    tk("spmv_ell_fp32", "ell32", "fp64", 0)
+    tk("sptrsv_L_fp64_exact", "lsolve", "fp64", 0)
+    tk("sptrsv_U_fp64_exact", "usolve", "fp64", 0)
+    tk("sptrsv_LU_bf16_exact", "lusolve", "bf16", 0)
+    tk(f"lu_bf16_sweeps{args.sweeps}", "lusolve", "bf16", args.sweeps)
+    tk(f"lu_fp64_sweeps{args.sweeps}", "lusolve", "fp64", args.sweeps)
     levels = P.levels()
-    dom = kern["lusolve_bf16"]
+    dom = kern[f"lu_bf16_sweeps{args.sweeps}"]
     lines = {
         "metric": METRIC, "value": ms_mix, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_mix, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (outer) / f32 (inner) / bf16 (factors)",
         "data": "synthetic (seeded stencil system, inputs larger than L2)",
-        "config": {"workload": WORKLOAD, "solver": "mixed-precision refinement, inner BiCGSTAB FP32, BF16 ILU(0)",
+        "config": {"workload": WORKLOAD, "format": fmt,
+                   "solver": f"mixed-precision refinement: FP64 outer residual/update, inner FP32 BiCGSTAB (rtol 1e-4), "
+                             f"BF16 ILU(0) factors, inner triangular solves by {args.sweeps} Jacobi sweeps",
                    "parallelism": f"replicas x{ws}", "l2": "inputs (175 MB matrix) larger than L2; kernels timed "
                                                            "with an L2 flush between repetitions"},
-        "fp64_ms": ms_64, "speedup_mixed_vs_fp64": ms_64 / ms_mix, "iterations_fp64": it_64,
-        "iterations_mixed_inner": it_mix, "outer_steps": outer, "true_relres": relres, "setup_ms": setup_ms,
-        "levels": {"L": levels[0], "U": levels[1]},
+        "fp64_ms": res["fp64_exact"]["ms"], "speedup_vs_fp64": res["fp64_exact"]["ms"] / ms_mix,
+        "variants": res, "levels": {"L": levels[0], "U": levels[1]},
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "sync-free SpTRSV L+U (BF16 factors, FP32 vectors)",
+        "gpu_launches": int(res["mixed_sweeps"]["launches_per_solve"] * args.steps),
+        "roofline": {"bound": "hbm", "kernel": f"ILU(0) apply, BF16 factors, FP32 vectors, {args.sweeps} Jacobi sweeps",
                      "achieved": dom["GBs"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
                      "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes": dom["bytes"]},
         "kernels": kern,
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu and ws == 1:
+        it64 = res["fp64_exact"]["iterations"]
         t_setup, t_it = cpu_reference_sample(A, b, 8, None)
-        cpu_ms = (t_setup + t_it * it_64) * 1e3
+        cpu_ms = (t_setup + t_it * it64) * 1e3
         lines["cpu_baseline"] = {"value": cpu_ms, "unit": "ms", "cores": 1, "kind": "port",
                                  "sample": f"restated reference BiCGSTAB + ILU(0) (FP64): ILU(0) setup + 8 iterations "
-                                           f"timed, scaled to the {it_64} iterations of the FP64 solve",
+                                           f"timed, scaled to the {it64} iterations of the FP64 solve",
                                  "host_threads_available": os.cpu_count()}
     if rank == 0:
         print(json.dumps(lines), flush=True)
@@ -312,6 +338,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--format", default="ell", choices=["csr", "ell"])
+    ap.add_argument("--sweeps", type=int, default=3)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

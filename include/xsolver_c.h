@@ -232,6 +232,9 @@ int xs_plan_get_factors(xs_plan_t p, int *nnzL, int *nnzU, int *lrp, int *lci, d
 int xs_plan_get_lu_values(xs_plan_t p, double *luv);
 /* factor storage precision for the solves below: 0 FP64, 1 FP32, 2 BF16, 3 FP16 */
 int xs_plan_set_factor_precision(xs_plan_t p, int prec);
+/* triangular solve mode of the plan's LU solves: 0 exact sync-free, k > 0
+ * k Jacobi sweeps per triangle */
+int xs_plan_set_trsv(xs_plan_t p, int mode);
 /* z = (L D U')^{-1} x with sync-free solves (vec_prec 0 FP64 / 1 FP32) */
 int xs_plan_lusolve(xs_plan_t p, int vec_prec, const void *d_x, void *d_z);
 /* z = (L D U')^{-T} x */

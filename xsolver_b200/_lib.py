@@ -81,6 +81,7 @@ def _declare(L):
         "xs_plan_get_lu_values": [C.c_void_p, _dp],
         "xs_plan_set_factor_precision": [C.c_void_p, C.c_int],
         "xs_plan_lusolve": [C.c_void_p, C.c_int, _vp, _vp],
+        "xs_plan_set_trsv": [C.c_void_p, C.c_int],
         "xs_plan_lusolve_t": [C.c_void_p, _vp, _vp],
         "xs_plan_sync": [C.c_void_p],
         "xs_plan_debug_break_dependency": [C.c_void_p, C.c_int, C.c_int],

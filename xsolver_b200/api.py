@@ -246,6 +246,10 @@ class Plan:
         check(self._L.xs_plan_set_factor_precision(self.p, self.PREC[prec]), "set_factor_precision")
         return self
 
+    def set_trsv(self, mode: int):
+        check(self._L.xs_plan_set_trsv(self.p, mode), "set_trsv")
+        return self
+
     def lusolve(self, x, z):
         prec = 0 if str(x.dtype) == "torch.float64" else 1
         check(self._L.xs_plan_lusolve(self.p, prec, C.c_void_p(x.data_ptr()), C.c_void_p(z.data_ptr())), "lusolve")

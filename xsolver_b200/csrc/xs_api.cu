@@ -456,13 +456,12 @@ static void build_precond(Handle &h)
         check_launch();
         load_tri_values(h, M.L, h.fv.p, need32);
         load_tri_values(h, M.U, h.fv.p, need32);
+        load_tri_ell(M.L, h.fv.p, need32, h.s);
+        load_tri_ell(M.U, h.fv.p, need32, h.s);
         load_dinv(h, h.fv.p, h.udiag_src.p, need32);
         M.ensure_buffers64(h.s);
         if (need32) M.ensure_buffers32(h.s);
-        if (h.trsv_mode > 0) {
-            M.tmp64a.alloc(n); M.tmp64b.alloc(n);
-            if (need32) { M.tmp32a.alloc(n); M.tmp32b.alloc(n); }
-        }
+        if (h.trsv_mode > 0) M.ensure_sweep_buffers(need32);
         M.have_factors = true;
     } else if (type == PC_PARILUT) {
         parilut_build(h.s, h.err.p, n, h.A, h.hrp, h.hci, h.parilut_fill, h.parilut_sweeps, h.parilut_droptol, h.ilut);
@@ -470,10 +469,7 @@ static void build_precond(Handle &h)
         ilut_to_tri(h.s, n, h.ilut, M.L, M.U, need32);
         M.ensure_buffers64(h.s);
         if (need32) M.ensure_buffers32(h.s);
-        if (h.trsv_mode > 0) {
-            M.tmp64a.alloc(n); M.tmp64b.alloc(n);
-            if (need32) { M.tmp32a.alloc(n); M.tmp32b.alloc(n); }
-        }
+        if (h.trsv_mode > 0) M.ensure_sweep_buffers(need32);
         M.have_factors = true;
     }
     XS_CUDA(cudaEventRecord(e1, h.s));
@@ -810,7 +806,9 @@ static void adjoint_prepare(Handle &h)
         k_gather_dinv<double><<<g, 256, 0, h.s>>>(n, nullptr, diagsrc, vals, T.U.dinv64_nat.p);
         check_launch();
         T.ensure_buffers64(h.s);
-        if (T.trsv_mode > 0) { T.tmp64a.alloc(n); T.tmp64b.alloc(n); }
+        load_tri_ell(T.L, vals, false, h.s);
+        load_tri_ell(T.U, vals, false, h.s);
+        if (T.trsv_mode > 0) T.ensure_sweep_buffers(false);
         XS_CUDA(cudaStreamSynchronize(h.s));
     }
     a.have_Mt = true;

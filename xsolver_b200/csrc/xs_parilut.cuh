@@ -686,6 +686,7 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
                 k_gather_convert<__half><<<g, 256, 0, s>>>(T.nnz, T.src_nat.p, vals, T.nvh.p);
             }
         }
+        load_tri_ell(T, vals, need32, s);
         check_launch();
         XS_CUDA(cudaStreamSynchronize(s));
     };

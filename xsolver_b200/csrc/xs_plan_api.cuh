@@ -192,6 +192,16 @@ int xs_plan_set_factor_precision(xs_plan_t p, int prec)
         p->h->factor_prec = prec;
     });
 }
+int xs_plan_set_trsv(xs_plan_t p, int mode)
+{
+    return guarded([&] {
+        if (!p || mode < 0 || mode > 1000) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        h.trsv_mode = mode;
+        h.M.trsv_mode = mode;
+        if (mode > 0) h.M.ensure_sweep_buffers(h.inner32 != 0);
+    });
+}
 int xs_plan_lusolve(xs_plan_t p, int vec_prec, const void *x, void *z)
 {
     return guarded([&] {
@@ -280,9 +290,19 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
             const int fp = h.M.factor_prec;
             const double V = fp == 0 ? 8 : (fp == 1 ? 4 : 2);
             const double X = fp == 0 ? 8 : 4;  // vector element
-            const double l = (V + I) * h.M.L.nnz + I * (n + 1) + 2 * X * n;
-            const double u = (V + I) * h.M.U.nnz + I * (n + 1) + 3 * X * n;
-            *bytes = op == 3 ? l : (op == 4 ? u : l + u);
+            const int k = h.M.trsv_mode;
+            if (k == 0) {
+                // exact solve: factor entries + row pointers, rhs read, result written (+ dinv for U)
+                const double l = (V + I) * h.M.L.nnz + I * (n + 1) + 2 * X * n;
+                const double u = (V + I) * h.M.U.nnz + I * (n + 1) + 3 * X * n;
+                *bytes = op == 3 ? l : (op == 4 ? u : l + u);
+            } else {
+                // k Jacobi sweeps = k-1 passes per triangle: entries, rhs, previous iterate, result (+ dinv for U)
+                const double passes = k > 1 ? k - 1 : 0;
+                const double l = passes * ((V + I) * h.M.L.nnz + 3 * X * n);
+                const double u = passes * ((V + I) * h.M.U.nnz + 4 * X * n) + (k <= 1 ? 3 * X * n : 0);
+                *bytes = op == 3 ? l : (op == 4 ? u : l + u);
+            }
             break;
         }
         default: throw Status(XS_ERR_INVALID);

@@ -32,8 +32,8 @@ struct PrecondDev {
     DBuf<double> jdiag64;
     DBuf<float> jdiag32;
     TriDev L, U;
-    DBuf<double> lbuf64, ubuf64, tmp64a, tmp64b;
-    DBuf<float> lbuf32, ubuf32, tmp32a, tmp32b;
+    DBuf<double> lbuf64, ubuf64, tmp64a, tmp64b, tmp64c;
+    DBuf<float> lbuf32, ubuf32, tmp32a, tmp32b, tmp32c;
     int *err = nullptr;
     bool have_factors = false;
 
@@ -56,6 +56,12 @@ struct PrecondDev {
             k_fill_sentinel<float><<<256, 256, 0, s>>>(ubuf32, n);
             check_launch();
         }
+    }
+    // temporaries of the Jacobi-sweep mode
+    void ensure_sweep_buffers(bool need32)
+    {
+        if (tmp64a.n != (size_t)n) { tmp64a.alloc(n); tmp64b.alloc(n); tmp64c.alloc(n); }
+        if (need32 && tmp32a.n != (size_t)n) { tmp32a.alloc(n); tmp32b.alloc(n); tmp32c.alloc(n); }
     }
     // re-arm the sentinel buffers (after an aborted solve)
     void rearm(cudaStream_t s)
@@ -149,34 +155,53 @@ struct PrecondDev {
     void apply_sweeps(const VT *x, VT *z, const int *done_flag, cudaStream_t s)
     {
         using DT = VT;
-        VT *ta, *tb;
+        VT *ta, *tb, *tc;
         const DT *dinv;
-        if constexpr (std::is_same<VT, double>::value) { ta = tmp64a.p; tb = tmp64b.p; dinv = U.dinv64_nat.p; }
-        else { ta = tmp32a.p; tb = tmp32b.p; dinv = U.dinv32_nat.p; }
-        const int g = geom().sms * 4;
-        // L: y_1 = x, y_{t+1} = x - L y_t ; ends in ta
+        if constexpr (std::is_same<VT, double>::value) { ta = tmp64a.p; tb = tmp64b.p; tc = tmp64c.p; dinv = U.dinv64_nat.p; }
+        else { ta = tmp32a.p; tb = tmp32b.p; tc = tmp32c.p; dinv = U.dinv32_nat.p; }
+        const int g = geom().sms * 8;
+        const int k = trsv_mode;
+        // one sweep pass over triangle T: ELL when available, else CSR
+        auto pass = [&](const TriDev &T, bool upper, bool first2, const VT *rhs, const VT *yin, VT *yout) {
+            if (T.ell_w > 0) {
+                const FT *ev = T.evals<FT>();
+                if (upper) {
+                    if (first2) k_trsv_sweep_ell<VT, FT, DT, true, true><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, dinv, rhs, yin, yout, done_flag);
+                    else k_trsv_sweep_ell<VT, FT, DT, true, false><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, dinv, rhs, yin, yout, done_flag);
+                } else {
+                    if (first2) k_trsv_sweep_ell<VT, FT, DT, false, true><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
+                    else k_trsv_sweep_ell<VT, FT, DT, false, false><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
+                }
+            } else {
+                // CSR: the first sweep is a separate pass (yin = null -> y_1)
+                if (first2) {
+                    VT *tmp = tc;  // distinct from every buffer the stages read or write
+                    if (upper) k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), dinv, rhs, (const VT *)nullptr, tmp, 1, done_flag);
+                    else k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), (const DT *)nullptr, rhs, (const VT *)nullptr, tmp, 1, done_flag);
+                    yin = tmp;
+                }
+                if (upper) k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), dinv, rhs, yin, yout, 0, done_flag);
+                else k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), (const DT *)nullptr, rhs, yin, yout, 0, done_flag);
+            }
+        };
+        if (k <= 1) {
+            // L^-1 x ~ x ; U'^-1 (dinv y) ~ dinv y
+            k_diag_scale<VT, DT><<<g, 256, 0, s>>>(n, dinv, x, z, done_flag);
+            return;
+        }
+        // L: passes 2..k, result in `cur` (ta or tb)
         VT *cur = ta, *other = tb;
-        k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, L.rp_nat, L.ci_nat, natvals<FT>(L), (const DT *)nullptr, x,
-                                                          (const VT *)nullptr, cur, 1, done_flag);
-        for (int t = 1; t < trsv_mode; t++) {
-            k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, L.rp_nat, L.ci_nat, natvals<FT>(L), (const DT *)nullptr,
-                                                              x, cur, other, 0, done_flag);
+        pass(L, false, true, x, nullptr, cur);
+        for (int t = 3; t <= k; t++) {
+            pass(L, false, false, x, cur, other);
             std::swap(cur, other);
         }
-        // U: w_1 = dinv*y, w_{t+1} = dinv*y - U' w_t ; result in z
+        // U on y = cur: k-1 passes ping-ponging between `other` and z, ending in z
         const VT *yv = cur;
-        VT *wa = other, *wb = z;
-        // ping-pong between `other` and z, finishing in z
-        int sweeps = trsv_mode;
-        VT *bufs[2] = {(sweeps % 2 == 1) ? z : other, (sweeps % 2 == 1) ? other : z};
-        k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, U.rp_nat, U.ci_nat, natvals<FT>(U), dinv, yv,
-                                                         (const VT *)nullptr, bufs[0], 1, done_flag);
-        for (int t = 1; t < sweeps; t++) {
-            k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, U.rp_nat, U.ci_nat, natvals<FT>(U), dinv, yv,
-                                                             bufs[(t - 1) & 1], bufs[t & 1], 0, done_flag);
-        }
-        (void)wa;
-        (void)wb;
+        const int passes = k - 1;
+        VT *bufs[2] = {(passes % 2 == 1) ? z : other, (passes % 2 == 1) ? other : z};
+        pass(U, true, true, yv, nullptr, bufs[0]);
+        for (int t = 1; t < passes; t++) pass(U, true, false, yv, bufs[(t - 1) & 1], bufs[t & 1]);
     }
 };
 

@@ -338,7 +338,12 @@ inline void build_tiling(const int *h_rp, int n, int max_rows, int cap, SpmvTili
     rb.push_back(n);
     t.nblocks = (int)lr.size();
     t.max_rows = max_rows;
-    t.cap = cap;
+    // shared-memory stage = the largest staged range actually needed (so
+    // short rows leave room for more resident blocks), rounded to 64 entries
+    long need = 4;
+    for (size_t b = 0; b < lr.size(); b++)
+        if (!lr[b]) need = std::max(need, (long)(((h_rp[rb[b + 1]] + 3) & ~3) - (h_rp[rb[b]] & ~3)));
+    t.cap = (int)std::min<long>(cap, (need + 63) & ~63L);
     t.rb.alloc(rb.size());
     t.rb.upload(rb.data(), rb.size(), s);
     t.longrow.alloc(std::max<size_t>(lr.size(), 1));
@@ -361,21 +366,24 @@ inline size_t spmv_smem(int cap)
 }
 
 template <typename VT, typename MT, typename Epi>
-inline int spmv_grid(int nblocks)
+inline int spmv_grid(int nblocks, int cap)
 {
-    static int per_sm = -1;
-    static int dev_sms = 0;
-    if (per_sm < 0) {
-        int cap = spmv_cap<MT>();
-        size_t sm = spmv_smem<MT>(cap);
+    static int cached_cap = -1;
+    static int per_sm = 1;
+    static bool attr = false;
+    if (!attr) {
         XS_CUDA(cudaFuncSetAttribute(k_csr_spmv_tiled<VT, MT, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sm));
-        int occ = 0;
-        XS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_csr_spmv_tiled<VT, MT, Epi>, SPMV_THREADS, sm));
-        per_sm = occ > 0 ? occ : 1;
-        dev_sms = geom().sms;
+                                     (int)spmv_smem<MT>(spmv_cap<MT>())));
+        attr = true;
     }
-    long g = (long)per_sm * dev_sms;
+    if (cap != cached_cap) {
+        int occ = 0;
+        XS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_csr_spmv_tiled<VT, MT, Epi>, SPMV_THREADS,
+                                                              spmv_smem<MT>(cap)));
+        per_sm = occ > 0 ? occ : 1;
+        cached_cap = cap;
+    }
+    long g = (long)per_sm * geom().sms;
     if (g > nblocks) g = nblocks;
     return (int)(g > 0 ? g : 1);
 }
@@ -388,7 +396,7 @@ inline void launch_csr(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot 
     CsrTileArgs<MT> a;
     if constexpr (std::is_same<MT, double>::value) a = op.csr64();
     else a = op.csr32();
-    int g = grid > 0 ? grid : spmv_grid<VT, MT, Epi>(t.nblocks);
+    int g = grid > 0 ? grid : spmv_grid<VT, MT, Epi>(t.nblocks, t.cap);
     size_t sm = spmv_smem<MT>(t.cap);
     k_csr_spmv_tiled<VT, MT, Epi><<<g, SPMV_THREADS, sm, s>>>(a, x, y, epi, slot);
     check_launch();

@@ -349,6 +349,46 @@ __global__ void k_trsv_sweep(int n, const int *__restrict__ rp, const int *__res
     }
 }
 
+// Jacobi sweeps on a column-major ELL copy of the triangle (natural order,
+// padding column = the row itself with value 0): every load is coalesced.
+// FIRST2 folds the first sweep into the second: the previous iterate of the
+// first sweep is x itself (L) or dinv*x (U), so k sweeps cost k-1 passes.
+template <typename VT, typename FT, typename DT, bool UPPER, bool FIRST2>
+__global__ void __launch_bounds__(256) k_trsv_sweep_ell(int n, int w, const int *__restrict__ eci,
+                                                       const FT *__restrict__ ev, const DT *__restrict__ dinv,
+                                                       const VT *__restrict__ x, const VT *__restrict__ yin,
+                                                       VT *__restrict__ yout, const int *done_flag)
+{
+    if (done_flag && *done_flag) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        VT acc = UPPER ? (VT)(x[i] * (VT)dinv[i]) : x[i];
+        for (int k = 0; k < w; k++) {
+            const long o = (long)k * n + i;
+            const int c = __ldg(eci + o);
+            const VT v = (VT)FVal<FT>::ld(ev, o);
+            VT y;
+            if (FIRST2) y = UPPER ? (VT)(x[c] * (VT)dinv[c]) : x[c];
+            else y = yin[c];
+            acc = msub(acc, y, v);
+        }
+        yout[i] = acc;
+    }
+}
+
+// dst[q] = src >= 0 ? (FT) vals[src[q]] : 0
+template <typename FT>
+__global__ void k_gather_convert_pad(long m, const long *__restrict__ src, const double *__restrict__ vals, FT *dst)
+{
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < m; q += (long)gridDim.x * blockDim.x) {
+        const long s = src[q];
+        const double v = s >= 0 ? vals[s] : 0.0;
+        if constexpr (std::is_same<FT, double>::value) dst[q] = v;
+        else if constexpr (std::is_same<FT, float>::value) dst[q] = (float)v;
+        else if constexpr (std::is_same<FT, __nv_bfloat16>::value) dst[q] = __double2bfloat16(v);
+        else dst[q] = __double2half(v);
+    }
+}
+
 // ---------------------------------------------------------------- host plan building
 // Host-side analysis of a triangular pattern.
 struct TriHostPlan {
@@ -507,6 +547,16 @@ struct TriDev {
     DBuf<double> dinv64_nat;
     DBuf<float> dinv32_nat;
     DBuf<unsigned> ticket;
+    // natural-order ELL copy for the Jacobi-sweep mode (ell_w = 0: none)
+    int ell_w = 0;
+    DBuf<int> eci;
+    DBuf<long> esrc;
+    DBuf<double> ev64;
+    DBuf<float> ev32;
+    DBuf<__nv_bfloat16> evbf;
+    DBuf<__half> evh;
+    template <typename FT>
+    const FT *evals() const;
     // chunked layout (perm/prp/pci then hold the chunk-major order, pci encoded)
     bool chunked = false;
     int nchunks = 0, ch = 0;
@@ -522,6 +572,14 @@ struct TriDev {
     template <typename FT>
     const FT *vals() const;
 };
+template <>
+inline const double *TriDev::evals<double>() const { return ev64.p; }
+template <>
+inline const float *TriDev::evals<float>() const { return ev32.p; }
+template <>
+inline const __nv_bfloat16 *TriDev::evals<__nv_bfloat16>() const { return evbf.p; }
+template <>
+inline const __half *TriDev::evals<__half>() const { return evh.p; }
 template <>
 inline const double *TriDev::vals<double>() const { return pv64.p; }
 template <>
@@ -608,8 +666,47 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     std::vector<long> ns(T.nnz);
     for (long k = 0; k < T.nnz; k++) ns[k] = src_of((int)k);
     T.src_nat.alloc(m); if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
+    // ELL copy when the rows are nearly uniform (padding at most 2x)
+    int w = 0;
+    for (int i = 0; i < n; i++) w = std::max(w, rp[i + 1] - rp[i]);
+    T.ell_w = 0;
+    if (w > 0 && w <= 64 && (long)w * n <= 2 * std::max<long>(T.nnz, 1)) {
+        std::vector<int> ec((size_t)w * n);
+        std::vector<long> es((size_t)w * n);
+        for (int i = 0; i < n; i++) {
+            int k = 0;
+            for (int q = rp[i]; q < rp[i + 1]; q++, k++) {
+                ec[(size_t)k * n + i] = ci[q];
+                es[(size_t)k * n + i] = src_of(q);
+            }
+            for (; k < w; k++) {
+                ec[(size_t)k * n + i] = i;
+                es[(size_t)k * n + i] = -1;
+            }
+        }
+        T.ell_w = w;
+        T.eci.alloc((size_t)w * n); T.eci.upload(ec.data(), (size_t)w * n, s);
+        T.esrc.alloc((size_t)w * n); T.esrc.upload(es.data(), (size_t)w * n, s);
+    }
     T.ticket.alloc(1);
     XS_CUDA(cudaStreamSynchronize(s));
+}
+
+// gather the ELL copy's values (FP64 always, reduced precisions on request)
+inline void load_tri_ell(TriDev &T, const double *vals, bool need32, cudaStream_t s)
+{
+    if (T.ell_w == 0) return;
+    const long m = (long)T.ell_w * T.n;
+    const int g = geom().sms * 4;
+    if (T.ev64.n != (size_t)m) T.ev64.alloc(m);
+    k_gather_convert_pad<double><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.ev64.p);
+    if (need32) {
+        if (T.ev32.n != (size_t)m) { T.ev32.alloc(m); T.evbf.alloc(m); T.evh.alloc(m); }
+        k_gather_convert_pad<float><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.ev32.p);
+        k_gather_convert_pad<__nv_bfloat16><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.evbf.p);
+        k_gather_convert_pad<__half><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.evh.p);
+    }
+    check_launch();
 }
 
 template <typename VT, typename FT, typename DT, bool UPPER>
