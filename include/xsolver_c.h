@@ -101,7 +101,10 @@ const char *xsolver_error_string(int status);
  * selected ksp type).  factor "fp64", "fp32", "bf16" or "fp16": storage of
  * the ILU factor values (dinv is kept in FP32/FP64). */
 void xsolver_set_precision(const char *outer, const char *inner, const char *factor);
-/* inner relative tolerance and iteration cap of the refinement's inner solve */
+/* inner relative tolerance and iteration cap of the refinement's inner
+ * solve.  A step whose outer residual is already within 1/inner_rtol of the
+ * target solves only to 0.25 * target / ||r|| (never tighter than inner_rtol,
+ * never looser than 0.5). */
 void xsolver_set_inner(double inner_rtol, int inner_maxiter);
 /* ParILU sweep count (default 20, hip/Precond/precon_gpuilu0.cpp:5) */
 void xsolver_pc_setparilu(int sweeps);
@@ -130,6 +133,10 @@ typedef struct xs_handle_s *xs_handle_t;
 int xs_create(xs_handle_t *h);
 int xs_destroy(xs_handle_t h);
 int xs_mat_setup(xs_handle_t h, int n, const int *rowptr, const int *colidx, const double *val, int format);
+/* new values for the pattern given to xs_mat_setup, in the caller's entry
+ * order (cpu_mat_update + gpu_mat_update for a handle, intel/HostMatrix.h:196-200,
+ * cuda/DeviceMatrix.h:145-148); the preconditioner is rebuilt on the next solve */
+int xs_mat_update(xs_handle_t h, const double *val);
 int xs_ksp_settype(xs_handle_t h, const char *fmt);
 int xs_ksp_setoption(xs_handle_t h, double tol, int maxiter, int *usediter, double *resvec, int restart);
 int xs_ksp_set_absolute_tol(xs_handle_t h, double absolute_tol);
@@ -291,6 +298,12 @@ int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, 
  * XS_TRSV_BACKOFF_NS, XS_TRSV_CHUNK_ROWS override them at first use.  The
  * layout is fixed when a preconditioner is built: set before factorising. */
 int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
+/* Column storage of ELL copies (the ELL SpMV and the Jacobi-sweep triangle
+ * copies): index_bits 16 stores each column as a 16-bit offset from its row
+ * whenever every |col - row| <= 32767 (default; halves the index bytes of
+ * banded matrices), 32 always stores 32-bit columns.  Environment
+ * XS_ELL_INDEX16=0 selects 32 at first use.  Applies to copies built later. */
+int xs_set_ell_index_bits(int index_bits);
 
 /* library identification */
 const char *xs_version(void);

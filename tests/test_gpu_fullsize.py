@@ -1,0 +1,146 @@
+"""Parity at the full sizes of the benchmark configurations.
+
+  * 3D 7-point Poisson 128^3 (n = 2,097,152), BiCGSTAB + ILU(0), rtol 1e-10,
+    FP64 on the GPU (CSR and ELL) against the restated reference on the host:
+    ILU(0) factors bit for bit, per-iteration residual history within the
+    calibrated bound of tests/parity.py, iteration count within +-1, final
+    solution within the same calibration.  The mixed-precision refinement
+    (BF16 and FP16 factors) must reach 1e-10 and agree with the host FP64
+    solve converged to 1e-14 to the conditioning bound.
+  * Variable-coefficient 7-point diffusion 96^3 (n = 884,736), a batch of 8
+    right-hand sides: forward PCG + ILU(0) to 1e-12, adjoint for
+    L = 1/2 ||x - x*||^2.  Checked: A^T lambda = dL/dx to 1e-10, dL/dA equal
+    to -lambda_i x_j on the pattern, and central finite differences with
+    h = 1e-6 on 64 random entries of A and 64 of b, within 1e-6 relative.
+
+The finite differences at this size are formed from increments: x(p +- h)
+= x + delta+-, where delta+- solves the perturbed system for the increment
+exactly ((A + hE) delta = -h E x for an entry of A; A delta = h e_i for an
+entry of b), so L(p + h) - L(p - h) = (delta+ - delta-) . (x - x* +
+(delta+ + delta-)/2) carries no cancellation between two O(1) losses.  That
+is the central difference quotient itself, evaluated without the 1e-4
+rounding floor that subtracting two independently solved 884,736-vectors
+would put on it.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from parity import history_ok, reference_with_bounds
+from xsolver_b200 import stencils as st
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c2():
+    A = st.poisson3d_7pt(128)
+    b = st.rhs_uniform(A.n, 0)
+    F = oracle.ilu0(A)
+    ref = reference_with_bounds("bicgstab", A, b, tol=1e-10, maxiter=1000, pc="lu", factors=F)
+    x14, _, _ = oracle.solve("bicgstab", A, b, tol=1e-14, maxiter=2000, pc="lu", factors=F)
+    return A, b, F, ref, x14
+
+
+def test_c2_ilu0_factors_bitwise(cuda, c2):
+    from xsolver_b200.api import Plan
+
+    A, b, F, _, _ = c2
+    G = Plan(A).factor("ilu0").factors()
+    for k in ("lrp", "lci", "lv", "dinv", "urp", "uci", "uv"):
+        assert np.array_equal(G[k], getattr(F, k)), k
+
+
+@pytest.mark.parametrize("fmt", ["csr", "ell"])
+def test_c2_fp64_bicgstab_ilu0_vs_reference(cuda, c2, fmt):
+    from xsolver_b200.api import Solver
+
+    A, b, F, (xo, ro, uo, hb, xb), _ = c2
+    S = Solver(A, fmt=fmt).ksp_settype("bicgstab").ksp_setoption(1e-10, 1000).pc_settype("ilu0")
+    x = S.solve(b)
+    hist = S.resvec()
+    assert abs(S.usediter - (uo + 1)) <= 1, (S.usediter, uo + 1)
+    ok, worst = history_ok(hist[1:] / hist[0], ro, hb)
+    assert ok, worst
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
+    r = b - A.to_scipy() @ x
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10
+
+
+@pytest.mark.parametrize("factor", ["bf16", "fp16"])
+@pytest.mark.parametrize("trsv", [0, 3])
+def test_c2_mixed_refinement_vs_fp64_1e14(cuda, c2, factor, trsv):
+    from xsolver_b200.api import Solver
+
+    A, b, _, _, x14 = c2
+    S = Solver(A, fmt="ell").ksp_settype("bicgstab").ksp_setoption(1e-10, 3000).pc_settype("ilu0").pc_set_trsv(trsv)
+    S.set_precision("fp64", "fp32", factor).set_inner(1e-4, 300)
+    x = S.solve(b)
+    relres = np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)
+    assert relres < 1e-10, relres
+    assert S.outer_steps() >= 2
+    # ||x - x14|| / ||x14|| <= cond(A) * relres; cond of this operator is ~6.7e3
+    err = np.linalg.norm(x - x14) / np.linalg.norm(x14)
+    assert err < 6.7e3 * max(relres, 1e-14) + 1e-12, (err, relres)
+
+
+def _probe_solver(A, trsv=3):
+    from xsolver_b200.api import Solver
+
+    return (Solver(A).ksp_settype("bicgstab").ksp_setoption(1e-14, 3000).ksp_set_absolute_tol(1e-300)
+            .pc_settype("ilu0").pc_set_trsv(trsv))
+
+
+def test_c5_adjoint_batch8_96(cuda):
+    from xsolver_b200.api import Solver
+
+    A = st.varcoef3d_7pt(96, 0)
+    n = A.n
+    Asp = A.to_scipy()
+    rng = np.random.default_rng(0)
+    B = np.stack([st.rhs_uniform(n, s) for s in range(8)])
+    XS = rng.uniform(-1, 1, (8, n))
+    S = Solver(A).ksp_settype("cgm").ksp_setoption(1e-12, 3000).pc_settype("ilu0")
+    X = S.solve_batch(B)
+    G = X - XS
+    DB, DA = S.adjoint_batch(X, G)
+    rows = np.repeat(np.arange(n), np.diff(A.rowptr))
+    for k in range(8):
+        # recurrence residuals at 1e-12; the true residuals may sit a little above
+        assert np.linalg.norm(B[k] - Asp @ X[k]) / np.linalg.norm(B[k]) < 1e-10
+        assert np.linalg.norm(G[k] - Asp.T @ DB[k]) / np.linalg.norm(G[k]) < 1e-10
+        assert np.allclose(DA[k], -DB[k][rows] * X[k][A.colidx], rtol=1e-14, atol=0.0)
+
+    # central finite differences, h = 1e-6, for the first right-hand side
+    h = 1e-6
+    x, xs, lam, dA = X[0], XS[0], DB[0], DA[0]
+    P = _probe_solver(A)
+
+    def dL(dp, dm):
+        return np.dot(dp - dm, x - xs + 0.5 * (dp + dm)) / (2 * h)
+
+    fd_b, ad_b = [], []
+    for i in rng.choice(n, 64, replace=False):
+        e = np.zeros(n)
+        e[i] = h
+        fd_b.append(dL(P.solve(e), P.solve(-e)))
+        ad_b.append(lam[i])
+    fd_a, ad_a = [], []
+    vals = A.val.copy()
+    for k in rng.choice(A.nnz, 64, replace=False):
+        i, j = rows[k], A.colidx[k]
+        rhs = np.zeros(n)
+        rhs[i] = -h * x[j]
+        vals[k] = A.val[k] + h
+        P.mat_update(vals)
+        dp = P.solve(rhs)
+        vals[k] = A.val[k] - h
+        P.mat_update(vals)
+        dm = P.solve(-rhs)
+        vals[k] = A.val[k]
+        fd_a.append(dL(dp, dm))
+        ad_a.append(dA[k])
+    for fd, ad in ((np.array(fd_b), np.array(ad_b)), (np.array(fd_a), np.array(ad_a))):
+        floor = 1e-3 * np.max(np.abs(ad))
+        rel = np.abs(fd - ad) / np.maximum(np.abs(ad), floor)
+        assert rel.max() < 1e-6, (rel.max(), int(rel.argmax()))

@@ -154,3 +154,35 @@ def test_autograd_function(cuda):
     gA = Ad.grad.numpy()[rows, A.colidx]
     assert np.allclose(b.grad.numpy(), bd.grad.numpy(), rtol=1e-8, atol=1e-12)
     assert np.allclose(vals.grad.numpy(), gA, rtol=1e-8, atol=1e-12)
+
+
+def test_unsorted_input_keeps_caller_entry_order(cuda):
+    """Rows given with unsorted columns: the solve equals the sorted input's,
+    dL/dA comes back in the caller's entry order, and xs_mat_update takes
+    values in that order too."""
+    from xsolver_b200.api import Solver
+
+    A = st.convdiff3d_27pt(7)
+    n = A.n
+    rng = np.random.default_rng(5)
+    perm = np.concatenate([A.rowptr[i] + rng.permutation(A.rowptr[i + 1] - A.rowptr[i]) for i in range(n)])
+    U = st.CSRMatrix(n, A.rowptr.copy(), A.colidx[perm].copy(), A.val[perm].copy(), "unsorted")
+    b = st.rhs_uniform(n, 4, 0.0, 1.0)
+    g = st.rhs_uniform(n, 5)
+
+    def run(M):
+        S = Solver(M).ksp_settype("gmres").ksp_setoption(1e-12, 2000, 30).pc_settype("ilu0")
+        x = S.solve(b)
+        db, da = S.adjoint(g)
+        v2 = M.val * 1.5  # scaled values in the matrix's own entry order
+        S.mat_update(v2)
+        x2 = S.solve(b)
+        return x, db, da, x2
+
+    xs, dbs, das, x2s = run(A)
+    xu, dbu, dau, x2u = run(U)
+    assert np.array_equal(xs, xu)
+    assert np.array_equal(dbs, dbu)
+    assert np.array_equal(das[perm], dau)
+    assert np.array_equal(x2s, x2u)
+    assert np.allclose(x2s, xs / 1.5, rtol=1e-9, atol=1e-12)

@@ -51,6 +51,7 @@ def _declare(L):
         "xs_create": [C.POINTER(C.c_void_p)],
         "xs_destroy": [C.c_void_p],
         "xs_mat_setup": [C.c_void_p, C.c_int, _ip, _ip, _dp, C.c_int],
+        "xs_mat_update": [C.c_void_p, _dp],
         "xs_ksp_settype": [C.c_void_p, C.c_char_p],
         "xs_ksp_setoption": [C.c_void_p, C.c_double, C.c_int, _ip, _dp, C.c_int],
         "xs_ksp_set_absolute_tol": [C.c_void_p, C.c_double],
@@ -91,6 +92,7 @@ def _declare(L):
         "xs_device_count": [],
         "xs_tri_levels": [C.c_int, _ip, _ip, C.c_int, _ip, _ip, _ip],
         "xs_set_trsv_tuning": [C.c_int, C.c_int, C.c_int],
+        "xs_set_ell_index_bits": [C.c_int],
         "xs_lusolve_noalloc": [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         "xsolver_last_error": [],
     }

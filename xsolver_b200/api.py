@@ -52,6 +52,12 @@ class Solver:
         self._resvec = None
         self.maxiter = 0
 
+    def mat_update(self, val):
+        """New values for the same pattern (caller entry order)."""
+        self._v = np.ascontiguousarray(val, dtype=np.float64)
+        check(self._L.xs_mat_update(self.h, _d(self._v)), "xs_mat_update")
+        return self
+
     def close(self):
         if self.h:
             self._L.xs_destroy(self.h)

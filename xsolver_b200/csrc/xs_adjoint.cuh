@@ -48,6 +48,7 @@ struct AdjointState {
     bool have_Mt = false;
     int Mt_type = -1;
     DBuf<double> lam, rhs, grad_tmp;
+    DBuf<double> gb, gA;  // gradient staging, kept across calls
     RunSet<double> runs;
     // forget the transposed operator/preconditioner (matrix or values changed)
     void reset()

@@ -44,6 +44,17 @@ Geom &geom()
     return g;
 }
 
+FormatTuning &format_tuning()
+{
+    static FormatTuning t;
+    static bool init = false;
+    if (!init) {
+        if (const char *e = getenv("XS_ELL_INDEX16")) t.ell_index16 = atoi(e) != 0;
+        init = true;
+    }
+    return t;
+}
+
 TrsvTuning &trsv_tuning()
 {
     static TrsvTuning t;
@@ -112,6 +123,10 @@ void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const doub
     int n = op.n, w = 0;
     for (int i = 0; i < n; i++) w = std::max(w, rp0[i + 1] - rp0[i]);
     op.ell_w = w;
+    long maxoff = 0;
+    for (int i = 0; i < n; i++)
+        for (int q = rp0[i]; q < rp0[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci0[q] - i));
+    op.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
     std::vector<int> c((size_t)w * n);
     std::vector<double> vv((size_t)w * n);
     for (int i = 0; i < n; i++) {
@@ -125,8 +140,18 @@ void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const doub
             vv[(size_t)k * n + i] = 0.0;
         }
     }
-    op.eci.alloc((size_t)w * n);
-    op.eci.upload(c.data(), (size_t)w * n, s);
+    if (op.ell16) {
+        std::vector<short> o((size_t)w * n);
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < w; k++) o[(size_t)k * n + i] = (short)(c[(size_t)k * n + i] - i);
+        op.eco.alloc((size_t)w * n);
+        op.eco.upload(o.data(), (size_t)w * n, s);
+        op.eci.free();
+    } else {
+        op.eci.alloc((size_t)w * n);
+        op.eci.upload(c.data(), (size_t)w * n, s);
+        op.eco.free();
+    }
     op.ev.alloc((size_t)w * n);
     op.ev.upload(vv.data(), (size_t)w * n, s);
     if (want32) {
@@ -134,7 +159,7 @@ void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const doub
         k_convert_f32<<<geom().sms * 4, 256, 0, s>>>((long)w * n, op.ev.p, op.ev32.p);
         check_launch();
     }
-    op.ell_grid = std::min(geom().sms * 8, (n + 255) / 256);
+    op.ell_grid = std::min(geom().sms * ELL_BLOCKS_PER_SM, (n + 255) / 256);
     if (op.ell_grid < 1) op.ell_grid = 1;
     XS_CUDA(cudaStreamSynchronize(s));
 }
@@ -147,6 +172,9 @@ struct Handle {
     long nnz = 0;
     std::vector<int> hrp, hci;  // 0-based host copy
     std::vector<double> hv;
+    // caller entry of each stored entry when set_matrix had to sort a row's
+    // columns (empty: stored order = caller order)
+    std::vector<long> vperm;
     Operator A;
     bool have_matrix = false;
     int format = 0;
@@ -237,6 +265,7 @@ static void set_matrix(Handle &h, int n, const int *rp, const int *ci, const dou
     if (nnz < 0 || nnz > 0x7fffffffL - 16) throw Status(XS_ERR_INVALID);
     h.n = n;
     h.nnz = nnz;
+    h.vperm.clear();
     h.hrp.resize(n + 1);
     h.hci.resize(nnz);
     h.hv.assign(v, v + nnz);
@@ -254,10 +283,18 @@ static void set_matrix(Handle &h, int n, const int *rp, const int *ci, const dou
         for (int k = h.hrp[i] + 1; k < h.hrp[i + 1]; k++)
             if (h.hci[k] <= h.hci[k - 1]) { sorted = false; break; }
         if (!sorted) {
-            std::vector<std::pair<int, double>> e;
-            for (int k = h.hrp[i]; k < h.hrp[i + 1]; k++) e.emplace_back(h.hci[k], h.hv[k]);
+            if (h.vperm.empty()) {
+                h.vperm.resize(nnz);
+                for (long k = 0; k < nnz; k++) h.vperm[k] = k;
+            }
+            std::vector<std::pair<int, long>> e;
+            for (int k = h.hrp[i]; k < h.hrp[i + 1]; k++) e.emplace_back(h.hci[k], (long)k);
             std::sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.first < b.first; });
-            for (size_t q = 0; q < e.size(); q++) { h.hci[h.hrp[i] + q] = e[q].first; h.hv[h.hrp[i] + q] = e[q].second; }
+            for (size_t q = 0; q < e.size(); q++) {
+                h.hci[h.hrp[i] + q] = e[q].first;
+                h.hv[h.hrp[i] + q] = v[e[q].second];
+                h.vperm[h.hrp[i] + q] = e[q].second;
+            }
         }
     }
     h.A = Operator();
@@ -276,7 +313,10 @@ static void set_matrix(Handle &h, int n, const int *rp, const int *ci, const dou
 static void update_values(Handle &h, const double *v)
 {
     if (!h.have_matrix) throw Status(XS_ERR_ORDER);
-    h.hv.assign(v, v + h.nnz);
+    if (!v) throw Status(XS_ERR_INVALID);
+    if (h.vperm.empty()) h.hv.assign(v, v + h.nnz);
+    else
+        for (long k = 0; k < h.nnz; k++) h.hv[k] = v[h.vperm[k]];
     h.A.v.upload(h.hv.data(), h.nnz, h.s);
     if (h.A.v32.p) {
         k_convert_f32<<<geom().sms * 4, 256, 0, h.s>>>(h.nnz, h.A.v.p, h.A.v32.p);
@@ -564,6 +604,9 @@ struct EpiOuterResid {
     }
 };
 
+// safety factor of the adaptive inner tolerance of the refinement
+constexpr double INNER_SAFETY = 0.25;
+
 // Solve with device vectors b (rhs) and x (x0 in, solution out), FP64.
 // Writes the conventions requested by the caller into usediter/resvec.
 static void solve_device(Handle &h, const double *d_b, double *d_x)
@@ -639,7 +682,13 @@ static void solve_device(Handle &h, const double *d_b, double *d_x)
             XS_CUDA(cudaMemsetAsync(d32, 0, sizeof(float) * n, h.s));
             check_launch();
             int inner_max = std::min(h.inner_maxiter, h.maxiter - iters);
-            prepare_state(h, inner_max, h.inner_rtol, 0.0, true);
+            // the inner tolerance is loosened (never tightened) to what the
+            // outer target still needs, with a safety factor: the last step
+            // does not overshoot the target by orders of magnitude
+            const double target = std::max(h.tol * (r0 + KSMALL), h.abstol);
+            const double need = INNER_SAFETY * target / rn;
+            const double irtol = std::min(std::max(h.inner_rtol, need), 0.5);
+            prepare_state(h, inner_max, irtol, 0.0, true);
             run_method<float>(h, h.method, r32, d32, restart);
             XS_CUDA(cudaMemcpyAsync(h.W.h_st, h.W.st.p, sizeof(KState), cudaMemcpyDeviceToHost, h.s));
             XS_CUDA(cudaStreamSynchronize(h.s));
@@ -830,13 +879,27 @@ static void adjoint_solve(Handle &h, const double *dLdx, double *dLdb, double *d
     run_method_on<double>(a.runs, a.At, a.Mt, h.W, h.s, n, 0, method, a.rhs.p, a.lam.p, effective_restart(h));
     // gradients
     double *db = nullptr, *dA = nullptr;
-    DBuf<double> gb, gA;
-    if (dLdb) { gb.alloc(n); db = gb.p; }
-    if (dLdA) { gA.alloc(std::max<long>(h.nnz, 1)); dA = gA.p; }
+    DBuf<double> &gb = a.gb, &gA = a.gA;
+    if (dLdb) {
+        if (gb.n != (size_t)n) gb.alloc(n);
+        db = gb.p;
+    }
+    if (dLdA) {
+        if (gA.n != (size_t)std::max<long>(h.nnz, 1)) gA.alloc(std::max<long>(h.nnz, 1));
+        dA = gA.p;
+    }
     k_adjoint_grad<<<geom().sms * 4, 256, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, a.lam.p, a.x_last.p, db, dA);
     check_launch();
     if (dLdb) gb.download(dLdb, n, h.s);
-    if (dLdA) gA.download(dLdA, h.nnz, h.s);
+    if (dLdA) {
+        if (h.vperm.empty()) gA.download(dLdA, h.nnz, h.s);
+        else {
+            std::vector<double> t(h.nnz);
+            gA.download(t.data(), h.nnz, h.s);
+            XS_CUDA(cudaStreamSynchronize(h.s));
+            for (long k = 0; k < h.nnz; k++) dLdA[h.vperm[k]] = t[k];
+        }
+    }
     XS_CUDA(cudaStreamSynchronize(h.s));
     int e = read_dev_err(h) | h.W.h_st->err;
     XS_CUDA(cudaMemcpyAsync(h.W.h_st, h.W.st.p, sizeof(KState), cudaMemcpyDeviceToHost, h.s));
@@ -939,6 +1002,14 @@ static int check_gpu()
 extern "C" {
 
 const char *xs_version(void) { return "xsolver_b200 1.0 (sm_100a)"; }
+
+int xs_set_ell_index_bits(int bits)
+{
+    return guarded([&] {
+        if (bits != 16 && bits != 32) throw Status(XS_ERR_INVALID);
+        format_tuning().ell_index16 = bits == 16;
+    });
+}
 
 int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows)
 {
@@ -1152,6 +1223,13 @@ int xs_solve_batch(xs_handle_t h, int nrhs, const double *rhs, double *sol)
         if (nrhs < 0 || (nrhs > 0 && (!rhs || !sol))) throw Status(XS_ERR_INVALID);
         Handle &H = *h->h;
         for (int k = 0; k < nrhs; k++) solve_host(H, rhs + (size_t)k * H.n, sol + (size_t)k * H.n);
+    });
+}
+int xs_mat_update(xs_handle_t h, const double *val)
+{
+    return guarded([&] {
+        if (!h) throw Status(XS_ERR_INVALID);
+        update_values(*h->h, val);
     });
 }
 int xs_adjoint(xs_handle_t h, const double *dLdx, double *dLdb, double *dLdA)

@@ -225,11 +225,11 @@ struct FVal<float> {
 };
 template <>
 struct FVal<__nv_bfloat16> {
-    __device__ static float ld(const __nv_bfloat16 *p, long i) { return __bfloat162float(p[i]); }
+    __device__ static float ld(const __nv_bfloat16 *p, long i) { return __bfloat162float(__ldg(p + i)); }
 };
 template <>
 struct FVal<__half> {
-    __device__ static float ld(const __half *p, long i) { return __half2float(p[i]); }
+    __device__ static float ld(const __half *p, long i) { return __half2float(__ldg(p + i)); }
 };
 
 // ---------------------------------------------------------------- deterministic reductions

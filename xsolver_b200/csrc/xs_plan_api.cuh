@@ -282,9 +282,10 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
         const double I = 4.0;
         switch (op) {
         case 0: *bytes = (8 + I) * nnz + I * (n + 1) + 8 * n + 8 * n; break;
-        case 1: *bytes = (8 + I) * h.A.ell_w * n + 2 * 8 * n; break;
+        // ELL: stored entries (padding included) with the stored index width
+        case 1: *bytes = (8 + (h.A.ell16 ? 2.0 : I)) * h.A.ell_w * n + 2 * 8 * n; break;
         case 2: *bytes = (4 + I) * nnz + I * (n + 1) + 4 * n + 4 * n; break;
-        case 6: *bytes = (4 + I) * h.A.ell_w * n + 2 * 4 * n; break;
+        case 6: *bytes = (4 + (h.A.ell16 ? 2.0 : I)) * h.A.ell_w * n + 2 * 4 * n; break;
         case 3: case 4: case 5: {
             if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
             const int fp = h.M.factor_prec;
@@ -296,11 +297,17 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
                 const double l = (V + I) * h.M.L.nnz + I * (n + 1) + 2 * X * n;
                 const double u = (V + I) * h.M.U.nnz + I * (n + 1) + 3 * X * n;
                 *bytes = op == 3 ? l : (op == 4 ? u : l + u);
+            } else if (k <= 1) {
+                *bytes = 3 * X * n;  // z = dinv * x
             } else {
-                // k Jacobi sweeps = k-1 passes per triangle: entries, rhs, previous iterate, result (+ dinv for U)
-                const double passes = k > 1 ? k - 1 : 0;
-                const double l = passes * ((V + I) * h.M.L.nnz + 3 * X * n);
-                const double u = passes * ((V + I) * h.M.U.nnz + 4 * X * n) + (k <= 1 ? 3 * X * n : 0);
+                // k Jacobi sweeps = k-1 passes per triangle.  Each pass reads
+                // the triangle's entries (index width of the copy in use); the
+                // first pass reads x (L) or x and dinv (U) and writes its
+                // iterate, every later pass also reads the previous iterate.
+                const double IL = (h.M.L.ell_w > 0 && h.M.L.ell16) ? 2.0 : I;
+                const double IU = (h.M.U.ell_w > 0 && h.M.U.ell16) ? 2.0 : I;
+                const double l = (k - 1) * (V + IL) * h.M.L.nnz + 2 * X * n + (k - 2) * 3 * X * n;
+                const double u = (k - 1) * (V + IU) * h.M.U.nnz + 3 * X * n + (k - 2) * 4 * X * n;
                 *bytes = op == 3 ? l : (op == 4 ? u : l + u);
             }
             break;

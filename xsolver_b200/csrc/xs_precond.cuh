@@ -159,19 +159,24 @@ struct PrecondDev {
         const DT *dinv;
         if constexpr (std::is_same<VT, double>::value) { ta = tmp64a.p; tb = tmp64b.p; tc = tmp64c.p; dinv = U.dinv64_nat.p; }
         else { ta = tmp32a.p; tb = tmp32b.p; tc = tmp32c.p; dinv = U.dinv32_nat.p; }
-        const int g = geom().sms * 8;
+        const int g = std::min(geom().sms * ELL_BLOCKS_PER_SM, (n + 255) / 256);
         const int k = trsv_mode;
         // one sweep pass over triangle T: ELL when available, else CSR
         auto pass = [&](const TriDev &T, bool upper, bool first2, const VT *rhs, const VT *yin, VT *yout) {
             if (T.ell_w > 0) {
                 const FT *ev = T.evals<FT>();
-                if (upper) {
-                    if (first2) k_trsv_sweep_ell<VT, FT, DT, true, true><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, dinv, rhs, yin, yout, done_flag);
-                    else k_trsv_sweep_ell<VT, FT, DT, true, false><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, dinv, rhs, yin, yout, done_flag);
-                } else {
-                    if (first2) k_trsv_sweep_ell<VT, FT, DT, false, true><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
-                    else k_trsv_sweep_ell<VT, FT, DT, false, false><<<g, 256, 0, s>>>(n, T.ell_w, T.eci, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
-                }
+                auto go = [&](auto cols) {
+                    using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
+                    if (upper) {
+                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, true, true><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, dinv, rhs, yin, yout, done_flag);
+                        else k_trsv_sweep_ell<VT, FT, DT, CT, true, false><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, dinv, rhs, yin, yout, done_flag);
+                    } else {
+                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, false, true><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
+                        else k_trsv_sweep_ell<VT, FT, DT, CT, false, false><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
+                    }
+                };
+                if (T.ell16) go((const short *)T.eco.p);
+                else go((const int *)T.eci.p);
             } else {
                 // CSR: the first sweep is a separate pass (yin = null -> y_1)
                 if (first2) {

@@ -116,6 +116,8 @@ struct CsrTileArgs {
     int *err;
 };
 
+constexpr int CSR_CH = 8;  // entries per gather chunk
+
 template <typename VT, typename MT, typename Epi>
 __global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const VT *__restrict__ x, VT *__restrict__ y,
                                                         Epi epi, RedSlot slot)
@@ -182,17 +184,17 @@ __global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const
                 const MT *vv = vbuf[s];
                 const int *cc = cbuf[s];
                 double sum = 0.0;
-                int k = k0;
-                for (; k + 4 <= k1; k += 4) {
-                    const int c0 = cc[k], c1 = cc[k + 1], c2 = cc[k + 2], c3 = cc[k + 3];
-                    const double x0 = (double)__ldg(x + c0), x1 = (double)__ldg(x + c1);
-                    const double x2 = (double)__ldg(x + c2), x3 = (double)__ldg(x + c3);
-                    sum += (double)vv[k] * x0;
-                    sum += (double)vv[k + 1] * x1;
-                    sum += (double)vv[k + 2] * x2;
-                    sum += (double)vv[k + 3] * x3;
+                // chunks of CSR_CH entries: every gather of x in a chunk is
+                // issued before the chunk's (in-order) sum
+                for (int kb = k0; kb < k1; kb += CSR_CH) {
+                    double xv[CSR_CH];
+#pragma unroll
+                    for (int j = 0; j < CSR_CH; j++)
+                        if (kb + j < k1) xv[j] = (double)__ldg(x + cc[kb + j]);
+#pragma unroll
+                    for (int j = 0; j < CSR_CH; j++)
+                        if (kb + j < k1) sum += (double)vv[kb + j] * xv[j];
                 }
-                for (; k < k1; k++) sum += (double)vv[k] * (double)__ldg(x + cc[k]);
                 VT o = epi.out(r, sum);
                 y[r] = o;
                 if (Epi::K > 0) epi.acc(r, (double)o, acc);
@@ -224,16 +226,84 @@ __global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const
 }
 
 // ---------------------------------------------------------------- ELL kernel
-template <typename MT>
+constexpr int ELL_CH = 8;  // entries per load chunk
+// Column storage of an ELL copy: CT = int holds absolute columns, CT = short
+// holds the offset c - row (used when every |c - row| <= 32767, as for
+// stencil and other banded matrices: 2 index bytes per entry instead of 4).
+template <typename CT>
+__device__ __forceinline__ int ell_col(CT c, int row)
+{
+    if constexpr (sizeof(CT) == 2) return row + (int)c;
+    else return (int)c;
+}
+
+template <typename MT, typename CT>
 struct EllArgs {
     int n, w;
-    const int *ci;
+    const CT *ci;
     const MT *v;
 };
 
-template <typename VT, typename MT, typename Epi>
-__global__ void __launch_bounds__(256) k_ell_spmv(EllArgs<MT> A, const VT *__restrict__ x, VT *__restrict__ y, Epi epi,
-                                                  RedSlot slot)
+// Launch shape of the ELL kernels (SpMV and the Jacobi-sweep triangle
+// kernels): CTAs of 256 threads, ELL_MIN_BLOCKS of them resident per SM
+// (register cap 65536 / (256 * ELL_MIN_BLOCKS)), ELL_BLOCKS_PER_SM per SM in
+// the grid, rows grid-strided.
+#ifndef XS_ELL_MIN_BLOCKS
+#define XS_ELL_MIN_BLOCKS 4
+#endif
+#ifndef XS_ELL_BLOCKS_PER_SM
+#define XS_ELL_BLOCKS_PER_SM 8
+#endif
+constexpr int ELL_MIN_BLOCKS = XS_ELL_MIN_BLOCKS;
+constexpr int ELL_BLOCKS_PER_SM = XS_ELL_BLOCKS_PER_SM;
+
+// C consecutive ELL entries of row r (C known at compile time): all column
+// and value loads first, then all gathers of x, then the in-order sum.
+template <int C, typename VT, typename MT, typename CT>
+__device__ __forceinline__ double ell_chunk(const CT *&cp, const MT *&vp, long n, const VT *__restrict__ x, int r,
+                                            double sum)
+{
+    int c[C];
+    MT v[C];
+    VT xv[C];
+#pragma unroll
+    for (int j = 0; j < C; j++) {
+        c[j] = ell_col<CT>(__ldg(cp), r);
+        v[j] = __ldg(vp);
+        cp += n;
+        vp += n;
+    }
+#pragma unroll
+    for (int j = 0; j < C; j++) xv[j] = __ldg(x + c[j]);
+#pragma unroll
+    for (int j = 0; j < C; j++) sum += (double)v[j] * (double)xv[j];
+    return sum;
+}
+
+// sum over the w entries of row r in entry order, in chunks of up to 8
+// (the chunk length is warp-uniform, so the switch does not diverge)
+template <typename VT, typename MT, typename CT>
+__device__ __forceinline__ double ell_row(const CT *cp, const MT *vp, int w, long n, const VT *__restrict__ x, int r)
+{
+    double sum = 0.0;
+    for (int k0 = 0; k0 < w; k0 += ELL_CH) {
+        switch (min(ELL_CH, w - k0)) {
+        case 8: sum = ell_chunk<8>(cp, vp, n, x, r, sum); break;
+        case 7: sum = ell_chunk<7>(cp, vp, n, x, r, sum); break;
+        case 6: sum = ell_chunk<6>(cp, vp, n, x, r, sum); break;
+        case 5: sum = ell_chunk<5>(cp, vp, n, x, r, sum); break;
+        case 4: sum = ell_chunk<4>(cp, vp, n, x, r, sum); break;
+        case 3: sum = ell_chunk<3>(cp, vp, n, x, r, sum); break;
+        case 2: sum = ell_chunk<2>(cp, vp, n, x, r, sum); break;
+        default: sum = ell_chunk<1>(cp, vp, n, x, r, sum); break;
+        }
+    }
+    return sum;
+}
+
+template <typename VT, typename MT, typename CT, typename Epi>
+__global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_ell_spmv(EllArgs<MT, CT> A, const VT *__restrict__ x,
+                                                                   VT *__restrict__ y, Epi epi, RedSlot slot)
 {
     constexpr int KK = Epi::K > 0 ? Epi::K : 1;
     if (!epi.active()) return;
@@ -243,24 +313,7 @@ __global__ void __launch_bounds__(256) k_ell_spmv(EllArgs<MT> A, const VT *__res
     for (int k = 0; k < KK; k++) acc[k] = 0.0;
     const int n = A.n;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        double sum = 0.0;
-        const int *cp = A.ci + r;
-        const MT *vp = A.v + r;
-        int k = 0;
-        for (; k + 4 <= A.w; k += 4) {
-            const long o0 = (long)k * n, o1 = o0 + n, o2 = o1 + n, o3 = o2 + n;
-            const int c0 = __ldg(cp + o0), c1 = __ldg(cp + o1), c2 = __ldg(cp + o2), c3 = __ldg(cp + o3);
-            const double v0 = (double)__ldg(vp + o0), v1 = (double)__ldg(vp + o1);
-            const double v2 = (double)__ldg(vp + o2), v3 = (double)__ldg(vp + o3);
-            sum += v0 * (double)__ldg(x + c0);
-            sum += v1 * (double)__ldg(x + c1);
-            sum += v2 * (double)__ldg(x + c2);
-            sum += v3 * (double)__ldg(x + c3);
-        }
-        for (; k < A.w; k++) {
-            const long o = (long)k * n;
-            sum += (double)__ldg(vp + o) * (double)__ldg(x + __ldg(cp + o));
-        }
+        const double sum = ell_row<VT, MT, CT>(A.ci + r, A.v + r, A.w, (long)n, x, r);
         VT o = epi.out(r, sum);
         y[r] = o;
         if (Epi::K > 0) epi.acc(r, (double)o, acc);
@@ -284,9 +337,11 @@ struct Operator {
     DBuf<float> v32;
     SpmvTiling tile64, tile32;
     int grid64 = 0, grid32 = 0;  // persistent grid sizes
-    // ELL
+    // ELL (columns in eci, or as 16-bit row offsets in eco when ell16)
     int ell_w = 0;
+    bool ell16 = false;
     DBuf<int> eci;
+    DBuf<short> eco;
     DBuf<double> ev;
     DBuf<float> ev32;
     int ell_grid = 0;
@@ -300,8 +355,15 @@ struct Operator {
     {
         return CsrTileArgs<float>{n, rp.p, ci.p, v32.p, tile32.rb.p, tile32.longrow.p, tile32.nblocks, tile32.cap, err};
     }
-    EllArgs<double> ell64() const { return EllArgs<double>{n, ell_w, eci.p, ev.p}; }
-    EllArgs<float> ell32() const { return EllArgs<float>{n, ell_w, eci.p, ev32.p}; }
+    template <typename MT, typename CT>
+    EllArgs<MT, CT> ell() const
+    {
+        const MT *vals;
+        if constexpr (std::is_same<MT, double>::value) vals = ev.p;
+        else vals = ev32.p;
+        if constexpr (sizeof(CT) == 2) return EllArgs<MT, CT>{n, ell_w, eco.p, vals};
+        else return EllArgs<MT, CT>{n, ell_w, eci.p, vals};
+    }
 };
 
 // Cut rows into blocks: at most max_rows rows, and the 4-aligned entry range
@@ -405,11 +467,9 @@ inline void launch_csr(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot 
 template <typename VT, typename MT, typename Epi>
 inline void launch_ell(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot slot, cudaStream_t s)
 {
-    EllArgs<MT> a;
-    if constexpr (std::is_same<MT, double>::value) a = op.ell64();
-    else a = op.ell32();
     int g = op.ell_grid;
-    k_ell_spmv<VT, MT, Epi><<<g, 256, 0, s>>>(a, x, y, epi, slot);
+    if (op.ell16) k_ell_spmv<VT, MT, short, Epi><<<g, 256, 0, s>>>(op.ell<MT, short>(), x, y, epi, slot);
+    else k_ell_spmv<VT, MT, int, Epi><<<g, 256, 0, s>>>(op.ell<MT, int>(), x, y, epi, slot);
     check_launch();
 }
 

@@ -31,6 +31,7 @@
 #include <vector>
 #include <algorithm>
 #include "xs_internal.cuh"
+#include "xs_spmv.cuh"  // ELL column storage and launch shape
 
 namespace xs {
 
@@ -61,6 +62,13 @@ __device__ __forceinline__ float msub(float acc, float y, float v) { return __fm
 //                  no persistence)
 //   backoff_ns     upper bound of the exponential back-off between polls of a
 //                  pending dependency (0: spin without sleeping)
+// ELL column storage: 1 = 16-bit row offsets whenever they fit (default),
+// 0 = always 32-bit columns.  Applies to ELL copies built afterwards.
+struct FormatTuning {
+    int ell_index16 = 1;
+};
+FormatTuning &format_tuning();
+
 struct TrsvTuning {
     int blocks_per_sm = 2;
     int backoff_ns = 128;
@@ -349,27 +357,61 @@ __global__ void k_trsv_sweep(int n, const int *__restrict__ rp, const int *__res
     }
 }
 
+// C consecutive entries of row i of a sweep pass: acc -= v * y(c), with
+// y(c) = x[c] (L, first pass), dinv[c]*x[c] (U, first pass) or yin[c].
+template <int C, typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
+__device__ __forceinline__ VT sweep_chunk(const CT *&cp, const FT *&vp, long n, int i, const DT *__restrict__ dinv,
+                                          const VT *__restrict__ x, const VT *__restrict__ yin, VT acc)
+{
+    int c[C];
+    VT v[C], y[C];
+#pragma unroll
+    for (int j = 0; j < C; j++) {
+        c[j] = ell_col<CT>(__ldg(cp), i);
+        v[j] = (VT)FVal<FT>::ld(vp, 0);
+        cp += n;
+        vp += n;
+    }
+#pragma unroll
+    for (int j = 0; j < C; j++) {
+        if (FIRST2) y[j] = UPPER ? (VT)(__ldg(x + c[j]) * (VT)__ldg(dinv + c[j])) : __ldg(x + c[j]);
+        else y[j] = __ldg(yin + c[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < C; j++) acc = msub(acc, y[j], v[j]);
+    return acc;
+}
+
 // Jacobi sweeps on a column-major ELL copy of the triangle (natural order,
 // padding column = the row itself with value 0): every load is coalesced.
 // FIRST2 folds the first sweep into the second: the previous iterate of the
 // first sweep is x itself (L) or dinv*x (U), so k sweeps cost k-1 passes.
-template <typename VT, typename FT, typename DT, bool UPPER, bool FIRST2>
-__global__ void __launch_bounds__(256) k_trsv_sweep_ell(int n, int w, const int *__restrict__ eci,
-                                                       const FT *__restrict__ ev, const DT *__restrict__ dinv,
-                                                       const VT *__restrict__ x, const VT *__restrict__ yin,
-                                                       VT *__restrict__ yout, const int *done_flag)
+// Entries go in chunks of up to 8 of compile-time length (the switch is
+// warp-uniform): loads of a chunk are issued before its gathers.
+template <typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
+__global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, int w, const CT *__restrict__ eci,
+                                                                         const FT *__restrict__ ev,
+                                                                         const DT *__restrict__ dinv,
+                                                                         const VT *__restrict__ x,
+                                                                         const VT *__restrict__ yin,
+                                                                         VT *__restrict__ yout, const int *done_flag)
 {
     if (done_flag && *done_flag) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         VT acc = UPPER ? (VT)(x[i] * (VT)dinv[i]) : x[i];
-        for (int k = 0; k < w; k++) {
-            const long o = (long)k * n + i;
-            const int c = __ldg(eci + o);
-            const VT v = (VT)FVal<FT>::ld(ev, o);
-            VT y;
-            if (FIRST2) y = UPPER ? (VT)(x[c] * (VT)dinv[c]) : x[c];
-            else y = yin[c];
-            acc = msub(acc, y, v);
+        const CT *cp = eci + i;
+        const FT *vp = ev + i;
+        for (int k0 = 0; k0 < w; k0 += ELL_CH) {
+            switch (min(ELL_CH, w - k0)) {
+            case 8: acc = sweep_chunk<8, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            case 7: acc = sweep_chunk<7, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            case 6: acc = sweep_chunk<6, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            case 5: acc = sweep_chunk<5, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            case 4: acc = sweep_chunk<4, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            case 3: acc = sweep_chunk<3, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            case 2: acc = sweep_chunk<2, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            default: acc = sweep_chunk<1, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
+            }
         }
         yout[i] = acc;
     }
@@ -427,12 +469,17 @@ inline void tri_analyse(int n, const int *rp, const int *ci, bool upper, SrcF sr
         }
     }
     h.nlevels = n > 0 ? maxl + 1 : 0;
-    // counting sort by level, rows ascending within a level
+    // counting sort by level; inside a level rows follow the solve direction
+    // (L ascending, U descending), so the first rows of a level depend on the
+    // first rows of the level before and can start while its tail still runs
     std::vector<int> cnt(h.nlevels + 1, 0);
     for (int i = 0; i < n; i++) cnt[h.level[i] + 1]++;
     for (int l = 0; l < h.nlevels; l++) cnt[l + 1] += cnt[l];
     h.perm.assign(n, 0);
-    for (int i = 0; i < n; i++) h.perm[cnt[h.level[i]]++] = i;
+    if (!upper)
+        for (int i = 0; i < n; i++) h.perm[cnt[h.level[i]]++] = i;
+    else
+        for (int i = n - 1; i >= 0; i--) h.perm[cnt[h.level[i]]++] = i;
     h.prp.assign(n + 1, 0);
     for (int p = 0; p < n; p++) {
         int r = h.perm[p];
@@ -549,7 +596,9 @@ struct TriDev {
     DBuf<unsigned> ticket;
     // natural-order ELL copy for the Jacobi-sweep mode (ell_w = 0: none)
     int ell_w = 0;
+    bool ell16 = false;  // columns as 16-bit row offsets in eco
     DBuf<int> eci;
+    DBuf<short> eco;
     DBuf<long> esrc;
     DBuf<double> ev64;
     DBuf<float> ev32;
@@ -685,7 +734,20 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
             }
         }
         T.ell_w = w;
-        T.eci.alloc((size_t)w * n); T.eci.upload(ec.data(), (size_t)w * n, s);
+        long maxoff = 0;
+        for (int i = 0; i < n; i++)
+            for (int q = rp[i]; q < rp[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci[q] - i));
+        T.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
+        if (T.ell16) {
+            std::vector<short> eo((size_t)w * n);
+            for (int i = 0; i < n; i++)
+                for (int k = 0; k < w; k++) eo[(size_t)k * n + i] = (short)(ec[(size_t)k * n + i] - i);
+            T.eco.alloc((size_t)w * n); T.eco.upload(eo.data(), (size_t)w * n, s);
+            T.eci.free();
+        } else {
+            T.eci.alloc((size_t)w * n); T.eci.upload(ec.data(), (size_t)w * n, s);
+            T.eco.free();
+        }
         T.esrc.alloc((size_t)w * n); T.esrc.upload(es.data(), (size_t)w * n, s);
     }
     T.ticket.alloc(1);
