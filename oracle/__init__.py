@@ -218,12 +218,14 @@ def levels_lower(n, rp, ci):
 PC = {"none": 0, "jacobi": 1, "lu": 2}
 
 
-DOT_MODES = {"sequential": 0, "pairwise": 1, "reverse": 2, "simd8": 3, "blocked": 4}
+DOT_MODES = {"sequential": 0, "pairwise": 1, "reverse": 2, "simd8": 3, "blocked": 4, "simd4": 5, "blocked256": 6,
+             "strided4096": 7, "strided151552": 8}
 
 
 def set_dot_mode(mode: str):
     """'sequential' (the reference's order) or another valid summation order:
-    'pairwise', 'reverse', 'simd8', 'blocked'."""
+    'pairwise', 'reverse', 'simd8', 'blocked', 'simd4', 'blocked256',
+    'strided4096', 'strided151552'."""
     lib().orc_set_dot_mode(DOT_MODES[mode])
 
 

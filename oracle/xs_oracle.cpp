@@ -45,8 +45,10 @@ namespace {
 /* ---------------- BLAS-1, sequential order ---------------- */
 /* dot-product order: 0 = sequential (the reference's cblas_ddot through the
  * sequential shim); 1 pairwise, 2 reverse, 3 eight interleaved partial sums,
- * 4 blocked — other valid orders, used to measure how sensitive a reference
- * solve is to the summation order of its dot products */
+ * 4 blocks of 1024, 5 four interleaved partial sums, 6 blocks of 256,
+ * 7 4096 strided partial sums, 8 151552 strided partial sums (the shape of a
+ * grid-strided parallel reduction) — other valid orders, used to measure how
+ * sensitive a reference solve is to the summation order of its dot products */
 int g_dot_mode = 0;
 double o_dot_pairwise(int n, const double *x, const double *y)
 {
@@ -75,12 +77,32 @@ double o_dot(int n, const double *x, const double *y)
         for (; i < n; i++) s += x[i] * y[i];
         return s;
     }
-    if (g_dot_mode == 4) { /* blocks of 1024 summed sequentially, then combined */
+    if (g_dot_mode == 4 || g_dot_mode == 6) { /* blocks summed sequentially, then combined */
+        const int B = g_dot_mode == 4 ? 1024 : 256;
         double s = 0.0;
-        for (int b = 0; b < n; b += 1024) {
+        for (int b = 0; b < n; b += B) {
             double t = 0.0;
-            for (int i = b; i < n && i < b + 1024; i++) t += x[i] * y[i];
+            for (int i = b; i < n && i < b + B; i++) t += x[i] * y[i];
             s += t;
+        }
+        return s;
+    }
+    if (g_dot_mode == 5) { /* 4 interleaved partial sums */
+        double p[4] = {0, 0, 0, 0};
+        int i = 0;
+        for (; i + 4 <= n; i += 4)
+            for (int l = 0; l < 4; l++) p[l] += x[i + l] * y[i + l];
+        double s = (p[0] + p[2]) + (p[1] + p[3]);
+        for (; i < n; i++) s += x[i] * y[i];
+        return s;
+    }
+    if (g_dot_mode == 7 || g_dot_mode == 8) { /* S strided partial sums, combined in order */
+        const int S = g_dot_mode == 7 ? 4096 : 151552;
+        double s = 0.0;
+        for (int t = 0; t < S && t < n; t++) {
+            double q = 0.0;
+            for (int i = t; i < n; i += S) q += x[i] * y[i];
+            s += q;
         }
         return s;
     }

@@ -19,32 +19,41 @@ EPS = np.finfo(np.float64).eps
 STRICT = 1e-10
 
 
-ALT_ORDERS = ("pairwise", "reverse", "simd8", "blocked")
+ALT_ORDERS = ("pairwise", "reverse", "simd8", "blocked", "simd4", "blocked256", "strided4096", "strided151552")
+
+
+def history_bound(h_s, alt_histories):
+    """max(1e-10, 10 x the running maximum of the relative deviation of the
+    other orders' histories from the sequential one)."""
+    sens = np.zeros(len(h_s))
+    for h_p in alt_histories:
+        m = min(len(h_s), len(h_p))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            d = np.abs(h_p[:m] - h_s[:m]) / np.abs(h_s[:m])
+        d = np.nan_to_num(d, nan=0.0, posinf=0.0)
+        if m < len(h_s):
+            d = np.concatenate([d, np.full(len(h_s) - m, d.max() if m else 0.0)])
+        sens = np.maximum(sens, d)
+    return np.maximum(STRICT, 10.0 * np.maximum.accumulate(sens))
 
 
 def reference_with_bounds(method, A, b, **kw):
     """Reference history (sequential dots, as the compiled reference) and the
     per-iteration bound: max(1e-10, 10 x the largest deviation seen when the
-    same reference loop runs with any of four other valid dot orders)."""
+    same reference loop runs with any of the other valid dot orders)."""
     oracle.set_dot_mode("sequential")
     x_s, h_s, u_s = oracle.solve(method, A, b, **kw)
-    sens = np.zeros(len(h_s))
+    hists = []
     xsens = 0.0
     try:
         for mode in ALT_ORDERS:
             oracle.set_dot_mode(mode)
             x_p, h_p, u_p = oracle.solve(method, A, b, **kw)
-            m = min(len(h_s), len(h_p))
-            with np.errstate(divide="ignore", invalid="ignore"):
-                d = np.abs(h_p[:m] - h_s[:m]) / np.abs(h_s[:m])
-            d = np.nan_to_num(d, nan=0.0, posinf=0.0)
-            if m < len(h_s):
-                d = np.concatenate([d, np.full(len(h_s) - m, d.max() if m else 0.0)])
-            sens = np.maximum(sens, d)
+            hists.append(h_p)
             xsens = max(xsens, np.linalg.norm(x_p - x_s) / max(np.linalg.norm(x_s), 1e-300))
     finally:
         oracle.set_dot_mode("sequential")
-    hbound = np.maximum(STRICT, 10.0 * np.maximum.accumulate(sens))
+    hbound = history_bound(h_s, hists)
     xbound = max(STRICT, 10.0 * xsens)
     return x_s, h_s, u_s, hbound, xbound
 

@@ -3,8 +3,11 @@
   * 3D 7-point Poisson 128^3 (n = 2,097,152), BiCGSTAB + ILU(0), rtol 1e-10,
     FP64 on the GPU (CSR and ELL) against the restated reference on the host:
     ILU(0) factors bit for bit, per-iteration residual history within the
-    calibrated bound of tests/parity.py, iteration count within +-1, final
-    solution within the same calibration.  The mixed-precision refinement
+    calibrated bound of tests/parity.py, final solution within the same
+    calibration.  At this size the reference's own iteration count moves
+    over a range of several iterations when only the summation order of its
+    dot products changes (tests/golden/c2_orders.npz, nine valid orders); the
+    GPU count must lie within that range widened by one.  The mixed-precision refinement
     (BF16 and FP16 factors) must reach 1e-10 and agree with the host FP64
     solve converged to 1e-14 to the conditioning bound.
   * Variable-coefficient 7-point diffusion 96^3 (n = 884,736), a batch of 8
@@ -22,14 +25,19 @@ is the central difference quotient itself, evaluated without the 1e-4
 rounding floor that subtracting two independently solved 884,736-vectors
 would put on it.
 """
+import os
+
 import numpy as np
 import pytest
 
 import oracle
-from parity import history_ok, reference_with_bounds
+from parity import history_bound, history_ok
 from xsolver_b200 import stencils as st
 
 pytestmark = pytest.mark.gpu
+
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
 @pytest.fixture(scope="module")
@@ -37,9 +45,15 @@ def c2():
     A = st.poisson3d_7pt(128)
     b = st.rhs_uniform(A.n, 0)
     F = oracle.ilu0(A)
-    ref = reference_with_bounds("bicgstab", A, b, tol=1e-10, maxiter=1000, pc="lu", factors=F)
+    xo, ho, uo = oracle.solve("bicgstab", A, b, tol=1e-10, maxiter=1000, pc="lu", factors=F)
+    z = np.load(os.path.join(GOLD, "c2_orders.npz"))
+    assert np.array_equal(z["sequential/hist"], ho) and int(z["sequential/usediter"]) == uo
+    orders = [str(o) for o in z["orders"]]
+    hb = history_bound(ho, [z[f"{o}/hist"] for o in orders if o != "sequential"])
+    its = [int(z[f"{o}/usediter"]) for o in orders]
+    xb = max(1e-10, 10.0 * float(z["xsens"]))
     x14, _, _ = oracle.solve("bicgstab", A, b, tol=1e-14, maxiter=2000, pc="lu", factors=F)
-    return A, b, F, ref, x14
+    return A, b, F, (xo, ho, (min(its), max(its)), hb, xb), x14
 
 
 def test_c2_ilu0_factors_bitwise(cuda, c2):
@@ -55,13 +69,14 @@ def test_c2_ilu0_factors_bitwise(cuda, c2):
 def test_c2_fp64_bicgstab_ilu0_vs_reference(cuda, c2, fmt):
     from xsolver_b200.api import Solver
 
-    A, b, F, (xo, ro, uo, hb, xb), _ = c2
+    A, b, F, (xo, ro, (umin, umax), hb, xb), _ = c2
     S = Solver(A, fmt=fmt).ksp_settype("bicgstab").ksp_setoption(1e-10, 1000).pc_settype("ilu0")
     x = S.solve(b)
     hist = S.resvec()
-    assert abs(S.usediter - (uo + 1)) <= 1, (S.usediter, uo + 1)
     ok, worst = history_ok(hist[1:] / hist[0], ro, hb)
     assert ok, worst
+    # usediter counts iterations (the oracle reports the last index)
+    assert umin + 1 - 1 <= S.usediter <= umax + 1 + 1, (S.usediter, umin + 1, umax + 1, worst)
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
     r = b - A.to_scipy() @ x
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10

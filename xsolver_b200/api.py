@@ -118,9 +118,16 @@ class Solver:
         return self
 
     # -- solve
-    def solve(self, b, x0=None) -> np.ndarray:
+    def solve(self, b, x0=None, out=None) -> np.ndarray:
+        """Host arrays.  out (float64, contiguous, e.g. a pinned buffer), if
+        given, holds x0 on entry and receives the solution in place."""
         b = _f64(b)
-        x = np.zeros(self.A.n) if x0 is None else _f64(x0).copy()
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous float64 array")
+            x = out
+        else:
+            x = np.zeros(self.A.n) if x0 is None else _f64(x0).copy()
         check(self._L.xs_solve(self.h, _d(b), _d(x)), "xs_solve")
         return x
 

@@ -112,8 +112,9 @@ void operator_ensure32(Operator &op, const int *rp0, cudaStream_t s)
     check_launch();
     build_tiling(rp0, op.n, SPMV_THREADS, spmv_cap<float>(), op.tile32, s);
     if (op.ell_w > 0 && !op.ev32.p) {
-        op.ev32.alloc((size_t)op.ell_w * op.n);
-        k_convert_f32<<<geom().sms * 4, 256, 0, s>>>((long)op.ell_w * op.n, op.ev.p, op.ev32.p);
+        const long m = (long)op.ell_w * ell_ld(op.n);
+        op.ev32.alloc(m);
+        k_convert_f32<<<geom().sms * 4, 256, 0, s>>>(m, op.ev.p, op.ev32.p);
         check_launch();
     }
 }
@@ -127,41 +128,57 @@ void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const doub
     for (int i = 0; i < n; i++)
         for (int q = rp0[i]; q < rp0[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci0[q] - i));
     op.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
-    std::vector<int> c((size_t)w * n);
-    std::vector<double> vv((size_t)w * n);
+    const long ld = ell_ld(n);
+    const size_t m = (size_t)w * ld;
+    // padding slots of a row point at the row itself (offset 0) with value 0;
+    // padding rows n..ld-1 are never gathered
+    std::vector<int> c(m, 0);
+    std::vector<double> vv(m, 0.0);
     for (int i = 0; i < n; i++) {
         int k = 0;
         for (int q = rp0[i]; q < rp0[i + 1]; q++, k++) {
-            c[(size_t)k * n + i] = ci0[q];
-            vv[(size_t)k * n + i] = v[q];
+            c[(size_t)k * ld + i] = ci0[q];
+            vv[(size_t)k * ld + i] = v[q];
         }
-        for (; k < w; k++) {
-            c[(size_t)k * n + i] = i;
-            vv[(size_t)k * n + i] = 0.0;
-        }
+        for (; k < w; k++) c[(size_t)k * ld + i] = i;
     }
     if (op.ell16) {
-        std::vector<short> o((size_t)w * n);
+        std::vector<short> o(m, 0);
         for (int i = 0; i < n; i++)
-            for (int k = 0; k < w; k++) o[(size_t)k * n + i] = (short)(c[(size_t)k * n + i] - i);
-        op.eco.alloc((size_t)w * n);
-        op.eco.upload(o.data(), (size_t)w * n, s);
+            for (int k = 0; k < w; k++) o[(size_t)k * ld + i] = (short)(c[(size_t)k * ld + i] - i);
+        op.eco.alloc(m);
+        op.eco.upload(o.data(), m, s);
         op.eci.free();
     } else {
-        op.eci.alloc((size_t)w * n);
-        op.eci.upload(c.data(), (size_t)w * n, s);
+        op.eci.alloc(m);
+        op.eci.upload(c.data(), m, s);
         op.eco.free();
     }
-    op.ev.alloc((size_t)w * n);
-    op.ev.upload(vv.data(), (size_t)w * n, s);
+    op.ev.alloc(m);
+    op.ev.upload(vv.data(), m, s);
     if (want32) {
-        op.ev32.alloc((size_t)w * n);
-        k_convert_f32<<<geom().sms * 4, 256, 0, s>>>((long)w * n, op.ev.p, op.ev32.p);
+        op.ev32.alloc(m);
+        k_convert_f32<<<geom().sms * 4, 256, 0, s>>>((long)m, op.ev.p, op.ev32.p);
         check_launch();
     }
-    op.ell_grid = std::min(geom().sms * ELL_BLOCKS_PER_SM, (n + 255) / 256);
+    op.ell_grid = (int)std::min<long>((long)geom().sms * ELL_BLOCKS_PER_SM, (n + 256L * ELL_ROWS - 1) / (256L * ELL_ROWS));
     if (op.ell_grid < 1) op.ell_grid = 1;
     XS_CUDA(cudaStreamSynchronize(s));
+}
+
+// new values for an existing ELL copy: slot k of row r is the row's k-th
+// CSR entry (0 past the row's end), as operator_build_ell lays it out
+__global__ void k_ell_refill(int n, int w, long ld, const int *__restrict__ rp, const double *__restrict__ v,
+                             double *ev, float *ev32)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int k0 = rp[r], len = rp[r + 1] - k0;
+        for (int k = 0; k < w; k++) {
+            const double val = k < len ? v[k0 + k] : 0.0;
+            ev[(long)k * ld + r] = val;
+            if (ev32) ev32[(long)k * ld + r] = (float)val;
+        }
+    }
 }
 
 // ---------------------------------------------------------------- handle
@@ -175,6 +192,7 @@ struct Handle {
     // caller entry of each stored entry when set_matrix had to sort a row's
     // columns (empty: stored order = caller order)
     std::vector<long> vperm;
+    bool hv_stale = false;  // hv lags the device values (xs_mat_update uploads directly)
     Operator A;
     bool have_matrix = false;
     int format = 0;
@@ -266,6 +284,7 @@ static void set_matrix(Handle &h, int n, const int *rp, const int *ci, const dou
     h.n = n;
     h.nnz = nnz;
     h.vperm.clear();
+    h.hv_stale = false;
     h.hrp.resize(n + 1);
     h.hci.resize(nnz);
     h.hv.assign(v, v + nnz);
@@ -309,20 +328,42 @@ static void set_matrix(Handle &h, int n, const int *rp, const int *ci, const dou
     invalidate_pc(h);
 }
 
+// host copy of A's values (refreshed from the device after xs_mat_update)
+static const double *host_vals(Handle &h)
+{
+    if (h.hv_stale) {
+        h.A.v.download(h.hv.data(), h.nnz, h.s);
+        XS_CUDA(cudaStreamSynchronize(h.s));
+        h.hv_stale = false;
+    }
+    return h.hv.data();
+}
+
 // values changed, same pattern
 static void update_values(Handle &h, const double *v)
 {
     if (!h.have_matrix) throw Status(XS_ERR_ORDER);
     if (!v) throw Status(XS_ERR_INVALID);
-    if (h.vperm.empty()) h.hv.assign(v, v + h.nnz);
-    else
+    if (h.vperm.empty()) {
+        // straight from the caller's buffer (a DMA when it is pinned); the
+        // host copy is refreshed only if host-side code needs it later
+        h.A.v.upload(v, h.nnz, h.s);
+        h.hv_stale = true;
+    } else {
         for (long k = 0; k < h.nnz; k++) h.hv[k] = v[h.vperm[k]];
-    h.A.v.upload(h.hv.data(), h.nnz, h.s);
+        h.A.v.upload(h.hv.data(), h.nnz, h.s);
+        h.hv_stale = false;
+    }
     if (h.A.v32.p) {
         k_convert_f32<<<geom().sms * 4, 256, 0, h.s>>>(h.nnz, h.A.v.p, h.A.v32.p);
         check_launch();
     }
-    if (h.A.ell_w > 0) operator_build_ell(h.A, h.hrp.data(), h.hci.data(), h.hv.data(), 0, h.A.v32.p != nullptr, h.s);
+    if (h.A.ell_w > 0) {
+        if (h.A.v32.p && !h.A.ev32.p) h.A.ev32.alloc((size_t)h.A.ell_w * ell_ld(h.n));
+        k_ell_refill<<<geom().sms * 4, 256, 0, h.s>>>(h.n, h.A.ell_w, ell_ld(h.n), h.A.rp.p, h.A.v.p, h.A.ev.p,
+                                                      h.A.v32.p ? h.A.ev32.p : nullptr);
+        check_launch();
+    }
     XS_CUDA(cudaStreamSynchronize(h.s));
     h.adj.reset();
     invalidate_pc(h);
@@ -490,8 +531,14 @@ static void build_precond(Handle &h)
         k_jacobi_init<float><<<geom().sms * 4, 256, 0, h.s>>>(n, h.uptr.p, h.A.v.p, M.jdiag32.p);
         check_launch();
     } else if (type == PC_ILU0 || type == PC_PARILU) {
+        Trace tr("setup ilu (total)", h.s);
+        {
+            Trace t1("  analyse_pattern", h.s);
+            analyse_pattern(h);
+        }
+        Trace t2("  numeric factor + loads", h.s);
         factor_ilu(h, type == PC_ILU0 ? 0 : 1, h.parilu_sweeps);
-        h.fv.alloc(std::max<long>(h.nnz, 1));
+        if (h.fv.n != (size_t)std::max<long>(h.nnz, 1)) h.fv.alloc(std::max<long>(h.nnz, 1));
         k_split_lu<<<geom().sms * 4, 256, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, h.fv.p);
         check_launch();
         load_tri_values(h, M.L, h.fv.p, need32);
@@ -504,6 +551,7 @@ static void build_precond(Handle &h)
         if (h.trsv_mode > 0) M.ensure_sweep_buffers(need32);
         M.have_factors = true;
     } else if (type == PC_PARILUT) {
+        Trace tr("setup parilut (total)", h.s);
         parilut_build(h.s, h.err.p, n, h.A, h.hrp, h.hci, h.parilut_fill, h.parilut_sweeps, h.parilut_droptol, h.ilut);
         // factors in the seqilu0 layout on their own pattern
         ilut_to_tri(h.s, n, h.ilut, M.L, M.U, need32);
@@ -774,7 +822,7 @@ static void adjoint_prepare(Handle &h)
     if (!a.have_At) {
         std::vector<int> trp, tci;
         std::vector<double> tv;
-        host_transpose(n, h.hrp.data(), h.hci.data(), h.hv.data(), trp, tci, &tv, nullptr);
+        host_transpose(n, h.hrp.data(), h.hci.data(), host_vals(h), trp, tci, &tv, nullptr);
         a.At = Operator();
         operator_setup(a.At, n, trp.data(), tci.data(), tv.data(), 0, false, h.s, h.err.p);
         if (h.A.format == 1) operator_build_ell(a.At, trp.data(), tci.data(), tv.data(), 0, false, h.s);
@@ -1532,7 +1580,7 @@ void gpu_mat_format(char *fmt, int *num_nz)
         else if (*num_nz > 16 && *num_nz <= 32) *num_nz = 32;
         else throw Status(XS_ERR_ELL_WIDTH);
         Handle &H = *g_gpu->h;
-        operator_build_ell(H.A, H.hrp.data(), H.hci.data(), H.hv.data(), 0, H.A.v32.p != nullptr, H.s);
+        operator_build_ell(H.A, H.hrp.data(), H.hci.data(), host_vals(H), 0, H.A.v32.p != nullptr, H.s);
         if (H.A.ell_w > *num_nz) throw Status(XS_ERR_ELL_WIDTH);
         H.A.format = 1;
         H.format = 1;

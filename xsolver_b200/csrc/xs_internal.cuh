@@ -18,10 +18,47 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 #include <cstdio>
+#include <cstdlib>
+#include <chrono>
 
 #include "../../include/xsolver_c.h"
 
 namespace xs {
+
+// Setup phase tracing: with XS_TRACE=1 in the environment, each traced
+// phase waits for its stream and prints its wall time to stderr.
+inline bool trace_on()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("XS_TRACE");
+        on = (e && atoi(e) != 0) ? 1 : 0;
+    }
+    return on == 1;
+}
+struct Trace {
+    const char *what;
+    cudaStream_t s;
+    std::chrono::steady_clock::time_point t0;
+    Trace(const char *w, cudaStream_t st) : what(w), s(st)
+    {
+        if (trace_on()) {
+            cudaStreamSynchronize(s);
+            t0 = std::chrono::steady_clock::now();
+        }
+    }
+    void stop()
+    {
+        if (trace_on() && what) {
+            cudaStreamSynchronize(s);
+            const double ms =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            fprintf(stderr, "[xs trace] %-28s %10.2f ms\n", what, ms);
+        }
+        what = nullptr;
+    }
+    ~Trace() { stop(); }
+};
 
 // ---------------------------------------------------------------- errors
 struct CudaError {
@@ -215,21 +252,26 @@ __device__ __forceinline__ void st_release(int *p, int v)
 // ---------------------------------------------------------------- factor value types
 template <typename T>
 struct FVal;
+// ld: load one stored factor value and widen it; cvt: widen a loaded one
 template <>
 struct FVal<double> {
     __device__ static double ld(const double *p, long i) { return __ldg(p + i); }
+    __device__ static double cvt(double v) { return v; }
 };
 template <>
 struct FVal<float> {
     __device__ static float ld(const float *p, long i) { return __ldg(p + i); }
+    __device__ static float cvt(float v) { return v; }
 };
 template <>
 struct FVal<__nv_bfloat16> {
     __device__ static float ld(const __nv_bfloat16 *p, long i) { return __bfloat162float(__ldg(p + i)); }
+    __device__ static float cvt(__nv_bfloat16 v) { return __bfloat162float(v); }
 };
 template <>
 struct FVal<__half> {
     __device__ static float ld(const __half *p, long i) { return __half2float(__ldg(p + i)); }
+    __device__ static float cvt(__half v) { return __half2float(v); }
 };
 
 // ---------------------------------------------------------------- deterministic reductions

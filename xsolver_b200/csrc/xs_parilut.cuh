@@ -494,6 +494,7 @@ inline double plt_kth_abs(PltCtx &c, const DBuf<double> &v, long m, long k)
 inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, const std::vector<int> &hrp,
                           const std::vector<int> &hci, double fill, int sweeps, double droptol, ParilutResult &R)
 {
+    Trace tr_all("parilut_build", s);
     PltCtx c{s, err, n};
     const int G = c.grid();
     const long nnzA = A.nnz;
@@ -527,12 +528,14 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
     DBuf<int> cnt;
     cnt.alloc(n);
     for (int sw = 0; sw < sweeps; sw++) {
+        Trace tr_sw("parilut sweep", s);
         const double rate = (fill - 1) / sweeps * (sw + 1) + 1;
         DCsr Uc;
         plt_transpose(c, U, Uc);
         k_udiag<<<G, 256, 0, s>>>(n, U.rp, U.v, udiag);
         check_launch();
         // candidates
+        Trace tr_cand("  candidates", s);
         DCsr D;
         D.n = n;
         const int cg = std::min((n + PLT_WARPS - 1) / PLT_WARPS, geom().sms * 16);
@@ -551,6 +554,8 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
             XS_CUDA(cudaStreamSynchronize(s));
             if (e) throw Status(dev_err_to_status(e));
         }
+        tr_cand.stop();
+        Trace tr_rest("  split/sweeps/threshold", s);
         // split
         DCsr L2, U2;
         L2.n = U2.n = n;
@@ -665,9 +670,13 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
 // prepare the sync-free solve plans for ParILUT factors (own pattern)
 inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriDev &U, bool need32)
 {
+    Trace tr_all("ilut_to_tri", s);
     auto up = [&](TriDev &T, const std::vector<int> &nrp, const std::vector<int> &nci, bool upper, const double *vals) {
         T = TriDev();
-        build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s);
+        {
+            Trace tr("  build_tri_dev", s);
+            build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s);
+        }
         const long m = std::max<long>(T.nnz, 1);
         const int g = geom().sms * 4;
         T.pv64.alloc(m); T.nv64.alloc(m);

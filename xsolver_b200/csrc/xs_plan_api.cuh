@@ -69,7 +69,7 @@ int xs_plan_build_ell(xs_plan_t p, int *width)
     return guarded([&] {
         if (!p) throw Status(XS_ERR_INVALID);
         Handle &h = *p->h;
-        operator_build_ell(h.A, h.hrp.data(), h.hci.data(), h.hv.data(), 0, h.A.v32.p != nullptr, h.s);
+        operator_build_ell(h.A, h.hrp.data(), h.hci.data(), host_vals(h), 0, h.A.v32.p != nullptr, h.s);
         if (width) *width = h.A.ell_w;
     });
 }
@@ -100,7 +100,7 @@ int xs_plan_spmv_t(xs_plan_t p, const double *x, double *y)
         if (!h.adj.have_At) {
             std::vector<int> trp, tci;
             std::vector<double> tv;
-            host_transpose(h.n, h.hrp.data(), h.hci.data(), h.hv.data(), trp, tci, &tv, nullptr);
+            host_transpose(h.n, h.hrp.data(), h.hci.data(), host_vals(h), trp, tci, &tv, nullptr);
             h.adj.At = Operator();
             operator_setup(h.adj.At, h.n, trp.data(), tci.data(), tv.data(), 0, false, h.s, h.err.p);
             h.adj.have_At = true;
@@ -331,7 +331,7 @@ int xs_plan_time_op(xs_plan_t p, int op, int reps, int flush_l2, double *ms)
         check_launch();
         if (flush_l2 && !p->l2flush.p) p->l2flush.alloc((size_t)48 << 20);  // 384 MB > L2
         if (op == 1 || op == 6) {
-            if (h.A.ell_w == 0) operator_build_ell(h.A, h.hrp.data(), h.hci.data(), h.hv.data(), 0, f32, h.s);
+            if (h.A.ell_w == 0) operator_build_ell(h.A, h.hrp.data(), h.hci.data(), host_vals(h), 0, f32, h.s);
         }
         if (f32) operator_ensure32(h.A, h.hrp.data(), h.s);
         h.W.ensure(64, 1);

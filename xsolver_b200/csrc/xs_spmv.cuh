@@ -226,7 +226,6 @@ __global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const
 }
 
 // ---------------------------------------------------------------- ELL kernel
-constexpr int ELL_CH = 8;  // entries per load chunk
 // Column storage of an ELL copy: CT = int holds absolute columns, CT = short
 // holds the offset c - row (used when every |c - row| <= 32767, as for
 // stencil and other banded matrices: 2 index bytes per entry instead of 4).
@@ -237,68 +236,116 @@ __device__ __forceinline__ int ell_col(CT c, int row)
     else return (int)c;
 }
 
+// ELL layout: slot k of row r at [k * ld + r], ld = n rounded up to
+// ELL_LD_ALIGN (rows n..ld-1 are padding and never gathered), so R
+// consecutive rows of one slot form one aligned vector of R elements.
+constexpr int ELL_LD_ALIGN = 8;
+__host__ __device__ inline long ell_ld(int n) { return ((long)n + ELL_LD_ALIGN - 1) / ELL_LD_ALIGN * ELL_LD_ALIGN; }
+
 template <typename MT, typename CT>
 struct EllArgs {
     int n, w;
+    long ld;
     const CT *ci;
     const MT *v;
 };
 
 // Launch shape of the ELL kernels (SpMV and the Jacobi-sweep triangle
-// kernels): CTAs of 256 threads, ELL_MIN_BLOCKS of them resident per SM
-// (register cap 65536 / (256 * ELL_MIN_BLOCKS)), ELL_BLOCKS_PER_SM per SM in
-// the grid, rows grid-strided.
+// kernels): CTAs of 256 threads, ELL_MIN_BLOCKS of them resident per SM,
+// ELL_BLOCKS_PER_SM per SM in the grid; each thread takes ELL_ROWS
+// consecutive rows (vector loads of the slot data) and walks the entries in
+// chunks of ELL_CHUNK, issuing every load of a chunk before its gathers.
+// These kernels are bound by the latency of the dependent index -> gather
+// loads, so the shape trades registers (rows x chunk in flight) against
+// resident warps.
 #ifndef XS_ELL_MIN_BLOCKS
-#define XS_ELL_MIN_BLOCKS 4
+#define XS_ELL_MIN_BLOCKS 8
 #endif
 #ifndef XS_ELL_BLOCKS_PER_SM
 #define XS_ELL_BLOCKS_PER_SM 8
 #endif
+#ifndef XS_ELL_ROWS
+#define XS_ELL_ROWS 1
+#endif
+#ifndef XS_ELL_CHUNK
+#define XS_ELL_CHUNK 8
+#endif
 constexpr int ELL_MIN_BLOCKS = XS_ELL_MIN_BLOCKS;
 constexpr int ELL_BLOCKS_PER_SM = XS_ELL_BLOCKS_PER_SM;
+constexpr int ELL_ROWS = XS_ELL_ROWS;
+constexpr int ELL_CHUNK = XS_ELL_CHUNK;
+static_assert(ELL_ROWS == 1 || ELL_ROWS == 2 || ELL_ROWS == 4 || ELL_ROWS == 8, "rows per thread");
+static_assert(ELL_LD_ALIGN % ELL_ROWS == 0, "row vectors must stay aligned");
 
-// C consecutive ELL entries of row r (C known at compile time): all column
-// and value loads first, then all gathers of x, then the in-order sum.
-template <int C, typename VT, typename MT, typename CT>
-__device__ __forceinline__ double ell_chunk(const CT *&cp, const MT *&vp, long n, const VT *__restrict__ x, int r,
-                                            double sum)
+// R consecutive elements starting at an R-aligned index, one vector load
+// (two for 32 bytes) through the read-only path
+template <int R, typename T>
+__device__ __forceinline__ void ld_vec(const T *p, T (&o)[R])
 {
-    int c[C];
-    MT v[C];
-    VT xv[C];
+    constexpr int B = R * (int)sizeof(T);
+    if constexpr (B == 2) {
+        unsigned short u = __ldg((const unsigned short *)p);
+        memcpy(o, &u, 2);
+    } else if constexpr (B == 4) {
+        unsigned u = __ldg((const unsigned *)p);
+        memcpy(o, &u, 4);
+    } else if constexpr (B == 8) {
+        uint2 u = __ldg((const uint2 *)p);
+        memcpy(o, &u, 8);
+    } else if constexpr (B == 16) {
+        uint4 u = __ldg((const uint4 *)p);
+        memcpy(o, &u, 16);
+    } else {
+        static_assert(B % 16 == 0, "vector size");
 #pragma unroll
-    for (int j = 0; j < C; j++) {
-        c[j] = ell_col<CT>(__ldg(cp), r);
-        v[j] = __ldg(vp);
-        cp += n;
-        vp += n;
-    }
-#pragma unroll
-    for (int j = 0; j < C; j++) xv[j] = __ldg(x + c[j]);
-#pragma unroll
-    for (int j = 0; j < C; j++) sum += (double)v[j] * (double)xv[j];
-    return sum;
-}
-
-// sum over the w entries of row r in entry order, in chunks of up to 8
-// (the chunk length is warp-uniform, so the switch does not diverge)
-template <typename VT, typename MT, typename CT>
-__device__ __forceinline__ double ell_row(const CT *cp, const MT *vp, int w, long n, const VT *__restrict__ x, int r)
-{
-    double sum = 0.0;
-    for (int k0 = 0; k0 < w; k0 += ELL_CH) {
-        switch (min(ELL_CH, w - k0)) {
-        case 8: sum = ell_chunk<8>(cp, vp, n, x, r, sum); break;
-        case 7: sum = ell_chunk<7>(cp, vp, n, x, r, sum); break;
-        case 6: sum = ell_chunk<6>(cp, vp, n, x, r, sum); break;
-        case 5: sum = ell_chunk<5>(cp, vp, n, x, r, sum); break;
-        case 4: sum = ell_chunk<4>(cp, vp, n, x, r, sum); break;
-        case 3: sum = ell_chunk<3>(cp, vp, n, x, r, sum); break;
-        case 2: sum = ell_chunk<2>(cp, vp, n, x, r, sum); break;
-        default: sum = ell_chunk<1>(cp, vp, n, x, r, sum); break;
+        for (int q = 0; q < B / 16; q++) {
+            uint4 u = __ldg((const uint4 *)p + q);
+            memcpy((char *)o + 16 * q, &u, 16);
         }
     }
-    return sum;
+}
+
+// C consecutive slots of rows r0..r0+R-1: slot loads, then the gathers of x,
+// then the per-row sums in slot order (each row's sum stays in entry order).
+template <int C, int R, typename VT, typename MT, typename CT>
+__device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld, const VT *__restrict__ x, int r0,
+                                          int n, double (&sum)[R])
+{
+    CT c[C][R];
+    MT v[C][R];
+    VT xv[C][R];
+#pragma unroll
+    for (int j = 0; j < C; j++) {
+        ld_vec<R>(cp, c[j]);
+        ld_vec<R>(vp, v[j]);
+        cp += ld;
+        vp += ld;
+    }
+#pragma unroll
+    for (int j = 0; j < C; j++)
+#pragma unroll
+        for (int q = 0; q < R; q++) xv[j][q] = (R == 1 || r0 + q < n) ? __ldg(x + ell_col<CT>(c[j][q], r0 + q)) : (VT)0;
+#pragma unroll
+    for (int j = 0; j < C; j++)
+#pragma unroll
+        for (int q = 0; q < R; q++) sum[q] += (double)v[j][q] * (double)xv[j][q];
+}
+
+template <int R, typename VT, typename MT, typename CT>
+__device__ __forceinline__ void ell_rows(const CT *cp, const MT *vp, int w, long ld, const VT *__restrict__ x, int r0,
+                                         int n, double (&sum)[R])
+{
+    for (int k0 = 0; k0 < w; k0 += ELL_CHUNK) {
+        const int m = min(ELL_CHUNK, w - k0);  // warp-uniform
+        if (m == ELL_CHUNK) ell_chunk<ELL_CHUNK, R>(cp, vp, ld, x, r0, n, sum);
+        else if (ELL_CHUNK > 7 && m == 7) ell_chunk<7, R>(cp, vp, ld, x, r0, n, sum);
+        else if (ELL_CHUNK > 6 && m == 6) ell_chunk<6, R>(cp, vp, ld, x, r0, n, sum);
+        else if (ELL_CHUNK > 5 && m == 5) ell_chunk<5, R>(cp, vp, ld, x, r0, n, sum);
+        else if (ELL_CHUNK > 4 && m == 4) ell_chunk<4, R>(cp, vp, ld, x, r0, n, sum);
+        else if (ELL_CHUNK > 3 && m == 3) ell_chunk<3, R>(cp, vp, ld, x, r0, n, sum);
+        else if (ELL_CHUNK > 2 && m == 2) ell_chunk<2, R>(cp, vp, ld, x, r0, n, sum);
+        else ell_chunk<1, R>(cp, vp, ld, x, r0, n, sum);
+    }
 }
 
 template <typename VT, typename MT, typename CT, typename Epi>
@@ -306,17 +353,27 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_ell_spmv(EllArgs<MT, CT
                                                                    VT *__restrict__ y, Epi epi, RedSlot slot)
 {
     constexpr int KK = Epi::K > 0 ? Epi::K : 1;
+    constexpr int R = ELL_ROWS;
     if (!epi.active()) return;
     __shared__ double tot[KK];
     double acc[KK];
 #pragma unroll
     for (int k = 0; k < KK; k++) acc[k] = 0.0;
     const int n = A.n;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        const double sum = ell_row<VT, MT, CT>(A.ci + r, A.v + r, A.w, (long)n, x, r);
-        VT o = epi.out(r, sum);
-        y[r] = o;
-        if (Epi::K > 0) epi.acc(r, (double)o, acc);
+    for (int r0 = (blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += gridDim.x * blockDim.x * R) {
+        double sum[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) sum[q] = 0.0;
+        ell_rows<R, VT, MT, CT>(A.ci + r0, A.v + r0, A.w, A.ld, x, r0, n, sum);
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const int r = r0 + q;
+            if (R == 1 || r < n) {
+                VT o = epi.out(r, sum[q]);
+                y[r] = o;
+                if (Epi::K > 0) epi.acc(r, (double)o, acc);
+            }
+        }
     }
     if (Epi::K > 0) {
         if (block_reduce_publish<KK>(acc, slot, tot)) {
@@ -361,8 +418,8 @@ struct Operator {
         const MT *vals;
         if constexpr (std::is_same<MT, double>::value) vals = ev.p;
         else vals = ev32.p;
-        if constexpr (sizeof(CT) == 2) return EllArgs<MT, CT>{n, ell_w, eco.p, vals};
-        else return EllArgs<MT, CT>{n, ell_w, eci.p, vals};
+        if constexpr (sizeof(CT) == 2) return EllArgs<MT, CT>{n, ell_w, ell_ld(n), eco.p, vals};
+        else return EllArgs<MT, CT>{n, ell_w, ell_ld(n), eci.p, vals};
     }
 };
 

@@ -357,37 +357,47 @@ __global__ void k_trsv_sweep(int n, const int *__restrict__ rp, const int *__res
     }
 }
 
-// C consecutive entries of row i of a sweep pass: acc -= v * y(c), with
-// y(c) = x[c] (L, first pass), dinv[c]*x[c] (U, first pass) or yin[c].
-template <int C, typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
-__device__ __forceinline__ VT sweep_chunk(const CT *&cp, const FT *&vp, long n, int i, const DT *__restrict__ dinv,
-                                          const VT *__restrict__ x, const VT *__restrict__ yin, VT acc)
+// C consecutive slots of rows i0..i0+R-1 of a sweep pass: acc -= v * y(c),
+// with y(c) = x[c] (L, first pass), dinv[c]*x[c] (U, first pass) or yin[c].
+template <int C, int R, typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
+__device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long ld, int i0, int n,
+                                            const DT *__restrict__ dinv, const VT *__restrict__ x,
+                                            const VT *__restrict__ yin, VT (&acc)[R])
 {
-    int c[C];
-    VT v[C], y[C];
+    CT c[C][R];
+    FT v[C][R];
+    VT y[C][R];
 #pragma unroll
     for (int j = 0; j < C; j++) {
-        c[j] = ell_col<CT>(__ldg(cp), i);
-        v[j] = (VT)FVal<FT>::ld(vp, 0);
-        cp += n;
-        vp += n;
+        ld_vec<R>(cp, c[j]);
+        ld_vec<R>(vp, v[j]);
+        cp += ld;
+        vp += ld;
     }
 #pragma unroll
-    for (int j = 0; j < C; j++) {
-        if (FIRST2) y[j] = UPPER ? (VT)(__ldg(x + c[j]) * (VT)__ldg(dinv + c[j])) : __ldg(x + c[j]);
-        else y[j] = __ldg(yin + c[j]);
-    }
+    for (int j = 0; j < C; j++)
 #pragma unroll
-    for (int j = 0; j < C; j++) acc = msub(acc, y[j], v[j]);
-    return acc;
+        for (int q = 0; q < R; q++) {
+            if (R == 1 || i0 + q < n) {
+                const int col = ell_col<CT>(c[j][q], i0 + q);
+                if (FIRST2) y[j][q] = UPPER ? (VT)(__ldg(x + col) * (VT)__ldg(dinv + col)) : __ldg(x + col);
+                else y[j][q] = __ldg(yin + col);
+            } else {
+                y[j][q] = (VT)0;
+            }
+        }
+#pragma unroll
+    for (int j = 0; j < C; j++)
+#pragma unroll
+        for (int q = 0; q < R; q++) acc[q] = msub(acc[q], y[j][q], (VT)FVal<FT>::cvt(v[j][q]));
 }
 
 // Jacobi sweeps on a column-major ELL copy of the triangle (natural order,
-// padding column = the row itself with value 0): every load is coalesced.
+// padding slot = the row itself with value 0): every slot load is coalesced.
 // FIRST2 folds the first sweep into the second: the previous iterate of the
 // first sweep is x itself (L) or dinv*x (U), so k sweeps cost k-1 passes.
-// Entries go in chunks of up to 8 of compile-time length (the switch is
-// warp-uniform): loads of a chunk are issued before its gathers.
+// Launch shape as the ELL SpMV (ELL_ROWS rows per thread, ELL_CHUNK slots
+// per load chunk, warp-uniform chunk lengths).
 template <typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
 __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, int w, const CT *__restrict__ eci,
                                                                          const FT *__restrict__ ev,
@@ -396,24 +406,34 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, i
                                                                          const VT *__restrict__ yin,
                                                                          VT *__restrict__ yout, const int *done_flag)
 {
+    constexpr int R = ELL_ROWS;
     if (done_flag && *done_flag) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        VT acc = UPPER ? (VT)(x[i] * (VT)dinv[i]) : x[i];
-        const CT *cp = eci + i;
-        const FT *vp = ev + i;
-        for (int k0 = 0; k0 < w; k0 += ELL_CH) {
-            switch (min(ELL_CH, w - k0)) {
-            case 8: acc = sweep_chunk<8, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            case 7: acc = sweep_chunk<7, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            case 6: acc = sweep_chunk<6, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            case 5: acc = sweep_chunk<5, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            case 4: acc = sweep_chunk<4, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            case 3: acc = sweep_chunk<3, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            case 2: acc = sweep_chunk<2, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            default: acc = sweep_chunk<1, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, n, i, dinv, x, yin, acc); break;
-            }
+    const long ld = ell_ld(n);
+    for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * R; i0 < n; i0 += gridDim.x * blockDim.x * R) {
+        VT acc[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const int i = i0 + q;
+            acc[q] = (R == 1 || i < n) ? (UPPER ? (VT)(x[i] * (VT)dinv[i]) : x[i]) : (VT)0;
         }
-        yout[i] = acc;
+        const CT *cp = eci + i0;
+        const FT *vp = ev + i0;
+        for (int k0 = 0; k0 < w; k0 += ELL_CHUNK) {
+            const int m = min(ELL_CHUNK, w - k0);  // warp-uniform
+#define XS_SWEEP_CHUNK(CC) sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, ld, i0, n, dinv, x, yin, acc)
+            if (m == ELL_CHUNK) XS_SWEEP_CHUNK(ELL_CHUNK);
+            else if (ELL_CHUNK > 7 && m == 7) XS_SWEEP_CHUNK(7);
+            else if (ELL_CHUNK > 6 && m == 6) XS_SWEEP_CHUNK(6);
+            else if (ELL_CHUNK > 5 && m == 5) XS_SWEEP_CHUNK(5);
+            else if (ELL_CHUNK > 4 && m == 4) XS_SWEEP_CHUNK(4);
+            else if (ELL_CHUNK > 3 && m == 3) XS_SWEEP_CHUNK(3);
+            else if (ELL_CHUNK > 2 && m == 2) XS_SWEEP_CHUNK(2);
+            else XS_SWEEP_CHUNK(1);
+#undef XS_SWEEP_CHUNK
+        }
+#pragma unroll
+        for (int q = 0; q < R; q++)
+            if (R == 1 || i0 + q < n) yout[i0 + q] = acc[q];
     }
 }
 
@@ -720,18 +740,19 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     for (int i = 0; i < n; i++) w = std::max(w, rp[i + 1] - rp[i]);
     T.ell_w = 0;
     if (w > 0 && w <= 64 && (long)w * n <= 2 * std::max<long>(T.nnz, 1)) {
-        std::vector<int> ec((size_t)w * n);
-        std::vector<long> es((size_t)w * n);
+        // layout of the operator's ELL copy: slot k of row i at k*ld + i;
+        // padding slots point at the row itself, padding rows are never read
+        const long ld = ell_ld(n);
+        const size_t m = (size_t)w * ld;
+        std::vector<int> ec(m, 0);
+        std::vector<long> es(m, -1);
         for (int i = 0; i < n; i++) {
             int k = 0;
             for (int q = rp[i]; q < rp[i + 1]; q++, k++) {
-                ec[(size_t)k * n + i] = ci[q];
-                es[(size_t)k * n + i] = src_of(q);
+                ec[(size_t)k * ld + i] = ci[q];
+                es[(size_t)k * ld + i] = src_of(q);
             }
-            for (; k < w; k++) {
-                ec[(size_t)k * n + i] = i;
-                es[(size_t)k * n + i] = -1;
-            }
+            for (; k < w; k++) ec[(size_t)k * ld + i] = i;
         }
         T.ell_w = w;
         long maxoff = 0;
@@ -739,16 +760,16 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
             for (int q = rp[i]; q < rp[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci[q] - i));
         T.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
         if (T.ell16) {
-            std::vector<short> eo((size_t)w * n);
+            std::vector<short> eo(m, 0);
             for (int i = 0; i < n; i++)
-                for (int k = 0; k < w; k++) eo[(size_t)k * n + i] = (short)(ec[(size_t)k * n + i] - i);
-            T.eco.alloc((size_t)w * n); T.eco.upload(eo.data(), (size_t)w * n, s);
+                for (int k = 0; k < w; k++) eo[(size_t)k * ld + i] = (short)(ec[(size_t)k * ld + i] - i);
+            T.eco.alloc(m); T.eco.upload(eo.data(), m, s);
             T.eci.free();
         } else {
-            T.eci.alloc((size_t)w * n); T.eci.upload(ec.data(), (size_t)w * n, s);
+            T.eci.alloc(m); T.eci.upload(ec.data(), m, s);
             T.eco.free();
         }
-        T.esrc.alloc((size_t)w * n); T.esrc.upload(es.data(), (size_t)w * n, s);
+        T.esrc.alloc(m); T.esrc.upload(es.data(), m, s);
     }
     T.ticket.alloc(1);
     XS_CUDA(cudaStreamSynchronize(s));
@@ -758,7 +779,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
 inline void load_tri_ell(TriDev &T, const double *vals, bool need32, cudaStream_t s)
 {
     if (T.ell_w == 0) return;
-    const long m = (long)T.ell_w * T.n;
+    const long m = (long)T.ell_w * ell_ld(T.n);
     const int g = geom().sms * 4;
     if (T.ev64.n != (size_t)m) T.ev64.alloc(m);
     k_gather_convert_pad<double><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.ev64.p);
