@@ -298,6 +298,13 @@ int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, 
  * XS_TRSV_BACKOFF_NS, XS_TRSV_CHUNK_ROWS override them at first use.  The
  * layout is fixed when a preconditioner is built: set before factorising. */
 int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
+/* Exact LU solves of systems with at most max_rows rows, whose solution
+ * vector fits in one SM's shared memory (FP64: 25600 rows), run in one CTA
+ * that walks the dependency levels with a block barrier between them
+ * (bitwise the same result as the sync-free solve, without its cross-SM
+ * hand-off per level).  0 disables it; default: no row limit beyond the
+ * shared-memory one.  Environment XS_TRSV_BLOCK_ROWS sets it at first use. */
+int xs_set_trsv_block_rows(int max_rows);
 /* Column storage of ELL copies (the ELL SpMV and the Jacobi-sweep triangle
  * copies): index_bits 16 stores each column as a 16-bit offset from its row
  * whenever every |col - row| <= 32767 (default; halves the index bytes of

@@ -206,13 +206,51 @@ def test_parilut_bitwise_vs_oracle(cuda):
             assert np.array_equal(G[k], getattr(F, k)), (A.name, k)
 
 
+def test_block_and_syncfree_lusolve_bitwise(cuda):
+    """The single-CTA solve (small systems) and the sync-free multi-CTA solve
+    give the same bits, FP64 and FP32/BF16 factors."""
+    import torch
+    from xsolver_b200 import _lib
+    from xsolver_b200.api import Plan
+
+    L = _lib.lib()
+    for A in (st.poisson2d_5pt(128), st.convdiff3d_27pt(14)):
+        x = st.rhs_uniform(A.n, 11)
+        outs = []
+        for rows in (1 << 30, 0):
+            assert L.xs_set_trsv_block_rows(rows) == 0
+            try:
+                P = Plan(A).factor("ilu0")
+                z = torch.zeros(A.n, dtype=torch.float64, device=cuda)
+                P.lusolve(_dev(x, cuda), z)
+                P.set_factor_precision("bf16")
+                z32 = torch.zeros(A.n, dtype=torch.float32, device=cuda)
+                P.lusolve(_dev(x.astype(np.float32), cuda), z32)
+                P.sync()
+                outs.append((z.cpu().numpy(), z32.cpu().numpy()))
+            finally:
+                L.xs_set_trsv_block_rows(1 << 30)
+        assert np.array_equal(outs[0][0], outs[1][0]), A.name
+        assert np.array_equal(outs[0][1], outs[1][1]), A.name
+        assert np.array_equal(outs[0][0], oracle.lusolve(oracle.ilu0(A), x)), A.name
+
+
 def test_syncfree_wait_times_out_and_recovers(cuda):
     """A dependency nothing publishes: the bounded wait gives up (about 1 s),
     the error is reported, and the plan works again after the dependency is
-    restored."""
+    restored.  (Sync-free solve forced: the single-CTA solve has no waits.)"""
     import torch
+    from xsolver_b200 import _lib
     from xsolver_b200.api import Plan, XsError
 
+    _lib.lib().xs_set_trsv_block_rows(0)
+    try:
+        _timeout_case(cuda, torch, Plan, XsError)
+    finally:
+        _lib.lib().xs_set_trsv_block_rows(1 << 30)
+
+
+def _timeout_case(cuda, torch, Plan, XsError):
     A = st.poisson3d_7pt(16)
     P = Plan(A).factor("ilu0")
     F = oracle.ilu0(A)

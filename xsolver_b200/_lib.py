@@ -93,6 +93,7 @@ def _declare(L):
         "xs_tri_levels": [C.c_int, _ip, _ip, C.c_int, _ip, _ip, _ip],
         "xs_set_trsv_tuning": [C.c_int, C.c_int, C.c_int],
         "xs_set_ell_index_bits": [C.c_int],
+        "xs_set_trsv_block_rows": [C.c_int],
         "xs_lusolve_noalloc": [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         "xsolver_last_error": [],
     }

@@ -63,6 +63,7 @@ TrsvTuning &trsv_tuning()
         if (const char *e = getenv("XS_TRSV_BLOCKS_PER_SM")) t.blocks_per_sm = atoi(e);
         if (const char *e = getenv("XS_TRSV_BACKOFF_NS")) t.backoff_ns = std::max(8, atoi(e));
         if (const char *e = getenv("XS_TRSV_CHUNK_ROWS")) t.chunk_rows = std::max(0, atoi(e));
+        if (const char *e = getenv("XS_TRSV_BLOCK_ROWS")) t.block_max_rows = std::max(0, atoi(e));
         init = true;
     }
     return t;
@@ -1050,6 +1051,14 @@ static int check_gpu()
 extern "C" {
 
 const char *xs_version(void) { return "xsolver_b200 1.0 (sm_100a)"; }
+
+int xs_set_trsv_block_rows(int max_rows)
+{
+    return guarded([&] {
+        if (max_rows < 0) throw Status(XS_ERR_INVALID);
+        trsv_tuning().block_max_rows = max_rows;
+    });
+}
 
 int xs_set_ell_index_bits(int bits)
 {

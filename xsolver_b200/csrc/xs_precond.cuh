@@ -115,6 +115,13 @@ struct PrecondDev {
     template <typename VT, typename FT>
     void apply_exact(const VT *x, VT *z, const int *done_flag, cudaStream_t s)
     {
+        if (lu_block_ok<VT>(L, U)) {
+            const VT *dinv;
+            if constexpr (std::is_same<VT, double>::value) dinv = U.dinv64.p;
+            else dinv = U.dinv32.p;
+            launch_lu_block<VT, FT, VT>(L, U, dinv, x, z, done_flag, s);
+            return;
+        }
         exact_half<VT, FT>(0, x, z, done_flag, s);
         exact_half<VT, FT>(1, x, z, done_flag, s);
     }

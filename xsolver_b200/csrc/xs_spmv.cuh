@@ -257,15 +257,18 @@ struct EllArgs {
 // chunks of ELL_CHUNK, issuing every load of a chunk before its gathers.
 // These kernels are bound by the latency of the dependent index -> gather
 // loads, so the shape trades registers (rows x chunk in flight) against
-// resident warps.
+// resident warps.  Default (5 CTAs of 256 resident, 51 registers, 10 CTAs
+// per SM in the grid, 2 rows x 8 slots per thread) was the fastest of nine
+// shapes timed on B200 for the 128^3 7-point ELL SpMV (FP32/FP64) and the
+// BF16/FP32/FP64 Jacobi-sweep passes.
 #ifndef XS_ELL_MIN_BLOCKS
-#define XS_ELL_MIN_BLOCKS 8
+#define XS_ELL_MIN_BLOCKS 5
 #endif
 #ifndef XS_ELL_BLOCKS_PER_SM
-#define XS_ELL_BLOCKS_PER_SM 8
+#define XS_ELL_BLOCKS_PER_SM 10
 #endif
 #ifndef XS_ELL_ROWS
-#define XS_ELL_ROWS 1
+#define XS_ELL_ROWS 2
 #endif
 #ifndef XS_ELL_CHUNK
 #define XS_ELL_CHUNK 8

@@ -73,6 +73,9 @@ struct TrsvTuning {
     int blocks_per_sm = 2;
     int backoff_ns = 128;
     int chunk_rows = 0;  // chunked kernel: rows per CTA chunk (0: level-ordered kernel)
+    // single-CTA solve (k_lu_block) for systems of at most this many rows
+    // whose solution fits in shared memory; 0 disables it
+    int block_max_rows = 1 << 30;
 };
 TrsvTuning &trsv_tuning();
 
@@ -451,6 +454,31 @@ __global__ void k_gather_convert_pad(long m, const long *__restrict__ src, const
     }
 }
 
+// ELL copy of a triangle from its natural CSR: slot k of row i at k*ld + i
+// (column, or the 16-bit offset col - i when CT = short) and the source index
+// of its value (-1: padding; padding slots point at the row itself, padding
+// rows n..ld-1 are never read by the solves)
+template <typename CT>
+__global__ void k_tri_ell_build(int n, int w, long ld, const int *__restrict__ rp, const int *__restrict__ ci,
+                                const long *__restrict__ src, CT *ecol, long *esrc)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < ld; i += (long)gridDim.x * blockDim.x) {
+        const int k0 = i < n ? rp[i] : 0;
+        const int len = i < n ? rp[i + 1] - k0 : 0;
+        for (int k = 0; k < w; k++) {
+            int c = (int)(i < n ? i : 0);
+            long es = -1;
+            if (k < len) {
+                c = ci[k0 + k];
+                es = src[k0 + k];
+            }
+            if constexpr (sizeof(CT) == 2) ecol[(long)k * ld + i] = (CT)(i < n ? c - (int)i : 0);
+            else ecol[(long)k * ld + i] = (CT)c;
+            esrc[(long)k * ld + i] = es;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- host plan building
 // Host-side analysis of a triangular pattern.
 struct TriHostPlan {
@@ -461,6 +489,7 @@ struct TriHostPlan {
     std::vector<int> pci;   // dependency row per entry
     std::vector<long> src;  // source index of each entry in the value array
     std::vector<int> level; // per row
+    std::vector<int> lstart;  // first position of each level (nlevels + 1)
 };
 
 // rp/ci: CSR of the strict triangle (0-based); src_of(k) maps entry k of the
@@ -495,6 +524,7 @@ inline void tri_analyse(int n, const int *rp, const int *ci, bool upper, SrcF sr
     std::vector<int> cnt(h.nlevels + 1, 0);
     for (int i = 0; i < n; i++) cnt[h.level[i] + 1]++;
     for (int l = 0; l < h.nlevels; l++) cnt[l + 1] += cnt[l];
+    h.lstart.assign(cnt.begin(), cnt.end());
     h.perm.assign(n, 0);
     if (!upper)
         for (int i = 0; i < n; i++) h.perm[cnt[h.level[i]]++] = i;
@@ -603,6 +633,7 @@ struct TriDev {
     bool upper = false;
     DBuf<int> perm, prp, pci;
     DBuf<long> src;
+    DBuf<int> lstart;            // level-ordered layout: first position of each level
     DBuf<int> rp_nat, ci_nat;    // natural-order CSR of the triangle (Jacobi-sweep mode)
     DBuf<long> src_nat;
     DBuf<double> pv64, nv64;     // position-order and natural-order values (FP64)
@@ -718,6 +749,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
         T.pci.alloc(m); if (T.nnz) T.pci.upload(P.pci.data(), T.nnz, s);
         T.src.alloc(m); if (T.nnz) T.src.upload(P.src.data(), T.nnz, s);
+        T.lstart.alloc(P.nlevels + 1); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
     } else {
         TriChunkPlan C;
         tri_analyse_chunked(n, rp.data(), ci.data(), upper, src_of, chr, C);
@@ -740,36 +772,27 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     for (int i = 0; i < n; i++) w = std::max(w, rp[i + 1] - rp[i]);
     T.ell_w = 0;
     if (w > 0 && w <= 64 && (long)w * n <= 2 * std::max<long>(T.nnz, 1)) {
-        // layout of the operator's ELL copy: slot k of row i at k*ld + i;
-        // padding slots point at the row itself, padding rows are never read
-        const long ld = ell_ld(n);
-        const size_t m = (size_t)w * ld;
-        std::vector<int> ec(m, 0);
-        std::vector<long> es(m, -1);
-        for (int i = 0; i < n; i++) {
-            int k = 0;
-            for (int q = rp[i]; q < rp[i + 1]; q++, k++) {
-                ec[(size_t)k * ld + i] = ci[q];
-                es[(size_t)k * ld + i] = src_of(q);
-            }
-            for (; k < w; k++) ec[(size_t)k * ld + i] = i;
-        }
-        T.ell_w = w;
+        // layout of the operator's ELL copy, built on the device from the
+        // natural CSR just uploaded
         long maxoff = 0;
         for (int i = 0; i < n; i++)
             for (int q = rp[i]; q < rp[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci[q] - i));
+        T.ell_w = w;
         T.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
+        const long ld = ell_ld(n);
+        const size_t m = (size_t)w * ld;
+        T.esrc.alloc(m);
+        const int g = geom().sms * 4;
         if (T.ell16) {
-            std::vector<short> eo(m, 0);
-            for (int i = 0; i < n; i++)
-                for (int k = 0; k < w; k++) eo[(size_t)k * ld + i] = (short)(ec[(size_t)k * ld + i] - i);
-            T.eco.alloc(m); T.eco.upload(eo.data(), m, s);
+            T.eco.alloc(m);
             T.eci.free();
+            k_tri_ell_build<short><<<g, 256, 0, s>>>(n, w, ld, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, T.eco.p, T.esrc.p);
         } else {
-            T.eci.alloc(m); T.eci.upload(ec.data(), m, s);
+            T.eci.alloc(m);
             T.eco.free();
+            k_tri_ell_build<int><<<g, 256, 0, s>>>(n, w, ld, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, T.eci.p, T.esrc.p);
         }
-        T.esrc.alloc(m); T.esrc.upload(es.data(), m, s);
+        check_launch();
     }
     T.ticket.alloc(1);
     XS_CUDA(cudaStreamSynchronize(s));
@@ -790,6 +813,76 @@ inline void load_tri_ell(TriDev &T, const double *vals, bool need32, cudaStream_
         k_gather_convert_pad<__half><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.evh.p);
     }
     check_launch();
+}
+
+// ---------------------------------------------------------------- single-CTA LU solve
+// For small systems the cross-SM hand-off of the sync-free solve (a store
+// becoming visible in L2, then a poll) costs more per dependency level than
+// the level's work.  One CTA walks the levels instead: z = U'^-1 (dinv *
+// L^-1 x) with the whole solution vector in shared memory, a __syncthreads
+// between levels, the L result overwritten in place by the U result (a row's
+// own y value is read only by that row; its dependencies hold final z values
+// from earlier levels).  Row arithmetic and entry order are those of
+// trsv_row, so results are bitwise identical to the sync-free solve.  The
+// sync-free solve buffers are not touched (they stay armed).
+constexpr int LU_BLOCK_THREADS = 1024;
+constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
+
+template <typename VT, typename FT, typename DT>
+__global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_block(TrsvArgs<FT> L, const int *__restrict__ lstart, int nlL,
+                                                                TrsvArgs<FT> U, const int *__restrict__ ustart, int nlU,
+                                                                const DT *__restrict__ dinv, const VT *__restrict__ x,
+                                                                VT *__restrict__ z, const int *done_flag)
+{
+    extern __shared__ __align__(16) unsigned char lu_smem[];
+    VT *ys = (VT *)lu_smem;
+    if (done_flag && *done_flag) return;
+    for (int l = 0; l < nlL; l++) {
+        const int p1 = lstart[l + 1];
+        for (int p = lstart[l] + (int)threadIdx.x; p < p1; p += blockDim.x) {
+            const int row = __ldg(L.perm + p);
+            VT acc = x[row];
+            const int k1 = __ldg(L.prp + p + 1);
+            for (int k = __ldg(L.prp + p); k < k1; k++) acc = msub(acc, ys[__ldg(L.pci + k)], (VT)FVal<FT>::ld(L.pv, k));
+            ys[row] = acc;
+        }
+        __syncthreads();
+    }
+    for (int l = 0; l < nlU; l++) {
+        const int p1 = ustart[l + 1];
+        for (int p = ustart[l] + (int)threadIdx.x; p < p1; p += blockDim.x) {
+            const int row = __ldg(U.perm + p);
+            VT acc = ys[row] * (VT)__ldg(dinv + p);
+            const int k1 = __ldg(U.prp + p + 1);
+            for (int k = __ldg(U.prp + p); k < k1; k++) acc = msub(acc, ys[__ldg(U.pci + k)], (VT)FVal<FT>::ld(U.pv, k));
+            ys[row] = acc;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) z[i] = ys[i];
+}
+
+// whether the single-CTA solve serves this pair of plans for vectors of VT
+template <typename VT>
+inline bool lu_block_ok(const TriDev &L, const TriDev &U)
+{
+    const TrsvTuning &t = trsv_tuning();
+    return !L.chunked && !U.chunked && L.n > 0 && L.n <= t.block_max_rows &&
+           (size_t)L.n * sizeof(VT) <= LU_BLOCK_SMEM_MAX && L.lstart.p && U.lstart.p;
+}
+
+template <typename VT, typename FT, typename DT>
+inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, const VT *x, VT *z, const int *done_flag,
+                            cudaStream_t s)
+{
+    static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
+    const size_t smem = (size_t)L.n * sizeof(VT);
+    if (smem > attr) {
+        XS_CUDA(cudaFuncSetAttribute(k_lu_block<VT, FT, DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = smem;
+    }
+    k_lu_block<VT, FT, DT><<<1, LU_BLOCK_THREADS, smem, s>>>(L.args<FT>(), L.lstart.p, L.nlevels, U.args<FT>(),
+                                                              U.lstart.p, U.nlevels, dinv, x, z, done_flag);
 }
 
 template <typename VT, typename FT, typename DT, bool UPPER>
