@@ -306,10 +306,13 @@ int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
  * shared-memory one.  Environment XS_TRSV_BLOCK_ROWS sets it at first use. */
 int xs_set_trsv_block_rows(int max_rows);
 /* Column storage of ELL copies (the ELL SpMV and the Jacobi-sweep triangle
- * copies): index_bits 16 stores each column as a 16-bit offset from its row
- * whenever every |col - row| <= 32767 (default; halves the index bytes of
- * banded matrices), 32 always stores 32-bit columns.  Environment
- * XS_ELL_INDEX16=0 selects 32 at first use.  Applies to copies built later. */
+ * copies).  index_bits 0 (default): diagonal slots when every entry lies on
+ * one of at most 32 diagonals with at most 25% padding (stencil matrices):
+ * no index per entry, one presence mask per row; otherwise as 16.
+ * 16: each column as a 16-bit offset from its row whenever every
+ * |col - row| <= 32767, else as 32.  32: 32-bit columns.  Environment
+ * XS_ELL_DIAGONAL=0 / XS_ELL_INDEX16=0 turn the first two off at first use.
+ * Applies to copies built later. */
 int xs_set_ell_index_bits(int index_bits);
 
 /* library identification */

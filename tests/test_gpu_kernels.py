@@ -50,16 +50,32 @@ def _long_row_matrix():
     return st.CSRMatrix(n, rp, ci, v, "ragged")
 
 
+@pytest.fixture(params=[0, 16, 32], ids=["diag", "idx16", "idx32"])
+def ell_columns(request):
+    """ELL column storage for copies built inside the test: diagonal slots
+    (where the pattern allows), 16-bit row offsets, 32-bit columns."""
+    from xsolver_b200 import _lib
+
+    L = _lib.lib()
+    assert L.xs_set_ell_index_bits(request.param) == 0
+    yield request.param
+    L.xs_set_ell_index_bits(0)
+
+
 @pytest.mark.parametrize("fmt", ["csr", "ell"])
-def test_spmv_fp64_bitwise(cuda, fmt):
+def test_spmv_fp64_bitwise(cuda, fmt, ell_columns):
     import torch
     from xsolver_b200.api import Plan
 
+    if fmt == "csr" and ell_columns != 0:
+        pytest.skip("column storage only affects the ELL copy")
     for A in list(_matrices()) + ([_long_row_matrix()] if fmt == "csr" else []):
         P = Plan(A)
         if fmt == "ell":
             w = P.build_ell()
-            assert w == int(np.max(np.diff(A.rowptr)))
+            # diagonal slots: one slot per diagonal; otherwise the longest row
+            offs = np.unique(A.colidx - np.repeat(np.arange(A.n), np.diff(A.rowptr)))
+            assert w == (len(offs) if ell_columns == 0 else int(np.max(np.diff(A.rowptr))))
         x = st.rhs_uniform(A.n, 1)
         y = torch.zeros(A.n, dtype=torch.float64, device=cuda)
         P.spmv(_dev(x, cuda), y, fmt=fmt)
@@ -268,7 +284,7 @@ def _timeout_case(cuda, torch, Plan, XsError):
 
 
 @pytest.mark.parametrize("k", [1, 2, 3, 5])
-def test_jacobi_sweep_lusolve_matches_emulation(cuda, k):
+def test_jacobi_sweep_lusolve_matches_emulation(cuda, k, ell_columns):
     """The approximate solve of the reference GPU path (k Jacobi sweeps per
     triangle, DeviceMatrixCSR.cpp:281-304), ELL layout on the device, against
     a numpy emulation of the same sweeps on the oracle's factors."""

@@ -50,6 +50,7 @@ FormatTuning &format_tuning()
     static bool init = false;
     if (!init) {
         if (const char *e = getenv("XS_ELL_INDEX16")) t.ell_index16 = atoi(e) != 0;
+        if (const char *e = getenv("XS_ELL_DIAGONAL")) t.ell_dia = atoi(e) != 0;
         init = true;
     }
     return t;
@@ -120,47 +121,104 @@ void operator_ensure32(Operator &op, const int *rp0, cudaStream_t s)
     }
 }
 
+// Diagonal-slot eligibility of a CSR pattern: the ascending list of distinct
+// offsets c - row if there are at most ELL_DIA_MAX of them and the slots
+// would hold at most 25% padding; empty otherwise.
+std::vector<int> dia_offsets(int n, const int *rp, const int *ci)
+{
+    std::vector<int> offs;  // kept sorted
+    if (!format_tuning().ell_dia || n <= 0) return offs;
+    long nnz = (long)rp[n] - rp[0];
+    for (int i = 0; i < n; i++)
+        for (int q = rp[i]; q < rp[i + 1]; q++) {
+            const int o = ci[q] - i;
+            auto it = std::lower_bound(offs.begin(), offs.end(), o);
+            if (it == offs.end() || *it != o) {
+                offs.insert(it, o);
+                if ((int)offs.size() > ELL_DIA_MAX) return {};
+            }
+        }
+    if ((long)offs.size() * n > nnz + nnz / 4) return {};
+    return offs;
+}
+
 void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const double *v, int, bool want32, cudaStream_t s)
 {
     int n = op.n, w = 0;
     for (int i = 0; i < n; i++) w = std::max(w, rp0[i + 1] - rp0[i]);
-    op.ell_w = w;
-    long maxoff = 0;
-    for (int i = 0; i < n; i++)
-        for (int q = rp0[i]; q < rp0[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci0[q] - i));
-    op.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
     const long ld = ell_ld(n);
-    const size_t m = (size_t)w * ld;
-    // padding slots of a row point at the row itself (offset 0) with value 0;
-    // padding rows n..ld-1 are never gathered
-    std::vector<int> c(m, 0);
-    std::vector<double> vv(m, 0.0);
-    for (int i = 0; i < n; i++) {
-        int k = 0;
-        for (int q = rp0[i]; q < rp0[i + 1]; q++, k++) {
-            c[(size_t)k * ld + i] = ci0[q];
-            vv[(size_t)k * ld + i] = v[q];
-        }
-        for (; k < w; k++) c[(size_t)k * ld + i] = i;
-    }
-    if (op.ell16) {
-        std::vector<short> o(m, 0);
+    const std::vector<int> offs = dia_offsets(n, rp0, ci0);
+    op.ell_dia = !offs.empty();
+    op.eci.free();
+    op.eco.free();
+    op.emask8.free();
+    op.emask32.free();
+    op.doff.free();
+    if (op.ell_dia) {
+        // slot = diagonal; mask bit k = slot k present in the row
+        w = (int)offs.size();
+        op.ell_w = w;
+        op.ell16 = false;
+        const size_t m = (size_t)w * ld;
+        std::vector<double> vv(m, 0.0);
+        std::vector<uint32_t> mask(ld, 0u);
         for (int i = 0; i < n; i++)
-            for (int k = 0; k < w; k++) o[(size_t)k * ld + i] = (short)(c[(size_t)k * ld + i] - i);
-        op.eco.alloc(m);
-        op.eco.upload(o.data(), m, s);
-        op.eci.free();
+            for (int q = rp0[i]; q < rp0[i + 1]; q++) {
+                const int k = (int)(std::lower_bound(offs.begin(), offs.end(), ci0[q] - i) - offs.begin());
+                vv[(size_t)k * ld + i] = v[q];
+                mask[i] |= 1u << k;
+            }
+        op.doff.alloc(w);
+        op.doff.upload(offs.data(), w, s);
+        if (w <= 8) {
+            std::vector<uint8_t> m8(mask.begin(), mask.end());
+            op.emask8.alloc(ld);
+            op.emask8.upload(m8.data(), ld, s);
+        } else {
+            op.emask32.alloc(ld);
+            op.emask32.upload(mask.data(), ld, s);
+        }
+        op.ev.alloc(m);
+        op.ev.upload(vv.data(), m, s);
     } else {
-        op.eci.alloc(m);
-        op.eci.upload(c.data(), m, s);
-        op.eco.free();
+        op.ell_w = w;
+        long maxoff = 0;
+        for (int i = 0; i < n; i++)
+            for (int q = rp0[i]; q < rp0[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci0[q] - i));
+        op.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
+        const size_t m = (size_t)w * ld;
+        // padding slots of a row point at the row itself (offset 0) with
+        // value 0; padding rows n..ld-1 are never gathered
+        std::vector<int> c(m, 0);
+        std::vector<double> vv(m, 0.0);
+        for (int i = 0; i < n; i++) {
+            int k = 0;
+            for (int q = rp0[i]; q < rp0[i + 1]; q++, k++) {
+                c[(size_t)k * ld + i] = ci0[q];
+                vv[(size_t)k * ld + i] = v[q];
+            }
+            for (; k < w; k++) c[(size_t)k * ld + i] = i;
+        }
+        if (op.ell16) {
+            std::vector<short> o(m, 0);
+            for (int i = 0; i < n; i++)
+                for (int k = 0; k < w; k++) o[(size_t)k * ld + i] = (short)(c[(size_t)k * ld + i] - i);
+            op.eco.alloc(m);
+            op.eco.upload(o.data(), m, s);
+        } else {
+            op.eci.alloc(m);
+            op.eci.upload(c.data(), m, s);
+        }
+        op.ev.alloc(m);
+        op.ev.upload(vv.data(), m, s);
     }
-    op.ev.alloc(m);
-    op.ev.upload(vv.data(), m, s);
     if (want32) {
+        const long m = (long)op.ell_w * ld;
         op.ev32.alloc(m);
-        k_convert_f32<<<geom().sms * 4, 256, 0, s>>>((long)m, op.ev.p, op.ev32.p);
+        k_convert_f32<<<geom().sms * 4, 256, 0, s>>>(m, op.ev.p, op.ev32.p);
         check_launch();
+    } else {
+        op.ev32.free();
     }
     op.ell_grid = (int)std::min<long>((long)geom().sms * ELL_BLOCKS_PER_SM, (n + 256L * ELL_ROWS - 1) / (256L * ELL_ROWS));
     if (op.ell_grid < 1) op.ell_grid = 1;
@@ -169,15 +227,27 @@ void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const doub
 
 // new values for an existing ELL copy: slot k of row r is the row's k-th
 // CSR entry (0 past the row's end), as operator_build_ell lays it out
-__global__ void k_ell_refill(int n, int w, long ld, const int *__restrict__ rp, const double *__restrict__ v,
-                             double *ev, float *ev32)
+// (diagonal slots, doff != null: the entry at column c goes to the slot of
+// offset c - r; absent slots keep 0)
+__global__ void k_ell_refill(int n, int w, long ld, const int *__restrict__ rp, const int *__restrict__ ci,
+                             const double *__restrict__ v, const int *__restrict__ doff, double *ev, float *ev32)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         const int k0 = rp[r], len = rp[r + 1] - k0;
-        for (int k = 0; k < w; k++) {
-            const double val = k < len ? v[k0 + k] : 0.0;
-            ev[(long)k * ld + r] = val;
-            if (ev32) ev32[(long)k * ld + r] = (float)val;
+        if (!doff) {
+            for (int k = 0; k < w; k++) {
+                const double val = k < len ? v[k0 + k] : 0.0;
+                ev[(long)k * ld + r] = val;
+                if (ev32) ev32[(long)k * ld + r] = (float)val;
+            }
+        } else {
+            for (int q = 0; q < len; q++) {
+                const int off = ci[k0 + q] - r;
+                int k = 0;
+                while (k < w - 1 && doff[k] != off) k++;
+                ev[(long)k * ld + r] = v[k0 + q];
+                if (ev32) ev32[(long)k * ld + r] = (float)v[k0 + q];
+            }
         }
     }
 }
@@ -361,7 +431,8 @@ static void update_values(Handle &h, const double *v)
     }
     if (h.A.ell_w > 0) {
         if (h.A.v32.p && !h.A.ev32.p) h.A.ev32.alloc((size_t)h.A.ell_w * ell_ld(h.n));
-        k_ell_refill<<<geom().sms * 4, 256, 0, h.s>>>(h.n, h.A.ell_w, ell_ld(h.n), h.A.rp.p, h.A.v.p, h.A.ev.p,
+        k_ell_refill<<<geom().sms * 4, 256, 0, h.s>>>(h.n, h.A.ell_w, ell_ld(h.n), h.A.rp.p, h.A.ci.p, h.A.v.p,
+                                                      h.A.ell_dia ? h.A.doff.p : nullptr, h.A.ev.p,
                                                       h.A.v32.p ? h.A.ev32.p : nullptr);
         check_launch();
     }
@@ -1063,8 +1134,9 @@ int xs_set_trsv_block_rows(int max_rows)
 int xs_set_ell_index_bits(int bits)
 {
     return guarded([&] {
-        if (bits != 16 && bits != 32) throw Status(XS_ERR_INVALID);
-        format_tuning().ell_index16 = bits == 16;
+        if (bits != 0 && bits != 16 && bits != 32) throw Status(XS_ERR_INVALID);
+        format_tuning().ell_dia = bits == 0;
+        format_tuning().ell_index16 = bits != 32;
     });
 }
 
@@ -1589,8 +1661,11 @@ void gpu_mat_format(char *fmt, int *num_nz)
         else if (*num_nz > 16 && *num_nz <= 32) *num_nz = 32;
         else throw Status(XS_ERR_ELL_WIDTH);
         Handle &H = *g_gpu->h;
+        // the reference's limit is on the longest row (its ELL width)
+        int wmax = 0;
+        for (int i = 0; i < H.n; i++) wmax = std::max(wmax, H.hrp[i + 1] - H.hrp[i]);
+        if (wmax > *num_nz) throw Status(XS_ERR_ELL_WIDTH);
         operator_build_ell(H.A, H.hrp.data(), H.hci.data(), host_vals(H), 0, H.A.v32.p != nullptr, H.s);
-        if (H.A.ell_w > *num_nz) throw Status(XS_ERR_ELL_WIDTH);
         H.A.format = 1;
         H.format = 1;
     });

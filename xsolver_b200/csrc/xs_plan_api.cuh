@@ -282,10 +282,17 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
         const double I = 4.0;
         switch (op) {
         case 0: *bytes = (8 + I) * nnz + I * (n + 1) + 8 * n + 8 * n; break;
-        // ELL: stored entries (padding included) with the stored index width
-        case 1: *bytes = (8 + (h.A.ell16 ? 2.0 : I)) * h.A.ell_w * n + 2 * 8 * n; break;
+        // ELL: stored slots (padding included) with the stored column data:
+        // a 32- or 16-bit index per slot, or (diagonal slots) no index and
+        // one mask per row
+        case 1: case 6: {
+            const double V = op == 1 ? 8.0 : 4.0;
+            const double slot = h.A.ell_dia ? V : V + (h.A.ell16 ? 2.0 : I);
+            const double row = h.A.ell_dia ? (h.A.ell_w <= 8 ? 1.0 : 4.0) : 0.0;
+            *bytes = slot * h.A.ell_w * n + row * n + 2 * V * n;
+            break;
+        }
         case 2: *bytes = (4 + I) * nnz + I * (n + 1) + 4 * n + 4 * n; break;
-        case 6: *bytes = (4 + (h.A.ell16 ? 2.0 : I)) * h.A.ell_w * n + 2 * 4 * n; break;
         case 3: case 4: case 5: {
             if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
             const int fp = h.M.factor_prec;
@@ -304,10 +311,15 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
                 // the triangle's entries (index width of the copy in use); the
                 // first pass reads x (L) or x and dinv (U) and writes its
                 // iterate, every later pass also reads the previous iterate.
-                const double IL = (h.M.L.ell_w > 0 && h.M.L.ell16) ? 2.0 : I;
-                const double IU = (h.M.U.ell_w > 0 && h.M.U.ell16) ? 2.0 : I;
-                const double l = (k - 1) * (V + IL) * h.M.L.nnz + 2 * X * n + (k - 2) * 3 * X * n;
-                const double u = (k - 1) * (V + IU) * h.M.U.nnz + 3 * X * n + (k - 2) * 4 * X * n;
+                auto idx = [&](const TriDev &T) {  // index bytes per entry
+                    return T.ell_w > 0 && T.ell_dia ? 0.0 : (T.ell_w > 0 && T.ell16 ? 2.0 : I);
+                };
+                auto msk = [&](const TriDev &T) {  // mask bytes per row
+                    return T.ell_w > 0 && T.ell_dia ? (T.ell_w <= 8 ? 1.0 : 4.0) : 0.0;
+                };
+                const TriDev &Lt = h.M.L, &Ut = h.M.U;
+                const double l = (k - 1) * ((V + idx(Lt)) * Lt.nnz + msk(Lt) * n) + 2 * X * n + (k - 2) * 3 * X * n;
+                const double u = (k - 1) * ((V + idx(Ut)) * Ut.nnz + msk(Ut) * n) + 3 * X * n + (k - 2) * 4 * X * n;
                 *bytes = op == 3 ? l : (op == 4 ? u : l + u);
             }
             break;

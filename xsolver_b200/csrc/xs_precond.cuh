@@ -172,17 +172,23 @@ struct PrecondDev {
         auto pass = [&](const TriDev &T, bool upper, bool first2, const VT *rhs, const VT *yin, VT *yout) {
             if (T.ell_w > 0) {
                 const FT *ev = T.evals<FT>();
+                const int *doff = T.doff.p;
+                const int gs = std::max(1, std::min(g * ELL_ROWS / ell_rows_for<FT>(),
+                                                    (n + 256 * ell_rows_for<FT>() - 1) / (256 * ell_rows_for<FT>())));
                 auto go = [&](auto cols) {
                     using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
+                    const DT *dv = upper ? dinv : (const DT *)nullptr;
                     if (upper) {
-                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, true, true><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, dinv, rhs, yin, yout, done_flag);
-                        else k_trsv_sweep_ell<VT, FT, DT, CT, true, false><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, dinv, rhs, yin, yout, done_flag);
+                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, true, true><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        else k_trsv_sweep_ell<VT, FT, DT, CT, true, false><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
                     } else {
-                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, false, true><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
-                        else k_trsv_sweep_ell<VT, FT, DT, CT, false, false><<<g, 256, 0, s>>>(n, T.ell_w, cols, ev, (const DT *)nullptr, rhs, yin, yout, done_flag);
+                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, false, true><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        else k_trsv_sweep_ell<VT, FT, DT, CT, false, false><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
                     }
                 };
-                if (T.ell16) go((const short *)T.eco.p);
+                if (T.ell_dia && T.ell_w <= 8) go((const uint8_t *)T.emask8.p);
+                else if (T.ell_dia) go((const uint32_t *)T.emask32.p);
+                else if (T.ell16) go((const short *)T.eco.p);
                 else go((const int *)T.eci.p);
             } else {
                 // CSR: the first sweep is a separate pass (yin = null -> y_1)

@@ -20,6 +20,7 @@
 //   entries point at the row itself with value 0.  Consecutive threads read
 //   consecutive addresses for every k.
 #pragma once
+#include <type_traits>
 #include "xs_internal.cuh"
 
 namespace xs {
@@ -226,9 +227,22 @@ __global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const
 }
 
 // ---------------------------------------------------------------- ELL kernel
-// Column storage of an ELL copy: CT = int holds absolute columns, CT = short
-// holds the offset c - row (used when every |c - row| <= 32767, as for
-// stencil and other banded matrices: 2 index bytes per entry instead of 4).
+// Column storage of an ELL copy, chosen per matrix when it is built:
+//   CT = int       absolute column per slot
+//   CT = short     offset c - row per slot (every |c - row| <= 32767, as for
+//                  banded matrices: 2 index bytes per entry instead of 4)
+//   CT = uint8_t / uint32_t   diagonal slots: every entry lies on one of at
+//                  most 8 / 32 fixed diagonals (stencil matrices), slot k
+//                  holds the entry at column row + off[k] (offsets ascending,
+//                  so slot order is entry order) and the per-row bit mask in
+//                  ci says which slots are present.  No per-entry index is
+//                  stored and a gather address is known before any load.
+template <typename CT>
+struct EllDiag {
+    static constexpr bool value = std::is_same<CT, uint8_t>::value || std::is_same<CT, uint32_t>::value;
+};
+constexpr int ELL_DIA_MAX = 32;
+
 template <typename CT>
 __device__ __forceinline__ int ell_col(CT c, int row)
 {
@@ -246,9 +260,21 @@ template <typename MT, typename CT>
 struct EllArgs {
     int n, w;
     long ld;
-    const CT *ci;
+    const CT *ci;     // columns / offsets per slot, or the per-row masks (diagonal slots)
     const MT *v;
+    const int *doff;  // diagonal slots: the w offsets
 };
+
+// the diagonal offsets of a launch, staged in shared memory (slot index is
+// not a compile-time constant inside the chunk loop)
+template <typename CT>
+__device__ __forceinline__ void ell_stage_offsets(const int *doff, int w, int *s_off)
+{
+    if constexpr (EllDiag<CT>::value) {
+        if (threadIdx.x < (unsigned)w) s_off[threadIdx.x] = doff[threadIdx.x];
+        __syncthreads();
+    }
+}
 
 // Launch shape of the ELL kernels (SpMV and the Jacobi-sweep triangle
 // kernels): CTAs of 256 threads, ELL_MIN_BLOCKS of them resident per SM,
@@ -279,6 +305,13 @@ constexpr int ELL_ROWS = XS_ELL_ROWS;
 constexpr int ELL_CHUNK = XS_ELL_CHUNK;
 static_assert(ELL_ROWS == 1 || ELL_ROWS == 2 || ELL_ROWS == 4 || ELL_ROWS == 8, "rows per thread");
 static_assert(ELL_LD_ALIGN % ELL_ROWS == 0, "row vectors must stay aligned");
+// rows per thread for values of type MT: one row for 8-byte values (two
+// rows of FP64 chunks do not fit the register budget without spilling)
+template <typename MT>
+__host__ __device__ constexpr int ell_rows_for()
+{
+    return sizeof(MT) >= 8 ? 1 : ELL_ROWS;
+}
 
 // R consecutive elements starting at an R-aligned index, one vector load
 // (two for 32 bytes) through the read-only path
@@ -286,7 +319,10 @@ template <int R, typename T>
 __device__ __forceinline__ void ld_vec(const T *p, T (&o)[R])
 {
     constexpr int B = R * (int)sizeof(T);
-    if constexpr (B == 2) {
+    if constexpr (B == 1) {
+        unsigned char u = __ldg((const unsigned char *)p);
+        memcpy(o, &u, 1);
+    } else if constexpr (B == 2) {
         unsigned short u = __ldg((const unsigned short *)p);
         memcpy(o, &u, 2);
     } else if constexpr (B == 4) {
@@ -308,46 +344,74 @@ __device__ __forceinline__ void ld_vec(const T *p, T (&o)[R])
     }
 }
 
-// C consecutive slots of rows r0..r0+R-1: slot loads, then the gathers of x,
-// then the per-row sums in slot order (each row's sum stays in entry order).
+// C consecutive slots (k0 .. k0+C-1) of rows r0..r0+R-1: slot loads, then
+// the gathers of x, then the per-row sums in slot order (each row's sum stays
+// in entry order; a slot absent from a row adds nothing).
 template <int C, int R, typename VT, typename MT, typename CT>
 __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld, const VT *__restrict__ x, int r0,
-                                          int n, double (&sum)[R])
+                                          int n, int k0, const CT (&mask)[R], const int *s_off, double (&sum)[R])
 {
-    CT c[C][R];
     MT v[C][R];
     VT xv[C][R];
+    if constexpr (EllDiag<CT>::value) {
 #pragma unroll
-    for (int j = 0; j < C; j++) {
-        ld_vec<R>(cp, c[j]);
-        ld_vec<R>(vp, v[j]);
-        cp += ld;
-        vp += ld;
+        for (int j = 0; j < C; j++) {
+            ld_vec<R>(vp, v[j]);
+            vp += ld;
+        }
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+            const int off = s_off[k0 + j];
+#pragma unroll
+            for (int q = 0; q < R; q++)
+                xv[j][q] = ((mask[q] >> (k0 + j)) & 1u) ? __ldg(x + (r0 + q + off)) : (VT)0;
+        }
+#pragma unroll
+        for (int j = 0; j < C; j++)
+#pragma unroll
+            for (int q = 0; q < R; q++)
+                if ((mask[q] >> (k0 + j)) & 1u) sum[q] += (double)v[j][q] * (double)xv[j][q];
+    } else {
+        CT c[C][R];
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+            ld_vec<R>(cp, c[j]);
+            ld_vec<R>(vp, v[j]);
+            cp += ld;
+            vp += ld;
+        }
+#pragma unroll
+        for (int j = 0; j < C; j++)
+#pragma unroll
+            for (int q = 0; q < R; q++)
+                xv[j][q] = (R == 1 || r0 + q < n) ? __ldg(x + ell_col<CT>(c[j][q], r0 + q)) : (VT)0;
+#pragma unroll
+        for (int j = 0; j < C; j++)
+#pragma unroll
+            for (int q = 0; q < R; q++) sum[q] += (double)v[j][q] * (double)xv[j][q];
     }
-#pragma unroll
-    for (int j = 0; j < C; j++)
-#pragma unroll
-        for (int q = 0; q < R; q++) xv[j][q] = (R == 1 || r0 + q < n) ? __ldg(x + ell_col<CT>(c[j][q], r0 + q)) : (VT)0;
-#pragma unroll
-    for (int j = 0; j < C; j++)
-#pragma unroll
-        for (int q = 0; q < R; q++) sum[q] += (double)v[j][q] * (double)xv[j][q];
 }
 
 template <int R, typename VT, typename MT, typename CT>
 __device__ __forceinline__ void ell_rows(const CT *cp, const MT *vp, int w, long ld, const VT *__restrict__ x, int r0,
-                                         int n, double (&sum)[R])
+                                         int n, const int *s_off, double (&sum)[R])
 {
+    CT mask[R];
+    if constexpr (EllDiag<CT>::value) {
+        ld_vec<R>(cp, mask);  // cp points at the row's mask (padding rows: 0)
+    }
     for (int k0 = 0; k0 < w; k0 += ELL_CHUNK) {
         const int m = min(ELL_CHUNK, w - k0);  // warp-uniform
-        if (m == ELL_CHUNK) ell_chunk<ELL_CHUNK, R>(cp, vp, ld, x, r0, n, sum);
-        else if (ELL_CHUNK > 7 && m == 7) ell_chunk<7, R>(cp, vp, ld, x, r0, n, sum);
-        else if (ELL_CHUNK > 6 && m == 6) ell_chunk<6, R>(cp, vp, ld, x, r0, n, sum);
-        else if (ELL_CHUNK > 5 && m == 5) ell_chunk<5, R>(cp, vp, ld, x, r0, n, sum);
-        else if (ELL_CHUNK > 4 && m == 4) ell_chunk<4, R>(cp, vp, ld, x, r0, n, sum);
-        else if (ELL_CHUNK > 3 && m == 3) ell_chunk<3, R>(cp, vp, ld, x, r0, n, sum);
-        else if (ELL_CHUNK > 2 && m == 2) ell_chunk<2, R>(cp, vp, ld, x, r0, n, sum);
-        else ell_chunk<1, R>(cp, vp, ld, x, r0, n, sum);
+#define XS_ELL_CHUNK_CALL(CC) ell_chunk<CC, R>(cp, vp, ld, x, r0, n, k0, mask, s_off, sum)
+        if (m == ELL_CHUNK) XS_ELL_CHUNK_CALL(ELL_CHUNK);
+        else if (ELL_CHUNK > 7 && m == 7) XS_ELL_CHUNK_CALL(7);
+        else if (ELL_CHUNK > 6 && m == 6) XS_ELL_CHUNK_CALL(6);
+        else if (ELL_CHUNK > 5 && m == 5) XS_ELL_CHUNK_CALL(5);
+        else if (ELL_CHUNK > 4 && m == 4) XS_ELL_CHUNK_CALL(4);
+        else if (ELL_CHUNK > 3 && m == 3) XS_ELL_CHUNK_CALL(3);
+        else if (ELL_CHUNK > 2 && m == 2) XS_ELL_CHUNK_CALL(2);
+        else XS_ELL_CHUNK_CALL(1);
+#undef XS_ELL_CHUNK_CALL
     }
 }
 
@@ -356,9 +420,11 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_ell_spmv(EllArgs<MT, CT
                                                                    VT *__restrict__ y, Epi epi, RedSlot slot)
 {
     constexpr int KK = Epi::K > 0 ? Epi::K : 1;
-    constexpr int R = ELL_ROWS;
+    constexpr int R = ell_rows_for<MT>();
     if (!epi.active()) return;
     __shared__ double tot[KK];
+    __shared__ int s_off[ELL_DIA_MAX];
+    ell_stage_offsets<CT>(A.doff, A.w, s_off);
     double acc[KK];
 #pragma unroll
     for (int k = 0; k < KK; k++) acc[k] = 0.0;
@@ -367,7 +433,7 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_ell_spmv(EllArgs<MT, CT
         double sum[R];
 #pragma unroll
         for (int q = 0; q < R; q++) sum[q] = 0.0;
-        ell_rows<R, VT, MT, CT>(A.ci + r0, A.v + r0, A.w, A.ld, x, r0, n, sum);
+        ell_rows<R, VT, MT, CT>(A.ci + r0, A.v + r0, A.w, A.ld, x, r0, n, s_off, sum);
 #pragma unroll
         for (int q = 0; q < R; q++) {
             const int r = r0 + q;
@@ -397,11 +463,16 @@ struct Operator {
     DBuf<float> v32;
     SpmvTiling tile64, tile32;
     int grid64 = 0, grid32 = 0;  // persistent grid sizes
-    // ELL (columns in eci, or as 16-bit row offsets in eco when ell16)
+    // ELL: columns in eci, 16-bit row offsets in eco (ell16), or diagonal
+    // slots (ell_dia: offsets in doff, per-row masks in emask8 / emask32)
     int ell_w = 0;
     bool ell16 = false;
+    bool ell_dia = false;
     DBuf<int> eci;
     DBuf<short> eco;
+    DBuf<int> doff;
+    DBuf<uint8_t> emask8;
+    DBuf<uint32_t> emask32;
     DBuf<double> ev;
     DBuf<float> ev32;
     int ell_grid = 0;
@@ -421,8 +492,12 @@ struct Operator {
         const MT *vals;
         if constexpr (std::is_same<MT, double>::value) vals = ev.p;
         else vals = ev32.p;
-        if constexpr (sizeof(CT) == 2) return EllArgs<MT, CT>{n, ell_w, ell_ld(n), eco.p, vals};
-        else return EllArgs<MT, CT>{n, ell_w, ell_ld(n), eci.p, vals};
+        const CT *c;
+        if constexpr (std::is_same<CT, uint8_t>::value) c = emask8.p;
+        else if constexpr (std::is_same<CT, uint32_t>::value) c = emask32.p;
+        else if constexpr (sizeof(CT) == 2) c = eco.p;
+        else c = eci.p;
+        return EllArgs<MT, CT>{n, ell_w, ell_ld(n), c, vals, doff.p};
     }
 };
 
@@ -527,8 +602,12 @@ inline void launch_csr(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot 
 template <typename VT, typename MT, typename Epi>
 inline void launch_ell(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot slot, cudaStream_t s)
 {
-    int g = op.ell_grid;
-    if (op.ell16) k_ell_spmv<VT, MT, short, Epi><<<g, 256, 0, s>>>(op.ell<MT, short>(), x, y, epi, slot);
+    // the grid covers the rows at ell_rows_for<MT>() rows per thread
+    const int g = (int)std::min<long>((long)op.ell_grid * ELL_ROWS / ell_rows_for<MT>(),
+                                      (op.n + 256L * ell_rows_for<MT>() - 1) / (256L * ell_rows_for<MT>()));
+    if (op.ell_dia && op.ell_w <= 8) k_ell_spmv<VT, MT, uint8_t, Epi><<<g, 256, 0, s>>>(op.ell<MT, uint8_t>(), x, y, epi, slot);
+    else if (op.ell_dia) k_ell_spmv<VT, MT, uint32_t, Epi><<<g, 256, 0, s>>>(op.ell<MT, uint32_t>(), x, y, epi, slot);
+    else if (op.ell16) k_ell_spmv<VT, MT, short, Epi><<<g, 256, 0, s>>>(op.ell<MT, short>(), x, y, epi, slot);
     else k_ell_spmv<VT, MT, int, Epi><<<g, 256, 0, s>>>(op.ell<MT, int>(), x, y, epi, slot);
     check_launch();
 }

@@ -62,12 +62,17 @@ __device__ __forceinline__ float msub(float acc, float y, float v) { return __fm
 //                  no persistence)
 //   backoff_ns     upper bound of the exponential back-off between polls of a
 //                  pending dependency (0: spin without sleeping)
-// ELL column storage: 1 = 16-bit row offsets whenever they fit (default),
-// 0 = always 32-bit columns.  Applies to ELL copies built afterwards.
+// ELL column storage: diagonal slots when the pattern lies on few diagonals
+// (ell_dia), else 16-bit row offsets whenever they fit (ell_index16), else
+// 32-bit columns.  Applies to ELL copies built afterwards.
 struct FormatTuning {
     int ell_index16 = 1;
+    int ell_dia = 1;  // diagonal slots when the pattern has few diagonals
 };
 FormatTuning &format_tuning();
+// ascending distinct diagonal offsets of a CSR pattern if it qualifies for
+// diagonal ELL slots (at most ELL_DIA_MAX, at most 25% padding), else empty
+std::vector<int> dia_offsets(int n, const int *rp, const int *ci);
 
 struct TrsvTuning {
     int blocks_per_sm = 2;
@@ -363,28 +368,51 @@ __global__ void k_trsv_sweep(int n, const int *__restrict__ rp, const int *__res
 // C consecutive slots of rows i0..i0+R-1 of a sweep pass: acc -= v * y(c),
 // with y(c) = x[c] (L, first pass), dinv[c]*x[c] (U, first pass) or yin[c].
 template <int C, int R, typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
-__device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long ld, int i0, int n,
-                                            const DT *__restrict__ dinv, const VT *__restrict__ x,
-                                            const VT *__restrict__ yin, VT (&acc)[R])
+__device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long ld, int i0, int n, int k0,
+                                            const CT (&mask)[R], const int *s_off, const DT *__restrict__ dinv,
+                                            const VT *__restrict__ x, const VT *__restrict__ yin, VT (&acc)[R])
 {
-    CT c[C][R];
     FT v[C][R];
     VT y[C][R];
+    bool pr[C][R];
+    int col[C][R];
+    if constexpr (EllDiag<CT>::value) {
 #pragma unroll
-    for (int j = 0; j < C; j++) {
-        ld_vec<R>(cp, c[j]);
-        ld_vec<R>(vp, v[j]);
-        cp += ld;
-        vp += ld;
+        for (int j = 0; j < C; j++) {
+            ld_vec<R>(vp, v[j]);
+            vp += ld;
+            const int off = s_off[k0 + j];
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                pr[j][q] = (mask[q] >> (k0 + j)) & 1u;
+                col[j][q] = i0 + q + off;
+            }
+        }
+    } else {
+        CT c[C][R];
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+            ld_vec<R>(cp, c[j]);
+            ld_vec<R>(vp, v[j]);
+            cp += ld;
+            vp += ld;
+        }
+#pragma unroll
+        for (int j = 0; j < C; j++)
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                pr[j][q] = R == 1 || i0 + q < n;
+                col[j][q] = ell_col<CT>(c[j][q], i0 + q);
+            }
     }
 #pragma unroll
     for (int j = 0; j < C; j++)
 #pragma unroll
         for (int q = 0; q < R; q++) {
-            if (R == 1 || i0 + q < n) {
-                const int col = ell_col<CT>(c[j][q], i0 + q);
-                if (FIRST2) y[j][q] = UPPER ? (VT)(__ldg(x + col) * (VT)__ldg(dinv + col)) : __ldg(x + col);
-                else y[j][q] = __ldg(yin + col);
+            if (pr[j][q]) {
+                const int cc = col[j][q];
+                if (FIRST2) y[j][q] = UPPER ? (VT)(__ldg(x + cc) * (VT)__ldg(dinv + cc)) : __ldg(x + cc);
+                else y[j][q] = __ldg(yin + cc);
             } else {
                 y[j][q] = (VT)0;
             }
@@ -392,7 +420,8 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
 #pragma unroll
     for (int j = 0; j < C; j++)
 #pragma unroll
-        for (int q = 0; q < R; q++) acc[q] = msub(acc[q], y[j][q], (VT)FVal<FT>::cvt(v[j][q]));
+        for (int q = 0; q < R; q++)
+            if (!EllDiag<CT>::value || pr[j][q]) acc[q] = msub(acc[q], y[j][q], (VT)FVal<FT>::cvt(v[j][q]));
 }
 
 // Jacobi sweeps on a column-major ELL copy of the triangle (natural order,
@@ -403,14 +432,17 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
 // per load chunk, warp-uniform chunk lengths).
 template <typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
 __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, int w, const CT *__restrict__ eci,
+                                                                         const int *__restrict__ doff,
                                                                          const FT *__restrict__ ev,
                                                                          const DT *__restrict__ dinv,
                                                                          const VT *__restrict__ x,
                                                                          const VT *__restrict__ yin,
                                                                          VT *__restrict__ yout, const int *done_flag)
 {
-    constexpr int R = ELL_ROWS;
+    constexpr int R = ell_rows_for<FT>();
     if (done_flag && *done_flag) return;
+    __shared__ int s_off[ELL_DIA_MAX];
+    ell_stage_offsets<CT>(doff, w, s_off);
     const long ld = ell_ld(n);
     for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * R; i0 < n; i0 += gridDim.x * blockDim.x * R) {
         VT acc[R];
@@ -421,9 +453,12 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, i
         }
         const CT *cp = eci + i0;
         const FT *vp = ev + i0;
+        CT mask[R];
+        if constexpr (EllDiag<CT>::value) ld_vec<R>(cp, mask);
         for (int k0 = 0; k0 < w; k0 += ELL_CHUNK) {
             const int m = min(ELL_CHUNK, w - k0);  // warp-uniform
-#define XS_SWEEP_CHUNK(CC) sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, ld, i0, n, dinv, x, yin, acc)
+#define XS_SWEEP_CHUNK(CC) \
+    sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, ld, i0, n, k0, mask, s_off, dinv, x, yin, acc)
             if (m == ELL_CHUNK) XS_SWEEP_CHUNK(ELL_CHUNK);
             else if (ELL_CHUNK > 7 && m == 7) XS_SWEEP_CHUNK(7);
             else if (ELL_CHUNK > 6 && m == 6) XS_SWEEP_CHUNK(6);
@@ -476,6 +511,28 @@ __global__ void k_tri_ell_build(int n, int w, long ld, const int *__restrict__ r
             else ecol[(long)k * ld + i] = (CT)c;
             esrc[(long)k * ld + i] = es;
         }
+    }
+}
+
+// diagonal-slot copy of a triangle: per-row slot mask and the source index
+// of each slot's value (-1: absent; padding rows have mask 0)
+template <typename MaskT>
+__global__ void k_tri_dia_build(int n, int D, long ld, const int *__restrict__ rp, const int *__restrict__ ci,
+                                const long *__restrict__ src, const int *__restrict__ doff, MaskT *mask, long *esrc)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < ld; i += (long)gridDim.x * blockDim.x) {
+        for (int k = 0; k < D; k++) esrc[(long)k * ld + i] = -1;
+        uint32_t m = 0;
+        if (i < n) {
+            for (int q = rp[i]; q < rp[i + 1]; q++) {
+                const int off = ci[q] - (int)i;
+                int k = 0;
+                while (k < D - 1 && doff[k] != off) k++;
+                esrc[(long)k * ld + i] = src[q];
+                m |= 1u << k;
+            }
+        }
+        mask[i] = (MaskT)m;
     }
 }
 
@@ -647,9 +704,13 @@ struct TriDev {
     DBuf<unsigned> ticket;
     // natural-order ELL copy for the Jacobi-sweep mode (ell_w = 0: none)
     int ell_w = 0;
-    bool ell16 = false;  // columns as 16-bit row offsets in eco
+    bool ell16 = false;    // columns as 16-bit row offsets in eco
+    bool ell_dia = false;  // diagonal slots: offsets in doff, per-row masks in emask8 / emask32
     DBuf<int> eci;
     DBuf<short> eco;
+    DBuf<int> doff;
+    DBuf<uint8_t> emask8;
+    DBuf<uint32_t> emask32;
     DBuf<long> esrc;
     DBuf<double> ev64;
     DBuf<float> ev32;
@@ -771,7 +832,28 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     int w = 0;
     for (int i = 0; i < n; i++) w = std::max(w, rp[i + 1] - rp[i]);
     T.ell_w = 0;
-    if (w > 0 && w <= 64 && (long)w * n <= 2 * std::max<long>(T.nnz, 1)) {
+    const std::vector<int> offs = w > 0 ? dia_offsets(n, rp.data(), ci.data()) : std::vector<int>();
+    T.ell_dia = !offs.empty();
+    if (T.ell_dia) {
+        // diagonal slots, built on the device from the natural CSR
+        const int D = (int)offs.size();
+        const long ld = ell_ld(n);
+        T.ell_w = D;
+        T.ell16 = false;
+        T.doff.alloc(D); T.doff.upload(offs.data(), D, s);
+        T.esrc.alloc((size_t)D * ld);
+        const int g = geom().sms * 4;
+        if (D <= 8) {
+            T.emask8.alloc(ld);
+            k_tri_dia_build<uint8_t><<<g, 256, 0, s>>>(n, D, ld, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, T.doff.p,
+                                                       T.emask8.p, T.esrc.p);
+        } else {
+            T.emask32.alloc(ld);
+            k_tri_dia_build<uint32_t><<<g, 256, 0, s>>>(n, D, ld, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, T.doff.p,
+                                                        T.emask32.p, T.esrc.p);
+        }
+        check_launch();
+    } else if (w > 0 && w <= 64 && (long)w * n <= 2 * std::max<long>(T.nnz, 1)) {
         // layout of the operator's ELL copy, built on the device from the
         // natural CSR just uploaded
         long maxoff = 0;
