@@ -237,11 +237,15 @@ def test_block_and_syncfree_lusolve_bitwise(cuda):
             assert L.xs_set_trsv_block_rows(rows) == 0
             try:
                 P = Plan(A).factor("ilu0")
+                # device inputs stay referenced until the plan's stream is synchronised
+                # (the solves run on the plan's own stream, not torch's)
+                dx, dx32 = _dev(x, cuda), _dev(x.astype(np.float32), cuda)
                 z = torch.zeros(A.n, dtype=torch.float64, device=cuda)
-                P.lusolve(_dev(x, cuda), z)
-                P.set_factor_precision("bf16")
                 z32 = torch.zeros(A.n, dtype=torch.float32, device=cuda)
-                P.lusolve(_dev(x.astype(np.float32), cuda), z32)
+                P.lusolve(dx, z)
+                P.sync()
+                P.set_factor_precision("bf16")
+                P.lusolve(dx32, z32)
                 P.sync()
                 outs.append((z.cpu().numpy(), z32.cpu().numpy()))
             finally:

@@ -202,6 +202,7 @@ class Plan:
         self.A = A
         self.p = C.c_void_p()
         self._keep = (A.rowptr, A.colidx, A.val)
+        self._pending = []
         check(self._L.xs_plan_create(C.byref(self.p), A.n, _i(A.rowptr), _i(A.colidx), _d(A.val)), "xs_plan_create")
         self.ell_width = 0
         self.kind = None
@@ -223,13 +224,21 @@ class Plan:
         self.ell_width = w.value
         return w.value
 
+    def _hold(self, *tensors):
+        """Device tensors used by work queued on the plan's stream stay
+        referenced until sync(): torch's allocator does not see that stream
+        and could otherwise hand their memory to a new tensor first."""
+        self._pending.extend(tensors)
+
     def spmv(self, x, y, fmt="csr", precision="fp64"):
         check(self._L.xs_plan_spmv(self.p, 1 if fmt == "ell" else 0, 0 if precision == "fp64" else 1,
                                    C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "spmv")
+        self._hold(x, y)
         return y
 
     def spmv_t(self, x, y):
         check(self._L.xs_plan_spmv_t(self.p, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "spmv_t")
+        self._hold(x, y)
         return y
 
     def factor(self, kind="ilu0", sweeps=20, fill=2.0, droptol=0.0):
@@ -266,14 +275,19 @@ class Plan:
     def lusolve(self, x, z):
         prec = 0 if str(x.dtype) == "torch.float64" else 1
         check(self._L.xs_plan_lusolve(self.p, prec, C.c_void_p(x.data_ptr()), C.c_void_p(z.data_ptr())), "lusolve")
+        self._hold(x, z)
         return z
 
     def lusolve_t(self, x, z):
         check(self._L.xs_plan_lusolve_t(self.p, C.c_void_p(x.data_ptr()), C.c_void_p(z.data_ptr())), "lusolve_t")
+        self._hold(x, z)
         return z
 
     def sync(self):
-        check(self._L.xs_plan_sync(self.p), "plan sync")
+        try:
+            check(self._L.xs_plan_sync(self.p), "plan sync")
+        finally:
+            self._pending.clear()
 
     def debug_break_dependency(self, position: int, enable: bool = True):
         check(self._L.xs_plan_debug_break_dependency(self.p, position, 1 if enable else 0), "debug_break_dependency")

@@ -675,7 +675,7 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
         T = TriDev();
         {
             Trace tr("  build_tri_dev", s);
-            build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s);
+            build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s, /*identity_src=*/true);
         }
         const long m = std::max<long>(T.nnz, 1);
         const int g = geom().sms * 4;

@@ -305,12 +305,24 @@ constexpr int ELL_ROWS = XS_ELL_ROWS;
 constexpr int ELL_CHUNK = XS_ELL_CHUNK;
 static_assert(ELL_ROWS == 1 || ELL_ROWS == 2 || ELL_ROWS == 4 || ELL_ROWS == 8, "rows per thread");
 static_assert(ELL_LD_ALIGN % ELL_ROWS == 0, "row vectors must stay aligned");
-// rows per thread for values of type MT: one row for 8-byte values (two
-// rows of FP64 chunks do not fit the register budget without spilling)
+// rows per thread and slots per chunk for values of type MT (8-byte values
+// have their own pair: their chunks take twice the registers)
+#ifndef XS_ELL_ROWS64
+#define XS_ELL_ROWS64 2
+#endif
+#ifndef XS_ELL_CHUNK64
+#define XS_ELL_CHUNK64 4
+#endif
+static_assert(XS_ELL_ROWS64 == 1 || XS_ELL_ROWS64 == 2 || XS_ELL_ROWS64 == 4, "rows per thread (8-byte values)");
 template <typename MT>
 __host__ __device__ constexpr int ell_rows_for()
 {
-    return sizeof(MT) >= 8 ? 1 : ELL_ROWS;
+    return sizeof(MT) >= 8 ? XS_ELL_ROWS64 : ELL_ROWS;
+}
+template <typename MT>
+__host__ __device__ constexpr int ell_chunk_for()
+{
+    return sizeof(MT) >= 8 ? XS_ELL_CHUNK64 : ELL_CHUNK;
 }
 
 // R consecutive elements starting at an R-aligned index, one vector load
@@ -396,20 +408,21 @@ template <int R, typename VT, typename MT, typename CT>
 __device__ __forceinline__ void ell_rows(const CT *cp, const MT *vp, int w, long ld, const VT *__restrict__ x, int r0,
                                          int n, const int *s_off, double (&sum)[R])
 {
+    constexpr int CH = ell_chunk_for<MT>();
     CT mask[R];
     if constexpr (EllDiag<CT>::value) {
         ld_vec<R>(cp, mask);  // cp points at the row's mask (padding rows: 0)
     }
-    for (int k0 = 0; k0 < w; k0 += ELL_CHUNK) {
-        const int m = min(ELL_CHUNK, w - k0);  // warp-uniform
+    for (int k0 = 0; k0 < w; k0 += CH) {
+        const int m = min(CH, w - k0);  // warp-uniform
 #define XS_ELL_CHUNK_CALL(CC) ell_chunk<CC, R>(cp, vp, ld, x, r0, n, k0, mask, s_off, sum)
-        if (m == ELL_CHUNK) XS_ELL_CHUNK_CALL(ELL_CHUNK);
-        else if (ELL_CHUNK > 7 && m == 7) XS_ELL_CHUNK_CALL(7);
-        else if (ELL_CHUNK > 6 && m == 6) XS_ELL_CHUNK_CALL(6);
-        else if (ELL_CHUNK > 5 && m == 5) XS_ELL_CHUNK_CALL(5);
-        else if (ELL_CHUNK > 4 && m == 4) XS_ELL_CHUNK_CALL(4);
-        else if (ELL_CHUNK > 3 && m == 3) XS_ELL_CHUNK_CALL(3);
-        else if (ELL_CHUNK > 2 && m == 2) XS_ELL_CHUNK_CALL(2);
+        if (m == CH) XS_ELL_CHUNK_CALL(CH);
+        else if (CH > 7 && m == 7) XS_ELL_CHUNK_CALL(7);
+        else if (CH > 6 && m == 6) XS_ELL_CHUNK_CALL(6);
+        else if (CH > 5 && m == 5) XS_ELL_CHUNK_CALL(5);
+        else if (CH > 4 && m == 4) XS_ELL_CHUNK_CALL(4);
+        else if (CH > 3 && m == 3) XS_ELL_CHUNK_CALL(3);
+        else if (CH > 2 && m == 2) XS_ELL_CHUNK_CALL(2);
         else XS_ELL_CHUNK_CALL(1);
 #undef XS_ELL_CHUNK_CALL
     }

@@ -455,17 +455,18 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, i
         const FT *vp = ev + i0;
         CT mask[R];
         if constexpr (EllDiag<CT>::value) ld_vec<R>(cp, mask);
-        for (int k0 = 0; k0 < w; k0 += ELL_CHUNK) {
-            const int m = min(ELL_CHUNK, w - k0);  // warp-uniform
+        constexpr int CH = ell_chunk_for<FT>();
+        for (int k0 = 0; k0 < w; k0 += CH) {
+            const int m = min(CH, w - k0);  // warp-uniform
 #define XS_SWEEP_CHUNK(CC) \
     sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, ld, i0, n, k0, mask, s_off, dinv, x, yin, acc)
-            if (m == ELL_CHUNK) XS_SWEEP_CHUNK(ELL_CHUNK);
-            else if (ELL_CHUNK > 7 && m == 7) XS_SWEEP_CHUNK(7);
-            else if (ELL_CHUNK > 6 && m == 6) XS_SWEEP_CHUNK(6);
-            else if (ELL_CHUNK > 5 && m == 5) XS_SWEEP_CHUNK(5);
-            else if (ELL_CHUNK > 4 && m == 4) XS_SWEEP_CHUNK(4);
-            else if (ELL_CHUNK > 3 && m == 3) XS_SWEEP_CHUNK(3);
-            else if (ELL_CHUNK > 2 && m == 2) XS_SWEEP_CHUNK(2);
+            if (m == CH) XS_SWEEP_CHUNK(CH);
+            else if (CH > 7 && m == 7) XS_SWEEP_CHUNK(7);
+            else if (CH > 6 && m == 6) XS_SWEEP_CHUNK(6);
+            else if (CH > 5 && m == 5) XS_SWEEP_CHUNK(5);
+            else if (CH > 4 && m == 4) XS_SWEEP_CHUNK(4);
+            else if (CH > 3 && m == 3) XS_SWEEP_CHUNK(3);
+            else if (CH > 2 && m == 2) XS_SWEEP_CHUNK(2);
             else XS_SWEEP_CHUNK(1);
 #undef XS_SWEEP_CHUNK
         }
@@ -536,6 +537,26 @@ __global__ void k_tri_dia_build(int n, int D, long ld, const int *__restrict__ r
     }
 }
 
+// level-ordered entry arrays from the natural CSR: position p holds row
+// perm[p]; its entries in increasing column order (L) or decreasing (U)
+__global__ void k_pos_entries(int n, bool upper, const int *__restrict__ perm, const int *__restrict__ prp,
+                              const int *__restrict__ rp, const int *__restrict__ ci, const long *__restrict__ src_nat,
+                              int *pci, long *src)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int row = perm[p], o = prp[p], len = prp[p + 1] - o;
+        for (int k = 0; k < len; k++) {
+            const int q = upper ? rp[row + 1] - 1 - k : rp[row] + k;
+            pci[o + k] = ci[q];
+            src[o + k] = src_nat ? src_nat[q] : (long)q;
+        }
+    }
+}
+__global__ void k_iota_long(long m, long *a)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < m; i += (long)gridDim.x * blockDim.x) a[i] = i;
+}
+
 // ---------------------------------------------------------------- host plan building
 // Host-side analysis of a triangular pattern.
 struct TriHostPlan {
@@ -554,7 +575,8 @@ struct TriHostPlan {
 // from.  upper: dependencies on larger rows, entries summed in decreasing
 // column order.
 template <typename SrcF>
-inline void tri_analyse(int n, const int *rp, const int *ci, bool upper, SrcF src_of, TriHostPlan &h)
+inline void tri_analyse(int n, const int *rp, const int *ci, bool upper, SrcF src_of, TriHostPlan &h,
+                        bool entries = true)
 {
     h.n = n;
     h.level.assign(n, 0);
@@ -592,6 +614,7 @@ inline void tri_analyse(int n, const int *rp, const int *ci, bool upper, SrcF sr
         int r = h.perm[p];
         h.prp[p + 1] = h.prp[p] + (rp[r + 1] - rp[r]);
     }
+    if (!entries) return;  // pci/src are built on the device (k_pos_entries)
     long nnz = h.prp[n];
     h.pci.assign(nnz, 0);
     h.src.assign(nnz, 0);
@@ -793,23 +816,39 @@ namespace xs {
 // an entry to its index in the value array) in the layout the tuning selects,
 // plus the natural-order copy used by the Jacobi-sweep mode.
 template <typename SrcF>
+// identity_src: entry k's value is vals[k] (src_of is not called)
 inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const std::vector<int> &ci, bool upper, SrcF src_of,
-                          cudaStream_t s)
+                          cudaStream_t s, bool identity_src = false)
 {
     TriHostPlan P;  // level analysis (also gives the level count)
-    tri_analyse(n, rp.data(), ci.data(), upper, src_of, P);
+    const int chr = trsv_tuning().chunk_rows;
+    T.chunked = chr > 0;
+    tri_analyse(n, rp.data(), ci.data(), upper, src_of, P, /*entries=*/false);
     T.n = n;
     T.nnz = P.prp[n];
     T.nlevels = P.nlevels;
     T.upper = upper;
     const long m = std::max<long>(T.nnz, 1);
-    const int chr = trsv_tuning().chunk_rows;
-    T.chunked = chr > 0;
+    const int g = geom().sms * 4;
+    // natural CSR and the source index of each entry's value
+    T.rp_nat.alloc(n + 1); T.rp_nat.upload(rp.data(), n + 1, s);
+    T.ci_nat.alloc(m); if (T.nnz) T.ci_nat.upload(ci.data(), T.nnz, s);
+    T.src_nat.alloc(m);
+    if (identity_src) {
+        k_iota_long<<<g, 256, 0, s>>>(T.nnz, T.src_nat.p);
+    } else {
+        std::vector<long> ns(T.nnz);
+        for (long k = 0; k < T.nnz; k++) ns[k] = src_of((int)k);
+        if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
+    }
     if (!T.chunked) {
         T.perm.alloc(n); T.perm.upload(P.perm.data(), n, s);
         T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
-        T.pci.alloc(m); if (T.nnz) T.pci.upload(P.pci.data(), T.nnz, s);
-        T.src.alloc(m); if (T.nnz) T.src.upload(P.src.data(), T.nnz, s);
+        T.pci.alloc(m);
+        T.src.alloc(m);
+        k_pos_entries<<<g, 256, 0, s>>>(n, upper, T.perm.p, T.prp.p, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, T.pci.p,
+                                        T.src.p);
+        check_launch();
         T.lstart.alloc(P.nlevels + 1); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
     } else {
         TriChunkPlan C;
@@ -823,11 +862,6 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         T.lvl_off.alloc(C.lvl_off.size()); T.lvl_off.upload(C.lvl_off.data(), C.lvl_off.size(), s);
         T.lvl_ptr.alloc(C.lvl_ptr.size()); T.lvl_ptr.upload(C.lvl_ptr.data(), C.lvl_ptr.size(), s);
     }
-    T.rp_nat.alloc(n + 1); T.rp_nat.upload(rp.data(), n + 1, s);
-    T.ci_nat.alloc(m); if (T.nnz) T.ci_nat.upload(ci.data(), T.nnz, s);
-    std::vector<long> ns(T.nnz);
-    for (long k = 0; k < T.nnz; k++) ns[k] = src_of((int)k);
-    T.src_nat.alloc(m); if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
     // ELL copy when the rows are nearly uniform (padding at most 2x)
     int w = 0;
     for (int i = 0; i < n; i++) w = std::max(w, rp[i + 1] - rp[i]);
@@ -910,6 +944,80 @@ inline void load_tri_ell(TriDev &T, const double *vals, bool need32, cudaStream_
 constexpr int LU_BLOCK_THREADS = 1024;
 constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
 
+// One thread's row of a level, loaded ahead: the row, its entry range, the
+// first LU_PF entries and the row's scalar input (x[row] for L, dinv for U).
+constexpr int LU_PF = 8;
+template <typename VT, typename FT>
+struct LuRow {
+    int row, k0, len;
+    int c[LU_PF];
+    FT v[LU_PF];
+    VT in;
+};
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+__device__ __forceinline__ void lu_row_load(const TrsvArgs<FT> &P, int p, const VT *__restrict__ x,
+                                            const DT *__restrict__ dinv, LuRow<VT, FT> &r)
+{
+    r.row = __ldg(P.perm + p);
+    r.k0 = __ldg(P.prp + p);
+    r.len = __ldg(P.prp + p + 1) - r.k0;
+#pragma unroll
+    for (int j = 0; j < LU_PF; j++) {
+        if (j < r.len) {
+            r.c[j] = __ldg(P.pci + r.k0 + j);
+            r.v[j] = P.pv[r.k0 + j];
+        }
+    }
+    if (UPPER) r.in = (VT)__ldg(dinv + p);
+    else r.in = x[r.row];
+}
+
+template <typename VT, typename FT, bool UPPER>
+__device__ __forceinline__ void lu_row_solve(const TrsvArgs<FT> &P, const LuRow<VT, FT> &r, VT *ys)
+{
+    VT acc = UPPER ? ys[r.row] * r.in : r.in;
+#pragma unroll
+    for (int j = 0; j < LU_PF; j++)
+        if (j < r.len) acc = msub(acc, ys[r.c[j]], (VT)FVal<FT>::cvt(r.v[j]));
+    for (int k = r.k0 + LU_PF; k < r.k0 + r.len; k++) acc = msub(acc, ys[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
+    ys[r.row] = acc;
+}
+
+// walk the levels of one triangle; the row a thread takes in level l+1 is
+// loaded before the barrier that ends level l, so its global loads overlap
+// the barrier instead of starting after it
+template <typename VT, typename FT, typename DT, bool UPPER>
+__device__ __forceinline__ void lu_block_phase(const TrsvArgs<FT> &P, const int *__restrict__ ls, int nl,
+                                               const VT *__restrict__ x, const DT *__restrict__ dinv, VT *ys)
+{
+    LuRow<VT, FT> nxt;
+    bool have = nl > 0 && __ldg(ls) + (int)threadIdx.x < __ldg(ls + 1);
+    if (have) lu_row_load<VT, FT, DT, UPPER>(P, __ldg(ls) + threadIdx.x, x, dinv, nxt);
+    for (int l = 0; l < nl; l++) {
+        const int p0 = __ldg(ls + l), p1 = __ldg(ls + l + 1);
+        if (have) {
+            const LuRow<VT, FT> cur = nxt;
+            lu_row_solve<VT, FT, UPPER>(P, cur, ys);
+        }
+        // rows beyond the first blockDim.x of a wide level, without look-ahead
+        for (int p = p0 + (int)threadIdx.x + (int)blockDim.x; p < p1; p += blockDim.x) {
+            LuRow<VT, FT> r;
+            lu_row_load<VT, FT, DT, UPPER>(P, p, x, dinv, r);
+            lu_row_solve<VT, FT, UPPER>(P, r, ys);
+        }
+        have = false;
+        if (l + 1 < nl) {
+            const int q = p1 + (int)threadIdx.x;
+            if (q < __ldg(ls + l + 2)) {
+                lu_row_load<VT, FT, DT, UPPER>(P, q, x, dinv, nxt);
+                have = true;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <typename VT, typename FT, typename DT>
 __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_block(TrsvArgs<FT> L, const int *__restrict__ lstart, int nlL,
                                                                 TrsvArgs<FT> U, const int *__restrict__ ustart, int nlU,
@@ -919,28 +1027,8 @@ __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_block(TrsvArgs<FT> L, c
     extern __shared__ __align__(16) unsigned char lu_smem[];
     VT *ys = (VT *)lu_smem;
     if (done_flag && *done_flag) return;
-    for (int l = 0; l < nlL; l++) {
-        const int p1 = lstart[l + 1];
-        for (int p = lstart[l] + (int)threadIdx.x; p < p1; p += blockDim.x) {
-            const int row = __ldg(L.perm + p);
-            VT acc = x[row];
-            const int k1 = __ldg(L.prp + p + 1);
-            for (int k = __ldg(L.prp + p); k < k1; k++) acc = msub(acc, ys[__ldg(L.pci + k)], (VT)FVal<FT>::ld(L.pv, k));
-            ys[row] = acc;
-        }
-        __syncthreads();
-    }
-    for (int l = 0; l < nlU; l++) {
-        const int p1 = ustart[l + 1];
-        for (int p = ustart[l] + (int)threadIdx.x; p < p1; p += blockDim.x) {
-            const int row = __ldg(U.perm + p);
-            VT acc = ys[row] * (VT)__ldg(dinv + p);
-            const int k1 = __ldg(U.prp + p + 1);
-            for (int k = __ldg(U.prp + p); k < k1; k++) acc = msub(acc, ys[__ldg(U.pci + k)], (VT)FVal<FT>::ld(U.pv, k));
-            ys[row] = acc;
-        }
-        __syncthreads();
-    }
+    lu_block_phase<VT, FT, DT, false>(L, lstart, nlL, x, dinv, ys);
+    lu_block_phase<VT, FT, DT, true>(U, ustart, nlU, x, dinv, ys);
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) z[i] = ys[i];
 }
 
