@@ -37,7 +37,7 @@ Geom &geom()
         cudaDeviceProp p;
         if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) {
             g.sms = p.multiProcessorCount;
-            g.red_grid = 4 * g.sms;
+            g.red_grid = 8 * g.sms;
         }
         init = true;
     }

@@ -182,7 +182,7 @@ struct KState {
 // ---------------------------------------------------------------- launch geometry
 struct Geom {
     int sms = 148;
-    int red_grid = 592;  // fixed grid for reductions: 4 blocks per SM
+    int red_grid = 1184;  // fixed grid of the vector-op reductions: 8 CTAs of 256 per SM (full occupancy)
     int red_block = 256;
 };
 Geom &geom();

@@ -33,7 +33,7 @@ constexpr double KSMALL = 1e-20;
 
 // ---------------------------------------------------------------- generic vector-op kernel
 template <class Op>
-__global__ void __launch_bounds__(256) k_vecop(Op op, RedSlot slot)
+__global__ void __launch_bounds__(256, 8) k_vecop(Op op, RedSlot slot)
 {
     constexpr int KK = Op::K > 0 ? Op::K : 1;
     __shared__ double tot[KK];
@@ -576,7 +576,7 @@ struct Workspace {
     }
     void ensure(int max_k, int maxiter)
     {
-        int G = std::max(geom().red_grid, geom().sms * 8);
+        int G = std::max(geom().red_grid, geom().sms * 16);  // covers every reduction grid (ELL: <= 10 CTAs per SM)
         if (part_cap < max_k * G) {
             part.alloc((size_t)max_k * G);
             part_cap = max_k * G;
