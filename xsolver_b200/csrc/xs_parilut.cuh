@@ -12,7 +12,8 @@
 //      c = -a_ij; c += l_ik u_kj (k ascending); r = -c.
 //   3. split into L (unit diagonal last) and U, U also by columns (CSC).
 //   4. one synchronous sweep over every L and U entry (fixed point of the
-//      ILU equations on the current pattern).
+//      ILU equations on the current pattern), row-wise: a warp per row
+//      subtracts l_ik * u_kj walking the U rows k of its L row.
 //   5. if the candidate count exceeds round(rate*nnz(A)): per factor keep
 //      (int)(rate*nnz0) entries — threshold = k-th smallest |v| by an 8-pass
 //      radix select on the IEEE bit patterns — plus the optional drop
@@ -52,12 +53,6 @@ constexpr int PLT_CAP = 2048;  // candidate columns gathered per row (with dupli
 constexpr int PLT_WARPS = 4;
 
 // ---------------------------------------------------------------- helpers
-__global__ void k_rowof(int n, const int *__restrict__ rp, int *__restrict__ rowof)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        for (int k = rp[i]; k < rp[i + 1]; k++) rowof[k] = i;
-}
-
 __global__ void k_count_cols(int n, const int *__restrict__ rp, const int *__restrict__ ci, int *cnt)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -183,51 +178,118 @@ __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int 
 }
 
 // candidate values (warp per row, lanes over the row's entries)
-__global__ void k_candidate_values(int n, const int *__restrict__ arp, const int *__restrict__ aci,
-                                   const double *__restrict__ av, const int *__restrict__ lrp,
-                                   const int *__restrict__ lci, const double *__restrict__ lv,
-                                   const int *__restrict__ urp, const int *__restrict__ uci,
-                                   const double *__restrict__ uv, const int *__restrict__ ucp,
-                                   const int *__restrict__ ucr, const double *__restrict__ ucv,
-                                   const double *__restrict__ udiag, const int *__restrict__ drp,
-                                   const int *__restrict__ dci, double *__restrict__ dv)
+// value of candidate (i, j): an entry already in L or U keeps its value, a
+// new one gets r_ij (/u_jj below the diagonal), r = A - L*U accumulated as
+// c = -a_ij; c += l_ik u_kj over the merge of L row i and U column j
+__device__ __forceinline__ double cand_value(int i, int j, const int *arp, const int *aci, const double *av,
+                                            const int *lrp, const int *lci, const double *lv, const int *urp,
+                                            const int *uci, const double *uv, const int *ucp, const int *ucr,
+                                            const double *ucv, const double *udiag)
 {
-    const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
-    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
-        for (int q = drp[i] + lane; q < drp[i + 1]; q += 32) {
-            const int j = dci[q];
-            double d;
+    int pos = -1;
+    if (j < i) pos = find_pos(lci, lrp[i], lrp[i + 1], j);
+    if (pos >= 0) return lv[pos];
+    const int pu = (j >= i) ? find_pos(uci, urp[i], urp[i + 1], j) : -1;
+    if (pu >= 0) return uv[pu];
+    const int pa = find_pos(aci, arp[i], arp[i + 1], j);
+    double c = -(pa >= 0 ? av[pa] : 0.0);
+    int il = lrp[i], iu = ucp[j];
+    const int ile = lrp[i + 1], iue = ucp[j + 1];
+    while (il < ile && iu < iue) {
+        const int lj = lci[il], ui = ucr[iu];
+        if (lj == ui) {
+            c += lv[il] * ucv[iu];
+            il++;
+            iu++;
+        } else if (lj < ui)
+            il++;
+        else
+            iu++;
+    }
+    const double r = -c;
+    return (j < i) ? r / udiag[j] : r;
+}
+
+// Candidate values, one warp per row i.  Existing entries copy their value;
+// for the new ones the row's accumulators c_j = -a_ij are staged in shared
+// memory and every k of L row i (increasing, the stored unit diagonal
+// included) adds l_ik u_kj for each u_kj of U row k whose column is a new
+// candidate of row i — the products and order of the per-entry merge, with
+// contiguous reads of U rows.  Rows with more than PLT_CAND_CAP candidates
+// use the per-entry merge.
+constexpr int PLT_CAND_CAP = 512;
+constexpr int PLT_CV_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * PLT_CV_WARPS) k_candidate_values(
+    int n, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
+    const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv,
+    const int *__restrict__ urp, const int *__restrict__ uci, const double *__restrict__ uv,
+    const int *__restrict__ ucp, const int *__restrict__ ucr, const double *__restrict__ ucv,
+    const double *__restrict__ udiag, const int *__restrict__ drp, const int *__restrict__ dci,
+    double *__restrict__ dv)
+{
+    __shared__ int s_col[PLT_CV_WARPS][PLT_CAND_CAP];
+    __shared__ double s_c[PLT_CV_WARPS][PLT_CAND_CAP];
+    __shared__ unsigned char s_new[PLT_CV_WARPS][PLT_CAND_CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int *col = s_col[w];
+    double *cc = s_c[w];
+    unsigned char *isnew = s_new[w];
+    for (int i = blockIdx.x * PLT_CV_WARPS + w; i < n; i += gridDim.x * PLT_CV_WARPS) {
+        const int d0 = drp[i], m = drp[i + 1] - d0;
+        if (m > PLT_CAND_CAP) {
+            for (int q = lane; q < m; q += 32)
+                dv[d0 + q] = cand_value(i, dci[d0 + q], arp, aci, av, lrp, lci, lv, urp, uci, uv, ucp, ucr, ucv, udiag);
+            continue;
+        }
+        bool any_new = false;
+        for (int q = lane; q < m; q += 32) {
+            const int j = dci[d0 + q];
+            col[q] = j;
             int pos = -1;
             if (j < i) pos = find_pos(lci, lrp[i], lrp[i + 1], j);
             if (pos >= 0) {
-                d = lv[pos];
-            } else {
-                int pu = (j >= i) ? find_pos(uci, urp[i], urp[i + 1], j) : -1;
-                if (pu >= 0) {
-                    d = uv[pu];
-                } else {
-                    const int pa = find_pos(aci, arp[i], arp[i + 1], j);
-                    double c = -(pa >= 0 ? av[pa] : 0.0);
-                    int il = lrp[i], iu = ucp[j];
-                    const int ile = lrp[i + 1], iue = ucp[j + 1];
-                    while (il < ile && iu < iue) {
-                        const int lj = lci[il], ui = ucr[iu];
-                        if (lj == ui) {
-                            c += lv[il] * ucv[iu];
-                            il++;
-                            iu++;
-                        } else if (lj < ui)
-                            il++;
-                        else
-                            iu++;
-                    }
-                    const double r = -c;
-                    d = (j < i) ? r / udiag[j] : r;
-                }
+                dv[d0 + q] = lv[pos];
+                isnew[q] = 0;
+                continue;
             }
-            dv[q] = d;
+            const int pu = (j >= i) ? find_pos(uci, urp[i], urp[i + 1], j) : -1;
+            if (pu >= 0) {
+                dv[d0 + q] = uv[pu];
+                isnew[q] = 0;
+                continue;
+            }
+            const int pa = find_pos(aci, arp[i], arp[i + 1], j);
+            cc[q] = -(pa >= 0 ? av[pa] : 0.0);
+            isnew[q] = 1;
+            any_new = true;
         }
+        if (!__any_sync(0xffffffffu, any_new)) continue;
+        __syncwarp();
+        const int l0 = lrp[i], l1 = lrp[i + 1];
+        for (int kq = l0; kq < l1; kq++) {
+            const int k = lci[kq];
+            const double lk = lv[kq];
+            const int e1 = urp[k + 1];
+            for (int e = urp[k] + lane; e < e1; e += 32) {
+                const int j = uci[e];
+                int lo = 0, hi = m;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (col[mid] < j) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo < m && col[lo] == j && isnew[lo]) cc[lo] += lk * uv[e];
+            }
+            __syncwarp();
+        }
+        for (int q = lane; q < m; q += 32) {
+            if (!isnew[q]) continue;
+            const int j = col[q];
+            const double r = -cc[q];
+            dv[d0 + q] = (j < i) ? r / udiag[j] : r;
+        }
+        __syncwarp();
     }
 }
 
@@ -282,31 +344,96 @@ __device__ __forceinline__ double plt_sweep_value(const int *arp, const int *aci
     return t;
 }
 
-// sweep over L entries (off-diagonal): lnew = value / u_jj
-__global__ void k_plt_sweep_L(long nnzl, const int *__restrict__ lrow, const int *__restrict__ arp,
-                              const int *__restrict__ aci, const double *__restrict__ av, const int *__restrict__ lrp,
-                              const int *__restrict__ lci, const double *__restrict__ lv, const int *__restrict__ ucp,
-                              const int *__restrict__ ucr, const double *__restrict__ ucv, double *__restrict__ lnew)
+// Row-wise synchronous sweep, one warp per row i.  The row's pattern (L row
+// i without its stored unit diagonal, then U row i) and its values
+// t_ij = a_ij are staged in shared memory; then for every k of L row i in
+// increasing order the lanes walk U row k (CSR) and, for each column j != k
+// found in row i's pattern, subtract l_ik * u_kj.  That is the same set of
+// products, subtracted in the same (increasing k) order, as the per-entry
+// merge of plt_sweep_value, so the values are identical; but U rows are read
+// contiguously and no lane walks a dependent index chain.  Results: L part
+// t / u_jj into lnew (CSR position), U part t into unew at row i's position
+// in U's column j (CSC).  parts: 1 L only, 2 U only, 3 both.  Rows whose
+// pattern exceeds PLT_ROW_CAP fall back to the per-entry merge.
+constexpr int PLT_ROW_CAP = 256;
+constexpr int PLT_SW_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
+    int n, int parts, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
+    const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv_k,
+    const double *__restrict__ lv_old, const int *__restrict__ urp, const int *__restrict__ uci,
+    const double *__restrict__ uv, const int *__restrict__ ucp, const int *__restrict__ ucr,
+    const double *__restrict__ ucv, double *__restrict__ lnew, double *__restrict__ unew)
 {
-    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nnzl; k += (long)gridDim.x * blockDim.x) {
-        const int i = lrow[k], j = lci[k];
-        if (j >= i) {
-            lnew[k] = lv[k];
+    __shared__ int s_col[PLT_SW_WARPS][PLT_ROW_CAP];
+    __shared__ double s_t[PLT_SW_WARPS][PLT_ROW_CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int *col = s_col[w];
+    double *t = s_t[w];
+    for (int i = blockIdx.x * PLT_SW_WARPS + w; i < n; i += gridDim.x * PLT_SW_WARPS) {
+        const int l0 = lrp[i], l1 = lrp[i + 1];
+        // L row i: strict entries first (ascending), the unit diagonal (col i) last
+        const int nl = (l1 > l0 && lci[l1 - 1] >= i) ? l1 - l0 - 1 : l1 - l0;
+        const int u0 = urp[i], nu = urp[i + 1] - u0;
+        const int m = nl + nu;
+        if (m > PLT_ROW_CAP) {
+            // per-entry merge for an unusually long row
+            for (int q = lane; q < l1 - l0; q += 32) {
+                const int k = l0 + q, j = lci[k];
+                if (!(parts & 1)) continue;
+                if (j >= i) { lnew[k] = lv_old[k]; continue; }
+                const double tv = plt_sweep_value(arp, aci, av, lrp, lci, lv_k, ucp, ucr, ucv, i, j);
+                lnew[k] = tv / ucv[ucp[j + 1] - 1];
+            }
+            if (parts & 2) {
+                for (int q = lane; q < nu; q += 32) {
+                    const int j = uci[u0 + q];
+                    const int pc = find_pos(ucr, ucp[j], ucp[j + 1], i);
+                    unew[pc] = plt_sweep_value(arp, aci, av, lrp, lci, lv_k, ucp, ucr, ucv, i, j);
+                }
+            }
             continue;
         }
-        const double t = plt_sweep_value(arp, aci, av, lrp, lci, lv, ucp, ucr, ucv, i, j);
-        lnew[k] = t / ucv[ucp[j + 1] - 1];
-    }
-}
-// sweep over U entries (CSC order): unew = value
-__global__ void k_plt_sweep_U(long nnzu, const int *__restrict__ ucol, const int *__restrict__ arp,
-                              const int *__restrict__ aci, const double *__restrict__ av, const int *__restrict__ lrp,
-                              const int *__restrict__ lci, const double *__restrict__ lv, const int *__restrict__ ucp,
-                              const int *__restrict__ ucr, const double *__restrict__ ucv, double *__restrict__ unew)
-{
-    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nnzu; k += (long)gridDim.x * blockDim.x) {
-        const int j = ucol[k], i = ucr[k];
-        unew[k] = plt_sweep_value(arp, aci, av, lrp, lci, lv, ucp, ucr, ucv, i, j);
+        for (int q = lane; q < m; q += 32) {
+            const int j = q < nl ? lci[l0 + q] : uci[u0 + q - nl];
+            col[q] = j;
+            const int pa = find_pos(aci, arp[i], arp[i + 1], j);
+            t[q] = pa >= 0 ? av[pa] : 0.0;
+        }
+        __syncwarp();
+        // only the products that reach a requested part: L part needs k < j < i
+        // (every k of L row i may contribute); U part needs k < i
+        for (int kq = 0; kq < nl; kq++) {
+            const int k = lci[l0 + kq];
+            const double lk = lv_k[l0 + kq];
+            const int e1 = urp[k + 1];
+            for (int e = urp[k] + lane; e < e1; e += 32) {
+                const int j = uci[e];
+                if (j == k) continue;
+                if (!(parts & 2) && j >= i) continue;
+                if (!(parts & 1) && j < i) continue;
+                // binary search of j in the row's sorted pattern
+                int lo = 0, hi = m;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (col[mid] < j) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo < m && col[lo] == j) t[lo] = t[lo] - lk * uv[e];
+            }
+            __syncwarp();
+        }
+        for (int q = lane; q < m; q += 32) {
+            const int j = col[q];
+            if (q < nl) {
+                if (parts & 1) lnew[l0 + q] = t[q] / uv[urp[j]];  // u_jj: first entry of U row j
+            } else if (parts & 2) {
+                const int pc = find_pos(ucr, ucp[j], ucp[j + 1], i);
+                unew[pc] = t[q];
+            }
+        }
+        if ((parts & 1) && nl < l1 - l0 && lane == 0) lnew[l1 - 1] = lv_old[l1 - 1];  // unit diagonal unchanged
+        __syncwarp();
     }
 }
 
@@ -545,8 +672,9 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
         D.ci.alloc(std::max<long>(D.nnz, 1));
         D.v.alloc(std::max<long>(D.nnz, 1));
         k_candidates<<<cg, 32 * PLT_WARPS, 0, s>>>(n, A.rp, A.ci, L.rp, L.ci, U.rp, U.ci, 1, nullptr, D.rp, D.ci, err);
-        k_candidate_values<<<G, 256, 0, s>>>(n, A.rp, A.ci, A.v, L.rp, L.ci, L.v, U.rp, U.ci, U.v, Uc.rp, Uc.ci, Uc.v,
-                                             udiag, D.rp, D.ci, D.v);
+        k_candidate_values<<<std::max(1, std::min((n + PLT_CV_WARPS - 1) / PLT_CV_WARPS, geom().sms * 16)),
+                             32 * PLT_CV_WARPS, 0, s>>>(n, A.rp, A.ci, A.v, L.rp, L.ci, L.v, U.rp, U.ci, U.v, Uc.rp,
+                                                        Uc.ci, Uc.v, udiag, D.rp, D.ci, D.v);
         check_launch();
         {
             int e = 0;
@@ -571,25 +699,19 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
         D = DCsr();
         DCsr U2c;
         plt_transpose(c, U2, U2c);
-        U2 = DCsr();
-        // LU sweep (synchronous)
-        DBuf<int> lrow, ucol;
-        lrow.alloc(L2.nnz);
-        ucol.alloc(std::max<long>(U2c.nnz, 1));
-        k_rowof<<<G, 256, 0, s>>>(n, L2.rp, lrow);
-        k_rowof<<<G, 256, 0, s>>>(n, U2c.rp, ucol);
+        // LU sweep (synchronous): both parts from the old values
+        const int rg = std::max(1, std::min((n + PLT_SW_WARPS - 1) / PLT_SW_WARPS, geom().sms * 16));
         {
             DBuf<double> lnew, unew;
             lnew.alloc(L2.nnz);
             unew.alloc(std::max<long>(U2c.nnz, 1));
-            k_plt_sweep_L<<<G, 256, 0, s>>>(L2.nnz, lrow, A.rp, A.ci, A.v, L2.rp, L2.ci, L2.v, U2c.rp, U2c.ci, U2c.v,
-                                            lnew);
-            k_plt_sweep_U<<<G, 256, 0, s>>>(U2c.nnz, ucol, A.rp, A.ci, A.v, L2.rp, L2.ci, L2.v, U2c.rp, U2c.ci, U2c.v,
-                                            unew);
+            k_plt_sweep_rows<<<rg, 32 * PLT_SW_WARPS, 0, s>>>(n, 3, A.rp, A.ci, A.v, L2.rp, L2.ci, L2.v, L2.v, U2.rp,
+                                                               U2.ci, U2.v, U2c.rp, U2c.ci, U2c.v, lnew, unew);
             check_launch();
             L2.v = std::move(lnew);
             U2c.v = std::move(unew);
         }
+        U2 = DCsr();
         // threshold removal
         const long keep_nnz = std::lround(rate * (double)nnzA);
         const long remove_nnz = nnzD - keep_nnz;
@@ -619,21 +741,19 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
             L3 = std::move(L2);
             U3c = std::move(U2c);
         }
-        // L sweep, then U sweep with the new L
-        lrow.alloc(L3.nnz);
-        ucol.alloc(std::max<long>(U3c.nnz, 1));
-        k_rowof<<<G, 256, 0, s>>>(n, L3.rp, lrow);
-        k_rowof<<<G, 256, 0, s>>>(n, U3c.rp, ucol);
+        // L sweep, then U sweep with the new L (U rows by CSR for the products)
         {
+            DCsr U3;
+            plt_transpose(c, U3c, U3);
             DBuf<double> lnew, unew;
             lnew.alloc(L3.nnz);
-            k_plt_sweep_L<<<G, 256, 0, s>>>(L3.nnz, lrow, A.rp, A.ci, A.v, L3.rp, L3.ci, L3.v, U3c.rp, U3c.ci, U3c.v,
-                                            lnew);
+            k_plt_sweep_rows<<<rg, 32 * PLT_SW_WARPS, 0, s>>>(n, 1, A.rp, A.ci, A.v, L3.rp, L3.ci, L3.v, L3.v, U3.rp,
+                                                               U3.ci, U3.v, U3c.rp, U3c.ci, U3c.v, lnew, nullptr);
             check_launch();
             L3.v = std::move(lnew);
             unew.alloc(std::max<long>(U3c.nnz, 1));
-            k_plt_sweep_U<<<G, 256, 0, s>>>(U3c.nnz, ucol, A.rp, A.ci, A.v, L3.rp, L3.ci, L3.v, U3c.rp, U3c.ci, U3c.v,
-                                            unew);
+            k_plt_sweep_rows<<<rg, 32 * PLT_SW_WARPS, 0, s>>>(n, 2, A.rp, A.ci, A.v, L3.rp, L3.ci, L3.v, L3.v, U3.rp,
+                                                               U3.ci, U3.v, U3c.rp, U3c.ci, U3c.v, nullptr, unew);
             check_launch();
             U3c.v = std::move(unew);
         }

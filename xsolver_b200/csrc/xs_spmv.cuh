@@ -359,13 +359,21 @@ __device__ __forceinline__ void ld_vec(const T *p, T (&o)[R])
 // C consecutive slots (k0 .. k0+C-1) of rows r0..r0+R-1: slot loads, then
 // the gathers of x, then the per-row sums in slot order (each row's sum stays
 // in entry order; a slot absent from a row adds nothing).
-template <int C, int R, typename VT, typename MT, typename CT>
+// Row sums accumulate in FP64, except for FP32 values and vectors (the
+// inner solve of the mixed-precision refinement), which accumulate in FP32.
+template <typename VT, typename MT>
+using EllAcc = typename std::conditional<std::is_same<VT, float>::value && std::is_same<MT, float>::value, float,
+                                         double>::type;
+
+template <int C, int R, typename VT, typename MT, typename CT, typename AT>
 __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld, const VT *__restrict__ x, int r0,
-                                          int n, int k0, const CT (&mask)[R], const int *s_off, double (&sum)[R])
+                                          int n, int k0, const CT (&mask)[R], const int *s_off, AT (&sum)[R])
 {
     MT v[C][R];
     VT xv[C][R];
     if constexpr (EllDiag<CT>::value) {
+        // gathers do not wait for the mask: every slot's column is clamped
+        // into [0, n) and loaded, and the mask decides what is summed
 #pragma unroll
         for (int j = 0; j < C; j++) {
             ld_vec<R>(vp, v[j]);
@@ -375,14 +383,13 @@ __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld,
         for (int j = 0; j < C; j++) {
             const int off = s_off[k0 + j];
 #pragma unroll
-            for (int q = 0; q < R; q++)
-                xv[j][q] = ((mask[q] >> (k0 + j)) & 1u) ? __ldg(x + (r0 + q + off)) : (VT)0;
+            for (int q = 0; q < R; q++) xv[j][q] = __ldg(x + min(max(r0 + q + off, 0), n - 1));
         }
 #pragma unroll
         for (int j = 0; j < C; j++)
 #pragma unroll
             for (int q = 0; q < R; q++)
-                if ((mask[q] >> (k0 + j)) & 1u) sum[q] += (double)v[j][q] * (double)xv[j][q];
+                if ((mask[q] >> (k0 + j)) & 1u) sum[q] += (AT)v[j][q] * (AT)xv[j][q];
     } else {
         CT c[C][R];
 #pragma unroll
@@ -400,13 +407,13 @@ __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld,
 #pragma unroll
         for (int j = 0; j < C; j++)
 #pragma unroll
-            for (int q = 0; q < R; q++) sum[q] += (double)v[j][q] * (double)xv[j][q];
+            for (int q = 0; q < R; q++) sum[q] += (AT)v[j][q] * (AT)xv[j][q];
     }
 }
 
-template <int R, typename VT, typename MT, typename CT>
+template <int R, typename VT, typename MT, typename CT, typename AT>
 __device__ __forceinline__ void ell_rows(const CT *cp, const MT *vp, int w, long ld, const VT *__restrict__ x, int r0,
-                                         int n, const int *s_off, double (&sum)[R])
+                                         int n, const int *s_off, AT (&sum)[R])
 {
     constexpr int CH = ell_chunk_for<MT>();
     CT mask[R];
@@ -442,16 +449,17 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_ell_spmv(EllArgs<MT, CT
 #pragma unroll
     for (int k = 0; k < KK; k++) acc[k] = 0.0;
     const int n = A.n;
+    using AT = EllAcc<VT, MT>;
     for (int r0 = (blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += gridDim.x * blockDim.x * R) {
-        double sum[R];
+        AT sum[R];
 #pragma unroll
-        for (int q = 0; q < R; q++) sum[q] = 0.0;
-        ell_rows<R, VT, MT, CT>(A.ci + r0, A.v + r0, A.w, A.ld, x, r0, n, s_off, sum);
+        for (int q = 0; q < R; q++) sum[q] = (AT)0;
+        ell_rows<R, VT, MT, CT, AT>(A.ci + r0, A.v + r0, A.w, A.ld, x, r0, n, s_off, sum);
 #pragma unroll
         for (int q = 0; q < R; q++) {
             const int r = r0 + q;
             if (R == 1 || r < n) {
-                VT o = epi.out(r, sum[q]);
+                VT o = epi.out(r, (double)sum[q]);
                 y[r] = o;
                 if (Epi::K > 0) epi.acc(r, (double)o, acc);
             }

@@ -377,6 +377,8 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
     bool pr[C][R];
     int col[C][R];
     if constexpr (EllDiag<CT>::value) {
+        // gathers do not wait for the mask: columns clamped into [0, n),
+        // the mask decides what is subtracted
 #pragma unroll
         for (int j = 0; j < C; j++) {
             ld_vec<R>(vp, v[j]);
@@ -385,7 +387,7 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
 #pragma unroll
             for (int q = 0; q < R; q++) {
                 pr[j][q] = (mask[q] >> (k0 + j)) & 1u;
-                col[j][q] = i0 + q + off;
+                col[j][q] = min(max(i0 + q + off, 0), n - 1);
             }
         }
     } else {
@@ -409,7 +411,7 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
     for (int j = 0; j < C; j++)
 #pragma unroll
         for (int q = 0; q < R; q++) {
-            if (pr[j][q]) {
+            if (EllDiag<CT>::value || pr[j][q]) {
                 const int cc = col[j][q];
                 if (FIRST2) y[j][q] = UPPER ? (VT)(__ldg(x + cc) * (VT)__ldg(dinv + cc)) : __ldg(x + cc);
                 else y[j][q] = __ldg(yin + cc);
@@ -946,7 +948,7 @@ constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
 
 // One thread's row of a level, loaded ahead: the row, its entry range, the
 // first LU_PF entries and the row's scalar input (x[row] for L, dinv for U).
-constexpr int LU_PF = 8;
+constexpr int LU_PF = 4;
 template <typename VT, typename FT>
 struct LuRow {
     int row, k0, len;
