@@ -310,7 +310,15 @@ def test_jacobi_sweep_lusolve_matches_emulation(cuda, k, ell_columns):
         w = d.copy()
         for _ in range(k - 1):
             w = d - U @ w
-        z = torch.zeros(n, dtype=torch.float64, device=cuda)
-        P.lusolve(_dev(x, cuda), z)
-        P.sync()
-        assert np.allclose(z.cpu().numpy(), w, rtol=1e-12, atol=1e-13), (A.name, k)
+        from xsolver_b200 import _lib
+
+        got = []
+        for fuse in (1, 0):  # sweeps 2 and 3 in one pass, or in two
+            _lib.lib().xs_set_sweep_fusion(fuse)
+            z = torch.zeros(n, dtype=torch.float64, device=cuda)
+            P.lusolve(_dev(x, cuda), z)
+            P.sync()
+            got.append(z.cpu().numpy())
+        _lib.lib().xs_set_sweep_fusion(1)
+        assert np.array_equal(got[0], got[1]), (A.name, k)
+        assert np.allclose(got[0], w, rtol=1e-12, atol=1e-13), (A.name, k)

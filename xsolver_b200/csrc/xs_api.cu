@@ -65,6 +65,7 @@ TrsvTuning &trsv_tuning()
         if (const char *e = getenv("XS_TRSV_BACKOFF_NS")) t.backoff_ns = std::max(8, atoi(e));
         if (const char *e = getenv("XS_TRSV_CHUNK_ROWS")) t.chunk_rows = std::max(0, atoi(e));
         if (const char *e = getenv("XS_TRSV_BLOCK_ROWS")) t.block_max_rows = std::max(0, atoi(e));
+        if (const char *e = getenv("XS_SWEEP_FUSE")) t.fuse_sweeps = atoi(e) != 0;
         init = true;
     }
     return t;
@@ -413,6 +414,7 @@ static const double *host_vals(Handle &h)
 // values changed, same pattern
 static void update_values(Handle &h, const double *v)
 {
+    Trace tr("update_values", h.s);
     if (!h.have_matrix) throw Status(XS_ERR_ORDER);
     if (!v) throw Status(XS_ERR_INVALID);
     if (h.vperm.empty()) {
@@ -731,6 +733,7 @@ constexpr double INNER_SAFETY = 0.25;
 // Writes the conventions requested by the caller into usediter/resvec.
 static void solve_device(Handle &h, const double *d_b, double *d_x)
 {
+    Trace tr("solve_device", h.s);
     if (!h.have_matrix) throw Status(XS_ERR_ORDER);
     if (h.method == 0) throw Status(XS_ERR_ORDER);
     build_precond(h);
@@ -1122,6 +1125,11 @@ static int check_gpu()
 extern "C" {
 
 const char *xs_version(void) { return "xsolver_b200 1.0 (sm_100a)"; }
+
+int xs_set_sweep_fusion(int enable)
+{
+    return guarded([&] { trsv_tuning().fuse_sweeps = enable != 0; });
+}
 
 int xs_set_trsv_block_rows(int max_rows)
 {

@@ -318,8 +318,13 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
                     return T.ell_w > 0 && T.ell_dia ? (T.ell_w <= 8 ? 1.0 : 4.0) : 0.0;
                 };
                 const TriDev &Lt = h.M.L, &Ut = h.M.U;
-                const double l = (k - 1) * ((V + idx(Lt)) * Lt.nnz + msk(Lt) * n) + 2 * X * n + (k - 2) * 3 * X * n;
-                const double u = (k - 1) * ((V + idx(Ut)) * Ut.nnz + msk(Ut) * n) + 3 * X * n + (k - 2) * 4 * X * n;
+                // passes over each triangle: k-1, or k-2 when sweeps 2 and 3
+                // share one pass (its re-reads of neighbour rows are not
+                // compulsory traffic)
+                const bool fused = k >= 3 && Lt.ell_w > 0 && Ut.ell_w > 0 && trsv_tuning().fuse_sweeps;
+                const int P = fused ? k - 2 : k - 1;
+                const double l = P * ((V + idx(Lt)) * Lt.nnz + msk(Lt) * n) + 2 * X * n + (P - 1) * 3 * X * n;
+                const double u = P * ((V + idx(Ut)) * Ut.nnz + msk(Ut) * n) + 3 * X * n + (P - 1) * 4 * X * n;
                 *bytes = op == 3 ? l : (op == 4 ? u : l + u);
             }
             break;

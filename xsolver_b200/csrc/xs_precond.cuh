@@ -207,6 +207,37 @@ struct PrecondDev {
             k_diag_scale<VT, DT><<<g, 256, 0, s>>>(n, dinv, x, z, done_flag);
             return;
         }
+        // sweeps 2 and 3 of a triangle in one pass (ELL copies), further
+        // sweeps as single passes
+        auto pass23 = [&](const TriDev &T, bool upper, const VT *rhs, VT *yout) {
+            const FT *ev = T.evals<FT>();
+            const int *doff = T.doff.p;
+            const int gs = std::max(1, std::min(g, (n + 255) / 256));
+            auto go = [&](auto cols) {
+                using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
+                if (upper) k_trsv_sweep23_ell<VT, FT, DT, CT, true><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dinv, rhs, yout, done_flag);
+                else k_trsv_sweep23_ell<VT, FT, DT, CT, false><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, (const DT *)nullptr, rhs, yout, done_flag);
+            };
+            if (T.ell_dia && T.ell_w <= 8) go((const uint8_t *)T.emask8.p);
+            else if (T.ell_dia) go((const uint32_t *)T.emask32.p);
+            else if (T.ell16) go((const short *)T.eco.p);
+            else go((const int *)T.eci.p);
+        };
+        if (k >= 3 && L.ell_w > 0 && U.ell_w > 0 && trsv_tuning().fuse_sweeps) {
+            VT *cur = ta, *other = tb;
+            pass23(L, false, x, cur);
+            for (int t = 4; t <= k; t++) {
+                pass(L, false, false, x, cur, other);
+                std::swap(cur, other);
+            }
+            const VT *yv = cur;
+            const int rest = k - 3;  // single U passes after the fused pair
+            VT *first = (rest % 2 == 0) ? z : other;
+            pass23(U, true, yv, first);
+            VT *bufs[2] = {first, first == z ? other : z};
+            for (int t = 0; t < rest; t++) pass(U, true, false, yv, bufs[t & 1], bufs[(t + 1) & 1]);
+            return;
+        }
         // L: passes 2..k, result in `cur` (ta or tb)
         VT *cur = ta, *other = tb;
         pass(L, false, true, x, nullptr, cur);

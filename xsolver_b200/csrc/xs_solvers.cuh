@@ -44,13 +44,29 @@ struct GraphCache {
     GraphCache &operator=(const GraphCache &) = delete;
     cudaGraphExec_t exec = nullptr;
     std::vector<const void *> key;
+    // polling resources, created on first use and kept (a pinned allocation
+    // per solve would cost more than a short solve)
+    int *hflag = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
     void reset()
     {
         if (exec) cudaGraphExecDestroy(exec);
         exec = nullptr;
         key.clear();
     }
-    ~GraphCache() { reset(); }
+    void ensure_polling()
+    {
+        if (!hflag) XS_CUDA(cudaMallocHost((void **)&hflag, sizeof(int) * 2));
+        for (int q = 0; q < 2; q++)
+            if (!ev[q]) XS_CUDA(cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming));
+    }
+    ~GraphCache()
+    {
+        reset();
+        if (hflag) cudaFreeHost(hflag);
+        for (int q = 0; q < 2; q++)
+            if (ev[q]) cudaEventDestroy(ev[q]);
+    }
 };
 
 struct SolveCtx {
@@ -76,6 +92,7 @@ inline void run_graph_loop(SolveCtx &c, GraphCache &gc, const std::vector<const 
                            int max_launches, Body body)
 {
     if (!gc.exec || gc.key != key) {
+        Trace tr("graph capture", c.s);
         gc.reset();
         cudaGraph_t g;
         XS_CUDA(cudaStreamBeginCapture(c.s, cudaStreamCaptureModeRelaxed));
@@ -97,11 +114,9 @@ inline void run_graph_loop(SolveCtx &c, GraphCache &gc, const std::vector<const 
         gc.key = key;
     }
     // pipelined polling: check launch k-1's flag after enqueueing launch k
-    int *hflag = nullptr;
-    XS_CUDA(cudaMallocHost((void **)&hflag, sizeof(int) * 2));
-    cudaEvent_t ev[2];
-    XS_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-    XS_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    gc.ensure_polling();
+    int *hflag = gc.hflag;
+    cudaEvent_t *ev = gc.ev;
     KState *dst = c.W->st.p;
     bool stop = false;
     for (int l = 0; l < max_launches && !stop; l++) {
@@ -115,9 +130,6 @@ inline void run_graph_loop(SolveCtx &c, GraphCache &gc, const std::vector<const 
         }
     }
     XS_CUDA(cudaStreamSynchronize(c.s));
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
-    cudaFreeHost(hflag);
 }
 
 // ---------------------------------------------------------------- PCG (cgm)
