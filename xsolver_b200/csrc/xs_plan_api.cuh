@@ -321,7 +321,10 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes)
                 // passes over each triangle: k-1, or k-2 when sweeps 2 and 3
                 // share one pass (its re-reads of neighbour rows are not
                 // compulsory traffic)
-                const bool fused = k >= 3 && Lt.ell_w > 0 && Ut.ell_w > 0 && trsv_tuning().fuse_sweeps;
+                auto fusable = [&](const TriDev &T) {
+                    return T.ell_w > 0 && T.ell_dia && T.ell_w <= (fp == 0 ? 3 : 4);
+                };
+                const bool fused = k >= 3 && fusable(Lt) && fusable(Ut) && trsv_tuning().fuse_sweeps;
                 const int P = fused ? k - 2 : k - 1;
                 const double l = P * ((V + idx(Lt)) * Lt.nnz + msk(Lt) * n) + 2 * X * n + (P - 1) * 3 * X * n;
                 const double u = P * ((V + idx(Ut)) * Ut.nnz + msk(Ut) * n) + 3 * X * n + (P - 1) * 4 * X * n;

@@ -207,23 +207,31 @@ struct PrecondDev {
             k_diag_scale<VT, DT><<<g, 256, 0, s>>>(n, dinv, x, z, done_flag);
             return;
         }
-        // sweeps 2 and 3 of a triangle in one pass (ELL copies), further
-        // sweeps as single passes
+        // sweeps 2 and 3 of a triangle in one pass (diagonal-slot copies with
+        // few slots), further sweeps as single passes
         auto pass23 = [&](const TriDev &T, bool upper, const VT *rhs, VT *yout) {
             const FT *ev = T.evals<FT>();
-            const int *doff = T.doff.p;
             const int gs = std::max(1, std::min(g, (n + 255) / 256));
-            auto go = [&](auto cols) {
-                using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
-                if (upper) k_trsv_sweep23_ell<VT, FT, DT, CT, true><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dinv, rhs, yout, done_flag);
-                else k_trsv_sweep23_ell<VT, FT, DT, CT, false><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, (const DT *)nullptr, rhs, yout, done_flag);
-            };
-            if (T.ell_dia && T.ell_w <= 8) go((const uint8_t *)T.emask8.p);
-            else if (T.ell_dia) go((const uint32_t *)T.emask32.p);
-            else if (T.ell16) go((const short *)T.eco.p);
-            else go((const int *)T.eci.p);
+            const uint8_t *m = T.emask8.p;
+            const int *doff = T.doff.p;
+            const DT *dv = upper ? dinv : (const DT *)nullptr;
+#define XS_SW23(WW)                                                                                                  \
+    case WW:                                                                                                         \
+        if (upper) k_trsv_sweep23_dia<WW, VT, FT, DT, true><<<gs, 256, 0, s>>>(n, m, doff, ev, dv, rhs, yout, done_flag); \
+        else k_trsv_sweep23_dia<WW, VT, FT, DT, false><<<gs, 256, 0, s>>>(n, m, doff, ev, dv, rhs, yout, done_flag);     \
+        break;
+            switch (T.ell_w) {
+                XS_SW23(1) XS_SW23(2) XS_SW23(3) XS_SW23(4)
+            default: throw Status(XS_ERR_INVALID);
+            }
+#undef XS_SW23
         };
-        if (k >= 3 && L.ell_w > 0 && U.ell_w > 0 && trsv_tuning().fuse_sweeps) {
+        // a row keeps W^2 neighbour values and gathers in registers: at most
+        // 4 slots (3 for 8-byte vectors) stay within the register budget
+        auto fusable = [](const TriDev &T) {
+            return T.ell_w > 0 && T.ell_dia && T.ell_w <= (sizeof(VT) >= 8 ? 3 : 4);
+        };
+        if (k >= 3 && fusable(L) && fusable(U) && trsv_tuning().fuse_sweeps) {
             VT *cur = ta, *other = tb;
             pass23(L, false, x, cur);
             for (int t = 4; t <= k; t++) {

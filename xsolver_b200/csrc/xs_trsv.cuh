@@ -481,44 +481,21 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, i
     }
 }
 
-// Sweeps 2 and 3 in one pass (the first sweep folded in as in FIRST2):
+// Sweeps 2 and 3 in one pass (the first sweep folded in as in FIRST2), for
+// diagonal-slot copies with W <= 4 slots (W a compile-time constant):
 //   L: y3_i = x_i - sum_j L_ij y2_j,  y2_j = x_j - sum_k L_jk x_k
 //   U: w3_i = d_i - sum_j U_ij w2_j,  w2_j = d_j - sum_k U_jk d_k,  d = dinv*y
-// Each row recomputes y2 / w2 at its own neighbours instead of reading them
-// from a grid-wide first pass: the neighbours' slot data is read again but
-// mostly from L2 (neighbours are rows being swept at the same time), and the
-// first pass's write and read of y2 and its second read of the factor and of
-// x disappear — about half the DRAM traffic of two passes, one launch instead
-// of two.  Every y2_j / w2_j is computed with the same operations in the same
-// order as the separate pass, so the result is identical.
-template <typename VT, typename FT, typename DT, typename CT, bool UPPER>
-__device__ __forceinline__ VT sweep_inner(int j, int n, int w, long ld, const CT *__restrict__ eci,
-                                          const int *s_off, const FT *__restrict__ ev, const DT *__restrict__ dinv,
-                                          const VT *__restrict__ x)
-{
-    VT acc = UPPER ? (VT)(__ldg(x + j) * (VT)__ldg(dinv + j)) : __ldg(x + j);
-    unsigned m = 0;
-    if constexpr (EllDiag<CT>::value) m = (unsigned)__ldg(eci + j);
-    for (int b = 0; b < w; b++) {
-        const long o = (long)b * ld + j;
-        int k;
-        bool pr;
-        if constexpr (EllDiag<CT>::value) {
-            pr = (m >> b) & 1u;
-            k = min(max(j + s_off[b], 0), n - 1);
-        } else {
-            pr = true;
-            k = ell_col<CT>(__ldg(eci + o), j);
-        }
-        const VT yk = UPPER ? (VT)(__ldg(x + k) * (VT)__ldg(dinv + k)) : __ldg(x + k);
-        const VT v = (VT)FVal<FT>::ld(ev, o);
-        if (pr) acc = msub(acc, yk, v);
-    }
-    return acc;
-}
-
-template <typename VT, typename FT, typename DT, typename CT, bool UPPER>
-__global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep23_ell(int n, int w, const CT *__restrict__ eci,
+// Each row recomputes y2 / w2 at its W neighbours instead of reading them
+// from a grid-wide first pass.  With diagonal slots every address is known
+// from the row index alone, so all loads of a row — its mask and values, its
+// neighbours' masks and values, and the gathers of x (and dinv) — issue in
+// one round; the neighbours' slot data comes mostly from L2 (rows being swept
+// at the same time).  The first pass's write and read of y2 and its second
+// read of the factor disappear: about half the DRAM traffic of two passes,
+// one launch instead of two.  y2_j / w2_j are computed with the operations
+// and order of the separate pass, so the result is identical.
+template <int W, typename VT, typename FT, typename DT, bool UPPER>
+__global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep23_dia(int n, const uint8_t *__restrict__ mask,
                                                                            const int *__restrict__ doff,
                                                                            const FT *__restrict__ ev,
                                                                            const DT *__restrict__ dinv,
@@ -526,28 +503,39 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep23_ell(int n,
                                                                            VT *__restrict__ yout, const int *done_flag)
 {
     if (done_flag && *done_flag) return;
-    __shared__ int s_off[ELL_DIA_MAX];
-    ell_stage_offsets<CT>(doff, w, s_off);
+    int off[W];
+#pragma unroll
+    for (int a = 0; a < W; a++) off[a] = __ldg(doff + a);
     const long ld = ell_ld(n);
+    auto xin = [&](int c) -> VT { return UPPER ? (VT)(__ldg(x + c) * (VT)__ldg(dinv + c)) : __ldg(x + c); };
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        VT acc = UPPER ? (VT)(x[i] * (VT)dinv[i]) : x[i];
-        unsigned m = 0;
-        if constexpr (EllDiag<CT>::value) m = (unsigned)__ldg(eci + i);
-        for (int a = 0; a < w; a++) {
-            const long o = (long)a * ld + i;
-            int j;
-            bool pr;
-            if constexpr (EllDiag<CT>::value) {
-                pr = (m >> a) & 1u;
-                j = min(max(i + s_off[a], 0), n - 1);
-            } else {
-                pr = true;
-                j = ell_col<CT>(__ldg(eci + o), i);
+        const unsigned mi = __ldg(mask + i);
+        int j[W];
+        VT vi[W];
+        unsigned mj[W];
+        VT xj[W];
+        VT vj[W][W], xk[W][W];
+#pragma unroll
+        for (int a = 0; a < W; a++) {
+            j[a] = min(max(i + off[a], 0), n - 1);
+            vi[a] = (VT)FVal<FT>::ld(ev, (long)a * ld + i);
+            mj[a] = __ldg(mask + j[a]);
+            xj[a] = xin(j[a]);
+#pragma unroll
+            for (int b = 0; b < W; b++) {
+                vj[a][b] = (VT)FVal<FT>::ld(ev, (long)b * ld + j[a]);
+                xk[a][b] = xin(min(max(j[a] + off[b], 0), n - 1));
             }
-            if (!pr) continue;
-            const VT v = (VT)FVal<FT>::ld(ev, o);
-            const VT y2 = sweep_inner<VT, FT, DT, CT, UPPER>(j, n, w, ld, eci, s_off, ev, dinv, x);
-            acc = msub(acc, y2, v);
+        }
+        VT acc = xin(i);
+#pragma unroll
+        for (int a = 0; a < W; a++) {
+            if (!((mi >> a) & 1u)) continue;
+            VT y2 = xj[a];
+#pragma unroll
+            for (int b = 0; b < W; b++)
+                if ((mj[a] >> b) & 1u) y2 = msub(y2, xk[a][b], vj[a][b]);
+            acc = msub(acc, y2, vi[a]);
         }
         yout[i] = acc;
     }
