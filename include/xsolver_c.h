@@ -305,10 +305,11 @@ int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
  * hand-off per level).  0 disables it; default: no row limit beyond the
  * shared-memory one.  Environment XS_TRSV_BLOCK_ROWS sets it at first use. */
 int xs_set_trsv_block_rows(int max_rows);
-/* Jacobi-sweep preconditioner apply: 1 (default) computes sweeps 2 and 3 of
- * each triangle in one pass (each row recomputes the second-sweep values of
- * its neighbours; same result, about half the memory traffic), 0 runs them
- * as separate passes.  Environment XS_SWEEP_FUSE sets it at first use. */
+/* Jacobi-sweep preconditioner apply: 1 computes sweeps 2 and 3 of each
+ * narrow diagonal-slot triangle in one pass (each row recomputes the
+ * second-sweep values of its neighbours; same result, about half the DRAM
+ * traffic, more L2 traffic), 0 (default) runs them as separate passes.
+ * Environment XS_SWEEP_FUSE sets it at first use. */
 int xs_set_sweep_fusion(int enable);
 /* Column storage of ELL copies (the ELL SpMV and the Jacobi-sweep triangle
  * copies).  index_bits 0 (default): diagonal slots when every entry lies on

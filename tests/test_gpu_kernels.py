@@ -319,6 +319,6 @@ def test_jacobi_sweep_lusolve_matches_emulation(cuda, k, ell_columns):
             P.lusolve(_dev(x, cuda), z)
             P.sync()
             got.append(z.cpu().numpy())
-        _lib.lib().xs_set_sweep_fusion(1)
+        _lib.lib().xs_set_sweep_fusion(0)
         assert np.array_equal(got[0], got[1]), (A.name, k)
         assert np.allclose(got[0], w, rtol=1e-12, atol=1e-13), (A.name, k)
