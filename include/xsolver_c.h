@@ -148,6 +148,12 @@ int xs_pc_set_trsv(xs_handle_t h, int mode);
 int xs_set_precision(xs_handle_t h, const char *outer, const char *inner, const char *factor);
 int xs_set_inner(xs_handle_t h, double inner_rtol, int inner_maxiter);
 int xs_set_compat(xs_handle_t h, int reference_quirks);
+/* Mixed-precision BiCGSTAB: 1 (default) keeps one FP32 BiCGSTAB iteration
+ * running across the refinement steps (at each step x += d in FP64, the FP64
+ * residual b - A x replaces the inner residual, and the iteration continues
+ * with its search directions); 0 restarts the inner solve at every step on
+ * r/||r|| (classic iterative refinement, as for the other methods). */
+int xs_set_refinement_mode(xs_handle_t h, int carry_krylov);
 /* host rhs/sol (sol = x0 on entry) */
 int xs_solve(xs_handle_t h, const double *rhs, double *sol);
 /* device-resident rhs/sol (device pointers, n doubles each) */

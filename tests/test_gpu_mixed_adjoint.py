@@ -15,15 +15,18 @@ from xsolver_b200 import stencils as st
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("ksp", ["bicgstab", "gmres"])
+@pytest.mark.parametrize("ksp,carry", [("bicgstab", True), ("bicgstab", False), ("gmres", False)])
 @pytest.mark.parametrize("factor", ["fp32", "bf16", "fp16"])
-def test_mixed_refinement_reaches_1e10(cuda, ksp, factor):
+def test_mixed_refinement_reaches_1e10(cuda, ksp, carry, factor):
+    """carry: BiCGSTAB keeps one FP32 iteration across the refinement steps
+    (residual replaced by the FP64 residual at each step) instead of
+    restarting it."""
     from xsolver_b200.api import Solver
 
     A = st.poisson3d_7pt(40) if ksp == "bicgstab" else st.convdiff3d_27pt(20)
     b = st.rhs_uniform(A.n, 0, -1.0 if ksp == "bicgstab" else 0.0, 1.0)
     S = Solver(A).ksp_settype(ksp).ksp_setoption(1e-10, 2000, 30).pc_settype("ilu0")
-    S.set_precision("fp64", "fp32", factor).set_inner(1e-4, 200)
+    S.set_precision("fp64", "fp32", factor).set_inner(1e-4, 200).set_refinement_mode(carry)
     x = S.solve(b)
     r = b - A.to_scipy() @ x
     relres = np.linalg.norm(r) / np.linalg.norm(b)

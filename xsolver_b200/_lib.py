@@ -52,6 +52,7 @@ def _declare(L):
         "xs_destroy": [C.c_void_p],
         "xs_mat_setup": [C.c_void_p, C.c_int, _ip, _ip, _dp, C.c_int],
         "xs_mat_update": [C.c_void_p, _dp],
+        "xs_set_refinement_mode": [C.c_void_p, C.c_int],
         "xs_ksp_settype": [C.c_void_p, C.c_char_p],
         "xs_ksp_setoption": [C.c_void_p, C.c_double, C.c_int, _ip, _dp, C.c_int],
         "xs_ksp_set_absolute_tol": [C.c_void_p, C.c_double],

@@ -113,6 +113,10 @@ class Solver:
         check(self._L.xs_set_inner(self.h, rtol, maxiter), "set_inner")
         return self
 
+    def set_refinement_mode(self, carry_krylov: bool):
+        check(self._L.xs_set_refinement_mode(self.h, 1 if carry_krylov else 0), "set_refinement_mode")
+        return self
+
     def set_compat(self, quirks: int):
         check(self._L.xs_set_compat(self.h, quirks), "set_compat")
         return self

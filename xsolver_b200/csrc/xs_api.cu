@@ -300,6 +300,9 @@ struct Handle {
     int factor_prec = FP_F64;
     double inner_rtol = 1e-4;
     int inner_maxiter = 200;
+    // mixed BiCGSTAB: refinement steps continue one inner iteration (true
+    // residual replaced at each step) instead of restarting it
+    int carry_krylov = 1;
     int last_outer = 0;
     // work
     Workspace W;
@@ -706,7 +709,7 @@ __global__ void k_d2f(int n, const double *__restrict__ a, float *__restrict__ b
 // x += d * scale (FP64 update of the refinement)
 __global__ void k_refine_update(int n, double *__restrict__ x, const float *__restrict__ d, const double *scale)
 {
-    const double s = *scale;
+    const double s = scale ? *scale : 1.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = x[i] + (double)d[i] * s;
 }
 template <typename VT>
@@ -774,6 +777,83 @@ static void solve_device(Handle &h, const double *d_b, double *d_x)
             }
         }
         h.last_outer = 0;
+    } else if (h.method == KSP_BICGSTAB && h.carry_krylov) {
+        // ---- mixed precision refinement carrying the Krylov iteration
+        // One FP32 BiCGSTAB runs across all refinement steps.  A step ends
+        // when its recurrence residual has dropped by the inner tolerance;
+        // then x += d (FP64), r = b - A x (FP64), the inner residual is
+        // replaced by float(r) and beta = (rhat, r) recomputed, and the same
+        // iteration continues (p, u, rhat and the scalars are kept) — a
+        // restart would throw away the search space it has built.  Vectors
+        // stay unscaled (FP32 range covers the 1e10 reduction).
+        DBuf<OuterState> &os_buf = h.outer_st;
+        if (!os_buf.p) os_buf.alloc(1);
+        OuterState *os = os_buf.p;
+        double *r = h.vpool64.get(2, n);
+        float *r32 = h.vpool32.get(0, n), *d32 = h.vpool32.get(1, n);
+        operator_ensure32(h.A, h.hrp.data(), h.s);
+        h.W.ensure(64, std::max(h.maxiter, 1) + 8);  // history capacity for the whole solve
+        prepare_state(h, std::max(h.inner_maxiter, 1), h.inner_rtol, 0.0, true);
+        const RedSlot sl = h.W.slot();
+        spmv<double, double>(h.A, x, r, EpiOuterResid<double>{os, b}, sl, h.s);
+        OuterState hos;
+        XS_CUDA(cudaMemcpyAsync(&hos, os, sizeof(OuterState), cudaMemcpyDeviceToHost, h.s));
+        XS_CUDA(cudaStreamSynchronize(h.s));
+        const double r0 = hos.rnorm;
+        hist.push_back(r0);
+        double rn = r0;
+        int outer = 0, it_prev = 0;
+        const int max_outer = 100;
+        done = 0;
+        SolveCtx c{h.s, &h.A, &h.M, &h.W, n, 8, h.quirk, &h.launches};
+        if (n < 200000) c.chunk = 16;
+        BicgRun<float, float> &bi = h.r32.bicg;
+        while (true) {
+            if (!(rn == rn)) { devflags |= DEV_NAN; done = 3; break; }
+            if (rn == 0.0 || rn / (r0 + KSMALL) < h.tol || rn <= h.abstol) { done = 1; break; }
+            if (iters >= h.maxiter || outer >= max_outer) { done = 2; break; }
+            const double target = std::max(h.tol * (r0 + KSMALL), h.abstol);
+            const double irtol = std::min(std::max(h.inner_rtol, INNER_SAFETY * target / rn), 0.5);
+            const int more = std::max(1, std::min(h.inner_maxiter, h.maxiter - iters));
+            XS_CUDA(cudaMemsetAsync(d32, 0, sizeof(float) * n, h.s));
+            if (outer == 0) {
+                k_d2f<<<geom().sms * 4, 256, 0, h.s>>>(n, r, r32, nullptr);
+                check_launch();
+                prepare_state(h, more, irtol, 0.0, true);
+                bi.run(c, r32, d32, false);
+            } else {
+                float *ri = bi.residual(n);
+                k_d2f<<<geom().sms * 4, 256, 0, h.s>>>(n, r, ri, nullptr);
+                // clear done first: vector ops skip their work while it is set
+                k_resume_state<<<1, 1, 0, h.s>>>(h.W.st.p, rn, irtol, more);
+                check_launch();
+                vecop(OpBicgRho<float>{n, h.W.st.p, bi.shadow(n), ri}, sl, h.s);
+                h.W.h_st->maxiter = more;  // iterations this step may add (caps the graph replays)
+                bi.run(c, r32, d32, true);
+            }
+            XS_CUDA(cudaMemcpyAsync(h.W.h_st, h.W.st.p, sizeof(KState), cudaMemcpyDeviceToHost, h.s));
+            XS_CUDA(cudaStreamSynchronize(h.s));
+            const int it_in = h.W.h_st->iter - it_prev;
+            it_prev = h.W.h_st->iter;
+            devflags |= h.W.h_st->err;
+            if (devflags & (DEV_TRSV_TIMEOUT | DEV_TMA_TIMEOUT)) { done = 3; break; }
+            k_refine_update<<<geom().sms * 4, 256, 0, h.s>>>(n, x, d32, nullptr);
+            check_launch();
+            spmv<double, double>(h.A, x, r, EpiOuterResid<double>{os, b}, sl, h.s);
+            XS_CUDA(cudaMemcpyAsync(&hos, os, sizeof(OuterState), cudaMemcpyDeviceToHost, h.s));
+            XS_CUDA(cudaStreamSynchronize(h.s));
+            iters += std::max(it_in, 1);
+            h.launches += 8;  // replacement, rho, resume, refinement update, outer residual
+            rn = hos.rnorm;
+            hist.push_back(rn);
+            outer++;
+            if (h.W.h_st->done == 3 && (devflags & (DEV_BREAKDOWN | DEV_NAN))) { done = 3; break; }
+        }
+        h.last_outer = outer;
+        h.final_relres = rn / (r0 + KSMALL);
+        if (h.resvec) {
+            for (size_t k = 0; k < hist.size(); k++) h.resvec[k] = h.intel_conv ? hist[k] / (r0 + KSMALL) : hist[k];
+        }
     } else {
         // ---- mixed precision iterative refinement
         // outer: r = b - A x (FP64), x += d (FP64); inner: FP32 solve of
@@ -1329,6 +1409,13 @@ int xs_set_inner(xs_handle_t h, double rtol, int maxit)
         if (!(rtol > 0) || maxit < 1) throw Status(XS_ERR_INVALID);
         h->h->inner_rtol = rtol;
         h->h->inner_maxiter = maxit;
+    });
+}
+int xs_set_refinement_mode(xs_handle_t h, int carry_krylov)
+{
+    return guarded([&] {
+        HCHK(h);
+        h->h->carry_krylov = carry_krylov != 0;
     });
 }
 int xs_set_compat(xs_handle_t h, int q)

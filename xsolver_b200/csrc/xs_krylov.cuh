@@ -481,6 +481,38 @@ struct OpBicgX {
     }
 };
 
+// Residual replacement in a running BiCGSTAB (mixed-precision refinement
+// without restart): r was just overwritten by the true residual, so
+// beta = (rhat, r) is recomputed and the pending omega, which is
+// proportional to beta, rescaled with it.
+template <typename VT>
+struct OpBicgRho {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    const VT *rhat, *r;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[1]) const { a[0] += (double)rhat[i] * (double)r[i]; }
+    __device__ void finalize(const double *t) const
+    {
+        const double old = st->sc[S_BETA], beta = t[0];
+        st->sc[S_OMEGA] = st->sc[S_OMEGA] * (beta / (old + KSMALL));
+        st->sc[S_BETA] = beta;
+        st->sc[S_BETO] = beta;
+        if (!isfinite(beta)) { st->err |= DEV_BREAKDOWN; st->done = 3; }
+    }
+};
+
+// continue a stopped solve: new stopping test (relative to res0), the
+// iteration cap raised by `more`, done cleared; scalars and history kept
+__global__ void k_resume_state(KState *st, double res0, double tol, int more)
+{
+    st->res0 = res0;
+    st->tol = tol;
+    st->maxiter = st->iter + more;
+    st->done = 0;
+}
+
 // restarted methods: res0 = ||res|| ; beta = res0
 template <typename VT>
 struct OpGmInit {

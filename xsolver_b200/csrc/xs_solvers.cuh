@@ -208,7 +208,11 @@ template <typename VT, typename MT>
 struct BicgRun {
     VecPool<VT> pool;
     GraphCache gc;
-    void run(SolveCtx &c, const VT *b, VT *x)
+    VT *residual(int n) { return pool.get(0, n); }
+    VT *shadow(int n) { return pool.get(1, n); }
+    // resume: continue the previous run's iteration (same p, u, rhat and
+    // scalars; r may have been replaced meanwhile) instead of starting anew
+    void run(SolveCtx &c, const VT *b, VT *x, bool resume = false)
     {
         const int n = c.n;
         VT *r = pool.get(0, n), *rhat = pool.get(1, n), *p = pool.get(2, n), *u = pool.get(3, n);
@@ -216,8 +220,10 @@ struct BicgRun {
         KState *st = c.W->st.p;
         RedSlot sl = c.W->slot();
         const int *done = &st->done;
-        spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
-        vecop(OpBicgInit<VT>{n, st, r, rhat, p, u}, sl, c.s);
+        if (!resume) {
+            spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
+            vecop(OpBicgInit<VT>{n, st, r, rhat, p, u}, sl, c.s);
+        }
         auto body = [&]() {
             vecop(OpBicgP<VT>{n, st, p, r, u, (VT)0, (VT)0}, sl, c.s);
             c.M->apply<VT>(p, z1, done, c.s);
