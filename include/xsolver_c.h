@@ -317,6 +317,13 @@ int xs_set_trsv_block_rows(int max_rows);
  * traffic, more L2 traffic), 0 (default) runs them as separate passes.
  * Environment XS_SWEEP_FUSE sets it at first use. */
 int xs_set_sweep_fusion(int enable);
+/* Programmatic dependent launch for the kernels of the Krylov iterations
+ * (SpMV, vector updates, Jacobi sweeps): 1 (default) lets a kernel start
+ * while its predecessor drains (each waits on the hardware dependency before
+ * touching the predecessor's results), 0 serialises them fully.  Results are
+ * identical either way.  Environment XS_PDL sets it at first use; graphs
+ * captured earlier keep the mode they were captured with. */
+int xs_set_launch_overlap(int enable);
 /* Column storage of ELL copies (the ELL SpMV and the Jacobi-sweep triangle
  * copies).  index_bits 0 (default): diagonal slots when every entry lies on
  * one of at most 32 diagonals with at most 25% padding (stencil matrices):

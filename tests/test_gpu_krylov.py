@@ -267,3 +267,29 @@ def test_gmres_gcr_parilut_convdiff(cuda):
                                                    quirk=0)
         assert abs(S.usediter - (uo + (0 if om == "hip_igcr" else 1))) <= 1
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
+
+
+def test_launch_overlap_gives_identical_results(cuda):
+    """Programmatic dependent launch only changes when kernels start: the
+    FP64 BiCGSTAB and mixed-precision solves are bit-identical with it off."""
+    from xsolver_b200 import _lib
+
+    A = st.poisson3d_7pt(40)
+    b = st.rhs_uniform(A.n, 3)
+    L = _lib.lib()
+    out = []
+    try:
+        for on in (1, 0):
+            assert L.xs_set_launch_overlap(on) == 0
+            for fmt in ("csr", "ell"):
+                S = _solver(A, "bicgstab", "ilu0", 1e-10, 500, fmt=fmt)
+                S.pc_set_trsv(3)
+                x64 = S.solve(b)
+                S.set_precision("fp64", "fp32", "bf16")
+                xm = S.solve(b)
+                out.append((x64, xm, S.resvec()))
+                S.close()
+    finally:
+        L.xs_set_launch_overlap(1)
+    for a, c in zip(out[:2], out[2:]):
+        assert np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1]) and np.array_equal(a[2], c[2])

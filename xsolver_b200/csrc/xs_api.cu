@@ -44,6 +44,17 @@ Geom &geom()
     return g;
 }
 
+PdlTuning &pdl_tuning()
+{
+    static PdlTuning t;
+    static bool init = false;
+    if (!init) {
+        if (const char *e = getenv("XS_PDL")) t.enabled = atoi(e) != 0;
+        init = true;
+    }
+    return t;
+}
+
 FormatTuning &format_tuning()
 {
     static FormatTuning t;
@@ -1205,6 +1216,11 @@ static int check_gpu()
 extern "C" {
 
 const char *xs_version(void) { return "xsolver_b200 1.0 (sm_100a)"; }
+
+int xs_set_launch_overlap(int enable)
+{
+    return guarded([&] { pdl_tuning().enabled = enable != 0; });
+}
 
 int xs_set_sweep_fusion(int enable)
 {

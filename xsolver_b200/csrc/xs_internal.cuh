@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <chrono>
+#include <utility>
 
 #include "../../include/xsolver_c.h"
 
@@ -79,6 +80,39 @@ struct Status {
     int code;
     explicit Status(int c) : code(c) {}
 };
+
+// ---------------------------------------------------------------- programmatic dependent launch
+// Kernels of the Krylov iteration bodies are launched with programmatic
+// stream serialization: a kernel may start while its predecessor on the
+// stream drains, run its independent prologue (shared-memory staging, loads
+// of constant matrix data), and must execute pdl_wait() before it reads
+// anything the predecessor produced or writes anything the predecessor
+// reads.  pdl_trigger() lets the successor launch once every block of this
+// kernel has started.  Outside a programmatic launch both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+struct PdlTuning {
+    int enabled = 1;
+};
+PdlTuning &pdl_tuning();
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdl_tuning().enabled ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+    if (e != cudaSuccess) throw Status(XS_ERR_CUDA);
+}
 
 inline void check_launch()
 {

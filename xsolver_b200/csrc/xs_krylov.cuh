@@ -37,6 +37,8 @@ __global__ void __launch_bounds__(256, 8) k_vecop(Op op, RedSlot slot)
 {
     constexpr int KK = Op::K > 0 ? Op::K : 1;
     __shared__ double tot[KK];
+    pdl_trigger();
+    pdl_wait();
     if (op.st->done) return;
     Op o = op;
     o.load();
@@ -54,8 +56,7 @@ __global__ void __launch_bounds__(256, 8) k_vecop(Op op, RedSlot slot)
 template <class Op>
 inline void vecop(const Op &op, RedSlot slot, cudaStream_t s)
 {
-    k_vecop<Op><<<geom().red_grid, 256, 0, s>>>(op, slot);
-    check_launch();
+    launch_pdl(k_vecop<Op>, dim3(geom().red_grid), dim3(256), 0, s, op, slot);
 }
 
 // single-thread scalar step

@@ -179,11 +179,11 @@ struct PrecondDev {
                     using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
                     const DT *dv = upper ? dinv : (const DT *)nullptr;
                     if (upper) {
-                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, true, true><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
-                        else k_trsv_sweep_ell<VT, FT, DT, CT, true, false><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        if (first2) launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, true, true>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        else launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, true, false>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
                     } else {
-                        if (first2) k_trsv_sweep_ell<VT, FT, DT, CT, false, true><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
-                        else k_trsv_sweep_ell<VT, FT, DT, CT, false, false><<<gs, 256, 0, s>>>(n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        if (first2) launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, false, true>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        else launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, false, false>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
                     }
                 };
                 if (T.ell_dia && T.ell_w <= 8) go((const uint8_t *)T.emask8.p);
@@ -194,12 +194,12 @@ struct PrecondDev {
                 // CSR: the first sweep is a separate pass (yin = null -> y_1)
                 if (first2) {
                     VT *tmp = tc;  // distinct from every buffer the stages read or write
-                    if (upper) k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), dinv, rhs, (const VT *)nullptr, tmp, 1, done_flag);
-                    else k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), (const DT *)nullptr, rhs, (const VT *)nullptr, tmp, 1, done_flag);
+                    if (upper) launch_pdl(k_trsv_sweep<VT, FT, DT, true>, dim3(g), dim3(256), 0, s, n, T.rp_nat, T.ci_nat, natvals<FT>(T), dinv, rhs, (const VT *)nullptr, tmp, 1, done_flag);
+                    else launch_pdl(k_trsv_sweep<VT, FT, DT, false>, dim3(g), dim3(256), 0, s, n, T.rp_nat, T.ci_nat, natvals<FT>(T), (const DT *)nullptr, rhs, (const VT *)nullptr, tmp, 1, done_flag);
                     yin = tmp;
                 }
-                if (upper) k_trsv_sweep<VT, FT, DT, true><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), dinv, rhs, yin, yout, 0, done_flag);
-                else k_trsv_sweep<VT, FT, DT, false><<<g, 256, 0, s>>>(n, T.rp_nat, T.ci_nat, natvals<FT>(T), (const DT *)nullptr, rhs, yin, yout, 0, done_flag);
+                if (upper) launch_pdl(k_trsv_sweep<VT, FT, DT, true>, dim3(g), dim3(256), 0, s, n, T.rp_nat, T.ci_nat, natvals<FT>(T), dinv, rhs, yin, yout, 0, done_flag);
+                else launch_pdl(k_trsv_sweep<VT, FT, DT, false>, dim3(g), dim3(256), 0, s, n, T.rp_nat, T.ci_nat, natvals<FT>(T), (const DT *)nullptr, rhs, yin, yout, 0, done_flag);
             }
         };
         if (k <= 1) {

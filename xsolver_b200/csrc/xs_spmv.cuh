@@ -124,6 +124,8 @@ __global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const
                                                         Epi epi, RedSlot slot)
 {
     constexpr int KK = Epi::K > 0 ? Epi::K : 1;
+    pdl_trigger();
+    pdl_wait();
     if (!epi.active()) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bars[2];
@@ -441,10 +443,12 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_ell_spmv(EllArgs<MT, CT
 {
     constexpr int KK = Epi::K > 0 ? Epi::K : 1;
     constexpr int R = ell_rows_for<MT>();
-    if (!epi.active()) return;
     __shared__ double tot[KK];
     __shared__ int s_off[ELL_DIA_MAX];
-    ell_stage_offsets<CT>(A.doff, A.w, s_off);
+    ell_stage_offsets<CT>(A.doff, A.w, s_off);  // constant data: before the dependency wait
+    pdl_trigger();
+    pdl_wait();
+    if (!epi.active()) return;
     double acc[KK];
 #pragma unroll
     for (int k = 0; k < KK; k++) acc[k] = 0.0;
@@ -616,8 +620,7 @@ inline void launch_csr(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot 
     else a = op.csr32();
     int g = grid > 0 ? grid : spmv_grid<VT, MT, Epi>(t.nblocks, t.cap);
     size_t sm = spmv_smem<MT>(t.cap);
-    k_csr_spmv_tiled<VT, MT, Epi><<<g, SPMV_THREADS, sm, s>>>(a, x, y, epi, slot);
-    check_launch();
+    launch_pdl(k_csr_spmv_tiled<VT, MT, Epi>, dim3(g), dim3(SPMV_THREADS), sm, s, a, x, y, epi, slot);
 }
 
 template <typename VT, typename MT, typename Epi>
@@ -626,11 +629,14 @@ inline void launch_ell(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot 
     // the grid covers the rows at ell_rows_for<MT>() rows per thread
     const int g = (int)std::min<long>((long)op.ell_grid * ELL_ROWS / ell_rows_for<MT>(),
                                       (op.n + 256L * ell_rows_for<MT>() - 1) / (256L * ell_rows_for<MT>()));
-    if (op.ell_dia && op.ell_w <= 8) k_ell_spmv<VT, MT, uint8_t, Epi><<<g, 256, 0, s>>>(op.ell<MT, uint8_t>(), x, y, epi, slot);
-    else if (op.ell_dia) k_ell_spmv<VT, MT, uint32_t, Epi><<<g, 256, 0, s>>>(op.ell<MT, uint32_t>(), x, y, epi, slot);
-    else if (op.ell16) k_ell_spmv<VT, MT, short, Epi><<<g, 256, 0, s>>>(op.ell<MT, short>(), x, y, epi, slot);
-    else k_ell_spmv<VT, MT, int, Epi><<<g, 256, 0, s>>>(op.ell<MT, int>(), x, y, epi, slot);
-    check_launch();
+    if (op.ell_dia && op.ell_w <= 8)
+        launch_pdl(k_ell_spmv<VT, MT, uint8_t, Epi>, dim3(g), dim3(256), 0, s, op.ell<MT, uint8_t>(), x, y, epi, slot);
+    else if (op.ell_dia)
+        launch_pdl(k_ell_spmv<VT, MT, uint32_t, Epi>, dim3(g), dim3(256), 0, s, op.ell<MT, uint32_t>(), x, y, epi, slot);
+    else if (op.ell16)
+        launch_pdl(k_ell_spmv<VT, MT, short, Epi>, dim3(g), dim3(256), 0, s, op.ell<MT, short>(), x, y, epi, slot);
+    else
+        launch_pdl(k_ell_spmv<VT, MT, int, Epi>, dim3(g), dim3(256), 0, s, op.ell<MT, int>(), x, y, epi, slot);
 }
 
 // Dispatch on the operator's format.  The grid of each path is fixed per

@@ -360,6 +360,8 @@ __global__ void k_trsv_sweep(int n, const int *__restrict__ rp, const int *__res
                              const DT *__restrict__ dinv_row, const VT *__restrict__ x, const VT *__restrict__ yin,
                              VT *__restrict__ yout, int first, const int *done_flag)
 {
+    pdl_trigger();
+    pdl_wait();
     if (done_flag && *done_flag) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         VT acc = UPPER ? (VT)(x[i] * (VT)dinv_row[i]) : x[i];
@@ -447,9 +449,11 @@ __global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, i
                                                                          VT *__restrict__ yout, const int *done_flag)
 {
     constexpr int R = ell_rows_for<FT>();
-    if (done_flag && *done_flag) return;
     __shared__ int s_off[ELL_DIA_MAX];
-    ell_stage_offsets<CT>(doff, w, s_off);
+    ell_stage_offsets<CT>(doff, w, s_off);  // constant data: before the dependency wait
+    pdl_trigger();
+    pdl_wait();
+    if (done_flag && *done_flag) return;
     const long ld = ell_ld(n);
     for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * R; i0 < n; i0 += gridDim.x * blockDim.x * R) {
         VT acc[R];
