@@ -207,7 +207,10 @@ def run_ours(args):
         S = Solver(A, fmt=fmt).ksp_settype("bicgstab").ksp_setoption(1e-10, 3000).pc_settype("ilu0")
         S.pc_set_trsv(trsv)
         if mixed:
-            S.set_precision("fp64", "fp32", "bf16").set_inner(1e-4, 300)
+            # one FP32 BiCGSTAB carried across the refinement steps, the true
+            # residual replaced every two decades (the best interval of those
+            # measured over six right-hand sides)
+            S.set_precision("fp64", "fp32", "bf16").set_inner(1e-2, 300).set_refinement_mode(True)
         return S
 
     # headline: mixed-precision refinement with BF16 ILU(0) factors and the
@@ -318,8 +321,9 @@ def run_ours(args):
         "dtype": "f64 (outer) / f32 (inner) / bf16 (factors)",
         "data": "synthetic (seeded stencil system, inputs larger than L2)",
         "config": {"workload": WORKLOAD, "format": fmt,
-                   "solver": f"mixed-precision refinement: FP64 outer residual/update, inner FP32 BiCGSTAB (rtol 1e-4), "
-                             f"BF16 ILU(0) factors, inner triangular solves by {args.sweeps} Jacobi sweeps",
+                   "solver": f"mixed-precision refinement: FP64 outer residual/update, one FP32 BiCGSTAB carried "
+                             f"across the steps (residual replaced by the FP64 residual every 1e-2 drop), "
+                             f"BF16 ILU(0) factors, triangular solves by {args.sweeps} Jacobi sweeps",
                    "parallelism": f"replicas x{ws}", "l2": "inputs (175 MB matrix) larger than L2; kernels timed "
                                                            "with an L2 flush between repetitions"},
         "fp64_ms": res["fp64_exact"]["ms"], "speedup_vs_fp64": res["fp64_exact"]["ms"] / ms_mix,
