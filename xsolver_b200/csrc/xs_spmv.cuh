@@ -326,6 +326,24 @@ __host__ __device__ constexpr int ell_chunk_for()
 {
     return sizeof(MT) >= 8 ? XS_ELL_CHUNK64 : ELL_CHUNK;
 }
+// resident CTAs per SM the register budget is sized for, by value type:
+// the SpMV keeps 5 for every type; the Jacobi-sweep passes with 2- and
+// 4-byte factor values run fastest at full occupancy (8 CTAs, 32 registers:
+// 46.3 against 49.7 us for the BF16 apply at 128^3), the FP32 SpMV at 5
+// (26.7 against 34.8 us at 8)
+#ifndef XS_SWEEP_MIN_BLOCKS_NARROW
+#define XS_SWEEP_MIN_BLOCKS_NARROW 8
+#endif
+template <typename MT>
+__host__ __device__ constexpr int ell_min_blocks_for()
+{
+    return ELL_MIN_BLOCKS;
+}
+template <typename FT>
+__host__ __device__ constexpr int sweep_min_blocks_for()
+{
+    return sizeof(FT) >= 8 ? ELL_MIN_BLOCKS : XS_SWEEP_MIN_BLOCKS_NARROW;
+}
 
 // R consecutive elements starting at an R-aligned index, one vector load
 // (two for 32 bytes) through the read-only path
@@ -438,7 +456,7 @@ __device__ __forceinline__ void ell_rows(const CT *cp, const MT *vp, int w, long
 }
 
 template <typename VT, typename MT, typename CT, typename Epi>
-__global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_ell_spmv(EllArgs<MT, CT> A, const VT *__restrict__ x,
+__global__ void __launch_bounds__(256, ell_min_blocks_for<MT>()) k_ell_spmv(EllArgs<MT, CT> A, const VT *__restrict__ x,
                                                                    VT *__restrict__ y, Epi epi, RedSlot slot)
 {
     constexpr int KK = Epi::K > 0 ? Epi::K : 1;

@@ -440,7 +440,7 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
 // Launch shape as the ELL SpMV (ELL_ROWS rows per thread, ELL_CHUNK slots
 // per load chunk, warp-uniform chunk lengths).
 template <typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
-__global__ void __launch_bounds__(256, ELL_MIN_BLOCKS) k_trsv_sweep_ell(int n, int w, const CT *__restrict__ eci,
+__global__ void __launch_bounds__(256, sweep_min_blocks_for<FT>()) k_trsv_sweep_ell(int n, int w, const CT *__restrict__ eci,
                                                                          const int *__restrict__ doff,
                                                                          const FT *__restrict__ ev,
                                                                          const DT *__restrict__ dinv,
