@@ -100,6 +100,24 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def profile_traffic(name: str):
+    """DRAM bytes (read + write) summed over the launches of an ncu summary
+    committed under profiles/ (one capture of the kernel's launches on this
+    workload), or None when the summary is absent."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    total = 0.0
+    for line in open(path):
+        for what in ("| DRAM read (", "| DRAM write ("):
+            if line.startswith(what):
+                unit = line[len(what):].split(")")[0]
+                vals = [c.strip() for c in line.split("|")[2:-1]]
+                total += sum(float(v) for v in vals) * scale[unit]
+    return total or None
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -332,7 +350,8 @@ def run_ours(args):
                              f"across the steps (residual replaced by the FP64 residual every 1e-2 drop), "
                              f"BF16 ILU(0) factors, triangular solves by {args.sweeps} Jacobi sweeps",
                    "parallelism": f"replicas x{ws}", "l2": "inputs (175 MB matrix) larger than L2; kernels timed "
-                                                           "with an L2 flush between repetitions"},
+                                                           "with an L2 flush (384 MB written, then 384 MB read) "
+                                                           "between repetitions"},
         "fp64_ms": res["fp64_exact"]["ms"], "speedup_vs_fp64": res["fp64_exact"]["ms"] / ms_mix,
         "variants": res, "levels": {"L": levels[0], "U": levels[1]},
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": A.nnz * 8 + 2 * n * 8,
@@ -345,7 +364,11 @@ def run_ours(args):
         "gpu_launches": int(res["mixed_sweeps"]["launches_per_solve"] * args.steps),
         "roofline": {"bound": "hbm", "kernel": f"ILU(0) apply, BF16 factors, FP32 vectors, {args.sweeps} Jacobi sweeps",
                      "achieved": dom["GBs"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
-                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes": dom["bytes"]},
+                     "peak_kind": peak_kind,
+                     "traffic": profile_traffic("sweep_bf16_diagonal_ell_128cubed.md"),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over the 4 launches of one "
+                                       "apply, profiles/sweep_bf16_diagonal_ell_128cubed.md (writes land in L2)",
+                     "algorithmic_bytes": dom["bytes"]},
         "kernels": kern,
         "clocks": clk,
     }
