@@ -382,8 +382,13 @@ __device__ __forceinline__ void ld_vec(const T *p, T (&o)[R])
 // Row sums accumulate in FP64 for every value type (an FP32 accumulator in
 // the inner solve of the mixed-precision refinement measurably raised its
 // iteration count on the 128^3 benchmark: 183 against 162 inner iterations).
+#ifndef XS_ELL_ACC32
+#define XS_ELL_ACC32 0
+#endif
 template <typename VT, typename MT>
-using EllAcc = double;
+using EllAcc = typename std::conditional<XS_ELL_ACC32 && std::is_same<VT, float>::value &&
+                                             std::is_same<MT, float>::value,
+                                         float, double>::type;
 
 template <int C, int R, typename VT, typename MT, typename CT, typename AT>
 __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld, const VT *__restrict__ x, int r0,
