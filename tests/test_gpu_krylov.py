@@ -195,7 +195,8 @@ def test_nan_rhs_reports_error(cuda):
     assert np.all(np.isfinite(x))
 
 
-def test_missing_diagonal_reports_error(cuda):
+@pytest.mark.parametrize("pc", ["ilu0", "parilut"])
+def test_missing_diagonal_reports_error(cuda, pc):
     from xsolver_b200.api import XsError
 
     A = st.poisson2d_5pt(8)
@@ -204,7 +205,7 @@ def test_missing_diagonal_reports_error(cuda):
     rp = np.zeros(A.n + 1, np.int32)
     np.cumsum(np.bincount(rows[keep], minlength=A.n), out=rp[1:])
     B = st.CSRMatrix(A.n, rp, A.colidx[keep], A.val[keep])
-    S = _solver(B, "bicgstab", "ilu0", 1e-8, 50)
+    S = _solver(B, "bicgstab", pc, 1e-8, 50)
     with pytest.raises(XsError) as e:
         S.solve(np.ones(B.n))
     assert e.value.code == 4

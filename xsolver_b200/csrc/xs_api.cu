@@ -138,20 +138,63 @@ void operator_ensure32(Operator &op, const int *rp0, cudaStream_t s)
 // would hold at most 25% padding; empty otherwise.
 std::vector<int> dia_offsets(int n, const int *rp, const int *ci)
 {
-    std::vector<int> offs;  // kept sorted
-    if (!format_tuning().ell_dia || n <= 0) return offs;
-    long nnz = (long)rp[n] - rp[0];
-    for (int i = 0; i < n; i++)
+    if (!format_tuning().ell_dia || n <= 0) return {};
+    const long nnz = (long)rp[n] - rp[0];
+    // slot count allowed: ELL_DIA_MAX, and slots * n <= nnz + nnz / 4
+    const long cap = std::min<long>(ELL_DIA_MAX, (nnz + nnz / 4) / n);
+    if (cap <= 0) return {};
+    auto add_row = [&](std::vector<int> &offs, long i) {
         for (int q = rp[i]; q < rp[i + 1]; q++) {
-            const int o = ci[q] - i;
+            const int o = ci[q] - (int)i;
             auto it = std::lower_bound(offs.begin(), offs.end(), o);
             if (it == offs.end() || *it != o) {
                 offs.insert(it, o);
-                if ((int)offs.size() > ELL_DIA_MAX) return {};
+                if ((long)offs.size() > cap) return false;
             }
         }
-    if ((long)offs.size() * n > nnz + nnz / 4) return {};
+        return true;
+    };
+    // a sample of rows: its offsets are a subset of all of them, so a sample
+    // over the cap rejects without the full scan
+    {
+        std::vector<int> offs;
+        const long S = std::min(n, 4096);
+        for (long t = 0; t < S; t++)
+            if (!add_row(offs, (long)n * t / S)) return {};
+    }
+    // every row, in ranges over host threads; the union of the range sets
+    std::vector<std::vector<int>> part(16);
+    std::vector<char> ok(16, 1);
+    const int T = host_parallel_rows(n, [&](long lo, long hi, int t) {
+        for (long i = lo; i < hi; i++)
+            if (!add_row(part[t], i)) {
+                ok[t] = 0;
+                return;
+            }
+    });
+    std::vector<int> offs;
+    for (int t = 0; t < T; t++) {
+        if (!ok[t]) return {};
+        for (int o : part[t]) {
+            auto it = std::lower_bound(offs.begin(), offs.end(), o);
+            if (it == offs.end() || *it != o) offs.insert(it, o);
+        }
+        if ((long)offs.size() > cap) return {};
+    }
     return offs;
+}
+
+// largest |c - row| over a CSR pattern (host threads)
+long max_col_offset(int n, const int *rp, const int *ci)
+{
+    std::vector<long> part(16, 0);
+    const int T = host_parallel_rows(n, [&](long lo, long hi, int t) {
+        long m = 0;
+        for (long i = lo; i < hi; i++)
+            for (int q = rp[i]; q < rp[i + 1]; q++) m = std::max(m, std::labs((long)ci[q] - i));
+        part[t] = m;
+    });
+    return *std::max_element(part.begin(), part.begin() + T);
 }
 
 void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const double *v, int, bool want32, cudaStream_t s)
@@ -194,9 +237,7 @@ void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const doub
         op.ev.upload(vv.data(), m, s);
     } else {
         op.ell_w = w;
-        long maxoff = 0;
-        for (int i = 0; i < n; i++)
-            for (int q = rp0[i]; q < rp0[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci0[q] - i));
+        const long maxoff = max_col_offset(n, rp0, ci0);
         op.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
         const size_t m = (size_t)w * ld;
         // padding slots of a row point at the row itself (offset 0) with
@@ -640,9 +681,10 @@ static void build_precond(Handle &h)
         M.have_factors = true;
     } else if (type == PC_PARILUT) {
         Trace tr("setup parilut (total)", h.s);
-        parilut_build(h.s, h.err.p, n, h.A, h.hrp, h.hci, h.parilut_fill, h.parilut_sweeps, h.parilut_droptol, h.ilut);
+        parilut_build(h.s, h.err.p, n, h.A, h.parilut_fill, h.parilut_sweeps, h.parilut_droptol, h.ilut);
         // factors in the seqilu0 layout on their own pattern
         ilut_to_tri(h.s, n, h.ilut, M.L, M.U, need32);
+        pool_trim(h.s);
         M.ensure_buffers64(h.s);
         if (need32) M.ensure_buffers32(h.s);
         if (h.trsv_mode > 0) M.ensure_sweep_buffers(need32);

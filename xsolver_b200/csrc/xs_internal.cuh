@@ -19,8 +19,12 @@
 #include <stdint.h>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <chrono>
+#include <mutex>
+#include <thread>
 #include <utility>
+#include <vector>
 
 #include "../../include/xsolver_c.h"
 
@@ -60,6 +64,25 @@ struct Trace {
     }
     ~Trace() { stop(); }
 };
+
+// Host pattern scans over [0, n) split into contiguous ranges, one per host
+// thread (at most 16, and none for ranges under 64K rows); fn(lo, hi, t)
+// must not throw.  Returns the number of ranges.
+template <typename F>
+inline int host_parallel_rows(long n, F fn)
+{
+    const long hc = std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::max(1L, std::min(std::min(hc, 16L), n / 65536));
+    if (T == 1) {
+        fn(0L, n, 0);
+        return 1;
+    }
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (int t = 0; t < T; t++) th.emplace_back([&, t] { fn(n * t / T, n * (t + 1) / T, t); });
+    for (auto &x : th) x.join();
+    return T;
+}
 
 // ---------------------------------------------------------------- errors
 struct CudaError {
@@ -123,18 +146,94 @@ inline void check_launch()
     }
 }
 
+// ---------------------------------------------------------------- scratch pool
+// A stream-ordered memory pool per device for the temporaries of a factor
+// builder that allocates and frees multi-GB buffers every sweep.  Freed
+// memory stays in the pool (release threshold: never) until pool_trim().
+inline cudaMemPool_t scratch_pool()
+{
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    XS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Status(XS_ERR_CUDA);
+    std::lock_guard<std::mutex> g(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        XS_CUDA(cudaMemPoolCreate(&pools[dev], &props));
+        unsigned long long never = ~0ull;
+        XS_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &never));
+    }
+    return pools[dev];
+}
+
+// While a PoolScope is open on this host thread, DBuf::alloc takes memory
+// from scratch_pool() in the order of the scope's stream and such a buffer is
+// returned with cudaFreeAsync on that stream: every use of it must be on
+// that stream.
+struct PoolScope {
+    static cudaStream_t &stream()
+    {
+        static thread_local cudaStream_t s = nullptr;
+        return s;
+    }
+    static bool &open()
+    {
+        static thread_local bool o = false;
+        return o;
+    }
+    cudaStream_t prev_s;
+    bool prev_o, ended = false;
+    explicit PoolScope(cudaStream_t s) : prev_s(stream()), prev_o(open())
+    {
+        stream() = s;
+        open() = true;
+    }
+    void end()
+    {
+        if (ended) return;
+        stream() = prev_s;
+        open() = prev_o;
+        ended = true;
+    }
+    ~PoolScope() { end(); }
+};
+
+// hand the pool's unused memory back to the device once the frees queued on
+// stream s have run
+inline void pool_trim(cudaStream_t s)
+{
+    XS_CUDA(cudaStreamSynchronize(s));
+    XS_CUDA(cudaMemPoolTrimTo(scratch_pool(), 0));
+}
+
 // ---------------------------------------------------------------- device buffers
 template <typename T>
 struct DBuf {
     T *p = nullptr;
     size_t n = 0;
+    cudaStream_t ps = nullptr;  // pooled buffers: the stream that frees them
+    bool pooled = false;
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
-    DBuf(DBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf(DBuf &&o) noexcept : p(o.p), n(o.n), ps(o.ps), pooled(o.pooled)
+    {
+        o.p = nullptr;
+        o.n = 0;
+        o.pooled = false;
+    }
     DBuf &operator=(DBuf &&o) noexcept
     {
-        if (this != &o) { free(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        if (this != &o) {
+            free();
+            p = o.p; n = o.n; ps = o.ps; pooled = o.pooled;
+            o.p = nullptr; o.n = 0; o.pooled = false;
+        }
         return *this;
     }
     ~DBuf() { free(); }
@@ -144,19 +243,30 @@ struct DBuf {
         free();
         size_t bytes = (count + pad) * sizeof(T);
         if (bytes == 0) bytes = 16;
-        XS_CUDA(cudaMalloc((void **)&p, bytes));
-        // zero and wait: the handle's stream does not synchronise with the
-        // legacy default stream, so an asynchronous memset there could land
-        // after the handle's own first writes to this buffer
-        XS_CUDA(cudaMemsetAsync(p, 0, bytes, 0));
-        XS_CUDA(cudaStreamSynchronize(0));
+        if (PoolScope::open()) {
+            ps = PoolScope::stream();
+            XS_CUDA(cudaMallocFromPoolAsync((void **)&p, bytes, scratch_pool(), ps));
+            pooled = true;
+            XS_CUDA(cudaMemsetAsync(p, 0, bytes, ps));
+        } else {
+            XS_CUDA(cudaMalloc((void **)&p, bytes));
+            // zero and wait: the handle's stream does not synchronise with the
+            // legacy default stream, so an asynchronous memset there could land
+            // after the handle's own first writes to this buffer
+            XS_CUDA(cudaMemsetAsync(p, 0, bytes, 0));
+            XS_CUDA(cudaStreamSynchronize(0));
+        }
         n = count;
     }
     void free()
     {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled) cudaFreeAsync(p, ps);
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
+        pooled = false;
     }
     void upload(const T *h, size_t count, cudaStream_t s)
     {
@@ -179,13 +289,15 @@ enum DevErr : int {
     DEV_NAN = 4,
     DEV_TMA_TIMEOUT = 8,
     DEV_CAPACITY = 16,
-    DEV_FACTOR_TIMEOUT = 32
+    DEV_FACTOR_TIMEOUT = 32,
+    DEV_NO_DIAG = 64
 };
 
 inline int dev_err_to_status(int e)
 {
     if (e & (DEV_TRSV_TIMEOUT | DEV_FACTOR_TIMEOUT | DEV_TMA_TIMEOUT)) return XS_ERR_TRSV_TIMEOUT;
     if (e & DEV_CAPACITY) return XS_ERR_CAPACITY;
+    if (e & DEV_NO_DIAG) return XS_ERR_NO_DIAG;
     if (e & DEV_NAN) return XS_ERR_NAN;
     if (e & DEV_BREAKDOWN) return XS_ERR_BREAKDOWN;
     return XS_OK;

@@ -4,13 +4,16 @@
 // removal :283-380 and bucket k-th select par_ilut_hip/select_kth.h:501).
 //
 // Per sweep s (rate = (fill-1)/sweeps*(s+1)+1, :692):
-//   1. candidates = pattern(A) u pattern(L*U): one warp per row gathers A's
-//      row and the U rows selected by L's row into shared memory, bitonic-sorts
-//      and de-duplicates them (symbolic pass counts, second pass writes).
+//   1. candidates = pattern(A) u pattern(L*U): one warp per row marks A's
+//      row and the U rows selected by L's row in a shared-memory bitmap over
+//      the row's column window and reads the set bits back in order (rows
+//      whose window exceeds the bitmap gather, bitonic-sort and de-duplicate
+//      instead); a symbolic pass counts, a second pass writes.
 //   2. values: entries already in L/U keep their value; a new entry gets
 //      r_ij/u_jj (lower) or r_ij (upper), r = A - L*U accumulated as
 //      c = -a_ij; c += l_ik u_kj (k ascending); r = -c.
-//   3. split into L (unit diagonal last) and U, U also by columns (CSC).
+//   3. split into L (CSR, unit diagonal last) and U (CSR, diagonal first);
+//      both factors stay row-major throughout, so no transposes are formed.
 //   4. one synchronous sweep over every L and U entry (fixed point of the
 //      ILU equations on the current pattern), row-wise: a warp per row
 //      subtracts l_ik * u_kj walking the U rows k of its L row.
@@ -53,42 +56,6 @@ constexpr int PLT_CAP = 2048;  // candidate columns gathered per row (with dupli
 constexpr int PLT_WARPS = 4;
 
 // ---------------------------------------------------------------- helpers
-__global__ void k_count_cols(int n, const int *__restrict__ rp, const int *__restrict__ ci, int *cnt)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        for (int k = rp[i]; k < rp[i + 1]; k++) atomicAdd(cnt + ci[k], 1);
-}
-__global__ void k_scatter_t(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ v,
-                            const int *__restrict__ trp, int *fillc, int *tci, double *tv)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        for (int k = rp[i]; k < rp[i + 1]; k++) {
-            const int c = ci[k];
-            const int p = trp[c] + atomicAdd(fillc + c, 1);
-            tci[p] = i;
-            tv[p] = v[k];
-        }
-}
-// sort every segment by index (insertion sort, segments are short)
-__global__ void k_sort_segments(int n, const int *__restrict__ rp, int *ci, double *v)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int a = rp[i], b = rp[i + 1];
-        for (int k = a + 1; k < b; k++) {
-            const int key = ci[k];
-            const double val = v[k];
-            int q = k - 1;
-            while (q >= a && ci[q] > key) {
-                ci[q + 1] = ci[q];
-                v[q + 1] = v[q];
-                q--;
-            }
-            ci[q + 1] = key;
-            v[q + 1] = val;
-        }
-    }
-}
-
 // device binary search: position of column j in row [a, b) of ci, or -1
 __device__ __forceinline__ int find_pos(const int *ci, int a, int b, int j)
 {
@@ -104,6 +71,14 @@ __device__ __forceinline__ int find_pos(const int *ci, int a, int b, int j)
 // ---------------------------------------------------------------- candidates
 // mode 0: count unique candidate columns per row into cnt[i]
 // mode 1: write them (sorted) into dci[drp[i] ...]
+// Row i's candidates lie in [lo, hi]: the smallest/largest column of A's row
+// and the first/last column of the U rows k of L row i (U rows are sorted).  When the window fits PLT_BM_WORDS*32 columns the
+// warp marks a bitmap with shared atomics and reads the set bits back word by
+// word (ascending, a warp prefix sum gives each word's output offset); wider
+// windows gather every column (duplicates included, at most PLT_CAP) and
+// bitonic-sort them.
+constexpr int PLT_BM_WORDS = PLT_CAP;  // bitmap words per warp (same buffer)
+
 __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int *__restrict__ arp,
                                                                const int *__restrict__ aci, const int *__restrict__ lrp,
                                                                const int *__restrict__ lci, const int *__restrict__ urp,
@@ -114,10 +89,71 @@ __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int 
     __shared__ int scount[PLT_WARPS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int *buf = sbuf[w];
+    unsigned *bm = reinterpret_cast<unsigned *>(buf);
     for (int i = blockIdx.x * PLT_WARPS + w; i < n; i += gridDim.x * PLT_WARPS) {
+        const int a0 = arp[i], a1 = arp[i + 1], l0 = lrp[i], l1 = lrp[i + 1];
+        int lo = INT_MAX, hi = INT_MIN;
+        for (int q = a0 + lane; q < a1; q += 32) {
+            lo = min(lo, aci[q]);
+            hi = max(hi, aci[q]);
+        }
+        for (int q = l0 + lane; q < l1; q += 32) {
+            const int k = lci[q];
+            const int e0 = urp[k], e1 = urp[k + 1];
+            if (e1 > e0) {
+                lo = min(lo, uci[e0]);
+                hi = max(hi, uci[e1 - 1]);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        const long words = hi >= lo ? (((long)hi - lo) >> 5) + 1 : 0;
+        if (words <= PLT_BM_WORDS) {
+            const int nw = (int)words;
+            for (int q = lane; q < nw; q += 32) bm[q] = 0u;
+            __syncwarp();
+            const unsigned span = (unsigned)nw << 5;  // every column lies in [lo, hi]; the test only bounds the store
+            for (int q = a0 + lane; q < a1; q += 32) {
+                const unsigned d = (unsigned)(aci[q] - lo);
+                if (d < span) atomicOr(bm + (d >> 5), 1u << (d & 31));
+            }
+            for (int q = l0; q < l1; q++) {
+                const int k = lci[q];
+                for (int t = urp[k] + lane; t < urp[k + 1]; t += 32) {
+                    const unsigned d = (unsigned)(uci[t] - lo);
+                    if (d < span) atomicOr(bm + (d >> 5), 1u << (d & 31));
+                }
+            }
+            __syncwarp();
+            int run = 0;
+            for (int base = 0; base < nw; base += 32) {
+                const int q = base + lane;
+                unsigned wv = q < nw ? bm[q] : 0u;
+                const int c = __popc(wv);
+                int incl = c;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                if (mode == 1 && wv) {
+                    int p = drp[i] + run + incl - c;
+                    const int colbase = lo + (q << 5);
+                    while (wv) {
+                        dci[p++] = colbase + __ffs(wv) - 1;
+                        wv &= wv - 1;
+                    }
+                }
+                run += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (mode == 0 && lane == 0) cnt[i] = run;
+            __syncwarp();
+            continue;
+        }
         // total with duplicates (A's row counted once, by lane 0)
-        int tot = lane == 0 ? arp[i + 1] - arp[i] : 0;
-        for (int q = lrp[i] + lane; q < lrp[i + 1]; q += 32) {
+        int tot = lane == 0 ? a1 - a0 : 0;
+        for (int q = l0 + lane; q < l1; q += 32) {
             const int k = lci[q];
             tot += urp[k + 1] - urp[k];
         }
@@ -131,8 +167,8 @@ __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int 
         }
         if (lane == 0) scount[w] = 0;
         __syncwarp();
-        for (int q = arp[i] + lane; q < arp[i + 1]; q += 32) buf[atomicAdd(&scount[w], 1)] = aci[q];
-        for (int q = lrp[i]; q < lrp[i + 1]; q++) {
+        for (int q = a0 + lane; q < a1; q += 32) buf[atomicAdd(&scount[w], 1)] = aci[q];
+        for (int q = l0; q < l1; q++) {
             const int k = lci[q];
             for (int t = urp[k] + lane; t < urp[k + 1]; t += 32) buf[atomicAdd(&scount[w], 1)] = uci[t];
         }
@@ -180,11 +216,11 @@ __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int 
 // candidate values (warp per row, lanes over the row's entries)
 // value of candidate (i, j): an entry already in L or U keeps its value, a
 // new one gets r_ij (/u_jj below the diagonal), r = A - L*U accumulated as
-// c = -a_ij; c += l_ik u_kj over the merge of L row i and U column j
+// c = -a_ij; c += l_ik u_kj for k of L row i (increasing) with (k, j) in U
+// (the products of the merge of L row i with U column j, in its order)
 __device__ __forceinline__ double cand_value(int i, int j, const int *arp, const int *aci, const double *av,
                                             const int *lrp, const int *lci, const double *lv, const int *urp,
-                                            const int *uci, const double *uv, const int *ucp, const int *ucr,
-                                            const double *ucv, const double *udiag)
+                                            const int *uci, const double *uv, const double *udiag)
 {
     int pos = -1;
     if (j < i) pos = find_pos(lci, lrp[i], lrp[i + 1], j);
@@ -193,18 +229,10 @@ __device__ __forceinline__ double cand_value(int i, int j, const int *arp, const
     if (pu >= 0) return uv[pu];
     const int pa = find_pos(aci, arp[i], arp[i + 1], j);
     double c = -(pa >= 0 ? av[pa] : 0.0);
-    int il = lrp[i], iu = ucp[j];
-    const int ile = lrp[i + 1], iue = ucp[j + 1];
-    while (il < ile && iu < iue) {
-        const int lj = lci[il], ui = ucr[iu];
-        if (lj == ui) {
-            c += lv[il] * ucv[iu];
-            il++;
-            iu++;
-        } else if (lj < ui)
-            il++;
-        else
-            iu++;
+    for (int q = lrp[i]; q < lrp[i + 1]; q++) {
+        const int k = lci[q];
+        const int pk = find_pos(uci, urp[k], urp[k + 1], j);
+        if (pk >= 0) c += lv[q] * uv[pk];
     }
     const double r = -c;
     return (j < i) ? r / udiag[j] : r;
@@ -224,7 +252,6 @@ __global__ void __launch_bounds__(32 * PLT_CV_WARPS) k_candidate_values(
     int n, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
     const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv,
     const int *__restrict__ urp, const int *__restrict__ uci, const double *__restrict__ uv,
-    const int *__restrict__ ucp, const int *__restrict__ ucr, const double *__restrict__ ucv,
     const double *__restrict__ udiag, const int *__restrict__ drp, const int *__restrict__ dci,
     double *__restrict__ dv)
 {
@@ -239,7 +266,7 @@ __global__ void __launch_bounds__(32 * PLT_CV_WARPS) k_candidate_values(
         const int d0 = drp[i], m = drp[i + 1] - d0;
         if (m > PLT_CAND_CAP) {
             for (int q = lane; q < m; q += 32)
-                dv[d0 + q] = cand_value(i, dci[d0 + q], arp, aci, av, lrp, lci, lv, urp, uci, uv, ucp, ucr, ucv, udiag);
+                dv[d0 + q] = cand_value(i, dci[d0 + q], arp, aci, av, lrp, lci, lv, urp, uci, uv, udiag);
             continue;
         }
         bool any_new = false;
@@ -298,48 +325,62 @@ __global__ void k_udiag(int n, const int *__restrict__ urp, const double *__rest
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) d[j] = uv[urp[j]];
 }
 
-// split counts: lower entries + 1 (unit diagonal), upper entries
+// split counts: lower entries + 1 (unit diagonal), upper entries (warp per row)
 __global__ void k_split_count(int n, const int *__restrict__ drp, const int *__restrict__ dci, int *lc, int *uc)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
+        const int a = drp[i], b = drp[i + 1];
         int l = 0;
-        for (int k = drp[i]; k < drp[i + 1]; k++) l += dci[k] < i;
-        lc[i] = l + 1;
-        uc[i] = (drp[i + 1] - drp[i]) - l;
+        for (int k = a + lane; k < b; k += 32) l += dci[k] < i;
+        for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+        if (lane == 0) {
+            lc[i] = l + 1;
+            uc[i] = (b - a) - l;
+        }
     }
 }
+// rows are sorted, so the lower part is the prefix [a, a + nl) and the upper
+// part the rest; L gets its unit diagonal last
 __global__ void k_split_fill(int n, const int *__restrict__ drp, const int *__restrict__ dci, const double *__restrict__ dv,
                              const int *__restrict__ lrp, int *lci, double *lv, const int *__restrict__ urp, int *uci,
                              double *uv)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int pl = lrp[i], pu = urp[i];
-        for (int k = drp[i]; k < drp[i + 1]; k++) {
-            if (dci[k] < i) { lci[pl] = dci[k]; lv[pl] = dv[k]; pl++; }
-            else { uci[pu] = dci[k]; uv[pu] = dv[k]; pu++; }
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
+        const int a = drp[i], b = drp[i + 1];
+        const int pl = lrp[i], nl = lrp[i + 1] - pl - 1, pu = urp[i];
+        for (int k = a + lane; k < b; k += 32) {
+            const int q = k - a;
+            if (q < nl) { lci[pl + q] = dci[k]; lv[pl + q] = dv[k]; }
+            else { uci[pu + q - nl] = dci[k]; uv[pu + q - nl] = dv[k]; }
         }
-        lci[pl] = i;
-        lv[pl] = 1.0;
+        if (lane == 0) {
+            lci[pl + nl] = i;
+            lv[pl + nl] = 1.0;
+        }
     }
 }
 
-// ParILUT sweep value: a_ij - sum_{k<min(i,j)} l_ik u_kj (L row i CSR with the
-// unit diagonal last, U column j CSC with the diagonal last)
+// ParILUT sweep value of entry (i, j) by a walk of L row i: a_ij minus
+// l_ik * u_kj for every k of L row i (increasing) with k < min(i, j) and
+// (k, j) in U, u_kj found by binary search in U row k (CSR, diagonal first).
+// The same products in the same order as the merge of L row i with U column
+// j in the reference's sweep (hip/Precond/parilut.cpp:392-441).
 __device__ __forceinline__ double plt_sweep_value(const int *arp, const int *aci, const double *av, const int *lrp,
-                                                  const int *lci, const double *lv, const int *ucp, const int *ucr,
-                                                  const double *ucv, int i, int j)
+                                                  const int *lci, const double *lv, const int *urp, const int *uci,
+                                                  const double *uv, int i, int j)
 {
     const int pa = find_pos(aci, arp[i], arp[i + 1], j);
     double t = pa >= 0 ? av[pa] : 0.0;
-    int il = lrp[i], iu = ucp[j];
     const int last = (i <= j) ? i : j;
-    while (true) {
-        const int lj = lci[il], ui = ucr[iu];
-        const int check = (i <= j) ? ui : lj;
-        if (check >= last) break;
-        if (lj == ui) t = t - lv[il] * ucv[iu];
-        il += (lj <= ui);
-        iu += (ui <= lj);
+    for (int q = lrp[i]; q < lrp[i + 1]; q++) {
+        const int k = lci[q];
+        if (k >= last) break;
+        const int pu = find_pos(uci, urp[k], urp[k + 1], j);
+        if (pu >= 0) t = t - lv[q] * uv[pu];
     }
     return t;
 }
@@ -350,11 +391,11 @@ __device__ __forceinline__ double plt_sweep_value(const int *arp, const int *aci
 // increasing order the lanes walk U row k (CSR) and, for each column j != k
 // found in row i's pattern, subtract l_ik * u_kj.  That is the same set of
 // products, subtracted in the same (increasing k) order, as the per-entry
-// merge of plt_sweep_value, so the values are identical; but U rows are read
+// walk of plt_sweep_value, so the values are identical; but U rows are read
 // contiguously and no lane walks a dependent index chain.  Results: L part
-// t / u_jj into lnew (CSR position), U part t into unew at row i's position
-// in U's column j (CSC).  parts: 1 L only, 2 U only, 3 both.  Rows whose
-// pattern exceeds PLT_ROW_CAP fall back to the per-entry merge.
+// t / u_jj into lnew, U part t into unew, both at the entry's CSR position.
+// parts: 1 L only, 2 U only, 3 both.  Rows whose pattern exceeds
+// PLT_ROW_CAP fall back to the per-entry walk.
 constexpr int PLT_ROW_CAP = 256;
 constexpr int PLT_SW_WARPS = 4;
 
@@ -362,8 +403,7 @@ __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
     int n, int parts, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
     const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv_k,
     const double *__restrict__ lv_old, const int *__restrict__ urp, const int *__restrict__ uci,
-    const double *__restrict__ uv, const int *__restrict__ ucp, const int *__restrict__ ucr,
-    const double *__restrict__ ucv, double *__restrict__ lnew, double *__restrict__ unew)
+    const double *__restrict__ uv, double *__restrict__ lnew, double *__restrict__ unew)
 {
     __shared__ int s_col[PLT_SW_WARPS][PLT_ROW_CAP];
     __shared__ double s_t[PLT_SW_WARPS][PLT_ROW_CAP];
@@ -377,20 +417,18 @@ __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
         const int u0 = urp[i], nu = urp[i + 1] - u0;
         const int m = nl + nu;
         if (m > PLT_ROW_CAP) {
-            // per-entry merge for an unusually long row
-            for (int q = lane; q < l1 - l0; q += 32) {
-                const int k = l0 + q, j = lci[k];
-                if (!(parts & 1)) continue;
-                if (j >= i) { lnew[k] = lv_old[k]; continue; }
-                const double tv = plt_sweep_value(arp, aci, av, lrp, lci, lv_k, ucp, ucr, ucv, i, j);
-                lnew[k] = tv / ucv[ucp[j + 1] - 1];
+            // per-entry walk for an unusually long row
+            if (parts & 1) {
+                for (int q = lane; q < l1 - l0; q += 32) {
+                    const int k = l0 + q, j = lci[k];
+                    if (j >= i) { lnew[k] = lv_old[k]; continue; }
+                    const double tv = plt_sweep_value(arp, aci, av, lrp, lci, lv_k, urp, uci, uv, i, j);
+                    lnew[k] = tv / uv[urp[j]];
+                }
             }
             if (parts & 2) {
-                for (int q = lane; q < nu; q += 32) {
-                    const int j = uci[u0 + q];
-                    const int pc = find_pos(ucr, ucp[j], ucp[j + 1], i);
-                    unew[pc] = plt_sweep_value(arp, aci, av, lrp, lci, lv_k, ucp, ucr, ucv, i, j);
-                }
+                for (int q = lane; q < nu; q += 32)
+                    unew[u0 + q] = plt_sweep_value(arp, aci, av, lrp, lci, lv_k, urp, uci, uv, i, uci[u0 + q]);
             }
             continue;
         }
@@ -428,8 +466,7 @@ __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
             if (q < nl) {
                 if (parts & 1) lnew[l0 + q] = t[q] / uv[urp[j]];  // u_jj: first entry of U row j
             } else if (parts & 2) {
-                const int pc = find_pos(ucr, ucp[j], ucp[j + 1], i);
-                unew[pc] = t[q];
+                unew[u0 + q - nl] = t[q];
             }
         }
         if ((parts & 1) && nl < l1 - l0 && lane == 0) lnew[l1 - 1] = lv_old[l1 - 1];  // unit diagonal unchanged
@@ -455,39 +492,54 @@ __global__ void k_radix_hist(long m, const double *__restrict__ v, unsigned long
         if (sh[q]) atomicAdd(hist + q, (unsigned long long)sh[q]);
 }
 
-// keep flags -> counts per segment; diag = last entry of each segment
-__global__ void k_keep_count(int n, const int *__restrict__ rp, const double *__restrict__ v, double thr, double droptol,
-                             int upper, int *cnt)
+// Threshold keep rule, one row of L (upper = 0: unit diagonal last, drop
+// |l_ij| < droptol) or of U (upper = 1: diagonal first, drop |u_ij| <
+// droptol*|u_jj|, u_jj the first entry of U row j); diagonals are kept.
+__device__ __forceinline__ bool plt_keep(int k, int a, int b, int upper, const int *rp, const int *ci, const double *v,
+                                         double thr, double droptol)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (k == (upper ? a : b - 1)) return true;
+    const double x = fabs(v[k]);
+    if (x < thr) return false;
+    if (droptol > 0) {
+        const double lim = upper ? droptol * fabs(v[rp[ci[k]]]) : droptol;
+        if (x < lim) return false;
+    }
+    return true;
+}
+// keep counts per row (warp per row)
+__global__ void k_keep_count(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                             const double *__restrict__ v, double thr, double droptol, int upper, int *cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
         const int a = rp[i], b = rp[i + 1];
-        const double dj = b > a ? fabs(v[b - 1]) : 0.0;
         int c = 0;
-        for (int k = a; k < b; k++) {
-            const double x = fabs(v[k]);
-            const bool keep = (k == b - 1) ||
-                              (x >= thr && !(droptol > 0 && x < (upper ? droptol * dj : droptol)));
-            c += keep;
-        }
-        cnt[i] = c;
+        for (int k = a + lane; k < b; k += 32) c += plt_keep(k, a, b, upper, rp, ci, v, thr, droptol);
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) cnt[i] = c;
     }
 }
+// kept entries in order (warp per row, ballot compaction)
 __global__ void k_keep_fill(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ v,
                             double thr, double droptol, int upper, const int *__restrict__ nrp, int *nci, double *nv)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
         const int a = rp[i], b = rp[i + 1];
-        const double dj = b > a ? fabs(v[b - 1]) : 0.0;
         int p = nrp[i];
-        for (int k = a; k < b; k++) {
-            const double x = fabs(v[k]);
-            const bool keep = (k == b - 1) ||
-                              (x >= thr && !(droptol > 0 && x < (upper ? droptol * dj : droptol)));
+        for (int base = a; base < b; base += 32) {
+            const int k = base + lane;
+            const bool keep = k < b && plt_keep(k, a, b, upper, rp, ci, v, thr, droptol);
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
             if (keep) {
-                nci[p] = ci[k];
-                nv[p] = v[k];
-                p++;
+                const int q = p + __popc(m & ((1u << lane) - 1));
+                nci[q] = ci[k];
+                nv[q] = v[k];
             }
+            p += __popc(m);
         }
     }
 }
@@ -520,6 +572,17 @@ __global__ void k_plt_final_fill(int n, const int *__restrict__ lrp, const int *
     }
 }
 
+// position of each row's diagonal entry (binary search of the sorted row);
+// a row without one sets DEV_NO_DIAG
+__global__ void k_plt_diag_pos(int n, const int *__restrict__ arp, const int *__restrict__ aci, int *uptr, int *err)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int p = find_pos(aci, arp[i], arp[i + 1], i);
+        uptr[i] = p;
+        if (p < 0) atomicOr(err, DEV_NO_DIAG);
+    }
+}
+
 // initial factors: L = strict lower(A)/a_jj + unit diag (last), U = upper(A)
 __global__ void k_plt_init_count(int n, const int *__restrict__ arp, const int *__restrict__ aci, int *lc, int *uc)
 {
@@ -547,48 +610,122 @@ __global__ void k_plt_init_fill(int n, const int *__restrict__ arp, const int *_
 }
 
 // ---------------------------------------------------------------- host driver
+// Exclusive scan of the per-row counts into a row pointer, on the device:
+// tile sums (SCAN_TILE counts per block), one block scans the tile sums,
+// then every tile rescans its counts from its offset.  Totals are formed in
+// 64 bits; a row pointer that would pass INT_MAX - 64 sets DEV_CAPACITY.
+constexpr int SCAN_THREADS = 1024, SCAN_IPT = 8, SCAN_TILE = SCAN_THREADS * SCAN_IPT;
+
+__device__ __forceinline__ long block_excl_scan(long v, long *sw, long &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    long incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) sw[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        long x = lane < nw ? sw[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < nw) sw[lane] = x;  // inclusive warp totals
+    }
+    __syncthreads();
+    total = sw[nw - 1];
+    const long r = (w > 0 ? sw[w - 1] : 0) + incl - v;
+    __syncthreads();  // sw is reused by the next call
+    return r;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_sums(int n, const int *__restrict__ cnt, long *bsum)
+{
+    __shared__ long sw[32];
+    const long base = (long)blockIdx.x * SCAN_TILE;
+    long v = 0;
+    for (int q = threadIdx.x; q < SCAN_TILE; q += SCAN_THREADS)
+        if (base + q < n) v += cnt[base + q];
+    long total;
+    block_excl_scan(v, sw, total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// one block: exclusive scan of nb tile sums in place, grand total into bsum[nb]
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_offsets(int nb, long *bsum)
+{
+    __shared__ long sw[32];
+    long carry = 0;
+    for (int base = 0; base < nb; base += SCAN_THREADS) {
+        const int q = base + threadIdx.x;
+        const long v = q < nb ? bsum[q] : 0;
+        long total;
+        const long e = block_excl_scan(v, sw, total);
+        if (q < nb) bsum[q] = carry + e;
+        carry += total;
+    }
+    if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_write(int n, const int *__restrict__ cnt,
+                                                                  const long *__restrict__ boff, int *rp, int *err)
+{
+    __shared__ long sw[32];
+    const long base = (long)blockIdx.x * SCAN_TILE + (long)threadIdx.x * SCAN_IPT;
+    int c[SCAN_IPT];
+    long v = 0;
+#pragma unroll
+    for (int u = 0; u < SCAN_IPT; u++) {
+        c[u] = base + u < n ? cnt[base + u] : 0;
+        v += c[u];
+    }
+    long total;
+    long acc = boff[blockIdx.x] + block_excl_scan(v, sw, total);
+    bool over = false;
+#pragma unroll
+    for (int u = 0; u < SCAN_IPT; u++) {
+        if (base + u < n) {
+            over |= acc > 0x7fffffffL - 64;
+            rp[base + u] = (int)acc;
+        }
+        acc += c[u];
+    }
+    if (base < n && base + SCAN_IPT >= n) {  // the thread holding the last row writes rp[n]
+        over |= acc > 0x7fffffffL - 64;
+        rp[n] = (int)acc;
+    }
+    if (over) atomicOr(err, DEV_CAPACITY);
+}
+
 struct PltCtx {
     cudaStream_t s;
     int *err;
     int n;
+    DBuf<long> bsum;
     int grid() const { return geom().sms * 8; }
 };
 
-// counts (device, n) -> rowptr (device, n+1) via a host scan; returns nnz
+// counts (device, n) -> rowptr (device, n+1) on the device; returns nnz
 inline long scan_counts(PltCtx &c, const DBuf<int> &cnt, DBuf<int> &rp)
 {
-    std::vector<int> h(c.n);
-    cnt.download(h.data(), c.n, c.s);
-    XS_CUDA(cudaStreamSynchronize(c.s));
-    std::vector<int> r(c.n + 1);
-    long acc = 0;
-    r[0] = 0;
-    for (int i = 0; i < c.n; i++) {
-        acc += h[i];
-        if (acc > 0x7fffffffL - 64) throw Status(XS_ERR_CAPACITY);
-        r[i + 1] = (int)acc;
-    }
-    if (rp.n != (size_t)c.n + 1) rp.alloc(c.n + 1);
-    rp.upload(r.data(), c.n + 1, c.s);
-    return acc;
-}
-
-// transpose with rows sorted within each column
-inline void plt_transpose(PltCtx &c, const DCsr &a, DCsr &t)
-{
     const int n = c.n;
-    DBuf<int> cnt;
-    cnt.alloc(n);
-    k_count_cols<<<c.grid(), 256, 0, c.s>>>(n, a.rp, a.ci, cnt);
+    const int nb = std::max(1, (n + SCAN_TILE - 1) / SCAN_TILE);
+    if (c.bsum.n < (size_t)nb + 1) c.bsum.alloc(nb + 1);
+    if (rp.n != (size_t)n + 1) rp.alloc(n + 1);
+    k_scan_tile_sums<<<nb, SCAN_THREADS, 0, c.s>>>(n, cnt, c.bsum);
+    k_scan_tile_offsets<<<1, SCAN_THREADS, 0, c.s>>>(nb, c.bsum);
+    k_scan_tile_write<<<nb, SCAN_THREADS, 0, c.s>>>(n, cnt, c.bsum, rp, c.err);
     check_launch();
-    t.n = n;
-    t.nnz = scan_counts(c, cnt, t.rp);
-    XS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * n, c.s));
-    t.ci.alloc(std::max<long>(t.nnz, 1));
-    t.v.alloc(std::max<long>(t.nnz, 1));
-    k_scatter_t<<<c.grid(), 256, 0, c.s>>>(n, a.rp, a.ci, a.v, t.rp, cnt, t.ci, t.v);
-    k_sort_segments<<<c.grid(), 256, 0, c.s>>>(n, t.rp, t.ci, t.v);
-    check_launch();
+    long total = 0;
+    int e = 0;
+    XS_CUDA(cudaMemcpyAsync(&total, c.bsum.p + nb, sizeof(long), cudaMemcpyDeviceToHost, c.s));
+    XS_CUDA(cudaMemcpyAsync(&e, c.err, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    XS_CUDA(cudaStreamSynchronize(c.s));
+    if (e) throw Status(dev_err_to_status(e));
+    if (total > 0x7fffffffL - 64) throw Status(XS_ERR_CAPACITY);
+    return total;
 }
 
 // k-th smallest |v| (1-based) by radix select over the IEEE bit patterns
@@ -618,23 +755,28 @@ inline double plt_kth_abs(PltCtx &c, const DBuf<double> &v, long m, long k)
     return out;
 }
 
-inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, const std::vector<int> &hrp,
-                          const std::vector<int> &hci, double fill, int sweeps, double droptol, ParilutResult &R)
+inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, double fill, int sweeps, double droptol,
+                          ParilutResult &R)
 {
     Trace tr_all("parilut_build", s);
-    PltCtx c{s, err, n};
+    // every temporary of the sweeps comes from the stream-ordered pool
+    PoolScope pool(s);
+    Trace tr_init("  initial factors", s);
+    PltCtx c{s, err, n, {}};
     const int G = c.grid();
     const long nnzA = A.nnz;
-    // diagonal positions (host)
-    std::vector<int> uptr(n, -1);
-    for (int i = 0; i < n; i++)
-        for (int k = hrp[i]; k < hrp[i + 1]; k++)
-            if (hci[k] == i) uptr[i] = k;
-    for (int i = 0; i < n; i++)
-        if (uptr[i] < 0) throw Status(XS_ERR_NO_DIAG);
+    XS_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    // diagonal positions (rows are sorted)
     DBuf<int> d_uptr;
     d_uptr.alloc(n);
-    d_uptr.upload(uptr.data(), n, s);
+    k_plt_diag_pos<<<G, 256, 0, s>>>(n, A.rp, A.ci, d_uptr, err);
+    check_launch();
+    {
+        int e = 0;
+        XS_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        XS_CUDA(cudaStreamSynchronize(s));
+        if (e) throw Status(dev_err_to_status(e));
+    }
     // initial factors
     DCsr L, U;
     DBuf<int> lc, uc;
@@ -654,11 +796,10 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
     udiag.alloc(n);
     DBuf<int> cnt;
     cnt.alloc(n);
+    tr_init.stop();
     for (int sw = 0; sw < sweeps; sw++) {
         Trace tr_sw("parilut sweep", s);
         const double rate = (fill - 1) / sweeps * (sw + 1) + 1;
-        DCsr Uc;
-        plt_transpose(c, U, Uc);
         k_udiag<<<G, 256, 0, s>>>(n, U.rp, U.v, udiag);
         check_launch();
         // candidates
@@ -672,9 +813,12 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
         D.ci.alloc(std::max<long>(D.nnz, 1));
         D.v.alloc(std::max<long>(D.nnz, 1));
         k_candidates<<<cg, 32 * PLT_WARPS, 0, s>>>(n, A.rp, A.ci, L.rp, L.ci, U.rp, U.ci, 1, nullptr, D.rp, D.ci, err);
+        check_launch();
+        tr_cand.stop();
+        Trace tr_val("  candidate values", s);
         k_candidate_values<<<std::max(1, std::min((n + PLT_CV_WARPS - 1) / PLT_CV_WARPS, geom().sms * 16)),
-                             32 * PLT_CV_WARPS, 0, s>>>(n, A.rp, A.ci, A.v, L.rp, L.ci, L.v, U.rp, U.ci, U.v, Uc.rp,
-                                                        Uc.ci, Uc.v, udiag, D.rp, D.ci, D.v);
+                             32 * PLT_CV_WARPS, 0, s>>>(n, A.rp, A.ci, A.v, L.rp, L.ci, L.v, U.rp, U.ci, U.v, udiag,
+                                                        D.rp, D.ci, D.v);
         check_launch();
         {
             int e = 0;
@@ -682,8 +826,8 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
             XS_CUDA(cudaStreamSynchronize(s));
             if (e) throw Status(dev_err_to_status(e));
         }
-        tr_cand.stop();
-        Trace tr_rest("  split/sweeps/threshold", s);
+        tr_val.stop();
+        Trace tr_split("  split", s);
         // split
         DCsr L2, U2;
         L2.n = U2.n = n;
@@ -697,72 +841,73 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
         check_launch();
         const long nnzD = D.nnz;
         D = DCsr();
-        DCsr U2c;
-        plt_transpose(c, U2, U2c);
+        tr_split.stop();
+        Trace tr_s1("  LU sweep", s);
         // LU sweep (synchronous): both parts from the old values
         const int rg = std::max(1, std::min((n + PLT_SW_WARPS - 1) / PLT_SW_WARPS, geom().sms * 16));
         {
             DBuf<double> lnew, unew;
             lnew.alloc(L2.nnz);
-            unew.alloc(std::max<long>(U2c.nnz, 1));
+            unew.alloc(std::max<long>(U2.nnz, 1));
             k_plt_sweep_rows<<<rg, 32 * PLT_SW_WARPS, 0, s>>>(n, 3, A.rp, A.ci, A.v, L2.rp, L2.ci, L2.v, L2.v, U2.rp,
-                                                               U2.ci, U2.v, U2c.rp, U2c.ci, U2c.v, lnew, unew);
+                                                               U2.ci, U2.v, lnew, unew);
             check_launch();
             L2.v = std::move(lnew);
-            U2c.v = std::move(unew);
+            U2.v = std::move(unew);
         }
-        U2 = DCsr();
+        tr_s1.stop();
+        Trace tr_th("  threshold", s);
         // threshold removal
         const long keep_nnz = std::lround(rate * (double)nnzA);
         const long remove_nnz = nnzD - keep_nnz;
-        DCsr L3, U3c;
+        DCsr L3, U3;
         if (remove_nnz > 0 || droptol > 0) {
             double lthr = 0.0, uthr = 0.0;
             if (remove_nnz > 0) {
                 const long lkeep = (long)(rate * l0nnz);
                 const long lremove = std::max(L2.nnz - lkeep, 0L);
                 const long ukeep = (long)(rate * u0nnz);
-                const long uremove = std::max(U2c.nnz - ukeep, 0L);
+                const long uremove = std::max(U2.nnz - ukeep, 0L);
                 lthr = plt_kth_abs(c, L2.v, L2.nnz, lremove);
-                uthr = plt_kth_abs(c, U2c.v, U2c.nnz, uremove);
+                uthr = plt_kth_abs(c, U2.v, U2.nnz, uremove);
             }
-            L3.n = U3c.n = n;
-            k_keep_count<<<G, 256, 0, s>>>(n, L2.rp, L2.v, lthr, droptol, 0, lc);
-            k_keep_count<<<G, 256, 0, s>>>(n, U2c.rp, U2c.v, uthr, droptol, 1, uc);
+            L3.n = U3.n = n;
+            k_keep_count<<<G, 256, 0, s>>>(n, L2.rp, L2.ci, L2.v, lthr, droptol, 0, lc);
+            k_keep_count<<<G, 256, 0, s>>>(n, U2.rp, U2.ci, U2.v, uthr, droptol, 1, uc);
             check_launch();
             L3.nnz = scan_counts(c, lc, L3.rp);
-            U3c.nnz = scan_counts(c, uc, U3c.rp);
+            U3.nnz = scan_counts(c, uc, U3.rp);
             L3.ci.alloc(L3.nnz); L3.v.alloc(L3.nnz);
-            U3c.ci.alloc(std::max<long>(U3c.nnz, 1)); U3c.v.alloc(std::max<long>(U3c.nnz, 1));
+            U3.ci.alloc(std::max<long>(U3.nnz, 1)); U3.v.alloc(std::max<long>(U3.nnz, 1));
             k_keep_fill<<<G, 256, 0, s>>>(n, L2.rp, L2.ci, L2.v, lthr, droptol, 0, L3.rp, L3.ci, L3.v);
-            k_keep_fill<<<G, 256, 0, s>>>(n, U2c.rp, U2c.ci, U2c.v, uthr, droptol, 1, U3c.rp, U3c.ci, U3c.v);
+            k_keep_fill<<<G, 256, 0, s>>>(n, U2.rp, U2.ci, U2.v, uthr, droptol, 1, U3.rp, U3.ci, U3.v);
             check_launch();
         } else {
             L3 = std::move(L2);
-            U3c = std::move(U2c);
+            U3 = std::move(U2);
         }
-        // L sweep, then U sweep with the new L (U rows by CSR for the products)
+        tr_th.stop();
+        Trace tr_s2("  L/U sweeps", s);
+        // L sweep, then U sweep with the new L
         {
-            DCsr U3;
-            plt_transpose(c, U3c, U3);
             DBuf<double> lnew, unew;
             lnew.alloc(L3.nnz);
             k_plt_sweep_rows<<<rg, 32 * PLT_SW_WARPS, 0, s>>>(n, 1, A.rp, A.ci, A.v, L3.rp, L3.ci, L3.v, L3.v, U3.rp,
-                                                               U3.ci, U3.v, U3c.rp, U3c.ci, U3c.v, lnew, nullptr);
+                                                               U3.ci, U3.v, lnew, nullptr);
             check_launch();
             L3.v = std::move(lnew);
-            unew.alloc(std::max<long>(U3c.nnz, 1));
+            unew.alloc(std::max<long>(U3.nnz, 1));
             k_plt_sweep_rows<<<rg, 32 * PLT_SW_WARPS, 0, s>>>(n, 2, A.rp, A.ci, A.v, L3.rp, L3.ci, L3.v, L3.v, U3.rp,
-                                                               U3.ci, U3.v, U3c.rp, U3c.ci, U3c.v, nullptr, unew);
+                                                               U3.ci, U3.v, nullptr, unew);
             check_launch();
-            U3c.v = std::move(unew);
+            U3.v = std::move(unew);
         }
         L = std::move(L3);
-        DCsr Unew;
-        plt_transpose(c, U3c, Unew);
-        U = std::move(Unew);
+        U = std::move(U3);
     }
-    // seqilu0 layout
+    // seqilu0 layout (kept after the build: ordinary allocations)
+    pool.end();
+    Trace tr_fin("  final layout + download", s);
     R.n = n;
     k_plt_final_count<<<G, 256, 0, s>>>(n, L.rp, U.rp, lc, uc);
     check_launch();
@@ -791,11 +936,12 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, co
 inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriDev &U, bool need32)
 {
     Trace tr_all("ilut_to_tri", s);
-    auto up = [&](TriDev &T, const std::vector<int> &nrp, const std::vector<int> &nci, bool upper, const double *vals) {
+    auto up = [&](TriDev &T, const std::vector<int> &nrp, const std::vector<int> &nci, const int *drp, const int *dci,
+                  bool upper, const double *vals) {
         T = TriDev();
         {
             Trace tr("  build_tri_dev", s);
-            build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s, /*identity_src=*/true);
+            build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s, /*identity_src=*/true, drp, dci);
         }
         const long m = std::max<long>(T.nnz, 1);
         const int g = geom().sms * 4;
@@ -819,8 +965,8 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
         check_launch();
         XS_CUDA(cudaStreamSynchronize(s));
     };
-    up(L, R.hlrp, R.hlci, false, R.lv.p);
-    up(U, R.hurp, R.huci, true, R.uv.p);
+    up(L, R.hlrp, R.hlci, R.lrp.p, R.lci.p, false, R.lv.p);
+    up(U, R.hurp, R.huci, R.urp.p, R.uci.p, true, R.uv.p);
     const int g = geom().sms * 4;
     U.dinv64.alloc(n); U.dinv64_nat.alloc(n);
     k_gather_dinv<double><<<g, 256, 0, s>>>(n, U.perm.p, R.diag_ident.p, R.dinv.p, U.dinv64.p);

@@ -73,6 +73,7 @@ FormatTuning &format_tuning();
 // ascending distinct diagonal offsets of a CSR pattern if it qualifies for
 // diagonal ELL slots (at most ELL_DIA_MAX, at most 25% padding), else empty
 std::vector<int> dia_offsets(int n, const int *rp, const int *ci);
+long max_col_offset(int n, const int *rp, const int *ci);
 
 struct TrsvTuning {
     int blocks_per_sm = 2;
@@ -888,13 +889,18 @@ namespace xs {
 // plus the natural-order copy used by the Jacobi-sweep mode.
 template <typename SrcF>
 // identity_src: entry k's value is vals[k] (src_of is not called)
+// d_rp/d_ci: the same pattern already on the device (copied instead of uploaded)
 inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const std::vector<int> &ci, bool upper, SrcF src_of,
-                          cudaStream_t s, bool identity_src = false)
+                          cudaStream_t s, bool identity_src = false, const int *d_rp = nullptr,
+                          const int *d_ci = nullptr)
 {
     TriHostPlan P;  // level analysis (also gives the level count)
     const int chr = trsv_tuning().chunk_rows;
     T.chunked = chr > 0;
+    Trace tr_an("    level analysis", s);
     tri_analyse(n, rp.data(), ci.data(), upper, src_of, P, /*entries=*/false);
+    tr_an.stop();
+    Trace tr_up("    upload + positions", s);
     T.n = n;
     T.nnz = P.prp[n];
     T.nlevels = P.nlevels;
@@ -902,8 +908,15 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     const long m = std::max<long>(T.nnz, 1);
     const int g = geom().sms * 4;
     // natural CSR and the source index of each entry's value
-    T.rp_nat.alloc(n + 1); T.rp_nat.upload(rp.data(), n + 1, s);
-    T.ci_nat.alloc(m); if (T.nnz) T.ci_nat.upload(ci.data(), T.nnz, s);
+    T.rp_nat.alloc(n + 1);
+    T.ci_nat.alloc(m);
+    if (d_rp && d_ci) {
+        XS_CUDA(cudaMemcpyAsync(T.rp_nat.p, d_rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, s));
+        if (T.nnz) XS_CUDA(cudaMemcpyAsync(T.ci_nat.p, d_ci, sizeof(int) * T.nnz, cudaMemcpyDeviceToDevice, s));
+    } else {
+        T.rp_nat.upload(rp.data(), n + 1, s);
+        if (T.nnz) T.ci_nat.upload(ci.data(), T.nnz, s);
+    }
     T.src_nat.alloc(m);
     if (identity_src) {
         k_iota_long<<<g, 256, 0, s>>>(T.nnz, T.src_nat.p);
@@ -933,6 +946,8 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         T.lvl_off.alloc(C.lvl_off.size()); T.lvl_off.upload(C.lvl_off.data(), C.lvl_off.size(), s);
         T.lvl_ptr.alloc(C.lvl_ptr.size()); T.lvl_ptr.upload(C.lvl_ptr.data(), C.lvl_ptr.size(), s);
     }
+    tr_up.stop();
+    Trace tr_ell("    ELL copy", s);
     // ELL copy when the rows are nearly uniform (padding at most 2x)
     int w = 0;
     for (int i = 0; i < n; i++) w = std::max(w, rp[i + 1] - rp[i]);
@@ -961,9 +976,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     } else if (w > 0 && w <= 64 && (long)w * n <= 2 * std::max<long>(T.nnz, 1)) {
         // layout of the operator's ELL copy, built on the device from the
         // natural CSR just uploaded
-        long maxoff = 0;
-        for (int i = 0; i < n; i++)
-            for (int q = rp[i]; q < rp[i + 1]; q++) maxoff = std::max(maxoff, std::labs((long)ci[q] - i));
+        const long maxoff = max_col_offset(n, rp.data(), ci.data());
         T.ell_w = w;
         T.ell16 = format_tuning().ell_index16 && maxoff <= 32767;
         const long ld = ell_ld(n);
