@@ -144,6 +144,36 @@ def test_ilu0_bitwise_vs_oracle_large(cuda):
             assert np.array_equal(G[k], getattr(F, k)), (A.name, k)
 
 
+def _wide_rows_matrix():
+    """2D 5-point Poisson 40x40 plus 5 rows coupled to 40-60 random columns
+    (weakly, so the pivots stay away from zero): rows wider than 32 entries,
+    the row-width class the lane-group ILU(0) kernel leaves to the
+    thread-per-row kernel, next to ordinary rows."""
+    A = st.poisson2d_5pt(40)
+    n = A.n
+    rng = np.random.default_rng(3)
+    S = A.to_scipy().tolil()
+    for i in (100, 555, 800, 1201, 1599):
+        for j in rng.choice(n, int(rng.integers(40, 61)), replace=False):
+            if j != i:
+                S[i, j] = -0.01 * rng.random()
+                S[j, i] = -0.01 * rng.random()
+    S = S.tocsr()
+    S.sort_indices()
+    return st.CSRMatrix(n, S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data.copy(), "wide-rows")
+
+
+def test_ilu0_bitwise_vs_oracle_wide_and_narrow_rows(cuda):
+    """Both ILU(0) row kernels against the oracle: lane groups of 4, 8 and 32
+    (5-, 7- and 27-point rows) and the thread-per-row kernel (rows over 32
+    entries)."""
+    from xsolver_b200.api import Plan
+
+    for A in (st.poisson2d_5pt(64), st.poisson3d_7pt(20), st.convdiff3d_27pt(14), _wide_rows_matrix()):
+        P = Plan(A).factor("ilu0")
+        assert np.array_equal(P.lu_values(), oracle.ilu0_values(A)), A.name
+
+
 def test_parilu_bitwise_vs_oracle(cuda):
     from xsolver_b200.api import Plan
 

@@ -325,6 +325,7 @@ struct Handle {
     std::vector<int> huptr;
     DBuf<int> uptr, rowof, ucp, ucpos, flags;
     int ilu_epoch = 0;
+    int max_row_len = -1;  // longest row of the pattern (-1: not yet counted)
     DBuf<unsigned> fticket;
     TriHostPlan hL, hU;
     DBuf<double> luv, fv, tmpv;
@@ -553,6 +554,7 @@ static void analyse_pattern(Handle &h)
     h.udiag_src.upload(ud.data(), n, h.s);
     h.flags.alloc(n);
     h.ilu_epoch = 0;
+    h.max_row_len = -1;
     XS_CUDA(cudaStreamSynchronize(h.s));
     h.analysed = true;
 }
@@ -614,9 +616,46 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
             XS_CUDA(cudaMemsetAsync(h.flags.p, 0, sizeof(int) * n, h.s));
             h.ilu_epoch = 1;
         }
-        const int gl = (n + 127) / 128;
-        k_ilu0_rows<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.luv.p, h.flags.p, h.ilu_epoch,
-                                         h.err.p, h.fticket.p);
+        // persistent CTAs per SM: 8 for the lane-group kernel (7.9 ms for the
+        // 128^3 7-point refactorisation, 9-25 ms at 4 or 16), 1 for the
+        // thread-per-row kernel (12 ms; 21-45 ms with a CTA per 128 rows)
+        static const int ilu_bps_env = [] {
+            const char *e = getenv("XS_ILU_BLOCKS_PER_SM");
+            return e ? std::max(1, atoi(e)) : 0;
+        }();
+        static const int ilu_backoff = [] {
+            const char *e = getenv("XS_ILU_BACKOFF_NS");
+            return e ? std::max(32, atoi(e)) : 256;
+        }();
+        static const int ilu_group = [] {
+            const char *e = getenv("XS_ILU_GROUP");
+            return e ? atoi(e) : 1;
+        }();
+        // lanes per row: the longest row rounded up to a power of two (<= 32)
+        if (h.max_row_len < 0) {
+            int wmax = 0;
+            for (int i = 0; i < n; i++) wmax = std::max(wmax, h.hrp[i + 1] - h.hrp[i]);
+            h.max_row_len = wmax;
+        }
+        const int wmax = h.max_row_len;
+        int G = 4;
+        while (G < wmax && G < 64) G <<= 1;
+        if (ilu_group && G <= 32) {
+            const int rpb = 128 / G;
+            const int gl = std::min((n + rpb - 1) / rpb, geom().sms * (ilu_bps_env ? ilu_bps_env : 8));
+            auto go = [&](auto kern) {
+                kern<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.luv.p, h.flags.p,
+                                          h.ilu_epoch, h.err.p, h.fticket.p, ilu_backoff);
+            };
+            if (G == 4) go(k_ilu0_groups<4>);
+            else if (G == 8) go(k_ilu0_groups<8>);
+            else if (G == 16) go(k_ilu0_groups<16>);
+            else go(k_ilu0_groups<32>);
+        } else {
+            const int gl = std::min((n + 127) / 128, geom().sms * (ilu_bps_env ? ilu_bps_env : 1));
+            k_ilu0_rows<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.luv.p, h.flags.p,
+                                             h.ilu_epoch, h.err.p, h.fticket.p, ilu_backoff);
+        }
         check_launch();
     } else {
         h.tmpv.alloc(std::max<long>(h.nnz, 1));

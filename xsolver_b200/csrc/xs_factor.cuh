@@ -24,64 +24,195 @@
 namespace xs {
 
 
-// exact ILU(0), thread per row in level order (perm/level from the L analysis)
+// position of column c in the sorted index range [a, b) of ci, or -1
+__device__ __forceinline__ int find_col(const int *__restrict__ ci, int a, int b, int c)
+{
+    int l = a, r = b;
+    while (l < r) {
+        const int m = (l + r) >> 1;
+        if (__ldg(ci + m) < c) l = m + 1;
+        else r = m;
+    }
+    return (l < b && __ldg(ci + l) == c) ? l : -1;
+}
+
+// exact ILU(0), thread per row in level order (perm/level from the L analysis);
+// used for patterns with rows of more than 32 entries.  Persistent CTAs take
+// 128-row tickets in order, so only the rows a few tickets ahead of the
+// slowest level are in flight: a launch with one CTA per 128 rows kept every
+// resident row polling its dependencies, and those polls crowded the L2 that
+// the rows on the critical path read their pivots from.  Waits back off
+// exponentially up to backoff_ns.  Every ticket depends only on smaller
+// tickets (level order), each held by a running CTA, so the loop progresses.
 __global__ void __launch_bounds__(128) k_ilu0_rows(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                                                   const int *__restrict__ uptr, const int *__restrict__ perm, double *luv,
-                                                  int *flag, int epoch, int *err, unsigned *ticket)
+                                                  int *flag, int epoch, int *err, unsigned *ticket, int backoff_ns)
 {
     __shared__ int s_blk;
-    if (threadIdx.x == 0) {
-        unsigned t = atomicAdd(ticket, 1u);
-        if (t == gridDim.x - 1) *ticket = 0u;
-        s_blk = (int)t;
-    }
-    __syncthreads();
-    const int p = s_blk * 128 + (int)threadIdx.x;
-    if (p >= n) return;
-    const int i = perm[p];
-    const int rs = rp[i], re = rp[i + 1], up = uptr[i];
-    for (int j = rs; j < up; j++) {
-        const int k = ci[j];
-        long spins = 0;
-        unsigned long long t0 = 0;
-        while (ld_acquire(flag + k) != epoch) {
-            __nanosleep(32);  // yield point: the producer may be a lane of this warp
-            if ((++spins & 255) == 0) {
-                const unsigned long long t = gtimer();
-                if (t0 == 0) t0 = t;
-                else if (t - t0 > WAIT_LIMIT_NS) {
-                    atomicOr(err, DEV_FACTOR_TIMEOUT);
-                    return;
+    const int ntk = (n + 127) / 128;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            // every CTA ends with one failing claim; the last of them re-arms
+            if (t == (unsigned)(ntk + gridDim.x - 1)) *ticket = 0u;
+            s_blk = (int)t;
+        }
+        __syncthreads();
+        const int blk = s_blk;
+        __syncthreads();
+        if (blk >= ntk) return;
+        const int p = blk * 128 + (int)threadIdx.x;
+        if (p >= n) continue;
+        if (*(volatile int *)err) continue;
+        const int i = perm[p];
+        const int rs = rp[i], re = rp[i + 1], up = uptr[i];
+        bool ok = true;
+        for (int j = rs; j < up && ok; j++) {
+            const int k = ci[j];
+            long spins = 0;
+            unsigned long long t0 = 0;
+            unsigned ns = 32;
+            while (ld_acquire(flag + k) != epoch) {
+                __nanosleep(ns);  // yield point: the producer may be a lane of this warp
+                if (ns < (unsigned)backoff_ns) ns <<= 1;
+                if ((++spins & 63) == 0) {
+                    const unsigned long long t = gtimer();
+                    if (t0 == 0) t0 = t;
+                    else if (t - t0 > WAIT_LIMIT_NS) {
+                        atomicOr(err, DEV_FACTOR_TIMEOUT);
+                        ok = false;
+                        break;
+                    }
+                    if (*(volatile int *)err) {
+                        ok = false;
+                        break;
+                    }
                 }
-                if (*(volatile int *)err) return;
+            }
+            if (!ok) break;
+            const int ukp = uptr[k];
+            const int kend = rp[k + 1];
+            double piv = __ldcg(luv + ukp);
+            if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
+            const double lij = luv[j] / piv;
+            luv[j] = lij;
+            int subptr = ukp;
+            for (int jj = j + 1; jj < re; jj++) {
+                const int kk = ci[jj];
+                while (subptr < kend && __ldg(ci + subptr) < kk) subptr++;
+                if (subptr < kend) {
+                    if (__ldg(ci + subptr) == kk) {
+                        const double t = lij * __ldcg(luv + subptr);
+                        luv[jj] = luv[jj] - t;
+                    }
+                } else
+                    break;
             }
         }
-        const int ukp = uptr[k];
-        const int kend = rp[k + 1];
-        double piv = __ldcg(luv + ukp);
-        if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
-        const double lij = luv[j] / piv;
-        luv[j] = lij;
-        int subptr = ukp;
-        for (int jj = j + 1; jj < re; jj++) {
-            const int kk = ci[jj];
-            while (subptr < kend && __ldg(ci + subptr) < kk) subptr++;
-            if (subptr < kend) {
-                if (__ldg(ci + subptr) == kk) {
-                    const double t = lij * __ldcg(luv + subptr);
-                    luv[jj] = luv[jj] - t;
-                }
-            } else
-                break;
+        if (!ok) continue;
+        double d = luv[up];
+        if (fabs(d) < 1e-20) {
+            d = 1e-20;
+            luv[up] = d;
         }
+        __threadfence();
+        st_release(flag + i, epoch);
     }
-    double d = luv[up];
-    if (fabs(d) < 1e-20) {
-        d = 1e-20;
-        luv[up] = d;
+}
+
+// Exact ILU(0) with a group of G lanes per row (G >= the longest row, G a
+// power of two <= 32), 128/G rows per ticket, tickets in level order as in
+// k_ilu0_rows.  Lane q owns entries rs+q, rs+q+G, ... of row i.  For each L
+// entry j of row i in order (k = its column): every lane locates its first
+// entry's column in row k's upper part (pattern data: before the wait for
+// row k), lane 0 waits for row k's flag, then l_ij = a_ij / u_kk and every
+// lane subtracts l_ij * u_k,c from its entries with a match — the operations
+// of the thread-per-row update, entry by entry in the same k order, so the
+// factors are bitwise the same; but the merge with row k runs across the
+// lanes, and the critical path per k is one flag wait and one L2 round trip.
+template <int G>
+__global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                                    const int *__restrict__ uptr, const int *__restrict__ perm,
+                                                    double *luv, int *flag, int epoch, int *err, unsigned *ticket,
+                                                    int backoff_ns)
+{
+    constexpr int RPB = 128 / G;  // rows per ticket
+    __shared__ int s_blk, s_err;
+    const int g = threadIdx.x / G, q = threadIdx.x % G;
+    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+    const int ntk = (n + RPB - 1) / RPB;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            // every CTA ends with one failing claim; the last of them re-arms
+            if (t == (unsigned)(ntk + gridDim.x - 1)) *ticket = 0u;
+            s_blk = (int)t;
+            s_err = *(volatile int *)err;
+        }
+        __syncthreads();
+        const int blk = s_blk, blk_err = s_err;
+        __syncthreads();
+        if (blk >= ntk) return;
+        const int p = blk * RPB + g;
+        if (p >= n || blk_err) continue;  // uniform over the group
+        const int i = perm[p];
+        const int rs = rp[i], re = rp[i + 1], up = uptr[i];
+        bool ok = true;
+        for (int j = rs; j < up; j++) {
+            const int k = ci[j];
+            const int ukp = uptr[k], kend = rp[k + 1];
+            // this lane's first entry after j and its match in row k (pattern only)
+            const int e0 = j + 1 + q;
+            int pos0 = -1;
+            if (e0 < re) pos0 = find_col(ci, ukp + 1, kend, ci[e0]);
+            if (q == 0) {
+                long spins = 0;
+                unsigned long long t0 = 0;
+                unsigned ns = 32;
+                while (ld_acquire(flag + k) != epoch) {
+                    __nanosleep(ns);  // yield point: the producer may be a lane of this warp
+                    if (ns < (unsigned)backoff_ns) ns <<= 1;
+                    if ((++spins & 63) == 0) {
+                        const unsigned long long t = gtimer();
+                        if (t0 == 0) t0 = t;
+                        else if (t - t0 > WAIT_LIMIT_NS) {
+                            atomicOr(err, DEV_FACTOR_TIMEOUT);
+                            ok = false;
+                            break;
+                        }
+                        if (*(volatile int *)err) {
+                            ok = false;
+                            break;
+                        }
+                    }
+                }
+            }
+            ok = __shfl_sync(gmask, ok, 0, G);
+            if (!ok) break;
+            __syncwarp(gmask);  // orders the group's loads of row k after lane 0's acquire
+            double piv = __ldcg(luv + ukp);
+            if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
+            const double lij = luv[j] / piv;
+            __syncwarp(gmask);  // every lane has read a_ij before its owner overwrites it
+            if (((j - rs) % G) == q) luv[j] = lij;
+            for (int e = e0, pos = pos0; e < re; e += G) {
+                if (e != e0) pos = find_col(ci, ukp + 1, kend, ci[e]);
+                if (pos >= 0) {
+                    const double t = lij * __ldcg(luv + pos);
+                    luv[e] = luv[e] - t;
+                }
+            }
+            __syncwarp(gmask);  // the next L entry's value is final
+        }
+        if (!ok) continue;
+        if (((up - rs) % G) == q) {
+            const double d = luv[up];
+            if (fabs(d) < 1e-20) luv[up] = 1e-20;
+        }
+        __threadfence();
+        __syncwarp(gmask);
+        if (q == 0) st_release(flag + i, epoch);
     }
-    __threadfence();
-    st_release(flag + i, epoch);
 }
 
 // one synchronous ParILU sweep over A's nonzeros
