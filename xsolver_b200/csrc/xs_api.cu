@@ -273,7 +273,9 @@ void operator_build_ell(Operator &op, const int *rp0, const int *ci0, const doub
     } else {
         op.ev32.free();
     }
-    op.ell_grid = (int)std::min<long>((long)geom().sms * ELL_BLOCKS_PER_SM, (n + 256L * ELL_ROWS - 1) / (256L * ELL_ROWS));
+    // one wave of resident CTAs (the fused reductions' partial count follows
+    // the grid, which is fixed per operator)
+    op.ell_grid = (int)std::min<long>((long)geom().sms * ELL_MIN_BLOCKS, (n + 256L * ELL_ROWS - 1) / (256L * ELL_ROWS));
     if (op.ell_grid < 1) op.ell_grid = 1;
     XS_CUDA(cudaStreamSynchronize(s));
 }

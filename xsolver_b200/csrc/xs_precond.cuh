@@ -173,8 +173,9 @@ struct PrecondDev {
             if (T.ell_w > 0) {
                 const FT *ev = T.evals<FT>();
                 const int *doff = T.doff.p;
-                const int gs = std::max(1, std::min(g * ELL_ROWS / ell_rows_for<FT>(),
-                                                    (n + 256 * ell_rows_for<FT>() - 1) / (256 * ell_rows_for<FT>())));
+                // one wave of resident CTAs, grid-stride over the row blocks
+                const int rb = (n + 256 * ell_rows_for<FT>() - 1) / (256 * ell_rows_for<FT>());
+                const int gs = std::max(1, std::min(geom().sms * sweep_min_blocks_for<FT>(), rb));
                 auto go = [&](auto cols) {
                     using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
                     const DT *dv = upper ? dinv : (const DT *)nullptr;

@@ -279,16 +279,19 @@ __device__ __forceinline__ void ell_stage_offsets(const int *doff, int w, int *s
 }
 
 // Launch shape of the ELL kernels (SpMV and the Jacobi-sweep triangle
-// kernels): CTAs of 256 threads, ELL_MIN_BLOCKS of them resident per SM,
-// ELL_BLOCKS_PER_SM per SM in the grid; each thread takes ELL_ROWS
-// consecutive rows (vector loads of the slot data) and walks the entries in
-// chunks of ELL_CHUNK, issuing every load of a chunk before its gathers.
-// These kernels are bound by the latency of the dependent index -> gather
-// loads, so the shape trades registers (rows x chunk in flight) against
-// resident warps.  Default (5 CTAs of 256 resident, 51 registers, 10 CTAs
-// per SM in the grid, 2 rows x 8 slots per thread) was the fastest of nine
-// shapes timed on B200 for the 128^3 7-point ELL SpMV (FP32/FP64) and the
-// BF16/FP32/FP64 Jacobi-sweep passes.
+// kernels): CTAs of 256 threads, ELL_MIN_BLOCKS of them resident per SM;
+// each thread takes ELL_ROWS consecutive rows (vector loads of the slot
+// data) and walks the entries in chunks of ELL_CHUNK, issuing every load of
+// a chunk before its gathers.  These kernels are bound by the latency of the
+// dependent index -> gather loads, so the shape trades registers (rows x
+// chunk in flight) against resident warps.  Default (5 CTAs of 256
+// resident, 51 registers, 2 rows x 8 slots per thread) was the fastest of
+// nine shapes timed on B200 for the 128^3 7-point ELL SpMV (FP32/FP64) and
+// the BF16/FP32/FP64 Jacobi-sweep passes.  The grids are one wave of
+// resident CTAs with a grid-stride loop: the SpMV 5 CTAs per SM, each sweep
+// pass sweep_min_blocks_for<FT>() per SM (a second partial wave of CTAs cost
+// 4 us of the 44 us BF16 apply and 1.8 ms of the 27 ms mixed solve at 128^3).
+// ELL_BLOCKS_PER_SM sizes the grids of the CSR sweep and vector kernels.
 #ifndef XS_ELL_MIN_BLOCKS
 #define XS_ELL_MIN_BLOCKS 5
 #endif
