@@ -618,9 +618,11 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
             XS_CUDA(cudaMemsetAsync(h.flags.p, 0, sizeof(int) * n, h.s));
             h.ilu_epoch = 1;
         }
-        // persistent CTAs per SM: 8 for the lane-group kernel (7.9 ms for the
-        // 128^3 7-point refactorisation, 9-25 ms at 4 or 16), 1 for the
-        // thread-per-row kernel (12 ms; 21-45 ms with a CTA per 128 rows)
+        // persistent CTAs per SM: lane-group kernel 4 for groups of <= 8 lanes
+        // (128^3 7-point refactorisation 6.9 ms; 7.8 at 8, 7-49 at 16) and 8
+        // for wider groups (96^3 27-point 8.7 ms; 10.5 at 4, 13 at 16); the
+        // thread-per-row kernel 1 (12 ms at 128^3; 21-45 ms with a CTA per
+        // 128 rows)
         static const int ilu_bps_env = [] {
             const char *e = getenv("XS_ILU_BLOCKS_PER_SM");
             return e ? std::max(1, atoi(e)) : 0;
@@ -644,7 +646,8 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
         while (G < wmax && G < 64) G <<= 1;
         if (ilu_group && G <= 32) {
             const int rpb = 128 / G;
-            const int gl = std::min((n + rpb - 1) / rpb, geom().sms * (ilu_bps_env ? ilu_bps_env : 8));
+            const int bps = ilu_bps_env ? ilu_bps_env : (G <= 8 ? 4 : 8);
+            const int gl = std::min((n + rpb - 1) / rpb, geom().sms * bps);
             auto go = [&](auto kern) {
                 kern<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.luv.p, h.flags.p,
                                           h.ilu_epoch, h.err.p, h.fticket.p, ilu_backoff);

@@ -122,14 +122,24 @@ __global__ void __launch_bounds__(128) k_ilu0_rows(int n, const int *__restrict_
 
 // Exact ILU(0) with a group of G lanes per row (G >= the longest row, G a
 // power of two <= 32), 128/G rows per ticket, tickets in level order as in
-// k_ilu0_rows.  Lane q owns entries rs+q, rs+q+G, ... of row i.  For each L
-// entry j of row i in order (k = its column): every lane locates its first
-// entry's column in row k's upper part (pattern data: before the wait for
-// row k), lane 0 waits for row k's flag, then l_ij = a_ij / u_kk and every
-// lane subtracts l_ij * u_k,c from its entries with a match — the operations
-// of the thread-per-row update, entry by entry in the same k order, so the
-// factors are bitwise the same; but the merge with row k runs across the
-// lanes, and the critical path per k is one flag wait and one L2 round trip.
+// k_ilu0_rows.  Lane q holds entry rs+q of row i in a register.  Rows with at
+// most PLT_L_MAX strictly lower entries (nl) go in three phases:
+//   1. pattern only, before any wait: lane q finds its column in the upper
+//      part of every row k_j (k_j = column of L entry j < q);
+//   2. lanes 0..nl-1 wait for the flags of their own columns k_q at once,
+//      then every lane loads the values it needs (the pivots u_kk by lanes
+//      0..nl-1, u_{k_j,c_q} at the positions of phase 1) in one round;
+//   3. for j = 0..nl-1 in order: l = a_j / u_{k_j k_j} (a_j, u from lane j
+//      by shuffle), lane j keeps l, every lane q > j with a match does
+//      a_q = a_q - l * u_{k_j,c_q}; then the diagonal clamp, the row is
+//      written back and its flag released.
+// These are the operations of the thread-per-row IKJ update entry by entry
+// in the same j order, so the factors are bitwise the same; the critical
+// path of a row is one wait for its latest dependency, one L2 round trip
+// and a few shuffles.  Rows with more lower entries take the elimination
+// steps one at a time (locate, wait, load, update per L entry).
+constexpr int ILU_L_MAX = 16;
+
 template <int G>
 __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                                                     const int *__restrict__ uptr, const int *__restrict__ perm,
@@ -137,10 +147,31 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
                                                     int backoff_ns)
 {
     constexpr int RPB = 128 / G;  // rows per ticket
+    constexpr int LM = G - 1 < ILU_L_MAX ? G - 1 : ILU_L_MAX;  // register-resident L entries
     __shared__ int s_blk, s_err;
     const int g = threadIdx.x / G, q = threadIdx.x % G;
     const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
     const int ntk = (n + RPB - 1) / RPB;
+    // bounded wait of one lane for flag k; false after the limit or another error
+    auto wait_flag = [&](int k) -> bool {
+        long spins = 0;
+        unsigned long long t0 = 0;
+        unsigned ns = 32;
+        while (ld_acquire(flag + k) != epoch) {
+            __nanosleep(ns);  // yield point: the producer may be a lane of this warp
+            if (ns < (unsigned)backoff_ns) ns <<= 1;
+            if ((++spins & 63) == 0) {
+                const unsigned long long t = gtimer();
+                if (t0 == 0) t0 = t;
+                else if (t - t0 > WAIT_LIMIT_NS) {
+                    atomicOr(err, DEV_FACTOR_TIMEOUT);
+                    return false;
+                }
+                if (*(volatile int *)err) return false;
+            }
+        }
+        return true;
+    };
     while (true) {
         if (threadIdx.x == 0) {
             const unsigned t = atomicAdd(ticket, 1u);
@@ -157,57 +188,78 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
         if (p >= n || blk_err) continue;  // uniform over the group
         const int i = perm[p];
         const int rs = rp[i], re = rp[i + 1], up = uptr[i];
+        const int nl = up - rs;
         bool ok = true;
-        for (int j = rs; j < up; j++) {
-            const int k = ci[j];
-            const int ukp = uptr[k], kend = rp[k + 1];
-            // this lane's first entry after j and its match in row k (pattern only)
-            const int e0 = j + 1 + q;
-            int pos0 = -1;
-            if (e0 < re) pos0 = find_col(ci, ukp + 1, kend, ci[e0]);
-            if (q == 0) {
-                long spins = 0;
-                unsigned long long t0 = 0;
-                unsigned ns = 32;
-                while (ld_acquire(flag + k) != epoch) {
-                    __nanosleep(ns);  // yield point: the producer may be a lane of this warp
-                    if (ns < (unsigned)backoff_ns) ns <<= 1;
-                    if ((++spins & 63) == 0) {
-                        const unsigned long long t = gtimer();
-                        if (t0 == 0) t0 = t;
-                        else if (t - t0 > WAIT_LIMIT_NS) {
-                            atomicOr(err, DEV_FACTOR_TIMEOUT);
-                            ok = false;
-                            break;
-                        }
-                        if (*(volatile int *)err) {
-                            ok = false;
-                            break;
-                        }
+        if (nl <= LM) {
+            const bool mine = rs + q < re;
+            const int c = mine ? ci[rs + q] : 0;
+            double a = mine ? luv[rs + q] : 0.0;
+            // phase 1: pattern lookups
+            int pos[LM > 0 ? LM : 1];
+#pragma unroll
+            for (int j = 0; j < LM; j++) {
+                pos[j] = -1;
+                if (j < nl && j < q && mine) {
+                    const int k = ci[rs + j];
+                    pos[j] = find_col(ci, uptr[k] + 1, rp[k + 1], c);
+                }
+            }
+            // phase 2: wait for every dependency at once, then load
+            if (q < nl) ok = wait_flag(c);
+            ok = __all_sync(gmask, ok);
+            if (!ok) continue;
+            __syncwarp(gmask);  // orders the group's loads after the acquires
+            const double pv = q < nl ? __ldcg(luv + uptr[c]) : 1.0;
+            double u[LM > 0 ? LM : 1];
+#pragma unroll
+            for (int j = 0; j < LM; j++) u[j] = pos[j] >= 0 ? __ldcg(luv + pos[j]) : 0.0;
+            // phase 3: the eliminations in order, in registers
+#pragma unroll
+            for (int j = 0; j < LM; j++) {
+                if (j < nl) {
+                    double piv = __shfl_sync(gmask, pv, j, G);
+                    if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
+                    const double lij = __shfl_sync(gmask, a, j, G) / piv;
+                    if (q == j) a = lij;
+                    if (pos[j] >= 0) {
+                        const double t = lij * u[j];
+                        a = a - t;
                     }
                 }
             }
-            ok = __shfl_sync(gmask, ok, 0, G);
-            if (!ok) break;
-            __syncwarp(gmask);  // orders the group's loads of row k after lane 0's acquire
-            double piv = __ldcg(luv + ukp);
-            if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
-            const double lij = luv[j] / piv;
-            __syncwarp(gmask);  // every lane has read a_ij before its owner overwrites it
-            if (((j - rs) % G) == q) luv[j] = lij;
-            for (int e = e0, pos = pos0; e < re; e += G) {
-                if (e != e0) pos = find_col(ci, ukp + 1, kend, ci[e]);
-                if (pos >= 0) {
-                    const double t = lij * __ldcg(luv + pos);
-                    luv[e] = luv[e] - t;
+            if (q == nl && fabs(a) < 1e-20) a = 1e-20;  // diagonal clamp (entry up = rs + nl)
+            if (mine) luv[rs + q] = a;
+        } else {
+            for (int j = rs; j < up; j++) {
+                const int k = ci[j];
+                const int ukp = uptr[k], kend = rp[k + 1];
+                // this lane's first entry after j and its match in row k (pattern only)
+                const int e0 = j + 1 + q;
+                int pos0 = -1;
+                if (e0 < re) pos0 = find_col(ci, ukp + 1, kend, ci[e0]);
+                if (q == 0) ok = wait_flag(k);
+                ok = __shfl_sync(gmask, ok, 0, G);
+                if (!ok) break;
+                __syncwarp(gmask);  // orders the group's loads of row k after lane 0's acquire
+                double piv = __ldcg(luv + ukp);
+                if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
+                const double lij = luv[j] / piv;
+                __syncwarp(gmask);  // every lane has read a_ij before its owner overwrites it
+                if (((j - rs) % G) == q) luv[j] = lij;
+                for (int e = e0, pos = pos0; e < re; e += G) {
+                    if (e != e0) pos = find_col(ci, ukp + 1, kend, ci[e]);
+                    if (pos >= 0) {
+                        const double t = lij * __ldcg(luv + pos);
+                        luv[e] = luv[e] - t;
+                    }
                 }
+                __syncwarp(gmask);  // the next L entry's value is final
             }
-            __syncwarp(gmask);  // the next L entry's value is final
-        }
-        if (!ok) continue;
-        if (((up - rs) % G) == q) {
-            const double d = luv[up];
-            if (fabs(d) < 1e-20) luv[up] = 1e-20;
+            if (!ok) continue;
+            if (((up - rs) % G) == q) {
+                const double d = luv[up];
+                if (fabs(d) < 1e-20) luv[up] = 1e-20;
+            }
         }
         __threadfence();
         __syncwarp(gmask);
