@@ -252,6 +252,43 @@ def test_parilut_bitwise_vs_oracle(cuda):
             assert np.array_equal(G[k], getattr(F, k)), (A.name, k)
 
 
+def _parilut_fallback_matrix():
+    """2D 5-point Poisson 280x280 (n = 78,400) with (a) five long-range
+    couplings (i, i + 70000 mod n) and their transposes, so some rows'
+    candidate columns span more than the 65,536-column bitmap window, and (b)
+    one row and column coupled to 600 columns within +-30,000, so one row has
+    over 512 candidates and over 256 pattern entries in the sweeps: the
+    sort-based candidate path and the per-entry value and sweep paths next
+    to the bitmap and row-wise paths."""
+    A = st.poisson2d_5pt(280)
+    n = A.n
+    rng = np.random.default_rng(7)
+    S = A.to_scipy().tolil()
+    for i in (10, 20, 30, 77000, 78390):
+        j = (i + 70000) % n
+        S[i, j] = -0.05
+        S[j, i] = -0.05
+    r = 39000
+    for j in r - 30000 + rng.choice(60000, 600, replace=False):
+        if j != r:
+            S[r, j] = -0.001
+            S[j, r] = -0.001
+    S = S.tocsr()
+    S.sort_indices()
+    return st.CSRMatrix(n, S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data.copy(), "parilut-fallbacks")
+
+
+def test_parilut_fallback_paths_bitwise(cuda):
+    from xsolver_b200.api import Plan
+
+    A = _parilut_fallback_matrix()
+    for fill, sweeps, droptol in ((2.0, 3, 0.0), (1.5, 2, 1e-4)):
+        G = Plan(A).factor("parilut", sweeps=sweeps, fill=fill, droptol=droptol).factors()
+        F = oracle.parilut(A, fill=fill, sweeps=sweeps, droptol=droptol)
+        for k in ("lrp", "lci", "lv", "dinv", "urp", "uci", "uv"):
+            assert np.array_equal(G[k], getattr(F, k)), (fill, k)
+
+
 def test_block_and_syncfree_lusolve_bitwise(cuda):
     """The single-CTA solve (small systems) and the sync-free multi-CTA solve
     give the same bits, FP64 and FP32/BF16 factors."""

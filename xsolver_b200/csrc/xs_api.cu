@@ -352,6 +352,10 @@ struct Handle {
     int quirk = 0;
     // precision
     int inner32 = 0;
+    // plans keep every storage precision and layout of the factors (their
+    // callers switch precision and triangular-solve mode after factorising);
+    // handles build only what their configured solve reads
+    bool all_factor_copies = false;
     int factor_prec = FP_F64;
     double inner_rtol = 1e-4;
     int inner_maxiter = 200;
@@ -561,32 +565,53 @@ static void analyse_pattern(Handle &h)
     h.analysed = true;
 }
 
-// gather factor values (from an array over A's pattern) into every storage
-// precision the solves may use
-static void load_tri_values(Handle &h, TriDev &T, const double *vals, bool need32)
+// Which copies of the factor values the configured solve reads: position
+// order for the exact solves (trsv_mode 0), the ELL copy for the Jacobi
+// sweeps, the natural-order CSR for sweeps on a triangle without an ELL
+// copy; FP64 always, and with FP32 inner solves the one reduced precision
+// the factors are stored in (red: bit 0 FP32, bit 1 BF16, bit 2 FP16).
+struct FactorCopies {
+    bool pos = true, ell = true, nat = true;
+    unsigned red = 7u;
+};
+static FactorCopies factor_copies(const Handle &h, bool need32)
+{
+    FactorCopies c;
+    if (!need32) c.red = 0u;
+    if (h.all_factor_copies) return c;
+    c.pos = h.trsv_mode == 0;
+    c.ell = h.trsv_mode > 0;
+    c.nat = h.trsv_mode > 0;  // per triangle: only without an ELL copy
+    if (need32) c.red = h.factor_prec == FP_BF16 ? 2u : h.factor_prec == FP_F16 ? 4u : 1u;
+    return c;
+}
+
+// gather factor values (from an array over A's pattern) into the storage
+// precisions and layouts of `c`
+static void load_tri_values(Handle &h, TriDev &T, const double *vals, const FactorCopies &c)
 {
     const int g = geom().sms * 4;
-    long m = std::max<long>(T.nnz, 1);
-    if (T.pv64.n != (size_t)m) { T.pv64.alloc(m); T.nv64.alloc(m); }
-    if (T.nnz) {
-        k_gather_convert<double><<<g, 256, 0, h.s>>>(T.nnz, T.src.p, vals, T.pv64.p);
-        k_gather_convert<double><<<g, 256, 0, h.s>>>(T.nnz, T.src_nat.p, vals, T.nv64.p);
-    }
-    if (need32) {
-        if (T.pv32.n != (size_t)m) {
-            T.pv32.alloc(m); T.nv32.alloc(m);
-            T.pvbf.alloc(m); T.nvbf.alloc(m);
-            T.pvh.alloc(m); T.nvh.alloc(m);
+    const long m = std::max<long>(T.nnz, 1);
+    const bool pos = c.pos, nat = c.nat && (h.all_factor_copies || T.ell_w == 0);
+    auto one = [&](auto &pbuf, auto &nbuf) {
+        using FT = std::remove_pointer_t<decltype(pbuf.p)>;
+        if (pos) {
+            if (pbuf.n != (size_t)m) pbuf.alloc(m);
+            if (T.nnz) k_gather_convert<FT><<<g, 256, 0, h.s>>>(T.nnz, T.src.p, vals, pbuf.p);
+        } else {
+            pbuf.free();
         }
-        if (T.nnz) {
-            k_gather_convert<float><<<g, 256, 0, h.s>>>(T.nnz, T.src.p, vals, T.pv32.p);
-            k_gather_convert<float><<<g, 256, 0, h.s>>>(T.nnz, T.src_nat.p, vals, T.nv32.p);
-            k_gather_convert<__nv_bfloat16><<<g, 256, 0, h.s>>>(T.nnz, T.src.p, vals, T.pvbf.p);
-            k_gather_convert<__nv_bfloat16><<<g, 256, 0, h.s>>>(T.nnz, T.src_nat.p, vals, T.nvbf.p);
-            k_gather_convert<__half><<<g, 256, 0, h.s>>>(T.nnz, T.src.p, vals, T.pvh.p);
-            k_gather_convert<__half><<<g, 256, 0, h.s>>>(T.nnz, T.src_nat.p, vals, T.nvh.p);
+        if (nat) {
+            if (nbuf.n != (size_t)m) nbuf.alloc(m);
+            if (T.nnz) k_gather_convert<FT><<<g, 256, 0, h.s>>>(T.nnz, T.src_nat.p, vals, nbuf.p);
+        } else {
+            nbuf.free();
         }
-    }
+    };
+    one(T.pv64, T.nv64);
+    if (c.red & 1u) one(T.pv32, T.nv32); else { T.pv32.free(); T.nv32.free(); }
+    if (c.red & 2u) one(T.pvbf, T.nvbf); else { T.pvbf.free(); T.nvbf.free(); }
+    if (c.red & 4u) one(T.pvh, T.nvh); else { T.pvh.free(); T.nvh.free(); }
     check_launch();
 }
 
@@ -714,10 +739,15 @@ static void build_precond(Handle &h)
         if (h.fv.n != (size_t)std::max<long>(h.nnz, 1)) h.fv.alloc(std::max<long>(h.nnz, 1));
         k_split_lu<<<geom().sms * 4, 256, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, h.fv.p);
         check_launch();
-        load_tri_values(h, M.L, h.fv.p, need32);
-        load_tri_values(h, M.U, h.fv.p, need32);
-        load_tri_ell(M.L, h.fv.p, need32, h.s);
-        load_tri_ell(M.U, h.fv.p, need32, h.s);
+        const FactorCopies fc = factor_copies(h, need32);
+        load_tri_values(h, M.L, h.fv.p, fc);
+        load_tri_values(h, M.U, h.fv.p, fc);
+        if (fc.ell) {
+            load_tri_ell(M.L, h.fv.p, need32, h.s, fc.red);
+            load_tri_ell(M.U, h.fv.p, need32, h.s, fc.red);
+        } else {
+            for (TriDev *T : {&M.L, &M.U}) { T->ev64.free(); T->ev32.free(); T->evbf.free(); T->evh.free(); }
+        }
         load_dinv(h, h.fv.p, h.udiag_src.p, need32);
         M.ensure_buffers64(h.s);
         if (need32) M.ensure_buffers32(h.s);

@@ -60,6 +60,7 @@ int xs_plan_create(xs_plan_t *p, int n, const int *rp, const int *ci, const doub
         check_gpu();
         auto *w = new xs_plan_s;
         w->h.reset(new Handle());
+        w->h->all_factor_copies = true;
         try {
             set_matrix(*w->h, n, rp, ci, v, 0);
         } catch (...) {

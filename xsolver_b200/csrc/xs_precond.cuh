@@ -115,6 +115,7 @@ struct PrecondDev {
     template <typename VT, typename FT>
     void apply_exact(const VT *x, VT *z, const int *done_flag, cudaStream_t s)
     {
+        if (!L.vals<FT>() || !U.vals<FT>()) throw Status(XS_ERR_ORDER);  // copies not built for this configuration
         if (lu_block_ok<VT>(L, U)) {
             const VT *dinv;
             if constexpr (std::is_same<VT, double>::value) dinv = U.dinv64.p;
@@ -172,6 +173,7 @@ struct PrecondDev {
         auto pass = [&](const TriDev &T, bool upper, bool first2, const VT *rhs, const VT *yin, VT *yout) {
             if (T.ell_w > 0) {
                 const FT *ev = T.evals<FT>();
+                if (!ev) throw Status(XS_ERR_ORDER);  // copy not built for this configuration
                 const int *doff = T.doff.p;
                 // one wave of resident CTAs, grid-stride over the row blocks
                 const int rb = (n + 256 * ell_rows_for<FT>() - 1) / (256 * ell_rows_for<FT>());
@@ -192,6 +194,7 @@ struct PrecondDev {
                 else if (T.ell16) go((const short *)T.eco.p);
                 else go((const int *)T.eci.p);
             } else {
+                if (!natvals<FT>(T)) throw Status(XS_ERR_ORDER);  // copy not built for this configuration
                 // CSR: the first sweep is a separate pass (yin = null -> y_1)
                 if (first2) {
                     VT *tmp = tc;  // distinct from every buffer the stages read or write
@@ -212,6 +215,7 @@ struct PrecondDev {
         // few slots), further sweeps as single passes
         auto pass23 = [&](const TriDev &T, bool upper, const VT *rhs, VT *yout) {
             const FT *ev = T.evals<FT>();
+            if (!ev) throw Status(XS_ERR_ORDER);
             const int gs = std::max(1, std::min(g, (n + 255) / 256));
             const uint8_t *m = T.emask8.p;
             const int *doff = T.doff.p;

@@ -999,19 +999,26 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
 }
 
 // gather the ELL copy's values (FP64 always, reduced precisions on request)
-inline void load_tri_ell(TriDev &T, const double *vals, bool need32, cudaStream_t s)
+// red: reduced precisions built with need32 (bit 0 FP32, bit 1 BF16, bit 2 FP16)
+inline void load_tri_ell(TriDev &T, const double *vals, bool need32, cudaStream_t s, unsigned red = 7u)
 {
     if (T.ell_w == 0) return;
     const long m = (long)T.ell_w * ell_ld(T.n);
     const int g = geom().sms * 4;
     if (T.ev64.n != (size_t)m) T.ev64.alloc(m);
     k_gather_convert_pad<double><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.ev64.p);
-    if (need32) {
-        if (T.ev32.n != (size_t)m) { T.ev32.alloc(m); T.evbf.alloc(m); T.evh.alloc(m); }
-        k_gather_convert_pad<float><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.ev32.p);
-        k_gather_convert_pad<__nv_bfloat16><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.evbf.p);
-        k_gather_convert_pad<__half><<<g, 256, 0, s>>>(m, T.esrc.p, vals, T.evh.p);
-    }
+    auto one = [&](auto &buf, bool want) {
+        using FT = std::remove_pointer_t<decltype(buf.p)>;
+        if (!want) {
+            buf.free();
+            return;
+        }
+        if (buf.n != (size_t)m) buf.alloc(m);
+        k_gather_convert_pad<FT><<<g, 256, 0, s>>>(m, T.esrc.p, vals, buf.p);
+    };
+    one(T.ev32, need32 && (red & 1u));
+    one(T.evbf, need32 && (red & 2u));
+    one(T.evh, need32 && (red & 4u));
     check_launch();
 }
 
