@@ -196,7 +196,12 @@ __global__ void __launch_bounds__(256) k_csr_spmv_tiled(CsrTileArgs<MT> A, const
                         if (kb + j < k1) xv[j] = (double)__ldg(x + cc[kb + j]);
 #pragma unroll
                     for (int j = 0; j < CSR_CH; j++)
-                        if (kb + j < k1) sum += (double)vv[kb + j] * xv[j];
+                        if (kb + j < k1) {
+                            if constexpr (sizeof(MT) <= 4 && sizeof(VT) <= 4)
+                                sum = __fma_rn((double)vv[kb + j], xv[j], sum);  // exact product: same bits
+                            else
+                                sum += (double)vv[kb + j] * xv[j];
+                        }
                 }
                 VT o = epi.out(r, sum);
                 y[r] = o;
@@ -393,6 +398,20 @@ using EllAcc = typename std::conditional<XS_ELL_ACC32 && std::is_same<VT, float>
                                              std::is_same<MT, float>::value,
                                          float, double>::type;
 
+// sum + v * x in the accumulator type.  With FP64 sums of values and
+// vector entries of at most 4 bytes the FP64 product is exact (two mantissas
+// of <= 24 bits), so one fused multiply-add gives the bits of the multiply
+// followed by the add with one instruction fewer; FP64 operands keep the
+// separate multiply and add of the CPU order.
+template <typename AT, typename MT, typename VT>
+__device__ __forceinline__ AT ell_madd(AT sum, MT v, VT x)
+{
+    if constexpr (std::is_same<AT, double>::value && sizeof(MT) <= 4 && sizeof(VT) <= 4)
+        return __fma_rn((double)v, (double)x, sum);
+    else
+        return sum + (AT)v * (AT)x;
+}
+
 template <int C, int R, typename VT, typename MT, typename CT, typename AT>
 __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld, const VT *__restrict__ x, int r0,
                                           int n, int k0, const CT (&mask)[R], const int *s_off, AT (&sum)[R])
@@ -417,7 +436,7 @@ __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld,
         for (int j = 0; j < C; j++)
 #pragma unroll
             for (int q = 0; q < R; q++)
-                if ((mask[q] >> (k0 + j)) & 1u) sum[q] += (AT)v[j][q] * (AT)xv[j][q];
+                if ((mask[q] >> (k0 + j)) & 1u) sum[q] = ell_madd<AT>(sum[q], v[j][q], xv[j][q]);
     } else {
         CT c[C][R];
 #pragma unroll
@@ -435,7 +454,7 @@ __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld,
 #pragma unroll
         for (int j = 0; j < C; j++)
 #pragma unroll
-            for (int q = 0; q < R; q++) sum[q] += (AT)v[j][q] * (AT)xv[j][q];
+            for (int q = 0; q < R; q++) sum[q] = ell_madd<AT>(sum[q], v[j][q], xv[j][q]);
     }
 }
 
