@@ -119,11 +119,21 @@ __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int 
                 const unsigned d = (unsigned)(aci[q] - lo);
                 if (d < span) atomicOr(bm + (d >> 5), 1u << (d & 31));
             }
-            for (int q = l0; q < l1; q++) {
-                const int k = lci[q];
-                for (int t = urp[k] + lane; t < urp[k + 1]; t += 32) {
-                    const unsigned d = (unsigned)(uci[t] - lo);
-                    if (d < span) atomicOr(bm + (d >> 5), 1u << (d & 31));
+            // U row ranges of 32 L entries at a time, one per lane, by shuffle
+            for (int qb = l0; qb < l1; qb += 32) {
+                int mb = 0, me = 0;
+                if (qb + lane < l1) {
+                    const int k = lci[qb + lane];
+                    mb = urp[k];
+                    me = urp[k + 1];
+                }
+                const int cnt = min(32, l1 - qb);
+                for (int c = 0; c < cnt; c++) {
+                    const int t0 = __shfl_sync(0xffffffffu, mb, c), t1 = __shfl_sync(0xffffffffu, me, c);
+                    for (int t = t0 + lane; t < t1; t += 32) {
+                        const unsigned d = (unsigned)(uci[t] - lo);
+                        if (d < span) atomicOr(bm + (d >> 5), 1u << (d & 31));
+                    }
                 }
             }
             __syncwarp();
@@ -294,21 +304,32 @@ __global__ void __launch_bounds__(32 * PLT_CV_WARPS) k_candidate_values(
         if (!__any_sync(0xffffffffu, any_new)) continue;
         __syncwarp();
         const int l0 = lrp[i], l1 = lrp[i + 1];
-        for (int kq = l0; kq < l1; kq++) {
-            const int k = lci[kq];
-            const double lk = lv[kq];
-            const int e1 = urp[k + 1];
-            for (int e = urp[k] + lane; e < e1; e += 32) {
-                const int j = uci[e];
-                int lo = 0, hi = m;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (col[mid] < j) lo = mid + 1;
-                    else hi = mid;
-                }
-                if (lo < m && col[lo] == j && isnew[lo]) cc[lo] += lk * uv[e];
+        // L entries (value, U row range) 32 at a time, one per lane, by shuffle
+        for (int kb = l0; kb < l1; kb += 32) {
+            int mb = 0, me = 0;
+            double ml = 0.0;
+            if (kb + lane < l1) {
+                const int k = lci[kb + lane];
+                ml = lv[kb + lane];
+                mb = urp[k];
+                me = urp[k + 1];
             }
-            __syncwarp();
+            const int cnt = min(32, l1 - kb);
+            for (int cq = 0; cq < cnt; cq++) {
+                const double lk = __shfl_sync(0xffffffffu, ml, cq);
+                const int e0 = __shfl_sync(0xffffffffu, mb, cq), e1 = __shfl_sync(0xffffffffu, me, cq);
+                for (int e = e0 + lane; e < e1; e += 32) {
+                    const int j = uci[e];
+                    int lo = 0, hi = m;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (col[mid] < j) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    if (lo < m && col[lo] == j && isnew[lo]) cc[lo] += lk * uv[e];
+                }
+                __syncwarp();
+            }
         }
         for (int q = lane; q < m; q += 32) {
             if (!isnew[q]) continue;
@@ -398,6 +419,17 @@ __device__ __forceinline__ double plt_sweep_value(const int *arp, const int *aci
 // PLT_ROW_CAP fall back to the per-entry walk.
 constexpr int PLT_ROW_CAP = 256;
 constexpr int PLT_SW_WARPS = 4;
+// column -> pattern position of the row being swept: open addressing in
+// shared memory, key (column) and position packed in one 64-bit word, at most
+// half full (PLT_HASH >= 2 * PLT_ROW_CAP), linear probing; a lookup costs one
+// or two loads where a binary search over the sorted pattern costs eight
+constexpr int PLT_HASH = 512;
+constexpr unsigned long long PLT_HASH_EMPTY = ~0ull;
+__device__ __forceinline__ unsigned plt_hash_slot(int j)
+{
+    return ((unsigned)j * 2654435761u) >> (32 - 9);  // log2(PLT_HASH) = 9
+}
+static_assert(PLT_HASH == 512 && PLT_HASH >= 2 * PLT_ROW_CAP, "hash table size");
 
 __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
     int n, int parts, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
@@ -407,9 +439,11 @@ __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
 {
     __shared__ int s_col[PLT_SW_WARPS][PLT_ROW_CAP];
     __shared__ double s_t[PLT_SW_WARPS][PLT_ROW_CAP];
+    __shared__ unsigned long long s_h[PLT_SW_WARPS][PLT_HASH];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int *col = s_col[w];
     double *t = s_t[w];
+    unsigned long long *ht = s_h[w];
     for (int i = blockIdx.x * PLT_SW_WARPS + w; i < n; i += gridDim.x * PLT_SW_WARPS) {
         const int l0 = lrp[i], l1 = lrp[i + 1];
         // L row i: strict entries first (ascending), the unit diagonal (col i) last
@@ -432,34 +466,57 @@ __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
             }
             continue;
         }
+        for (int s2 = lane; s2 < PLT_HASH; s2 += 32) ht[s2] = PLT_HASH_EMPTY;
+        __syncwarp();
         for (int q = lane; q < m; q += 32) {
             const int j = q < nl ? lci[l0 + q] : uci[u0 + q - nl];
             col[q] = j;
             const int pa = find_pos(aci, arp[i], arp[i + 1], j);
             t[q] = pa >= 0 ? av[pa] : 0.0;
+            const unsigned long long kv = ((unsigned long long)(unsigned)j << 32) | (unsigned)q;
+            for (unsigned sl = plt_hash_slot(j);; sl = (sl + 1) & (PLT_HASH - 1))
+                if (atomicCAS(ht + sl, PLT_HASH_EMPTY, kv) == PLT_HASH_EMPTY) break;
         }
         __syncwarp();
         // only the products that reach a requested part: L part needs k < j < i
         // (every k of L row i may contribute); U part needs k < i
-        for (int kq = 0; kq < nl; kq++) {
-            const int k = lci[l0 + kq];
-            const double lk = lv_k[l0 + kq];
-            const int e1 = urp[k + 1];
-            for (int e = urp[k] + lane; e < e1; e += 32) {
-                const int j = uci[e];
-                if (j == k) continue;
-                if (!(parts & 2) && j >= i) continue;
-                if (!(parts & 1) && j < i) continue;
-                // binary search of j in the row's sorted pattern
-                int lo = 0, hi = m;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (col[mid] < j) lo = mid + 1;
-                    else hi = mid;
-                }
-                if (lo < m && col[lo] == j) t[lo] = t[lo] - lk * uv[e];
+        // the L entries' columns, values and U row ranges are loaded 32 at a
+        // time, one per lane, and handed out by shuffle: per L entry only the
+        // U row's own loads remain on the dependent path
+        for (int kb = 0; kb < nl; kb += 32) {
+            const int myq = kb + lane;
+            int mk = 0, mb = 0, me = 0;
+            double ml = 0.0;
+            if (myq < nl) {
+                mk = lci[l0 + myq];
+                ml = lv_k[l0 + myq];
+                mb = urp[mk];
+                me = urp[mk + 1];
             }
-            __syncwarp();
+            const int cnt = min(32, nl - kb);
+            for (int cq = 0; cq < cnt; cq++) {
+                const int k = __shfl_sync(0xffffffffu, mk, cq);
+                const double lk = __shfl_sync(0xffffffffu, ml, cq);
+                const int e0 = __shfl_sync(0xffffffffu, mb, cq), e1 = __shfl_sync(0xffffffffu, me, cq);
+                for (int e = e0 + lane; e < e1; e += 32) {
+                    const int j = uci[e];
+                    if (j == k) continue;
+                    if (!(parts & 2) && j >= i) continue;
+                    if (!(parts & 1) && j < i) continue;
+                    // position of j in the row's pattern (hash lookup)
+                    int pos = -1;
+                    for (unsigned sl = plt_hash_slot(j);; sl = (sl + 1) & (PLT_HASH - 1)) {
+                        const unsigned long long kv = ht[sl];
+                        if (kv == PLT_HASH_EMPTY) break;
+                        if ((int)(kv >> 32) == j) {
+                            pos = (int)(unsigned)kv;
+                            break;
+                        }
+                    }
+                    if (pos >= 0) t[pos] = t[pos] - lk * uv[e];
+                }
+                __syncwarp();
+            }
         }
         for (int q = lane; q < m; q += 32) {
             const int j = col[q];
