@@ -532,13 +532,14 @@ __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
 }
 
 // radix-select histogram: count |v| bit patterns whose bits above `shift+8`
-// equal `prefix`, binned by the 8 bits at `shift`
-__global__ void k_radix_hist(long m, const double *__restrict__ v, unsigned long long prefix, int shift,
+// equal the prefix selected so far (state[0]), binned by the 8 bits at `shift`
+__global__ void k_radix_hist(long m, const double *__restrict__ v, const unsigned long long *state, int shift,
                              unsigned long long *hist)
 {
     __shared__ unsigned int sh[256];
     for (int q = threadIdx.x; q < 256; q += blockDim.x) sh[q] = 0;
     __syncthreads();
+    const unsigned long long prefix = state[0];
     const int hi = shift + 8;
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < m; k += (long)gridDim.x * blockDim.x) {
         const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v[k]));
@@ -547,6 +548,23 @@ __global__ void k_radix_hist(long m, const double *__restrict__ v, unsigned long
     __syncthreads();
     for (int q = threadIdx.x; q < 256; q += blockDim.x)
         if (sh[q]) atomicAdd(hist + q, (unsigned long long)sh[q]);
+}
+
+// one thread: the bin holding the state[1]-th smallest pattern (1-based) of
+// this pass's histogram; state[0] = (state[0] << 8) | bin, state[1] -= the
+// counts of the bins below; the histogram is cleared for the next pass
+__global__ void k_radix_pick(unsigned long long *state, unsigned long long *hist)
+{
+    unsigned long long k = state[1];
+    int bin = 0;
+    for (; bin < 256; bin++) {
+        if (hist[bin] >= k) break;
+        k -= hist[bin];
+    }
+    if (bin == 256) bin = 255;
+    state[0] = (state[0] << 8) | (unsigned long long)bin;
+    state[1] = k;
+    for (int q = 0; q < 256; q++) hist[q] = 0;
 }
 
 // Threshold keep rule, one row of L (upper = 0: unit diagonal last, drop
@@ -789,24 +807,21 @@ inline long scan_counts(PltCtx &c, const DBuf<int> &cnt, DBuf<int> &rp)
 inline double plt_kth_abs(PltCtx &c, const DBuf<double> &v, long m, long k)
 {
     if (k <= 0 || m <= 0) return 0.0;
-    DBuf<unsigned long long> hist;
+    // the 8 passes run on the device (the bin of each pass picked by one
+    // thread); the host reads the selected pattern once
+    DBuf<unsigned long long> hist, state;
     hist.alloc(256);
-    unsigned long long prefix = 0;
-    std::vector<unsigned long long> h(256);
+    state.alloc(2);
+    const unsigned long long init[2] = {0ull, (unsigned long long)k};
+    state.upload(init, 2, c.s);
     for (int shift = 56; shift >= 0; shift -= 8) {
-        XS_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) * 256, c.s));
-        k_radix_hist<<<c.grid(), 256, 0, c.s>>>(m, v, prefix, shift, hist);
+        k_radix_hist<<<c.grid(), 256, 0, c.s>>>(m, v, state, shift, hist);
+        k_radix_pick<<<1, 1, 0, c.s>>>(state, hist);
         check_launch();
-        hist.download(h.data(), 256, c.s);
-        XS_CUDA(cudaStreamSynchronize(c.s));
-        int bin = 0;
-        for (; bin < 256; bin++) {
-            if ((long)h[bin] >= k) break;
-            k -= (long)h[bin];
-        }
-        if (bin == 256) bin = 255;
-        prefix = (prefix << 8) | (unsigned long long)bin;
     }
+    unsigned long long prefix = 0;
+    XS_CUDA(cudaMemcpyAsync(&prefix, state.p, sizeof(prefix), cudaMemcpyDeviceToHost, c.s));
+    XS_CUDA(cudaStreamSynchronize(c.s));
     double out;
     std::memcpy(&out, &prefix, sizeof(double));
     return out;
