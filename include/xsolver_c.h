@@ -206,6 +206,14 @@ void gpu_cg_solve(double *rhs, double *sol, double *tol, int *maxiter, double *s
 void gpu_cgm_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter, double *resvec);
 void gpu_bicgstab_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter,
                         double *resvec);
+/* The single-reduction CG variants of the reference's CPU path, on the GPU
+ * with the configured preconditioner: intel/mpisolver-C-v1.cpp:104 (icg,
+ * CG on M^-1 A with tao from a recurrence) and :273 (icgm, PCG with the five
+ * dot products of an iteration taken together); same arguments and
+ * conventions as gpu_cg_solve.  Handles select them with
+ * xs_ksp_settype(h, "icg" / "icgm"). */
+void gpu_icg_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter, double *resvec);
+void gpu_icgm_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter, double *resvec);
 /* cuda/mpicudasolver-C-v1.cu:939 / :1074 / :1221 / :1391 */
 void gpu_gcr_solve(double *rhs, double *sol, int *restart, double *tol, int *maxiter, double *sol_init, int *usediter,
                    double *resvec);

@@ -846,6 +846,107 @@ int orc_cg(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, co
     return written;
 }
 
+/* intel/mpisolver-C-v1.cpp:104-191 ("icg": left-preconditioned CG with the
+ * three dot products of an iteration taken together; tao from the
+ * recurrence taoo - 2 alpha rho + alpha^2 theta instead of r.r) */
+int orc_icg(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
+            int *usediter, double *resvec)
+{
+    ORC_CTX;
+    std::vector<double> pk(n), phi(n), res(n), Apk(n), qk(n);
+    double sigma, alpha, minalpha, taoo, tao, resl, rsm, beta, rho, theta;
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    M.apply(res.data(), res.data());
+    double res0 = o_dot(n, res.data(), res.data());
+    o_copy(n, res.data(), pk.data());
+    taoo = res0;
+    res0 = std::sqrt(res0);
+    for (int iiter = 0; iiter < maxiter; iiter++) {
+        *usediter = iiter;
+        A.spmv(pk.data(), Apk.data());
+        M.apply(Apk.data(), qk.data());
+        sigma = o_dot(n, pk.data(), qk.data());
+        rho = o_dot(n, res.data(), qk.data());
+        theta = o_dot(n, qk.data(), qk.data());
+        alpha = taoo / (sigma + small);
+        minalpha = minone * alpha;
+        o_axpy(n, alpha, pk.data(), phi.data());
+        o_axpy(n, minalpha, qk.data(), res.data());
+        resl = o_dot(n, res.data(), res.data());
+        resl = std::sqrt(resl);
+        rsm = resl / (res0 + small);
+        if (resvec) resvec[iiter] = rsm;
+        written = iiter + 1;
+        if (rsm < tol) {
+            *usediter = iiter;
+            o_copy(n, phi.data(), sol);
+            return written;
+        }
+        tao = taoo - 2.0 * alpha * rho + alpha * alpha * theta;
+        beta = tao / (taoo + small);
+        taoo = tao;
+        o_scal(n, beta, pk.data());
+        o_axpy(n, one, res.data(), pk.data());
+    }
+    o_copy(n, phi.data(), sol);
+    return written;
+}
+
+/* intel/mpisolver-C-v1.cpp:273-363 ("icgm": PCG with the five dot products
+ * of an iteration taken together before the update; the convergence test
+ * uses the residual from before the update, tau from the recurrence
+ * tau - alpha phi - alpha rho + alpha^2 theta) */
+int orc_icgm(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
+             int *usediter, double *resvec)
+{
+    ORC_CTX;
+    std::vector<double> pk(n), phi(n), zk(n), res(n), Apk(n), qk(n);
+    double sigma, alpha, minalpha, tauo, tau, resl, rsm, beta, rho, theta, fai;
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    M.apply(res.data(), zk.data());
+    double res0 = o_dot(n, res.data(), res.data());
+    tau = o_dot(n, res.data(), zk.data());
+    o_copy(n, zk.data(), pk.data());
+    res0 = std::sqrt(res0);
+    for (int iiter = 0; iiter < maxiter; iiter++) {
+        *usediter = iiter;
+        A.spmv(pk.data(), Apk.data());
+        M.apply(Apk.data(), qk.data());
+        sigma = o_dot(n, pk.data(), Apk.data());
+        rho = o_dot(n, res.data(), qk.data());
+        fai = o_dot(n, Apk.data(), zk.data());
+        theta = o_dot(n, qk.data(), Apk.data());
+        resl = o_dot(n, res.data(), res.data());
+        alpha = tau / (sigma + small);
+        minalpha = minone * alpha;
+        o_axpy(n, alpha, pk.data(), phi.data());
+        o_axpy(n, minalpha, Apk.data(), res.data());
+        M.apply(res.data(), zk.data());
+        tauo = tau;
+        tau = tau - alpha * fai - alpha * rho + alpha * alpha * theta;
+        beta = tau / (tauo + small);
+        o_scal(n, beta, pk.data());
+        o_axpy(n, one, zk.data(), pk.data());
+        resl = std::sqrt(resl);
+        rsm = resl / (res0 + small);
+        if (resvec) resvec[iiter] = rsm;
+        written = iiter + 1;
+        if (rsm < tol) {
+            *usediter = iiter;
+            o_copy(n, phi.data(), sol);
+            return written;
+        }
+    }
+    o_copy(n, phi.data(), sol);
+    return written;
+}
+
 /* intel/mpisolver-C-v1.cpp:193-272 (standard PCG, "cgm") */
 int orc_cgm(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
             int *usediter, double *resvec)

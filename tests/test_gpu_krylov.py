@@ -60,7 +60,7 @@ def _gpu_solve_intel(method, A, b, tol, maxiter, restart, pc="Jacobi"):
     resvec = np.zeros(maxiter + 2)
     used = C.c_int(-1)
     t, mi, rs = C.c_double(tol), C.c_int(maxiter), C.c_int(restart)
-    if method in ("cg", "cgm", "bicgstab"):
+    if method in ("cg", "cgm", "icg", "icgm", "bicgstab"):
         getattr(L, f"gpu_{method}_solve")(rhs.ctypes.data_as(dp), x.ctypes.data_as(dp), C.byref(t), C.byref(mi),
                                           x0.ctypes.data_as(dp), C.byref(used), resvec.ctypes.data_as(dp))
     else:
@@ -97,6 +97,36 @@ def test_gpu_api_vs_reference_golden(cuda, method):
         assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < xb, nm
         done += 1
     assert done >= 1
+
+
+@pytest.mark.parametrize("method", ["icg", "icgm"])
+def test_single_reduction_cg_vs_oracle(cuda, method):
+    """icg / icgm (intel/mpisolver-C-v1.cpp:104-191, 273-363; the restatement
+    is pinned bitwise to the compiled reference in test_oracle_pinned.py)
+    through gpu_*_solve with Jacobi, and through a handle with ILU(0).  Their
+    tau recurrences lose accuracy once the residual is small (the reference
+    stalls near 1e-7 and then diverges), so the tolerance is 1e-6."""
+    for A in (st.poisson2d_5pt(24), st.varcoef3d_7pt(10, 3)):
+        b = st.rhs_uniform(A.n, 5)
+        x, rv, used, code = _gpu_solve_intel(method, A, b, 1e-6, 400, 0)
+        assert code == 0
+        xo, ho, uo, hb, xb = reference_with_bounds(method, A, b, tol=1e-6, maxiter=400, pc="jacobi")
+        assert uo < 399, "the reference itself must converge"
+        assert abs(used - uo) <= 1, (A.name, used, uo)
+        ok, worst = history_ok(rv[: used + 1], ho, hb)
+        assert ok, (A.name, worst)
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb, A.name
+    A = st.poisson3d_7pt(24)
+    b = st.rhs_uniform(A.n, 6)
+    S = _solver(A, method, "ilu0", 1e-6, 400)
+    x = S.solve(b)
+    hist = S.resvec()
+    xo, ho, uo, hb, xb = reference_with_bounds(method, A, b, tol=1e-6, maxiter=400, pc="lu", factors=oracle.ilu0(A))
+    assert uo < 399
+    assert abs(S.usediter - (uo + 1)) <= 1, (S.usediter, uo)
+    ok, worst = history_ok(hist[1:] / hist[0], ho, hb)
+    assert ok, worst
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
 
 
 def _solver(A, ksp, pc, tol, maxiter, restart=0, fmt="csr"):

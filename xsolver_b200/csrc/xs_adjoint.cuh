@@ -20,6 +20,8 @@ template <typename VT>
 struct RunSet {
     PcgRun<VT, VT> pcg;
     CgLeftRun<VT, VT> cgl;
+    IcgRun<VT, VT> icg;
+    IcgmRun<VT, VT> icgm;
     BicgRun<VT, VT> bicg;
     GmresRun<VT, VT> gmres;
     GcrRun<VT, VT> gcr;

@@ -804,6 +804,8 @@ static void run_method_on(RunSet<VT> &R, Operator &A, PrecondDev &M, Workspace &
     switch (method) {
     case KSP_CGM: R.pcg.run(c, b, x); break;
     case KSP_CG_LEFT: R.cgl.run(c, b, x); break;
+    case KSP_ICG: R.icg.run(c, b, x); break;
+    case KSP_ICGM: R.icgm.run(c, b, x); break;
     case KSP_BICGSTAB: R.bicg.run(c, b, x); break;
     case KSP_GMRES_LEFT:
     case KSP_GMRES_RIGHT: R.gmres.run(c, b, x, restart, method == KSP_GMRES_RIGHT); break;
@@ -1268,6 +1270,8 @@ static int parse_ksp(const char *fmt, bool intel)
     if (ieq(fmt, "bicgstab")) return KSP_BICGSTAB;
     if (ieq(fmt, "cg")) return intel ? KSP_CG_LEFT : KSP_CGM;
     if (ieq(fmt, "cgm") || ieq(fmt, "pcg")) return KSP_CGM;
+    if (ieq(fmt, "icg")) return KSP_ICG;
+    if (ieq(fmt, "icgm")) return KSP_ICGM;
     if (ieq(fmt, "igcr")) return intel ? KSP_IGCR_LEFT : KSP_GCR_RIGHT;
     if (ieq(fmt, "gcr")) return intel ? KSP_GCR_LEFT : KSP_GCR_RIGHT;
     if (ieq(fmt, "gmres")) return intel ? KSP_GMRES_LEFT : KSP_GMRES_RIGHT;
@@ -1992,6 +1996,8 @@ static void gpu_solve_common(int method, double *rhs, double *sol, int restart, 
 
 GPU_SOLVE_1(gpu_cg_solve, KSP_CG_LEFT)
 GPU_SOLVE_1(gpu_cgm_solve, KSP_CGM)
+GPU_SOLVE_1(gpu_icg_solve, KSP_ICG)
+GPU_SOLVE_1(gpu_icgm_solve, KSP_ICGM)
 GPU_SOLVE_1(gpu_bicgstab_solve, KSP_BICGSTAB)
 GPU_SOLVE_2(gpu_gcr_solve, KSP_GCR_LEFT)
 GPU_SOLVE_2(gpu_igcr_solve, KSP_IGCR_LEFT)

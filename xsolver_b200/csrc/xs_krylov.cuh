@@ -377,6 +377,137 @@ struct OpCgP {  // p = beta*p + r
     __device__ void finalize(const double *) const {}
 };
 
+// ---- single-reduction CG variants (intel/mpisolver-C-v1.cpp:104-191 icg,
+// :273-363 icgm): every dot product of an iteration is taken in one pass
+
+// icg: sigma = p.q, rho = r.q, theta = q.q (q = M^-1 A p); then
+// alpha = taoo/(sigma+small), tao = taoo - 2 alpha rho + alpha^2 theta,
+// beta = tao/(taoo+small) (the reference computes tao and beta after its
+// convergence test; they do not depend on it)
+template <typename VT>
+struct OpIcgDots {
+    static constexpr int K = 3;
+    int n;
+    KState *st;
+    const VT *p, *r, *q;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[3]) const
+    {
+        const double qi = (double)q[i];
+        a[0] += (double)p[i] * qi;
+        a[1] += (double)r[i] * qi;
+        a[2] += qi * qi;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        const double sigma = t[0], rho = t[1], theta = t[2];
+        const double taoo = st->sc[S_TAOO];
+        const double alpha = taoo / (sigma + KSMALL);
+        const double tao = taoo - 2.0 * alpha * rho + alpha * alpha * theta;
+        st->sc[S_SIGMA] = sigma;
+        st->sc[S_ALPHA] = alpha;
+        st->sc[S_TAO] = tao;
+        st->sc[S_BETA] = tao / (taoo + KSMALL);
+        if (!isfinite(sigma) || !isfinite(rho) || !isfinite(theta)) {
+            st->err |= DEV_BREAKDOWN;
+            st->done = 3;
+        }
+    }
+};
+// icg: x += alpha p ; r -= alpha q ; p = beta p + r (new r) ; acc r.r, the
+// convergence test; taoo = tao while the iteration continues
+template <typename VT>
+struct OpIcgUpdate {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    VT *x, *r, *p;
+    const VT *q;
+    VT alpha, beta;
+    __device__ void load()
+    {
+        alpha = (VT)st->sc[S_ALPHA];
+        beta = (VT)st->sc[S_BETA];
+    }
+    __device__ void elem(int i, double (&a)[1]) const
+    {
+        const VT minalpha = -alpha;
+        const VT pi = p[i];
+        x[i] = x[i] + alpha * pi;
+        const VT ri = r[i] + minalpha * q[i];
+        r[i] = ri;
+        const VT t = beta * pi;
+        p[i] = t + ri;
+        a[0] += (double)ri * (double)ri;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        if (!record_and_test(st, sqrt(t[0]))) return;
+        st->sc[S_TAOO] = st->sc[S_TAO];
+    }
+};
+
+// icgm: sigma = p.Ap, rho = r.q, fai = Ap.z, theta = q.Ap and r.r (the
+// residual before this iteration's update, which the reference tests at the
+// end of the iteration); alpha = tau/(sigma+small),
+// tau' = tau - alpha fai - alpha rho + alpha^2 theta, beta = tau'/(tau+small)
+template <typename VT>
+struct OpIcgmDots {
+    static constexpr int K = 5;
+    int n;
+    KState *st;
+    const VT *p, *r, *q, *Ap, *z;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[5]) const
+    {
+        const double api = (double)Ap[i], qi = (double)q[i], ri = (double)r[i];
+        a[0] += (double)p[i] * api;
+        a[1] += ri * qi;
+        a[2] += api * (double)z[i];
+        a[3] += qi * api;
+        a[4] += ri * ri;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        const double sigma = t[0], rho = t[1], fai = t[2], theta = t[3];
+        const double tauo = st->sc[S_TAO];
+        const double alpha = tauo / (sigma + KSMALL);
+        const double tau = tauo - alpha * fai - alpha * rho + alpha * alpha * theta;
+        st->sc[S_SIGMA] = sigma;
+        st->sc[S_ALPHA] = alpha;
+        st->sc[S_TAO] = tau;
+        st->sc[S_BETA] = tau / (tauo + KSMALL);
+        st->sc[S_T0] = t[4];
+        bool ok = true;
+        for (int k = 0; k < 5; k++) ok = ok && isfinite(t[k]);
+        if (!ok) {
+            st->err |= DEV_BREAKDOWN;
+            st->done = 3;
+        }
+    }
+};
+// icgm: x += alpha p ; r -= alpha Ap ; then the convergence test on the
+// residual norm taken before the update (the reference tests after z and p
+// are updated; those updates do not change x, so a converged solve may skip
+// them)
+template <typename VT>
+struct OpIcgmUpdate {
+    static constexpr int K = 1;  // no sum; K = 1 for the finalize step
+    int n;
+    KState *st;
+    VT *x, *r;
+    const VT *p, *Ap;
+    VT alpha;
+    __device__ void load() { alpha = (VT)st->sc[S_ALPHA]; }
+    __device__ void elem(int i, double (&)[1]) const
+    {
+        const VT minalpha = -alpha;
+        x[i] = x[i] + alpha * p[i];
+        r[i] = r[i] + minalpha * Ap[i];
+    }
+    __device__ void finalize(const double *) const { record_and_test(st, sqrt(st->sc[S_T0])); }
+};
+
 // ---- BiCGSTAB
 // init: rhat = r ; acc r.r ; then beta = r.rhat = r.r, omega, beto
 template <typename VT>

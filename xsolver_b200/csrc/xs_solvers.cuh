@@ -15,7 +15,9 @@ enum Method {
     KSP_IGCR_LEFT = 5, // intel cpu_igcr_solve (modified GS)
     KSP_GCR_RIGHT = 6, // hip Xsolver_igcr (right preconditioned, MGS)
     KSP_GMRES_LEFT = 7,
-    KSP_GMRES_RIGHT = 8
+    KSP_GMRES_RIGHT = 8,
+    KSP_ICG = 9,       // intel cpu_icg_solve (single-reduction CG on M^-1 A)
+    KSP_ICGM = 10      // intel cpu_icgm_solve (single-reduction PCG)
 };
 
 // vectors owned by a solve, cached across solves of the same size
@@ -199,6 +201,64 @@ struct CgLeftRun {
             vecop(OpCgP<VT>{n, st, p, r, (VT)0}, sl, c.s);
         };
         std::vector<const void *> key{b, x, r, q, p, Ap, st, c.M, c.A, (const void *)cfg_key(c)};
+        run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
+    }
+};
+
+// ---------------------------------------------------------------- single-reduction CG
+// intel/mpisolver-C-v1.cpp:104-191: the initial sequence of CgLeftRun, then
+// per iteration SpMV, apply, one pass for the three dot products, one pass
+// for the x, r and p updates with the convergence test
+template <typename VT, typename MT>
+struct IcgRun {
+    VecPool<VT> pool;
+    GraphCache gc;
+    void run(SolveCtx &c, const VT *b, VT *x)
+    {
+        const int n = c.n;
+        VT *r = pool.get(0, n), *q = pool.get(1, n), *p = pool.get(2, n), *Ap = pool.get(3, n);
+        KState *st = c.W->st.p;
+        RedSlot sl = c.W->slot();
+        const int *done = &st->done;
+        spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
+        c.M->apply<VT>(r, r, done, c.s);
+        vecop(OpCgInit<VT>{n, st, r, p}, sl, c.s);
+        auto body = [&]() {
+            spmv<VT, MT>(*c.A, p, Ap, EpiActive<VT>{st}, sl, c.s);
+            c.M->apply<VT>(Ap, q, done, c.s);
+            vecop(OpIcgDots<VT>{n, st, p, r, q}, sl, c.s);
+            vecop(OpIcgUpdate<VT>{n, st, x, r, p, q, (VT)0, (VT)0}, sl, c.s);
+        };
+        std::vector<const void *> key{b, x, r, q, p, Ap, st, c.M, c.A, (const void *)cfg_key(c)};
+        run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
+    }
+};
+// intel/mpisolver-C-v1.cpp:273-363: the initial sequence of PcgRun, then per
+// iteration SpMV, apply, one pass for the five dot products, the x and r
+// updates with the convergence test, apply, p update
+template <typename VT, typename MT>
+struct IcgmRun {
+    VecPool<VT> pool;
+    GraphCache gc;
+    void run(SolveCtx &c, const VT *b, VT *x)
+    {
+        const int n = c.n;
+        VT *r = pool.get(0, n), *z = pool.get(1, n), *p = pool.get(2, n), *Ap = pool.get(3, n), *q = pool.get(4, n);
+        KState *st = c.W->st.p;
+        RedSlot sl = c.W->slot();
+        const int *done = &st->done;
+        spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
+        c.M->apply<VT>(r, z, done, c.s);
+        vecop(OpCgmInit<VT>{n, st, r, z, p}, sl, c.s);
+        auto body = [&]() {
+            spmv<VT, MT>(*c.A, p, Ap, EpiActive<VT>{st}, sl, c.s);
+            c.M->apply<VT>(Ap, q, done, c.s);
+            vecop(OpIcgmDots<VT>{n, st, p, r, q, Ap, z}, sl, c.s);
+            vecop(OpIcgmUpdate<VT>{n, st, x, r, p, Ap, (VT)0}, sl, c.s);
+            c.M->apply<VT>(r, z, done, c.s);
+            vecop(OpCgP<VT>{n, st, p, z, (VT)0}, sl, c.s);
+        };
+        std::vector<const void *> key{b, x, r, z, p, Ap, q, st, c.M, c.A, (const void *)cfg_key(c)};
         run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
     }
 };
