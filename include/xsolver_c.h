@@ -214,6 +214,11 @@ void gpu_bicgstab_solve(double *rhs, double *sol, double *tol, int *maxiter, dou
  * xs_ksp_settype(h, "icg" / "icgm"). */
 void gpu_icg_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter, double *resvec);
 void gpu_icgm_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter, double *resvec);
+/* intel/mpisolver-C-v1.cpp:484 (ibicgstab: right-preconditioned BiCGSTAB
+ * with the six dot products of an iteration taken together); arguments as
+ * gpu_cg_solve; handles: xs_ksp_settype(h, "ibicgstab"). */
+void gpu_ibicgstab_solve(double *rhs, double *sol, double *tol, int *maxiter, double *sol_init, int *usediter,
+                         double *resvec);
 /* cuda/mpicudasolver-C-v1.cu:939 / :1074 / :1221 / :1391 */
 void gpu_gcr_solve(double *rhs, double *sol, int *restart, double *tol, int *maxiter, double *sol_init, int *usediter,
                    double *resvec);

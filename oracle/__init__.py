@@ -231,8 +231,8 @@ def set_dot_mode(mode: str):
 
 def solve(method, A, rhs, x0=None, tol=1e-8, maxiter=1000, restart=30, pc="jacobi", factors: LU | None = None,
           quirk=1):
-    """Run a restated Krylov loop.  method: cg, cgm, icg, icgm, bicgstab, gcr,
-    igcr, hip_igcr, gmres, fgmres.  pc: none / jacobi / lu (needs factors).
+    """Run a restated Krylov loop.  method: cg, cgm, icg, icgm, bicgstab,
+    ibicgstab, gcr, igcr, hip_igcr, gmres, fgmres.  pc: none / jacobi / lu (needs factors).
 
     Returns (x, resvec, usediter).  resvec follows the restated loop's own
     convention: intel loops give relative residuals indexed by iteration;
@@ -247,8 +247,9 @@ def solve(method, A, rhs, x0=None, tol=1e-8, maxiter=1000, restart=30, pc="jacob
     fargs = factors.args() if (kind == 2) else (None,) * 7
     common = (n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), kind, *fargs)
     L = lib()
-    if method in ("cg", "cgm", "icg", "icgm", "bicgstab"):
-        f = {"cg": L.orc_cg, "cgm": L.orc_cgm, "icg": L.orc_icg, "icgm": L.orc_icgm, "bicgstab": L.orc_bicgstab}[method]
+    if method in ("cg", "cgm", "icg", "icgm", "bicgstab", "ibicgstab"):
+        f = {"cg": L.orc_cg, "cgm": L.orc_cgm, "icg": L.orc_icg, "icgm": L.orc_icgm, "bicgstab": L.orc_bicgstab,
+             "ibicgstab": L.orc_ibicgstab}[method]
         w = f(*common, _p(rhs), _p(x), C.c_double(tol), C.c_int(maxiter), _p(x0c), C.byref(used), _p(resvec))
     elif method in ("gcr", "igcr"):
         w = L.orc_gcr(*common, _p(rhs), _p(x), C.c_int(restart), C.c_double(tol), C.c_int(maxiter), _p(x0c),
@@ -290,9 +291,9 @@ def ref_solve(method, A, rhs, x0=None, tol=1e-8, maxiter=1000, restart=30):
     resvec = np.zeros(maxiter + 2)
     used = C.c_int(-1)
     t, mi, rs = C.c_double(tol), C.c_int(maxiter), C.c_int(restart)
-    if method in ("cg", "cgm", "icg", "icgm", "bicgstab"):
+    if method in ("cg", "cgm", "icg", "icgm", "bicgstab", "ibicgstab"):
         f = {"cg": R.cpu_cg_solve, "cgm": R.cpu_cgm_solve, "icg": R.cpu_icg_solve, "icgm": R.cpu_icgm_solve,
-             "bicgstab": R.cpu_bicgstab_solve}[method]
+             "bicgstab": R.cpu_bicgstab_solve, "ibicgstab": R.cpu_ibicgstab_solve}[method]
         f(_p(rhs), _p(x), C.byref(t), C.byref(mi), _p(x0c), C.byref(used), _p(resvec))
     else:
         f = {"gcr": R.cpu_gcr_solve, "igcr": R.cpu_igcr_solve, "gmres": R.cpu_gmres_solve,

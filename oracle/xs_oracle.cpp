@@ -947,6 +947,98 @@ int orc_icgm(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, 
     return written;
 }
 
+/* intel/mpisolver-C-v1.cpp:484-683 ("ibicgstab": right-preconditioned
+ * BiCGSTAB with the six dot products of an iteration taken together; the
+ * iterate phi lives in the preconditioned space and the solution is M^-1 phi;
+ * the start-up uses A M^-1 A phi when phi != 0, which gives the same values
+ * as the phi == 0 branch when phi is zero, so only that form is restated) */
+int orc_ibicgstab(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
+                  int *usediter, double *resvec)
+{
+    ORC_CTX;
+    std::vector<double> resm(n), phi(n), res(n), tk(n), pk(n), qk(n), zk(n), vk(n), vko(n), sk(n), reso(n);
+    double pi, tau, fai, sigma, alpha, minalpha, alphao, rou, rouo, omega, minomega;
+    double beta, delta, mindelta, theta, kappa, mu, nu;
+    double resl, rsm, tmp1, tmp2, mintmp2;
+    double small = 1e-20, one = 1.0, minone = -1.0;
+    int written = 0;
+    o_copy(n, sol_init ? sol_init : sol, phi.data());
+    A.bmax(rhs, phi.data(), res.data());
+    double res0 = o_dot(n, res.data(), res.data());
+    res0 = std::sqrt(res0);
+    o_copy(n, res.data(), reso.data());
+    std::fill(qk.begin(), qk.end(), 0.0);
+    std::fill(vk.begin(), vk.end(), 0.0);
+    std::fill(zk.begin(), zk.end(), 0.0);
+    alpha = 1.0; alphao = 1.0; rou = 1.0; rouo = 1.0; omega = 1.0; pi = 0.0; tau = 0.0; mu = 0.0;
+    // pk = A M^-1 A phi ; tk = A M^-1 res + pk
+    A.spmv(phi.data(), pk.data());
+    M.apply(pk.data(), resm.data());
+    A.spmv(resm.data(), pk.data());
+    M.apply(res.data(), resm.data());
+    A.spmv(resm.data(), tk.data());
+    o_axpy(n, one, pk.data(), tk.data());
+    fai = o_dot(n, res.data(), res.data());
+    sigma = o_dot(n, res.data(), tk.data());
+    for (int iiter = 0; iiter < maxiter; iiter++) {
+        *usediter = iiter;
+        rouo = rou;
+        rou = fai - omega * mu;
+        delta = (rou * alpha) / (rouo + small);
+        beta = delta / (omega + small);
+        tau = sigma + beta * tau - delta * pi;
+        alphao = alpha;
+        alpha = rou / (tau + small);
+        o_copy(n, vk.data(), vko.data());
+        o_copy(n, tk.data(), vk.data());
+        minomega = minone * omega;
+        o_axpy(n, minomega, pk.data(), vk.data());
+        o_axpy(n, beta, vko.data(), vk.data());
+        mindelta = minone * delta;
+        o_axpy(n, mindelta, qk.data(), vk.data());
+        M.apply(vk.data(), resm.data());
+        A.spmv(resm.data(), qk.data());
+        o_copy(n, res.data(), sk.data());
+        minalpha = minone * alpha;
+        o_axpy(n, minalpha, vk.data(), sk.data());
+        o_axpy(n, minomega, pk.data(), tk.data());
+        o_axpy(n, minalpha, qk.data(), tk.data());
+        tmp1 = (beta * alpha) / (alphao + small);
+        tmp2 = alpha * delta;
+        mintmp2 = minone * tmp2;
+        o_scal(n, tmp1, zk.data());
+        o_axpy(n, alpha, res.data(), zk.data());
+        o_axpy(n, mintmp2, vko.data(), zk.data());
+        M.apply(tk.data(), resm.data());
+        A.spmv(resm.data(), pk.data());
+        fai = o_dot(n, reso.data(), sk.data());
+        pi = o_dot(n, reso.data(), qk.data());
+        theta = o_dot(n, sk.data(), tk.data());
+        kappa = o_dot(n, tk.data(), tk.data());
+        mu = o_dot(n, reso.data(), tk.data());
+        nu = o_dot(n, reso.data(), pk.data());
+        omega = theta / (kappa + small);
+        sigma = mu - omega * nu;
+        o_copy(n, sk.data(), res.data());
+        minomega = minone * omega;
+        o_axpy(n, minomega, tk.data(), res.data());
+        o_axpy(n, one, zk.data(), phi.data());
+        o_axpy(n, omega, sk.data(), phi.data());
+        resl = o_dot(n, res.data(), res.data());
+        resl = std::sqrt(resl);
+        rsm = resl / (res0 + small);
+        if (resvec) resvec[iiter] = rsm;
+        written = iiter + 1;
+        if (rsm < tol) {
+            *usediter = iiter;
+            M.apply(phi.data(), sol);
+            return written;
+        }
+    }
+    M.apply(phi.data(), sol);
+    return written;
+}
+
 /* intel/mpisolver-C-v1.cpp:193-272 (standard PCG, "cgm") */
 int orc_cgm(ORC_ARGS, const double *rhs, double *sol, double tol, int maxiter, const double *sol_init,
             int *usediter, double *resvec)

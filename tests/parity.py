@@ -68,3 +68,23 @@ def history_ok(h_gpu, h_ref, hbound, scale=1.0):
     b = hbound[:m] if len(hbound) >= m else np.concatenate([hbound, np.full(m - len(hbound), hbound[-1])])
     r = np.where(mask, d / b, 0.0)
     return bool(np.all(r <= 1.0)), float(r.max() if m else 0.0)
+
+
+def iteration_range(method, A, b, **kw):
+    """(min, max) of the reference's iteration count over the sequential and
+    the alternative dot orders: the count a solve may end at when only its
+    summation order changes."""
+    counts = []
+    try:
+        for mode in ("sequential",) + ALT_ORDERS:
+            oracle.set_dot_mode(mode)
+            counts.append(oracle.solve(method, A, b, **kw)[2])
+    finally:
+        oracle.set_dot_mode("sequential")
+    return min(counts), max(counts)
+
+
+def count_ok(used, u_seq, urange):
+    """Iteration count within +-1 of the sequential reference, or within the
+    range the reference itself spans over the dot orders (+-1)."""
+    return abs(used - u_seq) <= 1 or urange[0] - 1 <= used <= urange[1] + 1

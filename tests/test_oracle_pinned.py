@@ -67,7 +67,7 @@ def test_ilu0_restatement_bitwise_vs_golden():
 
 
 @pytest.mark.skipif(oracle.ref_intel() is None, reason="compiled reference not present")
-@pytest.mark.parametrize("method", ["cg", "cgm", "icg", "icgm", "bicgstab", "gcr", "igcr", "gmres", "fgmres"])
+@pytest.mark.parametrize("method", ["cg", "cgm", "icg", "icgm", "bicgstab", "ibicgstab", "gcr", "igcr", "gmres", "fgmres"])
 def test_krylov_restatement_bitwise_vs_compiled_reference(method):
     A = st.poisson2d_5pt(20)
     b = st.rhs_uniform(A.n, 11)

@@ -150,7 +150,8 @@ def _declare(L):
     for name in ("gpu_preconditioner_setup", "gpu_preconditioner_update", "gpu_preconditioner_free"):
         getattr(L, name).argtypes = [C.c_char_p]
         getattr(L, name).restype = None
-    for name in ("gpu_cg_solve", "gpu_cgm_solve", "gpu_icg_solve", "gpu_icgm_solve", "gpu_bicgstab_solve"):
+    for name in ("gpu_cg_solve", "gpu_cgm_solve", "gpu_icg_solve", "gpu_icgm_solve", "gpu_bicgstab_solve",
+                 "gpu_ibicgstab_solve"):
         getattr(L, name).argtypes = [_dp, _dp, _dp, _ip, _dp, _ip, _dp]
         getattr(L, name).restype = None
     for name in ("gpu_gcr_solve", "gpu_igcr_solve", "gpu_gmres_solve", "gpu_fgmres_solve"):

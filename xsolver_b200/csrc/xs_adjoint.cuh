@@ -22,6 +22,7 @@ struct RunSet {
     CgLeftRun<VT, VT> cgl;
     IcgRun<VT, VT> icg;
     IcgmRun<VT, VT> icgm;
+    IbicgRun<VT, VT> ibicg;
     BicgRun<VT, VT> bicg;
     GmresRun<VT, VT> gmres;
     GcrRun<VT, VT> gcr;

@@ -806,6 +806,7 @@ static void run_method_on(RunSet<VT> &R, Operator &A, PrecondDev &M, Workspace &
     case KSP_CG_LEFT: R.cgl.run(c, b, x); break;
     case KSP_ICG: R.icg.run(c, b, x); break;
     case KSP_ICGM: R.icgm.run(c, b, x); break;
+    case KSP_IBICGSTAB: R.ibicg.run(c, b, x); break;
     case KSP_BICGSTAB: R.bicg.run(c, b, x); break;
     case KSP_GMRES_LEFT:
     case KSP_GMRES_RIGHT: R.gmres.run(c, b, x, restart, method == KSP_GMRES_RIGHT); break;
@@ -1272,6 +1273,7 @@ static int parse_ksp(const char *fmt, bool intel)
     if (ieq(fmt, "cgm") || ieq(fmt, "pcg")) return KSP_CGM;
     if (ieq(fmt, "icg")) return KSP_ICG;
     if (ieq(fmt, "icgm")) return KSP_ICGM;
+    if (ieq(fmt, "ibicgstab")) return KSP_IBICGSTAB;
     if (ieq(fmt, "igcr")) return intel ? KSP_IGCR_LEFT : KSP_GCR_RIGHT;
     if (ieq(fmt, "gcr")) return intel ? KSP_GCR_LEFT : KSP_GCR_RIGHT;
     if (ieq(fmt, "gmres")) return intel ? KSP_GMRES_LEFT : KSP_GMRES_RIGHT;
@@ -1998,6 +2000,7 @@ GPU_SOLVE_1(gpu_cg_solve, KSP_CG_LEFT)
 GPU_SOLVE_1(gpu_cgm_solve, KSP_CGM)
 GPU_SOLVE_1(gpu_icg_solve, KSP_ICG)
 GPU_SOLVE_1(gpu_icgm_solve, KSP_ICGM)
+GPU_SOLVE_1(gpu_ibicgstab_solve, KSP_IBICGSTAB)
 GPU_SOLVE_1(gpu_bicgstab_solve, KSP_BICGSTAB)
 GPU_SOLVE_2(gpu_gcr_solve, KSP_GCR_LEFT)
 GPU_SOLVE_2(gpu_igcr_solve, KSP_IGCR_LEFT)

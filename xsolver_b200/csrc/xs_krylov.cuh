@@ -147,7 +147,8 @@ enum EpiMode {
     M_BICG_GAMA = 2,      // gama = beta/(tmp+small)
     M_BICG_ALPHA = 3,     // alpha = t0/(t1+small)
     M_CG_SIGMA = 4,       // cg (left): alpha = taoo/(sigma+small)
-    M_STORE = 5           // sc[slot_out] = dot
+    M_STORE = 5,          // sc[slot_out] = dot
+    M_IBICG_NU = 6        // ibicgstab: nu = dot; sigma = mu - omega nu
 };
 
 // slot layout
@@ -155,6 +156,11 @@ enum {
     S_TAO = 0, S_TAOO, S_ALPHA, S_BETA, S_SIGMA, S_OMEGA, S_GAMA, S_BETO, S_T0, S_T1, S_TMP, S_RES0SQ,
     S_GCR_T0 = 12, S_GCR_T1, S_GCR_INV, S_GCR_COEF,
     S_H = 16  // GCR alpha[] (classical GS) stored from here (up to 32)
+};
+// ibicgstab scalars (GCR's slots from 16 on are free in this method)
+enum {
+    IB_ALPHA = 16, IB_ALPHAO, IB_ROU, IB_ROUO, IB_OMEGA, IB_PI, IB_TAU, IB_MU, IB_FAI, IB_SIGMA, IB_DELTA, IB_BETA,
+    IB_TMP1, IB_TMP2, IB_THETA, IB_KAPPA, IB_NU
 };
 
 template <typename VT>
@@ -170,6 +176,9 @@ __device__ void EpiDot1<VT>::finalize(const double *tot) const
     } else if (mode == M_BICG_GAMA) {
         st->sc[S_TMP] = d;
         st->sc[S_GAMA] = st->sc[S_BETA] / (d + KSMALL);
+    } else if (mode == M_IBICG_NU) {
+        st->sc[IB_NU] = d;
+        st->sc[IB_SIGMA] = st->sc[IB_MU] - st->sc[IB_OMEGA] * d;
     } else {
         st->sc[slot_out] = d;
     }
@@ -506,6 +515,165 @@ struct OpIcgmUpdate {
         r[i] = r[i] + minalpha * Ap[i];
     }
     __device__ void finalize(const double *) const { record_and_test(st, sqrt(st->sc[S_T0])); }
+};
+
+// ---- single-reduction BiCGSTAB (intel/mpisolver-C-v1.cpp:484-683,
+// right preconditioned: the iterate phi lives in the preconditioned space)
+// scalar prologue of an iteration, in the reference's evaluation order
+__device__ inline void ib_prologue(KState *st)
+{
+    double *c = st->sc;
+    c[IB_ROUO] = c[IB_ROU];
+    c[IB_ROU] = c[IB_FAI] - c[IB_OMEGA] * c[IB_MU];
+    c[IB_DELTA] = (c[IB_ROU] * c[IB_ALPHA]) / (c[IB_ROUO] + KSMALL);
+    c[IB_BETA] = c[IB_DELTA] / (c[IB_OMEGA] + KSMALL);
+    c[IB_TAU] = c[IB_SIGMA] + c[IB_BETA] * c[IB_TAU] - c[IB_DELTA] * c[IB_PI];
+    c[IB_ALPHAO] = c[IB_ALPHA];
+    c[IB_ALPHA] = c[IB_ROU] / (c[IB_TAU] + KSMALL);
+    c[IB_TMP1] = (c[IB_BETA] * c[IB_ALPHA]) / (c[IB_ALPHAO] + KSMALL);
+    c[IB_TMP2] = c[IB_ALPHA] * c[IB_DELTA];
+}
+// start-up: tk += pk (tk = A M^-1 res, pk = A M^-1 A phi) ; reso = res ;
+// qk = vk = zk = 0 ; fai = res.res, sigma = res.tk ; the scalars of
+// iteration 0
+template <typename VT>
+struct OpIbInit {
+    static constexpr int K = 2;
+    int n;
+    KState *st;
+    const VT *res, *pk;
+    VT *tk, *reso, *qk, *vk, *zk;
+    __device__ void load() {}
+    __device__ void elem(int i, double (&a)[2]) const
+    {
+        const VT ri = res[i];
+        const VT ti = tk[i] + pk[i];
+        tk[i] = ti;
+        reso[i] = ri;
+        qk[i] = (VT)0;
+        vk[i] = (VT)0;
+        zk[i] = (VT)0;
+        a[0] += (double)ri * (double)ri;
+        a[1] += (double)ri * (double)ti;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        double *c = st->sc;
+        c[IB_ALPHA] = 1.0; c[IB_ALPHAO] = 1.0; c[IB_ROU] = 1.0; c[IB_ROUO] = 1.0; c[IB_OMEGA] = 1.0;
+        c[IB_PI] = 0.0; c[IB_TAU] = 0.0; c[IB_MU] = 0.0;
+        c[IB_FAI] = t[0];
+        c[IB_SIGMA] = t[1];
+        init_record(st, sqrt(t[0]));
+        ib_prologue(st);
+    }
+};
+// vk = tk - omega pk + beta vk - delta qk ; sk = res - alpha vk ;
+// zk = tmp1 zk + alpha res - tmp2 vk_old   (the reference's daxpy sequences)
+template <typename VT>
+struct OpIbV {
+    static constexpr int K = 0;
+    int n;
+    KState *st;
+    const VT *tk, *pk, *qk, *res;
+    VT *vk, *sk, *zk;
+    VT minomega, beta, mindelta, minalpha, alpha, tmp1, mintmp2;
+    __device__ void load()
+    {
+        const double *c = st->sc;
+        minomega = -(VT)c[IB_OMEGA];
+        beta = (VT)c[IB_BETA];
+        mindelta = -(VT)c[IB_DELTA];
+        alpha = (VT)c[IB_ALPHA];
+        minalpha = -alpha;
+        tmp1 = (VT)c[IB_TMP1];
+        mintmp2 = -(VT)c[IB_TMP2];
+    }
+    __device__ void elem(int i, double (&)[1]) const
+    {
+        const VT vko = vk[i], ri = res[i];
+        VT v = tk[i];
+        v = v + minomega * pk[i];
+        v = v + beta * vko;
+        v = v + mindelta * qk[i];
+        vk[i] = v;
+        sk[i] = ri + minalpha * v;
+        VT z = tmp1 * zk[i];
+        z = z + alpha * ri;
+        zk[i] = z + mintmp2 * vko;
+    }
+    __device__ void finalize(const double *) const {}
+};
+// tk = tk - omega pk - alpha qk ; fai = reso.sk, pi = reso.qk, theta = sk.tk,
+// kappa = tk.tk, mu = reso.tk ; omega = theta/(kappa+small)
+template <typename VT>
+struct OpIbT {
+    static constexpr int K = 5;
+    int n;
+    KState *st;
+    VT *tk;
+    const VT *pk, *qk, *sk, *reso;
+    VT minomega, minalpha;
+    __device__ void load()
+    {
+        minomega = -(VT)st->sc[IB_OMEGA];
+        minalpha = -(VT)st->sc[IB_ALPHA];
+    }
+    __device__ void elem(int i, double (&a)[5]) const
+    {
+        VT t = tk[i] + minomega * pk[i];
+        const VT qi = qk[i];
+        t = t + minalpha * qi;
+        tk[i] = t;
+        const double ro = (double)reso[i], si = (double)sk[i], td = (double)t;
+        a[0] += ro * si;
+        a[1] += ro * (double)qi;
+        a[2] += si * td;
+        a[3] += td * td;
+        a[4] += ro * td;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        double *c = st->sc;
+        c[IB_FAI] = t[0];
+        c[IB_PI] = t[1];
+        c[IB_THETA] = t[2];
+        c[IB_KAPPA] = t[3];
+        c[IB_MU] = t[4];
+        c[IB_OMEGA] = t[2] / (t[3] + KSMALL);
+        bool ok = true;
+        for (int k = 0; k < 5; k++) ok = ok && isfinite(t[k]);
+        if (!ok) {
+            st->err |= DEV_BREAKDOWN;
+            st->done = 3;
+        }
+    }
+};
+// res = sk - omega tk ; phi = phi + zk + omega sk ; acc res.res, the
+// convergence test; then the next iteration's scalars
+template <typename VT>
+struct OpIbR {
+    static constexpr int K = 1;
+    int n;
+    KState *st;
+    VT *res, *phi;
+    const VT *sk, *tk, *zk;
+    VT omega;
+    __device__ void load() { omega = (VT)st->sc[IB_OMEGA]; }
+    __device__ void elem(int i, double (&a)[1]) const
+    {
+        const VT minomega = -omega;
+        const VT si = sk[i];
+        const VT ri = si + minomega * tk[i];
+        res[i] = ri;
+        VT f = phi[i] + zk[i];
+        phi[i] = f + omega * si;
+        a[0] += (double)ri * (double)ri;
+    }
+    __device__ void finalize(const double *t) const
+    {
+        if (!record_and_test(st, sqrt(t[0]))) return;
+        ib_prologue(st);
+    }
 };
 
 // ---- BiCGSTAB

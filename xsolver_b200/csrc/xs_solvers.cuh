@@ -17,7 +17,8 @@ enum Method {
     KSP_GMRES_LEFT = 7,
     KSP_GMRES_RIGHT = 8,
     KSP_ICG = 9,       // intel cpu_icg_solve (single-reduction CG on M^-1 A)
-    KSP_ICGM = 10      // intel cpu_icgm_solve (single-reduction PCG)
+    KSP_ICGM = 10,     // intel cpu_icgm_solve (single-reduction PCG)
+    KSP_IBICGSTAB = 11 // intel cpu_ibicgstab_solve (single-reduction, right preconditioned)
 };
 
 // vectors owned by a solve, cached across solves of the same size
@@ -260,6 +261,49 @@ struct IcgmRun {
         };
         std::vector<const void *> key{b, x, r, z, p, Ap, q, st, c.M, c.A, (const void *)cfg_key(c)};
         run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
+    }
+};
+
+// intel/mpisolver-C-v1.cpp:484-683: phi = x0, start-up products, then per
+// iteration: vk/sk/zk pass, apply + SpMV (qk), tk pass with five dot
+// products, apply + SpMV (pk) with the sixth in its epilogue, res/phi pass
+// with the convergence test; finally x = M^-1 phi.  The reference takes
+// A M^-1 A phi only for a nonzero phi; for phi = 0 that product is exactly
+// zero, so both of its branches are this one sequence.
+template <typename VT, typename MT>
+struct IbicgRun {
+    VecPool<VT> pool;
+    GraphCache gc;
+    void run(SolveCtx &c, const VT *b, VT *x)
+    {
+        const int n = c.n;
+        VT *res = pool.get(0, n), *reso = pool.get(1, n), *phi = pool.get(2, n), *tk = pool.get(3, n);
+        VT *pk = pool.get(4, n), *qk = pool.get(5, n), *zk = pool.get(6, n), *vk = pool.get(7, n);
+        VT *sk = pool.get(8, n), *resm = pool.get(9, n);
+        KState *st = c.W->st.p;
+        RedSlot sl = c.W->slot();
+        const int *done = &st->done;
+        XS_CUDA(cudaMemcpyAsync(phi, x, sizeof(VT) * n, cudaMemcpyDeviceToDevice, c.s));
+        spmv<VT, MT>(*c.A, phi, res, EpiResid<VT>{st, b}, sl, c.s);
+        spmv<VT, MT>(*c.A, phi, pk, EpiAx<VT>{}, sl, c.s);
+        c.M->apply<VT>(pk, resm, nullptr, c.s);
+        spmv<VT, MT>(*c.A, resm, pk, EpiAx<VT>{}, sl, c.s);
+        c.M->apply<VT>(res, resm, nullptr, c.s);
+        spmv<VT, MT>(*c.A, resm, tk, EpiAx<VT>{}, sl, c.s);
+        vecop(OpIbInit<VT>{n, st, res, pk, tk, reso, qk, vk, zk}, sl, c.s);
+        auto body = [&]() {
+            vecop(OpIbV<VT>{n, st, tk, pk, qk, res, vk, sk, zk}, sl, c.s);
+            c.M->apply<VT>(vk, resm, done, c.s);
+            spmv<VT, MT>(*c.A, resm, qk, EpiActive<VT>{st}, sl, c.s);
+            vecop(OpIbT<VT>{n, st, tk, pk, qk, sk, reso}, sl, c.s);
+            c.M->apply<VT>(tk, resm, done, c.s);
+            spmv<VT, MT>(*c.A, resm, pk, EpiDot1<VT>{st, reso, 0, M_IBICG_NU}, sl, c.s);
+            vecop(OpIbR<VT>{n, st, res, phi, sk, tk, zk}, sl, c.s);
+        };
+        std::vector<const void *> key{b, x, res, reso, phi, tk, pk, qk, zk, vk, sk, resm, st, c.M, c.A,
+                                      (const void *)cfg_key(c)};
+        run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
+        c.M->apply<VT>(phi, x, nullptr, c.s);
     }
 };
 
