@@ -284,6 +284,21 @@ int xs_plan_time_op(xs_plan_t p, int op, int reps, int flush_l2, double *ms);
 /* algorithmic bytes of op (counted once per array element) */
 int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes);
 
+/* Matrix Market coordinate files (host only, no GPU needed), replacing the
+ * reference's reader hip/Tool/ReadMatrix/csr_mmio_highlevel.h:8-233
+ * (mmio_info / mmio_data).  xs_mm_info gives the sizes, with nnz counted
+ * after the symmetric expansion; xs_mm_read fills rowptr[m+1],
+ * colidx[nnz], val[nnz] and, if diag is not NULL, diag[m] (the value of
+ * entry (i, i) as written).  With reference_quirks != 0 the result is the
+ * reference reader's: general files store -value; symmetric / hermitian
+ * files store value at (i, j) and (j, i); columns within a row keep the
+ * file's order.  reference_quirks = 0 keeps general files' values as
+ * written.  Real, double and integer fields; complex, pattern and
+ * skew-symmetric files give XS_ERR_UNSUPPORTED, malformed files
+ * XS_ERR_INVALID. */
+int xs_mm_info(const char *path, int *m, int *n, int *nnz, int *symmetric);
+int xs_mm_read(const char *path, int reference_quirks, int *rowptr, int *colidx, double *val, double *diag);
+
 /* Host-only dependency analysis of a strictly triangular CSR pattern (no
  * GPU needed): level[i] = 1 + max level of the rows row i depends on, perm =
  * rows sorted by (level, row) — the position order of the sync-free solve. */

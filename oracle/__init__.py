@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 _REF_INTEL = None
 _REF_ILU0 = None
+_REF_MMIO = None
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -73,6 +74,80 @@ def ref_ilu0():
             return None
         _REF_ILU0 = C.CDLL(path)
     return _REF_ILU0
+
+
+def ref_mmio():
+    """The reference's compiled Matrix Market reader, or None."""
+    global _REF_MMIO
+    if _REF_MMIO is None:
+        path = os.path.join(HERE, "_ref", "libxsref_mmio.so")
+        if not os.path.exists(path):
+            return None
+        _REF_MMIO = C.CDLL(path)
+    return _REF_MMIO
+
+
+def ref_read_mtx(path):
+    """(m, n, rowptr, colidx, val, diag, symmetric) from the reference's own
+    reader, or None when it was not built."""
+    R = ref_mmio()
+    if R is None:
+        return None
+    m, n, nnz, sym = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    assert R.ref_mmio_info(C.byref(m), C.byref(n), C.byref(nnz), C.byref(sym), path.encode()) == 0
+    rp = np.zeros(max(m.value, n.value) + 1, np.int32)
+    ci = np.zeros(max(nnz.value, 1), np.int32)
+    v = np.zeros(max(nnz.value, 1))
+    d = np.zeros(m.value)
+    assert R.ref_mmio_data(_p(rp, np.int32), _p(ci, np.int32), _p(v), _p(d), path.encode()) == 0
+    return m.value, n.value, rp[: m.value + 1], ci[: nnz.value], v[: nnz.value], d, sym.value
+
+
+def read_mtx(path):
+    """Restatement of the reference's Matrix Market reader
+    (hip/Tool/ReadMatrix/csr_mmio_highlevel.h:118-233, mmio_data; sizes as
+    mmio_info :8-116) for real/integer coordinate files: 1-based indices made
+    0-based; general files store -value (the reference's negation), symmetric
+    and hermitian files store value at (i, j) and, off the diagonal, at
+    (j, i) too; diag[i] = value of entry (i, i) as read; rows filled in file
+    order by a counting sort (:200-214).  Returns (m, n, rowptr, colidx, val,
+    diag, symmetric)."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    banner = lines[0].lower().split()
+    symmetric = int("symmetric" in banner or "hermitian" in banner)
+    k = 1
+    while lines[k].startswith("%") or not lines[k].strip():
+        k += 1
+    m, n, nnz_rep = (int(t) for t in lines[k].split()[:3])
+    rows, cols, vals = [], [], []
+    diag = np.zeros(m)
+    cnt = np.zeros(m + 1, np.int64)
+    for line in lines[k + 1 : k + 1 + nnz_rep]:
+        t = line.split()
+        i, j, v = int(t[0]) - 1, int(t[1]) - 1, float(t[2])
+        if not symmetric:
+            rows.append(i); cols.append(j); vals.append(-v)
+            cnt[i] += 1
+        else:
+            rows.append(i); cols.append(j); vals.append(v)
+            cnt[i] += 1
+            if i != j:
+                rows.append(j); cols.append(i); vals.append(v)
+                cnt[j] += 1
+        if i == j:
+            diag[i] = v
+    rp = np.zeros(m + 1, np.int32)
+    rp[1:] = np.cumsum(cnt[:m])
+    nnz = int(rp[m])
+    ci = np.zeros(nnz, np.int32)
+    va = np.zeros(nnz)
+    fill = rp[:-1].astype(np.int64).copy()
+    for r, c, v in zip(rows, cols, vals):
+        ci[fill[r]] = c
+        va[fill[r]] = v
+        fill[r] += 1
+    return m, n, rp, ci, va, diag, symmetric
 
 
 class LU:

@@ -24,6 +24,7 @@
 #include "xs_gmres.cuh"
 #include "xs_parilut.cuh"
 #include "xs_adjoint.cuh"
+#include "xs_mtx.cuh"
 
 namespace xs {
 
@@ -1377,6 +1378,32 @@ int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows)
         trsv_tuning().blocks_per_sm = blocks_per_sm;
         trsv_tuning().backoff_ns = backoff_ns;
         trsv_tuning().chunk_rows = chunk_rows;
+    });
+}
+
+int xs_mm_info(const char *path, int *m, int *n, int *nnz, int *symmetric)
+{
+    return guarded([&] {
+        if (!m || !n || !nnz) throw Status(XS_ERR_INVALID);
+        MmFile F;
+        mm_parse(path, F);
+        const long c = mm_csr_nnz(F);
+        if (c > 0x7fffffffL) throw Status(XS_ERR_CAPACITY);
+        *m = F.m;
+        *n = F.n;
+        *nnz = (int)c;
+        if (symmetric) *symmetric = F.symmetric ? 1 : 0;
+    });
+}
+
+int xs_mm_read(const char *path, int reference_quirks, int *rowptr, int *colidx, double *val, double *diag)
+{
+    return guarded([&] {
+        if (!rowptr || !colidx || !val) throw Status(XS_ERR_INVALID);
+        MmFile F;
+        mm_parse(path, F);
+        if (mm_csr_nnz(F) > 0x7fffffffL) throw Status(XS_ERR_CAPACITY);
+        mm_to_csr(F, reference_quirks != 0, rowptr, colidx, val, diag);
     });
 }
 
