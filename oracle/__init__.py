@@ -186,6 +186,59 @@ def ilu0(A) -> LU:
     return LU(n, lrp, lci[:nl], lv[:nl], dinv, urp, uci[:nu], uv[:nu])
 
 
+IC0_SMALLNUM = 1e-4  # Precond_ic0 defaults (hip/Precond/precon_ic0.h:14-15)
+IC0_DROPTOL = 1e-4
+
+
+def ic0_values(A, smallnum=IC0_SMALLNUM, droptol=IC0_DROPTOL) -> np.ndarray:
+    """IC(0) factor in A's layout (lower part; inverted diagonals)."""
+    out = np.zeros(A.nnz)
+    rc = lib().orc_ic0_values(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), C.c_double(smallnum),
+                              C.c_double(droptol), _p(out))
+    if rc != 0:
+        raise ValueError("matrix has a row without a diagonal entry")
+    return out
+
+
+def ic0(A, smallnum=IC0_SMALLNUM, droptol=IC0_DROPTOL) -> LU:
+    """IC(0) as the seqilu0 factors of the LU solve (HostMatrixCSR::seqic0)."""
+    nl, _ = _counts(A)
+    n = A.n
+    lrp = np.zeros(n + 1, np.int32); urp = np.zeros(n + 1, np.int32)
+    lci = np.zeros(max(nl, 1), np.int32); uci = np.zeros(max(nl, 1), np.int32)
+    lv = np.zeros(max(nl, 1)); uv = np.zeros(max(nl, 1)); dinv = np.zeros(n)
+    rc = lib().orc_ic0(n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), C.c_double(smallnum),
+                       C.c_double(droptol), _p(lrp, np.int32), _p(lci, np.int32), _p(lv), _p(dinv),
+                       _p(urp, np.int32), _p(uci, np.int32), _p(uv))
+    if rc != 0:
+        raise ValueError("matrix has a row without a diagonal entry")
+    return LU(n, lrp, lci[:nl], lv[:nl], dinv, urp, uci[:nl], uv[:nl])
+
+
+def ref_ic0_values(A, smallnum=IC0_SMALLNUM, droptol=IC0_DROPTOL):
+    """The reference's own ic0_csr_A (compiled into oracle/_ref), mapped
+    into A's layout, or None when it was not built."""
+    path = os.path.join(HERE, "_ref", "libxsref_ic0.so")
+    if not os.path.exists(path):
+        return None
+    R = C.CDLL(path)
+    n = A.n
+    cap = A.nnz + n
+    lptr = np.zeros(n + 1, np.int32)
+    lval = np.zeros(cap)
+    lcol = np.zeros(cap, np.int32)
+    R.ref_ic0_csr_A(n, _p(A.rowptr, np.int32), _p(np.ascontiguousarray(A.val)), _p(A.colidx, np.int32),
+                    _p(lptr, np.int32), _p(lval), _p(lcol, np.int32), C.c_double(smallnum), C.c_double(droptol))
+    out = A.val.astype(np.float64).copy()
+    for i in range(n):
+        k = A.rowptr[i]
+        for q in range(lptr[i], lptr[i + 1]):
+            assert A.colidx[k] == lcol[q]
+            out[k] = lval[q]
+            k += 1
+    return out
+
+
 def ilu0_values(A) -> np.ndarray:
     out = np.zeros(A.nnz)
     lib().orc_ilu0_values(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), _p(out))

@@ -342,6 +342,93 @@ void orc_csr_spmv_t(int n, const int *rp, const int *ci, const double *v, const 
         for (int k = rp[i] - base; k < rp[i + 1] - base; k++) y[ci[k] - base] += v[k] * x[i];
 }
 
+/* IC(0) of the lower part of A (hip/Precond/ic0.cpp:4-70, initLByA +
+ * ic0_fact, as called by HostMatrixCSR::seqic0 with the Precond_ic0
+ * defaults smallnum = droptol = 1e-4).  Rows must be sorted with the
+ * diagonal present.  luv (A's layout) receives, at the positions of A's
+ * lower part, the IC(0) factor with each diagonal stored inverted
+ * (1 / l_ii); upper positions are left as A's values.  tnorm_i = droptol *
+ * ||row i of A||; a pivot with |l_ii| < 1e-20 becomes
+ * smallnum / droptol * tnorm_i + tnorm_i.  Returns 1 for a row without a
+ * diagonal entry. */
+int orc_ic0_values(int n, const int *rp, const int *ci, const double *v, double smallnum, double droptol, double *luv)
+{
+    std::vector<int> diag(n, -1);
+    std::vector<double> tnorm(n, 0.0);
+    for (int i = 0; i < n; i++) {
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            luv[k] = v[k];
+            if (ci[k] == i) diag[i] = k;
+            tnorm[i] += v[k] * v[k];
+        }
+        tnorm[i] = std::sqrt(tnorm[i]);
+        tnorm[i] *= droptol;
+        if (diag[i] < 0) return 1;
+    }
+    for (int i = 0; i < n; i++) {
+        const int rs = rp[i], dl = diag[i];
+        for (int j = rs; j < dl; j++) {
+            const int c = ci[j];
+            int idxu = rp[c];
+            const int du = diag[c];
+            for (int k = rs; k < j; k++) {
+                for (int p = idxu; p < du; p++) {
+                    if (ci[p] == ci[k]) {
+                        luv[j] -= luv[k] * luv[p];
+                    } else if (ci[p] > ci[k]) {
+                        idxu = p;
+                        break;
+                    }
+                }
+            }
+            luv[j] *= luv[du];
+        }
+        for (int j = rs; j < dl; j++) luv[dl] -= luv[j] * luv[j];
+        luv[dl] = std::sqrt(luv[dl]);
+        if (std::fabs(luv[dl]) < 1e-20) luv[dl] = smallnum / droptol * tnorm[i] + tnorm[i];
+        luv[dl] = 1 / luv[dl];
+    }
+    return 0;
+}
+
+/* HostMatrixCSR::seqic0 (hip/HostMatrix/HostMatrixCSR.cpp:269-326): the
+ * IC(0) factor (orc_ic0_values layout) as the seqilu0 factors the LU solve
+ * takes: L strict l_ij * d_j, U' strict row j = (l_ij * d_j) for the L
+ * entries (i, j), i ascending, dinv_i = d_i * d_i (d = the stored inverted
+ * diagonals).  Outputs sized as for orc_ilu0 with nu = nl. */
+int orc_ic0(int n, const int *rp, const int *ci, const double *v, double smallnum, double droptol, int *lrp,
+            int *lci, double *lv, double *dinv, int *urp, int *uci, double *uv)
+{
+    std::vector<double> luv(rp[n]);
+    if (orc_ic0_values(n, rp, ci, v, smallnum, droptol, luv.data())) return 1;
+    std::vector<int> diag(n);
+    for (int i = 0; i < n; i++)
+        for (int k = rp[i]; k < rp[i + 1]; k++)
+            if (ci[k] == i) diag[i] = k;
+    lrp[0] = 0;
+    std::vector<int> ucnt(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        lrp[i + 1] = lrp[i] + (diag[i] - rp[i]);
+        for (int k = rp[i]; k < diag[i]; k++) ucnt[ci[k] + 1]++;
+    }
+    urp[0] = 0;
+    for (int j = 0; j < n; j++) urp[j + 1] = urp[j] + ucnt[j + 1];
+    std::vector<int> fill(urp, urp + n);
+    int il = 0;
+    for (int i = 0; i < n; i++) {
+        for (int k = rp[i]; k < diag[i]; k++) {
+            const int j = ci[k];
+            const double t = luv[k] * luv[diag[j]];
+            lv[il] = t;
+            lci[il++] = j;
+            uv[fill[j]] = t;
+            uci[fill[j]++] = i;
+        }
+    }
+    for (int i = 0; i < n; i++) dinv[i] = luv[diag[i]] * luv[diag[i]];
+    return 0;
+}
+
 /* ILU(0) + seqilu0 split.  Outputs sized by the caller: L arrays hold
  * nnz_strict_lower, U arrays nnz_strict_upper.  Returns 0 or -1 if a row
  * has no diagonal entry. */

@@ -174,6 +174,45 @@ def test_ilu0_bitwise_vs_oracle_wide_and_narrow_rows(cuda):
         assert np.array_equal(P.lu_values(), oracle.ilu0_values(A)), A.name
 
 
+def test_ic0_bitwise_vs_oracle(cuda):
+    """GPU IC(0) (the reference's ic0_csr_A order, bitwise vs the restatement
+    that is pinned to the compiled reference) and its conversion into the
+    LU solve's factors (HostMatrixCSR::seqic0)."""
+    from xsolver_b200.api import Plan
+
+    for A in (st.poisson2d_5pt(30), st.varcoef3d_7pt(11, 4), st.poisson3d_7pt(16)):
+        P = Plan(A).factor("ic0")
+        assert np.array_equal(P.lu_values()[_lower_mask(A)], oracle.ic0_values(A)[_lower_mask(A)]), A.name
+        G = P.factors()
+        F = oracle.ic0(A)
+        for k in ("lrp", "lci", "lv", "dinv", "urp", "uci", "uv"):
+            assert np.array_equal(G[k], getattr(F, k)), (A.name, k)
+
+
+def _lower_mask(A):
+    return A.colidx <= np.repeat(np.arange(A.n), np.diff(A.rowptr))
+
+
+def test_ic0_refuses_unsymmetric_pattern(cuda):
+    from xsolver_b200.api import Plan, XsError
+
+    A = st.convdiff3d_27pt(5)
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    keep = ~((rows == 3) & (A.colidx == 4))  # drop one upper entry, keep its lower twin (4, 3)
+    rp = np.zeros(A.n + 1, np.int32)
+    np.cumsum(np.bincount(rows[keep], minlength=A.n), out=rp[1:])
+    B = st.CSRMatrix(A.n, rp, A.colidx[keep], A.val[keep], "unsym")
+    keep2 = ~((rows == 4) & (A.colidx == 3))  # drop one lower entry, keep its upper twin (3, 4)
+    rp2 = np.zeros(A.n + 1, np.int32)
+    np.cumsum(np.bincount(rows[keep2], minlength=A.n), out=rp2[1:])
+    C2 = st.CSRMatrix(A.n, rp2, A.colidx[keep2], A.val[keep2], "unsym2")
+    # U is L's transpose (seqic0): either missing twin makes A's upper pattern differ from it
+    for M in (B, C2):
+        with pytest.raises(XsError) as e:
+            Plan(M).factor("ic0")
+        assert e.value.code == 10, M.name
+
+
 def test_parilu_bitwise_vs_oracle(cuda):
     from xsolver_b200.api import Plan
 

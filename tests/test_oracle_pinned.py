@@ -151,3 +151,10 @@ def test_levels_lower():
     np.cumsum(np.bincount(rows[m], minlength=A.n), out=lrp[1:])
     lev, nlev = oracle.levels_lower(A.n, lrp, np.ascontiguousarray(A.colidx[m]))
     assert nlev == 3 * 8 - 2
+
+
+@pytest.mark.skipif(oracle.ref_ic0_values(st.poisson2d_5pt(3)) is None, reason="compiled reference not present")
+def test_ic0_restatement_bitwise_vs_compiled_reference():
+    """IC(0) (hip/Precond/ic0.cpp, ic0_csr_A with the Precond_ic0 defaults)."""
+    for A in (st.poisson2d_5pt(15), st.varcoef3d_7pt(7, 2), st.poisson3d_7pt(8), st.varcoef3d_7pt(5, 7)):
+        assert np.array_equal(oracle.ic0_values(A), oracle.ref_ic0_values(A)), A.name

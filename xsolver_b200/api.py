@@ -197,7 +197,7 @@ class Solver:
 class Plan:
     """Kernel-level access on device tensors (torch CUDA tensors)."""
 
-    FACTOR_KIND = {"ilu0": 0, "parilu": 1, "parilut": 2}
+    FACTOR_KIND = {"ilu0": 0, "parilu": 1, "parilut": 2, "ic0": 3}
     PREC = {"fp64": 0, "fp32": 1, "bf16": 2, "fp16": 3}
     OPS = {"csr64": 0, "ell64": 1, "csr32": 2, "lsolve": 3, "usolve": 4, "lusolve": 5, "ell32": 6}
 

@@ -327,6 +327,8 @@ struct Handle {
     bool analysed = false;
     std::vector<int> huptr;
     DBuf<int> uptr, rowof, ucp, ucpos, flags;
+    DBuf<int> tpos;          // IC(0): position of the transposed entry (-1: none)
+    DBuf<double> ic0_tnorm;  // IC(0): droptol * row norms
     int ilu_epoch = 0;
     int max_row_len = -1;  // longest row of the pattern (-1: not yet counted)
     DBuf<unsigned> fticket;
@@ -631,6 +633,54 @@ static void load_dinv(Handle &h, const double *vals, const long *diagsrc, bool n
     check_launch();
 }
 
+// IC(0) needs a symmetric pattern: the upper entries take their values from
+// the transposed lower ones (the reference's seqic0 builds U as L's
+// transpose, which is the upper pattern of A only when A's pattern is
+// symmetric)
+constexpr double IC0_SMALLNUM = 1e-4, IC0_DROPTOL = 1e-4;  // Precond_ic0 defaults (hip/Precond/precon_ic0.h:14-15)
+static void ensure_ic0_maps(Handle &h)
+{
+    if (h.tpos.n == (size_t)std::max<long>(h.nnz, 1)) return;
+    const int n = h.n;
+    const int *rp = h.hrp.data(), *ci = h.hci.data();
+    std::vector<int> t(std::max<long>(h.nnz, 1), -1);
+    for (int r = 0; r < n; r++)
+        for (int k = rp[r]; k < rp[r + 1]; k++) {
+            const int c = ci[k];
+            const int *b = ci + rp[c], *e = ci + rp[c + 1];
+            const int *f = std::lower_bound(b, e, r);
+            if (f != e && *f == r) t[k] = (int)(f - ci);
+            else throw Status(XS_ERR_UNSUPPORTED);  // U is L's transpose: the pattern must be symmetric
+        }
+    h.tpos.alloc(t.size());
+    h.tpos.upload(t.data(), t.size(), h.s);
+    h.ic0_tnorm.alloc(n);
+}
+
+// IC(0) of A's lower part into h.luv (A's pattern; see k_ic0_rows)
+static void factor_ic0(Handle &h)
+{
+    analyse_pattern(h);
+    ensure_ic0_maps(h);
+    const int n = h.n;
+    h.luv.alloc(std::max<long>(h.nnz, 1));
+    XS_CUDA(cudaMemcpyAsync(h.luv.p, h.A.v.p, sizeof(double) * h.nnz, cudaMemcpyDeviceToDevice, h.s));
+    k_ic0_tnorm<<<geom().sms * 4, 256, 0, h.s>>>(n, h.A.rp.p, h.A.v.p, IC0_DROPTOL, h.ic0_tnorm.p);
+    h.ilu_epoch++;
+    if (h.ilu_epoch > 1000000000) {
+        XS_CUDA(cudaMemsetAsync(h.flags.p, 0, sizeof(int) * n, h.s));
+        h.ilu_epoch = 1;
+    }
+    const int gl = std::min((n + 127) / 128, geom().sms);
+    k_ic0_rows<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.ic0_tnorm.p, IC0_SMALLNUM,
+                                    IC0_DROPTOL, h.luv.p, h.flags.p, h.ilu_epoch, h.err.p, h.fticket.p, 512);
+    check_launch();
+    int e = 0;
+    XS_CUDA(cudaMemcpyAsync(&e, h.err.p, sizeof(int), cudaMemcpyDeviceToHost, h.s));
+    XS_CUDA(cudaStreamSynchronize(h.s));
+    if (e) throw Status(dev_err_to_status(e));
+}
+
 // exact ILU(0) (kind 0) or ParILU (kind 1) into h.luv (A's pattern)
 static void factor_ilu(Handle &h, int kind, int sweeps)
 {
@@ -732,16 +782,22 @@ static void build_precond(Handle &h)
         M.jdiag32.alloc(n);
         k_jacobi_init<float><<<geom().sms * 4, 256, 0, h.s>>>(n, h.uptr.p, h.A.v.p, M.jdiag32.p);
         check_launch();
-    } else if (type == PC_ILU0 || type == PC_PARILU) {
+    } else if (type == PC_ILU0 || type == PC_PARILU || type == PC_IC0) {
         Trace tr("setup ilu (total)", h.s);
         {
             Trace t1("  analyse_pattern", h.s);
             analyse_pattern(h);
         }
         Trace t2("  numeric factor + loads", h.s);
-        factor_ilu(h, type == PC_ILU0 ? 0 : 1, h.parilu_sweeps);
         if (h.fv.n != (size_t)std::max<long>(h.nnz, 1)) h.fv.alloc(std::max<long>(h.nnz, 1));
-        k_split_lu<<<geom().sms * 4, 256, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, h.fv.p);
+        if (type == PC_IC0) {
+            factor_ic0(h);
+            k_ic0_split<<<geom().sms * 4, 256, 0, h.s>>>(h.nnz, h.rowof.p, h.A.ci.p, h.uptr.p, h.tpos.p, h.luv.p,
+                                                         h.fv.p);
+        } else {
+            factor_ilu(h, type == PC_ILU0 ? 0 : 1, h.parilu_sweeps);
+            k_split_lu<<<geom().sms * 4, 256, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, h.fv.p);
+        }
         check_launch();
         const FactorCopies fc = factor_copies(h, need32);
         load_tri_values(h, M.L, h.fv.p, fc);
@@ -1130,7 +1186,7 @@ static void adjoint_prepare(Handle &h)
     if (M.type == PC_JACOBI) {
         T.jdiag64.alloc(n);
         XS_CUDA(cudaMemcpyAsync(T.jdiag64.p, M.jdiag64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, h.s));
-    } else if (M.type == PC_ILU0 || M.type == PC_PARILU || M.type == PC_PARILUT) {
+    } else if (M.type == PC_ILU0 || M.type == PC_PARILU || M.type == PC_PARILUT || M.type == PC_IC0) {
         // host patterns of L (strict lower) and U' (strict upper) with their
         // value sources, then the transposed triangles
         std::vector<int> lrp, lci, urp, uci;
@@ -1292,7 +1348,8 @@ static int parse_pc(const char *fmt)
     if (ieq(fmt, "parilu")) return PC_PARILU;
     if (ieq(fmt, "ilut") || ieq(fmt, "ilut_mkl") || ieq(fmt, "parilut")) return PC_PARILUT;
     if (ieq(fmt, "none")) return PC_NONE;
-    if (ieq(fmt, "ic0") || ieq(fmt, "ict")) return -2;
+    if (ieq(fmt, "ic0")) return PC_IC0;
+    if (ieq(fmt, "ict")) return -2;
     return -1;
 }
 

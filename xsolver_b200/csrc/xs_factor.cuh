@@ -267,6 +267,127 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
     }
 }
 
+// ---------------------------------------------------------------- IC(0)
+// hip/Precond/ic0.cpp:4-70 (initLByA + ic0_fact, Precond_ic0 defaults
+// smallnum = droptol = 1e-4) on A's lower part, in place in A's layout: at
+// the end entry (i, j<i) holds l_ij and the diagonal 1 / l_ii.
+// tnorm_i = droptol * ||row i of A|| (the pivot replacement scale).
+__global__ void k_ic0_tnorm(int n, const int *__restrict__ rp, const double *__restrict__ v, double droptol,
+                            double *__restrict__ tnorm)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double t = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) t += v[k] * v[k];
+        t = sqrt(t);
+        tnorm[i] = t * droptol;
+    }
+}
+
+// One thread per row, rows in L's level order, persistent CTAs taking
+// 128-row tickets as k_ilu0_rows.  Row i waits for each row c of its lower
+// part (acquire of c's epoch flag), then l_ij = (a_ij - sum_k l_ik l_ck) *
+// (1 / l_cc) with the reference's walk of row c (a column index that only
+// moves forward), then l_ii = sqrt(a_ii - sum_j l_ij^2) (a pivot under 1e-20
+// replaced by smallnum / droptol * tnorm_i + tnorm_i) stored inverted; the
+// operations and their order are the reference's, so the factor is bitwise
+// the same.
+__global__ void __launch_bounds__(128) k_ic0_rows(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                                 const int *__restrict__ uptr, const int *__restrict__ perm,
+                                                 const double *__restrict__ tnorm, double smallnum, double droptol,
+                                                 double *luv, int *flag, int epoch, int *err, unsigned *ticket,
+                                                 int backoff_ns)
+{
+    __shared__ int s_blk;
+    const int ntk = (n + 127) / 128;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            // every CTA ends with one failing claim; the last of them re-arms
+            if (t == (unsigned)(ntk + gridDim.x - 1)) *ticket = 0u;
+            s_blk = (int)t;
+        }
+        __syncthreads();
+        const int blk = s_blk;
+        __syncthreads();
+        if (blk >= ntk) return;
+        const int p = blk * 128 + (int)threadIdx.x;
+        if (p >= n) continue;
+        if (*(volatile int *)err) continue;
+        const int i = perm[p];
+        const int rs = rp[i], dl = uptr[i];
+        bool ok = true;
+        for (int j = rs; j < dl && ok; j++) {
+            const int c = ci[j];
+            long spins = 0;
+            unsigned long long t0 = 0;
+            unsigned ns = 32;
+            while (ld_acquire(flag + c) != epoch) {
+                __nanosleep(ns);  // yield point: the producer may be a lane of this warp
+                if (ns < (unsigned)backoff_ns) ns <<= 1;
+                if ((++spins & 63) == 0) {
+                    const unsigned long long t = gtimer();
+                    if (t0 == 0) t0 = t;
+                    else if (t - t0 > WAIT_LIMIT_NS) {
+                        atomicOr(err, DEV_FACTOR_TIMEOUT);
+                        ok = false;
+                        break;
+                    }
+                    if (*(volatile int *)err) {
+                        ok = false;
+                        break;
+                    }
+                }
+            }
+            if (!ok) break;
+            int idxu = rp[c];
+            const int du = uptr[c];
+            double a = luv[j];
+            for (int k = rs; k < j; k++) {
+                const int ck = ci[k];
+                for (int q = idxu; q < du; q++) {
+                    const int cq = __ldg(ci + q);
+                    if (cq == ck) {
+                        const double t = luv[k] * __ldcg(luv + q);
+                        a = a - t;
+                    } else if (cq > ck) {
+                        idxu = q;
+                        break;
+                    }
+                }
+            }
+            a = a * __ldcg(luv + du);
+            luv[j] = a;
+        }
+        if (!ok) continue;
+        double d = luv[dl];
+        for (int j = rs; j < dl; j++) {
+            const double t = luv[j] * luv[j];
+            d = d - t;
+        }
+        d = sqrt(d);
+        if (fabs(d) < 1e-20) d = smallnum / droptol * tnorm[i] + tnorm[i];
+        luv[dl] = 1 / d;
+        __threadfence();
+        st_release(flag + i, epoch);
+    }
+}
+
+// HostMatrixCSR::seqic0 (hip/HostMatrix/HostMatrixCSR.cpp:269-326): the
+// IC(0) factor as the seqilu0 values of the LU solve, in A's layout:
+// lower (i, j): l_ij * d_j; diagonal: d_i * d_i; upper (i, j): the lower
+// entry (j, i) (position tpos[k]) times d_i, with d the stored 1 / l_ii.
+__global__ void k_ic0_split(long nnz, const int *__restrict__ rowof, const int *__restrict__ ci,
+                            const int *__restrict__ uptr, const int *__restrict__ tpos, const double *__restrict__ luv,
+                            double *__restrict__ fv)
+{
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nnz; k += (long)gridDim.x * blockDim.x) {
+        const int i = rowof[k], j = ci[k];
+        if (j < i) fv[k] = luv[k] * luv[uptr[j]];
+        else if (j == i) fv[k] = luv[k] * luv[k];
+        else fv[k] = luv[tpos[k]] * luv[uptr[i]];
+    }
+}
+
 // one synchronous ParILU sweep over A's nonzeros
 //   rowof[k]  row of entry k;  uptr[i] diagonal position of row i
 //   ucp/ucpos: upper part by columns: for column j, positions ucpos[ucp[j]..ucp[j+1])

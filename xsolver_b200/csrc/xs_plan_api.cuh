@@ -127,6 +127,7 @@ int xs_plan_factor(xs_plan_t p, int kind, int sweeps, double fill, double dropto
         if (kind == 0) h.pc_req = PC_ILU0;
         else if (kind == 1) { h.pc_req = PC_PARILU; h.parilu_sweeps = sweeps; }
         else if (kind == 2) { h.pc_req = PC_PARILUT; h.parilut_fill = fill; h.parilut_sweeps = sweeps; h.parilut_droptol = droptol; }
+        else if (kind == 3) h.pc_req = PC_IC0;
         else throw Status(XS_ERR_INVALID);
         h.inner32 = 1;  // keep reduced-precision copies of the factors for the solves
         invalidate_pc(h);
@@ -140,7 +141,7 @@ int xs_plan_get_lu_values(xs_plan_t p, double *luv)
     return guarded([&] {
         if (!p || !luv) throw Status(XS_ERR_INVALID);
         Handle &h = *p->h;
-        if (!p->factored || p->factor_kind > 1) throw Status(XS_ERR_ORDER);
+        if (!p->factored || p->factor_kind == 2) throw Status(XS_ERR_ORDER);
         h.luv.download(luv, h.nnz, h.s);
         XS_CUDA(cudaStreamSynchronize(h.s));
     });

@@ -7,7 +7,7 @@
 
 namespace xs {
 
-enum PcType { PC_NONE = 0, PC_JACOBI = 1, PC_ILU0 = 2, PC_PARILU = 3, PC_PARILUT = 4 };
+enum PcType { PC_NONE = 0, PC_JACOBI = 1, PC_ILU0 = 2, PC_PARILU = 3, PC_PARILUT = 4, PC_IC0 = 5 };
 enum FactorPrec { FP_F64 = 0, FP_F32 = 1, FP_BF16 = 2, FP_F16 = 3 };
 
 template <typename VT>
