@@ -58,7 +58,7 @@ def _problem(name):
     return A, st.rhs_uniform(A.n, 3)
 
 
-def _worker(rank, ws, port, q, name, fail_rank):
+def _worker(rank, ws, port, q, name, fail_rank, pc="block"):
     import torch.distributed as dist
 
     sys.path.insert(0, ROOT)
@@ -75,7 +75,8 @@ def _worker(rank, ws, port, q, name, fail_rank):
         be = CpuBackend(plan, v)
         if rank == fail_rank:
             raise RuntimeError("injected failure before the first exchange")
-        x, rv, used = dd.bicgstab(be, plan, b[bounds[rank]:bounds[rank + 1]], tol=1e-10, maxiter=500)
+        M = dd.JacobiPC(plan, v, "cpu") if pc == "jacobi" else None
+        x, rv, used = dd.bicgstab(be, plan, b[bounds[rank]:bounds[rank + 1]], tol=1e-10, maxiter=500, pc=M)
         q.put((rank, "ok", x.numpy(), rv, used, plan.n_halo, [p for p, _, _ in plan.recv]))
     except Exception as e:  # reported to the test, then the rank leaves
         q.put((rank, "error", repr(e), None, None, None, None))
@@ -86,13 +87,13 @@ def _worker(rank, ws, port, q, name, fail_rank):
             pass
 
 
-def _run(ws, name, fail_rank=-1, wait=120):
+def _run(ws, name, fail_rank=-1, wait=120, pc="block"):
     import torch.multiprocessing as mp
 
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, ws, port, q, name, fail_rank)) for r in range(ws)]
+    procs = [ctx.Process(target=_worker, args=(r, ws, port, q, name, fail_rank, pc)) for r in range(ws)]
     for p in procs:
         p.start()
     out = sorted([q.get(timeout=wait) for _ in range(ws)], key=lambda t: t[0])
@@ -133,6 +134,33 @@ def test_block_jacobi_bicgstab_matches_serial_oracle(ws, name):
     assert ok, worst
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
     assert np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b) < 1e-9
+
+
+@pytest.mark.parametrize("ws", [2, 3])
+def test_jacobi_bicgstab_matches_compiled_reference(ws):
+    """The reference MPI driver's method (hip/mpi_solve_base.h: BiCGSTAB +
+    Jacobi) on ws CPU ranks against the reference's own compiled
+    cpu_bicgstab_solve on the whole system (bounds from the restatement,
+    which equals it bitwise)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    from parity import count_ok, history_ok, iteration_range, reference_with_bounds
+
+    if oracle.ref_intel() is None:
+        pytest.skip("compiled reference not present")
+    out = _run(ws, "c3", pc="jacobi")
+    assert all(o[1] == "ok" for o in out), [o[2] for o in out if o[1] != "ok"]
+    A, b = _problem("c3")
+    x = np.concatenate([o[2] for o in out])
+    rv, used = out[0][3], out[0][4]
+    xr, rr, ur = oracle.ref_solve("bicgstab", A, b, tol=1e-10, maxiter=500)
+    kw = dict(tol=1e-10, maxiter=500, pc="jacobi")
+    xo, ho, uo, hb, xb = reference_with_bounds("bicgstab", A, b, **kw)
+    assert uo == ur and np.array_equal(xo, xr)
+    assert count_ok(used, ur, iteration_range("bicgstab", A, b, **kw)), (used, ur)
+    ok, worst = history_ok(rv, rr[: ur + 1], hb)
+    assert ok, worst
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < xb
 
 
 def test_failed_rank_ends_the_peers_exchange():

@@ -17,9 +17,10 @@ exchange lists are built once, at setup, from the row patterns.
 
 The solver is the reference's BiCGSTAB (intel/mpisolver-C-v1.cpp:365-482,
 right preconditioned, solution M^-1 phi) with every dot product a local dot
-summed over the ranks (communicator_sum), preconditioned by block Jacobi:
-the local operator's own preconditioner on the owned diagonal block (ILU(0)
-of that block on the GPU).  The local work goes through a backend object
+summed over the ranks (communicator_sum), preconditioned either by block
+Jacobi (the local operator's own preconditioner on the owned diagonal
+block: ILU(0) of that block on the GPU) or by the reference MPI driver's
+pointwise Jacobi (JacobiPC, intel/HostMatrix.h:127-147).  The local work goes through a backend object
 with spmv(x_aug) -> y and precond(r) -> z on the rank's device;
 DeviceBackend uses this library's CUDA kernels.
 """
@@ -132,17 +133,37 @@ class DeviceBackend:
         return z
 
 
+class JacobiPC:
+    """The reference's Jacobi preconditioner on the owned rows
+    (intel/HostMatrix.h:127-147): dinv_i = 1 / (a_ii + 1e-20), z = dinv * r,
+    on the rank's device (a row without a diagonal entry has a_ii = 0)."""
+
+    def __init__(self, plan: HaloPlan, val, device):
+        n = plan.n_local
+        rows = np.repeat(np.arange(n), np.diff(plan.rowptr))
+        diag = np.zeros(n)
+        on = plan.colidx_aug == rows
+        diag[rows[on]] = np.asarray(val)[on]
+        self.dinv = torch.as_tensor(1.0 / (diag + 1e-20), dtype=torch.float64, device=device)
+
+    def precond(self, r):
+        return self.dinv * r
+
+
 def _gdot(a, b):
     t = torch.dot(a, b).reshape(1)
     dist.all_reduce(t)
     return float(t.item())
 
 
-def bicgstab(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000):
+def bicgstab(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000, pc=None):
     """The reference's BiCGSTAB (intel/mpisolver-C-v1.cpp:365-482) on the
-    rank's rows; every rank calls it with its own pieces.  Returns
-    (x_local, resvec, usediter) in the reference's convention (resvec[k] =
-    ||r_k|| / ||r_0||, usediter = index of the last iteration)."""
+    rank's rows; every rank calls it with its own pieces.  pc: an object
+    with precond(r) (e.g. JacobiPC); default the backend's block Jacobi.
+    Returns (x_local, resvec, usediter) in the reference's convention
+    (resvec[k] = ||r_k|| / ||r_0||, usediter = index of the last
+    iteration)."""
+    M = pc if pc is not None else backend
     dev = plan.device
     n, nh = plan.n_local, plan.n_halo
     small = 1e-20
@@ -171,11 +192,11 @@ def bicgstab(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=
         pk = pk + (-alpha) * uk
         pk = omega * pk
         pk = pk + res
-        uk = A(backend.precond(pk))
+        uk = A(M.precond(pk))
         tmp = _gdot(uk, reso)
         gama = beta / (tmp + small)
         sk = res + (-gama) * uk
-        vk = A(backend.precond(sk))
+        vk = A(M.precond(sk))
         t = torch.stack([torch.dot(vk, sk), torch.dot(vk, vk)])
         dist.all_reduce(t)
         t0, t1 = float(t[0]), float(t[1])
@@ -187,4 +208,4 @@ def bicgstab(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=
         resvec.append(rsm)
         if rsm < tol:
             break
-    return backend.precond(phi), np.asarray(resvec), used
+    return M.precond(phi), np.asarray(resvec), used
