@@ -58,7 +58,7 @@ def _problem(name):
     return A, st.rhs_uniform(A.n, 3)
 
 
-def _worker(rank, ws, port, q, name, fail_rank, pc="block"):
+def _worker(rank, ws, port, q, name, fail_rank, pc="block", method="bicgstab"):
     import torch.distributed as dist
 
     sys.path.insert(0, ROOT)
@@ -76,7 +76,8 @@ def _worker(rank, ws, port, q, name, fail_rank, pc="block"):
         if rank == fail_rank:
             raise RuntimeError("injected failure before the first exchange")
         M = dd.JacobiPC(plan, v, "cpu") if pc == "jacobi" else None
-        x, rv, used = dd.bicgstab(be, plan, b[bounds[rank]:bounds[rank + 1]], tol=1e-10, maxiter=500, pc=M)
+        solve = dd.pcg if method == "cgm" else dd.bicgstab
+        x, rv, used = solve(be, plan, b[bounds[rank]:bounds[rank + 1]], tol=1e-10, maxiter=500, pc=M)
         q.put((rank, "ok", x.numpy(), rv, used, plan.n_halo, [p for p, _, _ in plan.recv]))
     except Exception as e:  # reported to the test, then the rank leaves
         q.put((rank, "error", repr(e), None, None, None, None))
@@ -87,13 +88,13 @@ def _worker(rank, ws, port, q, name, fail_rank, pc="block"):
             pass
 
 
-def _run(ws, name, fail_rank=-1, wait=120, pc="block"):
+def _run(ws, name, fail_rank=-1, wait=120, pc="block", method="bicgstab"):
     import torch.multiprocessing as mp
 
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, ws, port, q, name, fail_rank, pc)) for r in range(ws)]
+    procs = [ctx.Process(target=_worker, args=(r, ws, port, q, name, fail_rank, pc, method)) for r in range(ws)]
     for p in procs:
         p.start()
     out = sorted([q.get(timeout=wait) for _ in range(ws)], key=lambda t: t[0])
@@ -136,28 +137,29 @@ def test_block_jacobi_bicgstab_matches_serial_oracle(ws, name):
     assert np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b) < 1e-9
 
 
-@pytest.mark.parametrize("ws", [2, 3])
-def test_jacobi_bicgstab_matches_compiled_reference(ws):
+@pytest.mark.parametrize("ws,method,name", [(2, "bicgstab", "c3"), (3, "bicgstab", "c3"), (2, "cgm", "p3"),
+                                            (3, "cgm", "p3")])
+def test_jacobi_solvers_match_compiled_reference(ws, method, name):
     """The reference MPI driver's method (hip/mpi_solve_base.h: BiCGSTAB +
-    Jacobi) on ws CPU ranks against the reference's own compiled
-    cpu_bicgstab_solve on the whole system (bounds from the restatement,
-    which equals it bitwise)."""
+    Jacobi) and PCG ("cgm") with Jacobi on ws CPU ranks against the
+    reference's own compiled cpu_*_solve on the whole system (bounds from
+    the restatement, which equals it bitwise)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle
     from parity import count_ok, history_ok, iteration_range, reference_with_bounds
 
     if oracle.ref_intel() is None:
         pytest.skip("compiled reference not present")
-    out = _run(ws, "c3", pc="jacobi")
+    out = _run(ws, name, pc="jacobi", method=method)
     assert all(o[1] == "ok" for o in out), [o[2] for o in out if o[1] != "ok"]
-    A, b = _problem("c3")
+    A, b = _problem(name)
     x = np.concatenate([o[2] for o in out])
     rv, used = out[0][3], out[0][4]
-    xr, rr, ur = oracle.ref_solve("bicgstab", A, b, tol=1e-10, maxiter=500)
+    xr, rr, ur = oracle.ref_solve(method, A, b, tol=1e-10, maxiter=500)
     kw = dict(tol=1e-10, maxiter=500, pc="jacobi")
-    xo, ho, uo, hb, xb = reference_with_bounds("bicgstab", A, b, **kw)
+    xo, ho, uo, hb, xb = reference_with_bounds(method, A, b, **kw)
     assert uo == ur and np.array_equal(xo, xr)
-    assert count_ok(used, ur, iteration_range("bicgstab", A, b, **kw)), (used, ur)
+    assert count_ok(used, ur, iteration_range(method, A, b, **kw)), (used, ur)
     ok, worst = history_ok(rv, rr[: ur + 1], hb)
     assert ok, worst
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < xb

@@ -15,8 +15,9 @@ each neighbour the owned values that neighbour reads and receives the halo
 values it reads itself, as the reference's communicator_p2p does; the
 exchange lists are built once, at setup, from the row patterns.
 
-The solver is the reference's BiCGSTAB (intel/mpisolver-C-v1.cpp:365-482,
-right preconditioned, solution M^-1 phi) with every dot product a local dot
+The solvers are the reference's BiCGSTAB (intel/mpisolver-C-v1.cpp:365-482,
+right preconditioned, solution M^-1 phi) and PCG ("cgm", :193-272), with
+every dot product a local dot
 summed over the ranks (communicator_sum), preconditioned either by block
 Jacobi (the local operator's own preconditioner on the owned diagonal
 block: ILU(0) of that block on the GPU) or by the reference MPI driver's
@@ -209,3 +210,48 @@ def bicgstab(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=
         if rsm < tol:
             break
     return M.precond(phi), np.asarray(resvec), used
+
+
+def pcg(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000, pc=None):
+    """The reference's standard PCG, "cgm" (intel/mpisolver-C-v1.cpp:193-272),
+    on the rank's rows with reduced dot products; pc as for bicgstab.
+    Returns (x_local, resvec, usediter) in the reference's convention."""
+    M = pc if pc is not None else backend
+    dev = plan.device
+    n, nh = plan.n_local, plan.n_halo
+    small = 1e-20
+    b = torch.as_tensor(b_local, dtype=torch.float64, device=dev)
+    aug = torch.zeros(n + nh, dtype=torch.float64, device=dev)
+
+    def A(v):
+        aug[:n] = v
+        plan.exchange(aug)
+        return backend.spmv(aug)
+
+    phi = torch.zeros(n, dtype=torch.float64, device=dev) if x0_local is None else \
+        torch.as_tensor(x0_local, dtype=torch.float64, device=dev).clone()
+    res = b - A(phi)
+    zk = M.precond(res)
+    t = torch.stack([torch.dot(res, res), torch.dot(res, zk)])
+    dist.all_reduce(t)
+    res0, tao = float(t[0]) ** 0.5, float(t[1])
+    pk = zk.clone()
+    resvec, used = [], 0
+    for it in range(maxiter):
+        used = it
+        taoo = tao
+        apk = A(pk)
+        sigma = _gdot(pk, apk)
+        alpha = tao / (sigma + small)
+        phi = phi + alpha * pk
+        res = res + (-alpha) * apk
+        zk = M.precond(res)
+        tao = _gdot(res, zk)
+        beta = tao / (taoo + small)
+        pk = beta * pk
+        pk = pk + zk
+        rsm = _gdot(res, res) ** 0.5 / (res0 + small)
+        resvec.append(rsm)
+        if rsm < tol:
+            break
+    return phi, np.asarray(resvec), used
