@@ -252,3 +252,34 @@ def test_device_backend_single_rank_solve(cuda):
     ok, worst = history_ok(rv, ho, hb)
     assert ok, worst
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
+
+
+@pytest.mark.gpu
+def test_device_pcg_jacobi_single_rank(cuda):
+    """World size 1 over NCCL: the decomposition's PCG with the reference's
+    Jacobi on the GPU (DeviceBackend SpMV, JacobiPC on the device) against
+    the serial oracle (bitwise equal to the compiled reference)."""
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from parity import count_ok, history_ok, iteration_range, reference_with_bounds
+    from xsolver_b200 import distributed as dd
+
+    A, b = _problem("p3")
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=30))
+    try:
+        bounds = dd.row_bounds(A.n, 1)
+        rp, ci, v = dd.local_rows(A, bounds, 0)
+        plan = dd.HaloPlan(rp, ci, bounds, 0, cuda)
+        be = dd.DeviceBackend(plan, v, cuda)
+        x, rv, used = dd.pcg(be, plan, b, tol=1e-10, maxiter=500, pc=dd.JacobiPC(plan, v, cuda))
+        x = x.cpu().numpy()
+    finally:
+        dist.destroy_process_group()
+    kw = dict(tol=1e-10, maxiter=500, pc="jacobi")
+    xo, ho, uo, hb, xb = reference_with_bounds("cgm", A, b, **kw)
+    assert count_ok(used, uo, iteration_range("cgm", A, b, **kw)), (used, uo)
+    ok, worst = history_ok(rv, ho, hb)
+    assert ok, worst
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
