@@ -16,8 +16,9 @@ values it reads itself, as the reference's communicator_p2p does; the
 exchange lists are built once, at setup, from the row patterns.
 
 The solvers are the reference's BiCGSTAB (intel/mpisolver-C-v1.cpp:365-482,
-right preconditioned, solution M^-1 phi) and PCG ("cgm", :193-272), with
-every dot product a local dot
+right preconditioned, solution M^-1 phi), PCG ("cgm", :193-272) and
+left-preconditioned GMRES(m) (:933-1087, modified Gram-Schmidt, Givens
+rotations on the host), with every dot product a local dot
 summed over the ranks (communicator_sum), preconditioned either by block
 Jacobi (the local operator's own preconditioner on the owned diagonal
 block: ILU(0) of that block on the GPU) or by the reference MPI driver's
@@ -254,4 +255,94 @@ def pcg(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000,
         resvec.append(rsm)
         if rsm < tol:
             break
+    return phi, np.asarray(resvec), used
+
+
+def _rotate(dx, dy, c, s):
+    """intel/mpisolver-C-v1.cpp:1249-1258 (applyplanerotationc)"""
+    t = c * dx + s * dy
+    return t, -s * dx + c * dy
+
+
+def _generate(dx, dy):
+    """intel/mpisolver-C-v1.cpp:1260-1279 (generateplanerotationc)"""
+    if dy == 0.0:
+        return 1.0, 0.0
+    if abs(dy) > abs(dx):
+        t = dx / dy
+        sn = 1.0 / (1.0 + t * t) ** 0.5
+        return t * sn, sn
+    t = dy / dx
+    cs = 1.0 / (1.0 + t * t) ** 0.5
+    return cs, t * cs
+
+
+def gmres(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000, restart=30, pc=None):
+    """The reference's left-preconditioned GMRES(restart)
+    (intel/mpisolver-C-v1.cpp:933-1087): modified Gram-Schmidt with each dot
+    product reduced over the ranks, Givens rotations and the back
+    substitution (updatec, :1281-1301) on the host, the reference's update
+    with i columns on convergence.  Returns (x_local, resvec, usediter);
+    resvec is indexed by the global iteration."""
+    M = pc if pc is not None else backend
+    dev = plan.device
+    n, nh = plan.n_local, plan.n_halo
+    small = 1e-20
+    m = restart
+    b = torch.as_tensor(b_local, dtype=torch.float64, device=dev)
+    aug = torch.zeros(n + nh, dtype=torch.float64, device=dev)
+
+    def A(v):
+        aug[:n] = v
+        plan.exchange(aug)
+        return backend.spmv(aug)
+
+    def update(phi, k, H, s, V):
+        y = list(s[:k])
+        for i in range(k - 1, -1, -1):
+            y[i] = y[i] / (H[i][i] + small)
+            for j in range(i - 1, -1, -1):
+                y[j] = y[j] - H[j][i] * y[i]
+        for i in range(k):
+            phi = phi + y[i] * V[i]
+        return phi
+
+    phi = torch.zeros(n, dtype=torch.float64, device=dev) if x0_local is None else \
+        torch.as_tensor(x0_local, dtype=torch.float64, device=dev).clone()
+    res = M.precond(b - A(phi))
+    res0 = _gdot(res, res) ** 0.5
+    beta = res0
+    resvec, used, j = [], 0, 0
+    while j < maxiter:
+        H = [[0.0] * m for _ in range(m + 1)]
+        s, cs, sn = [0.0] * (m + 1), [0.0] * (m + 1), [0.0] * (m + 1)
+        res = (1.0 / (beta + small)) * res
+        V = [res.clone()]
+        s[0] = beta
+        i = 0
+        while i < m and j < maxiter:
+            w = M.precond(A(V[i]))
+            for k in range(i + 1):
+                t = _gdot(w, V[k])
+                H[k][i] = t
+                w = w + (-t) * V[k]
+            t = _gdot(w, w) ** 0.5
+            H[i + 1][i] = t
+            w = (1.0 / (t + small)) * w
+            V.append(w)
+            for k in range(i):
+                H[k][i], H[k + 1][i] = _rotate(H[k][i], H[k + 1][i], cs[k], sn[k])
+            cs[i], sn[i] = _generate(H[i][i], H[i + 1][i])
+            H[i][i], H[i + 1][i] = _rotate(H[i][i], H[i + 1][i], cs[i], sn[i])
+            s[i], s[i + 1] = _rotate(s[i], s[i + 1], cs[i], sn[i])
+            err = abs(s[i + 1]) / (res0 + small)
+            resvec.append(err)
+            if err < tol:
+                return update(phi, i, H, s, V), np.asarray(resvec), j
+            i += 1
+            j += 1
+        phi = update(phi, m, H, s, V)
+        res = M.precond(b - A(phi))
+        beta = abs(s[m])
+        used = j
     return phi, np.asarray(resvec), used
