@@ -512,6 +512,7 @@ static void update_values(Handle &h, const double *v)
 static void analyse_pattern(Handle &h)
 {
     if (h.analysed) return;
+    h.tpos.free();  // IC(0) transpose map of the previous pattern
     const int n = h.n;
     const int *rp = h.hrp.data(), *ci = h.hci.data();
     h.huptr.assign(n, -1);
