@@ -51,7 +51,7 @@ enum xs_status {
     XS_ERR_NAN = 7,           /* non-finite input or residual                   */
     XS_ERR_ORDER = 8,         /* calls out of order (e.g. pc before ksp)        */
     XS_ERR_ELL_WIDTH = 9,     /* ELL width outside the supported range          */
-    XS_ERR_UNSUPPORTED = 10,  /* combination not provided (e.g. ic0 on GPU)     */
+    XS_ERR_UNSUPPORTED = 10,  /* combination not provided (e.g. ict on GPU)     */
     XS_ERR_CAPACITY = 11,     /* a fixed per-row capacity was exceeded          */
     XS_ERR_NO_GPU = 12        /* no CUDA device visible                         */
 };
@@ -66,7 +66,9 @@ enum xs_status {
  * arrays are borrowed and must outlive xsolver_free(), as in the reference. */
 void xsolver_mat_setup(int nInterior, int *rowptr, int *colidx, double *val, int *advanced_pam);
 /* hip/xsolver_c.cpp:103-130: "bicgstab", "cg", "igcr" (case variants as in
- * the reference), plus "gcr", "gmres", "fgmres". */
+ * the reference), plus "gcr", "gmres", "fgmres", "cgm"/"pcg", and the
+ * single-reduction "icg", "icgm", "ibicgstab" of intel/mpisolver-C-v1.cpp
+ * (left open at hip/xsolver_c.cpp:127). */
 void xsolver_ksp_settype(char *fmt);
 /* hip/xsolver_c.cpp:131-133 */
 void xsolver_ksp_set_absolute_tol(double absolute_tol);
@@ -74,15 +76,16 @@ void xsolver_ksp_set_absolute_tol(double absolute_tol);
  * must stay valid until xsolver_solve returns.  resvec[0] = ||r0||,
  * resvec[k+1] = ||r_k|| (absolute), *usediter = iterations used. */
 void xsolver_ksp_setoption(double tol, int maxiter, int *usediter, double *resvec, int restart);
-/* hip/xsolver_c.cpp:150-263: "jacobi", "ilu0", "ilut" (GPU ParILUT),
+/* hip/xsolver_c.cpp:150-263: "jacobi", "ilu0", "ic0", "ilut" (GPU ParILUT),
  * "ilu0_mkl"/"ilut_mkl" (mapped to ilu0/ilut as the reference does on GPU),
- * plus "parilu" and "none".  "ic0"/"ict" record XS_ERR_UNSUPPORTED (the
- * reference exits for them on GPU).  Must follow xsolver_ksp_settype. */
+ * plus "parilu" and "none".  "ic0" needs a structurally symmetric pattern
+ * (XS_ERR_UNSUPPORTED at solve otherwise); "ict" records XS_ERR_UNSUPPORTED
+ * (the reference exits for it on GPU).  Must follow xsolver_ksp_settype. */
 void xsolver_pc_settype(char *fmt);
 /* hip/xsolver_c.cpp:268-273.  For "ilut": max_fill is the ParILUT fill
  * factor, tol its drop tolerance. */
 void xsolver_pc_setilut(double tol, int max_fill);
-/* hip/xsolver_c.cpp:264-267 (IC-type preconditioners are not provided). */
+/* hip/xsolver_c.cpp:264-267.  ICT is not provided: records XS_ERR_UNSUPPORTED. */
 void xsolver_pc_setict(double tol, int max_fill);
 /* hip/xsolver_c.cpp:274-292.  sol holds x0 on entry, the solution on exit. */
 void xsolver_solve(double *rhs, double *sol);

@@ -268,6 +268,32 @@ def test_missing_diagonal_reports_error(cuda, pc):
     assert e.value.code == 4
 
 
+def test_rejected_pattern_keeps_previous_matrix(cuda):
+    """A pattern that fails validation (a column index past n, a row end past
+    rp[n]) leaves the handle with its previous matrix and preconditioner."""
+    from xsolver_b200 import _lib
+
+    A = st.poisson2d_5pt(20)
+    b = st.rhs_uniform(A.n, 3)
+    S = _solver(A, "bicgstab", "ilu0", 1e-10, 500)
+    x0 = S.solve(b)
+    it0 = S.usediter
+    L = _lib.lib()
+    bad_ci = A.colidx.copy()
+    bad_ci[7] = A.n
+    assert L.xs_mat_setup(S.h, A.n, A.rowptr.ctypes.data_as(C.POINTER(C.c_int)),
+                          bad_ci.ctypes.data_as(C.POINTER(C.c_int)),
+                          A.val.ctypes.data_as(C.POINTER(C.c_double)), 0) == 1
+    bad_rp = A.rowptr.copy()
+    bad_rp[3] = A.rowptr[-1] + 5
+    assert L.xs_mat_setup(S.h, A.n, bad_rp.ctypes.data_as(C.POINTER(C.c_int)),
+                          A.colidx.ctypes.data_as(C.POINTER(C.c_int)),
+                          A.val.ctypes.data_as(C.POINTER(C.c_double)), 0) == 1
+    x1 = S.solve(b)
+    assert abs(S.usediter - it0) <= 1
+    assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) < 1e-10
+
+
 def test_reference_setter_api_conventions(cuda):
     """xsolver_* globals: hip conventions (resvec[0] = ||r0||, absolute
     history, usediter = iterations) and call-order errors instead of exit."""

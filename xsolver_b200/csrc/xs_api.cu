@@ -418,41 +418,54 @@ static void set_matrix(Handle &h, int n, const int *rp, const int *ci, const dou
     if (base != 0 && base != 1) throw Status(XS_ERR_INVALID);
     long nnz = (long)rp[n] - base;
     if (nnz < 0 || nnz > 0x7fffffffL - 16) throw Status(XS_ERR_INVALID);
-    h.n = n;
-    h.nnz = nnz;
-    h.vperm.clear();
-    h.hv_stale = false;
-    h.hrp.resize(n + 1);
-    h.hci.resize(nnz);
-    h.hv.assign(v, v + nnz);
-    for (int i = 0; i <= n; i++) h.hrp[i] = rp[i] - base;
+    // Checked and sorted into locals first: a rejected pattern leaves the
+    // handle's previous matrix (host copy, device operator, factors) intact.
+    std::vector<int> hrp(n + 1), hci(nnz);
+    std::vector<double> hv(v, v + nnz);
+    std::vector<long> vperm;
+    for (int i = 0; i <= n; i++) hrp[i] = rp[i] - base;
     for (int i = 0; i < n; i++) {
-        if (h.hrp[i + 1] < h.hrp[i]) throw Status(XS_ERR_INVALID);
-        for (int k = h.hrp[i]; k < h.hrp[i + 1]; k++) {
+        // a row end past rp[n] would read beyond the caller's column array
+        if (hrp[i + 1] < hrp[i] || hrp[i + 1] > nnz) throw Status(XS_ERR_INVALID);
+        for (int k = hrp[i]; k < hrp[i + 1]; k++) {
             int c = ci[k] - base;
             if (c < 0 || c >= n) throw Status(XS_ERR_INVALID);
-            h.hci[k] = c;
+            hci[k] = c;
         }
         // columns must be sorted within a row (the reference requires it for
         // its ILU merges; sort here if the caller did not)
         bool sorted = true;
-        for (int k = h.hrp[i] + 1; k < h.hrp[i + 1]; k++)
-            if (h.hci[k] <= h.hci[k - 1]) { sorted = false; break; }
+        for (int k = hrp[i] + 1; k < hrp[i + 1]; k++)
+            if (hci[k] <= hci[k - 1]) { sorted = false; break; }
         if (!sorted) {
-            if (h.vperm.empty()) {
-                h.vperm.resize(nnz);
-                for (long k = 0; k < nnz; k++) h.vperm[k] = k;
+            if (vperm.empty()) {
+                vperm.resize(nnz);
+                for (long k = 0; k < nnz; k++) vperm[k] = k;
             }
             std::vector<std::pair<int, long>> e;
-            for (int k = h.hrp[i]; k < h.hrp[i + 1]; k++) e.emplace_back(h.hci[k], (long)k);
+            for (int k = hrp[i]; k < hrp[i + 1]; k++) e.emplace_back(hci[k], (long)k);
             std::sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.first < b.first; });
             for (size_t q = 0; q < e.size(); q++) {
-                h.hci[h.hrp[i] + q] = e[q].first;
-                h.hv[h.hrp[i] + q] = v[e[q].second];
-                h.vperm[h.hrp[i] + q] = e[q].second;
+                hci[hrp[i] + q] = e[q].first;
+                hv[hrp[i] + q] = v[e[q].second];
+                vperm[hrp[i] + q] = e[q].second;
             }
         }
     }
+    // From here on the handle holds the new pattern; until the device
+    // operator is complete it reports no matrix.
+    h.have_matrix = false;
+    h.analysed = false;
+    h.have_solution = false;
+    h.adj.reset();
+    invalidate_pc(h);
+    h.n = n;
+    h.nnz = nnz;
+    h.hrp.swap(hrp);
+    h.hci.swap(hci);
+    h.hv.swap(hv);
+    h.vperm.swap(vperm);
+    h.hv_stale = false;
     h.A = Operator();
     operator_setup(h.A, n, h.hrp.data(), h.hci.data(), h.hv.data(), 0, false, h.s, h.err.p);
     h.format = format;
@@ -1743,7 +1756,6 @@ int xs_last_outer_steps(xs_handle_t h, int *o)
 // ---------------------------------------------------------------- reference setter API (global handle)
 static std::mutex g_mu;
 static xs_handle_t g_h = nullptr;
-static int g_pam[3] = {0, 0, 0};
 
 static Handle &gh()
 {
@@ -1760,9 +1772,6 @@ void xsolver_mat_setup(int nInterior, int *rowptr, int *colidx, double *val, int
         int fmt = 0;
         bool unsupported = false;
         if (advanced_pam) {
-            g_pam[0] = advanced_pam[0];
-            g_pam[1] = advanced_pam[1];
-            g_pam[2] = advanced_pam[2];
             if (advanced_pam[0] == 1) unsupported = true;  // MPI distribution: one GPU only
             if (advanced_pam[1] == 1) fmt = 1;
             else if (advanced_pam[1] == 2) unsupported = true;  // CSC: CPU-only in the reference
@@ -1906,7 +1915,6 @@ static struct {
     int *offrp = nullptr, *offci = nullptr;
 } g_mc;
 static xs_handle_t g_gpu = nullptr;
-static int g_gpu_pc = PC_NONE;
 
 static void mcsr_to_csr(std::vector<int> &rp, std::vector<int> &ci, std::vector<double> &v)
 {
@@ -2018,7 +2026,6 @@ void gpu_preconditioner_setup(char *fmt)
         int t = parse_pc(fmt);
         if (ieq(fmt, "parilut")) t = PC_PARILUT;
         if (t < 0) throw Status(t == -2 ? XS_ERR_UNSUPPORTED : XS_ERR_INVALID);
-        g_gpu_pc = t;
         g_gpu->h->pc_req = t;
         invalidate_pc(*g_gpu->h);
         build_precond(*g_gpu->h);
