@@ -62,8 +62,12 @@ enum xs_status {
 
 /* hip/xsolver_c.cpp:41-102.  CSR with n rows; rowptr[0] selects 0- or
  * 1-based indexing.  advanced_pam[3] = {distribute (must be 0: one GPU),
- * SpMV format (0 CSR, 1 ELL), gpu (ignored: always the GPU)}.  The host
- * arrays are borrowed and must outlive xsolver_free(), as in the reference. */
+ * SpMV format (0 CSR, 1 ELL; 2 = CSC is CPU-only in the reference), gpu
+ * (ignored: always the GPU)}.  distribute = 1 or CSC records
+ * XS_ERR_UNSUPPORTED and leaves the previous matrix in place, as does a
+ * pattern that fails validation (XS_ERR_INVALID).  The arrays are copied:
+ * unlike the reference, which borrows them until xsolver_free(), the caller
+ * may release them when the call returns. */
 void xsolver_mat_setup(int nInterior, int *rowptr, int *colidx, double *val, int *advanced_pam);
 /* hip/xsolver_c.cpp:103-130: "bicgstab", "cg", "igcr" (case variants as in
  * the reference), plus "gcr", "gmres", "fgmres", "cgm"/"pcg", and the

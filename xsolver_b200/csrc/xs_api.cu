@@ -1691,7 +1691,7 @@ int xs_solve_batch(xs_handle_t h, int nrhs, const double *rhs, double *sol)
 int xs_mat_update(xs_handle_t h, const double *val)
 {
     return guarded([&] {
-        if (!h) throw Status(XS_ERR_INVALID);
+        HCHK(h);
         update_values(*h->h, val);
     });
 }
@@ -1770,17 +1770,17 @@ void xsolver_mat_setup(int nInterior, int *rowptr, int *colidx, double *val, int
     std::lock_guard<std::mutex> lk(g_mu);
     guarded([&] {
         int fmt = 0;
-        bool unsupported = false;
         if (advanced_pam) {
-            if (advanced_pam[0] == 1) unsupported = true;  // MPI distribution: one GPU only
+            // MPI distribution (one GPU only here) and CSC input (CPU-only in
+            // the reference) are refused before the matrix is taken, so no
+            // rank goes on to solve its local block as if it were the system
+            if (advanced_pam[0] == 1 || advanced_pam[1] == 2) throw Status(XS_ERR_UNSUPPORTED);
             if (advanced_pam[1] == 1) fmt = 1;
-            else if (advanced_pam[1] == 2) unsupported = true;  // CSC: CPU-only in the reference
         }
         Handle &H = gh();
         H.intel_conv = 0;
         H.quirk = 0;
         set_matrix(H, nInterior, rowptr, colidx, val, fmt);
-        if (unsupported) throw Status(XS_ERR_UNSUPPORTED);
     });
 }
 void xsolver_ksp_settype(char *fmt)
