@@ -81,12 +81,13 @@ class HaloPlan:
         if self.world == 1 or (not self.send and not self.recv):
             return x_aug
         bufs = [x_aug.index_select(0, idx).contiguous() for _, idx in self.send]
-        reqs = []
-        for q, off, cnt in self.recv:
-            reqs.append(dist.irecv(x_aug[self.n_local + off:self.n_local + off + cnt], src=q))
-        for (p, _), buf in zip(self.send, bufs):
-            reqs.append(dist.isend(buf, dst=p))
-        for r in reqs:
+        # One batch: NCCL runs the point-to-point calls between a pair of
+        # ranks on one stream, so a receive posted alone would block the
+        # send behind it while the peer's receive waits for that send.
+        ops = [dist.P2POp(dist.irecv, x_aug[self.n_local + off:self.n_local + off + cnt], q)
+               for q, off, cnt in self.recv]
+        ops += [dist.P2POp(dist.isend, buf, p) for (p, _), buf in zip(self.send, bufs)]
+        for r in dist.batch_isend_irecv(ops):
             r.wait()
         return x_aug
 
