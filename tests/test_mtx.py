@@ -75,6 +75,8 @@ def test_general_values_negated_unless_quirks_off(tmp_path):
     ("1 1 1\n1 1 1\n", 1),
     ("%%MatrixMarket matrix coordinate real general\n2 2 2\n1 1 1\n3 1 1\n", 1),
     ("%%MatrixMarket matrix coordinate real general\n2 2 3\n1 1 1\n2 2 1\n", 1),
+    ("%%MatrixMarket matrix coordinate real symmetric\n2 3 2\n1 1 1\n3 2 1\n", 1),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1000000000000\n1 1 1\n", 1),
 ])
 def test_reader_refuses_bad_files(tmp_path, text, code):
     from xsolver_b200._lib import XsError

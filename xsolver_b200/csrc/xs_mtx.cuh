@@ -93,6 +93,11 @@ inline void mm_parse(const char *path, MmFile &F)
     const long nnz = std::strtol(p, &q, 10);
     if (q == p || m < 0 || n < 0 || nnz < 0 || m > 0x7ffffffeL || n > 0x7ffffffeL) throw Status(XS_ERR_INVALID);
     p = q;
+    // a symmetric file mirrors (i, j) into row j: only square matrices
+    if (F.symmetric && m != n) throw Status(XS_ERR_INVALID);
+    // an entry takes at least "i j v" plus a separator: a count the rest of
+    // the file cannot hold is a short list, refused before any allocation
+    if (nnz > (long)(end - p) / 6 + 1) throw Status(XS_ERR_INVALID);
     F.m = (int)m;
     F.n = (int)n;
     F.reported = nnz;
