@@ -1923,6 +1923,13 @@ static void mcsr_to_csr(std::vector<int> &rp, std::vector<int> &ci, std::vector<
     ci.clear();
     v.clear();
     const int base = g_mc.offrp[0];
+    if (base != 0 && base != 1) throw Status(XS_ERR_INVALID);
+    // row offsets must not run backwards or past the nSizes off-diagonal
+    // entries the caller's arrays hold (when it states that count)
+    for (int i = 0; i < n; i++)
+        if (g_mc.offrp[i + 1] < g_mc.offrp[i] || (g_mc.nsizes > 0 && g_mc.offrp[i + 1] - base > g_mc.nsizes))
+            throw Status(XS_ERR_INVALID);
+    if (g_mc.offrp[n] > base && (!g_mc.offci || !g_mc.offv)) throw Status(XS_ERR_INVALID);
     for (int i = 0; i < n; i++) {
         std::vector<std::pair<int, double>> e;
         for (int k = g_mc.offrp[i] - base; k < g_mc.offrp[i + 1] - base; k++) e.emplace_back(g_mc.offci[k] - base, g_mc.offv[k]);
