@@ -84,3 +84,19 @@ def test_compute_calls_fail_loudly_without_gpu():
 
 def test_library_path_is_in_tree():
     assert LIB.endswith("xsolver_b200/libxsolver_b200.so")
+
+
+def test_wrapper_refuses_arrays_the_c_calls_would_overrun():
+    """The C entry points take n (or nnz) elements with no length argument;
+    the Python wrapper checks shapes, dtypes and devices before calling."""
+    import torch
+
+    from xsolver_b200 import api
+
+    assert api._vec([1, 2, 3], (3,), "b").dtype == np.float64
+    with pytest.raises(ValueError):
+        api._vec(np.zeros(2), (3,), "b")
+    with pytest.raises(ValueError):
+        api._vec(np.zeros((3, 1)), (3,), "b")
+    with pytest.raises(ValueError):
+        api._dev(torch.zeros(3, dtype=torch.float64), 3, "float64", "x")  # host tensor

@@ -37,6 +37,26 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def _vec(a, shape, what):
+    """A contiguous float64 host array of exactly `shape`: the C entry
+    points read and write n (or nnz) elements with no length argument."""
+    a = _f64(a)
+    if a.shape != tuple(shape):
+        raise ValueError(f"{what}: expected shape {tuple(shape)}, got {a.shape}")
+    return a
+
+
+def _dev(t, n, dtype, what):
+    """A CUDA tensor the kernels may read or write n elements of."""
+    if not getattr(t, "is_cuda", False):
+        raise ValueError(f"{what}: expected a CUDA tensor")
+    if str(t.dtype) != f"torch.{dtype}":
+        raise ValueError(f"{what}: expected {dtype}, got {t.dtype}")
+    if not t.is_contiguous() or t.numel() < n:
+        raise ValueError(f"{what}: expected a contiguous tensor of at least {n} elements")
+    return t
+
+
 class Solver:
     """A solver handle: matrix, Krylov method, preconditioner, precision."""
 
@@ -54,7 +74,7 @@ class Solver:
 
     def mat_update(self, val):
         """New values for the same pattern (caller entry order)."""
-        self._v = np.ascontiguousarray(val, dtype=np.float64)
+        self._v = _vec(val, (self.A.nnz,), "mat_update values")
         check(self._L.xs_mat_update(self.h, _d(self._v)), "xs_mat_update")
         return self
 
@@ -125,23 +145,28 @@ class Solver:
     def solve(self, b, x0=None, out=None) -> np.ndarray:
         """Host arrays.  out (float64, contiguous, e.g. a pinned buffer), if
         given, holds x0 on entry and receives the solution in place."""
-        b = _f64(b)
+        n = self.A.n
+        b = _vec(b, (n,), "rhs")
         if out is not None:
-            if out.dtype != np.float64 or not out.flags.c_contiguous:
-                raise ValueError("out must be a contiguous float64 array")
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != (n,):
+                raise ValueError(f"out must be a contiguous float64 array of shape ({n},)")
             x = out
         else:
-            x = np.zeros(self.A.n) if x0 is None else _f64(x0).copy()
+            x = np.zeros(n) if x0 is None else _vec(x0, (n,), "x0").copy()
         check(self._L.xs_solve(self.h, _d(b), _d(x)), "xs_solve")
         return x
 
     def solve_device(self, b, x):
         """b, x: CUDA tensors (float64, n); x holds x0 and receives the solution."""
+        _dev(b, self.A.n, "float64", "rhs")
+        _dev(x, self.A.n, "float64", "x")
         check(self._L.xs_solve_device(self.h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr())), "xs_solve_device")
         return x
 
     def solve_batch(self, B) -> np.ndarray:
-        B = np.ascontiguousarray(B, dtype=np.float64)
+        B = _f64(B)
+        if B.ndim != 2 or B.shape[1] != self.A.n:
+            raise ValueError(f"solve_batch: expected shape (k, {self.A.n}), got {B.shape}")
         X = np.zeros_like(B)
         check(self._L.xs_solve_batch(self.h, B.shape[0], _d(B), _d(X)), "xs_solve_batch")
         return X
@@ -177,7 +202,7 @@ class Solver:
 
     # -- adjoint
     def adjoint(self, dLdx, want_b=True, want_A=True):
-        g = _f64(dLdx)
+        g = _vec(dLdx, (self.A.n,), "dLdx")
         db = np.zeros(self.A.n) if want_b else None
         dA = np.zeros(self.A.nnz) if want_A else None
         check(self._L.xs_adjoint(self.h, _d(g), _d(db) if db is not None else None, _d(dA) if dA is not None else None),
@@ -185,8 +210,10 @@ class Solver:
         return db, dA
 
     def adjoint_batch(self, X, G):
-        X = np.ascontiguousarray(X, dtype=np.float64)
-        G = np.ascontiguousarray(G, dtype=np.float64)
+        X = _f64(X)
+        if X.ndim != 2 or X.shape[1] != self.A.n:
+            raise ValueError(f"adjoint_batch: expected X of shape (k, {self.A.n}), got {X.shape}")
+        G = _vec(G, X.shape, "adjoint_batch G")
         k = X.shape[0]
         DB = np.zeros_like(X)
         DA = np.zeros((k, self.A.nnz))
@@ -235,12 +262,17 @@ class Plan:
         self._pending.extend(tensors)
 
     def spmv(self, x, y, fmt="csr", precision="fp64"):
+        dt = "float64" if precision == "fp64" else "float32"
+        _dev(x, self.A.n, dt, "x")
+        _dev(y, self.A.n, dt, "y")
         check(self._L.xs_plan_spmv(self.p, 1 if fmt == "ell" else 0, 0 if precision == "fp64" else 1,
                                    C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "spmv")
         self._hold(x, y)
         return y
 
     def spmv_t(self, x, y):
+        _dev(x, self.A.n, "float64", "x")
+        _dev(y, self.A.n, "float64", "y")
         check(self._L.xs_plan_spmv_t(self.p, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "spmv_t")
         self._hold(x, y)
         return y
@@ -278,11 +310,16 @@ class Plan:
 
     def lusolve(self, x, z):
         prec = 0 if str(x.dtype) == "torch.float64" else 1
+        dt = "float64" if prec == 0 else "float32"
+        _dev(x, self.A.n, dt, "x")
+        _dev(z, self.A.n, dt, "z")
         check(self._L.xs_plan_lusolve(self.p, prec, C.c_void_p(x.data_ptr()), C.c_void_p(z.data_ptr())), "lusolve")
         self._hold(x, z)
         return z
 
     def lusolve_t(self, x, z):
+        _dev(x, self.A.n, "float64", "x")
+        _dev(z, self.A.n, "float64", "z")
         check(self._L.xs_plan_lusolve_t(self.p, C.c_void_p(x.data_ptr()), C.c_void_p(z.data_ptr())), "lusolve_t")
         self._hold(x, z)
         return z
@@ -349,8 +386,14 @@ def xsolver_pc_setilut(tol, max_fill):
 
 
 def xsolver_solve(rhs, sol):
-    rhs = np.ascontiguousarray(rhs, np.float64)
-    assert sol.dtype == np.float64 and sol.flags["C_CONTIGUOUS"]
+    rhs = _f64(rhs)
+    if "keep" in _g:  # the system set by xsolver_mat_setup fixes the length
+        n = len(_g["keep"][0]) - 1
+        rhs = _vec(rhs, (n,), "rhs")
+        if sol.shape != (n,):
+            raise ValueError(f"sol: expected shape ({n},), got {sol.shape}")
+    if sol.dtype != np.float64 or not sol.flags["C_CONTIGUOUS"]:
+        raise ValueError("sol must be a contiguous float64 array (x0 in, solution out)")
     lib().xsolver_solve(_d(rhs), _d(sol))
     return _lib.last_error()
 
