@@ -7,8 +7,17 @@ CPU code, compiled from its sources by oracle/Makefile into oracle/_ref:
                       usediter.
   ilu0.npz            hip ilu0_simple (hip/Precond/ilut_diag_in_csr.cpp:347)
                       combined LU values on small stencil matrices.
+  krylov_single_reduction.npz
+                      intel/ cpu_{icg,icgm,ibicgstab}_solve
+                      (intel/mpisolver-C-v1.cpp:104-191, 273-363, 484-683)
+                      with Jacobi on the same systems (icg/icgm on the
+                      symmetric ones); same fields as krylov_jacobi.npz.
+  ic0.npz             hip ic0_csr_A (hip/Precond/ic0.cpp:72-81) with the
+                      Precond_ic0 defaults, in A's layout, on small
+                      symmetric stencil matrices.
 
-Run here (where the reference sources exist):  python tests/golden/make_golden.py
+Run here (where the reference sources exist):
+    python tests/golden/make_golden.py [file.npz ...]   (default: all files)
 The fixtures are committed; tests never need the reference sources.
 """
 import os
@@ -29,12 +38,16 @@ PROBLEMS = {
     "vc3d_7pt_8": (lambda: st.varcoef3d_7pt(8, 3), 3, -1.0, 1.0),
 }
 METHODS = ["cg", "cgm", "bicgstab", "gcr", "igcr", "gmres", "fgmres"]
+SINGLE_REDUCTION = ["icg", "icgm", "ibicgstab"]
+IC0_MATRICES = {
+    "p2d_5pt_15": lambda: st.poisson2d_5pt(15),
+    "vc3d_7pt_7": lambda: st.varcoef3d_7pt(7, 2),
+    "p3d_7pt_8": lambda: st.poisson3d_7pt(8),
+    "vc3d_7pt_5": lambda: st.varcoef3d_7pt(5, 7),
+}
 
 
-def main():
-    oracle.build(ref=True)
-    if oracle.ref_intel() is None:
-        raise SystemExit("reference not built (needs the reference sources)")
+def krylov(methods):
     kr = {}
     for name, (gen, seed, lo, hi) in PROBLEMS.items():
         A = gen()
@@ -43,25 +56,44 @@ def main():
         kr[f"{name}/colidx"] = A.colidx
         kr[f"{name}/val"] = A.val
         kr[f"{name}/rhs"] = b
-        for m in METHODS:
+        for m in methods:
             sym = name.startswith(("p2d", "p3d", "vc3d"))
-            if m in ("cg", "cgm") and not sym:
+            if m in ("cg", "cgm", "icg", "icgm") and not sym:
                 continue
             x, rv, used = oracle.ref_solve(m, A, b, tol=1e-9, maxiter=400, restart=20)
             kr[f"{name}/{m}/x"] = x
             kr[f"{name}/{m}/resvec"] = rv
             kr[f"{name}/{m}/usediter"] = np.array(used)
-    np.savez_compressed(os.path.join(HERE, "krylov_jacobi.npz"), **kr)
-    il = {}
-    for name, (gen, _, _, _) in PROBLEMS.items():
+    return kr
+
+
+def factor_values(matrices, values):
+    out = {}
+    for name, gen in matrices.items():
         A = gen()
-        il[f"{name}/rowptr"] = A.rowptr
-        il[f"{name}/colidx"] = A.colidx
-        il[f"{name}/val"] = A.val
-        il[f"{name}/luv"] = oracle.ref_ilu0_values(A)
-    np.savez_compressed(os.path.join(HERE, "ilu0.npz"), **il)
-    print("wrote", sorted(os.listdir(HERE)))
+        out[f"{name}/rowptr"] = A.rowptr
+        out[f"{name}/colidx"] = A.colidx
+        out[f"{name}/val"] = A.val
+        out[f"{name}/luv"] = values(A)
+    return out
+
+
+FILES = {
+    "krylov_jacobi.npz": lambda: krylov(METHODS),
+    "ilu0.npz": lambda: factor_values({k: v[0] for k, v in PROBLEMS.items()}, oracle.ref_ilu0_values),
+    "krylov_single_reduction.npz": lambda: krylov(SINGLE_REDUCTION),
+    "ic0.npz": lambda: factor_values(IC0_MATRICES, oracle.ref_ic0_values),
+}
+
+
+def main(names):
+    oracle.build(ref=True)
+    if oracle.ref_intel() is None:
+        raise SystemExit("reference not built (needs the reference sources)")
+    for fname in names or FILES:
+        np.savez_compressed(os.path.join(HERE, fname), **FILES[fname]())
+        print("wrote", fname)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -66,6 +66,35 @@ def test_ilu0_restatement_bitwise_vs_golden():
         assert np.array_equal(oracle.ilu0_values(A), z[f"{nm}/luv"]), nm
 
 
+@pytest.mark.parametrize("method", ["icg", "icgm", "ibicgstab"])
+def test_single_reduction_restatement_bitwise_vs_golden(method):
+    """icg / icgm / ibicgstab with Jacobi against the compiled reference's
+    recorded outputs (tests/golden/krylov_single_reduction.npz)."""
+    z = _load("krylov_single_reduction.npz")
+    seen = 0
+    for nm, A in _problems(z):
+        key = f"{nm}/{method}/x"
+        if key not in z.files:
+            continue
+        x, rv, used = oracle.solve(method, A, z[f"{nm}/rhs"], tol=1e-9, maxiter=400, restart=20, pc="jacobi")
+        assert used == int(z[f"{nm}/{method}/usediter"]), (nm, method)
+        assert np.array_equal(x, z[key]), (nm, method)
+        assert np.array_equal(rv, z[f"{nm}/{method}/resvec"][: len(rv)]), (nm, method)
+        seen += 1
+    assert seen >= 3
+
+
+def test_ic0_restatement_bitwise_vs_golden():
+    """IC(0) against the compiled reference's ic0_csr_A recorded in
+    tests/golden/ic0.npz (Precond_ic0 defaults)."""
+    z = _load("ic0.npz")
+    seen = 0
+    for nm, A in _problems(z):
+        assert np.array_equal(oracle.ic0_values(A), z[f"{nm}/luv"]), nm
+        seen += 1
+    assert seen == 4
+
+
 @pytest.mark.skipif(oracle.ref_intel() is None, reason="compiled reference not present")
 @pytest.mark.parametrize("method", ["cg", "cgm", "icg", "icgm", "bicgstab", "ibicgstab", "gcr", "igcr", "gmres", "fgmres"])
 def test_krylov_restatement_bitwise_vs_compiled_reference(method):
