@@ -42,7 +42,7 @@ class CSRMatrix:
 
     @property
     def nnz(self):
-        return int(self.rowptr[-1])
+        return int(self.rowptr[-1] - self.rowptr[0])  # rowptr[0] is the index base (0 or 1)
 
     def to_scipy(self):
         import scipy.sparse as sp
