@@ -108,6 +108,38 @@ def test_krylov_restatement_bitwise_vs_compiled_reference(method):
         assert np.array_equal(rr[: len(ro)], ro)
 
 
+EDGE_CASES = {
+    # zero right-hand side (res0 = 0), a single iteration, a restart longer
+    # than the iteration budget, and a non-zero initial guess
+    "zero-b": (lambda n: np.zeros(n), None, dict(tol=1e-8, maxiter=50, restart=10)),
+    "maxiter1": (lambda n: st.rhs_uniform(n, 1), None, dict(tol=1e-8, maxiter=1, restart=10)),
+    "restart>maxiter": (lambda n: st.rhs_uniform(n, 2), None, dict(tol=1e-8, maxiter=7, restart=30)),
+    "x0": (lambda n: st.rhs_uniform(n, 3), lambda n: st.rhs_uniform(n, 9), dict(tol=1e-8, maxiter=40, restart=5)),
+}
+
+
+@pytest.mark.skipif(oracle.ref_intel() is None, reason="compiled reference not present")
+@pytest.mark.parametrize("case", sorted(EDGE_CASES))
+@pytest.mark.parametrize("method", ["cg", "cgm", "icg", "icgm", "bicgstab", "ibicgstab", "gcr", "igcr", "gmres", "fgmres"])
+def test_krylov_restatement_edge_cases_vs_compiled_reference(method, case):
+    """The restated intel/ loops equal the compiled ones bitwise on the
+    edge cases a caller can hit: count, solution and (outside GMRES's
+    inner-index history) the residual history."""
+    rhs, x0f, kw = EDGE_CASES[case]
+    mats = [st.poisson2d_5pt(12)]
+    if method not in ("cg", "cgm", "icg", "icgm"):
+        mats.append(st.convdiff3d_27pt(5, pe=5.0))
+    for A in mats:
+        b = rhs(A.n)
+        x0 = x0f(A.n) if x0f else None
+        xr, rr, ur = oracle.ref_solve(method, A, b, x0=x0, **kw)
+        xo, ro, uo = oracle.solve(method, A, b, x0=x0, pc="jacobi", **kw)
+        assert ur == uo, (A.name, ur, uo)
+        assert np.array_equal(xr, xo), A.name
+        if method not in ("gmres", "fgmres"):
+            assert np.array_equal(rr[: len(ro)], ro), A.name
+
+
 @pytest.mark.skipif(oracle.ref_ilu0() is None, reason="compiled reference not present")
 def test_ilu0_restatement_bitwise_vs_compiled_reference():
     for A in (st.convdiff3d_27pt(6, pe=5.0), st.varcoef3d_7pt(7, 9), st.poisson2d_5pt(13)):
