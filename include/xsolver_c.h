@@ -129,7 +129,10 @@ void xsolver_set_compat(int reference_quirks);
  * with the transposed SpMV and transposed triangular solves, then
  * dLdb = lambda and dLdA_vals[k] = -lambda_i * x_j for each stored entry
  * k = (i, j) of A (in A's CSR order).  Any output may be NULL.
- * The backward solve uses the forward solver type, tolerance and maxiter. */
+ * The backward solve uses the forward solver type, tolerance and maxiter.
+ * XS_ERR_ORDER when there is no solution to differentiate through: no
+ * solve yet, the last solve ended with an error, or the values changed
+ * since (xs_mat_update / gpu_mat_update). */
 void xsolver_adjoint(double *dLdx, double *dLdb, double *dLdA_vals);
 
 /* ------------------------------------------------------------------ */

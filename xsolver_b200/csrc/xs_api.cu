@@ -518,6 +518,7 @@ static void update_values(Handle &h, const double *v)
     }
     XS_CUDA(cudaStreamSynchronize(h.s));
     h.adj.reset();
+    h.have_solution = false;  // the last solution solved the old values
     invalidate_pc(h);
 }
 
@@ -1149,9 +1150,14 @@ static void solve_device(Handle &h, const double *d_b, double *d_x)
         XS_CUDA(cudaMemsetAsync(h.W.ticket.p, 0, sizeof(unsigned), h.s));
         XS_CUDA(cudaStreamSynchronize(h.s));
     }
+    // only a solve that ended without an error is one the adjoint may
+    // differentiate through
+    if (e) {
+        h.have_solution = false;
+        throw Status(dev_err_to_status(e));
+    }
     h.have_solution = true;
     adjoint_record_solution(h.adj, h.s, n, x);
-    if (e) throw Status(dev_err_to_status(e));
 }
 
 static void solve_host(Handle &h, const double *rhs, double *sol)
