@@ -444,7 +444,8 @@ static void set_matrix(Handle &h, int n, const int *rp, const int *ci, const dou
             }
             std::vector<std::pair<int, long>> e;
             for (int k = hrp[i]; k < hrp[i + 1]; k++) e.emplace_back(hci[k], (long)k);
-            std::sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.first < b.first; });
+            // stable: entries with the same column keep the caller's order
+            std::stable_sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.first < b.first; });
             for (size_t q = 0; q < e.size(); q++) {
                 hci[hrp[i] + q] = e[q].first;
                 hv[hrp[i] + q] = v[e[q].second];
@@ -1940,7 +1941,7 @@ static void mcsr_to_csr(std::vector<int> &rp, std::vector<int> &ci, std::vector<
         std::vector<std::pair<int, double>> e;
         for (int k = g_mc.offrp[i] - base; k < g_mc.offrp[i + 1] - base; k++) e.emplace_back(g_mc.offci[k] - base, g_mc.offv[k]);
         e.emplace_back(i, g_mc.diag[i]);
-        std::sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.first < b.first; });
+        std::stable_sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.first < b.first; });
         for (auto &q : e) {
             ci.push_back(q.first);
             v.push_back(q.second);
