@@ -190,7 +190,11 @@ int xs_last_outer_steps(xs_handle_t h, int *outer_steps);
 /* 2. reference cuda/ + intel/ Fortran-style API                       */
 /* ------------------------------------------------------------------ */
 /* intel/HostMatrix.h:187-195 (also cuda/HostMatrix.h): "diag + off-diagonal"
- * matrix, 0-based, borrowed host pointers.  nHalo must be 0 (one GPU). */
+ * matrix; 0- or 1-based (offdiag_row_offset[0] selects); borrowed host
+ * pointers, read by gpu_mat_setup / gpu_mat_update as in the reference.
+ * nHalo must be 0 (one GPU).  nSizes, when > 0, is the number of
+ * off-diagonal entries: row offsets that decrease or pass it are refused
+ * (XS_ERR_INVALID) at gpu_mat_setup. */
 void cpu_mat_setup(int *nInterior, int *nHalo, int *nSizes, double *diag_val, double *offdiag_val,
                    int *offdiag_row_offset, int *offdiag_col_index);
 /* intel/HostMatrix.h:196-200: new values, same pattern */
@@ -304,7 +308,8 @@ int xs_plan_op_bytes(xs_plan_t p, int op, double *bytes);
  * files store value at (i, j) and (j, i); columns within a row keep the
  * file's order.  reference_quirks = 0 keeps general files' values as
  * written.  Real, double and integer fields; complex, pattern and
- * skew-symmetric files give XS_ERR_UNSUPPORTED, malformed files
+ * skew-symmetric files give XS_ERR_UNSUPPORTED; malformed files, symmetric
+ * files that are not square and entry counts the file cannot hold give
  * XS_ERR_INVALID. */
 int xs_mm_info(const char *path, int *m, int *n, int *nnz, int *symmetric);
 int xs_mm_read(const char *path, int reference_quirks, int *rowptr, int *colidx, double *val, double *diag);
