@@ -1932,7 +1932,9 @@ static void mcsr_to_csr(std::vector<int> &rp, std::vector<int> &ci, std::vector<
     const int base = g_mc.offrp[0];
     if (base != 0 && base != 1) throw Status(XS_ERR_INVALID);
     // row offsets must not run backwards or past the nSizes off-diagonal
-    // entries the caller's arrays hold (when it states that count)
+    // entries the caller's arrays hold (when it states that count; the
+    // reference's device copy takes exactly nSizes entries,
+    // cuda/DeviceMatrixCSR.h:60-69)
     for (int i = 0; i < n; i++)
         if (g_mc.offrp[i + 1] < g_mc.offrp[i] || (g_mc.nsizes > 0 && g_mc.offrp[i + 1] - base > g_mc.nsizes))
             throw Status(XS_ERR_INVALID);
