@@ -289,3 +289,76 @@ def test_device_pcg_jacobi_single_rank(cuda):
     ok, worst = history_ok(rv, ho, hb)
     assert ok, worst
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
+
+
+def _exchange_worker(rank, ws, port, q):
+    """One-directional coupling: rank 0 only sends, the last rank only
+    receives, the middle rank does both; each rank checks its halo values and
+    its rows of A x against the global product."""
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    from xsolver_b200 import distributed as dd
+    from xsolver_b200.stencils import CSRMatrix
+
+    dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=10))
+    try:
+        n = 12
+        rows, cols, vals = [], [], []
+        for i in range(n):
+            entries = {i: 2.0}
+            if i > 0:
+                entries[i - 1] = -1.0  # reads the previous row (from the rank below at a block edge)
+            if i == n - 1:
+                entries[0] = 0.5  # the last rank also reads from rank 0
+            for c in sorted(entries):
+                rows.append(i), cols.append(c), vals.append(entries[c])
+        rp = np.zeros(n + 1, np.int32)
+        np.cumsum(np.bincount(rows, minlength=n), out=rp[1:])
+        A = CSRMatrix(n, rp, np.array(cols, np.int32), np.array(vals), "bidiagonal+corner")
+        bounds = dd.row_bounds(n, ws)
+        lrp, lci, lv = dd.local_rows(A, bounds, rank)
+        plan = dd.HaloPlan(lrp, lci, bounds, rank, "cpu")
+        xg = 1.5 * np.arange(n) + 1.0
+        aug = torch.zeros(plan.n_local + plan.n_halo, dtype=torch.float64)
+        aug[: plan.n_local] = torch.from_numpy(xg[bounds[rank]:bounds[rank + 1]])
+        plan.exchange(aug)
+        halo_cols = np.unique(lci[(lci < bounds[rank]) | (lci >= bounds[rank + 1])])
+        ok_halo = np.array_equal(aug[plan.n_local:].numpy(), xg[halo_cols])
+        import scipy.sparse as sp
+
+        Aloc = sp.csr_matrix((lv, plan.colidx_aug, plan.rowptr), shape=(plan.n_local, plan.n_local + plan.n_halo))
+        y = Aloc @ aug.numpy()
+        ok_y = np.array_equal(y, (A.to_scipy() @ xg)[bounds[rank]:bounds[rank + 1]])
+        q.put((rank, "ok", ok_halo, ok_y, len(plan.send), len(plan.recv)))
+    except Exception as e:
+        q.put((rank, "error", repr(e), None, None, None))
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:
+            pass
+
+
+def test_one_directional_halo_exchange():
+    import torch.multiprocessing as mp
+
+    ws = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_exchange_worker, args=(r, ws, port, q)) for r in range(ws)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=120) for _ in range(ws)], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+    for rank, status, ok_halo, ok_y, nsend, nrecv in out:
+        assert status == "ok", (rank, ok_halo)
+        assert ok_halo and ok_y, rank
+    # rank 0 sends to ranks 1 and 2 and receives nothing; rank 2 only receives
+    assert (out[0][4], out[0][5]) == (2, 0)
+    assert (out[1][4], out[1][5]) == (1, 1)
+    assert (out[2][4], out[2][5]) == (0, 2)
