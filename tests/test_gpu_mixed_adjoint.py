@@ -137,6 +137,38 @@ def test_adjoint_batch_matches_single(cuda):
         assert np.allclose(DA[k], da, rtol=1e-12, atol=1e-15)
 
 
+def test_adjoint_needs_a_valid_solution(cuda):
+    """XS_ERR_ORDER (8) with no solution to differentiate through: before any
+    solve, after a solve that ended with an error, and after new values
+    replaced the ones the last solve used."""
+    from xsolver_b200.api import Solver, XsError
+
+    A = st.varcoef3d_7pt(6, seed=2)
+    S = Solver(A).ksp_settype("cg").ksp_setoption(1e-12, 500).pc_settype("ilu0")
+    g = st.rhs_uniform(A.n, 1)
+    b = st.rhs_uniform(A.n, 2)
+    with pytest.raises(XsError) as e:
+        S.adjoint(g)
+    assert e.value.code == 8
+    b_nan = b.copy()
+    b_nan[3] = np.nan
+    with pytest.raises(XsError):
+        S.solve(b_nan)
+    with pytest.raises(XsError) as e:
+        S.adjoint(g)
+    assert e.value.code == 8
+    S.solve(b)
+    db, _ = S.adjoint(g)
+    assert np.all(np.isfinite(db))
+    S.mat_update(A.val * 2.0)
+    with pytest.raises(XsError) as e:
+        S.adjoint(g)
+    assert e.value.code == 8
+    S.solve(b)
+    db2, _ = S.adjoint(g)  # A^T doubled: lambda halves
+    assert np.allclose(db2, db / 2.0, rtol=1e-8, atol=1e-14)
+
+
 def test_autograd_function(cuda):
     import torch
     from xsolver_b200.autograd import SparseSolve, configured_solver
