@@ -99,6 +99,41 @@ def test_gpu_api_vs_reference_golden(cuda, method):
     assert done >= 1
 
 
+def test_gmres_budget_ends_cycle_early(cuda):
+    """maxiter 7 < restart 30: the reference's left GMRES then updates with
+    all 30 columns (intel/mpisolver-C-v1.cpp:1065), dividing by an unset
+    Hessenberg diagonal (its solution reaches ~1e15); the GPU updates with the
+    7 it built.  Same count and history as the reference; the solution is the
+    7-column least-squares one (numpy emulation below)."""
+    A = st.convdiff3d_27pt(5, pe=5.0)
+    b = st.rhs_uniform(A.n, 2)
+    x, rv, used, code = _gpu_solve_intel("gmres", A, b, 1e-8, 7, 30)
+    assert code == 0
+    xo, ho, uo, hb, xb = reference_with_bounds("gmres", A, b, tol=1e-8, maxiter=7, restart=30, pc="jacobi")
+    assert used == uo == 7
+    ok, worst = history_ok(rv[:used], ho, hb)
+    assert ok, worst
+    assert np.abs(xo).max() > 1e10  # the reference's own update
+    S = A.to_scipy()
+    minv = 1.0 / (S.diagonal() + 1e-20)
+    r0 = minv * b
+    beta = np.linalg.norm(r0)
+    V = [r0 / beta]
+    H = np.zeros((8, 7))
+    for i in range(7):
+        w = minv * (S @ V[i])
+        for k in range(i + 1):
+            H[k, i] = w @ V[k]
+            w = w - H[k, i] * V[k]
+        H[i + 1, i] = np.linalg.norm(w)
+        V.append(w / H[i + 1, i])
+    e1 = np.zeros(8)
+    e1[0] = beta
+    y = np.linalg.lstsq(H, e1, rcond=None)[0]
+    xe = sum(y[q] * V[q] for q in range(7))
+    assert np.linalg.norm(x - xe) / np.linalg.norm(xe) < 1e-8
+
+
 @pytest.mark.parametrize("method,tol", [("icg", 1e-6), ("icgm", 1e-6), ("ibicgstab", 1e-10)])
 def test_single_reduction_variants_vs_oracle(cuda, method, tol):
     """icg / icgm / ibicgstab (intel/mpisolver-C-v1.cpp:104-191, 273-363,
