@@ -74,7 +74,7 @@ def test_header_from_c_and_cxx(tmp_path):
     _build("gcc", "c99", C_SRC, tmp_path / "c_prog", tmp_path)
     out = subprocess.run([str(tmp_path / "c_prog"), str(mtx)], check=True, capture_output=True, text=True).stdout.split()
     rc, rm, m, n, nnz, sym, rr = (int(t) for t in out[:7])
-    assert rc in (0, 12)  # XS_OK on a GPU box, XS_ERR_NO_GPU here
+    assert rc in (0, 12)  # XS_OK with a GPU, XS_ERR_NO_GPU without
     assert (rm, m, n, nnz, sym, rr) == (0, 3, 3, 5, 1, 0)  # symmetric file: one off-diagonal mirrored
     assert float(out[7]) == 4.0 and float(out[8]) == 2.5
     assert " ".join(out[9:]) == "no CUDA device"
