@@ -323,15 +323,20 @@ int xs_tri_levels(int n, const int *rowptr, const int *colidx, int upper, int *l
  * z = (L D U')^{-1} x with the factors in the seqilu0 layout (L strict lower
  * CSR with unit diagonal implied, dinv = 1/u_ii, U' = dinv-row-scaled strict
  * upper CSR; natural row order, columns sorted), all device pointers, FP64,
- * enqueued on `stream` (a cudaStream_t, NULL = default stream) and waited
- * for before returning.  For callers that cannot allocate device memory
- * (a pool or allocator that owns all of it, a fixed memory budget after
- * start-up, buffers handed in by the caller only): the scratch lives in a
- * fixed 4 MiB __device__ array that every GPU loading the library holds
- * until exit.  n must be <= 262144 (XS_ERR_CAPACITY otherwise).  Calls that
- * overlap on the GPU share that array and race: serialise them.  The first
- * call on a device looks up the array's address; make it before any stream
- * capture.  Result bitwise equal to xs_plan_lusolve on the same factors. */
+ * enqueued on `stream` (a cudaStream_t, NULL = default stream).  Every call
+ * waits for `stream` (cudaStreamSynchronize) before it returns and reads the
+ * kernels' error word back to the host: XS_ERR_TRSV_TIMEOUT when a row's
+ * dependency was not ready within 1 s.  For callers that cannot allocate
+ * device memory (a pool or allocator that owns all of it, a fixed memory
+ * budget after start-up, buffers handed in by the caller only): the scratch
+ * lives in a fixed 4 MiB __device__ array that every GPU loading the library
+ * holds until exit.  n must be <= 262144 (XS_ERR_CAPACITY otherwise); when
+ * n > 0 every pointer must be non-NULL, also the column and value arrays of
+ * a factor without entries (XS_ERR_INVALID otherwise).  Calls that overlap
+ * on the GPU share that array and race: serialise them.  The first call on a
+ * device looks up the array's address and keeps it; make it before any
+ * stream capture, and do not let calls span a cudaDeviceReset of that
+ * device.  Result bitwise equal to xs_plan_lusolve on the same factors. */
 int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, const double *dinv, const int *urp,
                        const int *uci, const double *uv, const double *x, double *z, void *stream);
 

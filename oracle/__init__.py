@@ -33,7 +33,10 @@ def build(ref: bool = True) -> None:
     """Compile liboracle.so (and the reference libraries when the reference
     sources are present)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    refdir = os.environ.get("XS_REFERENCE_DIR", "/root/reference")
+    # the reference sources: XS_REFERENCE_DIR, else the directory "reference"
+    # beside this repository's root
+    refdir = os.environ.get("XS_REFERENCE_DIR",
+                            os.path.normpath(os.path.join(HERE, "..", "..", "reference")))
     if ref and os.path.isdir(os.path.join(refdir, "intel")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={refdir}"], check=True)
 

@@ -20,8 +20,15 @@
 //     sharing a device) race on the array and must be serialised by the
 //     caller.
 //   * The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     (cudaGetSymbolAddress) with that device current and keeps it for the
+//     rest of the process; make that first call before any stream capture.
+//     The kept address belongs to the device's current context, so calls
+//     must not span a cudaDeviceReset (or any destruction and re-creation of
+//     the primary context) on that device.
+//   * Every call waits for `stream` (cudaStreamSynchronize) before it
+//     returns, and reads the kernels' error word back to the host.
+//   * Every pointer must be a valid device pointer when n > 0, also the
+//     column and value arrays of a factor without entries.
 //
 // The solve itself is the same row computation as the plan-based sync-free
 // solve (L: increasing column, dinv scale, U': decreasing column, separate
@@ -165,7 +172,8 @@ extern "C" int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const d
                                   const int *urp, const int *uci, const double *uv, const double *x, double *z,
                                   void *stream)
 {
-    if (n < 0 || (n > 0 && (!lrp || !urp || !dinv || !x || !z))) return XS_ERR_INVALID;
+    if (n < 0) return XS_ERR_INVALID;
+    if (n > 0 && (!lrp || !lci || !lv || !dinv || !urp || !uci || !uv || !x || !z)) return XS_ERR_INVALID;
     if (n > NA_MAX_ROWS) return XS_ERR_CAPACITY;
     if (n == 0) return XS_OK;
     NaScratch s;
