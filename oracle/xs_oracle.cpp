@@ -38,9 +38,40 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 namespace {
+
+/* Run fn(i) for i in [0, n) on the host's threads (ORC_THREADS overrides
+ * their count), handing out chunks of `chunk` indices from a shared counter.
+ * Used only for loops whose iterations write disjoint outputs from a
+ * read-only snapshot, so results do not depend on the thread count. */
+template <typename F>
+void par_for(int n, int chunk, F fn)
+{
+    int T = (int)std::thread::hardware_concurrency();
+    if (const char *e = getenv("ORC_THREADS")) T = atoi(e);
+    T = std::max(1, std::min(T, 64));
+    if (T == 1 || n <= chunk) {
+        for (int i = 0; i < n; i++) fn(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        while (true) {
+            const int i0 = next.fetch_add(chunk);
+            if (i0 >= n) return;
+            const int i1 = std::min(n, i0 + chunk);
+            for (int i = i0; i < i1; i++) fn(i);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; t++) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+}
 
 /* ---------------- BLAS-1, sequential order ---------------- */
 /* dot-product order: 0 = sequential (the reference's cblas_ddot through the
@@ -657,45 +688,63 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
         /* u_jj from current U (CSR row j, first entry is the diagonal) */
         std::vector<double> udiag(n);
         for (int j = 0; j < n; j++) udiag[j] = U.v[U.rp[j]];
-        /* candidates D */
+        /* candidates D: rows in blocks, each block on one thread into its own
+         * buffers, then concatenated in row order (each row's candidates and
+         * values depend only on the sweep's snapshot, so the result does not
+         * depend on the thread count) */
         CSR D;
         D.n = n;
         D.rp.assign(n + 1, 0);
-        std::vector<int> cols;
-        for (int i = 0; i < n; i++) {
-            cols.clear();
-            for (int k = arp[i]; k < arp[i + 1]; k++) cols.push_back(aci[k]);
-            for (int kl = L.rp[i]; kl < L.rp[i + 1]; kl++) {
-                int k = L.ci[kl];
-                for (int ku = U.rp[k]; ku < U.rp[k + 1]; ku++) cols.push_back(U.ci[ku]);
-            }
-            std::sort(cols.begin(), cols.end());
-            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-            int pl = L.rp[i], pu = U.rp[i];
-            for (int j : cols) {
-                /* existing entries keep their value */
-                while (pl < L.rp[i + 1] && L.ci[pl] < j) pl++;
-                while (pu < U.rp[i + 1] && U.ci[pu] < j) pu++;
-                double d;
-                if (j < i && pl < L.rp[i + 1] && L.ci[pl] == j) d = L.v[pl];
-                else if (j >= i && pu < U.rp[i + 1] && U.ci[pu] == j) d = U.v[pu];
-                else {
-                    /* c = -a_ij + sum_k l_ik u_kj (k ascending, k <= min(i,j)) */
-                    double c = -find_in_row(A, i, j);
-                    int il = L.rp[i], iu = Uc.rp[j];
-                    while (il < L.rp[i + 1] && iu < Uc.rp[j + 1]) {
-                        int lj = L.ci[il], ui = Uc.ci[iu];
-                        if (lj == ui) { c += L.v[il] * Uc.v[iu]; il++; iu++; }
-                        else if (lj < ui) il++;
-                        else iu++;
-                    }
-                    double r = -c;
-                    d = (j < i) ? r / udiag[j] : r;
+        const int nblk = std::max(1, std::min(4096, n / 256));
+        std::vector<std::vector<int>> bci(nblk);
+        std::vector<std::vector<double>> bv(nblk);
+        par_for(nblk, 1, [&](int bk) {
+            const int i0 = (int)((long)n * bk / nblk), i1 = (int)((long)n * (bk + 1) / nblk);
+            std::vector<int> cols;
+            for (int i = i0; i < i1; i++) {
+                cols.clear();
+                for (int k = arp[i]; k < arp[i + 1]; k++) cols.push_back(aci[k]);
+                for (int kl = L.rp[i]; kl < L.rp[i + 1]; kl++) {
+                    int k = L.ci[kl];
+                    for (int ku = U.rp[k]; ku < U.rp[k + 1]; ku++) cols.push_back(U.ci[ku]);
                 }
-                D.ci.push_back(j);
-                D.v.push_back(d);
+                std::sort(cols.begin(), cols.end());
+                cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+                int pl = L.rp[i], pu = U.rp[i];
+                for (int j : cols) {
+                    /* existing entries keep their value */
+                    while (pl < L.rp[i + 1] && L.ci[pl] < j) pl++;
+                    while (pu < U.rp[i + 1] && U.ci[pu] < j) pu++;
+                    double d;
+                    if (j < i && pl < L.rp[i + 1] && L.ci[pl] == j) d = L.v[pl];
+                    else if (j >= i && pu < U.rp[i + 1] && U.ci[pu] == j) d = U.v[pu];
+                    else {
+                        /* c = -a_ij + sum_k l_ik u_kj (k ascending, k <= min(i,j)) */
+                        double c = -find_in_row(A, i, j);
+                        int il = L.rp[i], iu = Uc.rp[j];
+                        while (il < L.rp[i + 1] && iu < Uc.rp[j + 1]) {
+                            int lj = L.ci[il], ui = Uc.ci[iu];
+                            if (lj == ui) { c += L.v[il] * Uc.v[iu]; il++; iu++; }
+                            else if (lj < ui) il++;
+                            else iu++;
+                        }
+                        double r = -c;
+                        d = (j < i) ? r / udiag[j] : r;
+                    }
+                    bci[bk].push_back(j);
+                    bv[bk].push_back(d);
+                }
+                D.rp[i + 1] = (int)cols.size();  /* row length; prefix-summed below */
             }
-            D.rp[i + 1] = (int)D.ci.size();
+        });
+        for (int i = 0; i < n; i++) D.rp[i + 1] += D.rp[i];
+        D.ci.reserve(D.rp[n]);
+        D.v.reserve(D.rp[n]);
+        for (int bk = 0; bk < nblk; bk++) {
+            D.ci.insert(D.ci.end(), bci[bk].begin(), bci[bk].end());
+            D.v.insert(D.v.end(), bv[bk].begin(), bv[bk].end());
+            std::vector<int>().swap(bci[bk]);
+            std::vector<double>().swap(bv[bk]);
         }
         long nnzD = D.rp[n];
         if (getenv("ORC_DEBUG")) fprintf(stderr, "sweep %d rate %g nnzD %ld L %d U %d\n", s, rate, nnzD, L.rp[n], U.rp[n]);
@@ -717,18 +766,20 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
         /* LU sweep (synchronous): new values from the snapshot (L2, U2c) */
         {
             std::vector<double> lnew(L2.v), unew(U2c.v);
-            for (int i = 0; i < n; i++)
+            par_for(n, 1024, [&](int i) {
                 for (int k = L2.rp[i]; k < L2.rp[i + 1]; k++) {
                     int j = L2.ci[k];
                     if (j >= i) continue;
                     double t = sweep_value(A, L2, U2c, i, j);
                     lnew[k] = t / U2c.v[U2c.rp[j + 1] - 1];
                 }
-            for (int j = 0; j < n; j++)
+            });
+            par_for(n, 1024, [&](int j) {
                 for (int k = U2c.rp[j]; k < U2c.rp[j + 1]; k++) {
                     int i = U2c.ci[k];
                     unew[k] = sweep_value(A, L2, U2c, i, j);
                 }
+            });
             L2.v.swap(lnew);
             U2c.v.swap(unew);
         }
@@ -783,20 +834,22 @@ int orc_parilut(int n, const int *arp, const int *aci, const double *av, double 
         /* L sweep, then U sweep with the new L */
         {
             std::vector<double> lnew(L3.v);
-            for (int i = 0; i < n; i++)
+            par_for(n, 1024, [&](int i) {
                 for (int k = L3.rp[i]; k < L3.rp[i + 1]; k++) {
                     int j = L3.ci[k];
                     if (j >= i) continue;
                     double t = sweep_value(A, L3, U3c, i, j);
                     lnew[k] = t / U3c.v[U3c.rp[j + 1] - 1];
                 }
+            });
             L3.v.swap(lnew);
             std::vector<double> unew(U3c.v);
-            for (int j = 0; j < n; j++)
+            par_for(n, 1024, [&](int j) {
                 for (int k = U3c.rp[j]; k < U3c.rp[j + 1]; k++) {
                     int i = U3c.ci[k];
                     unew[k] = sweep_value(A, L3, U3c, i, j);
                 }
+            });
             U3c.v.swap(unew);
         }
         L = L3;

@@ -88,3 +88,17 @@ def count_ok(used, u_seq, urange):
     """Iteration count within +-1 of the sequential reference, or within the
     range the reference itself spans over the dot orders (+-1)."""
     return abs(used - u_seq) <= 1 or urange[0] - 1 <= used <= urange[1] + 1
+
+
+def strict_report(h_gpu, h_ref, scale=1.0):
+    """The north-star bound itself: (fraction of the compared iterations whose
+    relative difference is within 1e-10, worst relative difference / 1e-10),
+    over iterations where the reference value is above 1e3*eps*scale."""
+    m = min(len(h_gpu), len(h_ref))
+    mask = np.abs(h_ref[:m]) > 1e3 * EPS * scale
+    if not mask.any():
+        return 1.0, 0.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d = np.abs(h_gpu[:m] - h_ref[:m]) / np.abs(h_ref[:m])
+    d = d[mask]
+    return float(np.mean(d <= STRICT)), float(d.max() / STRICT)
