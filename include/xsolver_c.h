@@ -319,6 +319,24 @@ int xs_mm_read(const char *path, int reference_quirks, int *rowptr, int *colidx,
  * rows sorted by (level, row) — the position order of the sync-free solve. */
 int xs_tri_levels(int n, const int *rowptr, const int *colidx, int upper, int *level, int *perm, int *nlevels);
 
+/* Host-only box analysis of a strictly triangular CSR pattern (no GPU
+ * needed; no counterpart in the reference: it is the schedule the exact
+ * triangular solves use in place of hip/Precond/gpuparilu.cpp:257-364's
+ * row-per-thread flags on grid-shaped patterns).  Finds a grid nx*ny*nz = n
+ * on which every dependency lies within 2 steps per direction, the smallest
+ * shear (x' = x + a*y + b*z, y' = y + c*z) that makes every dependency point
+ * to smaller or equal sheared coordinates, and cuts the sheared grid into
+ * boxes of tx*ty*tz.  info[12] = {fits, nx, ny, nz, a, b, c, boxes, internal
+ * levels, halo entries, largest box, largest halo}; when fits is 0 nothing
+ * else is written.  Optional outputs (NULL to skip): perm[n] (position ->
+ * row: boxes in wavefront order, then internal level, then row order),
+ * prp[n+1], pci[nnz] (each dependency as a shared-memory slot: [0, rows of
+ * the box) the box's own positions, then its halo), tile_pos[boxes+1],
+ * tile_lvl[boxes+1], lvl_ptr[levels+1], halo_ptr[boxes+1],
+ * halo_row[halo entries]. */
+int xs_tri_tiles(int n, const int *rowptr, const int *colidx, int upper, int tx, int ty, int tz, int *info, int *perm,
+                 int *prp, int *pci, int *tile_pos, int *tile_lvl, int *lvl_ptr, int *halo_ptr, int *halo_row);
+
 /* LU solve that allocates nothing (no counterpart in the reference).
  * z = (L D U')^{-1} x with the factors in the seqilu0 layout (L strict lower
  * CSR with unit diagonal implied, dinv = 1/u_ii, U' = dinv-row-scaled strict
@@ -352,6 +370,16 @@ int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, 
  * XS_TRSV_BACKOFF_NS, XS_TRSV_CHUNK_ROWS override them at first use.  The
  * layout is fixed when a preconditioner is built: set before factorising. */
 int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
+/* Box-scheduled exact triangular solves (see xs_tri_tiles): enable = 1
+ * (default) uses them for triangles of at least min_rows rows (default
+ * 65536, at least 8) whose pattern fits a grid, with boxes of tx*ty*tz
+ * sheared grid steps (default 16*16*16, halved along the longest side until
+ * a box and its halo fit in shared memory); 0 keeps the level-ordered solve
+ * (the other arguments are then ignored).  Results are bitwise identical
+ * either way.  Environment XS_TRSV_TILES ("0" or "tx,ty,tz") and
+ * XS_TRSV_TILE_MIN_ROWS set it at first use.  Fixed when a preconditioner is
+ * built: set before factorising. */
+int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows);
 /* Exact LU solves of systems with at most max_rows rows, whose solution
  * vector fits in one SM's shared memory (FP64: 25600 rows), run in one CTA
  * that walks the dependency levels with a block barrier between them

@@ -66,6 +66,20 @@ def test_c2_ilu0_factors_bitwise(cuda, c2):
         assert np.array_equal(G[k], getattr(F, k)), k
 
 
+def test_c2_lusolve_bitwise(cuda, c2):
+    """The exact ILU(0) solve at full size (box-scheduled by default on this
+    grid) equals the oracle's LUsolve bit for bit."""
+    import torch
+    from xsolver_b200.api import Plan
+
+    A, b, F, _, _ = c2
+    P = Plan(A).factor("ilu0")
+    z = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    P.lusolve(torch.from_numpy(b).cuda(), z)
+    P.sync()
+    assert np.array_equal(z.cpu().numpy(), oracle.lusolve(F, b))
+
+
 @pytest.mark.parametrize("fmt", ["csr", "ell"])
 def test_c2_fp64_bicgstab_ilu0_vs_reference(cuda, c2, fmt):
     from xsolver_b200.api import Solver

@@ -95,6 +95,9 @@ def _declare(L):
         "xs_mm_info": [C.c_char_p, _ip, _ip, _ip, _ip],
         "xs_mm_read": [C.c_char_p, C.c_int, _ip, _ip, _dp, _dp],
         "xs_set_trsv_tuning": [C.c_int, C.c_int, C.c_int],
+        "xs_set_trsv_tiles": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
+        "xs_tri_tiles": [C.c_int, _ip, _ip, C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip, _ip, _ip,
+                         _ip, _ip],
         "xs_set_ell_index_bits": [C.c_int],
         "xs_set_trsv_block_rows": [C.c_int],
         "xs_set_sweep_fusion": [C.c_int],

@@ -68,6 +68,25 @@ FormatTuning &format_tuning()
     return t;
 }
 
+TileTuning &tile_tuning()
+{
+    static TileTuning t;
+    static bool init = false;
+    if (!init) {
+        // XS_TRSV_TILES: "0" keeps the level-ordered solve; "tx,ty,tz" sets the box size
+        if (const char *e = getenv("XS_TRSV_TILES")) {
+            int a = 0, b = 0, c = 0;
+            const int k = sscanf(e, "%d,%d,%d", &a, &b, &c);
+            if (k == 1 && a == 0) t.enable = 0;
+            else if (k == 3 && a > 0 && b > 0 && c > 0) { t.tx = a; t.ty = b; t.tz = c; }
+        }
+        if (const char *e = getenv("XS_TRSV_TILE_MIN_ROWS")) t.min_rows = std::max(8, atoi(e));
+        if (const char *e = getenv("XS_TRSV_TILE_BLOCKS_PER_SM")) t.blocks_per_sm = std::max(1, atoi(e));
+        init = true;
+    }
+    return t;
+}
+
 TrsvTuning &trsv_tuning()
 {
     static TrsvTuning t;
@@ -688,7 +707,7 @@ static void factor_ic0(Handle &h)
         h.ilu_epoch = 1;
     }
     const int gl = std::min((n + 127) / 128, geom().sms);
-    k_ic0_rows<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.ic0_tnorm.p, IC0_SMALLNUM,
+    k_ic0_rows<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.level_perm(), h.ic0_tnorm.p, IC0_SMALLNUM,
                                     IC0_DROPTOL, h.luv.p, h.flags.p, h.ilu_epoch, h.err.p, h.fticket.p, 512);
     check_launch();
     int e = 0;
@@ -744,7 +763,7 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
             const int bps = ilu_bps_env ? ilu_bps_env : (G <= 8 ? 4 : 8);
             const int gl = std::min((n + rpb - 1) / rpb, geom().sms * bps);
             auto go = [&](auto kern) {
-                kern<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.luv.p, h.flags.p,
+                kern<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.level_perm(), h.luv.p, h.flags.p,
                                           h.ilu_epoch, h.err.p, h.fticket.p, ilu_backoff);
             };
             if (G == 4) go(k_ilu0_groups<4>);
@@ -753,7 +772,7 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
             else go(k_ilu0_groups<32>);
         } else {
             const int gl = std::min((n + 127) / 128, geom().sms * (ilu_bps_env ? ilu_bps_env : 1));
-            k_ilu0_rows<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.perm.p, h.luv.p, h.flags.p,
+            k_ilu0_rows<<<gl, 128, 0, h.s>>>(n, h.A.rp.p, h.A.ci.p, h.uptr.p, h.M.L.level_perm(), h.luv.p, h.flags.p,
                                              h.ilu_epoch, h.err.p, h.fticket.p, ilu_backoff);
         }
         check_launch();
@@ -1494,6 +1513,48 @@ int xs_tri_levels(int n, const int *rp, const int *ci, int upper, int *level, in
         if (level) std::memcpy(level, P.level.data(), sizeof(int) * n);
         if (perm) std::memcpy(perm, P.perm.data(), sizeof(int) * n);
         if (nlevels) *nlevels = P.nlevels;
+    });
+}
+
+int xs_tri_tiles(int n, const int *rp, const int *ci, int upper, int tx, int ty, int tz, int *info, int *perm,
+                 int *prp, int *pci, int *tile_pos, int *tile_lvl, int *lvl_ptr, int *halo_ptr, int *halo_row)
+{
+    return guarded([&] {
+        if (n < 0 || !rp || !info || (!ci && n > 0 && rp[n] > 0) || tx < 1 || ty < 1 || tz < 1)
+            throw Status(XS_ERR_INVALID);
+        TileTuning tt;
+        tt.tx = tx; tt.ty = ty; tt.tz = tz;
+        TileHostPlan P;
+        const bool ok = tri_analyse_tiles(n, rp, ci, upper != 0, [](int k) { return (long)k; }, tt, P);
+        std::memset(info, 0, sizeof(int) * 12);
+        info[0] = ok ? 1 : 0;
+        if (!ok) return;
+        info[1] = P.nx; info[2] = P.ny; info[3] = P.nz;
+        info[4] = P.sa; info[5] = P.sb; info[6] = P.sc;
+        info[7] = P.ntiles;
+        info[8] = (int)P.lvl_ptr.size() - 1;
+        info[9] = (int)P.halo_row.size();
+        info[10] = P.max_rows;
+        info[11] = P.max_halo;
+        auto put = [](int *dst, const std::vector<int> &v) {
+            if (dst && !v.empty()) std::memcpy(dst, v.data(), sizeof(int) * v.size());
+        };
+        put(perm, P.perm); put(prp, P.prp); put(pci, P.pci); put(tile_pos, P.tile_pos);
+        put(tile_lvl, P.tile_lvl); put(lvl_ptr, P.lvl_ptr); put(halo_ptr, P.halo_ptr); put(halo_row, P.halo_row);
+    });
+}
+
+int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows)
+{
+    return guarded([&] {
+        if (enable && (tx < 1 || ty < 1 || tz < 1 || min_rows < 8)) throw Status(XS_ERR_INVALID);
+        tile_tuning().enable = enable != 0;
+        if (enable) {
+            tile_tuning().tx = tx;
+            tile_tuning().ty = ty;
+            tile_tuning().tz = tz;
+            tile_tuning().min_rows = min_rows;
+        }
     });
 }
 

@@ -241,6 +241,31 @@ int xs_plan_debug_break_dependency(xs_plan_t p, int position, int enable)
         TriDev &L = h.M.L;
         if (position < 0 || position >= L.n) throw Status(XS_ERR_INVALID);
         XS_CUDA(cudaStreamSynchronize(h.s));
+        if (L.tiled) {
+            // box layout: the box holding `position` waits for one of its own
+            // rows as if it were a halo value; that row is published only
+            // after the halo wait, so the wait runs out
+            static thread_local int saved_halo = 0, saved_at = -1;
+            if (enable) {
+                std::vector<int> tp(L.ntiles + 1);
+                XS_CUDA(cudaMemcpy(tp.data(), L.t_pos.p, sizeof(int) * tp.size(), cudaMemcpyDeviceToHost));
+                const int t = (int)(std::upper_bound(tp.begin(), tp.end(), position) - tp.begin()) - 1;
+                int hr[2];
+                XS_CUDA(cudaMemcpy(hr, L.t_hptr.p + t, sizeof(int) * 2, cudaMemcpyDeviceToHost));
+                if (hr[1] <= hr[0]) throw Status(XS_ERR_INVALID);  // the box reads nothing from earlier boxes
+                int row = 0;
+                XS_CUDA(cudaMemcpy(&row, L.perm.p + position, sizeof(int), cudaMemcpyDeviceToHost));
+                if (saved_at < 0) {
+                    XS_CUDA(cudaMemcpy(&saved_halo, L.t_hrow.p + hr[0], sizeof(int), cudaMemcpyDeviceToHost));
+                    saved_at = hr[0];
+                }
+                XS_CUDA(cudaMemcpy(L.t_hrow.p + saved_at, &row, sizeof(int), cudaMemcpyHostToDevice));
+            } else if (saved_at >= 0) {
+                XS_CUDA(cudaMemcpy(L.t_hrow.p + saved_at, &saved_halo, sizeof(int), cudaMemcpyHostToDevice));
+                saved_at = -1;
+            }
+            return;
+        }
         int k[2];
         XS_CUDA(cudaMemcpy(k, L.prp.p + position, sizeof(int) * 2, cudaMemcpyDeviceToHost));
         if (k[1] <= k[0]) throw Status(XS_ERR_INVALID);  // the row has no dependency to break

@@ -56,6 +56,11 @@ struct CalcT {
 // library is compiled without FMA contraction), FP32: fused.
 __device__ __forceinline__ double msub(double acc, double y, double v) { return acc - y * v; }
 __device__ __forceinline__ float msub(float acc, float y, float v) { return __fmaf_rn(-y, v, acc); }
+}  // namespace xs
+
+#include "xs_trsv_tiles.cuh"  // box-scheduled exact solves (uses msub)
+
+namespace xs {
 
 // Launch tuning of the sync-free solves (host side, process-wide):
 //   blocks_per_sm  persistent blocks per SM (0: one block per 128 positions,
@@ -817,6 +822,18 @@ struct TriDev {
     bool chunked = false;
     int nchunks = 0, ch = 0;
     DBuf<int> lvl_off, lvl_ptr;
+    // tile layout (perm/prp/pci then hold the box-major order, pci = shared-
+    // memory slots); lvperm keeps the dependency-level order for the
+    // factorisation kernels, which take rows in level order
+    bool tiled = false;
+    int ntiles = 0, tile_elems = 0;  // tile_elems: shared-memory values per box (rows + halo)
+    DBuf<int> t_pos, t_lvl, t_lptr, t_hptr, t_hrow, lvperm;
+    const int *level_perm() const { return tiled ? lvperm.p : perm.p; }
+    template <typename FT>
+    TileArgs<FT> targs() const
+    {
+        return TileArgs<FT>{n, ntiles, t_pos.p, t_lvl.p, t_lptr.p, t_hptr.p, t_hrow.p, perm.p, prp.p, pci.p, vals<FT>()};
+    }
 
     template <typename FT>
     TrsvArgs<FT> args() const;
@@ -925,7 +942,43 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         for (long k = 0; k < T.nnz; k++) ns[k] = src_of((int)k);
         if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
     }
-    if (!T.chunked) {
+    // box layout for patterns on a structured grid (large triangles only);
+    // boxes shrink until the rows and halo of one fit in shared memory
+    TileHostPlan TP;
+    T.tiled = false;
+    T.t_pos.free(); T.t_lvl.free(); T.t_lptr.free(); T.t_hptr.free(); T.t_hrow.free(); T.lvperm.free();
+    if (!T.chunked && tile_tuning().enable && n >= tile_tuning().min_rows) {
+        Trace tr_tile("    box analysis", s);
+        TileTuning tt = tile_tuning();
+        for (int attempt = 0; attempt < 6; attempt++) {
+            TP = TileHostPlan();
+            if (!tri_analyse_tiles(n, rp.data(), ci.data(), upper, src_of, tt, TP)) break;
+            if ((size_t)(TP.max_rows + TP.max_halo) * sizeof(double) <= TILE_SMEM_MAX) {
+                T.tiled = true;
+                break;
+            }
+            int &big = tt.tx >= tt.ty && tt.tx >= tt.tz ? tt.tx : (tt.ty >= tt.tz ? tt.ty : tt.tz);
+            if (big <= 2) break;
+            big /= 2;
+        }
+    }
+    if (T.tiled) {
+        T.ntiles = TP.ntiles;
+        T.tile_elems = TP.max_rows + TP.max_halo;
+        T.perm.alloc(n); T.perm.upload(TP.perm.data(), n, s);
+        T.prp.alloc(n + 1); T.prp.upload(TP.prp.data(), n + 1, s);
+        T.pci.alloc(m); if (T.nnz) T.pci.upload(TP.pci.data(), T.nnz, s);
+        T.src.alloc(m); if (T.nnz) T.src.upload(TP.src.data(), T.nnz, s);
+        T.t_pos.alloc(TP.tile_pos.size()); T.t_pos.upload(TP.tile_pos.data(), TP.tile_pos.size(), s);
+        T.t_lvl.alloc(TP.tile_lvl.size()); T.t_lvl.upload(TP.tile_lvl.data(), TP.tile_lvl.size(), s);
+        T.t_lptr.alloc(TP.lvl_ptr.size()); T.t_lptr.upload(TP.lvl_ptr.data(), TP.lvl_ptr.size(), s);
+        T.t_hptr.alloc(TP.halo_ptr.size()); T.t_hptr.upload(TP.halo_ptr.data(), TP.halo_ptr.size(), s);
+        T.t_hrow.alloc(std::max<size_t>(TP.halo_row.size(), 1));
+        if (!TP.halo_row.empty()) T.t_hrow.upload(TP.halo_row.data(), TP.halo_row.size(), s);
+        T.lvperm.alloc(n); T.lvperm.upload(P.perm.data(), n, s);
+        T.lstart.free();
+        XS_CUDA(cudaStreamSynchronize(s));  // the host plans go out of scope
+    } else if (!T.chunked) {
         T.perm.alloc(n); T.perm.upload(P.perm.data(), n, s);
         T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
         T.pci.alloc(m);
@@ -1151,7 +1204,21 @@ inline void launch_trsv(const TriDev &T, const DT *dinv, const VT *rhs, VT *self
                         const int *done_flag, int *err, cudaStream_t s)
 {
     const int bo = trsv_tuning().backoff_ns;
-    if (T.chunked) {
+    if (T.tiled) {
+        static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
+        const size_t smem = (size_t)T.tile_elems * sizeof(VT);
+        if (smem > attr) {
+            XS_CUDA(cudaFuncSetAttribute(k_trsv_tiles<VT, FT, DT, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+            attr = smem;
+        }
+        // resident boxes per SM: the tuning's count, fewer when shared memory limits it
+        const int fit = std::max(1, (int)((220u * 1024u) / std::max<size_t>(smem + 1024, 1)));
+        const int bps = std::max(1, std::min(tile_tuning().blocks_per_sm, fit));
+        const int g = std::min(T.ntiles, geom().sms * bps);
+        k_trsv_tiles<VT, FT, DT, UPPER><<<g, TILE_THREADS, smem, s>>>(T.targs<FT>(), dinv, rhs, self, out_user,
+                                                                     reset_other, done_flag, err, T.ticket.p, bo);
+    } else if (T.chunked) {
         static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
         const size_t smem = (size_t)T.ch * sizeof(VT);
         if (smem > attr) {

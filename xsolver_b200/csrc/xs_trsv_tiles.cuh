@@ -1,0 +1,478 @@
+// Tile-scheduled exact triangular solves for matrices on structured grids.
+//
+// Replaces, for stencil-like patterns, the level-ordered sync-free solve
+// (k_trsv_syncfree) that stands in for the reference's
+// Lcsr_trsv_sync_free / Ucsc_trsv_sync_free (hip/Precond/gpuparilu.cpp:
+// 257-364).  On a natural-order 3D grid the row dependency chain is
+// hundreds of levels deep (382 at 128^3 for the 7-point stencil), and a
+// row-per-thread solve pays one cross-SM hand-off (a store reaching L2, a
+// poll seeing it) per level.  Here one CTA owns a compact box of the grid (a
+// "tile") and resolves every dependency inside the box in shared memory,
+// with a block barrier between the box's internal levels; only the values
+// the box reads from earlier boxes (its "halo") cross SMs, once per box.
+//
+// Grid detection (host, from the triangle's pattern alone): find nx, ny, nz
+// with n = nx*ny*nz such that, with row q at (q % nx, q/nx % ny, q/(nx*ny)),
+// every dependency lies within 8 grid steps in each direction (for the
+// upper triangle q is the reversed row index n-1-row, so dependencies again
+// point to smaller q).  The dependency vectors d = coord(dep) - coord(row)
+// are then sheared, x' = x + a*y + b*z, y' = y + c*z, z' = z, with small
+// (a, b, c) that make every component of every d' <= 0 (7-point: no shear;
+// 27-point: (1, 2, 1); ParILUT fill of the 27-point operator reaches further
+// and needs a larger shear).  Boxes of the sheared grid then depend
+// only on boxes with smaller or equal coordinates, so ordering boxes by
+// wavefront (sum of box coordinates) is a topological order.  A pattern that
+// fits no grid keeps the level-ordered solve.
+//
+// Kernel: persistent CTAs take boxes in that order from a ticket counter (a
+// CTA only waits on boxes taken earlier, by running CTAs: forward progress
+// without co-residency).  A CTA first loads the data of its first rows,
+// then polls its halo values (the NaN sentinel of the solve buffer marks a
+// value not yet published, as in the level-ordered kernel; every wait is
+// bounded) into shared memory, then walks the box's internal levels: each
+// row's dependencies are shared-memory slots, its entries are summed in the
+// same order with the same operations as the CPU reference's LUsolve
+// (hip/HostMatrix/HostMatrixCSR.cpp:385-409), so FP64 results are bitwise
+// identical to the level-ordered solve and to the oracle.
+#pragma once
+#include <algorithm>
+#include <cstring>
+#include <vector>
+#include "xs_internal.cuh"
+
+namespace xs {
+
+// Tile sizes (in sheared grid steps) and when tiles are used: triangles
+// with at least min_rows rows whose pattern fits a grid.  Process-wide;
+// fixed when a preconditioner's triangles are analysed.
+struct TileTuning {
+    int enable = 1;
+    int tx = 16, ty = 16, tz = 16;
+    int min_rows = 65536;
+    int blocks_per_sm = 4;
+};
+TileTuning &tile_tuning();
+
+constexpr int TILE_THREADS = 256;
+constexpr int TILE_PF = 8;  // entries of a row held in registers ahead of its level
+constexpr int TILE_REACH_MAX = 8;  // largest grid step of a dependency in any direction
+constexpr size_t TILE_SMEM_MAX = 200 * 1024;
+
+struct TileHostPlan {
+    int n = 0, ntiles = 0, max_rows = 0, max_halo = 0;
+    int nx = 0, ny = 0, nz = 0, sa = 0, sb = 0, sc = 0;
+    std::vector<int> perm, prp, pci, tile_pos, tile_lvl, lvl_ptr, halo_ptr, halo_row;
+    std::vector<long> src;
+};
+
+// ---------------------------------------------------------------- grid fit
+struct GridCoord {
+    long nx, nxy;
+    void of(long q, int &x, int &y, int &z) const
+    {
+        z = (int)(q / nxy);
+        const long r = q - (long)z * nxy;
+        y = (int)(r / nx);
+        x = (int)(r - (long)y * nx);
+    }
+};
+
+// balanced digits of an offset o = dx + dy*nx + dz*nxy with |d| small
+inline bool offset_fits(long o, long nx, long nxy, int reach)
+{
+    const long dz = (o + (o >= 0 ? nxy / 2 : -nxy / 2)) / nxy;
+    const long r = o - dz * nxy;
+    const long dy = (r + (r >= 0 ? nx / 2 : -nx / 2)) / nx;
+    const long dx = r - dy * nx;
+    return std::labs(dz) <= reach && std::labs(dy) <= reach && std::labs(dx) <= reach;
+}
+
+// Largest coordinate step of any dependency under (nx, nxy), or reach+1 as
+// soon as one exceeds reach; the distinct dependency vectors go to vecs.
+// logical(r) maps a row to its logical index (dependencies at smaller ones).
+template <typename LogF>
+inline int grid_reach(int n, const int *rp, const int *ci, LogF logical, const GridCoord &g, int reach,
+                      std::vector<int> &vecs)
+{
+    const int W = 2 * reach + 1;
+    std::vector<char> seen((size_t)W * W * W, 0);
+    int worst = 0;
+    for (int r = 0; r < n; r++) {
+        int xi, yi, zi;
+        g.of(logical(r), xi, yi, zi);
+        for (int k = rp[r]; k < rp[r + 1]; k++) {
+            int xj, yj, zj;
+            g.of(logical(ci[k]), xj, yj, zj);
+            const int dx = xj - xi, dy = yj - yi, dz = zj - zi;
+            const int m = std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz)));
+            if (m > reach) return reach + 1;
+            worst = std::max(worst, m);
+            seen[((size_t)(dz + reach) * W + (dy + reach)) * W + (dx + reach)] = 1;
+        }
+    }
+    vecs.clear();
+    for (int z = 0; z < W; z++)
+        for (int y = 0; y < W; y++)
+            for (int x = 0; x < W; x++)
+                if (seen[((size_t)z * W + y) * W + x]) {
+                    vecs.push_back(x - reach);
+                    vecs.push_back(y - reach);
+                    vecs.push_back(z - reach);
+                }
+    return worst;
+}
+
+// Tile layout of a strict triangle; false when the pattern fits no grid
+// (the caller then keeps the level-ordered layout).  rp/ci: natural CSR of
+// the strict triangle, 0-based; upper: dependencies on larger rows, entries
+// summed in decreasing column order; src_of(k) maps entry k to the index of
+// its value.
+template <typename SrcF>
+inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, SrcF src_of, const TileTuning &tt,
+                              TileHostPlan &h)
+{
+    const long nnz = rp[n];
+    if (n < 8 || nnz == 0) return false;
+    auto logical = [&](int r) -> long { return upper ? (long)n - 1 - r : (long)r; };
+    // distinct offsets |row - dep| (give up beyond 512 of them)
+    std::vector<long> offs;
+    {
+        const int TAB = 2048;
+        std::vector<long> tab(TAB, -1);
+        int cnt = 0;
+        for (int r = 0; r < n && cnt <= 512; r++)
+            for (int k = rp[r]; k < rp[r + 1]; k++) {
+                const long o = std::labs((long)ci[k] - r);
+                unsigned hsh = (unsigned)((o * 2654435761ul) % TAB);
+                while (tab[hsh] != -1 && tab[hsh] != o) hsh = (hsh + 1) % TAB;
+                if (tab[hsh] == -1) {
+                    tab[hsh] = o;
+                    offs.push_back(o);
+                    if (++cnt > 512) break;
+                }
+            }
+        if (cnt > 512) return false;
+    }
+    std::sort(offs.begin(), offs.end());
+    // try growing reaches: a dependency may lie up to R grid steps away in
+    // each direction (ParILUT fill reaches several steps along x)
+    int best_reach = TILE_REACH_MAX + 1;
+    GridCoord g{0, 0};
+    std::vector<int> vecs, v;
+    for (int R = 2; R <= TILE_REACH_MAX && best_reach > TILE_REACH_MAX; R *= 2) {
+        // the smallest offset beyond a pure x step lies within R of nx
+        long o_y = -1;
+        for (long o : offs)
+            if (o > R) { o_y = o; break; }
+        if (o_y < 0) return false;  // a band of width <= R: nothing to gain
+        struct Cand { long nx, nxy; };
+        std::vector<Cand> cands;
+        for (long nx = std::max<long>(2 * R + 1, o_y - R); nx <= o_y + R; nx++) {
+            if (n % nx) continue;
+            long o_z = -1;
+            for (long o : offs)
+                if (o > R * nx + R) { o_z = o; break; }
+            std::vector<long> nxys;
+            if (o_z < 0) nxys.push_back(n);  // no step beyond y: a 2D grid
+            else
+                for (long dy = -R; dy <= R; dy++)
+                    for (long dx = -R; dx <= R; dx++) nxys.push_back(o_z - dy * nx - dx);
+            for (long nxy : nxys) {
+                if (nxy <= nx || nxy % nx || n % nxy) continue;
+                if (nxy < n && nxy / nx <= 2 * R) continue;  // y extent too small to tell y from z steps
+                bool ok = true;
+                for (long o : offs)
+                    if (!offset_fits(o, nx, nxy, R)) { ok = false; break; }
+                if (ok) cands.push_back({nx, nxy});
+            }
+        }
+        for (const Cand &c : cands) {
+            const GridCoord gc{c.nx, c.nxy};
+            const int r = grid_reach(n, rp, ci, logical, gc, R, v);
+            if (r <= R && r < best_reach) {
+                best_reach = r;
+                g = gc;
+                vecs = v;
+            }
+        }
+    }
+    if (best_reach > TILE_REACH_MAX) return false;
+    // a shear making every dependency vector non-positive, component by
+    // component: c from the vectors that step down in z, then a from those
+    // that stay in their z plane and step down in y, then b (for a fixed a)
+    // from the z steps; each the smallest that works.  Every dependency is
+    // lexicographically smaller in (z, y, x), so such a shear always exists.
+    auto ceil_div = [](int a, int b) { return a >= 0 ? (a + b - 1) / b : -((-a) / b); };  // b > 0
+    int sa = 0, sb = 0, sc = 0;
+    for (size_t q = 0; q < vecs.size(); q += 3) {
+        const int dx = vecs[q], dy = vecs[q + 1], dz = vecs[q + 2];
+        if (dz > 0 || (dz == 0 && dy > 0) || (dz == 0 && dy == 0 && dx >= 0)) return false;
+        if (dz < 0) sc = std::max(sc, ceil_div(dy, -dz));
+        else if (dy < 0) sa = std::max(sa, ceil_div(dx, -dy));
+    }
+    for (size_t q = 0; q < vecs.size(); q += 3) {
+        const int dx = vecs[q], dy = vecs[q + 1], dz = vecs[q + 2];
+        if (dz < 0) sb = std::max(sb, ceil_div(dx + sa * dy, -dz));
+    }
+    h.n = n;
+    h.nx = (int)g.nx;
+    h.ny = (int)(g.nxy / g.nx);
+    h.nz = (int)(n / g.nxy);
+    h.sa = sa; h.sb = sb; h.sc = sc;
+    // tile coordinates of every logical index
+    const int tx = std::max(1, tt.tx), ty = std::max(1, tt.ty), tz = std::max(1, tt.tz);
+    const long X = (long)(h.nx - 1) + (long)sa * (h.ny - 1) + (long)sb * (h.nz - 1) + 1;
+    const long Y = (long)(h.ny - 1) + (long)sc * (h.nz - 1) + 1;
+    const long Z = h.nz;
+    const long ntx = (X + tx - 1) / tx, nty = (Y + ty - 1) / ty, ntz = (Z + tz - 1) / tz;
+    if (ntx * nty * ntz > (1L << 26)) return false;
+    std::vector<int> tile_of(n);  // by logical index: box id in the sheared box grid
+    std::vector<int> cnt((size_t)(ntx * nty * ntz), 0);
+    for (long q = 0; q < n; q++) {
+        int x, y, z;
+        g.of(q, x, y, z);
+        const long xs = x + (long)sa * y + (long)sb * z, ys = y + (long)sc * z;
+        const int id = (int)(((long)(z / tz) * nty + ys / ty) * ntx + xs / tx);
+        tile_of[q] = id;
+        cnt[id]++;
+    }
+    // order the non-empty boxes by wavefront, then z, y, x
+    std::vector<std::pair<long, int>> order;
+    for (long id = 0; id < (long)cnt.size(); id++) {
+        if (!cnt[id]) continue;
+        const long bx = id % ntx, by = (id / ntx) % nty, bz = id / (ntx * nty);
+        order.push_back({((bx + by + bz) << 40) | id, (int)id});
+    }
+    std::sort(order.begin(), order.end());
+    h.ntiles = (int)order.size();
+    std::vector<int> rank_of(cnt.size(), -1);
+    for (int t = 0; t < h.ntiles; t++) rank_of[order[t].second] = t;
+    // rows of each box in increasing logical index (a topological order)
+    std::vector<int> start(h.ntiles + 1, 0);
+    for (int t = 0; t < h.ntiles; t++) start[t + 1] = start[t] + cnt[order[t].second];
+    std::vector<int> byq(n);
+    {
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (long q = 0; q < n; q++) {
+            const int t = rank_of[tile_of[q]];
+            tile_of[q] = t;  // from here on: the box's rank
+            byq[fill[t]++] = (int)q;
+        }
+    }
+    // local levels, then positions: box-major, level-major, logical index
+    std::vector<int> lev(n, 0);  // by logical index
+    auto row_of = [&](long q) -> int { return upper ? (int)(n - 1 - q) : (int)q; };
+    h.perm.assign(n, 0);
+    h.tile_pos.assign(h.ntiles + 1, 0);
+    h.tile_lvl.assign(h.ntiles + 1, 0);
+    h.lvl_ptr.clear();
+    std::vector<int> pos_of(n);  // by row
+    int pos = 0;
+    std::vector<int> lcnt;
+    for (int t = 0; t < h.ntiles; t++) {
+        int maxl = 0;
+        for (int k = start[t]; k < start[t + 1]; k++) {
+            const long q = byq[k];
+            const int r = row_of(q);
+            int l = 0;
+            for (int e = rp[r]; e < rp[r + 1]; e++) {
+                const long qd = logical(ci[e]);
+                if (tile_of[qd] == t) l = std::max(l, lev[qd] + 1);
+            }
+            lev[q] = l;
+            maxl = std::max(maxl, l);
+        }
+        const int nl = maxl + 1;
+        lcnt.assign(nl + 1, 0);
+        for (int k = start[t]; k < start[t + 1]; k++) lcnt[lev[byq[k]] + 1]++;
+        for (int l = 0; l < nl; l++) lcnt[l + 1] += lcnt[l];
+        h.tile_pos[t] = pos;
+        h.tile_lvl[t] = (int)h.lvl_ptr.size();
+        for (int l = 0; l < nl; l++) h.lvl_ptr.push_back(pos + lcnt[l]);
+        for (int k = start[t]; k < start[t + 1]; k++) {
+            const long q = byq[k];
+            const int p = pos + lcnt[lev[q]]++;
+            h.perm[p] = row_of(q);
+            pos_of[row_of(q)] = p;
+        }
+        pos += start[t + 1] - start[t];
+        h.max_rows = std::max(h.max_rows, start[t + 1] - start[t]);
+    }
+    h.tile_pos[h.ntiles] = n;
+    h.tile_lvl[h.ntiles] = (int)h.lvl_ptr.size();
+    h.lvl_ptr.push_back(n);
+    // entries in accumulation order; dependencies as shared-memory slots:
+    // [0, rows) the box's own rows by position, then the box's halo
+    h.prp.assign(n + 1, 0);
+    for (int p = 0; p < n; p++) {
+        const int r = h.perm[p];
+        h.prp[p + 1] = h.prp[p] + (rp[r + 1] - rp[r]);
+    }
+    h.pci.assign(nnz, 0);
+    h.src.assign(nnz, 0);
+    h.halo_ptr.assign(h.ntiles + 1, 0);
+    h.halo_row.clear();
+    std::vector<int> ext;
+    for (int t = 0; t < h.ntiles; t++) {
+        const int p0 = h.tile_pos[t], p1 = h.tile_pos[t + 1], rows = p1 - p0;
+        ext.clear();
+        for (int p = p0; p < p1; p++) {
+            const int r = h.perm[p];
+            for (int e = rp[r]; e < rp[r + 1]; e++)
+                if (tile_of[logical(ci[e])] != t) ext.push_back(ci[e]);
+        }
+        std::sort(ext.begin(), ext.end());
+        ext.erase(std::unique(ext.begin(), ext.end()), ext.end());
+        h.halo_ptr[t] = (int)h.halo_row.size();
+        h.halo_row.insert(h.halo_row.end(), ext.begin(), ext.end());
+        h.max_halo = std::max(h.max_halo, (int)ext.size());
+        for (int p = p0; p < p1; p++) {
+            const int r = h.perm[p];
+            int o = h.prp[p];
+            auto put = [&](int e) {
+                const int d = ci[e];
+                if (tile_of[logical(d)] == t) h.pci[o] = pos_of[d] - p0;
+                else h.pci[o] = rows + (int)(std::lower_bound(ext.begin(), ext.end(), d) - ext.begin());
+                h.src[o] = src_of(e);
+                o++;
+            };
+            if (!upper)
+                for (int e = rp[r]; e < rp[r + 1]; e++) put(e);
+            else
+                for (int e = rp[r + 1] - 1; e >= rp[r]; e--) put(e);
+        }
+    }
+    h.halo_ptr[h.ntiles] = (int)h.halo_row.size();
+    return true;
+}
+
+// ---------------------------------------------------------------- kernel
+template <typename FT>
+struct TileArgs {
+    int n, ntiles;
+    const int *tile_pos;  // ntiles + 1: first position of each box
+    const int *tile_lvl;  // ntiles + 1: first internal level of each box (index into lvl_ptr)
+    const int *lvl_ptr;   // first position of each internal level (+ n at the end)
+    const int *halo_ptr;  // ntiles + 1
+    const int *halo_row;  // rows of earlier boxes that a box reads
+    const int *perm;      // position -> row
+    const int *prp;       // position row pointer
+    const int *pci;       // shared-memory slot of each dependency
+    const FT *pv;
+};
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+struct TileRow {
+    int p = -1, row = 0, k0 = 0, k1 = 0;
+    VT rhsv = 0;
+    DT dv = 0;
+    int c[TILE_PF];
+    VT f[TILE_PF];
+    __device__ __forceinline__ void load(const TileArgs<FT> &P, const DT *dinv, const VT *rhs, int pos)
+    {
+        p = pos;
+        row = __ldg(P.perm + pos);
+        k0 = __ldg(P.prp + pos);
+        k1 = __ldg(P.prp + pos + 1);
+        rhsv = rhs[row];
+        if (UPPER) dv = __ldg(dinv + pos);
+#pragma unroll
+        for (int j = 0; j < TILE_PF; j++)
+            if (k0 + j < k1) {
+                c[j] = __ldg(P.pci + k0 + j);
+                f[j] = (VT)FVal<FT>::ld(P.pv, k0 + j);
+            }
+    }
+};
+
+// poll one published value (bounded); false on timeout or a recorded error
+template <typename VT>
+__device__ __forceinline__ bool tile_poll(const VT *p, int *err, int backoff_ns, VT &y)
+{
+    y = ld_poll(p);
+    if (!Sentinel<VT>::is(y)) return true;
+    const unsigned long long t0 = gtimer();
+    unsigned ns = 8;
+    long spins = 0;
+    while (Sentinel<VT>::is(y)) {
+        __nanosleep(ns);
+        if (ns < (unsigned)backoff_ns) ns <<= 1;
+        y = ld_poll(p);
+        if ((++spins & 63) == 0) {
+            if (gtimer() - t0 > WAIT_LIMIT_NS) {
+                atomicOr(err, DEV_TRSV_TIMEOUT);
+                return false;
+            }
+            if (*(volatile int *)err) return false;
+        }
+    }
+    return true;
+}
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+__global__ void __launch_bounds__(TILE_THREADS) k_trsv_tiles(TileArgs<FT> P, const DT *__restrict__ dinv,
+                                                             const VT *rhs, VT *self, VT *out_user, VT *reset_other,
+                                                             const int *done_flag, int *err, unsigned *ticket,
+                                                             int backoff_ns)
+{
+    if (done_flag && *done_flag) return;
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    VT *ysh = (VT *)tile_smem;
+    __shared__ int s_tile;
+    const unsigned last = (unsigned)P.ntiles + gridDim.x - 1;
+    bool ok = true;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            if (t == last) *ticket = 0u;  // every CTA has drawn its final ticket
+            s_tile = (int)t;
+        }
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= P.ntiles) break;
+        const int p0 = __ldg(P.tile_pos + t), p1 = __ldg(P.tile_pos + t + 1);
+        const int l0 = __ldg(P.tile_lvl + t), l1 = __ldg(P.tile_lvl + t + 1);
+        const int h0 = __ldg(P.halo_ptr + t), h1 = __ldg(P.halo_ptr + t + 1);
+        const int rows = p1 - p0;
+        // the first level's row data (HBM) is in flight while the halo is polled
+        TileRow<VT, FT, DT, UPPER> cur, nxt;
+        {
+            const int pos = __ldg(P.lvl_ptr + l0) + (int)threadIdx.x;
+            if (pos < __ldg(P.lvl_ptr + l0 + 1)) cur.load(P, dinv, rhs, pos);
+        }
+        for (int k = h0 + (int)threadIdx.x; k < h1; k += TILE_THREADS) {
+            VT y = (VT)0;
+            if (ok) ok = tile_poll<VT>(self + __ldg(P.halo_row + k), err, backoff_ns, y);
+            ysh[rows + (k - h0)] = y;
+        }
+        __syncthreads();
+        for (int l = l0; l < l1; l++) {
+            const int pa = __ldg(P.lvl_ptr + l), pb = __ldg(P.lvl_ptr + l + 1);
+            nxt.p = -1;
+            if (l + 1 < l1) {
+                const int pos = pb + (int)threadIdx.x;
+                if (pos < __ldg(P.lvl_ptr + l + 2)) nxt.load(P, dinv, rhs, pos);
+            }
+            for (int pos = pa + (int)threadIdx.x; pos < pb; pos += TILE_THREADS) {
+                TileRow<VT, FT, DT, UPPER> r;
+                if (pos == cur.p) r = cur;
+                else r.load(P, dinv, rhs, pos);
+                VT acc = UPPER ? (VT)(r.rhsv * (VT)r.dv) : r.rhsv;
+                if (reset_other) reset_other[r.row] = Sentinel<VT>::value();
+#pragma unroll
+                for (int j = 0; j < TILE_PF; j++)
+                    if (r.k0 + j < r.k1) acc = msub(acc, ysh[r.c[j]], r.f[j]);
+                for (int k = r.k0 + TILE_PF; k < r.k1; k++)
+                    acc = msub(acc, ysh[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
+                ysh[pos - p0] = acc;
+                st_publish(self + r.row, acc);
+                if (out_user) out_user[r.row] = acc;
+            }
+            cur = nxt;
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace xs
