@@ -370,6 +370,12 @@ int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, 
  * XS_TRSV_BACKOFF_NS, XS_TRSV_CHUNK_ROWS override them at first use.  The
  * layout is fixed when a preconditioner is built: set before factorising. */
 int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
+/* Vector updates of the Krylov iterations fused into the preconditioner
+ * pass that first reads their result (BiCGSTAB's s = r - gamma*u formed in
+ * the first L pass of a Jacobi-sweep apply with an ELL copy of L): 1
+ * (default) fuses, 0 runs them as separate kernels.  Same results either
+ * way.  Environment XS_VEC_FUSE sets it at first use. */
+int xs_set_vector_fusion(int enable);
 /* Box-scheduled exact triangular solves (see xs_tri_tiles): enable = 1
  * (default) uses them for triangles of at least min_rows rows (default
  * 65536, at least 8) whose pattern fits a grid, with boxes of tx*ty*tz

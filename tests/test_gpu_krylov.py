@@ -412,3 +412,30 @@ def test_launch_overlap_gives_identical_results(cuda):
         L.xs_set_launch_overlap(1)
     for a, c in zip(out[:2], out[2:]):
         assert np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1]) and np.array_equal(a[2], c[2])
+
+
+def test_vector_fusion_gives_identical_results(cuda):
+    """BiCGSTAB's s = r - gamma*u formed inside the first L sweep pass of the
+    second preconditioner apply computes the same values as the separate
+    vector update: FP64 and mixed solves are bit-identical either way."""
+    from xsolver_b200 import _lib
+
+    A = st.poisson3d_7pt(40)
+    b = st.rhs_uniform(A.n, 5)
+    L = _lib.lib()
+    out = []
+    try:
+        for on in (1, 0):
+            assert L.xs_set_vector_fusion(on) == 0
+            S = _solver(A, "bicgstab", "ilu0", 1e-10, 500, fmt="ell")
+            S.pc_set_trsv(3)
+            x64 = S.solve(b)
+            h64 = S.resvec()
+            S.set_precision("fp64", "fp32", "bf16").set_refinement_mode(True)
+            xm = S.solve(b)
+            out.append((x64, h64, xm))
+            S.close()
+    finally:
+        L.xs_set_vector_fusion(1)
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)

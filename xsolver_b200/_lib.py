@@ -102,6 +102,7 @@ def _declare(L):
         "xs_set_trsv_block_rows": [C.c_int],
         "xs_set_sweep_fusion": [C.c_int],
         "xs_set_launch_overlap": [C.c_int],
+        "xs_set_vector_fusion": [C.c_int],
         "xs_lusolve_noalloc": [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         "xsolver_last_error": [],
     }

@@ -68,6 +68,15 @@ FormatTuning &format_tuning()
     return t;
 }
 
+bool &vec_fusion_flag()
+{
+    static bool on = [] {
+        const char *e = getenv("XS_VEC_FUSE");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
 TileTuning &tile_tuning()
 {
     static TileTuning t;
@@ -1556,6 +1565,11 @@ int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows)
             tile_tuning().min_rows = min_rows;
         }
     });
+}
+
+int xs_set_vector_fusion(int enable)
+{
+    return guarded([&] { vec_fusion_flag() = enable != 0; });
 }
 
 int xs_device_count(void)

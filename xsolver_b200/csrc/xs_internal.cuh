@@ -119,6 +119,10 @@ struct PdlTuning {
     int enabled = 1;
 };
 PdlTuning &pdl_tuning();
+// vector updates fused into the preconditioner passes that read their
+// result (process-wide; results are identical either way)
+bool &vec_fusion_flag();
+inline bool vec_fusion() { return vec_fusion_flag(); }
 
 template <typename... KArgs, typename... Args>
 inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args)

@@ -746,6 +746,20 @@ struct OpBicgS {
     }
     __device__ void finalize(const double *) const {}
 };
+// s = r - gama u formed inside the first L pass of the preconditioner
+// apply that reads s (the same operations as OpBicgS, so the same values;
+// the pass stores s for the later passes and the next kernels)
+template <typename VT>
+struct SrcBicgS {
+    const VT *r, *u;
+    VT *s;
+    const KState *st;
+    VT mingama;
+    __device__ void load() { mingama = -(VT)st->sc[S_GAMA]; }
+    __device__ VT at(int c) const { return __ldg(r + c) + mingama * __ldg(u + c); }
+    __device__ void put(int i, VT v) const { s[i] = v; }
+};
+
 // x += gama z1 + alpha z2 ; r = s - alpha v ; acc r.r, r.rhat
 template <typename VT>
 struct OpBicgX {

@@ -159,8 +159,38 @@ struct PrecondDev {
     template <typename FT>
     const FT *natvals(const TriDev &T) const;
 
-    template <typename VT, typename FT>
-    void apply_sweeps(const VT *x, VT *z, const int *done_flag, cudaStream_t s)
+    // A vector update can be fused into the first L pass of an apply when
+    // the apply is a Jacobi-sweep solve of at least 2 sweeps whose L copy is
+    // an ELL layout (the pass that reads the right-hand side at neighbours)
+    bool fused_source_ok(int k) const { return k >= 2 && L.ell_w > 0; }
+    bool can_fuse_first_pass() const
+    {
+        return (type == PC_ILU0 || type == PC_PARILU || type == PC_PARILUT || type == PC_IC0) && trsv_mode >= 2 &&
+               fused_source_ok(trsv_mode);
+    }
+
+    // z = M^{-1} x where the first L pass forms x from `src` (x is written
+    // by that pass; see apply_sweeps).  Only when can_fuse_first_pass().
+    template <typename VT, class Src>
+    void apply_fused(const Src &src, const VT *x, VT *z, const int *done_flag, cudaStream_t s)
+    {
+        if (!can_fuse_first_pass()) throw Status(XS_ERR_INVALID);
+        if constexpr (std::is_same<VT, double>::value) apply_sweeps<double, double, Src>(x, z, done_flag, s, &src);
+        else {
+            switch (factor_prec) {
+            case FP_BF16: apply_sweeps<float, __nv_bfloat16, Src>(x, z, done_flag, s, &src); break;
+            case FP_F16: apply_sweeps<float, __half, Src>(x, z, done_flag, s, &src); break;
+            default: apply_sweeps<float, float, Src>(x, z, done_flag, s, &src); break;
+            }
+        }
+        check_launch();
+    }
+
+    // srcL (optional): the first L pass reads its right-hand side from this
+    // source instead of x (a vector update fused into the pass; the source
+    // writes x itself, which the later passes read)
+    template <typename VT, typename FT, class SrcL = SrcVec<VT>>
+    void apply_sweeps(const VT *x, VT *z, const int *done_flag, cudaStream_t s, const SrcL *srcL = nullptr)
     {
         using DT = VT;
         VT *ta, *tb, *tc;
@@ -170,7 +200,8 @@ struct PrecondDev {
         const int g = std::min(geom().sms * ELL_BLOCKS_PER_SM, (n + 255) / 256);
         const int k = trsv_mode;
         // one sweep pass over triangle T: ELL when available, else CSR
-        auto pass = [&](const TriDev &T, bool upper, bool first2, const VT *rhs, const VT *yin, VT *yout) {
+        auto pass = [&](const TriDev &T, bool upper, bool first2, const VT *rhs, const VT *yin, VT *yout,
+                        const SrcL *fused = nullptr) {
             if (T.ell_w > 0) {
                 const FT *ev = T.evals<FT>();
                 if (!ev) throw Status(XS_ERR_ORDER);  // copy not built for this configuration
@@ -181,12 +212,15 @@ struct PrecondDev {
                 auto go = [&](auto cols) {
                     using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
                     const DT *dv = upper ? dinv : (const DT *)nullptr;
+                    const SrcVec<VT> sv{rhs};
                     if (upper) {
-                        if (first2) launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, true, true>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
-                        else launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, true, false>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        if (first2) launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, true, true, SrcVec<VT>>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, sv, yin, yout, done_flag);
+                        else launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, true, false, SrcVec<VT>>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, sv, yin, yout, done_flag);
+                    } else if (fused) {
+                        launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, false, true, SrcL>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, *fused, yin, yout, done_flag);
                     } else {
-                        if (first2) launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, false, true>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
-                        else launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, false, false>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, rhs, yin, yout, done_flag);
+                        if (first2) launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, false, true, SrcVec<VT>>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, sv, yin, yout, done_flag);
+                        else launch_pdl(k_trsv_sweep_ell<VT, FT, DT, CT, false, false, SrcVec<VT>>, dim3(gs), dim3(256), 0, s, n, T.ell_w, cols, doff, ev, dv, sv, yin, yout, done_flag);
                     }
                 };
                 if (T.ell_dia && T.ell_w <= 8) go((const uint8_t *)T.emask8.p);
@@ -206,6 +240,7 @@ struct PrecondDev {
                 else launch_pdl(k_trsv_sweep<VT, FT, DT, false>, dim3(g), dim3(256), 0, s, n, T.rp_nat, T.ci_nat, natvals<FT>(T), (const DT *)nullptr, rhs, yin, yout, 0, done_flag);
             }
         };
+        if (srcL && !fused_source_ok(k)) throw Status(XS_ERR_INVALID);  // callers check first
         if (k <= 1) {
             // L^-1 x ~ x ; U'^-1 (dinv y) ~ dinv y
             k_diag_scale<VT, DT><<<g, 256, 0, s>>>(n, dinv, x, z, done_flag);
@@ -236,7 +271,7 @@ struct PrecondDev {
         auto fusable = [](const TriDev &T) {
             return T.ell_w > 0 && T.ell_dia && T.ell_w <= (sizeof(VT) >= 8 ? 3 : 4);
         };
-        if (k >= 3 && fusable(L) && fusable(U) && trsv_tuning().fuse_sweeps) {
+        if (!srcL && k >= 3 && fusable(L) && fusable(U) && trsv_tuning().fuse_sweeps) {
             VT *cur = ta, *other = tb;
             pass23(L, false, x, cur);
             for (int t = 4; t <= k; t++) {
@@ -253,7 +288,7 @@ struct PrecondDev {
         }
         // L: passes 2..k, result in `cur` (ta or tb)
         VT *cur = ta, *other = tb;
-        pass(L, false, true, x, nullptr, cur);
+        pass(L, false, true, x, nullptr, cur, srcL);
         for (int t = 3; t <= k; t++) {
             pass(L, false, false, x, cur, other);
             std::swap(cur, other);

@@ -328,16 +328,24 @@ struct BicgRun {
             spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
             vecop(OpBicgInit<VT>{n, st, r, rhat, p, u}, sl, c.s);
         }
+        // s = r - gama u inside the second apply's first pass when the
+        // preconditioner allows it (one launch and one pass over s fewer)
+        const bool fuse_s = vec_fusion() && c.M->can_fuse_first_pass();
         auto body = [&]() {
             vecop(OpBicgP<VT>{n, st, p, r, u, (VT)0, (VT)0}, sl, c.s);
             c.M->apply<VT>(p, z1, done, c.s);
             spmv<VT, MT>(*c.A, z1, u, EpiDot1<VT>{st, rhat, 0, M_BICG_GAMA}, sl, c.s);
-            vecop(OpBicgS<VT>{n, st, s, r, u, (VT)0}, sl, c.s);
-            c.M->apply<VT>(s, z2, done, c.s);
+            if (fuse_s) {
+                c.M->apply_fused<VT>(SrcBicgS<VT>{r, u, s, st, (VT)0}, s, z2, done, c.s);
+            } else {
+                vecop(OpBicgS<VT>{n, st, s, r, u, (VT)0}, sl, c.s);
+                c.M->apply<VT>(s, z2, done, c.s);
+            }
             spmv<VT, MT>(*c.A, z2, v, EpiDot2<VT>{st, s, M_BICG_ALPHA}, sl, c.s);
             vecop(OpBicgX<VT>{n, st, x, r, z1, z2, s, v, rhat, (VT)0, (VT)0}, sl, c.s);
         };
-        std::vector<const void *> key{b, x, r, rhat, p, u, s, v, z1, z2, st, c.M, c.A, (const void *)cfg_key(c)};
+        std::vector<const void *> key{b, x, r, rhat, p, u, s, v, z1, z2, st, c.M, c.A, (const void *)cfg_key(c),
+                                      (const void *)(long)fuse_s};
         run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
     }
 };

@@ -378,12 +378,23 @@ __global__ void k_trsv_sweep(int n, const int *__restrict__ rp, const int *__res
     }
 }
 
+// Source of a sweep pass's right-hand side x: a vector (SrcVec), or a value
+// formed on the fly from other vectors (a fused vector update, which also
+// stores the value of each row it owns through put()).
+template <typename VT>
+struct SrcVec {
+    const VT *x;
+    __device__ void load() {}
+    __device__ VT at(int c) const { return __ldg(x + c); }
+    __device__ void put(int, VT) const {}
+};
+
 // C consecutive slots of rows i0..i0+R-1 of a sweep pass: acc -= v * y(c),
 // with y(c) = x[c] (L, first pass), dinv[c]*x[c] (U, first pass) or yin[c].
-template <int C, int R, typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
+template <int C, int R, typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2, class Src>
 __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long ld, int i0, int n, int k0,
                                             const CT (&mask)[R], const int *s_off, const DT *__restrict__ dinv,
-                                            const VT *__restrict__ x, const VT *__restrict__ yin, VT (&acc)[R])
+                                            const Src &x, const VT *__restrict__ yin, VT (&acc)[R])
 {
     FT v[C][R];
     VT y[C][R];
@@ -426,7 +437,7 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
         for (int q = 0; q < R; q++) {
             if (EllDiag<CT>::value || pr[j][q]) {
                 const int cc = col[j][q];
-                if (FIRST2) y[j][q] = UPPER ? (VT)(__ldg(x + cc) * (VT)__ldg(dinv + cc)) : __ldg(x + cc);
+                if (FIRST2) y[j][q] = UPPER ? (VT)(x.at(cc) * (VT)__ldg(dinv + cc)) : x.at(cc);
                 else y[j][q] = __ldg(yin + cc);
             } else {
                 y[j][q] = (VT)0;
@@ -445,12 +456,12 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
 // first sweep is x itself (L) or dinv*x (U), so k sweeps cost k-1 passes.
 // Launch shape as the ELL SpMV (ELL_ROWS rows per thread, ELL_CHUNK slots
 // per load chunk, warp-uniform chunk lengths).
-template <typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2>
+template <typename VT, typename FT, typename DT, typename CT, bool UPPER, bool FIRST2, class Src>
 __global__ void __launch_bounds__(256, sweep_min_blocks_for<FT>()) k_trsv_sweep_ell(int n, int w, const CT *__restrict__ eci,
                                                                          const int *__restrict__ doff,
                                                                          const FT *__restrict__ ev,
                                                                          const DT *__restrict__ dinv,
-                                                                         const VT *__restrict__ x,
+                                                                         Src x,
                                                                          const VT *__restrict__ yin,
                                                                          VT *__restrict__ yout, const int *done_flag)
 {
@@ -460,13 +471,20 @@ __global__ void __launch_bounds__(256, sweep_min_blocks_for<FT>()) k_trsv_sweep_
     pdl_trigger();
     pdl_wait();
     if (done_flag && *done_flag) return;
+    x.load();  // scalars the source needs (after the wait: an earlier kernel computes them)
     const long ld = ell_ld(n);
     for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * R; i0 < n; i0 += gridDim.x * blockDim.x * R) {
         VT acc[R];
 #pragma unroll
         for (int q = 0; q < R; q++) {
             const int i = i0 + q;
-            acc[q] = (R == 1 || i < n) ? (UPPER ? (VT)(x[i] * (VT)dinv[i]) : x[i]) : (VT)0;
+            if (R == 1 || i < n) {
+                const VT xi = x.at(i);
+                x.put(i, xi);
+                acc[q] = UPPER ? (VT)(xi * (VT)dinv[i]) : xi;
+            } else {
+                acc[q] = (VT)0;
+            }
         }
         const CT *cp = eci + i0;
         const FT *vp = ev + i0;
@@ -476,7 +494,7 @@ __global__ void __launch_bounds__(256, sweep_min_blocks_for<FT>()) k_trsv_sweep_
         for (int k0 = 0; k0 < w; k0 += CH) {
             const int m = min(CH, w - k0);  // warp-uniform
 #define XS_SWEEP_CHUNK(CC) \
-    sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2>(cp, vp, ld, i0, n, k0, mask, s_off, dinv, x, yin, acc)
+    sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2, Src>(cp, vp, ld, i0, n, k0, mask, s_off, dinv, x, yin, acc)
             if (m == CH) XS_SWEEP_CHUNK(CH);
             else if (CH > 7 && m == 7) XS_SWEEP_CHUNK(7);
             else if (CH > 6 && m == 6) XS_SWEEP_CHUNK(6);
