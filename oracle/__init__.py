@@ -284,6 +284,37 @@ def parilu_values(A, sweeps=20) -> np.ndarray:
     return out
 
 
+def parilu_inplace_values(A, sweeps=20, order_seed=0) -> np.ndarray:
+    """ParILU with the reference's in-place (asynchronous-style) updates:
+    entries overwritten as they are computed, in A's order (order_seed 0)
+    or a seeded random order per sweep."""
+    out = np.zeros(A.nnz)
+    rc = lib().orc_parilu_inplace(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), C.c_int(sweeps),
+                                  C.c_uint(order_seed), _p(out))
+    if rc != 0:
+        raise ValueError("matrix has a row without a diagonal entry")
+    return out
+
+
+def parilu_inplace(A, sweeps=20, order_seed=0) -> LU:
+    return split_lu(A, parilu_inplace_values(A, sweeps, order_seed))
+
+
+def factor_residual(A, F: LU) -> float:
+    """||(A - L U)|_pattern(A)||_F / ||A||_F for factors in the seqilu0
+    layout (unit L, U = diag(1/dinv) U')."""
+    import scipy.sparse as sp
+
+    n = A.n
+    Ls = sp.csr_matrix((F.lv, F.lci, F.lrp), shape=(n, n)) + sp.identity(n, format="csr")
+    d = 1.0 / F.dinv
+    Us = sp.diags(d) @ sp.csr_matrix((F.uv, F.uci, F.urp), shape=(n, n)) + sp.diags(d)
+    P = (Ls @ Us).tocsr()
+    rows = np.repeat(np.arange(n), np.diff(A.rowptr))
+    lu = np.asarray(P[rows, A.colidx]).ravel()
+    return float(np.linalg.norm(A.val - lu) / np.linalg.norm(A.val))
+
+
 def parilu(A, sweeps=20) -> LU:
     return split_lu(A, parilu_values(A, sweeps))
 

@@ -593,6 +593,82 @@ int orc_parilu(int n, const int *rp, const int *ci, const double *v, int sweeps,
     return 0;
 }
 
+/* ParILU with the reference's own in-place updates (asynchronous-style):
+ * the same entry update as orc_parilu (hip/Precond/gpuparilu.cpp:46-102,
+ * ilu0_ij_aw: merge of L row i and U column j, pivot clamp 1e-10, a
+ * non-finite result keeps the old value), but every entry is overwritten in
+ * place, so later entries of the same sweep read values already updated in
+ * this sweep — the schedule one GPU thread sees when the threads handling
+ * earlier entries have finished (the reference's sweeps run unsynchronised
+ * in place, so any interleaving is a valid outcome).  order_seed 0 updates
+ * the entries in A's order; order_seed > 0 in a fresh pseudo-random order
+ * every sweep (another valid interleaving). */
+int orc_parilu_inplace(int n, const int *rp, const int *ci, const double *v, int sweeps, unsigned order_seed,
+                       double *luv)
+{
+    int nnz = rp[n];
+    std::vector<int> uptr(n, -1), rowof(nnz);
+    for (int i = 0; i < n; i++)
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            rowof[k] = i;
+            if (ci[k] == i) uptr[i] = k;
+        }
+    for (int i = 0; i < n; i++)
+        if (uptr[i] < 0) return -1;
+    std::vector<int> ucp(n + 1, 0), ucpos;
+    for (int k = 0; k < nnz; k++)
+        if (rowof[k] <= ci[k]) ucp[ci[k] + 1]++;
+    for (int j = 0; j < n; j++) ucp[j + 1] += ucp[j];
+    ucpos.resize(ucp[n]);
+    {
+        std::vector<int> pos(ucp.begin(), ucp.end() - 1);
+        for (int k = 0; k < nnz; k++)
+            if (rowof[k] <= ci[k]) ucpos[pos[ci[k]]++] = k;
+    }
+    std::vector<double> cur(v, v + nnz);
+    std::vector<int> order(nnz);
+    for (int k = 0; k < nnz; k++) order[k] = k;
+    unsigned long long rs = 0x9e3779b97f4a7c15ull ^ order_seed;
+    auto rnd = [&]() {
+        rs ^= rs << 13; rs ^= rs >> 7; rs ^= rs << 17;
+        return rs;
+    };
+    for (int s = 0; s < sweeps; s++) {
+        if (order_seed)
+            for (int k = nnz - 1; k > 0; k--) std::swap(order[k], order[(int)(rnd() % (unsigned long long)(k + 1))]);
+        for (int q = 0; q < nnz; q++) {
+            const int k = order[q];
+            int i = rowof[k], j = ci[k];
+            double sacc = v[k], sp = 0.0;
+            int il = rp[i], ilend = uptr[i] + 1;
+            int iu = ucp[j], iuend = ucp[j + 1];
+            while (il < ilend && iu < iuend) {
+                sp = 0.0;
+                int jl = ci[il];
+                int ju = rowof[ucpos[iu]];
+                double lval = (il == uptr[i]) ? 1.0 : cur[il];
+                double uval = cur[ucpos[iu]];
+                sp = (jl == ju) ? lval * uval : sp;
+                sacc = (jl == ju) ? sacc - sp : sacc;
+                il = (jl <= ju) ? il + 1 : il;
+                iu = (jl >= ju) ? iu + 1 : iu;
+            }
+            sacc += sp;
+            if (i > j) {
+                double t = cur[uptr[j]];
+                if (std::fabs(t) < 1e-10) t = (t >= 0 ? 1e-10 : -1e-10);
+                t = sacc / t;
+                if (std::isfinite(t)) cur[k] = t;
+            } else {
+                if (i == j && std::fabs(sacc) < 1e-10) sacc = (sacc >= 0 ? 1e-10 : -1e-10);
+                if (std::isfinite(sacc)) cur[k] = sacc;
+            }
+        }
+    }
+    std::memcpy(luv, cur.data(), sizeof(double) * nnz);
+    return 0;
+}
+
 /* Split combined LU values over A's pattern into (L strict, dinv, U'), the
  * seqilu0 layout.  Sizes as for orc_ilu0. */
 int orc_split_lu(int n, const int *rp, const int *ci, const double *luv,
