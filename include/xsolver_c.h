@@ -169,11 +169,27 @@ int xs_solve(xs_handle_t h, const double *rhs, double *sol);
 /* device-resident rhs/sol (device pointers, n doubles each) */
 int xs_solve_device(xs_handle_t h, const double *d_rhs, double *d_sol);
 /* nrhs independent right-hand sides stored contiguously (column i at
- * rhs + i*n); host pointers.  usediter/resvec of the handle receive the last
- * system's values. */
+ * rhs + i*n); host pointers; sol holds every column's x0 on entry.  New
+ * entry point beside hip/xsolver_c.cpp:274-292 (xsolver_solve, one
+ * right-hand side).  With PCG ("cg"/"cgm") and no, Jacobi or an ILU-family
+ * preconditioner applied by exact triangular solves in FP64, 2..16 columns
+ * iterate together (one pass over the matrix and one triangular-solve
+ * dependency chain serve all of them; every column keeps its own scalars
+ * and stops where its own solve would); otherwise the columns are solved
+ * one after another.  usediter/resvec of the handle receive the last
+ * system's values; xs_batch_iterations gives every column's count. */
 int xs_solve_batch(xs_handle_t h, int nrhs, const double *rhs, double *sol);
+/* iterations of each column of the last batched solve or adjoint (nrhs
+ * must equal that call's nrhs) */
+int xs_batch_iterations(xs_handle_t h, int nrhs, int *iters);
+/* 1 (default): xs_solve_batch / xs_adjoint_batch iterate eligible columns
+ * together; 0: always one after another.  Environment XS_BATCH. */
+int xs_set_batch_kernels(int enable);
 int xs_adjoint(xs_handle_t h, const double *dLdx, double *dLdb, double *dLdA_vals);
-/* batch adjoint: nrhs forward solutions (host, contiguous) and gradients */
+/* batch adjoint: nrhs forward solutions (host, contiguous) and gradients
+ * (dLdb: nrhs*n, dLdA_vals: nrhs*nnz, each column after the other); the
+ * transposed solves iterate together under the conditions of
+ * xs_solve_batch. */
 int xs_adjoint_batch(xs_handle_t h, int nrhs, const double *x, const double *dLdx, double *dLdb, double *dLdA_vals);
 /* timing of the last solve, in milliseconds (CUDA events around the solve
  * on the handle's stream): setup = preconditioner construction */
@@ -277,6 +293,12 @@ int xs_plan_set_factor_precision(xs_plan_t p, int prec);
 int xs_plan_set_trsv(xs_plan_t p, int mode);
 /* z = (L D U')^{-1} x with sync-free solves (vec_prec 0 FP64 / 1 FP32) */
 int xs_plan_lusolve(xs_plan_t p, int vec_prec, const void *d_x, void *d_z);
+/* k (1..16) LU solves at once on device vectors stored interleaved by row
+ * (entry (i, c) at i*k + c), FP64, exact triangular solves: each column's
+ * result is bitwise the one xs_plan_lusolve gives for that column alone.
+ * No counterpart in the reference; the batched solves of xs_solve_batch use
+ * it.  XS_ERR_UNSUPPORTED for Jacobi-sweep mode. */
+int xs_plan_lusolve_batch(xs_plan_t p, int k, const double *x, double *z);
 /* z = (L D U')^{-T} x */
 int xs_plan_lusolve_t(xs_plan_t p, const double *d_x, double *d_z);
 /* wait for the plan's stream; returns the device status word (e.g. a

@@ -85,6 +85,7 @@ def _declare(L):
         "xs_plan_lusolve": [C.c_void_p, C.c_int, _vp, _vp],
         "xs_plan_set_trsv": [C.c_void_p, C.c_int],
         "xs_plan_lusolve_t": [C.c_void_p, _vp, _vp],
+        "xs_plan_lusolve_batch": [C.c_void_p, C.c_int, _vp, _vp],
         "xs_plan_sync": [C.c_void_p],
         "xs_plan_debug_break_dependency": [C.c_void_p, C.c_int, C.c_int],
         "xs_plan_levels": [C.c_void_p, _ip, _ip],
@@ -103,6 +104,8 @@ def _declare(L):
         "xs_set_sweep_fusion": [C.c_int],
         "xs_set_launch_overlap": [C.c_int],
         "xs_set_vector_fusion": [C.c_int],
+        "xs_set_batch_kernels": [C.c_int],
+        "xs_batch_iterations": [C.c_void_p, C.c_int, _ip],
         "xs_lusolve_noalloc": [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         "xsolver_last_error": [],
     }

@@ -171,6 +171,11 @@ class Solver:
         check(self._L.xs_solve_batch(self.h, B.shape[0], _d(B), _d(X)), "xs_solve_batch")
         return X
 
+    def batch_iterations(self, k: int):
+        it = np.zeros(k, np.int32)
+        check(self._L.xs_batch_iterations(self.h, k, _i(it)), "xs_batch_iterations")
+        return it
+
     @property
     def usediter(self) -> int:
         return self._used.value
@@ -316,6 +321,18 @@ class Plan:
         check(self._L.xs_plan_lusolve(self.p, prec, C.c_void_p(x.data_ptr()), C.c_void_p(z.data_ptr())), "lusolve")
         self._hold(x, z)
         return z
+
+    def lusolve_batch(self, X, Z):
+        """k LU solves on (n, k) row-major CUDA tensors (column c of row i at
+        i*k + c), FP64."""
+        if X.dim() != 2 or X.shape[0] != self.A.n or tuple(Z.shape) != tuple(X.shape):
+            raise ValueError(f"lusolve_batch: expected X and Z of shape ({self.A.n}, k)")
+        _dev(X, X.numel(), "float64", "X")
+        _dev(Z, Z.numel(), "float64", "Z")
+        check(self._L.xs_plan_lusolve_batch(self.p, X.shape[1], C.c_void_p(X.data_ptr()), C.c_void_p(Z.data_ptr())),
+              "lusolve_batch")
+        self._hold(X, Z)
+        return Z
 
     def lusolve_t(self, x, z):
         _dev(x, self.A.n, "float64", "x")

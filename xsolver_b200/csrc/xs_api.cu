@@ -24,6 +24,7 @@
 #include "xs_gmres.cuh"
 #include "xs_parilut.cuh"
 #include "xs_adjoint.cuh"
+#include "xs_batch.cuh"
 #include "xs_mtx.cuh"
 
 namespace xs {
@@ -65,6 +66,16 @@ FormatTuning &format_tuning()
         if (const char *e = getenv("XS_ELL_DIAGONAL")) t.ell_dia = atoi(e) != 0;
         init = true;
     }
+    return t;
+}
+
+BatchTuning &batch_tuning()
+{
+    static BatchTuning t = [] {
+        BatchTuning b;
+        if (const char *e = getenv("XS_BATCH")) b.enabled = atoi(e) != 0;
+        return b;
+    }();
     return t;
 }
 
@@ -408,6 +419,8 @@ struct Handle {
     AdjointState adj;
     DBuf<OuterState> outer_st;
     bool have_solution = false;
+    // several right-hand sides at once (xs_solve_batch, xs_adjoint_batch)
+    BatchRuntime batch;
 
     Handle()
     {
@@ -1358,6 +1371,163 @@ static void adjoint_host(Handle &h, const double *dLdx, double *dLdb, double *dL
     adjoint_solve(h, dLdx, dLdb, dLdA);
 }
 
+// ---------------------------------------------------------------- several right-hand sides
+// PCG with an exact (or no / Jacobi) FP64 preconditioner solves k right-hand
+// sides together (xs_batch.cuh); anything else solves them one by one.
+static bool batch_ok(Handle &h, const PrecondDev &M, int k)
+{
+    return k >= 2 && k <= BATCH_MAX && h.method == KSP_CGM && !h.inner32 && batch_precond_ok(M) &&
+           batch_tuning().enabled;
+}
+
+static int batch_errors(Handle &h, BatchRuntime &R, BatchPrecond &bp)
+{
+    R.S.fetch(h.s);
+    int e = read_dev_err(h);
+    for (const KState &st : R.S.h) e |= st.err;
+    if (e & (DEV_TRSV_TIMEOUT | DEV_TMA_TIMEOUT)) {
+        bp.rearm(h.s);
+        XS_CUDA(cudaMemsetAsync(R.S.ticket.p, 0, sizeof(unsigned), h.s));
+        if (bp.ticket.p) XS_CUDA(cudaMemsetAsync(bp.ticket.p, 0, sizeof(unsigned), h.s));
+        XS_CUDA(cudaStreamSynchronize(h.s));
+    }
+    return e;
+}
+
+static void solve_batch(Handle &h, int k, const double *rhs, double *sol)
+{
+    build_precond(h);
+    if (!batch_ok(h, h.M, k)) {
+        for (int c = 0; c < k; c++) solve_host(h, rhs + (size_t)c * h.n, sol + (size_t)c * h.n);
+        return;
+    }
+    clear_dev_err(h);
+    const int n = h.n;
+    const long m = (long)n * k;
+    BatchRuntime &R = h.batch;
+    if (R.bB.n != (size_t)m) { R.bB.alloc(m); R.bX.alloc(m); R.tmp.alloc(m); }
+    const int g = geom().sms * 4;
+    R.tmp.upload(rhs, m, h.s);
+    k_interleave<<<g, 256, 0, h.s>>>(n, k, R.tmp.p, R.bB.p);
+    R.tmp.upload(sol, m, h.s);  // x0 of every column
+    k_interleave<<<g, 256, 0, h.s>>>(n, k, R.tmp.p, R.bX.p);
+    check_launch();
+    R.S.prepare(k, h.maxiter, h.tol, h.abstol, h.s);
+    cudaEvent_t e0, e1;
+    XS_CUDA(cudaEventCreate(&e0));
+    XS_CUDA(cudaEventCreate(&e1));
+    XS_CUDA(cudaEventRecord(e0, h.s));
+    h.launches = 2;
+    const DevCsr A{n, h.nnz, h.A.rp.p, h.A.ci.p, h.A.v.p, nullptr};
+    R.pcg.run(h.s, A, h.M, R.bp, R.S, k, R.bB.p, R.bX.p, &h.launches);
+    XS_CUDA(cudaEventRecord(e1, h.s));
+    k_deinterleave<<<g, 256, 0, h.s>>>(n, k, R.bX.p, R.tmp.p);
+    check_launch();
+    R.tmp.download(sol, m, h.s);
+    XS_CUDA(cudaStreamSynchronize(h.s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h.solve_ms = ms;
+    const int e = batch_errors(h, R, R.bp);
+    R.iters.assign(k, 0);
+    int itmax = 0;
+    for (int c = 0; c < k; c++) {
+        R.iters[c] = R.S.h[c].iter;
+        itmax = std::max(itmax, R.iters[c]);
+    }
+    h.last_iters = itmax;
+    // as for k single solves: usediter / resvec / the adjoint's solution
+    // describe the last right-hand side
+    const KState &lst = R.S.h[k - 1];
+    h.final_relres = lst.iter ? lst.rnorm / (lst.res0 + KSMALL) : (lst.res0 > 0 ? 1.0 : 0.0);
+    if (h.usediter) *h.usediter = lst.iter;
+    if (h.resvec) XS_CUDA(cudaMemcpy(h.resvec, lst.hist, sizeof(double) * (lst.iter + 1), cudaMemcpyDeviceToHost));
+    if (e) {
+        h.have_solution = false;
+        throw Status(dev_err_to_status(e));
+    }
+    h.have_solution = true;
+    adjoint_record_solution(h.adj, h.s, n, R.tmp.p + (size_t)(k - 1) * n);
+    XS_CUDA(cudaStreamSynchronize(h.s));
+}
+
+static void adjoint_batch(Handle &h, int k, const double *X, const double *G, double *DB, double *DA)
+{
+    build_precond(h);
+    bool ok = batch_ok(h, h.M, k);
+    if (ok) {
+        adjoint_prepare(h);
+        ok = batch_precond_ok(h.adj.Mt);
+    }
+    if (!ok) {
+        for (int c = 0; c < k; c++) {
+            adjoint_set_solution(h.adj, h.s, h.n, X + (size_t)c * h.n);
+            h.have_solution = true;
+            adjoint_solve(h, G + (size_t)c * h.n, DB ? DB + (size_t)c * h.n : nullptr,
+                          DA ? DA + (size_t)c * h.nnz : nullptr);
+        }
+        return;
+    }
+    clear_dev_err(h);
+    AdjointState &a = h.adj;
+    const int n = h.n;
+    const long m = (long)n * k;
+    BatchRuntime &R = h.batch;
+    if (R.bB.n != (size_t)m) { R.bB.alloc(m); R.bX.alloc(m); R.tmp.alloc(m); }
+    if (R.bY.n != (size_t)m) R.bY.alloc(m);
+    const int g = geom().sms * 4;
+    R.tmp.upload(G, m, h.s);
+    k_interleave<<<g, 256, 0, h.s>>>(n, k, R.tmp.p, R.bB.p);  // right-hand sides dL/dx
+    R.tmp.upload(X, m, h.s);
+    k_interleave<<<g, 256, 0, h.s>>>(n, k, R.tmp.p, R.bY.p);  // forward solutions
+    check_launch();
+    XS_CUDA(cudaMemsetAsync(R.bX.p, 0, sizeof(double) * m, h.s));  // lambda0 = 0
+    R.S.prepare(k, h.maxiter, h.tol, h.abstol, h.s);
+    cudaEvent_t e0, e1;
+    XS_CUDA(cudaEventCreate(&e0));
+    XS_CUDA(cudaEventCreate(&e1));
+    XS_CUDA(cudaEventRecord(e0, h.s));
+    const DevCsr At{n, h.nnz, a.At.rp.p, a.At.ci.p, a.At.v.p, nullptr};
+    R.pcg_t.run(h.s, At, a.Mt, R.bpt, R.S, k, R.bB.p, R.bX.p, nullptr);
+    // gradients: dL/db = lambda, dL/dA = -lambda_i x_j on A's pattern, per column
+    double *db = nullptr, *dA = nullptr;
+    if (DB) {
+        if (R.gb.n != (size_t)m) R.gb.alloc(m);
+        db = R.gb.p;
+    }
+    if (DA) {
+        const size_t mA = (size_t)k * std::max<long>(h.nnz, 1);
+        if (R.gA.n != mA) R.gA.alloc(mA);
+        dA = R.gA.p;
+    }
+    k_adjoint_grad_multi<<<g, 256, 0, h.s>>>(n, k, h.nnz, h.A.rp.p, h.A.ci.p, R.bX.p, R.bY.p, db, dA);
+    check_launch();
+    XS_CUDA(cudaEventRecord(e1, h.s));
+    if (DB) R.gb.download(DB, m, h.s);
+    if (DA) {
+        if (h.vperm.empty()) R.gA.download(DA, (size_t)k * h.nnz, h.s);
+        else {
+            std::vector<double> t((size_t)k * h.nnz);
+            R.gA.download(t.data(), t.size(), h.s);
+            XS_CUDA(cudaStreamSynchronize(h.s));
+            for (int c = 0; c < k; c++)
+                for (long e = 0; e < h.nnz; e++) DA[(size_t)c * h.nnz + h.vperm[e]] = t[(size_t)c * h.nnz + e];
+        }
+    }
+    XS_CUDA(cudaStreamSynchronize(h.s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h.solve_ms = ms;
+    const int e = batch_errors(h, R, R.bpt);
+    R.iters.assign(k, 0);
+    for (int c = 0; c < k; c++) R.iters[c] = R.S.h[c].iter;
+    if (e) throw Status(dev_err_to_status(e));
+}
+
 // ---------------------------------------------------------------- string helpers
 static bool ieq(const char *a, const char *b)
 {
@@ -1572,6 +1742,11 @@ int xs_set_vector_fusion(int enable)
     return guarded([&] { vec_fusion_flag() = enable != 0; });
 }
 
+int xs_set_batch_kernels(int enable)
+{
+    return guarded([&] { batch_tuning().enabled = enable != 0; });
+}
+
 int xs_device_count(void)
 {
     int c = 0;
@@ -1767,7 +1942,17 @@ int xs_solve_batch(xs_handle_t h, int nrhs, const double *rhs, double *sol)
         HCHK(h);
         if (nrhs < 0 || (nrhs > 0 && (!rhs || !sol))) throw Status(XS_ERR_INVALID);
         Handle &H = *h->h;
-        for (int k = 0; k < nrhs; k++) solve_host(H, rhs + (size_t)k * H.n, sol + (size_t)k * H.n);
+        if (nrhs == 1) solve_host(H, rhs, sol);
+        else if (nrhs > 1) solve_batch(H, nrhs, rhs, sol);
+    });
+}
+int xs_batch_iterations(xs_handle_t h, int nrhs, int *iters)
+{
+    return guarded([&] {
+        HCHK(h);
+        Handle &H = *h->h;
+        if (!iters || nrhs != (int)H.batch.iters.size()) throw Status(XS_ERR_INVALID);
+        for (int c = 0; c < nrhs; c++) iters[c] = H.batch.iters[c];
     });
 }
 int xs_mat_update(xs_handle_t h, const double *val)
@@ -1791,13 +1976,7 @@ int xs_adjoint_batch(xs_handle_t h, int nrhs, const double *x, const double *dLd
         HCHK(h);
         if (nrhs < 0 || (nrhs > 0 && (!x || !dLdx))) throw Status(XS_ERR_INVALID);
         Handle &H = *h->h;
-        build_precond(H);
-        for (int k = 0; k < nrhs; k++) {
-            adjoint_set_solution(H.adj, H.s, H.n, x + (size_t)k * H.n);
-            H.have_solution = true;
-            adjoint_solve(H, dLdx + (size_t)k * H.n, dLdb ? dLdb + (size_t)k * H.n : nullptr,
-                          dLdA ? dLdA + (size_t)k * H.nnz : nullptr);
-        }
+        if (nrhs > 0) adjoint_batch(H, nrhs, x, dLdx, dLdb, dLdA);
     });
 }
 int xs_last_timing(xs_handle_t h, double *setup_ms, double *solve_ms, int *iterations, double *relres)

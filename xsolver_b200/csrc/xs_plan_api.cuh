@@ -8,6 +8,8 @@ struct xs_plan_s {
     DBuf<double> l2flush;
     DBuf<double> bx64, by64, bz64;
     DBuf<float> bx32, by32, bz32;
+    xs::BatchPrecond bp;  // batched LU solves
+    DBuf<int> zero;       // an all-done word that stays 0
 };
 
 namespace xs {
@@ -220,6 +222,17 @@ int xs_plan_lusolve(xs_plan_t p, int vec_prec, const void *x, void *z)
         Handle &h = *p->h;
         if (vec_prec == 0) plan_lusolve64(h, (const double *)x, (double *)z);
         else plan_lusolve32(h, (const float *)x, (float *)z);
+    });
+}
+int xs_plan_lusolve_batch(xs_plan_t p, int k, const double *x, double *z)
+{
+    return guarded([&] {
+        if (!p || !x || !z || k < 1 || k > BATCH_MAX) throw Status(XS_ERR_INVALID);
+        Handle &h = *p->h;
+        if (!h.M.have_factors) throw Status(XS_ERR_ORDER);
+        if (!batch_precond_ok(h.M)) throw Status(XS_ERR_UNSUPPORTED);
+        if (!p->zero.p) p->zero.alloc(1);
+        batch_apply(h.M, p->bp, k, x, z, p->zero.p, h.s);
     });
 }
 int xs_plan_lusolve_t(xs_plan_t p, const double *x, double *z)
