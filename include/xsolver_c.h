@@ -393,18 +393,19 @@ int xs_lusolve_noalloc(int n, const int *lrp, const int *lci, const double *lv, 
  * layout is fixed when a preconditioner is built: set before factorising. */
 int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
 /* Vector updates of the Krylov iterations fused into the preconditioner
- * pass that first reads their result (BiCGSTAB's s = r - gamma*u formed in
- * the first L pass of a Jacobi-sweep apply with an ELL copy of L): 1
- * (default) fuses, 0 runs them as separate kernels.  Same results either
- * way.  Environment XS_VEC_FUSE sets it at first use. */
+ * pass that first reads their result (BiCGSTAB's p = omega (p - alpha u) + r
+ * and s = r - gamma u formed in the first L pass of the Jacobi-sweep apply
+ * that reads them, when L has an ELL copy): 1 (default) fuses, 0 runs them
+ * as separate kernels.  Same results either way.  Environment XS_VEC_FUSE
+ * sets it at first use. */
 int xs_set_vector_fusion(int enable);
 /* Box-scheduled exact triangular solves (see xs_tri_tiles): enable = 1
- * (default) uses them for triangles of at least min_rows rows (default
+ * uses them for triangles of at least min_rows rows (default
  * 65536, at least 8) whose pattern fits a grid, with boxes of tx*ty*tz
  * sheared grid steps (default 16*16*16, halved along the longest side until
  * a box and its halo fit in shared memory); 0 keeps the level-ordered solve
- * (the other arguments are then ignored).  Results are bitwise identical
- * either way.  Environment XS_TRSV_TILES ("0" or "tx,ty,tz") and
+ * (the other arguments are then ignored; the default).  Results are
+ * bitwise identical either way.  Environment XS_TRSV_TILES ("0" or "tx,ty,tz") and
  * XS_TRSV_TILE_MIN_ROWS set it at first use.  Fixed when a preconditioner is
  * built: set before factorising. */
 int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows);

@@ -327,6 +327,7 @@ struct KState {
     int cycle_i;          // GMRES/GCR: inner index inside the current cycle
     double *hist;         // device history: hist[0] = res0, hist[k+1] = after iteration k
     double *hist_rel;     // device history, method's relative residual per iteration (intel convention)
+    int pbuf;             // BiCGSTAB with the p update fused: which of its two p buffers holds p (0/1)
 };
 
 // ---------------------------------------------------------------- launch geometry

@@ -746,6 +746,43 @@ struct OpBicgS {
     }
     __device__ void finalize(const double *) const {}
 };
+// p = omega (p - alpha u) + r formed inside the first L pass of the
+// preconditioner apply that reads p (OpBicgP's operations, so the same
+// values).  The pass reads p from one buffer and stores the new p into the
+// other (its neighbours' old values are still being read), and records in
+// KState::pbuf which buffer now holds p.
+template <typename VT>
+struct SrcBicgP {
+    const VT *p, *u, *r;
+    VT *pout;
+    KState *st;
+    VT alpha, omega;
+    int which;
+    __device__ void load()
+    {
+        alpha = (VT)st->sc[S_ALPHA];
+        omega = (VT)st->sc[S_OMEGA];
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->pbuf = which;
+    }
+    __device__ VT at(int c) const
+    {
+        const VT minalpha = -alpha;
+        VT t = __ldg(p + c) + minalpha * __ldg(u + c);
+        t = omega * t;
+        return t + __ldg(r + c);
+    }
+    __device__ void put(int i, VT v) const { pout[i] = v; }
+};
+// bring p back into the first buffer before a resumed run (its graph starts
+// from there), then mark it home
+template <typename VT>
+__global__ void k_bicg_p_home(int n, const KState *st, VT *pa, const VT *pb)
+{
+    if (st->pbuf != 1) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pa[i] = pb[i];
+}
+__global__ void k_bicg_p_homed(KState *st) { st->pbuf = 0; }
+
 // s = r - gama u formed inside the first L pass of the preconditioner
 // apply that reads s (the same operations as OpBicgS, so the same values;
 // the pass stores s for the later passes and the next kernels)

@@ -324,16 +324,32 @@ struct BicgRun {
         KState *st = c.W->st.p;
         RedSlot sl = c.W->slot();
         const int *done = &st->done;
+        // the p and s updates inside the first L pass of the applies that
+        // read them when the preconditioner allows it (a launch and a pass
+        // over the vector fewer each); p then alternates between two
+        // buffers, starting from the first at every graph replay
+        const bool fuse = vec_fusion() && c.M->can_fuse_first_pass();
+        VT *p2 = fuse ? pool.get(8, n) : p;
         if (!resume) {
             spmv<VT, MT>(*c.A, x, r, EpiResid<VT>{st, b}, sl, c.s);
             vecop(OpBicgInit<VT>{n, st, r, rhat, p, u}, sl, c.s);
+        } else if (fuse) {
+            k_bicg_p_home<VT><<<geom().sms * 4, 256, 0, c.s>>>(n, st, p, p2);
+            k_bicg_p_homed<<<1, 1, 0, c.s>>>(st);
+            check_launch();
         }
-        // s = r - gama u inside the second apply's first pass when the
-        // preconditioner allows it (one launch and one pass over s fewer)
-        const bool fuse_s = vec_fusion() && c.M->can_fuse_first_pass();
+        const bool fuse_s = fuse;
+        int parity = 0;  // iteration index inside the captured chunk
         auto body = [&]() {
-            vecop(OpBicgP<VT>{n, st, p, r, u, (VT)0, (VT)0}, sl, c.s);
-            c.M->apply<VT>(p, z1, done, c.s);
+            if (fuse) {
+                VT *pin = (parity & 1) ? p2 : p, *pout = (parity & 1) ? p : p2;
+                c.M->apply_fused<VT>(SrcBicgP<VT>{pin, u, r, pout, st, (VT)0, (VT)0, (parity & 1) ? 0 : 1}, pout, z1,
+                                     done, c.s);
+                parity++;
+            } else {
+                vecop(OpBicgP<VT>{n, st, p, r, u, (VT)0, (VT)0}, sl, c.s);
+                c.M->apply<VT>(p, z1, done, c.s);
+            }
             spmv<VT, MT>(*c.A, z1, u, EpiDot1<VT>{st, rhat, 0, M_BICG_GAMA}, sl, c.s);
             if (fuse_s) {
                 c.M->apply_fused<VT>(SrcBicgS<VT>{r, u, s, st, (VT)0}, s, z2, done, c.s);
@@ -344,8 +360,9 @@ struct BicgRun {
             spmv<VT, MT>(*c.A, z2, v, EpiDot2<VT>{st, s, M_BICG_ALPHA}, sl, c.s);
             vecop(OpBicgX<VT>{n, st, x, r, z1, z2, s, v, rhat, (VT)0, (VT)0}, sl, c.s);
         };
-        std::vector<const void *> key{b, x, r, rhat, p, u, s, v, z1, z2, st, c.M, c.A, (const void *)cfg_key(c),
+        std::vector<const void *> key{b, x, r, rhat, p, p2, u, s, v, z1, z2, st, c.M, c.A, (const void *)cfg_key(c),
                                       (const void *)(long)fuse_s};
+        if (fuse && (c.chunk & 1)) throw Status(XS_ERR_INVALID);  // p must be back in its first buffer after a chunk
         run_graph_loop(c, gc, key, c.chunk, c.W->h_st->maxiter / c.chunk + 3, body);
     }
 };

@@ -46,7 +46,7 @@ namespace xs {
 // with at least min_rows rows whose pattern fits a grid.  Process-wide;
 // fixed when a preconditioner's triangles are analysed.
 struct TileTuning {
-    int enable = 1;
+    int enable = 0;  // off until the box kernel beats the level-ordered one on every measured case
     int tx = 16, ty = 16, tz = 16;
     int min_rows = 65536;
     int blocks_per_sm = 4;

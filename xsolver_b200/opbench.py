@@ -38,6 +38,10 @@ def main(argv=None):
     ap.add_argument("--solve", default="", help="Krylov method for whole solves (bicgstab, cg, gmres, gcr, ...)")
     ap.add_argument("--mixed", action="store_true", help="whole solves by mixed-precision refinement")
     ap.add_argument("--solves", type=int, default=1)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="k: PCG on k right-hand sides (seeds 0..k-1) with xs_solve_batch and xs_adjoint_batch, "
+                         "timed against k single solves")
+    ap.add_argument("--rtol", type=float, default=1e-10)
     a = ap.parse_args(argv)
     A = STENCILS[a.stencil](a.grid)
     out = {"stencil": a.stencil, "grid": a.grid, "n": A.n, "nnz": A.nnz}
@@ -51,6 +55,33 @@ def main(argv=None):
             by = P.op_bytes(op)
             out[op] = {"ms": ms, "bytes": by, "GBs": by / ms / 1e6}
         out["levels"] = P.levels()
+    if a.batch:
+        import time
+
+        import numpy as np
+
+        from . import _lib
+
+        k = a.batch
+        B = np.stack([st.rhs_uniform(A.n, c) for c in range(k)])
+        L = _lib.lib()
+        S = Solver(A).ksp_settype("cgm").ksp_setoption(a.rtol, 5000).pc_settype(a.factor).pc_set_trsv(a.trsv)
+        res = {}
+        for mode, on in (("batched", 1), ("one_by_one", 0)):
+            L.xs_set_batch_kernels(on)
+            Xw = S.solve_batch(B)  # setup and graph capture outside the timing
+            S.adjoint_batch(Xw, Xw - 0.5)
+            t0 = time.perf_counter()
+            X = S.solve_batch(B)
+            t1 = time.perf_counter()
+            its = S.batch_iterations(k).tolist() if on else None
+            G = X - 0.5
+            t2 = time.perf_counter()
+            S.adjoint_batch(X, G)
+            t3 = time.perf_counter()
+            res[mode] = {"forward_ms": (t1 - t0) * 1e3, "adjoint_ms": (t3 - t2) * 1e3, "iterations": its}
+        L.xs_set_batch_kernels(1)
+        out["batch"] = {"k": k, "rtol": a.rtol, **res}
     if a.solve:
         b = st.rhs_uniform(A.n, 0, 0.0 if a.stencil == "convdiff27" else -1.0, 1.0)
         S = Solver(A, fmt="ell").ksp_settype(a.solve).ksp_setoption(1e-10, 3000, 30).pc_settype(a.factor)
