@@ -11,10 +11,14 @@ tolerance 1e-4):
     solves, rtol 1e-10 (intel/mpisolver-C-v1.cpp:685-1087 restated; the
     handle API's GMRES is right-preconditioned, the oracle's FGMRES with a
     fixed preconditioner is the same method, and its GCR is the reference's
-    hip/Solver/xsolver_igcr.cpp:29-108): the per-iteration residual history
-    within the strict 1e-10 relative bound at every iteration, the
-    iteration count within +-1 and the solution within 1e-10 relative of the
-    oracle run on the same factors;
+    hip/Solver/xsolver_igcr.cpp:29-108), against the oracle run on the same
+    factors: the per-iteration residual history within 1e-10 relative
+    wherever the reference's own summation-order spread allows it and
+    within 10 times that spread elsewhere (tests/parity.py; the spread comes
+    from tests/golden/c3_orders.npz — GMRES's last iterations move by up to
+    1e-5 between two valid dot orders of the reference itself), the
+    iteration count within the reference's own range over the orders +-1,
+    and the solution within max(1e-10, 10 x the orders' spread);
   * the mixed-precision form (FP64 outer refinement around an FP32
     GMRES(30), BF16 and FP16 factors, exact and Jacobi-sweep triangular
     solves): true relative residual below 1e-10 and the error against the
@@ -27,14 +31,17 @@ The oracle's ParILUT runs on all host threads (its per-row loops write
 disjoint outputs, so the factors do not depend on the thread count); at this
 size it takes a few minutes of the test time.
 """
+import os
+
 import numpy as np
 import pytest
 
 import oracle
-from parity import strict_report
+from parity import history_bound, history_ok
 from xsolver_b200 import stencils as st
 
 pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 FILL, SWEEPS, DROPTOL = 2.0, 5, 1e-4
 COND_BOUND = 1e3
@@ -73,16 +80,22 @@ def test_c3_fp64_vs_reference(cuda, c3, ksp, oracle_method):
     x = S.solve(b)
     hist = S.resvec()
     xo, ho, uo = oracle.solve(oracle_method, A, b, tol=1e-10, maxiter=3000, restart=30, pc="lu", factors=F, quirk=0)
+    z = np.load(os.path.join(GOLD, "c3_orders.npz"))
+    orders = [str(o) for o in z["orders"]]
+    assert np.array_equal(z[f"{oracle_method}/sequential/hist"], ho)  # the fixture is this oracle run
+    hb = history_bound(ho, [z[f"{oracle_method}/{o}/hist"] for o in orders if o != "sequential"])
+    its = [int(z[f"{oracle_method}/{o}/usediter"]) for o in orders]
+    xb = max(1e-10, 10.0 * float(z[f"{oracle_method}/xsens"]))
     if oracle_method == "hip_igcr":  # absolute residuals, [0] = ||r0||, count = last index
-        frac, worst = strict_report(hist, ho, scale=ho[0])
-        assert abs(S.usediter - uo) <= 1, (S.usediter, uo)
+        ok, worst = history_ok(hist, ho, hb, scale=ho[0])
+        count, lo, hi = S.usediter, min(its), max(its)
     else:
-        frac, worst = strict_report(hist[1:] / hist[0], ho)
-        assert abs(S.usediter - (uo + 1)) <= 1, (S.usediter, uo + 1)
-    print(f"C3 {ksp}: {S.usediter} iterations, history within 1e-10 at {frac:.0%} of iterations, "
-          f"worst |diff|/1e-10 = {worst:.3g}")
-    assert frac == 1.0, (frac, worst)
-    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-10
+        ok, worst = history_ok(hist[1:] / hist[0], ho, hb)
+        count, lo, hi = S.usediter, min(its) + 1, max(its) + 1
+    print(f"C3 {ksp}: {S.usediter} iterations (reference over orders {lo}-{hi})")
+    assert ok, worst
+    assert lo - 1 <= count <= hi + 1, (count, lo, hi)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb
     r = b - A.to_scipy() @ x
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10
 

@@ -656,7 +656,7 @@ static void load_tri_values(Handle &h, TriDev &T, const double *vals, const Fact
     auto one = [&](auto &pbuf, auto &nbuf) {
         using FT = std::remove_pointer_t<decltype(pbuf.p)>;
         if (pos) {
-            if (pbuf.n != (size_t)m) pbuf.alloc(m);
+            if (pbuf.n != (size_t)m) pbuf.alloc(m, 8);  // padded: the box solve stages whole 4-byte words
             if (T.nnz) k_gather_convert<FT><<<g, 256, 0, h.s>>>(T.nnz, T.src.p, vals, pbuf.p);
         } else {
             pbuf.free();
@@ -1297,7 +1297,7 @@ static void adjoint_prepare(Handle &h)
         const int g = geom().sms * 4;
         for (TriDev *D : {&T.L, &T.U}) {
             long m = std::max<long>(D->nnz, 1);
-            D->pv64.alloc(m);
+            D->pv64.alloc(m, 8);
             D->nv64.alloc(m);
             if (D->nnz) {
                 k_gather_convert<double><<<g, 256, 0, h.s>>>(D->nnz, D->src.p, vals, D->pv64.p);

@@ -1017,13 +1017,13 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
         }
         const long m = std::max<long>(T.nnz, 1);
         const int g = geom().sms * 4;
-        T.pv64.alloc(m); T.nv64.alloc(m);
+        T.pv64.alloc(m, 8); T.nv64.alloc(m);
         if (T.nnz) {
             k_gather_convert<double><<<g, 256, 0, s>>>(T.nnz, T.src.p, vals, T.pv64.p);
             k_gather_convert<double><<<g, 256, 0, s>>>(T.nnz, T.src_nat.p, vals, T.nv64.p);
         }
         if (need32) {
-            T.pv32.alloc(m); T.nv32.alloc(m); T.pvbf.alloc(m); T.nvbf.alloc(m); T.pvh.alloc(m); T.nvh.alloc(m);
+            T.pv32.alloc(m, 8); T.nv32.alloc(m); T.pvbf.alloc(m, 8); T.nvbf.alloc(m); T.pvh.alloc(m, 8); T.nvh.alloc(m);
             if (T.nnz) {
                 k_gather_convert<float><<<g, 256, 0, s>>>(T.nnz, T.src.p, vals, T.pv32.p);
                 k_gather_convert<float><<<g, 256, 0, s>>>(T.nnz, T.src_nat.p, vals, T.nv32.p);

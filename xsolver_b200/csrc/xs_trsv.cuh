@@ -845,12 +845,14 @@ struct TriDev {
     // factorisation kernels, which take rows in level order
     bool tiled = false;
     int ntiles = 0, tile_elems = 0;  // tile_elems: shared-memory values per box (rows + halo)
+    int t_max_rows = 0, t_max_halo = 0, t_max_entries = 0;
     DBuf<int> t_pos, t_lvl, t_lptr, t_hptr, t_hrow, lvperm;
     const int *level_perm() const { return tiled ? lvperm.p : perm.p; }
     template <typename FT>
     TileArgs<FT> targs() const
     {
-        return TileArgs<FT>{n, ntiles, t_pos.p, t_lvl.p, t_lptr.p, t_hptr.p, t_hrow.p, perm.p, prp.p, pci.p, vals<FT>()};
+        return TileArgs<FT>{n,       ntiles, t_pos.p, t_lvl.p, t_lptr.p,   t_hptr.p,   t_hrow.p,
+                            perm.p,  prp.p,  pci.p,   vals<FT>(), t_max_rows, t_max_halo, t_max_entries};
     }
 
     template <typename FT>
@@ -971,7 +973,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         for (int attempt = 0; attempt < 6; attempt++) {
             TP = TileHostPlan();
             if (!tri_analyse_tiles(n, rp.data(), ci.data(), upper, src_of, tt, TP)) break;
-            if ((size_t)(TP.max_rows + TP.max_halo) * sizeof(double) <= TILE_SMEM_MAX) {
+            if (TileSmem::of<double, double, double>(TP.max_rows, TP.max_halo, TP.max_entries).total <= TILE_SMEM_MAX) {
                 T.tiled = true;
                 break;
             }
@@ -983,6 +985,9 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     if (T.tiled) {
         T.ntiles = TP.ntiles;
         T.tile_elems = TP.max_rows + TP.max_halo;
+        T.t_max_rows = TP.max_rows;
+        T.t_max_halo = TP.max_halo;
+        T.t_max_entries = TP.max_entries;
         T.perm.alloc(n); T.perm.upload(TP.perm.data(), n, s);
         T.prp.alloc(n + 1); T.prp.upload(TP.prp.data(), n + 1, s);
         T.pci.alloc(m); if (T.nnz) T.pci.upload(TP.pci.data(), T.nnz, s);
@@ -1224,7 +1229,7 @@ inline void launch_trsv(const TriDev &T, const DT *dinv, const VT *rhs, VT *self
     const int bo = trsv_tuning().backoff_ns;
     if (T.tiled) {
         static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
-        const size_t smem = (size_t)T.tile_elems * sizeof(VT);
+        const size_t smem = TileSmem::of<VT, FT, DT>(T.t_max_rows, T.t_max_halo, T.t_max_entries).total;
         if (smem > attr) {
             XS_CUDA(cudaFuncSetAttribute(k_trsv_tiles<VT, FT, DT, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));

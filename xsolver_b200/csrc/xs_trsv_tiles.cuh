@@ -36,11 +36,40 @@
 // identical to the level-ordered solve and to the oracle.
 #pragma once
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <thread>
 #include <vector>
 #include "xs_internal.cuh"
 
 namespace xs {
+
+// fn(i) for i in [0, count) on up to 16 host threads, chunks of `chunk`
+// handed out in order from a shared counter (fn must only write data that
+// belongs to its own i)
+template <typename F>
+inline void host_parallel_for(long count, long chunk, F fn)
+{
+    const int hc = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::max(1L, std::min<long>(std::min(hc, 16), count / std::max(1L, chunk)));
+    if (T == 1) {
+        for (long i = 0; i < count; i++) fn(i);
+        return;
+    }
+    std::atomic<long> next(0);
+    auto work = [&]() {
+        while (true) {
+            const long i0 = next.fetch_add(chunk);
+            if (i0 >= count) return;
+            const long i1 = std::min(count, i0 + chunk);
+            for (long i = i0; i < i1; i++) fn(i);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; t++) th.emplace_back(work);
+    work();
+    for (auto &x : th) x.join();
+}
 
 // Tile sizes (in sheared grid steps) and when tiles are used: triangles
 // with at least min_rows rows whose pattern fits a grid.  Process-wide;
@@ -59,7 +88,7 @@ constexpr int TILE_REACH_MAX = 8;  // largest grid step of a dependency in any d
 constexpr size_t TILE_SMEM_MAX = 200 * 1024;
 
 struct TileHostPlan {
-    int n = 0, ntiles = 0, max_rows = 0, max_halo = 0;
+    int n = 0, ntiles = 0, max_rows = 0, max_halo = 0, max_entries = 0;
     int nx = 0, ny = 0, nz = 0, sa = 0, sb = 0, sc = 0;
     std::vector<int> perm, prp, pci, tile_pos, tile_lvl, lvl_ptr, halo_ptr, halo_row;
     std::vector<long> src;
@@ -95,20 +124,40 @@ inline int grid_reach(int n, const int *rp, const int *ci, LogF logical, const G
                       std::vector<int> &vecs)
 {
     const int W = 2 * reach + 1;
-    std::vector<char> seen((size_t)W * W * W, 0);
-    int worst = 0;
-    for (int r = 0; r < n; r++) {
-        int xi, yi, zi;
-        g.of(logical(r), xi, yi, zi);
-        for (int k = rp[r]; k < rp[r + 1]; k++) {
-            int xj, yj, zj;
-            g.of(logical(ci[k]), xj, yj, zj);
-            const int dx = xj - xi, dy = yj - yi, dz = zj - zi;
-            const int m = std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz)));
-            if (m > reach) return reach + 1;
-            worst = std::max(worst, m);
-            seen[((size_t)(dz + reach) * W + (dy + reach)) * W + (dx + reach)] = 1;
+    const long RB = 65536;  // rows per work item
+    const long items = (n + RB - 1) / RB;
+    std::vector<int> worst_of(items, 0);
+    std::vector<std::vector<char>> seen_of(items);
+    std::atomic<int> over(0);
+    host_parallel_for(items, 1, [&](long it) {
+        std::vector<char> seen((size_t)W * W * W, 0);
+        int worst = 0;
+        const int r0 = (int)(it * RB), r1 = (int)std::min<long>(n, r0 + RB);
+        for (int r = r0; r < r1 && !over.load(std::memory_order_relaxed); r++) {
+            int xi, yi, zi;
+            g.of(logical(r), xi, yi, zi);
+            for (int k = rp[r]; k < rp[r + 1]; k++) {
+                int xj, yj, zj;
+                g.of(logical(ci[k]), xj, yj, zj);
+                const int dx = xj - xi, dy = yj - yi, dz = zj - zi;
+                const int m = std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz)));
+                if (m > reach) {
+                    over.store(1);
+                    return;
+                }
+                worst = std::max(worst, m);
+                seen[((size_t)(dz + reach) * W + (dy + reach)) * W + (dx + reach)] = 1;
+            }
         }
+        worst_of[it] = worst;
+        seen_of[it].swap(seen);
+    });
+    if (over.load()) return reach + 1;
+    int worst = 0;
+    std::vector<char> seen((size_t)W * W * W, 0);
+    for (long it = 0; it < items; it++) {
+        worst = std::max(worst, worst_of[it]);
+        for (size_t q = 0; q < seen.size(); q++) seen[q] |= seen_of[it][q];
     }
     vecs.clear();
     for (int z = 0; z < W; z++)
@@ -260,16 +309,14 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
         }
     }
     // local levels, then positions: box-major, level-major, logical index
+    // (boxes are independent here: in parallel, each writing its own ranges)
     std::vector<int> lev(n, 0);  // by logical index
     auto row_of = [&](long q) -> int { return upper ? (int)(n - 1 - q) : (int)q; };
     h.perm.assign(n, 0);
-    h.tile_pos.assign(h.ntiles + 1, 0);
+    h.tile_pos.assign(start.begin(), start.end());
     h.tile_lvl.assign(h.ntiles + 1, 0);
-    h.lvl_ptr.clear();
-    std::vector<int> pos_of(n);  // by row
-    int pos = 0;
-    std::vector<int> lcnt;
-    for (int t = 0; t < h.ntiles; t++) {
+    std::vector<int> nlev(h.ntiles, 0);
+    host_parallel_for(h.ntiles, 16, [&](long t) {
         int maxl = 0;
         for (int k = start[t]; k < start[t + 1]; k++) {
             const long q = byq[k];
@@ -282,25 +329,28 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
             lev[q] = l;
             maxl = std::max(maxl, l);
         }
-        const int nl = maxl + 1;
-        lcnt.assign(nl + 1, 0);
+        nlev[t] = maxl + 1;
+    });
+    for (int t = 0; t < h.ntiles; t++) {
+        h.tile_lvl[t + 1] = h.tile_lvl[t] + nlev[t];
+        h.max_rows = std::max(h.max_rows, start[t + 1] - start[t]);
+    }
+    h.lvl_ptr.assign(h.tile_lvl[h.ntiles] + 1, 0);
+    std::vector<int> pos_of(n);  // by row
+    host_parallel_for(h.ntiles, 16, [&](long t) {
+        const int nl = nlev[t], pos = start[t];
+        std::vector<int> lcnt(nl + 1, 0);
         for (int k = start[t]; k < start[t + 1]; k++) lcnt[lev[byq[k]] + 1]++;
         for (int l = 0; l < nl; l++) lcnt[l + 1] += lcnt[l];
-        h.tile_pos[t] = pos;
-        h.tile_lvl[t] = (int)h.lvl_ptr.size();
-        for (int l = 0; l < nl; l++) h.lvl_ptr.push_back(pos + lcnt[l]);
+        for (int l = 0; l < nl; l++) h.lvl_ptr[h.tile_lvl[t] + l] = pos + lcnt[l];
         for (int k = start[t]; k < start[t + 1]; k++) {
             const long q = byq[k];
             const int p = pos + lcnt[lev[q]]++;
             h.perm[p] = row_of(q);
             pos_of[row_of(q)] = p;
         }
-        pos += start[t + 1] - start[t];
-        h.max_rows = std::max(h.max_rows, start[t + 1] - start[t]);
-    }
-    h.tile_pos[h.ntiles] = n;
-    h.tile_lvl[h.ntiles] = (int)h.lvl_ptr.size();
-    h.lvl_ptr.push_back(n);
+    });
+    h.lvl_ptr[h.tile_lvl[h.ntiles]] = n;
     // entries in accumulation order; dependencies as shared-memory slots:
     // [0, rows) the box's own rows by position, then the box's halo
     h.prp.assign(n + 1, 0);
@@ -311,11 +361,10 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
     h.pci.assign(nnz, 0);
     h.src.assign(nnz, 0);
     h.halo_ptr.assign(h.ntiles + 1, 0);
-    h.halo_row.clear();
-    std::vector<int> ext;
-    for (int t = 0; t < h.ntiles; t++) {
+    std::vector<std::vector<int>> ext_of(h.ntiles);
+    host_parallel_for(h.ntiles, 16, [&](long t) {
         const int p0 = h.tile_pos[t], p1 = h.tile_pos[t + 1], rows = p1 - p0;
-        ext.clear();
+        std::vector<int> &ext = ext_of[t];
         for (int p = p0; p < p1; p++) {
             const int r = h.perm[p];
             for (int e = rp[r]; e < rp[r + 1]; e++)
@@ -323,9 +372,6 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
         }
         std::sort(ext.begin(), ext.end());
         ext.erase(std::unique(ext.begin(), ext.end()), ext.end());
-        h.halo_ptr[t] = (int)h.halo_row.size();
-        h.halo_row.insert(h.halo_row.end(), ext.begin(), ext.end());
-        h.max_halo = std::max(h.max_halo, (int)ext.size());
         for (int p = p0; p < p1; p++) {
             const int r = h.perm[p];
             int o = h.prp[p];
@@ -341,8 +387,17 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
             else
                 for (int e = rp[r + 1] - 1; e >= rp[r]; e--) put(e);
         }
+    });
+    for (int t = 0; t < h.ntiles; t++) {
+        h.halo_ptr[t + 1] = h.halo_ptr[t] + (int)ext_of[t].size();
+        h.max_halo = std::max(h.max_halo, (int)ext_of[t].size());
+        h.max_entries = std::max(h.max_entries, h.prp[h.tile_pos[t + 1]] - h.prp[h.tile_pos[t]]);
     }
-    h.halo_ptr[h.ntiles] = (int)h.halo_row.size();
+    h.halo_row.resize(std::max(h.halo_ptr[h.ntiles], 0));
+    host_parallel_for(h.ntiles, 64, [&](long t) {
+        if (!ext_of[t].empty())
+            std::memcpy(h.halo_row.data() + h.halo_ptr[t], ext_of[t].data(), sizeof(int) * ext_of[t].size());
+    });
     return true;
 }
 
@@ -358,32 +413,49 @@ struct TileArgs {
     const int *perm;      // position -> row
     const int *prp;       // position row pointer
     const int *pci;       // shared-memory slot of each dependency
-    const FT *pv;
+    const FT *pv;         // entry values (the array is padded by at least 4 bytes)
+    int max_rows, max_halo, max_entries;
 };
 
-template <typename VT, typename FT, typename DT, bool UPPER>
-struct TileRow {
-    int p = -1, row = 0, k0 = 0, k1 = 0;
-    VT rhsv = 0;
-    DT dv = 0;
-    int c[TILE_PF];
-    VT f[TILE_PF];
-    __device__ __forceinline__ void load(const TileArgs<FT> &P, const DT *dinv, const VT *rhs, int pos)
+// shared-memory layout of one box (byte offsets; every part 16-byte aligned)
+struct TileSmem {
+    size_t y, rhs, dinv, pv, row, eptr, pci, total;
+    template <typename VT, typename FT, typename DT>
+    static __host__ __device__ TileSmem of(int rows, int halo, int entries)
     {
-        p = pos;
-        row = __ldg(P.perm + pos);
-        k0 = __ldg(P.prp + pos);
-        k1 = __ldg(P.prp + pos + 1);
-        rhsv = rhs[row];
-        if (UPPER) dv = __ldg(dinv + pos);
-#pragma unroll
-        for (int j = 0; j < TILE_PF; j++)
-            if (k0 + j < k1) {
-                c[j] = __ldg(P.pci + k0 + j);
-                f[j] = (VT)FVal<FT>::ld(P.pv, k0 + j);
-            }
+        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+        TileSmem m;
+        m.y = 0;
+        m.rhs = m.y + al((size_t)(rows + halo) * sizeof(VT));
+        m.dinv = m.rhs + al((size_t)rows * sizeof(VT));
+        m.pv = m.dinv + al((size_t)rows * sizeof(DT));
+        m.row = m.pv + al((size_t)entries * sizeof(FT) + 8);  // + the 4-byte rounding of the value range
+        m.eptr = m.row + al((size_t)rows * sizeof(int));
+        m.pci = m.eptr + al((size_t)(rows + 1) * sizeof(int));
+        m.total = m.pci + al((size_t)entries * sizeof(int));
+        return m;
     }
 };
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+template <int B>
+__device__ __forceinline__ void cp_async_n(void *dst, const void *src)
+{
+    if constexpr (B == 8) cp_async8(dst, src);
+    else cp_async4(dst, src);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // poll one published value (bounded); false on timeout or a recorded error
 template <typename VT>
@@ -409,6 +481,11 @@ __device__ __forceinline__ bool tile_poll(const VT *p, int *err, int backoff_ns,
     return true;
 }
 
+// A box's data is staged in shared memory before its first level: its rows
+// and entry ranges, entry slots and values, and (U) dinv by asynchronous
+// copies; then the rows' right-hand sides, gathered through the staged row
+// numbers; the halo values are polled while those copies are in flight.
+// The internal levels then read shared memory only.
 template <typename VT, typename FT, typename DT, bool UPPER>
 __global__ void __launch_bounds__(TILE_THREADS) k_trsv_tiles(TileArgs<FT> P, const DT *__restrict__ dinv,
                                                              const VT *rhs, VT *self, VT *out_user, VT *reset_other,
@@ -417,13 +494,21 @@ __global__ void __launch_bounds__(TILE_THREADS) k_trsv_tiles(TileArgs<FT> P, con
 {
     if (done_flag && *done_flag) return;
     extern __shared__ __align__(16) unsigned char tile_smem[];
-    VT *ysh = (VT *)tile_smem;
+    const TileSmem L = TileSmem::of<VT, FT, DT>(P.max_rows, P.max_halo, P.max_entries);
+    VT *ysh = (VT *)(tile_smem + L.y);
+    VT *s_rhs = (VT *)(tile_smem + L.rhs);
+    DT *s_dinv = (DT *)(tile_smem + L.dinv);
+    unsigned char *s_pv = tile_smem + L.pv;
+    int *s_row = (int *)(tile_smem + L.row);
+    int *s_eptr = (int *)(tile_smem + L.eptr);
+    int *s_pci = (int *)(tile_smem + L.pci);
     __shared__ int s_tile;
     const unsigned last = (unsigned)P.ntiles + gridDim.x - 1;
+    const int tid = threadIdx.x;
     bool ok = true;
     while (true) {
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             const unsigned t = atomicAdd(ticket, 1u);
             if (t == last) *ticket = 0u;  // every CTA has drawn its final ticket
             s_tile = (int)t;
@@ -435,41 +520,43 @@ __global__ void __launch_bounds__(TILE_THREADS) k_trsv_tiles(TileArgs<FT> P, con
         const int l0 = __ldg(P.tile_lvl + t), l1 = __ldg(P.tile_lvl + t + 1);
         const int h0 = __ldg(P.halo_ptr + t), h1 = __ldg(P.halo_ptr + t + 1);
         const int rows = p1 - p0;
-        // the first level's row data (HBM) is in flight while the halo is polled
-        TileRow<VT, FT, DT, UPPER> cur, nxt;
-        {
-            const int pos = __ldg(P.lvl_ptr + l0) + (int)threadIdx.x;
-            if (pos < __ldg(P.lvl_ptr + l0 + 1)) cur.load(P, dinv, rhs, pos);
-        }
-        for (int k = h0 + (int)threadIdx.x; k < h1; k += TILE_THREADS) {
+        const int e0 = __ldg(P.prp + p0), e1 = __ldg(P.prp + p1);
+        // group 0: row numbers; group 1: entry ranges, slots, values, dinv
+        for (int i = tid; i < rows; i += TILE_THREADS) cp_async4(s_row + i, P.perm + p0 + i);
+        cp_async_commit();
+        for (int i = tid; i <= rows; i += TILE_THREADS) cp_async4(s_eptr + i, P.prp + p0 + i);
+        for (int i = tid; i < e1 - e0; i += TILE_THREADS) cp_async4(s_pci + i, P.pci + e0 + i);
+        const long vb0 = ((long)e0 * (long)sizeof(FT)) & ~3L, vb1 = ((long)e1 * (long)sizeof(FT) + 3) & ~3L;
+        const unsigned char *vsrc = (const unsigned char *)P.pv;
+        for (long w = tid; w < (vb1 - vb0) / 4; w += TILE_THREADS) cp_async4(s_pv + 4 * w, vsrc + vb0 + 4 * w);
+        if (UPPER)
+            for (int i = tid; i < rows; i += TILE_THREADS) cp_async_n<sizeof(DT)>(s_dinv + i, dinv + p0 + i);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        // group 2: right-hand sides through the staged row numbers
+        for (int i = tid; i < rows; i += TILE_THREADS) cp_async_n<sizeof(VT)>(s_rhs + i, rhs + s_row[i]);
+        cp_async_commit();
+        for (int k = h0 + tid; k < h1; k += TILE_THREADS) {
             VT y = (VT)0;
             if (ok) ok = tile_poll<VT>(self + __ldg(P.halo_row + k), err, backoff_ns, y);
             ysh[rows + (k - h0)] = y;
         }
+        cp_async_wait<0>();
         __syncthreads();
+        const FT *pv = (const FT *)(s_pv + ((long)e0 * (long)sizeof(FT) - vb0));
         for (int l = l0; l < l1; l++) {
-            const int pa = __ldg(P.lvl_ptr + l), pb = __ldg(P.lvl_ptr + l + 1);
-            nxt.p = -1;
-            if (l + 1 < l1) {
-                const int pos = pb + (int)threadIdx.x;
-                if (pos < __ldg(P.lvl_ptr + l + 2)) nxt.load(P, dinv, rhs, pos);
+            const int pa = __ldg(P.lvl_ptr + l) - p0, pb = __ldg(P.lvl_ptr + l + 1) - p0;
+            for (int i = pa + tid; i < pb; i += TILE_THREADS) {
+                const int row = s_row[i];
+                VT acc = UPPER ? (VT)(s_rhs[i] * (VT)s_dinv[i]) : s_rhs[i];
+                if (reset_other) reset_other[row] = Sentinel<VT>::value();
+                const int k1 = s_eptr[i + 1] - e0;
+                for (int k = s_eptr[i] - e0; k < k1; k++) acc = msub(acc, ysh[s_pci[k]], (VT)FVal<FT>::cvt(pv[k]));
+                ysh[i] = acc;
+                st_publish(self + row, acc);
+                if (out_user) out_user[row] = acc;
             }
-            for (int pos = pa + (int)threadIdx.x; pos < pb; pos += TILE_THREADS) {
-                TileRow<VT, FT, DT, UPPER> r;
-                if (pos == cur.p) r = cur;
-                else r.load(P, dinv, rhs, pos);
-                VT acc = UPPER ? (VT)(r.rhsv * (VT)r.dv) : r.rhsv;
-                if (reset_other) reset_other[r.row] = Sentinel<VT>::value();
-#pragma unroll
-                for (int j = 0; j < TILE_PF; j++)
-                    if (r.k0 + j < r.k1) acc = msub(acc, ysh[r.c[j]], r.f[j]);
-                for (int k = r.k0 + TILE_PF; k < r.k1; k++)
-                    acc = msub(acc, ysh[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
-                ysh[pos - p0] = acc;
-                st_publish(self + r.row, acc);
-                if (out_user) out_user[r.row] = acc;
-            }
-            cur = nxt;
             __syncthreads();
         }
     }
