@@ -105,6 +105,7 @@ def _declare(L):
         "xs_set_launch_overlap": [C.c_int],
         "xs_set_vector_fusion": [C.c_int],
         "xs_set_batch_kernels": [C.c_int],
+        "xs_set_persistent_iteration": [C.c_int],
         "xs_batch_iterations": [C.c_void_p, C.c_int, _ip],
         "xs_lusolve_noalloc": [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         "xsolver_last_error": [],

@@ -3,8 +3,9 @@
     python -m xsolver_b200.build            # build if sources are newer
     python -m xsolver_b200.build --force
 
-The library is built from csrc/*.cu (xs_api.cu includes the kernel headers;
-xs_noalloc.cu holds the allocation-free LU solve).  It is compiled without FMA contraction (-fmad=false) so that the
+The library is built from csrc/*.cu, one object each (xs_api.cu includes the
+kernel headers; xs_persist.cu holds the persistent BiCGSTAB iteration;
+xs_noalloc.cu the allocation-free LU solve), linked into one shared library.  It is compiled without FMA contraction (-fmad=false) so that the
 FP64 triangular solves and ILU(0) reproduce the CPU reference bit for bit;
 the FP32 kernels request fused multiply-adds explicitly where they want them.
 """
@@ -41,11 +42,30 @@ def needs_build() -> bool:
     return any(os.path.getmtime(s) > t for s in sources())
 
 
+# Per-unit flags: the persistent iteration reads, in one launch, vectors its
+# earlier phases wrote, so its plain global loads bypass L1 (-dlcm=cg).
+UNIT_FLAGS = {"xs_persist.cu": ["-Xptxas", "-dlcm=cg"]}
+
+
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     if not force and not needs_build():
         return LIB
     units = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    cmd = [NVCC, *FLAGS, *(extra or []), "-o", LIB + ".tmp", *units, "-lcudart"]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    cflags = [f for f in FLAGS if f != "-shared"]
+    procs, objs = [], []
+    for u in units:
+        o = os.path.join(objdir, os.path.basename(u) + ".o")
+        cmd = [NVCC, *cflags, *UNIT_FLAGS.get(os.path.basename(u), []), *(extra or []), "-c", "-o", o, u]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append(subprocess.Popen(cmd))
+        objs.append(o)
+    for p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, "nvcc")
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

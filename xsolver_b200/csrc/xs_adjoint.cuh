@@ -29,7 +29,7 @@ struct RunSet {
 };
 
 // dLdb = lambda ; dLdA[k] = -lambda_i * x_j for entry k = (i, j)
-__global__ void k_adjoint_grad(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+static __global__ void k_adjoint_grad(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                                const double *__restrict__ lambda, const double *__restrict__ x, double *__restrict__ dLdb,
                                double *__restrict__ dLdA)
 {

@@ -79,6 +79,16 @@ BatchTuning &batch_tuning()
     return t;
 }
 
+PersistTuning &persist_tuning()
+{
+    static PersistTuning t = [] {
+        PersistTuning q;
+        if (const char *e = getenv("XS_PERSIST")) q.enabled = atoi(e) != 0;
+        return q;
+    }();
+    return t;
+}
+
 bool &vec_fusion_flag()
 {
     static bool on = [] {
@@ -1740,6 +1750,11 @@ int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows)
 int xs_set_vector_fusion(int enable)
 {
     return guarded([&] { vec_fusion_flag() = enable != 0; });
+}
+
+int xs_set_persistent_iteration(int enable)
+{
+    return guarded([&] { persist_tuning().enabled = enable != 0; });
 }
 
 int xs_set_batch_kernels(int enable)

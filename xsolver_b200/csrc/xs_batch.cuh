@@ -445,14 +445,14 @@ inline void launch_trsv_multi(const TriDev &T, int k, unsigned *ticket, const do
     check_launch();
 }
 
-__global__ void k_bdiag_scale(long m, int k, const double *__restrict__ d, const double *__restrict__ x,
+static __global__ void k_bdiag_scale(long m, int k, const double *__restrict__ d, const double *__restrict__ x,
                               double *__restrict__ y, const int *all_done)
 {
     if (*all_done) return;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < m; q += (long)gridDim.x * blockDim.x)
         y[q] = x[q] * d[q / k];
 }
-__global__ void k_bcopy(long m, const double *__restrict__ x, double *__restrict__ y, const int *all_done)
+static __global__ void k_bcopy(long m, const double *__restrict__ x, double *__restrict__ y, const int *all_done)
 {
     if (*all_done) return;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < m; q += (long)gridDim.x * blockDim.x) y[q] = x[q];
@@ -602,7 +602,7 @@ struct BatchPcg {
 
 // ---------------------------------------------------------------- layout and gradients
 // Y[i*k + c] = X[c*n + i]  (k vectors one after another -> interleaved)
-__global__ void k_interleave(int n, int k, const double *__restrict__ X, double *__restrict__ Y)
+static __global__ void k_interleave(int n, int k, const double *__restrict__ X, double *__restrict__ Y)
 {
     const long m = (long)n * k;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < m; q += (long)gridDim.x * blockDim.x) {
@@ -611,7 +611,7 @@ __global__ void k_interleave(int n, int k, const double *__restrict__ X, double 
     }
 }
 // X[c*n + i] = Y[i*k + c]
-__global__ void k_deinterleave(int n, int k, const double *__restrict__ Y, double *__restrict__ X)
+static __global__ void k_deinterleave(int n, int k, const double *__restrict__ Y, double *__restrict__ X)
 {
     const long m = (long)n * k;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < m; q += (long)gridDim.x * blockDim.x) {
@@ -621,7 +621,7 @@ __global__ void k_deinterleave(int n, int k, const double *__restrict__ Y, doubl
 }
 // per column c: dLdb_c = lambda_c ; dLdA_c[e] = -lambda_c[i] * x_c[col(e)]
 // (lambda and x interleaved; outputs one vector after another)
-__global__ void k_adjoint_grad_multi(int n, int k, long nnz, const int *__restrict__ rp, const int *__restrict__ ci,
+static __global__ void k_adjoint_grad_multi(int n, int k, long nnz, const int *__restrict__ rp, const int *__restrict__ ci,
                                      const double *__restrict__ lam, const double *__restrict__ x, double *dLdb,
                                      double *dLdA)
 {

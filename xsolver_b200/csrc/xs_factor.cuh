@@ -44,7 +44,7 @@ __device__ __forceinline__ int find_col(const int *__restrict__ ci, int a, int b
 // the rows on the critical path read their pivots from.  Waits back off
 // exponentially up to backoff_ns.  Every ticket depends only on smaller
 // tickets (level order), each held by a running CTA, so the loop progresses.
-__global__ void __launch_bounds__(128) k_ilu0_rows(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+static __global__ void __launch_bounds__(128) k_ilu0_rows(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                                                   const int *__restrict__ uptr, const int *__restrict__ perm, double *luv,
                                                   int *flag, int epoch, int *err, unsigned *ticket, int backoff_ns)
 {
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
 // smallnum = droptol = 1e-4) on A's lower part, in place in A's layout: at
 // the end entry (i, j<i) holds l_ij and the diagonal 1 / l_ii.
 // tnorm_i = droptol * ||row i of A|| (the pivot replacement scale).
-__global__ void k_ic0_tnorm(int n, const int *__restrict__ rp, const double *__restrict__ v, double droptol,
+static __global__ void k_ic0_tnorm(int n, const int *__restrict__ rp, const double *__restrict__ v, double droptol,
                             double *__restrict__ tnorm)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -291,7 +291,7 @@ __global__ void k_ic0_tnorm(int n, const int *__restrict__ rp, const double *__r
 // replaced by smallnum / droptol * tnorm_i + tnorm_i) stored inverted; the
 // operations and their order are the reference's, so the factor is bitwise
 // the same.
-__global__ void __launch_bounds__(128) k_ic0_rows(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+static __global__ void __launch_bounds__(128) k_ic0_rows(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                                                  const int *__restrict__ uptr, const int *__restrict__ perm,
                                                  const double *__restrict__ tnorm, double smallnum, double droptol,
                                                  double *luv, int *flag, int epoch, int *err, unsigned *ticket,
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(128) k_ic0_rows(int n, const int *__restrict__
 // IC(0) factor as the seqilu0 values of the LU solve, in A's layout:
 // lower (i, j): l_ij * d_j; diagonal: d_i * d_i; upper (i, j): the lower
 // entry (j, i) (position tpos[k]) times d_i, with d the stored 1 / l_ii.
-__global__ void k_ic0_split(long nnz, const int *__restrict__ rowof, const int *__restrict__ ci,
+static __global__ void k_ic0_split(long nnz, const int *__restrict__ rowof, const int *__restrict__ ci,
                             const int *__restrict__ uptr, const int *__restrict__ tpos, const double *__restrict__ luv,
                             double *__restrict__ fv)
 {
@@ -392,7 +392,7 @@ __global__ void k_ic0_split(long nnz, const int *__restrict__ rowof, const int *
 //   rowof[k]  row of entry k;  uptr[i] diagonal position of row i
 //   ucp/ucpos: upper part by columns: for column j, positions ucpos[ucp[j]..ucp[j+1])
 //              of the entries (r, j) with r <= j, rows ascending (diagonal last)
-__global__ void k_parilu_sweep(long nnz, const int *__restrict__ rp, const int *__restrict__ ci,
+static __global__ void k_parilu_sweep(long nnz, const int *__restrict__ rp, const int *__restrict__ ci,
                                const int *__restrict__ rowof, const int *__restrict__ uptr, const int *__restrict__ ucp,
                                const int *__restrict__ ucpos, const double *__restrict__ a, const double *__restrict__ cur,
                                double *__restrict__ nxt)
@@ -432,7 +432,7 @@ __global__ void k_parilu_sweep(long nnz, const int *__restrict__ rp, const int *
 }
 
 // combined LU values -> seqilu0 layout (in place into fv)
-__global__ void k_split_lu(int n, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ uptr,
+static __global__ void k_split_lu(int n, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ uptr,
                            const double *__restrict__ luv, double *__restrict__ fv)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

@@ -114,7 +114,7 @@ struct OpScaleCopy {
 };
 
 // start of a cycle: zero H, s, cs, sn; s[0] = beta; inv = 1/(beta+small)
-__global__ void k_gm_cycle_init(KState *st, GmDev g)
+static __global__ void k_gm_cycle_init(KState *st, GmDev g)
 {
     if (st->done) return;
     const int m = g.m;
@@ -133,7 +133,7 @@ __global__ void k_gm_cycle_init(KState *st, GmDev g)
 }
 
 // end of a cycle: back-substitution (updatec) for k columns, y -> g.y
-__global__ void k_gm_backsub(KState *st, GmDev g)
+static __global__ void k_gm_backsub(KState *st, GmDev g)
 {
     if (threadIdx.x != 0) return;
     if (st->finalized) {

@@ -359,6 +359,17 @@ struct Sentinel<float> {
     __device__ static bool is(float v) { return (uint32_t)__float_as_int(v) == sentinel_bits32(); }
 };
 
+// Load of a vector element that kernels read while another kernel wrote it
+// earlier (gathers of x in SpMV, of iterates in sweep passes): through the
+// read-only path by default.  The persistent iteration (a kernel whose
+// phases write what its later phases read) is compiled with
+// XS_COHERENT_VECTOR_LOADS, which reads those elements from L2 instead.
+#ifdef XS_COHERENT_VECTOR_LOADS
+#define XS_VLD(p) __ldcg(p)
+#else
+#define XS_VLD(p) __ldg(p)
+#endif
+
 // nanosecond wall clock for bounding every spin-wait
 __device__ __forceinline__ unsigned long long gtimer()
 {

@@ -767,9 +767,9 @@ struct SrcBicgP {
     __device__ VT at(int c) const
     {
         const VT minalpha = -alpha;
-        VT t = __ldg(p + c) + minalpha * __ldg(u + c);
+        VT t = XS_VLD(p + c) + minalpha * XS_VLD(u + c);
         t = omega * t;
-        return t + __ldg(r + c);
+        return t + XS_VLD(r + c);
     }
     __device__ void put(int i, VT v) const { pout[i] = v; }
 };
@@ -781,7 +781,7 @@ __global__ void k_bicg_p_home(int n, const KState *st, VT *pa, const VT *pb)
     if (st->pbuf != 1) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pa[i] = pb[i];
 }
-__global__ void k_bicg_p_homed(KState *st) { st->pbuf = 0; }
+static __global__ void k_bicg_p_homed(KState *st) { st->pbuf = 0; }
 
 // s = r - gama u formed inside the first L pass of the preconditioner
 // apply that reads s (the same operations as OpBicgS, so the same values;
@@ -793,7 +793,7 @@ struct SrcBicgS {
     const KState *st;
     VT mingama;
     __device__ void load() { mingama = -(VT)st->sc[S_GAMA]; }
-    __device__ VT at(int c) const { return __ldg(r + c) + mingama * __ldg(u + c); }
+    __device__ VT at(int c) const { return XS_VLD(r + c) + mingama * XS_VLD(u + c); }
     __device__ void put(int i, VT v) const { s[i] = v; }
 };
 
@@ -856,7 +856,7 @@ struct OpBicgRho {
 
 // continue a stopped solve: new stopping test (relative to res0), the
 // iteration cap raised by `more`, done cleared; scalars and history kept
-__global__ void k_resume_state(KState *st, double res0, double tol, int more)
+static __global__ void k_resume_state(KState *st, double res0, double tol, int more)
 {
     st->res0 = res0;
     st->tol = tol;

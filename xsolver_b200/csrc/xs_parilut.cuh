@@ -79,7 +79,7 @@ __device__ __forceinline__ int find_pos(const int *ci, int a, int b, int j)
 // bitonic-sort them.
 constexpr int PLT_BM_WORDS = PLT_CAP;  // bitmap words per warp (same buffer)
 
-__global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int *__restrict__ arp,
+static __global__ void __launch_bounds__(32 * PLT_WARPS) k_candidates(int n, const int *__restrict__ arp,
                                                                const int *__restrict__ aci, const int *__restrict__ lrp,
                                                                const int *__restrict__ lci, const int *__restrict__ urp,
                                                                const int *__restrict__ uci, int mode, int *cnt,
@@ -258,7 +258,7 @@ __device__ __forceinline__ double cand_value(int i, int j, const int *arp, const
 constexpr int PLT_CAND_CAP = 512;
 constexpr int PLT_CV_WARPS = 4;
 
-__global__ void __launch_bounds__(32 * PLT_CV_WARPS) k_candidate_values(
+static __global__ void __launch_bounds__(32 * PLT_CV_WARPS) k_candidate_values(
     int n, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
     const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv,
     const int *__restrict__ urp, const int *__restrict__ uci, const double *__restrict__ uv,
@@ -341,13 +341,13 @@ __global__ void __launch_bounds__(32 * PLT_CV_WARPS) k_candidate_values(
     }
 }
 
-__global__ void k_udiag(int n, const int *__restrict__ urp, const double *__restrict__ uv, double *__restrict__ d)
+static __global__ void k_udiag(int n, const int *__restrict__ urp, const double *__restrict__ uv, double *__restrict__ d)
 {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) d[j] = uv[urp[j]];
 }
 
 // split counts: lower entries + 1 (unit diagonal), upper entries (warp per row)
-__global__ void k_split_count(int n, const int *__restrict__ drp, const int *__restrict__ dci, int *lc, int *uc)
+static __global__ void k_split_count(int n, const int *__restrict__ drp, const int *__restrict__ dci, int *lc, int *uc)
 {
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
@@ -364,7 +364,7 @@ __global__ void k_split_count(int n, const int *__restrict__ drp, const int *__r
 }
 // rows are sorted, so the lower part is the prefix [a, a + nl) and the upper
 // part the rest; L gets its unit diagonal last
-__global__ void k_split_fill(int n, const int *__restrict__ drp, const int *__restrict__ dci, const double *__restrict__ dv,
+static __global__ void k_split_fill(int n, const int *__restrict__ drp, const int *__restrict__ dci, const double *__restrict__ dv,
                              const int *__restrict__ lrp, int *lci, double *lv, const int *__restrict__ urp, int *uci,
                              double *uv)
 {
@@ -431,7 +431,7 @@ __device__ __forceinline__ unsigned plt_hash_slot(int j)
 }
 static_assert(PLT_HASH == 512 && PLT_HASH >= 2 * PLT_ROW_CAP, "hash table size");
 
-__global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
+static __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
     int n, int parts, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
     const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv_k,
     const double *__restrict__ lv_old, const int *__restrict__ urp, const int *__restrict__ uci,
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
 
 // radix-select histogram: count |v| bit patterns whose bits above `shift+8`
 // equal the prefix selected so far (state[0]), binned by the 8 bits at `shift`
-__global__ void k_radix_hist(long m, const double *__restrict__ v, const unsigned long long *state, int shift,
+static __global__ void k_radix_hist(long m, const double *__restrict__ v, const unsigned long long *state, int shift,
                              unsigned long long *hist)
 {
     __shared__ unsigned int sh[256];
@@ -553,7 +553,7 @@ __global__ void k_radix_hist(long m, const double *__restrict__ v, const unsigne
 // one thread: the bin holding the state[1]-th smallest pattern (1-based) of
 // this pass's histogram; state[0] = (state[0] << 8) | bin, state[1] -= the
 // counts of the bins below; the histogram is cleared for the next pass
-__global__ void k_radix_pick(unsigned long long *state, unsigned long long *hist)
+static __global__ void k_radix_pick(unsigned long long *state, unsigned long long *hist)
 {
     unsigned long long k = state[1];
     int bin = 0;
@@ -583,7 +583,7 @@ __device__ __forceinline__ bool plt_keep(int k, int a, int b, int upper, const i
     return true;
 }
 // keep counts per row (warp per row)
-__global__ void k_keep_count(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+static __global__ void k_keep_count(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                              const double *__restrict__ v, double thr, double droptol, int upper, int *cnt)
 {
     const int lane = threadIdx.x & 31;
@@ -597,7 +597,7 @@ __global__ void k_keep_count(int n, const int *__restrict__ rp, const int *__res
     }
 }
 // kept entries in order (warp per row, ballot compaction)
-__global__ void k_keep_fill(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ v,
+static __global__ void k_keep_fill(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ v,
                             double thr, double droptol, int upper, const int *__restrict__ nrp, int *nci, double *nv)
 {
     const int lane = threadIdx.x & 31;
@@ -620,14 +620,14 @@ __global__ void k_keep_fill(int n, const int *__restrict__ rp, const int *__rest
 }
 
 // final conversion: L strict (drop the unit diagonal), dinv, U' = dinv*U strict
-__global__ void k_plt_final_count(int n, const int *__restrict__ lrp, const int *__restrict__ urp, int *lc, int *uc)
+static __global__ void k_plt_final_count(int n, const int *__restrict__ lrp, const int *__restrict__ urp, int *lc, int *uc)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         lc[i] = lrp[i + 1] - lrp[i] - 1;
         uc[i] = urp[i + 1] - urp[i] - 1;
     }
 }
-__global__ void k_plt_final_fill(int n, const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv,
+static __global__ void k_plt_final_fill(int n, const int *__restrict__ lrp, const int *__restrict__ lci, const double *__restrict__ lv,
                                  const int *__restrict__ urp, const int *__restrict__ uci, const double *__restrict__ uv,
                                  const int *__restrict__ olrp, int *olci, double *olv, double *dinv,
                                  const int *__restrict__ ourp, int *ouci, double *ouv)
@@ -649,7 +649,7 @@ __global__ void k_plt_final_fill(int n, const int *__restrict__ lrp, const int *
 
 // position of each row's diagonal entry (binary search of the sorted row);
 // a row without one sets DEV_NO_DIAG
-__global__ void k_plt_diag_pos(int n, const int *__restrict__ arp, const int *__restrict__ aci, int *uptr, int *err)
+static __global__ void k_plt_diag_pos(int n, const int *__restrict__ arp, const int *__restrict__ aci, int *uptr, int *err)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int p = find_pos(aci, arp[i], arp[i + 1], i);
@@ -659,7 +659,7 @@ __global__ void k_plt_diag_pos(int n, const int *__restrict__ arp, const int *__
 }
 
 // initial factors: L = strict lower(A)/a_jj + unit diag (last), U = upper(A)
-__global__ void k_plt_init_count(int n, const int *__restrict__ arp, const int *__restrict__ aci, int *lc, int *uc)
+static __global__ void k_plt_init_count(int n, const int *__restrict__ arp, const int *__restrict__ aci, int *lc, int *uc)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int l = 0;
@@ -668,7 +668,7 @@ __global__ void k_plt_init_count(int n, const int *__restrict__ arp, const int *
         uc[i] = arp[i + 1] - arp[i] - l;
     }
 }
-__global__ void k_plt_init_fill(int n, const int *__restrict__ arp, const int *__restrict__ aci,
+static __global__ void k_plt_init_fill(int n, const int *__restrict__ arp, const int *__restrict__ aci,
                                 const double *__restrict__ av, const int *__restrict__ uptr, const int *__restrict__ lrp,
                                 int *lci, double *lv, const int *__restrict__ urp, int *uci, double *uv)
 {
@@ -716,7 +716,7 @@ __device__ __forceinline__ long block_excl_scan(long v, long *sw, long &total)
     return r;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_sums(int n, const int *__restrict__ cnt, long *bsum)
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_sums(int n, const int *__restrict__ cnt, long *bsum)
 {
     __shared__ long sw[32];
     const long base = (long)blockIdx.x * SCAN_TILE;
@@ -729,7 +729,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_sums(int n, const in
 }
 
 // one block: exclusive scan of nb tile sums in place, grand total into bsum[nb]
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_offsets(int nb, long *bsum)
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_offsets(int nb, long *bsum)
 {
     __shared__ long sw[32];
     long carry = 0;
@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_offsets(int nb, long
     if (threadIdx.x == 0) bsum[nb] = carry;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_write(int n, const int *__restrict__ cnt,
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_write(int n, const int *__restrict__ cnt,
                                                                   const long *__restrict__ boff, int *rp, int *err)
 {
     __shared__ long sw[32];

@@ -18,7 +18,7 @@ namespace xs {
 // larger than L2, then read the second half, so the timed kernel starts
 // with an L2 holding none of its data and no dirty lines still waiting to
 // be written back (which would otherwise drain into its own DRAM time)
-__global__ void k_flush(double *p, long m, double v, double *sink)
+static __global__ void k_flush(double *p, long m, double v, double *sink)
 {
     const long h = m / 2;
     const long stride = (long)gridDim.x * blockDim.x;
@@ -27,7 +27,7 @@ __global__ void k_flush(double *p, long m, double v, double *sink)
     for (long i = h + blockIdx.x * (long)blockDim.x + threadIdx.x; i < m; i += stride) acc += p[i];
     if (acc == 1.2345e300) *sink = acc;  // keeps the reads
 }
-__global__ void k_fill_rand(int n, double *x, float *x32, unsigned seed)
+static __global__ void k_fill_rand(int n, double *x, float *x32, unsigned seed)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         unsigned h = (unsigned)i * 2654435761u ^ seed;

@@ -4,6 +4,7 @@
 #include <vector>
 #include <cstring>
 #include "xs_krylov.cuh"
+#include "xs_persist.cuh"
 
 namespace xs {
 
@@ -312,6 +313,7 @@ template <typename VT, typename MT>
 struct BicgRun {
     VecPool<VT> pool;
     GraphCache gc;
+    DBuf<unsigned> bar;  // grid barrier of the persistent iteration
     VT *residual(int n) { return pool.get(0, n); }
     VT *shadow(int n) { return pool.get(1, n); }
     // resume: continue the previous run's iteration (same p, u, rhat and
@@ -360,6 +362,16 @@ struct BicgRun {
             spmv<VT, MT>(*c.A, z2, v, EpiDot2<VT>{st, s, M_BICG_ALPHA}, sl, c.s);
             vecop(OpBicgX<VT>{n, st, x, r, z1, z2, s, v, rhat, (VT)0, (VT)0}, sl, c.s);
         };
+        // the whole iteration as one persistent kernel when it serves this
+        // configuration (same vector updates fused into the sweep passes)
+        if (fuse && std::is_same<VT, MT>::value) {
+            if (!bar.p) bar.alloc(2);
+            const PersistVectors<VT> V{x, r, rhat, p, p2, u, s, v, z1, z2};
+            if (persist_bicgstab(c, V, c.W->h_st->maxiter + 2, bar.p)) {
+                XS_CUDA(cudaStreamSynchronize(c.s));
+                return;
+            }
+        }
         std::vector<const void *> key{b, x, r, rhat, p, p2, u, s, v, z1, z2, st, c.M, c.A, (const void *)cfg_key(c),
                                       (const void *)(long)fuse_s};
         if (fuse && (c.chunk & 1)) throw Status(XS_ERR_INVALID);  // p must be back in its first buffer after a chunk

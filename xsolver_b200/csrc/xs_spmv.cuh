@@ -430,7 +430,7 @@ __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld,
         for (int j = 0; j < C; j++) {
             const int off = s_off[k0 + j];
 #pragma unroll
-            for (int q = 0; q < R; q++) xv[j][q] = __ldg(x + min(max(r0 + q + off, 0), n - 1));
+            for (int q = 0; q < R; q++) xv[j][q] = XS_VLD(x + min(max(r0 + q + off, 0), n - 1));
         }
 #pragma unroll
         for (int j = 0; j < C; j++)
@@ -450,7 +450,7 @@ __device__ __forceinline__ void ell_chunk(const CT *&cp, const MT *&vp, long ld,
         for (int j = 0; j < C; j++)
 #pragma unroll
             for (int q = 0; q < R; q++)
-                xv[j][q] = (R == 1 || r0 + q < n) ? __ldg(x + ell_col<CT>(c[j][q], r0 + q)) : (VT)0;
+                xv[j][q] = (R == 1 || r0 + q < n) ? XS_VLD(x + ell_col<CT>(c[j][q], r0 + q)) : (VT)0;
 #pragma unroll
         for (int j = 0; j < C; j++)
 #pragma unroll

@@ -385,7 +385,7 @@ template <typename VT>
 struct SrcVec {
     const VT *x;
     __device__ void load() {}
-    __device__ VT at(int c) const { return __ldg(x + c); }
+    __device__ VT at(int c) const { return XS_VLD(x + c); }
     __device__ void put(int, VT) const {}
 };
 
@@ -438,7 +438,7 @@ __device__ __forceinline__ void sweep_chunk(const CT *&cp, const FT *&vp, long l
             if (EllDiag<CT>::value || pr[j][q]) {
                 const int cc = col[j][q];
                 if (FIRST2) y[j][q] = UPPER ? (VT)(x.at(cc) * (VT)__ldg(dinv + cc)) : x.at(cc);
-                else y[j][q] = __ldg(yin + cc);
+                else y[j][q] = XS_VLD(yin + cc);
             } else {
                 y[j][q] = (VT)0;
             }
@@ -634,7 +634,7 @@ __global__ void k_tri_dia_build(int n, int D, long ld, const int *__restrict__ r
 
 // level-ordered entry arrays from the natural CSR: position p holds row
 // perm[p]; its entries in increasing column order (L) or decreasing (U)
-__global__ void k_pos_entries(int n, bool upper, const int *__restrict__ perm, const int *__restrict__ prp,
+static __global__ void k_pos_entries(int n, bool upper, const int *__restrict__ perm, const int *__restrict__ prp,
                               const int *__restrict__ rp, const int *__restrict__ ci, const long *__restrict__ src_nat,
                               int *pci, long *src)
 {
@@ -647,7 +647,7 @@ __global__ void k_pos_entries(int n, bool upper, const int *__restrict__ perm, c
         }
     }
 }
-__global__ void k_iota_long(long m, long *a)
+static __global__ void k_iota_long(long m, long *a)
 {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < m; i += (long)gridDim.x * blockDim.x) a[i] = i;
 }
