@@ -400,11 +400,11 @@ int xs_set_trsv_tuning(int blocks_per_sm, int backoff_ns, int chunk_rows);
  * sets it at first use. */
 int xs_set_vector_fusion(int enable);
 /* BiCGSTAB with an ILU-family preconditioner applied by Jacobi sweeps, the
- * operator and both triangles in diagonal-slot ELL storage: 1 (default)
- * runs each solve's iterations as one persistent cooperative kernel (the
+ * operator and both triangles in diagonal-slot ELL storage: 1 runs each
+ * solve's iterations as one persistent cooperative kernel (the
  * phases of an iteration separated by grid barriers, the loop on the
  * device) instead of replaying a CUDA graph of ~11 kernels per iteration;
- * 0 replays the graph.  The arithmetic per element is the same; the dot
+ * 0 (default) replays the graph.  The arithmetic per element is the same; the dot
  * products' block partials follow the persistent grid, so results agree to
  * rounding.  Needs vector fusion on.  Environment XS_PERSIST. */
 int xs_set_persistent_iteration(int enable);

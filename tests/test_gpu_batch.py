@@ -7,12 +7,14 @@ the batched LU solve equals xs_plan_lusolve column by column, bit for bit.
 Dot products reduce in their own order, so a batched solve agrees with k
 single solves (the reference's one-right-hand-side loop,
 intel/mpisolver-C-v1.cpp:193-272 restated) to rounding: per column the
-iteration count within +-1, the residual history within 1e-10 relative and
-the solution within 1e-10 relative."""
+iteration count within +-1 and the solution within 1e-10 relative; the
+residual history against the reference loop within the calibrated bound of
+tests/parity.py (1e-10 wherever the reference's own dot order allows)."""
 import numpy as np
 import pytest
 
-from parity import strict_report
+import oracle
+from parity import history_ok, reference_with_bounds
 from xsolver_b200 import stencils as st
 
 pytestmark = pytest.mark.gpu
@@ -91,12 +93,17 @@ def test_batched_pcg_matches_single_solves(cuda, k, pc):
             h1 = S.resvec()
             assert abs(int(its[c]) - S.usediter) <= 1, (c, its[c], S.usediter)
             assert np.linalg.norm(X[c] - xs) / np.linalg.norm(xs) < 1e-10, c
-    # the handle's history is the last column's: against its single solve
+    # the handle's history is the last column's: against the reference loop
+    # (the oracle's PCG with the same preconditioner) within the calibrated
+    # bound of tests/parity.py, as the single solve is
     S2 = _pcg(A, pc)
     S2.solve_batch(B)
     hb = S2.resvec()
-    frac, worst = strict_report(hb[1:] / hb[0], h1[1:] / h1[0])
-    assert frac == 1.0, (frac, worst)
+    F = {"ilu0": oracle.ilu0, "ic0": oracle.ic0}.get(pc)
+    kw = dict(tol=1e-12, maxiter=3000, pc="lu", factors=F(A)) if F else dict(tol=1e-12, maxiter=3000, pc="jacobi")
+    _, ho, uo, hbnd, _ = reference_with_bounds("cgm", A, B[k - 1], **kw)
+    ok, worst = history_ok(hb[1:] / hb[0], ho, hbnd)
+    assert ok, worst
     Asp = A.to_scipy()
     for c in range(k):
         assert np.linalg.norm(B[c] - Asp @ X[c]) / np.linalg.norm(B[c]) < 1e-11

@@ -81,14 +81,16 @@ __device__ __forceinline__ void phase_sweep(int n, int w, const uint8_t *__restr
     using CT = uint8_t;
     constexpr int R = ell_rows_for<FT>();
     const long ld = ell_ld(n);
+    Src xs = x;
+    xs.load();  // scalars the source needs (written before the barrier that began this phase)
     for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * R; i0 < n; i0 += gridDim.x * blockDim.x * R) {
         VT acc[R];
 #pragma unroll
         for (int q = 0; q < R; q++) {
             const int i = i0 + q;
             if (R == 1 || i < n) {
-                const VT xi = x.at(i);
-                x.put(i, xi);
+                const VT xi = xs.at(i);
+                xs.put(i, xi);
                 acc[q] = UPPER ? (VT)(xi * (VT)dinv[i]) : xi;
             } else {
                 acc[q] = (VT)0;
@@ -102,7 +104,7 @@ __device__ __forceinline__ void phase_sweep(int n, int w, const uint8_t *__restr
         for (int k0 = 0; k0 < w; k0 += CH) {
             const int m = min(CH, w - k0);
 #define XS_PSWEEP(CC) \
-    sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2, Src>(cp, vp, ld, i0, n, k0, mask, s_off, dinv, x, yin, acc)
+    sweep_chunk<CC, R, VT, FT, DT, CT, UPPER, FIRST2, Src>(cp, vp, ld, i0, n, k0, mask, s_off, dinv, xs, yin, acc)
             if (m == CH) XS_PSWEEP(CH);
             else if (CH > 7 && m == 7) XS_PSWEEP(7);
             else if (CH > 6 && m == 6) XS_PSWEEP(6);

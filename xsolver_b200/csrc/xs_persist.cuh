@@ -15,7 +15,7 @@ struct PersistVectors {
 };
 
 struct PersistTuning {
-    int enabled = 1;
+    int enabled = 0;  // off by default: a fault in its first GPU run is not yet explained
 };
 PersistTuning &persist_tuning();
 
