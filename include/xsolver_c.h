@@ -409,12 +409,12 @@ int xs_set_vector_fusion(int enable);
  * rounding.  Needs vector fusion on.  Environment XS_PERSIST. */
 int xs_set_persistent_iteration(int enable);
 /* Box-scheduled exact triangular solves (see xs_tri_tiles): enable = 1
- * uses them for triangles of at least min_rows rows (default
+ * (default) uses them for triangles of at least min_rows rows (default
  * 65536, at least 8) whose pattern fits a grid, with boxes of tx*ty*tz
- * sheared grid steps (default 16*16*16, halved along the longest side until
- * a box and its halo fit in shared memory); 0 keeps the level-ordered solve
- * (the other arguments are then ignored; the default).  Results are
- * bitwise identical either way.  Environment XS_TRSV_TILES ("0" or "tx,ty,tz") and
+ * sheared grid steps (default 16*16*8, halved along the longest side until
+ * a box's staged data fits in shared memory); 0 keeps the level-ordered
+ * solve (the other arguments are then ignored).  Results are bitwise
+ * identical either way.  Environment XS_TRSV_TILES ("0" or "tx,ty,tz") and
  * XS_TRSV_TILE_MIN_ROWS set it at first use.  Fixed when a preconditioner is
  * built: set before factorising. */
 int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows);

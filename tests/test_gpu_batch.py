@@ -47,7 +47,7 @@ class tiles:
     def __exit__(self, *exc):
         from xsolver_b200 import _lib
 
-        _lib.lib().xs_set_trsv_tiles(0, 16, 16, 16, 65536)
+        _lib.lib().xs_set_trsv_tiles(1, 16, 16, 8, 65536)
 
 
 @pytest.mark.parametrize("box_layout", [True, False])

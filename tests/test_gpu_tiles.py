@@ -42,7 +42,7 @@ class tiles_forced:
         from xsolver_b200 import _lib
 
         L = _lib.lib()
-        L.xs_set_trsv_tiles(0, 16, 16, 16, 65536)
+        L.xs_set_trsv_tiles(1, 16, 16, 8, 65536)
         L.xs_set_trsv_block_rows(1 << 30)
 
 

@@ -267,33 +267,29 @@ __global__ void __launch_bounds__(TRSV_THREADS) k_trsv_level_multi(TrsvArgs<doub
 }
 
 // Box layout: work items are (box, column group) pairs of KC columns, taken
-// in box order; a box's halo and rows are as in k_trsv_tiles, with KC values
-// per shared-memory slot.  The KC threads of a row lane handle the row for
-// the group's columns; each lane's first row of the next level is loaded
-// ahead (its entries and right-hand side), as in the single-column kernel.
+// in box order.  As k_trsv_tiles, a box's rows, entries and (U) dinv are
+// staged in shared memory by asynchronous copies and its right-hand sides
+// gathered (KC per row) while the halo is polled; the internal levels then
+// read shared memory only, the KC threads of a row lane handling the row for
+// the group's columns.
 constexpr int TILEM_THREADS = 512;
 
-template <bool UPPER>
-struct TileRowM {
-    int p = -1, row = 0, k0 = 0, k1 = 0;
-    double rhsv = 0.0, dv = 0.0;
-    int c[TILE_PF];
-    double f[TILE_PF];
-    __device__ __forceinline__ void load(const TileArgs<double> &P, const double *dinv, const double *rhs, int pos,
-                                         int k, int col, bool col_ok)
+// shared-memory layout of one box item with KC columns (FP64)
+struct TileSmemM {
+    size_t y, rhs, dinv, pv, row, eptr, pci, total;
+    static __host__ __device__ TileSmemM of(int rows, int halo, int entries, int kc)
     {
-        p = pos;
-        row = __ldg(P.perm + pos);
-        k0 = __ldg(P.prp + pos);
-        k1 = __ldg(P.prp + pos + 1);
-        rhsv = col_ok ? rhs[(long)row * k + col] : 0.0;
-        if (UPPER) dv = __ldg(dinv + pos);
-#pragma unroll
-        for (int j = 0; j < TILE_PF; j++)
-            if (k0 + j < k1) {
-                c[j] = __ldg(P.pci + k0 + j);
-                f[j] = __ldg(P.pv + k0 + j);
-            }
+        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+        TileSmemM m;
+        m.y = 0;
+        m.rhs = m.y + al((size_t)(rows + halo) * kc * sizeof(double));
+        m.dinv = m.rhs + al((size_t)rows * kc * sizeof(double));
+        m.pv = m.dinv + al((size_t)rows * sizeof(double));
+        m.row = m.pv + al((size_t)entries * sizeof(double) + 8);
+        m.eptr = m.row + al((size_t)rows * sizeof(int));
+        m.pci = m.eptr + al((size_t)(rows + 1) * sizeof(int));
+        m.total = m.pci + al((size_t)entries * sizeof(int));
+        return m;
     }
 };
 
@@ -306,16 +302,23 @@ __global__ void __launch_bounds__(TILEM_THREADS) k_trsv_tiles_multi(TileArgs<dou
 {
     if (all_done && *all_done) return;
     extern __shared__ __align__(16) unsigned char tm_smem[];
-    double *ysh = (double *)tm_smem;
+    const TileSmemM L = TileSmemM::of(P.max_rows, P.max_halo, P.max_entries, KC);
+    double *ysh = (double *)(tm_smem + L.y);
+    double *s_rhs = (double *)(tm_smem + L.rhs);
+    double *s_dinv = (double *)(tm_smem + L.dinv);
+    double *s_pv = (double *)(tm_smem + L.pv);
+    int *s_row = (int *)(tm_smem + L.row);
+    int *s_eptr = (int *)(tm_smem + L.eptr);
+    int *s_pci = (int *)(tm_smem + L.pci);
     __shared__ int s_item;
     const int items = P.ntiles * ngroups;
     const unsigned last = (unsigned)items + gridDim.x - 1;
     constexpr int RSTEP = TILEM_THREADS / KC;  // row lanes
-    const int pc = threadIdx.x % KC, pr = threadIdx.x / KC;
+    const int tid = threadIdx.x, pc = tid % KC, pr = tid / KC;
     bool ok = true;
     while (true) {
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             const unsigned t = atomicAdd(ticket, 1u);
             if (t == last) *ticket = 0u;
             s_item = (int)t;
@@ -330,42 +333,45 @@ __global__ void __launch_bounds__(TILEM_THREADS) k_trsv_tiles_multi(TileArgs<dou
         const int l0 = __ldg(P.tile_lvl + t), l1 = __ldg(P.tile_lvl + t + 1);
         const int h0 = __ldg(P.halo_ptr + t), h1 = __ldg(P.halo_ptr + t + 1);
         const int rows = p1 - p0;
-        TileRowM<UPPER> cur, nxt;
-        {
-            const int pos = __ldg(P.lvl_ptr + l0) + pr;
-            if (pos < __ldg(P.lvl_ptr + l0 + 1)) cur.load(P, dinv, rhs, pos, k, col, col_ok);
+        const int e0 = __ldg(P.prp + p0), e1 = __ldg(P.prp + p1);
+        for (int i = tid; i < rows; i += TILEM_THREADS) cp_async4(s_row + i, P.perm + p0 + i);
+        cp_async_commit();
+        for (int i = tid; i <= rows; i += TILEM_THREADS) cp_async4(s_eptr + i, P.prp + p0 + i);
+        for (int i = tid; i < e1 - e0; i += TILEM_THREADS) {
+            cp_async4(s_pci + i, P.pci + e0 + i);
+            cp_async8(s_pv + i, P.pv + e0 + i);
         }
+        if (UPPER)
+            for (int i = tid; i < rows; i += TILEM_THREADS) cp_async8(s_dinv + i, dinv + p0 + i);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        for (int i = pr; i < rows; i += RSTEP)
+            if (col_ok) cp_async8(s_rhs + i * KC + pc, rhs + (long)s_row[i] * k + col);
+        cp_async_commit();
         for (int h = h0 + pr; h < h1; h += RSTEP) {
             double y = 0.0;
             if (ok && col_ok) ok = tile_poll<double>(self + (long)__ldg(P.halo_row + h) * k + col, err, backoff_ns, y);
             ysh[(rows + (h - h0)) * KC + pc] = y;
         }
+        cp_async_wait<0>();
         __syncthreads();
         for (int l = l0; l < l1; l++) {
-            const int pa = __ldg(P.lvl_ptr + l), pb = __ldg(P.lvl_ptr + l + 1);
-            nxt.p = -1;
-            if (l + 1 < l1) {
-                const int pos = pb + pr;
-                if (pos < __ldg(P.lvl_ptr + l + 2)) nxt.load(P, dinv, rhs, pos, k, col, col_ok);
-            }
-            for (int pos = pa + pr; pos < pb; pos += RSTEP) {
-                TileRowM<UPPER> r;
-                if (pos == cur.p) r = cur;
-                else r.load(P, dinv, rhs, pos, k, col, col_ok);
-                double acc = UPPER ? r.rhsv * r.dv : r.rhsv;
-                const long rq = (long)r.row * k + col;
-                if (reset_other && col_ok) reset_other[rq] = Sentinel<double>::value();
-#pragma unroll
-                for (int j = 0; j < TILE_PF; j++)
-                    if (r.k0 + j < r.k1) acc = msub(acc, ysh[r.c[j] * KC + pc], r.f[j]);
-                for (int e = r.k0 + TILE_PF; e < r.k1; e++) acc = msub(acc, ysh[__ldg(P.pci + e) * KC + pc], __ldg(P.pv + e));
-                ysh[(pos - p0) * KC + pc] = acc;
+            const int pa = __ldg(P.lvl_ptr + l) - p0, pb = __ldg(P.lvl_ptr + l + 1) - p0;
+            for (int i = pa + pr; i < pb; i += RSTEP) {
+                const int row = s_row[i];
+                double acc = 0.0;
+                if (col_ok) acc = UPPER ? s_rhs[i * KC + pc] * s_dinv[i] : s_rhs[i * KC + pc];
+                const int k1 = s_eptr[i + 1] - e0;
+                for (int q = s_eptr[i] - e0; q < k1; q++) acc = msub(acc, ysh[s_pci[q] * KC + pc], s_pv[q]);
+                ysh[i * KC + pc] = acc;
                 if (col_ok) {
+                    const long rq = (long)row * k + col;
+                    if (reset_other) reset_other[rq] = Sentinel<double>::value();
                     st_publish(self + rq, acc);
                     if (out_user) out_user[rq] = acc;
                 }
             }
-            cur = nxt;
             __syncthreads();
         }
     }
@@ -402,7 +408,7 @@ struct BatchPrecond {
 inline int tiles_multi_kc(const TriDev &T, int k)
 {
     int kc = std::min(k, 4);
-    while (kc > 1 && (size_t)T.tile_elems * kc * sizeof(double) > TILE_SMEM_MAX) kc--;
+    while (kc > 1 && TileSmemM::of(T.t_max_rows, T.t_max_halo, T.t_max_entries, kc).total > TILE_SMEM_MAX) kc--;
     return kc;
 }
 
@@ -415,7 +421,8 @@ inline void launch_trsv_multi(const TriDev &T, int k, unsigned *ticket, const do
     if (T.tiled) {
         const int kc = tiles_multi_kc(T, k);
         const int ng = (k + kc - 1) / kc;
-        const size_t smem = (size_t)T.tile_elems * kc * sizeof(double);
+        const size_t smem = TileSmemM::of(T.t_max_rows, T.t_max_halo, T.t_max_entries, kc).total;
+        if (smem > TILE_SMEM_MAX) throw Status(XS_ERR_UNSUPPORTED);
         const int fit = std::max(1, (int)((220u * 1024u) / (smem + 1024)));
         const int g = std::min(T.ntiles * ng, geom().sms * std::min(2, fit));
         // the largest dynamic shared memory is enabled once per kernel, at

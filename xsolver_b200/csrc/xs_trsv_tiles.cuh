@@ -75,8 +75,8 @@ inline void host_parallel_for(long count, long chunk, F fn)
 // with at least min_rows rows whose pattern fits a grid.  Process-wide;
 // fixed when a preconditioner's triangles are analysed.
 struct TileTuning {
-    int enable = 0;  // off until the box kernel beats the level-ordered one on every measured case
-    int tx = 16, ty = 16, tz = 16;
+    int enable = 1;
+    int tx = 16, ty = 16, tz = 8;
     int min_rows = 65536;
     int blocks_per_sm = 4;
 };
@@ -121,10 +121,10 @@ inline bool offset_fits(long o, long nx, long nxy, int reach)
 // logical(r) maps a row to its logical index (dependencies at smaller ones).
 template <typename LogF>
 inline int grid_reach(int n, const int *rp, const int *ci, LogF logical, const GridCoord &g, int reach,
-                      std::vector<int> &vecs)
+                      std::vector<int> &vecs, int row_step = 1)
 {
     const int W = 2 * reach + 1;
-    const long RB = 65536;  // rows per work item
+    const long RB = 65536L * row_step;  // rows per work item
     const long items = (n + RB - 1) / RB;
     std::vector<int> worst_of(items, 0);
     std::vector<std::vector<char>> seen_of(items);
@@ -133,7 +133,7 @@ inline int grid_reach(int n, const int *rp, const int *ci, LogF logical, const G
         std::vector<char> seen((size_t)W * W * W, 0);
         int worst = 0;
         const int r0 = (int)(it * RB), r1 = (int)std::min<long>(n, r0 + RB);
-        for (int r = r0; r < r1 && !over.load(std::memory_order_relaxed); r++) {
+        for (int r = r0; r < r1 && !over.load(std::memory_order_relaxed); r += row_step) {
             int xi, yi, zi;
             g.of(logical(r), xi, yi, zi);
             for (int k = rp[r]; k < rp[r + 1]; k++) {
@@ -183,13 +183,15 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
     const long nnz = rp[n];
     if (n < 8 || nnz == 0) return false;
     auto logical = [&](int r) -> long { return upper ? (long)n - 1 - r : (long)r; };
-    // distinct offsets |row - dep| (give up beyond 512 of them)
+    // distinct offsets |row - dep| of a sample of rows (give up beyond 512
+    // of them); a grid chosen from them is checked on every entry below
+    const int step = std::max(1, n / 16384);
     std::vector<long> offs;
     {
         const int TAB = 2048;
         std::vector<long> tab(TAB, -1);
         int cnt = 0;
-        for (int r = 0; r < n && cnt <= 512; r++)
+        for (int r = 0; r < n && cnt <= 512; r += step)
             for (int k = rp[r]; k < rp[r + 1]; k++) {
                 const long o = std::labs((long)ci[k] - r);
                 unsigned hsh = (unsigned)((o * 2654435761ul) % TAB);
@@ -235,13 +237,23 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
                 if (ok) cands.push_back({nx, nxy});
             }
         }
-        for (const Cand &c : cands) {
-            const GridCoord gc{c.nx, c.nxy};
+        // rank the candidates on the sampled rows, then check the best ones
+        // on every entry
+        std::vector<std::pair<int, int>> rank;  // (sampled reach, candidate)
+        for (int q = 0; q < (int)cands.size(); q++) {
+            const GridCoord gc{cands[q].nx, cands[q].nxy};
+            const int r = grid_reach(n, rp, ci, logical, gc, R, v, step);
+            if (r <= R) rank.push_back({r, q});
+        }
+        std::sort(rank.begin(), rank.end());
+        for (const auto &rq : rank) {
+            const GridCoord gc{cands[rq.second].nx, cands[rq.second].nxy};
             const int r = grid_reach(n, rp, ci, logical, gc, R, v);
             if (r <= R && r < best_reach) {
                 best_reach = r;
                 g = gc;
                 vecs = v;
+                break;
             }
         }
     }
