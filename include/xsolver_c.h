@@ -425,6 +425,12 @@ int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows);
  * hand-off per level).  0 disables it; default: no row limit beyond the
  * shared-memory one.  Environment XS_TRSV_BLOCK_ROWS sets it at first use. */
 int xs_set_trsv_block_rows(int max_rows);
+/* Single-CTA LU solve form: 1 (default) copies whole dependency levels, in
+ * batches of up to 512 rows and 2048 entries, into shared memory with
+ * asynchronous copies one batch ahead, so a level reads shared memory only;
+ * 0 loads each row's data from global memory one level ahead.  Same result
+ * either way.  Environment XS_LU_STAGED sets it at first use. */
+int xs_set_trsv_block_staging(int enable);
 /* Jacobi-sweep preconditioner apply: 1 computes sweeps 2 and 3 of each
  * narrow diagonal-slot triangle in one pass (each row recomputes the
  * second-sweep values of its neighbours; same result, about half the DRAM

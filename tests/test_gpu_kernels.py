@@ -329,18 +329,20 @@ def test_parilut_fallback_paths_bitwise(cuda):
 
 
 def test_block_and_syncfree_lusolve_bitwise(cuda):
-    """The single-CTA solve (small systems) and the sync-free multi-CTA solve
-    give the same bits, FP64 and FP32/BF16 factors."""
+    """The single-CTA solve (small systems; staged level batches and
+    per-level loads) and the sync-free multi-CTA solve give the same bits,
+    FP64 and FP32/BF16 factors."""
     import torch
     from xsolver_b200 import _lib
     from xsolver_b200.api import Plan
 
     L = _lib.lib()
-    for A in (st.poisson2d_5pt(128), st.convdiff3d_27pt(14)):
+    for A in (st.poisson2d_5pt(128), st.convdiff3d_27pt(14), st.convdiff3d_27pt(24)):
         x = st.rhs_uniform(A.n, 11)
         outs = []
-        for rows in (1 << 30, 0):
+        for rows, staged in ((1 << 30, 1), (1 << 30, 0), (0, 1)):
             assert L.xs_set_trsv_block_rows(rows) == 0
+            assert L.xs_set_trsv_block_staging(staged) == 0
             try:
                 P = Plan(A).factor("ilu0")
                 # device inputs stay referenced until the plan's stream is synchronised
@@ -356,8 +358,10 @@ def test_block_and_syncfree_lusolve_bitwise(cuda):
                 outs.append((z.cpu().numpy(), z32.cpu().numpy()))
             finally:
                 L.xs_set_trsv_block_rows(1 << 30)
-        assert np.array_equal(outs[0][0], outs[1][0]), A.name
-        assert np.array_equal(outs[0][1], outs[1][1]), A.name
+                L.xs_set_trsv_block_staging(1)
+        for o in outs[1:]:
+            assert np.array_equal(outs[0][0], o[0]), A.name
+            assert np.array_equal(outs[0][1], o[1]), A.name
         assert np.array_equal(outs[0][0], oracle.lusolve(oracle.ilu0(A), x)), A.name
 
 

@@ -101,6 +101,7 @@ def _declare(L):
                          _ip, _ip],
         "xs_set_ell_index_bits": [C.c_int],
         "xs_set_trsv_block_rows": [C.c_int],
+        "xs_set_trsv_block_staging": [C.c_int],
         "xs_set_sweep_fusion": [C.c_int],
         "xs_set_launch_overlap": [C.c_int],
         "xs_set_vector_fusion": [C.c_int],

@@ -127,6 +127,7 @@ TrsvTuning &trsv_tuning()
         if (const char *e = getenv("XS_TRSV_CHUNK_ROWS")) t.chunk_rows = std::max(0, atoi(e));
         if (const char *e = getenv("XS_TRSV_BLOCK_ROWS")) t.block_max_rows = std::max(0, atoi(e));
         if (const char *e = getenv("XS_SWEEP_FUSE")) t.fuse_sweeps = atoi(e) != 0;
+        if (const char *e = getenv("XS_LU_STAGED")) t.lu_staged = atoi(e) != 0;
         init = true;
     }
     return t;
@@ -1645,6 +1646,11 @@ int xs_set_trsv_block_rows(int max_rows)
         if (max_rows < 0) throw Status(XS_ERR_INVALID);
         trsv_tuning().block_max_rows = max_rows;
     });
+}
+
+int xs_set_trsv_block_staging(int enable)
+{
+    return guarded([&] { trsv_tuning().lu_staged = enable != 0; });
 }
 
 int xs_set_ell_index_bits(int bits)

@@ -37,6 +37,12 @@ namespace xs {
 
 constexpr int TRSV_THREADS = 128;
 constexpr int TRSV_CHUNK = 8;
+// single-CTA LU solve: the solution vector in shared memory (at most this
+// many bytes); the staged form also holds two level batches of at most
+// LUB_ROWS rows and LUB_ENTRIES entries
+constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
+constexpr int LUB_ROWS = 512, LUB_ENTRIES = 2048;
+constexpr size_t LU_SMEM_LIMIT = 227 * 1024;
 
 template <typename FT>
 struct TrsvArgs {
@@ -92,6 +98,9 @@ struct TrsvTuning {
     // 54 us against 55 us (BF16) and 94 against 87 us (FP64) — the neighbour
     // re-reads from L2 cost what the saved DRAM traffic gained)
     int fuse_sweeps = 0;
+    // single-CTA solve with its level batches staged in shared memory (1) or
+    // its row data loaded one level ahead from global memory (0)
+    int lu_staged = 1;
 };
 TrsvTuning &trsv_tuning();
 
@@ -843,6 +852,12 @@ struct TriDev {
     // tile layout (perm/prp/pci then hold the box-major order, pci = shared-
     // memory slots); lvperm keeps the dependency-level order for the
     // factorisation kernels, which take rows in level order
+    // single-CTA staged solve (small systems): consecutive whole levels in
+    // batches of at most LUB_ROWS rows and LUB_ENTRIES entries; lub[b] is
+    // batch b's first level (nlub + 1 values), or -1 - level for a level too
+    // large to stage (solved from global memory)
+    int nlub = 0;
+    DBuf<int> lub;
     bool tiled = false;
     int ntiles = 0, tile_elems = 0;  // tile_elems: shared-memory values per box (rows + halo)
     int t_max_rows = 0, t_max_halo = 0, t_max_entries = 0;
@@ -1010,6 +1025,38 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
                                         T.src.p);
         check_launch();
         T.lstart.alloc(P.nlevels + 1); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
+        // level batches of the staged single-CTA solve (systems it serves only)
+        T.nlub = 0;
+        T.lub.free();
+        if ((size_t)n * sizeof(double) <= LU_BLOCK_SMEM_MAX) {
+            std::vector<int> b;
+            int l = 0;
+            while (l < P.nlevels) {
+                const int p0 = P.lstart[l];
+                int l1 = l, rows = 0;
+                long ents = 0;
+                while (l1 < P.nlevels) {
+                    const int r = P.lstart[l1 + 1] - P.lstart[l1];
+                    const long e = (long)P.prp[P.lstart[l1 + 1]] - P.prp[P.lstart[l1]];
+                    if (rows + r > LUB_ROWS || ents + e > LUB_ENTRIES) break;
+                    rows += r;
+                    ents += e;
+                    l1++;
+                }
+                (void)p0;
+                if (l1 == l) {  // one level larger than a batch: solved unstaged
+                    b.push_back(-1 - l);
+                    l++;
+                } else {
+                    b.push_back(l);
+                    l = l1;
+                }
+            }
+            b.push_back(P.nlevels);
+            T.nlub = (int)b.size() - 1;
+            T.lub.alloc(b.size());
+            T.lub.upload(b.data(), b.size(), s);
+        }
     } else {
         TriChunkPlan C;
         tri_analyse_chunked(n, rp.data(), ci.data(), upper, src_of, chr, C);
@@ -1109,7 +1156,6 @@ inline void load_tri_ell(TriDev &T, const double *vals, bool need32, cudaStream_
 // trsv_row, so results are bitwise identical to the sync-free solve.  The
 // sync-free solve buffers are not touched (they stay armed).
 constexpr int LU_BLOCK_THREADS = 1024;
-constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
 
 // One thread's row of a level, loaded ahead: the row, its entry range, the
 // first LU_PF entries and the row's scalar input (x[row] for L, dinv for U).
@@ -1199,6 +1245,110 @@ __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_block(TrsvArgs<FT> L, c
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) z[i] = ys[i];
 }
 
+// ---- staged single-CTA solve: the level batches of each triangle are
+// copied into shared memory by asynchronous copies one batch ahead, so a
+// level reads only shared memory (the row data of the plain form above
+// arrives from global memory one level ahead, a memory latency per level).
+// The solution vector starts as x (its own slot is a row's right-hand side
+// in the L phase) and is overwritten level by level; row arithmetic and
+// entry order are those of trsv_row, so results are bitwise the same.
+template <typename FT, typename DT>
+struct LuBatchSmem {
+    static constexpr size_t row = 0;
+    static constexpr size_t eptr = row + ((LUB_ROWS * sizeof(int) + 15) & ~(size_t)15);
+    static constexpr size_t in = eptr + (((LUB_ROWS + 1) * sizeof(int) + 15) & ~(size_t)15);
+    static constexpr size_t pci = in + ((LUB_ROWS * sizeof(DT) + 15) & ~(size_t)15);
+    static constexpr size_t pv = pci + ((LUB_ENTRIES * sizeof(int) + 15) & ~(size_t)15);
+    static constexpr size_t bytes = pv + ((LUB_ENTRIES * sizeof(FT) + 8 + 15) & ~(size_t)15);
+};
+
+template <typename VT, typename FT, typename DT, bool UPPER>
+__device__ __forceinline__ void lus_phase(const TrsvArgs<FT> &P, const int *__restrict__ ls, const int *__restrict__ lub,
+                                          int nb, const DT *__restrict__ dinv, VT *ys, unsigned char *buf0,
+                                          unsigned char *buf1)
+{
+    using B = LuBatchSmem<FT, DT>;
+    const int tid = threadIdx.x, T = blockDim.x;
+    auto first_level = [&](int b) { const int v = __ldg(lub + b); return v < 0 ? -1 - v : v; };
+    auto stage = [&](int b, unsigned char *buf) {
+        if (b < nb && __ldg(lub + b) >= 0) {
+            const int pa = __ldg(ls + first_level(b)), pb = __ldg(ls + first_level(b + 1));
+            const int ea = __ldg(P.prp + pa), eb = __ldg(P.prp + pb);
+            int *s_row = (int *)(buf + B::row), *s_eptr = (int *)(buf + B::eptr), *s_pci = (int *)(buf + B::pci);
+            for (int i = tid; i < pb - pa; i += T) cp_async4(s_row + i, P.perm + pa + i);
+            for (int i = tid; i <= pb - pa; i += T) cp_async4(s_eptr + i, P.prp + pa + i);
+            for (int i = tid; i < eb - ea; i += T) cp_async4(s_pci + i, P.pci + ea + i);
+            const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L, vb1 = ((long)eb * (long)sizeof(FT) + 3) & ~3L;
+            const unsigned char *vsrc = (const unsigned char *)P.pv;
+            for (long w = tid; w < (vb1 - vb0) / 4; w += T) cp_async4(buf + B::pv + 4 * w, vsrc + vb0 + 4 * w);
+            if (UPPER)
+                for (int i = tid; i < pb - pa; i += T) cp_async_n<sizeof(DT)>((DT *)(buf + B::in) + i, dinv + pa + i);
+        }
+        cp_async_commit();  // an empty group for an unstaged or absent batch keeps the count uniform
+    };
+    stage(0, buf0);
+    for (int b = 0; b < nb; b++) {
+        unsigned char *cur = (b & 1) ? buf1 : buf0;
+        stage(b + 1, (b & 1) ? buf0 : buf1);
+        cp_async_wait<1>();  // batch b's copies have landed
+        __syncthreads();
+        const int lb = __ldg(lub + b);
+        if (lb >= 0) {
+            const int l0 = lb, l1 = first_level(b + 1);
+            const int pa = __ldg(ls + l0), ea = __ldg(P.prp + pa);
+            const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L;
+            const int *s_row = (const int *)(cur + B::row), *s_eptr = (const int *)(cur + B::eptr);
+            const int *s_pci = (const int *)(cur + B::pci);
+            const DT *s_in = (const DT *)(cur + B::in);
+            const FT *pv = (const FT *)(cur + B::pv + ((long)ea * (long)sizeof(FT) - vb0));
+            for (int l = l0; l < l1; l++) {
+                const int q0 = __ldg(ls + l) - pa, q1 = __ldg(ls + l + 1) - pa;
+                for (int i = q0 + tid; i < q1; i += T) {
+                    const int row = s_row[i];
+                    VT acc = UPPER ? (VT)(ys[row] * (VT)s_in[i]) : ys[row];
+                    const int k1 = s_eptr[i + 1] - ea;
+                    for (int k = s_eptr[i] - ea; k < k1; k++) acc = msub(acc, ys[s_pci[k]], (VT)FVal<FT>::cvt(pv[k]));
+                    ys[row] = acc;
+                }
+                __syncthreads();
+            }
+        } else {  // one level too large to stage: its rows from global memory
+            const int l = -1 - lb;
+            for (int p = __ldg(ls + l) + tid; p < __ldg(ls + l + 1); p += T) {
+                const int row = __ldg(P.perm + p);
+                VT acc = UPPER ? (VT)(ys[row] * (VT)__ldg(dinv + p)) : ys[row];
+                for (int k = __ldg(P.prp + p); k < __ldg(P.prp + p + 1); k++)
+                    acc = msub(acc, ys[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
+                ys[row] = acc;
+            }
+            __syncthreads();
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+}
+
+template <typename VT, typename FT, typename DT>
+__global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_staged(TrsvArgs<FT> L, const int *__restrict__ lstart,
+                                                                 const int *__restrict__ lubL, int nbL, TrsvArgs<FT> U,
+                                                                 const int *__restrict__ ustart,
+                                                                 const int *__restrict__ lubU, int nbU,
+                                                                 const DT *__restrict__ dinv, const VT *__restrict__ x,
+                                                                 VT *__restrict__ z, const int *done_flag)
+{
+    extern __shared__ __align__(16) unsigned char lus_smem[];
+    if (done_flag && *done_flag) return;
+    using B = LuBatchSmem<FT, DT>;
+    const size_t yb = ((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15;
+    VT *ys = (VT *)lus_smem;
+    unsigned char *buf0 = lus_smem + yb, *buf1 = buf0 + B::bytes;
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) ys[i] = x[i];
+    __syncthreads();
+    lus_phase<VT, FT, DT, false>(L, lstart, lubL, nbL, nullptr, ys, buf0, buf1);
+    lus_phase<VT, FT, DT, true>(U, ustart, lubU, nbU, dinv, ys, buf0, buf1);
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) z[i] = ys[i];
+}
+
 // whether the single-CTA solve serves this pair of plans for vectors of VT
 template <typename VT>
 inline bool lu_block_ok(const TriDev &L, const TriDev &U)
@@ -1212,6 +1362,21 @@ template <typename VT, typename FT, typename DT>
 inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, const VT *x, VT *z, const int *done_flag,
                             cudaStream_t s)
 {
+    // the staged form when both triangles have level batches and the
+    // solution vector plus two batches fit in shared memory
+    const size_t ssm = (((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15) + 2 * LuBatchSmem<FT, DT>::bytes;
+    if (L.nlub > 0 && U.nlub > 0 && ssm <= LU_SMEM_LIMIT && trsv_tuning().lu_staged) {
+        static size_t sattr = 0;
+        if (ssm > sattr) {
+            XS_CUDA(cudaFuncSetAttribute(k_lu_staged<VT, FT, DT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ssm));
+            sattr = ssm;
+        }
+        k_lu_staged<VT, FT, DT><<<1, LU_BLOCK_THREADS, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
+                                                                  U.args<FT>(), U.lstart.p, U.lub.p, U.nlub, dinv, x,
+                                                                  z, done_flag);
+        return;
+    }
     static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
     const size_t smem = (size_t)L.n * sizeof(VT);
     if (smem > attr) {
