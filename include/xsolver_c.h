@@ -83,13 +83,19 @@ void xsolver_ksp_setoption(double tol, int maxiter, int *usediter, double *resve
 /* hip/xsolver_c.cpp:150-263: "jacobi", "ilu0", "ic0", "ilut" (GPU ParILUT),
  * "ilu0_mkl"/"ilut_mkl" (mapped to ilu0/ilut as the reference does on GPU),
  * plus "parilu" and "none".  "ic0" needs a structurally symmetric pattern
- * (XS_ERR_UNSUPPORTED at solve otherwise); "ict" records XS_ERR_UNSUPPORTED
- * (the reference exits for it on GPU).  Must follow xsolver_ksp_settype. */
+ * (XS_ERR_UNSUPPORTED at solve otherwise).  "ict" (incomplete Cholesky with
+ * threshold, the reference's CPU-only ICT: it exits for it on GPU) and
+ * "ilup"/"ilut_saad" (Saad's ILUT, the reference's CPU "ilut") are factored
+ * on the host by the reference's sequential algorithms and applied by the
+ * GPU triangular solves.  Must follow xsolver_ksp_settype. */
 void xsolver_pc_settype(char *fmt);
 /* hip/xsolver_c.cpp:268-273.  For "ilut": max_fill is the ParILUT fill
- * factor, tol its drop tolerance. */
+ * factor, tol its drop tolerance; for "ilup": Saad ILUT's entries per row
+ * part (lfil) and drop tolerance (defaults 20, 1e-5). */
 void xsolver_pc_setilut(double tol, int max_fill);
-/* hip/xsolver_c.cpp:264-267.  ICT is not provided: records XS_ERR_UNSUPPORTED. */
+/* hip/xsolver_c.cpp:264-267.  For "ict" (ignored otherwise): drop tolerance
+ * and kept entries per row (defaults 1e-8, 100; max_fill is clamped to n-1).
+ * As in the reference, the pivot substitute uses the fixed scale 1e-4. */
 void xsolver_pc_setict(double tol, int max_fill);
 /* hip/xsolver_c.cpp:274-292.  sol holds x0 on entry, the solution on exit. */
 void xsolver_solve(double *rhs, double *sol);
@@ -151,7 +157,11 @@ int xs_ksp_settype(xs_handle_t h, const char *fmt);
 int xs_ksp_setoption(xs_handle_t h, double tol, int maxiter, int *usediter, double *resvec, int restart);
 int xs_ksp_set_absolute_tol(xs_handle_t h, double absolute_tol);
 int xs_pc_settype(xs_handle_t h, const char *fmt);
+/* ParILUT ("ilut") fill and drop tolerance, and Saad ILUT ("ilup") lfil and
+ * drop tolerance */
 int xs_pc_setilut(xs_handle_t h, double tol, int max_fill);
+/* ICT drop tolerance (> 0) and kept entries per row */
+int xs_pc_setict(xs_handle_t h, double tol, int max_fill);
 int xs_pc_setparilu(xs_handle_t h, int sweeps);
 int xs_pc_setparilut(xs_handle_t h, double fill, int sweeps, double droptol);
 int xs_pc_set_trsv(xs_handle_t h, int mode);
@@ -278,10 +288,23 @@ int xs_plan_spmv(xs_plan_t p, int format, int precision, const void *d_x, void *
 int xs_plan_spmv_t(xs_plan_t p, const double *d_x, double *d_y);
 /* ILU factorisation on the device: kind 0 exact ILU(0) (sync-free, same
  * operation order as the reference CPU ILU(0)), 1 ParILU (sweeps),
- * 2 ParILUT (fill, sweeps, droptol) */
+ * 2 ParILUT (fill, sweeps, droptol); on the host, applied on the device:
+ * 4 Saad ILUT (fill = lfil >= 1, droptol), 5 ICT (fill = kept entries per
+ * row, droptol > 0) */
 int xs_plan_factor(xs_plan_t p, int kind, int sweeps, double fill, double droptol);
 /* copy the factors to the host in the seqilu0 layout (L strict lower, dinv,
  * U' = dinv-row-scaled strict upper).  Pass NULL arrays to query nnzL/nnzU. */
+/* Host threshold factorizations without a device (no handle): Saad ILUT
+ * (hip/Precond/ilut_diag_in_csr.cpp:20-251 split as hip/HostMatrix/
+ * HostMatrixCSR.cpp:230-268) and ICT (hip/Precond/ict_l.cpp:112-212
+ * converted as hip/HostMatrix/HostMatrixCSR.cpp:327-384) of a sorted
+ * 0-based CSR matrix, in the layout of xs_plan_get_factors.  lci/lv and
+ * uci/uv hold at least n*lfil (ILUT) or n*min(maxfil, n-1) (ICT) entries;
+ * lrp/urp n+1, dinv n.  ICT: XS_ERR_NO_DIAG for a row without a diagonal. */
+int xs_host_ilut(int n, const int *rp, const int *ci, const double *v, int lfil, double droptol, int *nnzL, int *nnzU,
+                 int *lrp, int *lci, double *lv, double *dinv, int *urp, int *uci, double *uv);
+int xs_host_ict(int n, const int *rp, const int *ci, const double *v, int maxfil, double droptol, int *nnzL, int *nnzU,
+                int *lrp, int *lci, double *lv, double *dinv, int *urp, int *uci, double *uv);
 int xs_plan_get_factors(xs_plan_t p, int *nnzL, int *nnzU, int *lrp, int *lci, double *lv, double *dinv, int *urp,
                         int *uci, double *uv);
 /* combined LU values over A's pattern (exact ILU(0) / ParILU only) */

@@ -5,7 +5,9 @@ ctypes bindings for
                             (xs_oracle.cpp, every function cites the reference
                             file:line it restates), and
   _ref/libxsref_intel.so    the reference's own intel/ CPU solver compiled from
-  _ref/libxsref_ilu0.so     its sources, and its hip ilu0_simple (Makefile).
+  _ref/libxsref_ilu0.so     its sources, its hip ilu0_simple and ilutp_final,
+  _ref/libxsref_ic0.so      IC(0) and
+  _ref/libxsref_ict.so      ICT (Makefile).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
 this package, as the checker or the timed CPU baseline.  The product path
@@ -341,6 +343,95 @@ def parilut(A, fill=2.0, sweeps=5, droptol=0.0) -> LU:
         lib().orc_free(C.cast(p, C.c_void_p))
     del L
     return LU(n, lrp, lci, lv, dinv, urp, uci, uv)
+
+
+ICT_SMALLNUM = 1e-4  # the constant the reference's seqict passes (hip/HostMatrix/HostMatrixCSR.cpp:331)
+
+
+def _tri_out(n, cap):
+    cap = max(cap, 1)
+    return (np.zeros(n + 1, np.int32), np.zeros(cap, np.int32), np.zeros(cap), np.zeros(max(n, 1)),
+            np.zeros(n + 1, np.int32), np.zeros(cap, np.int32), np.zeros(cap))
+
+
+def _tri_lu(n, o):
+    lrp, lci, lv, dinv, urp, uci, uv = o
+    nl, nu = int(lrp[-1]), int(urp[-1])
+    return LU(n, lrp, lci[:nl].copy(), lv[:nl].copy(), dinv[:n].copy(), urp, uci[:nu].copy(), uv[:nu].copy())
+
+
+def ilut_saad(A, lfil=20, droptol=1e-5) -> LU:
+    """Saad ILUT (restatement of ilutp_final + seqilut) in the seqilu0 layout."""
+    o = _tri_out(A.n, A.n * lfil)
+    lib().orc_ilut_saad(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), C.c_int(lfil),
+                        C.c_double(droptol), *[_p(a, a.dtype.type) for a in o])
+    return _tri_lu(A.n, o)
+
+
+def ict(A, maxfil=100, droptol=1e-8) -> LU:
+    """ICT (restatement of ict_csr_A_l + seqict) in the seqilu0 layout."""
+    m = min(maxfil, max(A.n - 1, 0))
+    o = _tri_out(A.n, A.n * m)
+    rc = lib().orc_ict(A.n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), C.c_int(maxfil),
+                       C.c_double(droptol), *[_p(a, a.dtype.type) for a in o])
+    if rc >= 0:
+        raise ValueError(f"row {rc} has no diagonal entry")
+    return _tri_lu(A.n, o)
+
+
+def ref_ilut_saad(A, lfil=20, droptol=1e-5):
+    """The reference's own ilutp_final (compiled into oracle/_ref) split as
+    its seqilut does (hip/HostMatrix/HostMatrixCSR.cpp:230-268), or None
+    when it was not built."""
+    r = ref_ilu0()
+    if r is None or not hasattr(r, "ref_ilutp_final"):
+        return None
+    n = A.n
+    cap = (2 * lfil + 2) * n
+    luval = np.zeros(cap); lucols = np.zeros(cap, np.int32)
+    lurows = np.zeros(n + 1, np.int32); uptr = np.zeros(n + 1, np.int32); diag = np.zeros(max(n, 1))
+    r.ref_ilutp_final(_p(luval), _p(A.val.copy()), _p(A.rowptr.copy(), np.int32), _p(A.colidx.copy(), np.int32),
+                      C.c_int(n), _p(diag), C.c_int(lfil), _p(lucols, np.int32), _p(lurows, np.int32),
+                      _p(uptr, np.int32), C.c_double(droptol))
+    lrp = [0]; urp = [0]; lci = []; lv = []; uci = []; uv = []
+    for i in range(n):
+        lci.extend(lucols[lurows[i]:uptr[i]]); lv.extend(luval[lurows[i]:uptr[i]])
+        uci.extend(lucols[uptr[i] + 1:lurows[i + 1]]); uv.extend(luval[uptr[i] + 1:lurows[i + 1]] * diag[i])
+        lrp.append(len(lci)); urp.append(len(uci))
+    return LU(n, np.array(lrp, np.int32), np.array(lci, np.int32), np.array(lv), diag[:n].copy(),
+              np.array(urp, np.int32), np.array(uci, np.int32), np.array(uv))
+
+
+def ref_ict(A, maxfil=100, droptol=1e-8):
+    """The reference's own ict_csr_A_l (compiled into oracle/_ref), converted
+    as its seqict does (hip/HostMatrix/HostMatrixCSR.cpp:327-384), or None
+    when it was not built."""
+    path = os.path.join(HERE, "_ref", "libxsref_ict.so")
+    if not os.path.exists(path):
+        return None
+    R = C.CDLL(path)
+    n = A.n
+    m = min(maxfil, n - 1)  # hip/Precond/precon_ict.cpp:3-4
+    cap = m * n + n
+    lp = np.zeros(n + 1, np.int32); lval = np.zeros(cap); lcol = np.zeros(cap, np.int32)
+    R.ref_ict_csr_A_l(n, _p(A.rowptr.copy(), np.int32), _p(A.val.copy()), _p(A.colidx.copy(), np.int32),
+                      _p(lp, np.int32), _p(lval), _p(lcol, np.int32), C.c_double(ICT_SMALLNUM), C.c_double(droptol),
+                      C.c_int(m))
+    d = lval[lp[1:] - 1]
+    lrp = [0]; lci = []; lv = []
+    ucols = [[] for _ in range(n)]
+    for i in range(n):
+        for q in range(lp[i], lp[i + 1] - 1):
+            j = int(lcol[q]); x = lval[q] * d[j]
+            lci.append(j); lv.append(x); ucols[j].append((i, x))
+        lrp.append(len(lci))
+    urp = [0]; uci = []; uv = []
+    for j in range(n):
+        for i, x in ucols[j]:
+            uci.append(i); uv.append(x)
+        urp.append(len(uci))
+    return LU(n, np.array(lrp, np.int32), np.array(lci, np.int32), np.array(lv), d * d,
+              np.array(urp, np.int32), np.array(uci, np.int32), np.array(uv))
 
 
 def lusolve(F: LU, x) -> np.ndarray:

@@ -27,12 +27,18 @@
  *   - ParILUT: hip/Precond/parilut.cpp:621-1206 (parilut_clean) with the sweep
  *     kernels :392-560, threshold removal :283-380 and k-th select
  *     par_ilut_hip/select_kth.h:501; restated with synchronous sweeps.
+ *   - Saad ILUT: hip/Precond/ilut_diag_in_csr.cpp:20-251 (ilutp_final) with
+ *     the split of hip/HostMatrix/HostMatrixCSR.cpp:230-268 (seqilut).
+ *   - ICT: hip/Precond/ict_l.cpp:112-205 (calTnorm, ict_fact_l) with the
+ *     conversion of hip/HostMatrix/HostMatrixCSR.cpp:327-384 (seqict).
  *
  * The only deliberate departure from the intel loops: intel's
  * preconditionerCPU() is a no-op unless "Jacobi" was selected
  * (intel/HostMatrix.h:170-176); here "no preconditioner" is an identity copy.
  */
 #include <algorithm>
+#include <functional>
+#include <queue>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -1623,6 +1629,248 @@ int orc_levels_lower(int n, const int *rp, const int *ci, int *level)
         maxl = std::max(maxl, l);
     }
     return maxl + 1;
+}
+
+
+// ---------------------------------------------------------------- Saad ILUT
+// hip/Precond/ilut_diag_in_csr.cpp:20-251 (ilutp_final; lfil >= 1) and the
+// split of hip/HostMatrix/HostMatrixCSR.cpp:230-268.  Output arrays hold
+// n*lfil entries.  The kept entries of a row part form a heap with the
+// smallest magnitude on top: insertion sifts up past parents of strictly
+// larger magnitude (the std::push_heap of the reference with its
+// magnitude comparator, :7-15, :100-103), a replacement of the top sinks it
+// past children of magnitude <= its own (the reference's heap_swap, :2-19).
+namespace {
+struct KeptHeap {
+    std::vector<int> h;
+    const std::vector<double> *w;
+    double mag(int c) const { return std::fabs((*w)[c]); }
+    void push(int c)
+    {
+        size_t k = h.size();
+        h.push_back(c);
+        while (k > 0) {
+            const size_t par = (k - 1) / 2;
+            if (!(mag(h[par]) > mag(c))) break;
+            h[k] = h[par];
+            k = par;
+        }
+        h[k] = c;
+    }
+    void replace_top(int c)
+    {
+        const size_t len = h.size();
+        const double m = mag(c);
+        size_t hole = 0;
+        for (size_t ch = 1; ch < len; ch = 2 * ch + 1) {
+            if (ch + 1 < len && mag(h[ch]) > mag(h[ch + 1])) ch++;
+            if (mag(h[ch]) > m) break;
+            h[hole] = h[ch];
+            hole = ch;
+        }
+        h[hole] = c;
+    }
+};
+
+void ilut_offer(KeptHeap &K, int lfil, int c, std::vector<double> &w)
+{
+    if ((int)K.h.size() < lfil) {
+        K.push(c);
+    } else if (std::fabs(w[c]) > std::fabs(w[K.h[0]])) {
+        w[K.h[0]] = 0;
+        K.replace_top(c);
+    } else {
+        w[c] = 0;
+    }
+}
+}  // namespace
+
+int orc_ilut_saad(int n, const int *rp, const int *ci, const double *v, int lfil, double droptol, int *lrp, int *lci,
+                  double *lv, double *dinv, int *urp, int *uci, double *uv)
+{
+    std::vector<double> w(n, 0.0), dg(n, 0.0);
+    std::vector<std::vector<int>> ucols(n);      // U part of each factored row
+    std::vector<std::vector<double>> uvals(n);  // (unscaled u_kj)
+    int nl = 0, nu = 0;
+    lrp[0] = urp[0] = 0;
+    for (int i = 0; i < n; i++) {
+        std::priority_queue<int, std::vector<int>, std::greater<int>> lower;
+        std::vector<int> upper;
+        double tsum = 0;
+        for (int q = rp[i]; q < rp[i + 1]; q++) {
+            w[ci[q]] = v[q];
+            tsum += v[q] * v[q];
+            if (ci[q] < i) lower.push(ci[q]);
+            if (ci[q] > i) upper.push_back(ci[q]);
+        }
+        const double tn = std::sqrt(tsum) * droptol;
+        KeptHeap K{{}, &w};
+        while (!lower.empty()) {
+            const int k = lower.top();
+            lower.pop();
+            const double f = w[k] * dg[k];
+            if (std::fabs(f) < tn) {
+                w[k] = 0;
+                continue;
+            }
+            for (size_t t = 0; t < ucols[k].size(); t++) {
+                const int j = ucols[k][t];
+                if (w[j] == 0) {
+                    if (j < i) lower.push(j);
+                    if (j > i) upper.push_back(j);
+                }
+                w[j] = w[j] - f * uvals[k][t];
+            }
+            w[k] = f;
+            ilut_offer(K, lfil, k, w);
+        }
+        std::vector<int> keep = K.h;
+        std::sort(keep.begin(), keep.end());
+        for (int c : keep) {
+            lci[nl] = c;
+            lv[nl++] = w[c];
+            w[c] = 0;
+        }
+        double uii;
+        if (w[i] != 0) {
+            uii = w[i];
+            w[i] = 0;
+        } else {
+            uii = 1e-4 / droptol * tn + tn;
+        }
+        dg[i] = 1 / uii;
+        K.h.clear();
+        for (int c : upper) {
+            if (std::fabs(w[c]) > tn) ilut_offer(K, lfil, c, w);
+            else w[c] = 0;
+        }
+        keep = K.h;
+        std::sort(keep.begin(), keep.end());
+        for (int c : keep) {
+            ucols[i].push_back(c);
+            uvals[i].push_back(w[c]);
+            uci[nu] = c;
+            uv[nu++] = w[c] * dg[i];
+            w[c] = 0;
+        }
+        dinv[i] = dg[i];
+        lrp[i + 1] = nl;
+        urp[i + 1] = nu;
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------- ICT
+// hip/Precond/ict_l.cpp:112-129 (calTnorm), :130-195 (ict_fact_l) with the
+// smallNum the caller of :331 passes (1e-4) and the maxfil clamp of
+// hip/Precond/precon_ict.cpp:3-4; converted as hip/HostMatrix/
+// HostMatrixCSR.cpp:327-384: L' = L D, U' = L'^T, dinv = D^2 where D holds
+// the stored 1/sqrt(pivot).  Output arrays hold n*min(maxfil, n-1) entries.
+// Returns the first row without a diagonal, or -1.
+namespace {
+// sift of the candidate heap (smallest magnitude on top): an entry moves
+// below a child only when the child is strictly smaller (ict_l.cpp:3-22)
+void ict_sift(std::vector<std::pair<double, int>> &c, int i, int m)
+{
+    const std::pair<double, int> held = c[i];
+    int k = 2 * i + 1;
+    while (k < m) {
+        if (k + 1 < m && std::fabs(c[k].first) > std::fabs(c[k + 1].first)) k++;
+        if (std::fabs(c[k].first) < std::fabs(held.first)) {
+            c[i] = c[k];
+            i = k;
+            k = 2 * k + 1;
+        } else {
+            break;
+        }
+    }
+    c[i] = held;
+}
+}  // namespace
+
+int orc_ict(int n, const int *rp, const int *ci, const double *v, int maxfil, double droptol, int *lrp, int *lci,
+            double *lv, double *dinv, int *urp, int *uci, double *uv)
+{
+    if (n == 0) return -1;
+    maxfil = std::max(0, std::min(maxfil, n - 1));
+    const double small = 1e-4;
+    std::vector<double> tn(n, 0.0);
+    for (int i = 0; i < n; i++) {
+        bool has = false;
+        for (int q = rp[i]; q < rp[i + 1]; q++) {
+            tn[i] += v[q] * v[q];
+            has = has || ci[q] == i;
+        }
+        if (!has) return i;
+        tn[i] = std::sqrt(tn[i]) * droptol;
+    }
+    // factor rows: off-diagonal (column, value) pairs and the stored
+    // 1/sqrt(pivot)
+    std::vector<std::vector<std::pair<int, double>>> row(n);
+    std::vector<double> rs(n);
+    {
+        double a = v[0];
+        if (std::fabs(a) < 1e-20) a = small * (1 / droptol) * tn[0] + tn[0];
+        rs[0] = 1 / std::sqrt(std::fabs(a));
+    }
+    // first column of each factor row (the diagonal for a row with no kept entry)
+    auto first_col = [&](int r) { return row[r].empty() ? r : row[r][0].first; };
+    std::vector<double> w(n, 0.0);
+    for (int i = 1; i < n; i++) {
+        const int c0 = ci[rp[i]];
+        for (int j = (c0 < i ? first_col(c0) : i); j <= i; j++) w[j] = 0;
+        for (int q = rp[i]; q < rp[i + 1]; q++) w[ci[q]] = v[q];
+        std::vector<std::pair<double, int>> cand;
+        for (int j = c0; j < i; j++) {
+            double dot = 0;
+            for (const auto &e : row[j]) dot += w[e.first] * e.second;
+            w[j] -= dot;
+            w[j] *= rs[j];
+            if (std::fabs(w[j]) > tn[i]) {
+                cand.push_back({w[j], j});
+                w[i] -= w[j] * w[j];
+            }
+        }
+        if (std::fabs(w[i]) < 1e-20) w[i] = small * (1 / droptol) * tn[i] + tn[i];
+        rs[i] = 1 / std::sqrt(std::fabs(w[i]));
+        const int cnt = (int)cand.size();
+        if (cnt > maxfil) {
+            for (int t = maxfil / 2; t >= 0; t--) ict_sift(cand, t, maxfil);
+            for (int t = maxfil; t < cnt; t++) {
+                if (std::fabs(cand[t].first) > std::fabs(cand[0].first)) {
+                    cand[0] = cand[t];
+                    ict_sift(cand, 0, maxfil);
+                }
+            }
+            cand.resize(maxfil);
+            std::sort(cand.begin(), cand.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+                return a.second < b.second;
+            });
+        }
+        for (const auto &e : cand) row[i].push_back({e.second, e.first});
+    }
+    int nl = 0;
+    lrp[0] = 0;
+    std::vector<int> ucnt(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        for (const auto &e : row[i]) {
+            lci[nl] = e.first;
+            lv[nl++] = e.second * rs[e.first];
+            ucnt[e.first + 1]++;
+        }
+        lrp[i + 1] = nl;
+    }
+    urp[0] = 0;
+    for (int i = 0; i < n; i++) urp[i + 1] = urp[i] + ucnt[i + 1];
+    std::vector<int> pos(urp, urp + n);
+    for (int i = 0; i < n; i++) {
+        for (const auto &e : row[i]) {
+            uci[pos[e.first]] = i;
+            uv[pos[e.first]++] = e.second * rs[e.first];
+        }
+    }
+    for (int i = 0; i < n; i++) dinv[i] = rs[i] * rs[i];
+    return -1;
 }
 
 }  // extern "C"

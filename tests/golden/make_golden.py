@@ -15,6 +15,13 @@ CPU code, compiled from its sources by oracle/Makefile into oracle/_ref:
   ic0.npz             hip ic0_csr_A (hip/Precond/ic0.cpp:72-81) with the
                       Precond_ic0 defaults, in A's layout, on small
                       symmetric stencil matrices.
+  threshold_factors.npz
+                      hip ilutp_final (hip/Precond/ilut_diag_in_csr.cpp:20-251)
+                      split as seqilut, and ict_csr_A_l (hip/Precond/
+                      ict_l.cpp:196-201) converted as seqict, in the
+                      L / dinv / U' layout, for two parameter sets each on
+                      small matrices (one with a zero pivot, which takes the
+                      pivot substitute).
 
 Run here (where the reference sources exist):
     python tests/golden/make_golden.py [file.npz ...]   (default: all files)
@@ -67,6 +74,40 @@ def krylov(methods):
     return kr
 
 
+def _zero_pivot():
+    A = st.poisson2d_5pt(12)
+    v = A.val.copy()
+    v[A.rowptr[0]] = 0.0  # row 0's diagonal (its first entry)
+    return st.CSRMatrix(A.n, A.rowptr, A.colidx, v, "p2d_5pt_12_zero_pivot")
+
+
+THRESHOLD_MATRICES = {
+    "p2d_5pt_16": lambda: st.poisson2d_5pt(16),
+    "p3d_7pt_7": lambda: st.poisson3d_7pt(7),
+    "vc3d_7pt_6": lambda: st.varcoef3d_7pt(6, 4),
+    "p2d_zero_pivot": _zero_pivot,
+}
+ILUT_PARAMS = [(5, 1e-4), (2, 1e-2)]
+ICT_PARAMS = [(5, 1e-4), (20, 1e-6)]
+FACTOR_KEYS = ("lrp", "lci", "lv", "dinv", "urp", "uci", "uv")
+
+
+def threshold_factors():
+    out = {}
+    for name, gen in THRESHOLD_MATRICES.items():
+        A = gen()
+        out[f"{name}/rowptr"] = A.rowptr
+        out[f"{name}/colidx"] = A.colidx
+        out[f"{name}/val"] = A.val
+        for tag, params, fn in (("ilut", ILUT_PARAMS, oracle.ref_ilut_saad), ("ict", ICT_PARAMS, oracle.ref_ict)):
+            for p, (fill, tol) in enumerate(params):
+                F = fn(A, fill, tol)
+                out[f"{name}/{tag}{p}/params"] = np.array([fill, tol])
+                for k in FACTOR_KEYS:
+                    out[f"{name}/{tag}{p}/{k}"] = getattr(F, k)
+    return out
+
+
 def factor_values(matrices, values):
     out = {}
     for name, gen in matrices.items():
@@ -83,6 +124,7 @@ FILES = {
     "ilu0.npz": lambda: factor_values({k: v[0] for k, v in PROBLEMS.items()}, oracle.ref_ilu0_values),
     "krylov_single_reduction.npz": lambda: krylov(SINGLE_REDUCTION),
     "ic0.npz": lambda: factor_values(IC0_MATRICES, oracle.ref_ic0_values),
+    "threshold_factors.npz": threshold_factors,
 }
 
 

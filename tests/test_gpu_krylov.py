@@ -439,3 +439,46 @@ def test_vector_fusion_gives_identical_results(cuda):
         L.xs_set_vector_fusion(1)
     for a, c in zip(out[0], out[1]):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("pc,method,make", [
+    ("ilup", "bicgstab", lambda: st.convdiff3d_27pt(16)),
+    ("ict", "cgm", lambda: st.varcoef3d_7pt(16, 5)),
+])
+def test_host_threshold_factors_vs_oracle(cuda, pc, method, make):
+    """Saad ILUT (the reference's CPU "ilut") with BiCGSTAB and ICT with PCG:
+    factored on the host, applied by the GPU triangular solves.  The factors
+    equal the oracle's bit for bit, one FP64 LU solve equals the oracle's
+    LUsolve bit for bit, and the solve's history is the oracle's with the
+    same factors within the calibrated bound."""
+    import torch
+    from xsolver_b200.api import Plan
+
+    A = make()
+    b = st.rhs_uniform(A.n, 4)
+    fill, tol = (5, 1e-4) if pc == "ilup" else (6, 1e-4)
+    F = oracle.ilut_saad(A, fill, tol) if pc == "ilup" else oracle.ict(A, fill, tol)
+    P = Plan(A).factor(pc, fill=fill, droptol=tol)
+    G = P.factors()
+    for k in ("lrp", "lci", "lv", "dinv", "urp", "uci", "uv"):
+        assert np.array_equal(G[k], getattr(F, k)), k
+    dx = torch.from_numpy(b).to(cuda)
+    z = torch.zeros(A.n, dtype=torch.float64, device=cuda)
+    P.lusolve(dx, z)
+    P.sync()
+    assert np.array_equal(z.cpu().numpy(), oracle.lusolve(F, b))
+    S = _solver(A, "bicgstab" if method == "bicgstab" else "cgm", pc, 1e-10, 1000)
+    if pc == "ilup":
+        S.pc_setilut(tol, fill)
+    else:
+        S.pc_setict(tol, fill)
+    x = S.solve(b)
+    r = np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)
+    assert r < 1e-9
+    hist = S.resvec()
+    kw = dict(tol=1e-10, maxiter=1000, pc="lu", factors=F)
+    xo, ho, uo, hb, xb = reference_with_bounds(method, A, b, **kw)
+    assert count_ok(S.usediter - 1, uo, iteration_range(method, A, b, **kw)), (S.usediter, uo)
+    ok, worst = history_ok(hist[1:] / hist[0], ho, hb)
+    assert ok, worst
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xb

@@ -58,6 +58,9 @@ def _declare(L):
         "xs_ksp_set_absolute_tol": [C.c_void_p, C.c_double],
         "xs_pc_settype": [C.c_void_p, C.c_char_p],
         "xs_pc_setilut": [C.c_void_p, C.c_double, C.c_int],
+        "xs_pc_setict": [C.c_void_p, C.c_double, C.c_int],
+        "xs_host_ilut": [C.c_int, _ip, _ip, _dp, C.c_int, C.c_double, _ip, _ip, _ip, _ip, _dp, _dp, _ip, _ip, _dp],
+        "xs_host_ict": [C.c_int, _ip, _ip, _dp, C.c_int, C.c_double, _ip, _ip, _ip, _ip, _dp, _dp, _ip, _ip, _dp],
         "xs_pc_setparilu": [C.c_void_p, C.c_int],
         "xs_pc_setparilut": [C.c_void_p, C.c_double, C.c_int, C.c_double],
         "xs_pc_set_trsv": [C.c_void_p, C.c_int],

@@ -113,6 +113,10 @@ class Solver:
         check(self._L.xs_pc_setilut(self.h, tol, max_fill), "pc_setilut")
         return self
 
+    def pc_setict(self, tol: float, max_fill: int):
+        check(self._L.xs_pc_setict(self.h, tol, max_fill), "pc_setict")
+        return self
+
     def pc_setparilu(self, sweeps: int):
         check(self._L.xs_pc_setparilu(self.h, sweeps), "pc_setparilu")
         return self
@@ -229,7 +233,7 @@ class Solver:
 class Plan:
     """Kernel-level access on device tensors (torch CUDA tensors)."""
 
-    FACTOR_KIND = {"ilu0": 0, "parilu": 1, "parilut": 2, "ic0": 3}
+    FACTOR_KIND = {"ilu0": 0, "parilu": 1, "parilut": 2, "ic0": 3, "ilup": 4, "ict": 5}
     PREC = {"fp64": 0, "fp32": 1, "bf16": 2, "fp16": 3}
     OPS = {"csr64": 0, "ell64": 1, "csr32": 2, "lsolve": 3, "usolve": 4, "lusolve": 5, "ell32": 6}
 
@@ -431,3 +435,31 @@ def xsolver_free():
 __all__ = ["Solver", "Plan", "XsError", "xsolver_mat_setup", "xsolver_ksp_settype", "xsolver_ksp_setoption",
            "xsolver_pc_settype", "xsolver_pc_setilut", "xsolver_solve", "xsolver_free", "xsolver_usediter",
            "xsolver_resvec"]
+
+
+def _host_factor(fn, name, A, fill, droptol, cap):
+    n = A.n
+    rp = np.ascontiguousarray(A.rowptr, np.int32); ci = np.ascontiguousarray(A.colidx, np.int32)
+    v = np.ascontiguousarray(A.val, np.float64)
+    cap = max(cap, 1)
+    lrp = np.zeros(n + 1, np.int32); urp = np.zeros(n + 1, np.int32)
+    lci = np.zeros(cap, np.int32); uci = np.zeros(cap, np.int32)
+    lv = np.zeros(cap); uv = np.zeros(cap); dinv = np.zeros(max(n, 1))
+    nl, nu = C.c_int(), C.c_int()
+    check(fn(n, _i(rp), _i(ci), _d(v), fill, droptol, C.byref(nl), C.byref(nu), _i(lrp), _i(lci), _d(lv), _d(dinv),
+             _i(urp), _i(uci), _d(uv)), name)
+    return dict(lrp=lrp, lci=lci[:nl.value].copy(), lv=lv[:nl.value].copy(), dinv=dinv[:n].copy(), urp=urp,
+                uci=uci[:nu.value].copy(), uv=uv[:nu.value].copy())
+
+
+def host_ilut(A, lfil: int, droptol: float):
+    """Saad ILUT(droptol, lfil) of A computed by the library on the host (no
+    device needed), in the L / dinv / U' layout of Plan.factors()."""
+    return _host_factor(lib().xs_host_ilut, "host_ilut", A, int(lfil), float(droptol), A.n * int(lfil))
+
+
+def host_ict(A, maxfil: int, droptol: float):
+    """ICT(droptol, maxfil) of the symmetric A computed by the library on the
+    host, in the L / dinv / U' layout of Plan.factors()."""
+    m = min(int(maxfil), max(A.n - 1, 0))
+    return _host_factor(lib().xs_host_ict, "host_ict", A, int(maxfil), float(droptol), A.n * m)

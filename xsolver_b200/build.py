@@ -44,7 +44,10 @@ def needs_build() -> bool:
 
 # Per-unit flags: the persistent iteration reads, in one launch, vectors its
 # earlier phases wrote, so its plain global loads bypass L1 (-dlcm=cg).
-UNIT_FLAGS = {"xs_persist.cu": ["-Xptxas", "-dlcm=cg"]}
+UNIT_FLAGS = {"xs_persist.cu": ["-Xptxas", "-dlcm=cg"],
+              # host factorizations reproduce the reference's sequential CPU
+              # arithmetic: no contraction into fused multiply-adds
+              "xs_hostilu.cu": ["-Xcompiler", "-ffp-contract=off"]}
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:

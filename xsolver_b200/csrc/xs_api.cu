@@ -26,6 +26,7 @@
 #include "xs_adjoint.cuh"
 #include "xs_batch.cuh"
 #include "xs_mtx.cuh"
+#include "xs_hostilu.h"
 
 namespace xs {
 
@@ -393,8 +394,14 @@ struct Handle {
     double parilut_fill = 3.0;
     int parilut_sweeps = 10;
     double parilut_droptol = 0.0;
+    // host threshold factorizations: Saad ILUT (hip/Precond/precon_ilup.h:
+    // 17-24 defaults) and ICT (hip/Precond/precon_ict.h:14-16)
+    int ilup_fill = 20;
+    double ilup_tol = 1e-5;
+    int ict_fill = 100;
+    double ict_tol = 1e-8;
     int trsv_mode = 0;
-    ParilutResult ilut;  // ParILUT factors (own pattern)
+    ParilutResult ilut;  // factors on their own pattern (ParILUT, ILUT, ICT)
     // solver
     int method = 0;
     double tol = 1e-8, abstol = 0.0;
@@ -826,6 +833,47 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
     if (e) throw Status(dev_err_to_status(e));
 }
 
+// host-computed factors (L strict, dinv, U' strict) into the device layout
+// the threshold factorizations share
+static void upload_host_factors(cudaStream_t s, int n, HostTriFactors &F, ParilutResult &R)
+{
+    R = ParilutResult();
+    R.n = n;
+    R.nnzL = (long)F.lci.size();
+    R.nnzU = (long)F.uci.size();
+    R.lrp.alloc(n + 1); R.lrp.upload(F.lrp.data(), n + 1, s);
+    R.urp.alloc(n + 1); R.urp.upload(F.urp.data(), n + 1, s);
+    R.lci.alloc(std::max<long>(R.nnzL, 1)); R.lv.alloc(std::max<long>(R.nnzL, 1));
+    R.uci.alloc(std::max<long>(R.nnzU, 1)); R.uv.alloc(std::max<long>(R.nnzU, 1));
+    if (R.nnzL) { R.lci.upload(F.lci.data(), R.nnzL, s); R.lv.upload(F.lv.data(), R.nnzL, s); }
+    if (R.nnzU) { R.uci.upload(F.uci.data(), R.nnzU, s); R.uv.upload(F.uv.data(), R.nnzU, s); }
+    R.dinv.alloc(std::max(n, 1));
+    if (n) R.dinv.upload(F.dinv.data(), n, s);
+    std::vector<long> ident(n);
+    std::iota(ident.begin(), ident.end(), 0L);
+    R.diag_ident.alloc(std::max(n, 1));
+    if (n) R.diag_ident.upload(ident.data(), n, s);
+    XS_CUDA(cudaStreamSynchronize(s));  // the host arrays are released by the caller
+    R.hlrp = std::move(F.lrp); R.hlci = std::move(F.lci);
+    R.hurp = std::move(F.urp); R.huci = std::move(F.uci);
+}
+
+// factors out to caller arrays (any of them may be NULL)
+static void copy_host_factors(int n, const HostTriFactors &F, int *nnzL, int *nnzU, int *lrp, int *lci, double *lv,
+                              double *dinv, int *urp, int *uci, double *uv)
+{
+    const size_t nl = F.lci.size(), nu = F.uci.size();
+    if (nnzL) *nnzL = (int)nl;
+    if (nnzU) *nnzU = (int)nu;
+    if (lrp) std::memcpy(lrp, F.lrp.data(), sizeof(int) * (n + 1));
+    if (urp) std::memcpy(urp, F.urp.data(), sizeof(int) * (n + 1));
+    if (lci && nl) std::memcpy(lci, F.lci.data(), sizeof(int) * nl);
+    if (lv && nl) std::memcpy(lv, F.lv.data(), sizeof(double) * nl);
+    if (uci && nu) std::memcpy(uci, F.uci.data(), sizeof(int) * nu);
+    if (uv && nu) std::memcpy(uv, F.uv.data(), sizeof(double) * nu);
+    if (dinv && n) std::memcpy(dinv, F.dinv.data(), sizeof(double) * n);
+}
+
 static void build_precond(Handle &h)
 {
     if (h.pc_ready) return;
@@ -881,9 +929,21 @@ static void build_precond(Handle &h)
         if (need32) M.ensure_buffers32(h.s);
         if (h.trsv_mode > 0) M.ensure_sweep_buffers(need32);
         M.have_factors = true;
-    } else if (type == PC_PARILUT) {
-        Trace tr("setup parilut (total)", h.s);
-        parilut_build(h.s, h.err.p, n, h.A, h.parilut_fill, h.parilut_sweeps, h.parilut_droptol, h.ilut);
+    } else if (pc_own_pattern(type)) {
+        Trace tr("setup threshold factor (total)", h.s);
+        if (type == PC_PARILUT) {
+            parilut_build(h.s, h.err.p, n, h.A, h.parilut_fill, h.parilut_sweeps, h.parilut_droptol, h.ilut);
+        } else {
+            // sequential row chains: factored by the host, applied on the device
+            HostTriFactors F;
+            const double *hv = host_vals(h);
+            if (type == PC_ILUP) {
+                host_ilut(n, h.hrp.data(), h.hci.data(), hv, h.ilup_fill, h.ilup_tol, F);
+            } else if (host_ict(n, h.hrp.data(), h.hci.data(), hv, h.ict_fill, h.ict_tol, F) >= 0) {
+                throw Status(XS_ERR_NO_DIAG);
+            }
+            upload_host_factors(h.s, n, F, h.ilut);
+        }
         // factors in the seqilu0 layout on their own pattern
         ilut_to_tri(h.s, n, h.ilut, M.L, M.U, need32);
         pool_trim(h.s);
@@ -1259,7 +1319,7 @@ static void adjoint_prepare(Handle &h)
     if (M.type == PC_JACOBI) {
         T.jdiag64.alloc(n);
         XS_CUDA(cudaMemcpyAsync(T.jdiag64.p, M.jdiag64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, h.s));
-    } else if (M.type == PC_ILU0 || M.type == PC_PARILU || M.type == PC_PARILUT || M.type == PC_IC0) {
+    } else if (pc_triangular(M.type)) {
         // host patterns of L (strict lower) and U' (strict upper) with their
         // value sources, then the transposed triangles
         std::vector<int> lrp, lci, urp, uci;
@@ -1267,7 +1327,7 @@ static void adjoint_prepare(Handle &h)
         const double *vals;
         const long *diagsrc;
         DBuf<long> ident_diag;
-        if (M.type == PC_PARILUT) {
+        if (pc_own_pattern(M.type)) {
             ParilutResult &R = h.ilut;
             lrp = R.hlrp; lci = R.hlci; urp = R.hurp; uci = R.huci;
             lsrc.resize(lci.size()); usrc.resize(uci.size());
@@ -1579,7 +1639,8 @@ static int parse_pc(const char *fmt)
     if (ieq(fmt, "ilut") || ieq(fmt, "ilut_mkl") || ieq(fmt, "parilut")) return PC_PARILUT;
     if (ieq(fmt, "none")) return PC_NONE;
     if (ieq(fmt, "ic0")) return PC_IC0;
-    if (ieq(fmt, "ict")) return -2;
+    if (ieq(fmt, "ict")) return PC_ICT;
+    if (ieq(fmt, "ilup") || ieq(fmt, "ilut_saad")) return PC_ILUP;
     return -1;
 }
 
@@ -1871,7 +1932,39 @@ int xs_pc_setilut(xs_handle_t h, double tol, int max_fill)
         if (max_fill < 1 || tol < 0) throw Status(XS_ERR_INVALID);
         h->h->parilut_fill = (double)max_fill;
         h->h->parilut_droptol = tol;
+        h->h->ilup_fill = max_fill;
+        h->h->ilup_tol = tol;
         invalidate_pc(*h->h);
+    });
+}
+int xs_pc_setict(xs_handle_t h, double tol, int max_fill)
+{
+    return guarded([&] {
+        HCHK(h);
+        if (max_fill < 0 || !(tol > 0)) throw Status(XS_ERR_INVALID);
+        h->h->ict_fill = max_fill;
+        h->h->ict_tol = tol;
+        invalidate_pc(*h->h);
+    });
+}
+int xs_host_ilut(int n, const int *rp, const int *ci, const double *v, int lfil, double droptol, int *nnzL, int *nnzU,
+                 int *lrp, int *lci, double *lv, double *dinv, int *urp, int *uci, double *uv)
+{
+    return guarded([&] {
+        if (n < 0 || lfil < 1 || droptol < 0 || (n > 0 && (!rp || !ci || !v))) throw Status(XS_ERR_INVALID);
+        HostTriFactors F;
+        host_ilut(n, rp, ci, v, lfil, droptol, F);
+        copy_host_factors(n, F, nnzL, nnzU, lrp, lci, lv, dinv, urp, uci, uv);
+    });
+}
+int xs_host_ict(int n, const int *rp, const int *ci, const double *v, int maxfil, double droptol, int *nnzL, int *nnzU,
+                int *lrp, int *lci, double *lv, double *dinv, int *urp, int *uci, double *uv)
+{
+    return guarded([&] {
+        if (n < 0 || maxfil < 0 || !(droptol > 0) || (n > 0 && (!rp || !ci || !v))) throw Status(XS_ERR_INVALID);
+        HostTriFactors F;
+        if (host_ict(n, rp, ci, v, maxfil, droptol, F) >= 0) throw Status(XS_ERR_NO_DIAG);
+        copy_host_factors(n, F, nnzL, nnzU, lrp, lci, lv, dinv, urp, uci, uv);
     });
 }
 int xs_pc_setparilu(xs_handle_t h, int sweeps)
@@ -2116,17 +2209,29 @@ void xsolver_pc_setilut(double tol, int max_fill)
     std::lock_guard<std::mutex> lk(g_mu);
     guarded([&] {
         Handle &H = gh();
-        if (H.pc_req != PC_PARILUT) return;  // ignored otherwise, as in the reference
+        if (H.pc_req != PC_PARILUT && H.pc_req != PC_ILUP) return;  // ignored otherwise, as in the reference
         if (max_fill < 1 || tol < 0) throw Status(XS_ERR_INVALID);
-        H.parilut_fill = (double)max_fill;
-        H.parilut_droptol = tol;
+        if (H.pc_req == PC_PARILUT) {
+            H.parilut_fill = (double)max_fill;
+            H.parilut_droptol = tol;
+        } else {
+            H.ilup_fill = max_fill;
+            H.ilup_tol = tol;
+        }
         invalidate_pc(H);
     });
 }
-void xsolver_pc_setict(double, int)
+void xsolver_pc_setict(double tol, int max_fill)
 {
     std::lock_guard<std::mutex> lk(g_mu);
-    guarded([&] { throw Status(XS_ERR_UNSUPPORTED); });
+    guarded([&] {
+        Handle &H = gh();
+        if (H.pc_req != PC_ICT) return;  // ignored otherwise, as in the reference
+        if (max_fill < 0 || !(tol > 0)) throw Status(XS_ERR_INVALID);
+        H.ict_fill = max_fill;
+        H.ict_tol = tol;
+        invalidate_pc(H);
+    });
 }
 void xsolver_solve(double *rhs, double *sol)
 {
@@ -2315,7 +2420,6 @@ void gpu_preconditioner_setup(char *fmt)
     guarded([&] {
         if (!g_gpu) throw Status(XS_ERR_ORDER);
         int t = parse_pc(fmt);
-        if (ieq(fmt, "parilut")) t = PC_PARILUT;
         if (t < 0) throw Status(t == -2 ? XS_ERR_UNSUPPORTED : XS_ERR_INVALID);
         g_gpu->h->pc_req = t;
         invalidate_pc(*g_gpu->h);

@@ -470,7 +470,7 @@ static __global__ void k_bcopy(long m, const double *__restrict__ x, double *__r
 inline bool batch_precond_ok(const PrecondDev &M)
 {
     if (M.type == PC_NONE || M.type == PC_JACOBI) return true;
-    if (M.type == PC_ILU0 || M.type == PC_PARILU || M.type == PC_PARILUT || M.type == PC_IC0)
+    if (pc_triangular(M.type))
         return M.trsv_mode == 0 && !M.L.chunked && !M.U.chunked && M.L.pv64.p && M.U.pv64.p && M.U.dinv64.p;
     return false;
 }

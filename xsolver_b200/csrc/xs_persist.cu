@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(256, 4) k_persist_bicgstab(PersistBicgArgs<VT,
 template <typename VT>
 inline bool persist_ok(const Operator &A, const PrecondDev &M)
 {
-    if (M.type != PC_ILU0 && M.type != PC_PARILU && M.type != PC_PARILUT && M.type != PC_IC0) return false;
+    if (!pc_triangular(M.type)) return false;
     if (M.trsv_mode < 2) return false;
     if (A.format != 1 || !A.ell_dia || A.ell_w > 8 || !A.emask8.p) return false;
     for (const TriDev *T : {&M.L, &M.U})

@@ -130,7 +130,14 @@ int xs_plan_factor(xs_plan_t p, int kind, int sweeps, double fill, double dropto
         else if (kind == 1) { h.pc_req = PC_PARILU; h.parilu_sweeps = sweeps; }
         else if (kind == 2) { h.pc_req = PC_PARILUT; h.parilut_fill = fill; h.parilut_sweeps = sweeps; h.parilut_droptol = droptol; }
         else if (kind == 3) h.pc_req = PC_IC0;
-        else throw Status(XS_ERR_INVALID);
+        else if (kind == 4 || kind == 5) {
+            // host threshold factorizations: fill is the entry limit per row part
+            if (!(fill >= 0) || !(droptol >= 0) || (kind == 4 && fill < 1) || (kind == 5 && !(droptol > 0)))
+                throw Status(XS_ERR_INVALID);
+            h.pc_req = kind == 4 ? PC_ILUP : PC_ICT;
+            (kind == 4 ? h.ilup_fill : h.ict_fill) = (int)fill;
+            (kind == 4 ? h.ilup_tol : h.ict_tol) = droptol;
+        } else throw Status(XS_ERR_INVALID);
         h.inner32 = 1;  // keep reduced-precision copies of the factors for the solves
         invalidate_pc(h);
         build_precond(h);
@@ -143,7 +150,7 @@ int xs_plan_get_lu_values(xs_plan_t p, double *luv)
     return guarded([&] {
         if (!p || !luv) throw Status(XS_ERR_INVALID);
         Handle &h = *p->h;
-        if (!p->factored || p->factor_kind == 2) throw Status(XS_ERR_ORDER);
+        if (!p->factored || p->factor_kind == 2 || p->factor_kind >= 4) throw Status(XS_ERR_ORDER);
         h.luv.download(luv, h.nnz, h.s);
         XS_CUDA(cudaStreamSynchronize(h.s));
     });
@@ -156,7 +163,7 @@ int xs_plan_get_factors(xs_plan_t p, int *nnzL, int *nnzU, int *lrp, int *lci, d
         Handle &h = *p->h;
         if (!p->factored) throw Status(XS_ERR_ORDER);
         const int n = h.n;
-        if (p->factor_kind == 2) {
+        if (p->factor_kind == 2 || p->factor_kind >= 4) {  // own pattern
             ParilutResult &R = h.ilut;
             if (nnzL) *nnzL = (int)R.nnzL;
             if (nnzU) *nnzU = (int)R.nnzU;

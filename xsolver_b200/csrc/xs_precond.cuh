@@ -7,7 +7,14 @@
 
 namespace xs {
 
-enum PcType { PC_NONE = 0, PC_JACOBI = 1, PC_ILU0 = 2, PC_PARILU = 3, PC_PARILUT = 4, PC_IC0 = 5 };
+enum PcType { PC_NONE = 0, PC_JACOBI = 1, PC_ILU0 = 2, PC_PARILU = 3, PC_PARILUT = 4, PC_IC0 = 5, PC_ILUP = 6, PC_ICT = 7 };
+// preconditioners applied as z = U'^-1 (dinv * L^-1 x)
+inline bool pc_triangular(int t)
+{
+    return t == PC_ILU0 || t == PC_PARILU || t == PC_PARILUT || t == PC_IC0 || t == PC_ILUP || t == PC_ICT;
+}
+// ... whose factors have a pattern of their own (threshold factorizations)
+inline bool pc_own_pattern(int t) { return t == PC_PARILUT || t == PC_ILUP || t == PC_ICT; }
 enum FactorPrec { FP_F64 = 0, FP_F32 = 1, FP_BF16 = 2, FP_F16 = 3 };
 
 template <typename VT>
@@ -165,7 +172,7 @@ struct PrecondDev {
     bool fused_source_ok(int k) const { return k >= 2 && L.ell_w > 0; }
     bool can_fuse_first_pass() const
     {
-        return (type == PC_ILU0 || type == PC_PARILU || type == PC_PARILUT || type == PC_IC0) && trsv_mode >= 2 &&
+        return pc_triangular(type) && trsv_mode >= 2 &&
                fused_source_ok(trsv_mode);
     }
 
