@@ -985,16 +985,34 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     if (!T.chunked && tile_tuning().enable && n >= tile_tuning().min_rows) {
         Trace tr_tile("    box analysis", s);
         TileTuning tt = tile_tuning();
-        for (int attempt = 0; attempt < 6; attempt++) {
-            TP = TileHostPlan();
-            if (!tri_analyse_tiles(n, rp.data(), ci.data(), upper, src_of, tt, TP)) break;
-            if (TileSmem::of<double, double, double>(TP.max_rows, TP.max_halo, TP.max_entries).total <= TILE_SMEM_MAX) {
-                T.tiled = true;
-                break;
+        TileGrid G;
+        if (tile_detect(n, rp.data(), ci.data(), upper, G)) {
+            auto shrink = [&]() {
+                int &big = tt.tx >= tt.ty && tt.tx >= tt.tz ? tt.tx : (tt.ty >= tt.tz ? tt.ty : tt.tz);
+                if (big <= 2) return false;
+                big /= 2;
+                return true;
+            };
+            // first guess from the mean entries per row (a box's rows plus a
+            // quarter, its halo half its rows), then the layout's own sizes
+            const double per_row = (double)T.nnz / n;
+            for (;;) {
+                const int rows = tt.tx * tt.ty * tt.tz;
+                if (TileSmem::of<double, double, double>(rows, rows / 2, (int)(rows * per_row * 1.25)).total <=
+                        TILE_SMEM_MAX ||
+                    !shrink())
+                    break;
             }
-            int &big = tt.tx >= tt.ty && tt.tx >= tt.tz ? tt.tx : (tt.ty >= tt.tz ? tt.ty : tt.tz);
-            if (big <= 2) break;
-            big /= 2;
+            for (int attempt = 0; attempt < 6; attempt++) {
+                TP = TileHostPlan();
+                if (!tile_layout(n, rp.data(), ci.data(), upper, src_of, G, tt, TP)) break;
+                if (TileSmem::of<double, double, double>(TP.max_rows, TP.max_halo, TP.max_entries).total <=
+                    TILE_SMEM_MAX) {
+                    T.tiled = true;
+                    break;
+                }
+                if (!shrink()) break;
+            }
         }
     }
     if (T.tiled) {

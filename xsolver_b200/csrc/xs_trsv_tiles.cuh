@@ -171,14 +171,15 @@ inline int grid_reach(int n, const int *rp, const int *ci, LogF logical, const G
     return worst;
 }
 
-// Tile layout of a strict triangle; false when the pattern fits no grid
-// (the caller then keeps the level-ordered layout).  rp/ci: natural CSR of
-// the strict triangle, 0-based; upper: dependencies on larger rows, entries
-// summed in decreasing column order; src_of(k) maps entry k to the index of
-// its value.
-template <typename SrcF>
-inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, SrcF src_of, const TileTuning &tt,
-                              TileHostPlan &h)
+// The grid a strict triangle's pattern lives on and the shear that makes
+// every dependency vector non-positive (the first half of the analysis; it
+// does not depend on the box dimensions).
+struct TileGrid {
+    GridCoord g{0, 0};
+    int nx = 0, ny = 0, nz = 0, sa = 0, sb = 0, sc = 0;
+};
+
+inline bool tile_detect(int n, const int *rp, const int *ci, bool upper, TileGrid &G)
 {
     const long nnz = rp[n];
     if (n < 8 || nnz == 0) return false;
@@ -275,10 +276,27 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
         const int dx = vecs[q], dy = vecs[q + 1], dz = vecs[q + 2];
         if (dz < 0) sb = std::max(sb, ceil_div(dx + sa * dy, -dz));
     }
+    G.g = g;
+    G.nx = (int)g.nx;
+    G.ny = (int)(g.nxy / g.nx);
+    G.nz = (int)(n / g.nxy);
+    G.sa = sa; G.sb = sb; G.sc = sc;
+    return true;
+}
+
+// Box layout of a strict triangle on a detected grid (the second half).
+template <typename SrcF>
+inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF src_of, const TileGrid &G,
+                        const TileTuning &tt, TileHostPlan &h)
+{
+    const long nnz = rp[n];
+    auto logical = [&](int r) -> long { return upper ? (long)n - 1 - r : (long)r; };
+    const GridCoord g = G.g;
+    const int sa = G.sa, sb = G.sb, sc = G.sc;
     h.n = n;
-    h.nx = (int)g.nx;
-    h.ny = (int)(g.nxy / g.nx);
-    h.nz = (int)(n / g.nxy);
+    h.nx = G.nx;
+    h.ny = G.ny;
+    h.nz = G.nz;
     h.sa = sa; h.sb = sb; h.sc = sc;
     // tile coordinates of every logical index
     const int tx = std::max(1, tt.tx), ty = std::max(1, tt.ty), tz = std::max(1, tt.tz);
@@ -411,6 +429,19 @@ inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, S
             std::memcpy(h.halo_row.data() + h.halo_ptr[t], ext_of[t].data(), sizeof(int) * ext_of[t].size());
     });
     return true;
+}
+
+// Tile layout of a strict triangle (both halves, the given box dimensions); false when the pattern fits no grid
+// (the caller then keeps the level-ordered layout).  rp/ci: natural CSR of
+// the strict triangle, 0-based; upper: dependencies on larger rows, entries
+// summed in decreasing column order; src_of(k) maps entry k to the index of
+// its value.
+template <typename SrcF>
+inline bool tri_analyse_tiles(int n, const int *rp, const int *ci, bool upper, SrcF src_of, const TileTuning &tt,
+                              TileHostPlan &h)
+{
+    TileGrid G;
+    return tile_detect(n, rp, ci, upper, G) && tile_layout(n, rp, ci, upper, src_of, G, tt, h);
 }
 
 // ---------------------------------------------------------------- kernel
