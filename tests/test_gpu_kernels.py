@@ -144,6 +144,25 @@ def test_ilu0_bitwise_vs_oracle_large(cuda):
             assert np.array_equal(G[k], getattr(F, k)), (A.name, k)
 
 
+def test_ilu0_box_schedule_bitwise(cuda):
+    """The box-scheduled ILU(0) (systems whose L solve has boxes: at least
+    65536 rows on a grid) and the level-ordered lane groups give the oracle's
+    factors bit for bit: 7- and 27-point patterns, variable coefficients."""
+    from xsolver_b200 import _lib
+    from xsolver_b200.api import Plan
+
+    L = _lib.lib()
+    for A in (st.poisson3d_7pt(64), st.convdiff3d_27pt(48), st.varcoef3d_7pt(56, 2)):
+        ref = oracle.ilu0_values(A)
+        for on in (1, 0):
+            assert L.xs_set_ilu_tiles(on) == 0
+            try:
+                P = Plan(A).factor("ilu0")
+                assert np.array_equal(P.lu_values(), ref), (A.name, on)
+            finally:
+                L.xs_set_ilu_tiles(1)
+
+
 def _wide_rows_matrix():
     """2D 5-point Poisson 40x40 plus 5 rows coupled to 40-60 random columns
     (weakly, so the pivots stay away from zero): rows wider than 32 entries,

@@ -105,6 +105,7 @@ def _declare(L):
         "xs_set_ell_index_bits": [C.c_int],
         "xs_set_trsv_block_rows": [C.c_int],
         "xs_set_trsv_block_staging": [C.c_int],
+        "xs_set_ilu_tiles": [C.c_int],
         "xs_set_sweep_fusion": [C.c_int],
         "xs_set_launch_overlap": [C.c_int],
         "xs_set_vector_fusion": [C.c_int],

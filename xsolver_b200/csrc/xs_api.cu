@@ -99,6 +99,17 @@ bool &vec_fusion_flag()
     return on;
 }
 
+// box-scheduled exact ILU(0): on (1, default) or the level-ordered lane
+// groups (0); environment XS_ILU_TILES at first use
+static int &ilu_tiles_flag()
+{
+    static int f = [] {
+        const char *e = getenv("XS_ILU_TILES");
+        return e ? (atoi(e) != 0) : 1;
+    }();
+    return f;
+}
+
 TileTuning &tile_tuning()
 {
     static TileTuning t;
@@ -383,6 +394,14 @@ struct Handle {
     int ilu_epoch = 0;
     int max_row_len = -1;  // longest row of the pattern (-1: not yet counted)
     DBuf<unsigned> fticket;
+    // box-scheduled exact ILU(0) on the L solve's boxes: per position the
+    // offset of the row's values in its box's shared-memory area, per entry
+    // of A the offset of its column's row when that row is in the same box
+    // (-1 otherwise); built with the pattern analysis when L has boxes whose
+    // rows' values fit in shared memory
+    bool ilu_tiles = false;
+    size_t ilu_tiles_smem = 0;
+    DBuf<int> ilu_voff, ilu_dep;
     TriHostPlan hL, hU;
     DBuf<double> luv, fv, tmpv;
     DBuf<long> udiag_src;
@@ -583,6 +602,47 @@ static void update_values(Handle &h, const double *v)
 }
 
 // pattern analysis: diagonal positions, triangle plans, ParILU column maps
+// offsets of the box-scheduled ILU(0) (see Handle::ilu_voff) from L's boxes
+static void build_ilu_tiles(Handle &h)
+{
+    h.ilu_tiles = false;
+    h.ilu_voff.free();
+    h.ilu_dep.free();
+    const TriDev &L = h.M.L;
+    if (!L.tiled || L.ntiles <= 0) return;
+    const int n = h.n;
+    std::vector<int> perm(n), tpos(L.ntiles + 1);
+    L.perm.download(perm.data(), n, h.s);
+    L.t_pos.download(tpos.data(), L.ntiles + 1, h.s);
+    XS_CUDA(cudaStreamSynchronize(h.s));
+    const int *rp = h.hrp.data(), *ci = h.hci.data();
+    std::vector<int> voff(n), box_of(n), off_of(n);
+    long most = 0;
+    for (int t = 0; t < L.ntiles; t++) {
+        long o = 0;
+        for (int p = tpos[t]; p < tpos[t + 1]; p++) {
+            const int i = perm[p];
+            voff[p] = (int)o;
+            box_of[i] = t;
+            off_of[i] = (int)o;
+            o += rp[i + 1] - rp[i];
+        }
+        most = std::max(most, o);
+    }
+    if ((size_t)most * sizeof(double) > ILU_TILE_SMEM_MAX) return;
+    std::vector<int> dep(std::max<long>(h.nnz, 1), -1);
+    for (int i = 0; i < n; i++)
+        for (int k = rp[i]; k < h.huptr[i]; k++)
+            if (box_of[ci[k]] == box_of[i]) dep[k] = off_of[ci[k]];
+    h.ilu_voff.alloc(n);
+    h.ilu_voff.upload(voff.data(), n, h.s);
+    h.ilu_dep.alloc(dep.size());
+    h.ilu_dep.upload(dep.data(), dep.size(), h.s);
+    XS_CUDA(cudaStreamSynchronize(h.s));  // the host arrays go out of scope
+    h.ilu_tiles_smem = (size_t)most * sizeof(double);
+    h.ilu_tiles = true;
+}
+
 static void analyse_pattern(Handle &h)
 {
     if (h.analysed) return;
@@ -639,6 +699,7 @@ static void analyse_pattern(Handle &h)
     h.flags.alloc(n);
     h.ilu_epoch = 0;
     h.max_row_len = -1;
+    build_ilu_tiles(h);
     XS_CUDA(cudaStreamSynchronize(h.s));
     h.analysed = true;
 }
@@ -798,7 +859,22 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
         const int wmax = h.max_row_len;
         int G = 4;
         while (G < wmax && G < 64) G <<= 1;
-        if (ilu_group && G <= 32) {
+        if (h.ilu_tiles && ilu_tiles_flag()) {
+            // box schedule: CTAs per SM as the staged box area allows
+            const TriDev &L = h.M.L;
+            const size_t sm = std::max<size_t>(h.ilu_tiles_smem, 16);
+            static size_t attr = 0;
+            if (sm > attr) {
+                XS_CUDA(cudaFuncSetAttribute(k_ilu0_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                attr = sm;
+            }
+            const int per_sm = std::max(1, std::min(4, (int)((size_t)(220 * 1024) / (sm + 1024))));
+            const int gl = std::min(L.ntiles, geom().sms * per_sm);
+            k_ilu0_tiles<<<gl, ILU_TILE_THREADS, sm, h.s>>>(L.ntiles, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, L.t_pos.p,
+                                                            L.t_lvl.p, L.t_lptr.p, L.perm.p, L.t_hptr.p, L.t_hrow.p,
+                                                            h.ilu_voff.p, h.ilu_dep.p, h.flags.p, h.ilu_epoch,
+                                                            h.err.p, h.fticket.p);
+        } else if (ilu_group && G <= 32) {
             const int rpb = 128 / G;
             const int bps = ilu_bps_env ? ilu_bps_env : (G <= 8 ? 4 : 8);
             const int gl = std::min((n + rpb - 1) / rpb, geom().sms * bps);
@@ -1707,6 +1783,11 @@ int xs_set_trsv_block_rows(int max_rows)
         if (max_rows < 0) throw Status(XS_ERR_INVALID);
         trsv_tuning().block_max_rows = max_rows;
     });
+}
+
+int xs_set_ilu_tiles(int enable)
+{
+    return guarded([&] { ilu_tiles_flag() = enable != 0; });
 }
 
 int xs_set_trsv_block_staging(int enable)

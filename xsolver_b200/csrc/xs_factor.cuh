@@ -267,6 +267,117 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
     }
 }
 
+// ---------------------------------------------------------------- box-scheduled ILU(0)
+// Exact ILU(0) on the box schedule of the L solve (the dependency graph of
+// ILU(0) is L's): persistent CTAs take boxes in wavefront order by ticket.
+// A CTA copies the values of its box's rows into shared memory, waits once
+// for the published flags of the box's halo rows (dependencies in earlier
+// boxes, final in global memory), then updates the rows level by level in
+// shared memory with a barrier between levels, writes the rows back and
+// publishes their flags.  Each row update is the reference's IKJ step in its
+// order (pivot division, then the merge with row k's upper part), reading
+// row k from shared memory when k is in the box (dep[j] >= 0: the offset of
+// row k's values) and from global memory otherwise, so the factors are
+// bitwise those of the thread-per-row kernel.  Waits are bounded.
+constexpr int ILU_TILE_THREADS = 256;
+constexpr size_t ILU_TILE_SMEM_MAX = 200 * 1024;
+
+static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(
+    int ntiles, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ uptr, double *luv,
+    const int *__restrict__ tile_pos, const int *__restrict__ tile_lvl, const int *__restrict__ lvl_ptr,
+    const int *__restrict__ perm, const int *__restrict__ halo_ptr, const int *__restrict__ halo_row,
+    const int *__restrict__ voff, const int *__restrict__ dep, int *flag, int epoch, int *err, unsigned *ticket)
+{
+    extern __shared__ __align__(16) double ilu_sv[];
+    __shared__ int s_t, s_err;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            // every CTA ends with one failing claim; the last of them re-arms
+            if (t == (unsigned)(ntiles + gridDim.x - 1)) *ticket = 0u;
+            s_t = (int)t;
+            s_err = *(volatile int *)err;
+        }
+        __syncthreads();
+        const int t = s_t, e0 = s_err;
+        __syncthreads();
+        if (t >= ntiles) return;
+        if (e0) continue;
+        const int p0 = tile_pos[t], p1 = tile_pos[t + 1];
+        // the box's rows: A's values (nothing else writes them)
+        for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) {
+            const int i = perm[p];
+            double *dst = ilu_sv + voff[p];
+            for (int k = rp[i]; k < rp[i + 1]; k++) dst[k - rp[i]] = __ldcg(luv + k);
+        }
+        // the halo rows' flags (bounded waits)
+        bool ok = true;
+        for (int h = halo_ptr[t] + (int)threadIdx.x; h < halo_ptr[t + 1] && ok; h += blockDim.x) {
+            const int k = halo_row[h];
+            long spins = 0;
+            unsigned long long t0 = 0;
+            unsigned ns = 32;
+            while (ld_acquire(flag + k) != epoch) {
+                __nanosleep(ns);
+                if (ns < 512u) ns <<= 1;
+                if ((++spins & 63) == 0) {
+                    const unsigned long long tn = gtimer();
+                    if (t0 == 0) t0 = tn;
+                    else if (tn - t0 > WAIT_LIMIT_NS) {
+                        atomicOr(err, DEV_FACTOR_TIMEOUT);
+                        ok = false;
+                        break;
+                    }
+                    if (*(volatile int *)err) {
+                        ok = false;
+                        break;
+                    }
+                }
+            }
+        }
+        if (!__syncthreads_and(ok)) continue;
+        for (int l = tile_lvl[t]; l < tile_lvl[t + 1]; l++) {
+            for (int p = lvl_ptr[l] + (int)threadIdx.x; p < lvl_ptr[l + 1]; p += blockDim.x) {
+                const int i = perm[p];
+                const int rs = rp[i], re = rp[i + 1], up = uptr[i];
+                double *a = ilu_sv + voff[p];  // a[e - rs]: entry e of row i
+                for (int j = rs; j < up; j++) {
+                    const int k = ci[j];
+                    const int kb = rp[k], ukp = uptr[k], kend = rp[k + 1];
+                    const int dk = dep[j];  // row k in the box: its values at ilu_sv[dk + (e - kb)]
+                    double piv = dk >= 0 ? ilu_sv[dk + (ukp - kb)] : __ldcg(luv + ukp);
+                    if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
+                    const double lij = a[j - rs] / piv;
+                    a[j - rs] = lij;
+                    int subptr = ukp;
+                    for (int jj = j + 1; jj < re; jj++) {
+                        const int kk = ci[jj];
+                        while (subptr < kend && __ldg(ci + subptr) < kk) subptr++;
+                        if (subptr < kend) {
+                            if (__ldg(ci + subptr) == kk) {
+                                const double u = dk >= 0 ? ilu_sv[dk + (subptr - kb)] : __ldcg(luv + subptr);
+                                const double tt = lij * u;
+                                a[jj - rs] = a[jj - rs] - tt;
+                            }
+                        } else
+                            break;
+                    }
+                }
+                if (fabs(a[up - rs]) < 1e-20) a[up - rs] = 1e-20;
+            }
+            __syncthreads();
+        }
+        for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) {
+            const int i = perm[p];
+            const double *src = ilu_sv + voff[p];
+            for (int k = rp[i]; k < rp[i + 1]; k++) luv[k] = src[k - rp[i]];
+        }
+        __threadfence();
+        __syncthreads();
+        for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) st_release(flag + perm[p], epoch);
+    }
+}
+
 // ---------------------------------------------------------------- IC(0)
 // hip/Precond/ic0.cpp:4-70 (initLByA + ic0_fact, Precond_ic0 defaults
 // smallnum = droptol = 1e-4) on A's lower part, in place in A's layout: at

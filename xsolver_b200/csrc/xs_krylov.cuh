@@ -31,7 +31,50 @@ namespace xs {
 
 constexpr double KSMALL = 1e-20;
 
+// 16 bytes of consecutive elements at a 16-byte aligned address
+template <typename T, int W>
+__device__ __forceinline__ void ld16(const T *p, T (&o)[W])
+{
+    static_assert(W * sizeof(T) == 16, "16-byte vector");
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    memcpy(o, &u, 16);
+}
+template <typename T, int W>
+__device__ __forceinline__ void ldg16(const T *p, T (&o)[W])  // read-only for the whole launch
+{
+    static_assert(W * sizeof(T) == 16, "16-byte vector");
+    const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p));
+    memcpy(o, &u, 16);
+}
+template <typename T, int W>
+__device__ __forceinline__ void st16(T *p, const T (&v)[W])
+{
+    static_assert(W * sizeof(T) == 16, "16-byte vector");
+    uint4 u;
+    memcpy(&u, v, 16);
+    *reinterpret_cast<uint4 *>(p) = u;
+}
+inline bool aligned16(std::initializer_list<const void *> ps)
+{
+    for (const void *p : ps)
+        if (reinterpret_cast<uintptr_t>(p) % 16) return false;
+    return true;
+}
+
 // ---------------------------------------------------------------- generic vector-op kernel
+// An op may also provide elem_v(i, acc) for Op::V consecutive elements from
+// a V-aligned i with one 16-byte access per vector (used when its vec_ok
+// says every vector is 16-byte aligned): a thread then keeps V elements of
+// each vector in flight instead of one.
+template <class Op, class = void>
+struct OpVecWidth {
+    static constexpr int V = 1;
+};
+template <class Op>
+struct OpVecWidth<Op, std::void_t<decltype(Op::V)>> {
+    static constexpr int V = Op::V;
+};
+
 template <class Op>
 __global__ void __launch_bounds__(256, 8) k_vecop(Op op, RedSlot slot)
 {
@@ -45,7 +88,17 @@ __global__ void __launch_bounds__(256, 8) k_vecop(Op op, RedSlot slot)
     double acc[KK];
 #pragma unroll
     for (int k = 0; k < KK; k++) acc[k] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) o.elem(i, acc);
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    int i0 = 0;
+    if constexpr (OpVecWidth<Op>::V > 1) {
+        constexpr int V = OpVecWidth<Op>::V;
+        if (o.vec_ok) {
+            const int nv = o.n / V;
+            for (int j = tid; j < nv; j += stride) o.elem_v(j * V, acc);
+            i0 = nv * V;
+        }
+    }
+    for (int i = i0 + tid; i < o.n; i += stride) o.elem(i, acc);
     if (Op::K > 0) {
         if (block_reduce_publish<KK>(acc, slot, tot)) {
             if (threadIdx.x == 0) o.finalize(tot);
@@ -801,11 +854,13 @@ struct SrcBicgS {
 template <typename VT>
 struct OpBicgX {
     static constexpr int K = 2;
+    static constexpr int V = 16 / (int)sizeof(VT);
     int n;
     KState *st;
     VT *x, *r;
     const VT *z1, *z2, *s, *v, *rhat;
     VT gama, alpha;
+    bool vec_ok = false;
     __device__ void load()
     {
         gama = (VT)st->sc[S_GAMA];
@@ -820,6 +875,28 @@ struct OpBicgX {
         r[i] = ri;
         a[0] += (double)ri * (double)ri;
         a[1] += (double)ri * (double)rhat[i];
+    }
+    // the same arithmetic per element, V elements per 16-byte access
+    __device__ void elem_v(int i, double (&a)[2]) const
+    {
+        VT xv[V], z1v[V], z2v[V], sv[V], vv[V], hv[V], rv[V];
+        ld16(x + i, xv);
+        ldg16(z1 + i, z1v);
+        ldg16(z2 + i, z2v);
+        ldg16(s + i, sv);
+        ldg16(v + i, vv);
+        ldg16(rhat + i, hv);
+        const VT minalpha = -alpha;
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            const VT xi = xv[q] + gama * z1v[q];
+            xv[q] = xi + alpha * z2v[q];
+            rv[q] = sv[q] + minalpha * vv[q];
+            a[0] += (double)rv[q] * (double)rv[q];
+            a[1] += (double)rv[q] * (double)hv[q];
+        }
+        st16(x + i, xv);
+        st16(r + i, rv);
     }
     __device__ void finalize(const double *t) const
     {

@@ -360,7 +360,9 @@ struct BicgRun {
                 c.M->apply<VT>(s, z2, done, c.s);
             }
             spmv<VT, MT>(*c.A, z2, v, EpiDot2<VT>{st, s, M_BICG_ALPHA}, sl, c.s);
-            vecop(OpBicgX<VT>{n, st, x, r, z1, z2, s, v, rhat, (VT)0, (VT)0}, sl, c.s);
+            OpBicgX<VT> ox{n, st, x, r, z1, z2, s, v, rhat, (VT)0, (VT)0};
+            ox.vec_ok = aligned16({x, r, z1, z2, s, v, rhat});
+            vecop(ox, sl, c.s);
         };
         // the whole iteration as one persistent kernel when it serves this
         // configuration (same vector updates fused into the sweep passes)
