@@ -643,6 +643,39 @@ static void build_ilu_tiles(Handle &h)
     h.ilu_tiles = true;
 }
 
+// row of every entry (ParILU, IC(0) split) and, with columns, the U part by
+// columns (rows ascending, diagonal last; ParILU) of the analysed pattern
+static void ensure_entry_maps(Handle &h, bool columns)
+{
+    const int n = h.n;
+    const int *rp = h.hrp.data(), *ci = h.hci.data();
+    std::vector<int> rowof;
+    if (!h.rowof.p || (columns && !h.ucp.p)) {
+        rowof.resize(h.nnz);
+        for (int i = 0; i < n; i++)
+            for (int k = rp[i]; k < rp[i + 1]; k++) rowof[k] = i;
+    }
+    if (!h.rowof.p) {
+        h.rowof.alloc(std::max<long>(h.nnz, 1));
+        h.rowof.upload(rowof.data(), h.nnz, h.s);
+    }
+    if (columns && !h.ucp.p) {
+        std::vector<int> ucp(n + 1, 0), ucpos;
+        for (long k = 0; k < h.nnz; k++)
+            if (rowof[k] <= ci[k]) ucp[ci[k] + 1]++;
+        for (int j = 0; j < n; j++) ucp[j + 1] += ucp[j];
+        ucpos.resize(ucp[n]);
+        std::vector<int> pos(ucp.begin(), ucp.end() - 1);
+        for (long k = 0; k < h.nnz; k++)
+            if (rowof[k] <= ci[k]) ucpos[pos[ci[k]]++] = (int)k;
+        h.ucp.alloc(n + 1);
+        h.ucp.upload(ucp.data(), n + 1, h.s);
+        h.ucpos.alloc(std::max<size_t>(ucpos.size(), 1));
+        h.ucpos.upload(ucpos.data(), ucpos.size(), h.s);
+    }
+    XS_CUDA(cudaStreamSynchronize(h.s));  // the host arrays go out of scope
+}
+
 static void analyse_pattern(Handle &h)
 {
     if (h.analysed) return;
@@ -650,12 +683,9 @@ static void analyse_pattern(Handle &h)
     const int n = h.n;
     const int *rp = h.hrp.data(), *ci = h.hci.data();
     h.huptr.assign(n, -1);
-    std::vector<int> rowof(h.nnz);
     for (int i = 0; i < n; i++)
-        for (int k = rp[i]; k < rp[i + 1]; k++) {
-            rowof[k] = i;
+        for (int k = rp[i]; k < rp[i + 1]; k++)
             if (ci[k] == i) h.huptr[i] = k;
-        }
     for (int i = 0; i < n; i++)
         if (h.huptr[i] < 0) throw Status(XS_ERR_NO_DIAG);
     // strict triangles as CSR with source indices into A's value array
@@ -675,23 +705,9 @@ static void analyse_pattern(Handle &h)
     build_tri_dev(h.M.U, n, urp, uci, true, [&](int k) { return usrc[k]; }, h.s);
     h.uptr.alloc(n);
     h.uptr.upload(h.huptr.data(), n, h.s);
-    h.rowof.alloc(std::max<long>(h.nnz, 1));
-    h.rowof.upload(rowof.data(), h.nnz, h.s);
-    // U part by columns (rows ascending, diagonal last) for ParILU
-    std::vector<int> ucp(n + 1, 0), ucpos;
-    for (long k = 0; k < h.nnz; k++)
-        if (rowof[k] <= ci[k]) ucp[ci[k] + 1]++;
-    for (int j = 0; j < n; j++) ucp[j + 1] += ucp[j];
-    ucpos.resize(ucp[n]);
-    {
-        std::vector<int> pos(ucp.begin(), ucp.end() - 1);
-        for (long k = 0; k < h.nnz; k++)
-            if (rowof[k] <= ci[k]) ucpos[pos[ci[k]]++] = (int)k;
-    }
-    h.ucp.alloc(n + 1);
-    h.ucp.upload(ucp.data(), n + 1, h.s);
-    h.ucpos.alloc(std::max<size_t>(ucpos.size(), 1));
-    h.ucpos.upload(ucpos.data(), ucpos.size(), h.s);
+    h.rowof.free();  // row of each entry and U by columns: built when a factorisation needs them
+    h.ucp.free();
+    h.ucpos.free();
     std::vector<long> ud(n);
     for (int i = 0; i < n; i++) ud[i] = h.huptr[i];
     h.udiag_src.alloc(n);
@@ -893,6 +909,7 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
         }
         check_launch();
     } else {
+        ensure_entry_maps(h, true);
         h.tmpv.alloc(std::max<long>(h.nnz, 1));
         const int g = geom().sms * 8;
         double *cur = h.luv.p, *nxt = h.tmpv.p;
@@ -984,6 +1001,7 @@ static void build_precond(Handle &h)
         if (h.fv.n != (size_t)std::max<long>(h.nnz, 1)) h.fv.alloc(std::max<long>(h.nnz, 1));
         if (type == PC_IC0) {
             factor_ic0(h);
+            ensure_entry_maps(h, false);
             k_ic0_split<<<geom().sms * 4, 256, 0, h.s>>>(h.nnz, h.rowof.p, h.A.ci.p, h.uptr.p, h.tpos.p, h.luv.p,
                                                          h.fv.p);
         } else {

@@ -986,7 +986,10 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         Trace tr_tile("    box analysis", s);
         TileTuning tt = tile_tuning();
         TileGrid G;
-        if (tile_detect(n, rp.data(), ci.data(), upper, G)) {
+        Trace tr_det("      grid detection", s);
+        const bool on_grid = tile_detect(n, rp.data(), ci.data(), upper, G);
+        tr_det.stop();
+        if (on_grid) {
             auto shrink = [&]() {
                 int &big = tt.tx >= tt.ty && tt.tx >= tt.tz ? tt.tx : (tt.ty >= tt.tz ? tt.ty : tt.tz);
                 if (big <= 2) return false;
@@ -1005,7 +1008,9 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
             }
             for (int attempt = 0; attempt < 6; attempt++) {
                 TP = TileHostPlan();
+                Trace tr_lay("      box layout", s);
                 if (!tile_layout(n, rp.data(), ci.data(), upper, src_of, G, tt, TP)) break;
+                tr_lay.stop();
                 if (TileSmem::of<double, double, double>(TP.max_rows, TP.max_halo, TP.max_entries).total <=
                     TILE_SMEM_MAX) {
                     T.tiled = true;
