@@ -1013,7 +1013,8 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
         T = TriDev();
         {
             Trace tr("  build_tri_dev", s);
-            build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s, /*identity_src=*/true, drp, dci);
+            build_tri_dev(T, n, nrp, nci, upper, [](int k) { return (long)k; }, s, /*identity_src=*/true, drp, dci,
+                          /*need_levels=*/false);
         }
         const long m = std::max<long>(T.nnz, 1);
         const int g = geom().sms * 4;

@@ -942,20 +942,24 @@ namespace xs {
 template <typename SrcF>
 // identity_src: entry k's value is vals[k] (src_of is not called)
 // d_rp/d_ci: the same pattern already on the device (copied instead of uploaded)
+// need_levels: keep the level order of a triangle that gets boxes (the
+// level-ordered ILU(0)/IC(0) kernels read it); without it a boxed
+// triangle skips the level analysis (nlevels = -1)
 inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const std::vector<int> &ci, bool upper, SrcF src_of,
                           cudaStream_t s, bool identity_src = false, const int *d_rp = nullptr,
-                          const int *d_ci = nullptr)
+                          const int *d_ci = nullptr, bool need_levels = true)
 {
     TriHostPlan P;  // level analysis (also gives the level count)
     const int chr = trsv_tuning().chunk_rows;
     T.chunked = chr > 0;
-    Trace tr_an("    level analysis", s);
-    tri_analyse(n, rp.data(), ci.data(), upper, src_of, P, /*entries=*/false);
-    tr_an.stop();
+    auto level_analysis = [&]() {
+        Trace tr_an("    level analysis", s);
+        tri_analyse(n, rp.data(), ci.data(), upper, src_of, P, /*entries=*/false);
+    };
     Trace tr_up("    upload + positions", s);
     T.n = n;
-    T.nnz = P.prp[n];
-    T.nlevels = P.nlevels;
+    T.nnz = rp[n];
+    T.nlevels = -1;
     T.upper = upper;
     const long m = std::max<long>(T.nnz, 1);
     const int g = geom().sms * 4;
@@ -1036,10 +1040,16 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         T.t_hptr.alloc(TP.halo_ptr.size()); T.t_hptr.upload(TP.halo_ptr.data(), TP.halo_ptr.size(), s);
         T.t_hrow.alloc(std::max<size_t>(TP.halo_row.size(), 1));
         if (!TP.halo_row.empty()) T.t_hrow.upload(TP.halo_row.data(), TP.halo_row.size(), s);
-        T.lvperm.alloc(n); T.lvperm.upload(P.perm.data(), n, s);
+        if (need_levels) {
+            level_analysis();
+            T.nlevels = P.nlevels;
+            T.lvperm.alloc(n); T.lvperm.upload(P.perm.data(), n, s);
+        }
         T.lstart.free();
         XS_CUDA(cudaStreamSynchronize(s));  // the host plans go out of scope
     } else if (!T.chunked) {
+        level_analysis();
+        T.nlevels = P.nlevels;
         T.perm.alloc(n); T.perm.upload(P.perm.data(), n, s);
         T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
         T.pci.alloc(m);
@@ -1081,6 +1091,8 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
             T.lub.upload(b.data(), b.size(), s);
         }
     } else {
+        level_analysis();
+        T.nlevels = P.nlevels;
         TriChunkPlan C;
         tri_analyse_chunked(n, rp.data(), ci.data(), upper, src_of, chr, C);
         T.nchunks = C.nchunks;
