@@ -91,7 +91,11 @@ def test_gpu_api_vs_reference_golden(cuda, method):
         # gives the global-index history and the order-sensitivity bound
         xo, ho, uo, hb, xb = reference_with_bounds(method, A, b, tol=1e-9, maxiter=400, restart=20, pc="jacobi")
         assert np.array_equal(xo, xr) and uo == ur
-        assert abs(used - ur) <= 1, (nm, used, ur)
+        # within +-1 of the recorded count, or of the range the reference
+        # itself spans over dot-product orders (BiCGSTAB on the 24x24
+        # Poisson problem ends anywhere in 58-62)
+        urange = iteration_range(method, A, b, tol=1e-9, maxiter=400, restart=20, pc="jacobi")
+        assert count_ok(used, ur, urange), (nm, used, ur, urange)
         ok, worst = history_ok(rv[: used + 1], ho, hb)
         assert ok, (nm, worst)
         assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < xb, nm
@@ -349,7 +353,15 @@ def test_reference_setter_api_conventions(cuda):
     assert rv[used] / rv[0] < 1e-10
     r = b - A.to_scipy() @ x
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-9
-    assert api.xsolver_pc_settype("ict") == 10  # unsupported on GPU, no exit
+    assert api.xsolver_pc_settype("icx") == 1  # XS_ERR_INVALID: unknown name, no exit
+    # ICT (the reference exits for it on its GPU path): factored on the host,
+    # applied on the GPU, tuned by xsolver_pc_setict
+    assert api.xsolver_pc_settype("ict") == 0
+    assert api.xsolver_pc_setict(1e-4, 6) == 0
+    x = np.zeros(A.n)
+    assert api.xsolver_solve(b, x) == 0
+    r = b - A.to_scipy() @ x
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-9
     assert api.xsolver_free() == 0
 
 

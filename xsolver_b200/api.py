@@ -406,6 +406,11 @@ def xsolver_pc_setilut(tol, max_fill):
     return _lib.last_error()
 
 
+def xsolver_pc_setict(tol, max_fill):
+    lib().xsolver_pc_setict(tol, max_fill)
+    return _lib.last_error()
+
+
 def xsolver_solve(rhs, sol):
     rhs = _f64(rhs)
     if "keep" in _g:  # the system set by xsolver_mat_setup fixes the length
@@ -433,7 +438,7 @@ def xsolver_free():
 
 
 __all__ = ["Solver", "Plan", "XsError", "xsolver_mat_setup", "xsolver_ksp_settype", "xsolver_ksp_setoption",
-           "xsolver_pc_settype", "xsolver_pc_setilut", "xsolver_solve", "xsolver_free", "xsolver_usediter",
+           "xsolver_pc_settype", "xsolver_pc_setilut", "xsolver_pc_setict", "xsolver_solve", "xsolver_free", "xsolver_usediter",
            "xsolver_resvec"]
 
 

@@ -394,14 +394,13 @@ struct Handle {
     int ilu_epoch = 0;
     int max_row_len = -1;  // longest row of the pattern (-1: not yet counted)
     DBuf<unsigned> fticket;
-    // box-scheduled exact ILU(0) on the L solve's boxes: per position the
-    // offset of the row's values in its box's shared-memory area, per entry
-    // of A the offset of its column's row when that row is in the same box
-    // (-1 otherwise); built with the pattern analysis when L has boxes whose
-    // rows' values fit in shared memory
+    // box-scheduled exact ILU(0) on the L solve's boxes (k_ilu0_tiles: the
+    // arrays of IluTileArgs); built with the pattern analysis when L has
+    // boxes whose entries fit in shared memory
     bool ilu_tiles = false;
     size_t ilu_tiles_smem = 0;
-    DBuf<int> ilu_voff, ilu_dep;
+    int ilu_max_entries = 0, ilu_max_rows = 0;
+    DBuf<int> ilu_ebase, ilu_ent, ilu_roff, ilu_rdiag, ilu_dep;
     TriHostPlan hL, hU;
     DBuf<double> luv, fv, tmpv;
     DBuf<long> udiag_src;
@@ -602,44 +601,59 @@ static void update_values(Handle &h, const double *v)
 }
 
 // pattern analysis: diagonal positions, triangle plans, ParILU column maps
-// offsets of the box-scheduled ILU(0) (see Handle::ilu_voff) from L's boxes
+// the box-scheduled ILU(0)'s arrays (see k_ilu0_tiles) from L's boxes
 static void build_ilu_tiles(Handle &h)
 {
     h.ilu_tiles = false;
-    h.ilu_voff.free();
-    h.ilu_dep.free();
+    for (DBuf<int> *b : {&h.ilu_ebase, &h.ilu_ent, &h.ilu_roff, &h.ilu_rdiag, &h.ilu_dep}) b->free();
     const TriDev &L = h.M.L;
     if (!L.tiled || L.ntiles <= 0) return;
-    const int n = h.n;
-    std::vector<int> perm(n), tpos(L.ntiles + 1);
+    const int n = h.n, nt = L.ntiles;
+    std::vector<int> perm(n), tpos(nt + 1);
     L.perm.download(perm.data(), n, h.s);
-    L.t_pos.download(tpos.data(), L.ntiles + 1, h.s);
+    L.t_pos.download(tpos.data(), nt + 1, h.s);
     XS_CUDA(cudaStreamSynchronize(h.s));
     const int *rp = h.hrp.data(), *ci = h.hci.data();
-    std::vector<int> voff(n), box_of(n), off_of(n);
-    long most = 0;
-    for (int t = 0; t < L.ntiles; t++) {
-        long o = 0;
+    std::vector<int> ebase(nt + 1, 0), roff(n), rdiag(n), box_of(n), local_of(n);
+    int max_e = 0, max_r = 0;
+    for (int t = 0; t < nt; t++) {
+        int o = 0;
         for (int p = tpos[t]; p < tpos[t + 1]; p++) {
             const int i = perm[p];
-            voff[p] = (int)o;
+            roff[p] = o;
+            rdiag[p] = h.huptr[i] - rp[i];
             box_of[i] = t;
-            off_of[i] = (int)o;
+            local_of[i] = p - tpos[t];
             o += rp[i + 1] - rp[i];
         }
-        most = std::max(most, o);
+        ebase[t + 1] = ebase[t] + o;
+        max_e = std::max(max_e, o);
+        max_r = std::max(max_r, tpos[t + 1] - tpos[t]);
     }
-    if ((size_t)most * sizeof(double) > ILU_TILE_SMEM_MAX) return;
-    std::vector<int> dep(std::max<long>(h.nnz, 1), -1);
-    for (int i = 0; i < n; i++)
-        for (int k = rp[i]; k < h.huptr[i]; k++)
-            if (box_of[ci[k]] == box_of[i]) dep[k] = off_of[ci[k]];
-    h.ilu_voff.alloc(n);
-    h.ilu_voff.upload(voff.data(), n, h.s);
-    h.ilu_dep.alloc(dep.size());
-    h.ilu_dep.upload(dep.data(), dep.size(), h.s);
+    if (IluTileSmem::of(max_e, max_r).total > ILU_TILE_SMEM_MAX) return;
+    std::vector<int> ent(std::max<long>(h.nnz, 1)), dep(std::max<long>(h.nnz, 1), -1);
+    for (int t = 0; t < nt; t++)
+        for (int p = tpos[t]; p < tpos[t + 1]; p++) {
+            const int i = perm[p];
+            const int e0 = ebase[t] + roff[p];
+            for (int k = rp[i]; k < rp[i + 1]; k++) {
+                ent[e0 + (k - rp[i])] = k;
+                if (k < h.huptr[i] && box_of[ci[k]] == t) dep[e0 + (k - rp[i])] = local_of[ci[k]];
+            }
+        }
+    auto up = [&](DBuf<int> &b, const std::vector<int> &v) {
+        b.alloc(v.size());
+        b.upload(v.data(), v.size(), h.s);
+    };
+    up(h.ilu_ebase, ebase);
+    up(h.ilu_ent, ent);
+    up(h.ilu_roff, roff);
+    up(h.ilu_rdiag, rdiag);
+    up(h.ilu_dep, dep);
     XS_CUDA(cudaStreamSynchronize(h.s));  // the host arrays go out of scope
-    h.ilu_tiles_smem = (size_t)most * sizeof(double);
+    h.ilu_max_entries = max_e;
+    h.ilu_max_rows = max_r;
+    h.ilu_tiles_smem = IluTileSmem::of(max_e, max_r).total;
     h.ilu_tiles = true;
 }
 
@@ -886,10 +900,10 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
             }
             const int per_sm = std::max(1, std::min(4, (int)((size_t)(220 * 1024) / (sm + 1024))));
             const int gl = std::min(L.ntiles, geom().sms * per_sm);
-            k_ilu0_tiles<<<gl, ILU_TILE_THREADS, sm, h.s>>>(L.ntiles, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, L.t_pos.p,
-                                                            L.t_lvl.p, L.t_lptr.p, L.perm.p, L.t_hptr.p, L.t_hrow.p,
-                                                            h.ilu_voff.p, h.ilu_dep.p, h.flags.p, h.ilu_epoch,
-                                                            h.err.p, h.fticket.p);
+            const IluTileArgs args{L.ntiles, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, L.t_pos.p, L.t_lvl.p, L.t_lptr.p,
+                                   L.perm.p, L.t_hptr.p, L.t_hrow.p, h.ilu_ebase.p, h.ilu_ent.p, h.ilu_roff.p,
+                                   h.ilu_rdiag.p, h.ilu_dep.p, h.flags.p, h.ilu_epoch, h.err.p, h.fticket.p};
+            k_ilu0_tiles<<<gl, ILU_TILE_THREADS, sm, h.s>>>(args, h.ilu_max_entries, h.ilu_max_rows);
         } else if (ilu_group && G <= 32) {
             const int rpb = 128 / G;
             const int bps = ilu_bps_env ? ilu_bps_env : (G <= 8 ? 4 : 8);

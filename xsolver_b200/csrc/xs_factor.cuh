@@ -270,65 +270,106 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
 // ---------------------------------------------------------------- box-scheduled ILU(0)
 // Exact ILU(0) on the box schedule of the L solve (the dependency graph of
 // ILU(0) is L's): persistent CTAs take boxes in wavefront order by ticket.
-// A CTA copies the values of its box's rows into shared memory, waits once
-// for the published flags of the box's halo rows (dependencies in earlier
-// boxes, final in global memory), then updates the rows level by level in
-// shared memory with a barrier between levels, writes the rows back and
-// publishes their flags.  Each row update is the reference's IKJ step in its
-// order (pivot division, then the merge with row k's upper part), reading
-// row k from shared memory when k is in the box (dep[j] >= 0: the offset of
-// row k's values) and from global memory otherwise, so the factors are
-// bitwise those of the thread-per-row kernel.  Waits are bounded.
+// A CTA stages its box's entries — values and column indices, in the box's
+// entry order (rows by position, each row's entries in column order) — with
+// each row's entry offset and diagonal offset, waits once for the published
+// flags of the box's halo rows (dependencies in earlier boxes, final in
+// global memory), then updates the rows level by level with a barrier
+// between levels: a dependency row in the box is read from shared memory
+// (its local row from dep[], prefetched at the start of the row), a halo row
+// from global memory.  Each row update is the reference's IKJ step in its
+// order (pivot division, then the merge with row k's upper part), so the
+// factors are bitwise those of the thread-per-row kernel.  The rows are
+// written back and their flags released.  Waits are bounded.
+//   ent[e]   : A's entry index of box entry e (boxes consecutive; ebase[t])
+//   roff[p]  : entry offset of the row at position p within its box
+//   rdiag[p] : offset of that row's diagonal within the row
+//   dep[e]   : for a strictly lower entry, the local row (position - first
+//              position of the box) of its column when that row is in the
+//              box, else -1
 constexpr int ILU_TILE_THREADS = 256;
 constexpr size_t ILU_TILE_SMEM_MAX = 200 * 1024;
+constexpr int ILU_TILE_LPF = 16;  // strictly lower entries whose dep[] is prefetched
 
-static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(
-    int ntiles, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ uptr, double *luv,
-    const int *__restrict__ tile_pos, const int *__restrict__ tile_lvl, const int *__restrict__ lvl_ptr,
-    const int *__restrict__ perm, const int *__restrict__ halo_ptr, const int *__restrict__ halo_row,
-    const int *__restrict__ voff, const int *__restrict__ dep, int *flag, int epoch, int *err, unsigned *ticket)
+struct IluTileArgs {
+    int ntiles;
+    const int *rp, *ci, *uptr;
+    double *luv;
+    const int *tile_pos, *tile_lvl, *lvl_ptr, *perm, *halo_ptr, *halo_row;
+    const int *ebase, *ent, *roff, *rdiag, *dep;
+    int *flag, epoch, *err;
+    unsigned *ticket;
+};
+
+// shared-memory layout of a box with E entries and R rows
+struct IluTileSmem {
+    size_t val, col, row, diag, total;
+    static __host__ __device__ IluTileSmem of(int E, int R)
+    {
+        IluTileSmem m;
+        m.val = 0;
+        m.col = m.val + (size_t)E * sizeof(double);
+        m.row = m.col + (((size_t)E * sizeof(int) + 15) & ~(size_t)15);
+        m.diag = m.row + (((size_t)(R + 1) * sizeof(int) + 15) & ~(size_t)15);
+        m.total = m.diag + (((size_t)R * sizeof(int) + 15) & ~(size_t)15);
+        return m;
+    }
+};
+
+static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileArgs A, int max_entries, int max_rows)
 {
-    extern __shared__ __align__(16) double ilu_sv[];
+    extern __shared__ __align__(16) unsigned char ilu_smem[];
+    const IluTileSmem L = IluTileSmem::of(max_entries, max_rows);
+    double *sv = (double *)(ilu_smem + L.val);
+    int *sc = (int *)(ilu_smem + L.col);
+    int *srow = (int *)(ilu_smem + L.row);
+    int *sdg = (int *)(ilu_smem + L.diag);
     __shared__ int s_t, s_err;
     while (true) {
         if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(ticket, 1u);
+            const unsigned t = atomicAdd(A.ticket, 1u);
             // every CTA ends with one failing claim; the last of them re-arms
-            if (t == (unsigned)(ntiles + gridDim.x - 1)) *ticket = 0u;
+            if (t == (unsigned)(A.ntiles + gridDim.x - 1)) *A.ticket = 0u;
             s_t = (int)t;
-            s_err = *(volatile int *)err;
+            s_err = *(volatile int *)A.err;
         }
         __syncthreads();
         const int t = s_t, e0 = s_err;
         __syncthreads();
-        if (t >= ntiles) return;
+        if (t >= A.ntiles) return;
         if (e0) continue;
-        const int p0 = tile_pos[t], p1 = tile_pos[t + 1];
-        // the box's rows: A's values (nothing else writes them)
-        for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) {
-            const int i = perm[p];
-            double *dst = ilu_sv + voff[p];
-            for (int k = rp[i]; k < rp[i + 1]; k++) dst[k - rp[i]] = __ldcg(luv + k);
+        const int p0 = A.tile_pos[t], p1 = A.tile_pos[t + 1], rows = p1 - p0;
+        const int eb = A.ebase[t], E = A.ebase[t + 1] - eb;
+        // stage: entries (A's values: nothing else writes the box's rows), row offsets, diagonals
+        for (int e = threadIdx.x; e < E; e += blockDim.x) {
+            const int j = A.ent[eb + e];
+            sv[e] = __ldcg(A.luv + j);
+            sc[e] = __ldg(A.ci + j);
         }
+        for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+            srow[r] = A.roff[p0 + r];
+            sdg[r] = A.rdiag[p0 + r];
+        }
+        if (threadIdx.x == 0) srow[rows] = E;
         // the halo rows' flags (bounded waits)
         bool ok = true;
-        for (int h = halo_ptr[t] + (int)threadIdx.x; h < halo_ptr[t + 1] && ok; h += blockDim.x) {
-            const int k = halo_row[h];
+        for (int h = A.halo_ptr[t] + (int)threadIdx.x; h < A.halo_ptr[t + 1] && ok; h += blockDim.x) {
+            const int k = A.halo_row[h];
             long spins = 0;
             unsigned long long t0 = 0;
             unsigned ns = 32;
-            while (ld_acquire(flag + k) != epoch) {
+            while (ld_acquire(A.flag + k) != A.epoch) {
                 __nanosleep(ns);
                 if (ns < 512u) ns <<= 1;
                 if ((++spins & 63) == 0) {
                     const unsigned long long tn = gtimer();
                     if (t0 == 0) t0 = tn;
                     else if (tn - t0 > WAIT_LIMIT_NS) {
-                        atomicOr(err, DEV_FACTOR_TIMEOUT);
+                        atomicOr(A.err, DEV_FACTOR_TIMEOUT);
                         ok = false;
                         break;
                     }
-                    if (*(volatile int *)err) {
+                    if (*(volatile int *)A.err) {
                         ok = false;
                         break;
                     }
@@ -336,45 +377,67 @@ static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(
             }
         }
         if (!__syncthreads_and(ok)) continue;
-        for (int l = tile_lvl[t]; l < tile_lvl[t + 1]; l++) {
-            for (int p = lvl_ptr[l] + (int)threadIdx.x; p < lvl_ptr[l + 1]; p += blockDim.x) {
-                const int i = perm[p];
-                const int rs = rp[i], re = rp[i + 1], up = uptr[i];
-                double *a = ilu_sv + voff[p];  // a[e - rs]: entry e of row i
-                for (int j = rs; j < up; j++) {
-                    const int k = ci[j];
-                    const int kb = rp[k], ukp = uptr[k], kend = rp[k + 1];
-                    const int dk = dep[j];  // row k in the box: its values at ilu_sv[dk + (e - kb)]
-                    double piv = dk >= 0 ? ilu_sv[dk + (ukp - kb)] : __ldcg(luv + ukp);
-                    if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
-                    const double lij = a[j - rs] / piv;
-                    a[j - rs] = lij;
-                    int subptr = ukp;
-                    for (int jj = j + 1; jj < re; jj++) {
-                        const int kk = ci[jj];
-                        while (subptr < kend && __ldg(ci + subptr) < kk) subptr++;
-                        if (subptr < kend) {
-                            if (__ldg(ci + subptr) == kk) {
-                                const double u = dk >= 0 ? ilu_sv[dk + (subptr - kb)] : __ldcg(luv + subptr);
-                                const double tt = lij * u;
-                                a[jj - rs] = a[jj - rs] - tt;
-                            }
-                        } else
-                            break;
+        for (int l = A.tile_lvl[t]; l < A.tile_lvl[t + 1]; l++) {
+            for (int p = A.lvl_ptr[l] + (int)threadIdx.x; p < A.lvl_ptr[l + 1]; p += blockDim.x) {
+                const int r = p - p0;
+                const int b = srow[r], e = srow[r + 1], nd = sdg[r];
+                int dq[ILU_TILE_LPF];
+#pragma unroll
+                for (int q = 0; q < ILU_TILE_LPF; q++) dq[q] = q < nd ? __ldg(A.dep + eb + b + q) : -1;
+                for (int q = 0; q < nd; q++) {
+                    int dk = -1;
+#pragma unroll
+                    for (int w = 0; w < ILU_TILE_LPF; w++)
+                        if (w == q) dk = dq[w];
+                    if (q >= ILU_TILE_LPF) dk = __ldg(A.dep + eb + b + q);
+                    const int jl = b + q;  // this L entry
+                    if (dk >= 0) {  // row k in the box
+                        const int kb = srow[dk], ke = srow[dk + 1], kd = kb + sdg[dk];
+                        double piv = sv[kd];
+                        if (fabs(piv) < 1e-20) piv = 1e-20;  // no-op: row k clamped its own pivot
+                        const double lij = sv[jl] / piv;
+                        sv[jl] = lij;
+                        int sub = kd;
+                        for (int jj = jl + 1; jj < e; jj++) {
+                            const int kk = sc[jj];
+                            while (sub < ke && sc[sub] < kk) sub++;
+                            if (sub < ke) {
+                                if (sc[sub] == kk) {
+                                    const double tt = lij * sv[sub];
+                                    sv[jj] = sv[jj] - tt;
+                                }
+                            } else
+                                break;
+                        }
+                    } else {  // a halo row: final values in global memory
+                        const int k = sc[jl];
+                        const int ukp = __ldg(A.uptr + k), kend = __ldg(A.rp + k + 1);
+                        double piv = __ldcg(A.luv + ukp);
+                        if (fabs(piv) < 1e-20) piv = 1e-20;
+                        const double lij = sv[jl] / piv;
+                        sv[jl] = lij;
+                        int sub = ukp;
+                        for (int jj = jl + 1; jj < e; jj++) {
+                            const int kk = sc[jj];
+                            while (sub < kend && __ldg(A.ci + sub) < kk) sub++;
+                            if (sub < kend) {
+                                if (__ldg(A.ci + sub) == kk) {
+                                    const double tt = lij * __ldcg(A.luv + sub);
+                                    sv[jj] = sv[jj] - tt;
+                                }
+                            } else
+                                break;
+                        }
                     }
                 }
-                if (fabs(a[up - rs]) < 1e-20) a[up - rs] = 1e-20;
+                if (fabs(sv[b + nd]) < 1e-20) sv[b + nd] = 1e-20;
             }
             __syncthreads();
         }
-        for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) {
-            const int i = perm[p];
-            const double *src = ilu_sv + voff[p];
-            for (int k = rp[i]; k < rp[i + 1]; k++) luv[k] = src[k - rp[i]];
-        }
+        for (int e = threadIdx.x; e < E; e += blockDim.x) A.luv[A.ent[eb + e]] = sv[e];
         __threadfence();
         __syncthreads();
-        for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) st_release(flag + perm[p], epoch);
+        for (int r = threadIdx.x; r < rows; r += blockDim.x) st_release(A.flag + A.perm[p0 + r], A.epoch);
     }
 }
 
