@@ -1000,12 +1000,13 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
                 big /= 2;
                 return true;
             };
-            // first guess from the mean entries per row (a box's rows plus a
-            // quarter, its halo half its rows), then the layout's own sizes
+            // first guess from the mean entries per row (a box of mean rows,
+            // its halo a quarter of its rows: the smallest box the layout
+            // could accept), then the layout's own sizes decide
             const double per_row = (double)T.nnz / n;
             for (;;) {
                 const int rows = tt.tx * tt.ty * tt.tz;
-                if (TileSmem::of<double, double, double>(rows, rows / 2, (int)(rows * per_row * 1.25)).total <=
+                if (TileSmem::of<double, double, double>(rows, rows / 4, (int)(rows * per_row)).total <=
                         TILE_SMEM_MAX ||
                     !shrink())
                     break;
