@@ -454,10 +454,11 @@ int xs_set_trsv_block_rows(int max_rows);
  * 0 loads each row's data from global memory one level ahead.  Same result
  * either way.  Environment XS_LU_STAGED sets it at first use. */
 int xs_set_trsv_block_staging(int enable);
-/* Exact ILU(0) factorisation: 1 (default) on the box schedule of the L solve
- * when L has boxes (rows staged in shared memory, one halo wait per box,
- * barriers between the box's levels), 0 the level-ordered lane groups.  Same
- * factors either way.  Environment XS_ILU_TILES sets it at first use. */
+/* Exact ILU(0) factorisation: 1 on the box schedule of the L solve when L
+ * has boxes (entries staged in shared memory, one halo wait per box,
+ * barriers between the box's levels), 0 (default; faster as measured) the
+ * level-ordered lane groups.  Same factors either way.  Environment
+ * XS_ILU_TILES sets it at first use. */
 int xs_set_ilu_tiles(int enable);
 /* Jacobi-sweep preconditioner apply: 1 computes sweeps 2 and 3 of each
  * narrow diagonal-slot triangle in one pass (each row recomputes the

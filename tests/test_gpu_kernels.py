@@ -160,7 +160,7 @@ def test_ilu0_box_schedule_bitwise(cuda):
                 P = Plan(A).factor("ilu0")
                 assert np.array_equal(P.lu_values(), ref), (A.name, on)
             finally:
-                L.xs_set_ilu_tiles(1)
+                L.xs_set_ilu_tiles(0)
 
 
 def _wide_rows_matrix():
