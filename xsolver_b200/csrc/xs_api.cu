@@ -40,7 +40,11 @@ Geom &geom()
         cudaDeviceProp p;
         if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) {
             g.sms = p.multiProcessorCount;
-            g.red_grid = 8 * g.sms;
+            // CTAs per SM of the vector-op reductions (environment
+            // XS_RED_CTAS_PER_SM, 1-8; default 8: full occupancy)
+            int k = 8;
+            if (const char *e = getenv("XS_RED_CTAS_PER_SM")) k = std::max(1, std::min(8, atoi(e)));
+            g.red_grid = k * g.sms;
         }
         init = true;
     }
