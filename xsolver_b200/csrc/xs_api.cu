@@ -146,6 +146,7 @@ TrsvTuning &trsv_tuning()
         if (const char *e = getenv("XS_TRSV_BLOCK_ROWS")) t.block_max_rows = std::max(0, atoi(e));
         if (const char *e = getenv("XS_SWEEP_FUSE")) t.fuse_sweeps = atoi(e) != 0;
         if (const char *e = getenv("XS_LU_STAGED")) t.lu_staged = atoi(e) != 0;
+        if (const char *e = getenv("XS_SWEEP_BALANCED")) t.balanced_sweep_grid = atoi(e) != 0;
         init = true;
     }
     return t;

@@ -213,9 +213,16 @@ struct PrecondDev {
                 const FT *ev = T.evals<FT>();
                 if (!ev) throw Status(XS_ERR_ORDER);  // copy not built for this configuration
                 const int *doff = T.doff.p;
-                // one wave of resident CTAs, grid-stride over the row blocks
+                // one wave of resident CTAs, grid-stride over the row blocks;
+                // balanced: the smallest grid of at most one wave that gives
+                // every CTA the same number of row blocks (no partial last round)
                 const int rb = (n + 256 * ell_rows_for<FT>() - 1) / (256 * ell_rows_for<FT>());
-                const int gs = std::max(1, std::min(geom().sms * sweep_min_blocks_for<FT>(), rb));
+                const int wave = geom().sms * sweep_min_blocks_for<FT>();
+                int gs = std::max(1, std::min(wave, rb));
+                if (trsv_tuning().balanced_sweep_grid && rb > wave) {
+                    const int per = (rb + wave - 1) / wave;
+                    gs = (rb + per - 1) / per;
+                }
                 auto go = [&](auto cols) {
                     using CT = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
                     const DT *dv = upper ? dinv : (const DT *)nullptr;

@@ -668,12 +668,29 @@ inline void launch_csr(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot 
     launch_pdl(k_csr_spmv_tiled<VT, MT, Epi>, dim3(g), dim3(SPMV_THREADS), sm, s, a, x, y, epi, slot);
 }
 
+// ELL SpMV on a grid whose CTAs all take the same number of row blocks
+// (environment XS_ELL_BALANCED=1) instead of one full wave (default)
+inline bool ell_balanced_grid()
+{
+    static const bool b = [] {
+        const char *e = getenv("XS_ELL_BALANCED");
+        return e && atoi(e) != 0;
+    }();
+    return b;
+}
+
 template <typename VT, typename MT, typename Epi>
 inline void launch_ell(const Operator &op, const VT *x, VT *y, Epi epi, RedSlot slot, cudaStream_t s)
 {
-    // the grid covers the rows at ell_rows_for<MT>() rows per thread
-    const int g = (int)std::min<long>((long)op.ell_grid * ELL_ROWS / ell_rows_for<MT>(),
-                                      (op.n + 256L * ell_rows_for<MT>() - 1) / (256L * ell_rows_for<MT>()));
+    // the grid covers the rows at ell_rows_for<MT>() rows per thread;
+    // balanced: every CTA takes the same number of row blocks
+    const long rb = (op.n + 256L * ell_rows_for<MT>() - 1) / (256L * ell_rows_for<MT>());
+    const long wave = (long)op.ell_grid * ELL_ROWS / ell_rows_for<MT>();
+    int g = (int)std::min<long>(wave, rb);
+    if (ell_balanced_grid() && rb > wave) {
+        const long per = (rb + wave - 1) / wave;
+        g = (int)((rb + per - 1) / per);
+    }
     if (op.ell_dia && op.ell_w <= 8)
         launch_pdl(k_ell_spmv<VT, MT, uint8_t, Epi>, dim3(g), dim3(256), 0, s, op.ell<MT, uint8_t>(), x, y, epi, slot);
     else if (op.ell_dia)

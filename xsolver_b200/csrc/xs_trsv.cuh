@@ -101,6 +101,9 @@ struct TrsvTuning {
     // single-CTA solve with its level batches staged in shared memory (1) or
     // its row data loaded one level ahead from global memory (0)
     int lu_staged = 1;
+    // Jacobi-sweep passes on a grid whose CTAs all take the same number of
+    // row blocks (1) or on one full wave of CTAs (0)
+    int balanced_sweep_grid = 0;
 };
 TrsvTuning &trsv_tuning();
 

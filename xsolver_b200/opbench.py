@@ -30,7 +30,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--stencil", default="poisson7", choices=sorted(STENCILS))
     ap.add_argument("--grid", type=int, default=128)
-    ap.add_argument("--factor", default="ilu0", choices=["ilu0", "parilu", "parilut", "ic0"])
+    ap.add_argument("--factor", default="ilu0", choices=["ilu0", "parilu", "parilut", "ic0", "ilup", "ict"],
+                    help="ilup: Saad ILUT (lfil 5, 1e-4), ict: ICT (5, 1e-4), factored on the host")
     ap.add_argument("--ops", default="", help="comma-separated: " + ",".join(Plan.OPS))
     ap.add_argument("--prec", default="fp64", choices=list(Plan.PREC), help="factor storage precision")
     ap.add_argument("--trsv", type=int, default=0, help="0 exact triangular solves, k>0 k Jacobi sweeps")
@@ -84,9 +85,13 @@ def main(argv=None):
         out["batch"] = {"k": k, "rtol": a.rtol, **res}
     if a.solve:
         b = st.rhs_uniform(A.n, 0, 0.0 if a.stencil == "convdiff27" else -1.0, 1.0)
-        S = Solver(A, fmt="ell").ksp_settype(a.solve).ksp_setoption(1e-10, 3000, 30).pc_settype(a.factor)
+        S = Solver(A, fmt="ell").ksp_settype(a.solve).ksp_setoption(a.rtol, 3000, 30).pc_settype(a.factor)
         if a.factor == "parilut":
             S.pc_setparilut(2.0, 5, 1e-4)
+        elif a.factor == "ilup":
+            S.pc_setilut(1e-4, 5)
+        elif a.factor == "ict":
+            S.pc_setict(1e-4, 5)
         S.pc_set_trsv(a.trsv)
         if a.mixed:
             S.set_precision("fp64", "fp32", a.prec).set_inner(1e-4, 300)
