@@ -1912,7 +1912,7 @@ int xs_tri_tiles(int n, const int *rp, const int *ci, int upper, int tx, int ty,
         info[9] = (int)P.halo_row.size();
         info[10] = P.max_rows;
         info[11] = P.max_halo;
-        auto put = [](int *dst, const std::vector<int> &v) {
+        auto put = [](int *dst, const auto &v) {
             if (dst && !v.empty()) std::memcpy(dst, v.data(), sizeof(int) * v.size());
         };
         put(perm, P.perm); put(prp, P.prp); put(pci, P.pci); put(tile_pos, P.tile_pos);

@@ -860,6 +860,7 @@ struct TriDev {
     // batch b's first level (nlub + 1 values), or -1 - level for a level too
     // large to stage (solved from global memory)
     int nlub = 0;
+    int max_level_rows = 0;  // widest dependency level (level layout)
     DBuf<int> lub;
     bool tiled = false;
     int ntiles = 0, tile_elems = 0;  // tile_elems: shared-memory values per box (rows + halo)
@@ -1062,6 +1063,8 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
                                         T.src.p);
         check_launch();
         T.lstart.alloc(P.nlevels + 1); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
+        T.max_level_rows = 0;
+        for (int l = 0; l < P.nlevels; l++) T.max_level_rows = std::max(T.max_level_rows, P.lstart[l + 1] - P.lstart[l]);
         // level batches of the staged single-CTA solve (systems it serves only)
         T.nlub = 0;
         T.lub.free();
@@ -1411,7 +1414,12 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
                                          (int)ssm));
             sattr = ssm;
         }
-        k_lu_staged<VT, FT, DT><<<1, LU_BLOCK_THREADS, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
+        // as many threads as the widest level has rows (whole warps, at least
+        // 4): a level then takes one pass, and the barriers between levels
+        // wait for no idle warps
+        const int wide = std::max(L.max_level_rows, U.max_level_rows);
+        const int thr = std::min(LU_BLOCK_THREADS, std::max(128, (wide + 31) / 32 * 32));
+        k_lu_staged<VT, FT, DT><<<1, thr, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
                                                                   U.args<FT>(), U.lstart.p, U.lub.p, U.nlub, dinv, x,
                                                                   z, done_flag);
         return;

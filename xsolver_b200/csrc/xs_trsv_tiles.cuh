@@ -87,11 +87,39 @@ constexpr int TILE_PF = 8;  // entries of a row held in registers ahead of its l
 constexpr int TILE_REACH_MAX = 8;  // largest grid step of a dependency in any direction
 constexpr size_t TILE_SMEM_MAX = 200 * 1024;
 
+// an allocator whose resize leaves the elements uninitialised (arrays that
+// are written in full afterwards, by several threads: no serial zero fill)
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <typename U>
+    UninitAlloc(const UninitAlloc<U> &) noexcept
+    {
+    }
+    template <typename U>
+    void construct(U *p) noexcept
+    {
+        ::new ((void *)p) U;
+    }
+    template <typename U, typename... A>
+    void construct(U *p, A &&...a)
+    {
+        ::new ((void *)p) U(std::forward<A>(a)...);
+    }
+};
+template <typename T>
+using HostArray = std::vector<T, UninitAlloc<T>>;
+
 struct TileHostPlan {
     int n = 0, ntiles = 0, max_rows = 0, max_halo = 0, max_entries = 0;
     int nx = 0, ny = 0, nz = 0, sa = 0, sb = 0, sc = 0;
-    std::vector<int> perm, prp, pci, tile_pos, tile_lvl, lvl_ptr, halo_ptr, halo_row;
-    std::vector<long> src;
+    std::vector<int> perm, prp, tile_pos, tile_lvl, lvl_ptr, halo_ptr, halo_row;
+    HostArray<int> pci;   // every entry written by the layout
+    HostArray<long> src;
 };
 
 // ---------------------------------------------------------------- grid fit
@@ -305,16 +333,18 @@ inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF sr
     const long Z = h.nz;
     const long ntx = (X + tx - 1) / tx, nty = (Y + ty - 1) / ty, ntz = (Z + tz - 1) / tz;
     if (ntx * nty * ntz > (1L << 26)) return false;
-    std::vector<int> tile_of(n);  // by logical index: box id in the sheared box grid
+    HostArray<int> tile_of(n);  // by logical index: box id in the sheared box grid
     std::vector<int> cnt((size_t)(ntx * nty * ntz), 0);
-    for (long q = 0; q < n; q++) {
-        int x, y, z;
-        g.of(q, x, y, z);
-        const long xs = x + (long)sa * y + (long)sb * z, ys = y + (long)sc * z;
-        const int id = (int)(((long)(z / tz) * nty + ys / ty) * ntx + xs / tx);
-        tile_of[q] = id;
-        cnt[id]++;
-    }
+    host_parallel_for((n + 65535) / 65536, 1, [&](long b) {
+        const long q1 = std::min<long>(n, (b + 1) * 65536);
+        for (long q = b * 65536; q < q1; q++) {
+            int x, y, z;
+            g.of(q, x, y, z);
+            const long xs = x + (long)sa * y + (long)sb * z, ys = y + (long)sc * z;
+            tile_of[q] = (int)(((long)(z / tz) * nty + ys / ty) * ntx + xs / tx);
+        }
+    });
+    for (long q = 0; q < n; q++) cnt[tile_of[q]]++;
     // order the non-empty boxes by wavefront, then z, y, x
     std::vector<std::pair<long, int>> order;
     for (long id = 0; id < (long)cnt.size(); id++) {
@@ -388,8 +418,8 @@ inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF sr
         const int r = h.perm[p];
         h.prp[p + 1] = h.prp[p] + (rp[r + 1] - rp[r]);
     }
-    h.pci.assign(nnz, 0);
-    h.src.assign(nnz, 0);
+    h.pci.resize(nnz);  // written in full below (each box its rows' entries)
+    h.src.resize(nnz);
     h.halo_ptr.assign(h.ntiles + 1, 0);
     std::vector<std::vector<int>> ext_of(h.ntiles);
     host_parallel_for(h.ntiles, 16, [&](long t) {
