@@ -406,8 +406,8 @@ struct Handle {
     // boxes whose entries fit in shared memory
     bool ilu_tiles = false;
     size_t ilu_tiles_smem = 0;
-    int ilu_max_entries = 0, ilu_max_rows = 0;
-    DBuf<int> ilu_ebase, ilu_ent, ilu_roff, ilu_rdiag, ilu_dep;
+    int ilu_max_entries = 0, ilu_max_lower = 0, ilu_max_rows = 0;
+    DBuf<int> ilu_ebase, ilu_ent, ilu_roff, ilu_rdiag, ilu_lbase, ilu_loff, ilu_dep;
     TriHostPlan hL, hU;
     DBuf<double> luv, fv, tmpv;
     DBuf<long> udiag_src;
@@ -612,7 +612,8 @@ static void update_values(Handle &h, const double *v)
 static void build_ilu_tiles(Handle &h)
 {
     h.ilu_tiles = false;
-    for (DBuf<int> *b : {&h.ilu_ebase, &h.ilu_ent, &h.ilu_roff, &h.ilu_rdiag, &h.ilu_dep}) b->free();
+    for (DBuf<int> *b : {&h.ilu_ebase, &h.ilu_ent, &h.ilu_roff, &h.ilu_rdiag, &h.ilu_lbase, &h.ilu_loff, &h.ilu_dep})
+        b->free();
     const TriDev &L = h.M.L;
     if (!L.tiled || L.ntiles <= 0) return;
     const int n = h.n, nt = L.ntiles;
@@ -621,31 +622,35 @@ static void build_ilu_tiles(Handle &h)
     L.t_pos.download(tpos.data(), nt + 1, h.s);
     XS_CUDA(cudaStreamSynchronize(h.s));
     const int *rp = h.hrp.data(), *ci = h.hci.data();
-    std::vector<int> ebase(nt + 1, 0), roff(n), rdiag(n), box_of(n), local_of(n);
-    int max_e = 0, max_r = 0;
+    std::vector<int> ebase(nt + 1, 0), lbase(nt + 1, 0), roff(n), rdiag(n), loff(n), box_of(n), local_of(n);
+    int max_e = 0, max_l = 0, max_r = 0;
     for (int t = 0; t < nt; t++) {
-        int o = 0;
+        int o = 0, ol = 0;
         for (int p = tpos[t]; p < tpos[t + 1]; p++) {
             const int i = perm[p];
             roff[p] = o;
             rdiag[p] = h.huptr[i] - rp[i];
+            loff[p] = ol;
             box_of[i] = t;
             local_of[i] = p - tpos[t];
             o += rp[i + 1] - rp[i];
+            ol += h.huptr[i] - rp[i];
         }
         ebase[t + 1] = ebase[t] + o;
+        lbase[t + 1] = lbase[t] + ol;
         max_e = std::max(max_e, o);
+        max_l = std::max(max_l, ol);
         max_r = std::max(max_r, tpos[t + 1] - tpos[t]);
     }
-    if (IluTileSmem::of(max_e, max_r).total > ILU_TILE_SMEM_MAX) return;
-    std::vector<int> ent(std::max<long>(h.nnz, 1)), dep(std::max<long>(h.nnz, 1), -1);
+    if (IluTileSmem::of(max_e, max_l, max_r).total > ILU_TILE_SMEM_MAX) return;
+    std::vector<int> ent(std::max<long>(h.nnz, 1)), dep(std::max(lbase[nt], 1), -1);
     for (int t = 0; t < nt; t++)
         for (int p = tpos[t]; p < tpos[t + 1]; p++) {
             const int i = perm[p];
-            const int e0 = ebase[t] + roff[p];
+            const int e0 = ebase[t] + roff[p], l0 = lbase[t] + loff[p];
             for (int k = rp[i]; k < rp[i + 1]; k++) {
                 ent[e0 + (k - rp[i])] = k;
-                if (k < h.huptr[i] && box_of[ci[k]] == t) dep[e0 + (k - rp[i])] = local_of[ci[k]];
+                if (k < h.huptr[i] && box_of[ci[k]] == t) dep[l0 + (k - rp[i])] = local_of[ci[k]];
             }
         }
     auto up = [&](DBuf<int> &b, const std::vector<int> &v) {
@@ -656,11 +661,14 @@ static void build_ilu_tiles(Handle &h)
     up(h.ilu_ent, ent);
     up(h.ilu_roff, roff);
     up(h.ilu_rdiag, rdiag);
+    up(h.ilu_lbase, lbase);
+    up(h.ilu_loff, loff);
     up(h.ilu_dep, dep);
     XS_CUDA(cudaStreamSynchronize(h.s));  // the host arrays go out of scope
     h.ilu_max_entries = max_e;
+    h.ilu_max_lower = max_l;
     h.ilu_max_rows = max_r;
-    h.ilu_tiles_smem = IluTileSmem::of(max_e, max_r).total;
+    h.ilu_tiles_smem = IluTileSmem::of(max_e, max_l, max_r).total;
     h.ilu_tiles = true;
 }
 
@@ -909,8 +917,10 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
             const int gl = std::min(L.ntiles, geom().sms * per_sm);
             const IluTileArgs args{L.ntiles, h.A.rp.p, h.A.ci.p, h.uptr.p, h.luv.p, L.t_pos.p, L.t_lvl.p, L.t_lptr.p,
                                    L.perm.p, L.t_hptr.p, L.t_hrow.p, h.ilu_ebase.p, h.ilu_ent.p, h.ilu_roff.p,
-                                   h.ilu_rdiag.p, h.ilu_dep.p, h.flags.p, h.ilu_epoch, h.err.p, h.fticket.p};
-            k_ilu0_tiles<<<gl, ILU_TILE_THREADS, sm, h.s>>>(args, h.ilu_max_entries, h.ilu_max_rows);
+                                   h.ilu_rdiag.p, h.ilu_lbase.p, h.ilu_loff.p, h.ilu_dep.p, h.flags.p,
+                                   h.ilu_epoch, h.err.p, h.fticket.p};
+            k_ilu0_tiles<<<gl, ILU_TILE_THREADS, sm, h.s>>>(args, h.ilu_max_entries, h.ilu_max_lower,
+                                                            h.ilu_max_rows);
         } else if (ilu_group && G <= 32) {
             const int rpb = 128 / G;
             const int bps = ilu_bps_env ? ilu_bps_env : (G <= 8 ? 4 : 8);

@@ -272,58 +272,68 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
 // ILU(0) is L's): persistent CTAs take boxes in wavefront order by ticket.
 // A CTA stages its box's entries — values and column indices, in the box's
 // entry order (rows by position, each row's entries in column order) — with
-// each row's entry offset and diagonal offset, waits once for the published
-// flags of the box's halo rows (dependencies in earlier boxes, final in
-// global memory), then updates the rows level by level with a barrier
-// between levels: a dependency row in the box is read from shared memory
-// (its local row from dep[], prefetched at the start of the row), a halo row
-// from global memory.  Each row update is the reference's IKJ step in its
-// order (pivot division, then the merge with row k's upper part), so the
-// factors are bitwise those of the thread-per-row kernel.  The rows are
-// written back and their flags released.  Waits are bounded.
+// each row's entry offset and diagonal offset (= its count of strictly lower
+// entries) and, per strictly lower entry, the box-local row of its column
+// (-1 for a row of an earlier box); waits once for the published flags of
+// the box's halo rows; then updates the rows level by level with a barrier
+// between levels.  A dependency row in the box is read from shared memory; a
+// halo row (final in global memory) has its pivot and upper part loaded in
+// one round of independent loads.  Each row update is the reference's IKJ
+// step: the pivot division, then for every later entry of the row the
+// subtraction of l_ik * u_kj where row k's upper part has that column — the
+// same operations in the same order as the thread-per-row kernel, so the
+// factors are bitwise the same.  The rows are written back and their flags
+// released.  Waits are bounded.
 //   ent[e]   : A's entry index of box entry e (boxes consecutive; ebase[t])
 //   roff[p]  : entry offset of the row at position p within its box
 //   rdiag[p] : offset of that row's diagonal within the row
-//   dep[e]   : for a strictly lower entry, the local row (position - first
-//              position of the box) of its column when that row is in the
-//              box, else -1
+//   loff[p]  : offset of the row's strictly lower entries among the box's
+//              (boxes consecutive; lbase[t])
+//   dep[l]   : box-local row (position - first position of the box) of the
+//              column of strictly lower entry l, or -1 (a halo row)
 constexpr int ILU_TILE_THREADS = 256;
-constexpr size_t ILU_TILE_SMEM_MAX = 200 * 1024;
-constexpr int ILU_TILE_LPF = 16;  // strictly lower entries whose dep[] is prefetched
+constexpr size_t ILU_TILE_SMEM_MAX = 224 * 1024;
+constexpr int ILU_HALO_U = 8;  // upper-part entries of a halo row held in registers
 
 struct IluTileArgs {
     int ntiles;
     const int *rp, *ci, *uptr;
     double *luv;
     const int *tile_pos, *tile_lvl, *lvl_ptr, *perm, *halo_ptr, *halo_row;
-    const int *ebase, *ent, *roff, *rdiag, *dep;
+    const int *ebase, *ent, *roff, *rdiag, *lbase, *loff, *dep;
     int *flag, epoch, *err;
     unsigned *ticket;
 };
 
-// shared-memory layout of a box with E entries and R rows
+// shared-memory layout of a box with E entries, EL strictly lower ones and R rows
 struct IluTileSmem {
-    size_t val, col, row, diag, total;
-    static __host__ __device__ IluTileSmem of(int E, int R)
+    size_t val, col, row, diag, lof, dep, total;
+    static __host__ __device__ IluTileSmem of(int E, int EL, int R)
     {
+        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
         IluTileSmem m;
         m.val = 0;
-        m.col = m.val + (size_t)E * sizeof(double);
-        m.row = m.col + (((size_t)E * sizeof(int) + 15) & ~(size_t)15);
-        m.diag = m.row + (((size_t)(R + 1) * sizeof(int) + 15) & ~(size_t)15);
-        m.total = m.diag + (((size_t)R * sizeof(int) + 15) & ~(size_t)15);
+        m.col = m.val + al((size_t)E * sizeof(double));
+        m.row = m.col + al((size_t)E * sizeof(int));
+        m.diag = m.row + al((size_t)(R + 1) * sizeof(int));
+        m.lof = m.diag + al((size_t)R * sizeof(int));
+        m.dep = m.lof + al((size_t)R * sizeof(int));
+        m.total = m.dep + al((size_t)EL * sizeof(int));
         return m;
     }
 };
 
-static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileArgs A, int max_entries, int max_rows)
+static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileArgs A, int max_entries, int max_lower,
+                                                                          int max_rows)
 {
     extern __shared__ __align__(16) unsigned char ilu_smem[];
-    const IluTileSmem L = IluTileSmem::of(max_entries, max_rows);
+    const IluTileSmem L = IluTileSmem::of(max_entries, max_lower, max_rows);
     double *sv = (double *)(ilu_smem + L.val);
     int *sc = (int *)(ilu_smem + L.col);
     int *srow = (int *)(ilu_smem + L.row);
     int *sdg = (int *)(ilu_smem + L.diag);
+    int *slof = (int *)(ilu_smem + L.lof);
+    int *sdep = (int *)(ilu_smem + L.dep);
     __shared__ int s_t, s_err;
     while (true) {
         if (threadIdx.x == 0) {
@@ -340,7 +350,8 @@ static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileA
         if (e0) continue;
         const int p0 = A.tile_pos[t], p1 = A.tile_pos[t + 1], rows = p1 - p0;
         const int eb = A.ebase[t], E = A.ebase[t + 1] - eb;
-        // stage: entries (A's values: nothing else writes the box's rows), row offsets, diagonals
+        const int lb = A.lbase[t], EL = A.lbase[t + 1] - lb;
+        // stage (A's values: nothing else writes the box's rows)
         for (int e = threadIdx.x; e < E; e += blockDim.x) {
             const int j = A.ent[eb + e];
             sv[e] = __ldcg(A.luv + j);
@@ -349,7 +360,9 @@ static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileA
         for (int r = threadIdx.x; r < rows; r += blockDim.x) {
             srow[r] = A.roff[p0 + r];
             sdg[r] = A.rdiag[p0 + r];
+            slof[r] = A.loff[p0 + r];
         }
+        for (int l = threadIdx.x; l < EL; l += blockDim.x) sdep[l] = A.dep[lb + l];
         if (threadIdx.x == 0) srow[rows] = E;
         // the halo rows' flags (bounded waits)
         bool ok = true;
@@ -380,17 +393,10 @@ static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileA
         for (int l = A.tile_lvl[t]; l < A.tile_lvl[t + 1]; l++) {
             for (int p = A.lvl_ptr[l] + (int)threadIdx.x; p < A.lvl_ptr[l + 1]; p += blockDim.x) {
                 const int r = p - p0;
-                const int b = srow[r], e = srow[r + 1], nd = sdg[r];
-                int dq[ILU_TILE_LPF];
-#pragma unroll
-                for (int q = 0; q < ILU_TILE_LPF; q++) dq[q] = q < nd ? __ldg(A.dep + eb + b + q) : -1;
+                const int b = srow[r], e = srow[r + 1], nd = sdg[r], lo = slof[r];
                 for (int q = 0; q < nd; q++) {
-                    int dk = -1;
-#pragma unroll
-                    for (int w = 0; w < ILU_TILE_LPF; w++)
-                        if (w == q) dk = dq[w];
-                    if (q >= ILU_TILE_LPF) dk = __ldg(A.dep + eb + b + q);
                     const int jl = b + q;  // this L entry
+                    const int dk = sdep[lo + q];
                     if (dk >= 0) {  // row k in the box
                         const int kb = srow[dk], ke = srow[dk + 1], kd = kb + sdg[dk];
                         double piv = sv[kd];
@@ -413,20 +419,44 @@ static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileA
                         const int k = sc[jl];
                         const int ukp = __ldg(A.uptr + k), kend = __ldg(A.rp + k + 1);
                         double piv = __ldcg(A.luv + ukp);
+                        const int ulen = kend - ukp - 1;  // upper entries after the diagonal
+                        int uc[ILU_HALO_U];
+                        double uv[ILU_HALO_U];
+#pragma unroll
+                        for (int w = 0; w < ILU_HALO_U; w++) {
+                            uc[w] = w < ulen ? __ldg(A.ci + ukp + 1 + w) : 0x7fffffff;
+                            uv[w] = w < ulen ? __ldcg(A.luv + ukp + 1 + w) : 0.0;
+                        }
                         if (fabs(piv) < 1e-20) piv = 1e-20;
                         const double lij = sv[jl] / piv;
                         sv[jl] = lij;
-                        int sub = ukp;
-                        for (int jj = jl + 1; jj < e; jj++) {
-                            const int kk = sc[jj];
-                            while (sub < kend && __ldg(A.ci + sub) < kk) sub++;
-                            if (sub < kend) {
-                                if (__ldg(A.ci + sub) == kk) {
-                                    const double tt = lij * __ldcg(A.luv + sub);
-                                    sv[jj] = sv[jj] - tt;
+                        if (ulen <= ILU_HALO_U) {
+                            // row k's upper columns are distinct and sorted, as
+                            // are row i's later columns: subtracting at every
+                            // matching column is the two-pointer merge's update
+                            for (int jj = jl + 1; jj < e; jj++) {
+                                const int kk = sc[jj];
+#pragma unroll
+                                for (int w = 0; w < ILU_HALO_U; w++) {
+                                    if (uc[w] == kk) {
+                                        const double tt = lij * uv[w];
+                                        sv[jj] = sv[jj] - tt;
+                                    }
                                 }
-                            } else
-                                break;
+                            }
+                        } else {
+                            int sub = ukp;
+                            for (int jj = jl + 1; jj < e; jj++) {
+                                const int kk = sc[jj];
+                                while (sub < kend && __ldg(A.ci + sub) < kk) sub++;
+                                if (sub < kend) {
+                                    if (__ldg(A.ci + sub) == kk) {
+                                        const double tt = lij * __ldcg(A.luv + sub);
+                                        sv[jj] = sv[jj] - tt;
+                                    }
+                                } else
+                                    break;
+                            }
                         }
                     }
                 }
