@@ -147,6 +147,10 @@ TrsvTuning &trsv_tuning()
         if (const char *e = getenv("XS_SWEEP_FUSE")) t.fuse_sweeps = atoi(e) != 0;
         if (const char *e = getenv("XS_LU_STAGED")) t.lu_staged = atoi(e) != 0;
         if (const char *e = getenv("XS_SWEEP_BALANCED")) t.balanced_sweep_grid = atoi(e) != 0;
+        if (const char *e = getenv("XS_LU_STAGED_THREADS")) {
+            const int v = atoi(e);
+            t.lu_staged_threads = v >= 32 && v <= LU_BLOCK_THREADS && v % 32 == 0 ? v : 0;
+        }
         init = true;
     }
     return t;

@@ -293,7 +293,8 @@ __global__ void __launch_bounds__(128) k_ilu0_groups(int n, const int *__restric
 //              column of strictly lower entry l, or -1 (a halo row)
 constexpr int ILU_TILE_THREADS = 256;
 constexpr size_t ILU_TILE_SMEM_MAX = 224 * 1024;
-constexpr int ILU_HALO_U = 8;  // upper-part entries of a halo row held in registers
+constexpr int ILU_HALO_U = 8;   // upper-part entries of a halo row held in registers
+constexpr int ILU_STAGE_U = 8;  // entries per thread per staging round
 
 struct IluTileArgs {
     int ntiles;
@@ -351,11 +352,32 @@ static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileA
         const int p0 = A.tile_pos[t], p1 = A.tile_pos[t + 1], rows = p1 - p0;
         const int eb = A.ebase[t], E = A.ebase[t + 1] - eb;
         const int lb = A.lbase[t], EL = A.lbase[t + 1] - lb;
-        // stage (A's values: nothing else writes the box's rows)
-        for (int e = threadIdx.x; e < E; e += blockDim.x) {
-            const int j = A.ent[eb + e];
-            sv[e] = __ldcg(A.luv + j);
-            sc[e] = __ldg(A.ci + j);
+        // stage (A's values: nothing else writes the box's rows), ILU_STAGE_U
+        // entries per thread per round so their gathers are in flight together
+        for (int e0 = threadIdx.x; e0 < E; e0 += blockDim.x * ILU_STAGE_U) {
+            int jv[ILU_STAGE_U];
+#pragma unroll
+            for (int u = 0; u < ILU_STAGE_U; u++) {
+                const int e = e0 + u * (int)blockDim.x;
+                jv[u] = e < E ? __ldg(A.ent + eb + e) : -1;
+            }
+            double vv[ILU_STAGE_U];
+            int cv[ILU_STAGE_U];
+#pragma unroll
+            for (int u = 0; u < ILU_STAGE_U; u++) {
+                if (jv[u] >= 0) {
+                    vv[u] = __ldcg(A.luv + jv[u]);
+                    cv[u] = __ldg(A.ci + jv[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < ILU_STAGE_U; u++) {
+                if (jv[u] >= 0) {
+                    const int e = e0 + u * (int)blockDim.x;
+                    sv[e] = vv[u];
+                    sc[e] = cv[u];
+                }
+            }
         }
         for (int r = threadIdx.x; r < rows; r += blockDim.x) {
             srow[r] = A.roff[p0 + r];
@@ -464,7 +486,17 @@ static __global__ void __launch_bounds__(ILU_TILE_THREADS) k_ilu0_tiles(IluTileA
             }
             __syncthreads();
         }
-        for (int e = threadIdx.x; e < E; e += blockDim.x) A.luv[A.ent[eb + e]] = sv[e];
+        for (int e0 = threadIdx.x; e0 < E; e0 += blockDim.x * ILU_STAGE_U) {
+            int jv[ILU_STAGE_U];
+#pragma unroll
+            for (int u = 0; u < ILU_STAGE_U; u++) {
+                const int e = e0 + u * (int)blockDim.x;
+                jv[u] = e < E ? __ldg(A.ent + eb + e) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < ILU_STAGE_U; u++)
+                if (jv[u] >= 0) A.luv[jv[u]] = sv[e0 + u * (int)blockDim.x];
+        }
         __threadfence();
         __syncthreads();
         for (int r = threadIdx.x; r < rows; r += blockDim.x) st_release(A.flag + A.perm[p0 + r], A.epoch);
