@@ -101,8 +101,7 @@ struct TrsvTuning {
     // single-CTA solve with its level batches staged in shared memory (1) or
     // its row data loaded one level ahead from global memory (0)
     int lu_staged = 1;
-    // threads of the staged single-CTA solve (0: the widest level's rows,
-    // rounded to whole warps, 128-1024)
+    // threads of the staged single-CTA solve (0: LU_BLOCK_THREADS)
     int lu_staged_threads = 0;
     // Jacobi-sweep passes on a grid whose CTAs all take the same number of
     // row blocks (1) or on one full wave of CTAs (0)
@@ -1417,12 +1416,10 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
                                          (int)ssm));
             sattr = ssm;
         }
-        // as many threads as the widest level has rows (whole warps, at least
-        // 4): a level then takes one pass, and the barriers between levels
-        // wait for no idle warps
-        const int wide = std::max(L.max_level_rows, U.max_level_rows);
-        int thr = std::min(LU_BLOCK_THREADS, std::max(128, (wide + 31) / 32 * 32));
-        if (trsv_tuning().lu_staged_threads > 0) thr = trsv_tuning().lu_staged_threads;
+        // 1024 threads: the batch copies go faster with more threads (2D
+        // 128^2, levels of at most 128 rows: 286 us at 1024 threads, 294 at
+        // 256, 342 at 128)
+        const int thr = trsv_tuning().lu_staged_threads > 0 ? trsv_tuning().lu_staged_threads : LU_BLOCK_THREADS;
         k_lu_staged<VT, FT, DT><<<1, thr, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
                                                                   U.args<FT>(), U.lstart.p, U.lub.p, U.nlub, dinv, x,
                                                                   z, done_flag);
