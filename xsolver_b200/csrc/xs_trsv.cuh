@@ -101,7 +101,8 @@ struct TrsvTuning {
     // single-CTA solve with its level batches staged in shared memory (1) or
     // its row data loaded one level ahead from global memory (0)
     int lu_staged = 1;
-    // threads of the staged single-CTA solve (0: LU_BLOCK_THREADS)
+    // walker threads of the staged single-CTA solve (multiple of 32, at most
+    // 512; 0: the widest level's rows rounded to whole warps)
     int lu_staged_threads = 0;
     // Jacobi-sweep passes on a grid whose CTAs all take the same number of
     // row blocks (1) or on one full wave of CTAs (0)
@@ -1306,90 +1307,130 @@ struct LuBatchSmem {
     static constexpr size_t bytes = pv + ((LUB_ENTRIES * sizeof(FT) + 8 + 15) & ~(size_t)15);
 };
 
-template <typename VT, typename FT, typename DT, bool UPPER>
-__device__ __forceinline__ void lus_phase(const TrsvArgs<FT> &P, const int *__restrict__ ls, const int *__restrict__ lub,
-                                          int nb, const DT *__restrict__ dinv, VT *ys, unsigned char *buf0,
-                                          unsigned char *buf1)
+__device__ __forceinline__ void named_sync(int id, int count)
 {
-    using B = LuBatchSmem<FT, DT>;
-    const int tid = threadIdx.x, T = blockDim.x;
-    auto first_level = [&](int b) { const int v = __ldg(lub + b); return v < 0 ? -1 - v : v; };
-    auto stage = [&](int b, unsigned char *buf) {
-        if (b < nb && __ldg(lub + b) >= 0) {
-            const int pa = __ldg(ls + first_level(b)), pb = __ldg(ls + first_level(b + 1));
-            const int ea = __ldg(P.prp + pa), eb = __ldg(P.prp + pb);
-            int *s_row = (int *)(buf + B::row), *s_eptr = (int *)(buf + B::eptr), *s_pci = (int *)(buf + B::pci);
-            for (int i = tid; i < pb - pa; i += T) cp_async4(s_row + i, P.perm + pa + i);
-            for (int i = tid; i <= pb - pa; i += T) cp_async4(s_eptr + i, P.prp + pa + i);
-            for (int i = tid; i < eb - ea; i += T) cp_async4(s_pci + i, P.pci + ea + i);
-            const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L, vb1 = ((long)eb * (long)sizeof(FT) + 3) & ~3L;
-            const unsigned char *vsrc = (const unsigned char *)P.pv;
-            for (long w = tid; w < (vb1 - vb0) / 4; w += T) cp_async4(buf + B::pv + 4 * w, vsrc + vb0 + 4 * w);
-            if (UPPER)
-                for (int i = tid; i < pb - pa; i += T) cp_async_n<sizeof(DT)>((DT *)(buf + B::in) + i, dinv + pa + i);
-        }
-        cp_async_commit();  // an empty group for an unstaged or absent batch keeps the count uniform
-    };
-    stage(0, buf0);
-    for (int b = 0; b < nb; b++) {
-        unsigned char *cur = (b & 1) ? buf1 : buf0;
-        stage(b + 1, (b & 1) ? buf0 : buf1);
-        cp_async_wait<1>();  // batch b's copies have landed
-        __syncthreads();
-        const int lb = __ldg(lub + b);
-        if (lb >= 0) {
-            const int l0 = lb, l1 = first_level(b + 1);
-            const int pa = __ldg(ls + l0), ea = __ldg(P.prp + pa);
-            const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L;
-            const int *s_row = (const int *)(cur + B::row), *s_eptr = (const int *)(cur + B::eptr);
-            const int *s_pci = (const int *)(cur + B::pci);
-            const DT *s_in = (const DT *)(cur + B::in);
-            const FT *pv = (const FT *)(cur + B::pv + ((long)ea * (long)sizeof(FT) - vb0));
-            for (int l = l0; l < l1; l++) {
-                const int q0 = __ldg(ls + l) - pa, q1 = __ldg(ls + l + 1) - pa;
-                for (int i = q0 + tid; i < q1; i += T) {
-                    const int row = s_row[i];
-                    VT acc = UPPER ? (VT)(ys[row] * (VT)s_in[i]) : ys[row];
-                    const int k1 = s_eptr[i + 1] - ea;
-                    for (int k = s_eptr[i] - ea; k < k1; k++) acc = msub(acc, ys[s_pci[k]], (VT)FVal<FT>::cvt(pv[k]));
-                    ys[row] = acc;
-                }
-                __syncthreads();
-            }
-        } else {  // one level too large to stage: its rows from global memory
-            const int l = -1 - lb;
-            for (int p = __ldg(ls + l) + tid; p < __ldg(ls + l + 1); p += T) {
-                const int row = __ldg(P.perm + p);
-                VT acc = UPPER ? (VT)(ys[row] * (VT)__ldg(dinv + p)) : ys[row];
-                for (int k = __ldg(P.prp + p); k < __ldg(P.prp + p + 1); k++)
-                    acc = msub(acc, ys[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
-                ys[row] = acc;
-            }
-            __syncthreads();
-        }
-    }
-    cp_async_wait<0>();
-    __syncthreads();
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int count)
+{
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+// first level of batch b of a triangle's batch list
+__device__ __forceinline__ int lub_first_level(const int *__restrict__ lub, int b)
+{
+    const int v = __ldg(lub + b);
+    return v < 0 ? -1 - v : v;
+}
+
+// copy batch b (rows, entry offsets, columns, values, U's dinv) into buf;
+// threads tid of T; nothing for a level too large to stage
+template <typename FT, typename DT, bool UPPER>
+__device__ __forceinline__ void lu_stage_batch(const TrsvArgs<FT> &P, const int *__restrict__ ls,
+                                               const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
+                                               unsigned char *buf, int tid, int T)
+{
+    using B = LuBatchSmem<FT, DT>;
+    if (__ldg(lub + b) < 0) return;
+    const int pa = __ldg(ls + lub_first_level(lub, b)), pb = __ldg(ls + lub_first_level(lub, b + 1));
+    const int ea = __ldg(P.prp + pa), eb = __ldg(P.prp + pb);
+    int *s_row = (int *)(buf + B::row), *s_eptr = (int *)(buf + B::eptr), *s_pci = (int *)(buf + B::pci);
+    for (int i = tid; i < pb - pa; i += T) cp_async4(s_row + i, P.perm + pa + i);
+    for (int i = tid; i <= pb - pa; i += T) cp_async4(s_eptr + i, P.prp + pa + i);
+    for (int i = tid; i < eb - ea; i += T) cp_async4(s_pci + i, P.pci + ea + i);
+    const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L, vb1 = ((long)eb * (long)sizeof(FT) + 3) & ~3L;
+    const unsigned char *vsrc = (const unsigned char *)P.pv;
+    for (long w = tid; w < (vb1 - vb0) / 4; w += T) cp_async4(buf + B::pv + 4 * w, vsrc + vb0 + 4 * w);
+    if (UPPER)
+        for (int i = tid; i < pb - pa; i += T) cp_async_n<sizeof(DT)>((DT *)(buf + B::in) + i, dinv + pa + i);
+}
+
+// the levels of batch b by threads tid of T (a barrier of those T threads,
+// id LU_LEVEL_BAR, after each level)
+constexpr int LU_LEVEL_BAR = 5;
+template <typename VT, typename FT, typename DT, bool UPPER>
+__device__ __forceinline__ void lu_batch_levels(const TrsvArgs<FT> &P, const int *__restrict__ ls,
+                                                const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
+                                                VT *ys, const unsigned char *buf, int tid, int T)
+{
+    using B = LuBatchSmem<FT, DT>;
+    const int lb = __ldg(lub + b);
+    if (lb >= 0) {
+        const int l0 = lb, l1 = lub_first_level(lub, b + 1);
+        const int pa = __ldg(ls + l0), ea = __ldg(P.prp + pa);
+        const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L;
+        const int *s_row = (const int *)(buf + B::row), *s_eptr = (const int *)(buf + B::eptr);
+        const int *s_pci = (const int *)(buf + B::pci);
+        const DT *s_in = (const DT *)(buf + B::in);
+        const FT *pv = (const FT *)(buf + B::pv + ((long)ea * (long)sizeof(FT) - vb0));
+        for (int l = l0; l < l1; l++) {
+            const int q0 = __ldg(ls + l) - pa, q1 = __ldg(ls + l + 1) - pa;
+            for (int i = q0 + tid; i < q1; i += T) {
+                const int row = s_row[i];
+                VT acc = UPPER ? (VT)(ys[row] * (VT)s_in[i]) : ys[row];
+                const int k1 = s_eptr[i + 1] - ea;
+                for (int k = s_eptr[i] - ea; k < k1; k++) acc = msub(acc, ys[s_pci[k]], (VT)FVal<FT>::cvt(pv[k]));
+                ys[row] = acc;
+            }
+            named_sync(LU_LEVEL_BAR, T);
+        }
+    } else {  // one level too large to stage: its rows from global memory
+        const int l = -1 - lb;
+        for (int p = __ldg(ls + l) + tid; p < __ldg(ls + l + 1); p += T) {
+            const int row = __ldg(P.perm + p);
+            VT acc = UPPER ? (VT)(ys[row] * (VT)__ldg(dinv + p)) : ys[row];
+            for (int k = __ldg(P.prp + p); k < __ldg(P.prp + p + 1); k++)
+                acc = msub(acc, ys[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
+            ys[row] = acc;
+        }
+        named_sync(LU_LEVEL_BAR, T);
+    }
+}
+
+// Warp-specialised: the first cw warps walk the levels (a barrier of those
+// warps only between levels), the other warps copy the batches, L's then
+// U's, into two buffers one batch ahead; named barriers 1-2 ("batch in
+// buffer k landed": the copiers arrive, the walkers wait) and 3-4 ("buffer
+// k free": the walkers arrive, the copiers wait before reusing it) hand the
+// buffers over.
 template <typename VT, typename FT, typename DT>
 __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_staged(TrsvArgs<FT> L, const int *__restrict__ lstart,
                                                                  const int *__restrict__ lubL, int nbL, TrsvArgs<FT> U,
                                                                  const int *__restrict__ ustart,
                                                                  const int *__restrict__ lubU, int nbU,
                                                                  const DT *__restrict__ dinv, const VT *__restrict__ x,
-                                                                 VT *__restrict__ z, const int *done_flag)
+                                                                 VT *__restrict__ z, const int *done_flag, int cw)
 {
     extern __shared__ __align__(16) unsigned char lus_smem[];
     if (done_flag && *done_flag) return;
     using B = LuBatchSmem<FT, DT>;
     const size_t yb = ((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15;
     VT *ys = (VT *)lus_smem;
-    unsigned char *buf0 = lus_smem + yb, *buf1 = buf0 + B::bytes;
+    unsigned char *bufs[2] = {lus_smem + yb, lus_smem + yb + B::bytes};
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) ys[i] = x[i];
     __syncthreads();
-    lus_phase<VT, FT, DT, false>(L, lstart, lubL, nbL, nullptr, ys, buf0, buf1);
-    lus_phase<VT, FT, DT, true>(U, ustart, lubU, nbU, dinv, ys, buf0, buf1);
+    const int all = blockDim.x, ct = cw * 32, nb = nbL + nbU;
+    if ((int)threadIdx.x >= ct) {  // copiers
+        const int tid = threadIdx.x - ct, T = all - ct;
+        for (int g = 0; g < nb; g++) {
+            const int k = g & 1;
+            if (g >= 2) named_sync(3 + k, all);  // the walkers are done with batch g - 2
+            if (g < nbL) lu_stage_batch<FT, DT, false>(L, lstart, lubL, g, nullptr, bufs[k], tid, T);
+            else lu_stage_batch<FT, DT, true>(U, ustart, lubU, g - nbL, dinv, bufs[k], tid, T);
+            cp_async_commit();
+            cp_async_wait<0>();
+            named_arrive(1 + k, all);
+        }
+    } else {  // walkers
+        for (int g = 0; g < nb; g++) {
+            const int k = g & 1;
+            named_sync(1 + k, all);  // batch g landed
+            if (g < nbL) lu_batch_levels<VT, FT, DT, false>(L, lstart, lubL, g, nullptr, ys, bufs[k], threadIdx.x, ct);
+            else lu_batch_levels<VT, FT, DT, true>(U, ustart, lubU, g - nbL, dinv, ys, bufs[k], threadIdx.x, ct);
+            if (g + 2 < nb) named_arrive(3 + k, all);  // buffer k free for batch g + 2
+        }
+    }
+    __syncthreads();
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) z[i] = ys[i];
 }
 
@@ -1416,13 +1457,15 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
                                          (int)ssm));
             sattr = ssm;
         }
-        // 1024 threads: the batch copies go faster with more threads (2D
-        // 128^2, levels of at most 128 rows: 286 us at 1024 threads, 294 at
-        // 256, 342 at 128)
-        const int thr = trsv_tuning().lu_staged_threads > 0 ? trsv_tuning().lu_staged_threads : LU_BLOCK_THREADS;
+        // 1024 threads: walker warps for the widest level's rows (at most 16),
+        // the rest copy
+        const int thr = LU_BLOCK_THREADS;
+        const int wide = std::max(L.max_level_rows, U.max_level_rows);
+        int cw = std::max(1, std::min(16, (wide + 31) / 32));
+        if (trsv_tuning().lu_staged_threads > 0) cw = std::min(16, trsv_tuning().lu_staged_threads / 32);
         k_lu_staged<VT, FT, DT><<<1, thr, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
                                                                   U.args<FT>(), U.lstart.p, U.lub.p, U.nlub, dinv, x,
-                                                                  z, done_flag);
+                                                                  z, done_flag, cw);
         return;
     }
     static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
