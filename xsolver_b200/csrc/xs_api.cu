@@ -147,6 +147,14 @@ TrsvTuning &trsv_tuning()
         if (const char *e = getenv("XS_SWEEP_FUSE")) t.fuse_sweeps = atoi(e) != 0;
         if (const char *e = getenv("XS_LU_STAGED")) t.lu_staged = atoi(e) != 0;
         if (const char *e = getenv("XS_SWEEP_BALANCED")) t.balanced_sweep_grid = atoi(e) != 0;
+        if (const char *e = getenv("XS_LU_BATCH")) {  // "rows,entries,buffers"
+            int r = 0, en = 0, b = 0;
+            if (sscanf(e, "%d,%d,%d", &r, &en, &b) == 3 && r >= 32 && en >= 32 && b >= 2 && b <= LUB_MAX_BUFS) {
+                t.lub_rows = r;
+                t.lub_entries = en;
+                t.lub_bufs = b;
+            }
+        }
         if (const char *e = getenv("XS_LU_STAGED_THREADS")) {
             const int v = atoi(e);
             t.lu_staged_threads = v >= 32 && v <= LU_BLOCK_THREADS && v % 32 == 0 ? v : 0;

@@ -38,10 +38,10 @@ namespace xs {
 constexpr int TRSV_THREADS = 128;
 constexpr int TRSV_CHUNK = 8;
 // single-CTA LU solve: the solution vector in shared memory (at most this
-// many bytes); the staged form also holds two level batches of at most
-// LUB_ROWS rows and LUB_ENTRIES entries
+// many bytes); the staged form also holds up to LUB_MAX_BUFS level batches
+// (sizes in TrsvTuning), all within LU_SMEM_LIMIT
 constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
-constexpr int LUB_ROWS = 512, LUB_ENTRIES = 2048;
+constexpr int LUB_MAX_BUFS = 4;
 constexpr size_t LU_SMEM_LIMIT = 227 * 1024;
 
 template <typename FT>
@@ -104,6 +104,9 @@ struct TrsvTuning {
     // walker threads of the staged single-CTA solve (multiple of 32, at most
     // 512; 0: the widest level's rows rounded to whole warps)
     int lu_staged_threads = 0;
+    // its level batches: at most lub_rows rows and lub_entries entries, in
+    // lub_bufs shared-memory buffers (copied up to lub_bufs - 1 batches ahead)
+    int lub_rows = 512, lub_entries = 2048, lub_bufs = 2;
     // Jacobi-sweep passes on a grid whose CTAs all take the same number of
     // row blocks (1) or on one full wave of CTAs (0)
     int balanced_sweep_grid = 0;
@@ -859,7 +862,7 @@ struct TriDev {
     // memory slots); lvperm keeps the dependency-level order for the
     // factorisation kernels, which take rows in level order
     // single-CTA staged solve (small systems): consecutive whole levels in
-    // batches of at most LUB_ROWS rows and LUB_ENTRIES entries; lub[b] is
+    // batches of at most TrsvTuning::lub_rows rows and lub_entries entries; lub[b] is
     // batch b's first level (nlub + 1 values), or -1 - level for a level too
     // large to stage (solved from global memory)
     int nlub = 0;
@@ -1081,7 +1084,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
                 while (l1 < P.nlevels) {
                     const int r = P.lstart[l1 + 1] - P.lstart[l1];
                     const long e = (long)P.prp[P.lstart[l1 + 1]] - P.prp[P.lstart[l1]];
-                    if (rows + r > LUB_ROWS || ents + e > LUB_ENTRIES) break;
+                    if (rows + r > trsv_tuning().lub_rows || ents + e > trsv_tuning().lub_entries) break;
                     rows += r;
                     ents += e;
                     l1++;
@@ -1297,14 +1300,23 @@ __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_block(TrsvArgs<FT> L, c
 // The solution vector starts as x (its own slot is a row's right-hand side
 // in the L phase) and is overwritten level by level; row arithmetic and
 // entry order are those of trsv_row, so results are bitwise the same.
+// one batch buffer: rows (R), entry offsets (R+1), U's dinv (R), columns
+// (E) and values (E, plus the 4-byte rounding of the copied value range)
 template <typename FT, typename DT>
 struct LuBatchSmem {
-    static constexpr size_t row = 0;
-    static constexpr size_t eptr = row + ((LUB_ROWS * sizeof(int) + 15) & ~(size_t)15);
-    static constexpr size_t in = eptr + (((LUB_ROWS + 1) * sizeof(int) + 15) & ~(size_t)15);
-    static constexpr size_t pci = in + ((LUB_ROWS * sizeof(DT) + 15) & ~(size_t)15);
-    static constexpr size_t pv = pci + ((LUB_ENTRIES * sizeof(int) + 15) & ~(size_t)15);
-    static constexpr size_t bytes = pv + ((LUB_ENTRIES * sizeof(FT) + 8 + 15) & ~(size_t)15);
+    size_t row, eptr, in, pci, pv, bytes;
+    static __host__ __device__ LuBatchSmem of(int R, int E)
+    {
+        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+        LuBatchSmem m;
+        m.row = 0;
+        m.eptr = m.row + al((size_t)R * sizeof(int));
+        m.in = m.eptr + al((size_t)(R + 1) * sizeof(int));
+        m.pci = m.in + al((size_t)R * sizeof(DT));
+        m.pv = m.pci + al((size_t)E * sizeof(int));
+        m.bytes = m.pv + al((size_t)E * sizeof(FT) + 8);
+        return m;
+    }
 };
 
 __device__ __forceinline__ void named_sync(int id, int count)
@@ -1328,41 +1340,39 @@ __device__ __forceinline__ int lub_first_level(const int *__restrict__ lub, int 
 template <typename FT, typename DT, bool UPPER>
 __device__ __forceinline__ void lu_stage_batch(const TrsvArgs<FT> &P, const int *__restrict__ ls,
                                                const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
-                                               unsigned char *buf, int tid, int T)
+                                               unsigned char *buf, const LuBatchSmem<FT, DT> &B, int tid, int T)
 {
-    using B = LuBatchSmem<FT, DT>;
     if (__ldg(lub + b) < 0) return;
     const int pa = __ldg(ls + lub_first_level(lub, b)), pb = __ldg(ls + lub_first_level(lub, b + 1));
     const int ea = __ldg(P.prp + pa), eb = __ldg(P.prp + pb);
-    int *s_row = (int *)(buf + B::row), *s_eptr = (int *)(buf + B::eptr), *s_pci = (int *)(buf + B::pci);
+    int *s_row = (int *)(buf + B.row), *s_eptr = (int *)(buf + B.eptr), *s_pci = (int *)(buf + B.pci);
     for (int i = tid; i < pb - pa; i += T) cp_async4(s_row + i, P.perm + pa + i);
     for (int i = tid; i <= pb - pa; i += T) cp_async4(s_eptr + i, P.prp + pa + i);
     for (int i = tid; i < eb - ea; i += T) cp_async4(s_pci + i, P.pci + ea + i);
     const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L, vb1 = ((long)eb * (long)sizeof(FT) + 3) & ~3L;
     const unsigned char *vsrc = (const unsigned char *)P.pv;
-    for (long w = tid; w < (vb1 - vb0) / 4; w += T) cp_async4(buf + B::pv + 4 * w, vsrc + vb0 + 4 * w);
+    for (long w = tid; w < (vb1 - vb0) / 4; w += T) cp_async4(buf + B.pv + 4 * w, vsrc + vb0 + 4 * w);
     if (UPPER)
-        for (int i = tid; i < pb - pa; i += T) cp_async_n<sizeof(DT)>((DT *)(buf + B::in) + i, dinv + pa + i);
+        for (int i = tid; i < pb - pa; i += T) cp_async_n<sizeof(DT)>((DT *)(buf + B.in) + i, dinv + pa + i);
 }
 
 // the levels of batch b by threads tid of T (a barrier of those T threads,
-// id LU_LEVEL_BAR, after each level)
-constexpr int LU_LEVEL_BAR = 5;
+// id level_bar, after each level)
 template <typename VT, typename FT, typename DT, bool UPPER>
 __device__ __forceinline__ void lu_batch_levels(const TrsvArgs<FT> &P, const int *__restrict__ ls,
                                                 const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
-                                                VT *ys, const unsigned char *buf, int tid, int T)
+                                                VT *ys, const unsigned char *buf, const LuBatchSmem<FT, DT> &B, int tid,
+                                                int T, int level_bar)
 {
-    using B = LuBatchSmem<FT, DT>;
     const int lb = __ldg(lub + b);
     if (lb >= 0) {
         const int l0 = lb, l1 = lub_first_level(lub, b + 1);
         const int pa = __ldg(ls + l0), ea = __ldg(P.prp + pa);
         const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L;
-        const int *s_row = (const int *)(buf + B::row), *s_eptr = (const int *)(buf + B::eptr);
-        const int *s_pci = (const int *)(buf + B::pci);
-        const DT *s_in = (const DT *)(buf + B::in);
-        const FT *pv = (const FT *)(buf + B::pv + ((long)ea * (long)sizeof(FT) - vb0));
+        const int *s_row = (const int *)(buf + B.row), *s_eptr = (const int *)(buf + B.eptr);
+        const int *s_pci = (const int *)(buf + B.pci);
+        const DT *s_in = (const DT *)(buf + B.in);
+        const FT *pv = (const FT *)(buf + B.pv + ((long)ea * (long)sizeof(FT) - vb0));
         for (int l = l0; l < l1; l++) {
             const int q0 = __ldg(ls + l) - pa, q1 = __ldg(ls + l + 1) - pa;
             for (int i = q0 + tid; i < q1; i += T) {
@@ -1372,7 +1382,7 @@ __device__ __forceinline__ void lu_batch_levels(const TrsvArgs<FT> &P, const int
                 for (int k = s_eptr[i] - ea; k < k1; k++) acc = msub(acc, ys[s_pci[k]], (VT)FVal<FT>::cvt(pv[k]));
                 ys[row] = acc;
             }
-            named_sync(LU_LEVEL_BAR, T);
+            named_sync(level_bar, T);
         }
     } else {  // one level too large to stage: its rows from global memory
         const int l = -1 - lb;
@@ -1383,51 +1393,57 @@ __device__ __forceinline__ void lu_batch_levels(const TrsvArgs<FT> &P, const int
                 acc = msub(acc, ys[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
             ys[row] = acc;
         }
-        named_sync(LU_LEVEL_BAR, T);
+        named_sync(level_bar, T);
     }
 }
 
 // Warp-specialised: the first cw warps walk the levels (a barrier of those
 // warps only between levels), the other warps copy the batches, L's then
-// U's, into two buffers one batch ahead; named barriers 1-2 ("batch in
-// buffer k landed": the copiers arrive, the walkers wait) and 3-4 ("buffer
-// k free": the walkers arrive, the copiers wait before reusing it) hand the
-// buffers over.
+// U's, into nbuf buffers up to nbuf - 1 batches ahead; named barriers
+// 1..nbuf ("batch in buffer k landed": the copiers arrive, the walkers wait)
+// and nbuf+1..2*nbuf ("buffer k free": the walkers arrive, the copiers wait
+// before reusing it) hand the buffers over; barrier 2*nbuf+1 is the walkers'.
 template <typename VT, typename FT, typename DT>
 __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_staged(TrsvArgs<FT> L, const int *__restrict__ lstart,
                                                                  const int *__restrict__ lubL, int nbL, TrsvArgs<FT> U,
                                                                  const int *__restrict__ ustart,
                                                                  const int *__restrict__ lubU, int nbU,
                                                                  const DT *__restrict__ dinv, const VT *__restrict__ x,
-                                                                 VT *__restrict__ z, const int *done_flag, int cw)
+                                                                 VT *__restrict__ z, const int *done_flag, int cw,
+                                                                 int brows, int bents, int nbuf)
 {
     extern __shared__ __align__(16) unsigned char lus_smem[];
     if (done_flag && *done_flag) return;
-    using B = LuBatchSmem<FT, DT>;
+    const LuBatchSmem<FT, DT> B = LuBatchSmem<FT, DT>::of(brows, bents);
     const size_t yb = ((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15;
     VT *ys = (VT *)lus_smem;
-    unsigned char *bufs[2] = {lus_smem + yb, lus_smem + yb + B::bytes};
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) ys[i] = x[i];
     __syncthreads();
     const int all = blockDim.x, ct = cw * 32, nb = nbL + nbU;
+    const int level_bar = 2 * nbuf + 1;
     if ((int)threadIdx.x >= ct) {  // copiers
         const int tid = threadIdx.x - ct, T = all - ct;
         for (int g = 0; g < nb; g++) {
-            const int k = g & 1;
-            if (g >= 2) named_sync(3 + k, all);  // the walkers are done with batch g - 2
-            if (g < nbL) lu_stage_batch<FT, DT, false>(L, lstart, lubL, g, nullptr, bufs[k], tid, T);
-            else lu_stage_batch<FT, DT, true>(U, ustart, lubU, g - nbL, dinv, bufs[k], tid, T);
+            const int k = g % nbuf;
+            unsigned char *buf = lus_smem + yb + (size_t)k * B.bytes;
+            if (g >= nbuf) named_sync(1 + nbuf + k, all);  // the walkers are done with batch g - nbuf
+            if (g < nbL) lu_stage_batch<FT, DT, false>(L, lstart, lubL, g, nullptr, buf, B, tid, T);
+            else lu_stage_batch<FT, DT, true>(U, ustart, lubU, g - nbL, dinv, buf, B, tid, T);
             cp_async_commit();
             cp_async_wait<0>();
             named_arrive(1 + k, all);
         }
     } else {  // walkers
         for (int g = 0; g < nb; g++) {
-            const int k = g & 1;
+            const int k = g % nbuf;
+            const unsigned char *buf = lus_smem + yb + (size_t)k * B.bytes;
             named_sync(1 + k, all);  // batch g landed
-            if (g < nbL) lu_batch_levels<VT, FT, DT, false>(L, lstart, lubL, g, nullptr, ys, bufs[k], threadIdx.x, ct);
-            else lu_batch_levels<VT, FT, DT, true>(U, ustart, lubU, g - nbL, dinv, ys, bufs[k], threadIdx.x, ct);
-            if (g + 2 < nb) named_arrive(3 + k, all);  // buffer k free for batch g + 2
+            if (g < nbL)
+                lu_batch_levels<VT, FT, DT, false>(L, lstart, lubL, g, nullptr, ys, buf, B, threadIdx.x, ct, level_bar);
+            else
+                lu_batch_levels<VT, FT, DT, true>(U, ustart, lubU, g - nbL, dinv, ys, buf, B, threadIdx.x, ct,
+                                                  level_bar);
+            if (g + nbuf < nb) named_arrive(1 + nbuf + k, all);  // buffer k free for batch g + nbuf
         }
     }
     __syncthreads();
@@ -1449,7 +1465,9 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
 {
     // the staged form when both triangles have level batches and the
     // solution vector plus two batches fit in shared memory
-    const size_t ssm = (((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15) + 2 * LuBatchSmem<FT, DT>::bytes;
+    const TrsvTuning &tu = trsv_tuning();
+    const size_t ssm = (((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15) +
+                       (size_t)tu.lub_bufs * LuBatchSmem<FT, DT>::of(tu.lub_rows, tu.lub_entries).bytes;
     if (L.nlub > 0 && U.nlub > 0 && ssm <= LU_SMEM_LIMIT && trsv_tuning().lu_staged) {
         static size_t sattr = 0;
         if (ssm > sattr) {
@@ -1465,7 +1483,8 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
         if (trsv_tuning().lu_staged_threads > 0) cw = std::min(16, trsv_tuning().lu_staged_threads / 32);
         k_lu_staged<VT, FT, DT><<<1, thr, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
                                                                   U.args<FT>(), U.lstart.p, U.lub.p, U.nlub, dinv, x,
-                                                                  z, done_flag, cw);
+                                                                  z, done_flag, cw, tu.lub_rows, tu.lub_entries,
+                                                                  tu.lub_bufs);
         return;
     }
     static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
