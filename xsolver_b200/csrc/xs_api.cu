@@ -153,6 +153,7 @@ TrsvTuning &trsv_tuning()
                 t.lub_rows = r;
                 t.lub_entries = en;
                 t.lub_bufs = b;
+                t.lub_auto = 0;
             }
         }
         if (const char *e = getenv("XS_LU_STAGED_THREADS")) {

@@ -44,6 +44,25 @@ constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
 constexpr int LUB_MAX_BUFS = 4;
 constexpr size_t LU_SMEM_LIMIT = 227 * 1024;
 
+// one batch buffer: rows (R), entry offsets (R+1), U's dinv (R), columns
+// (E) and values (E, plus the 4-byte rounding of the copied value range)
+template <typename FT, typename DT>
+struct LuBatchSmem {
+    size_t row, eptr, in, pci, pv, bytes;
+    static __host__ __device__ LuBatchSmem of(int R, int E)
+    {
+        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+        LuBatchSmem m;
+        m.row = 0;
+        m.eptr = m.row + al((size_t)R * sizeof(int));
+        m.in = m.eptr + al((size_t)(R + 1) * sizeof(int));
+        m.pci = m.in + al((size_t)R * sizeof(DT));
+        m.pv = m.pci + al((size_t)E * sizeof(int));
+        m.bytes = m.pv + al((size_t)E * sizeof(FT) + 8);
+        return m;
+    }
+};
+
 template <typename FT>
 struct TrsvArgs {
     int n;
@@ -105,8 +124,12 @@ struct TrsvTuning {
     // 512; 0: the widest level's rows rounded to whole warps)
     int lu_staged_threads = 0;
     // its level batches: at most lub_rows rows and lub_entries entries, in
-    // lub_bufs shared-memory buffers (copied up to lub_bufs - 1 batches ahead)
-    int lub_rows = 512, lub_entries = 2048, lub_bufs = 2;
+    // lub_bufs shared-memory buffers (copied up to lub_bufs - 1 batches
+    // ahead); lub_auto sizes two buffers to fill the shared memory the
+    // solution vector leaves (fewer, larger batches measured faster: 2D
+    // 128^2 231 us with 768-row batches against 234 at 512 and 260-311 with
+    // 3-4 smaller buffers)
+    int lub_rows = 512, lub_entries = 2048, lub_bufs = 2, lub_auto = 1;
     // Jacobi-sweep passes on a grid whose CTAs all take the same number of
     // row blocks (1) or on one full wave of CTAs (0)
     int balanced_sweep_grid = 0;
@@ -866,6 +889,7 @@ struct TriDev {
     // batch b's first level (nlub + 1 values), or -1 - level for a level too
     // large to stage (solved from global memory)
     int nlub = 0;
+    int lub_rows = 0, lub_entries = 0;  // batch limits the list was built with
     int max_level_rows = 0;  // widest dependency level (level layout)
     DBuf<int> lub;
     bool tiled = false;
@@ -1075,6 +1099,21 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         T.nlub = 0;
         T.lub.free();
         if ((size_t)n * sizeof(double) <= LU_BLOCK_SMEM_MAX) {
+            const TrsvTuning &tu = trsv_tuning();
+            int brows = tu.lub_rows, bents = tu.lub_entries;
+            if (tu.lub_auto) {
+                // two buffers in what the FP64 solution vector leaves
+                const size_t ysb = ((size_t)n * sizeof(double) + 15) & ~(size_t)15;
+                const double epr = std::max(1.0, (double)T.nnz / std::max(n, 1));
+                brows = (int)((double)((LU_SMEM_LIMIT - ysb) / 2) / (16.0 + 12.0 * epr));
+                for (; brows > 32; brows -= 16) {
+                    bents = (int)std::ceil(brows * epr) + 32;
+                    if (ysb + 2 * LuBatchSmem<double, double>::of(brows, bents).bytes <= LU_SMEM_LIMIT) break;
+                }
+                brows = std::max(brows, 32);
+            }
+            T.lub_rows = brows;
+            T.lub_entries = bents;
             std::vector<int> b;
             int l = 0;
             while (l < P.nlevels) {
@@ -1084,7 +1123,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
                 while (l1 < P.nlevels) {
                     const int r = P.lstart[l1 + 1] - P.lstart[l1];
                     const long e = (long)P.prp[P.lstart[l1 + 1]] - P.prp[P.lstart[l1]];
-                    if (rows + r > trsv_tuning().lub_rows || ents + e > trsv_tuning().lub_entries) break;
+                    if (rows + r > brows || ents + e > bents) break;
                     rows += r;
                     ents += e;
                     l1++;
@@ -1300,24 +1339,6 @@ __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_block(TrsvArgs<FT> L, c
 // The solution vector starts as x (its own slot is a row's right-hand side
 // in the L phase) and is overwritten level by level; row arithmetic and
 // entry order are those of trsv_row, so results are bitwise the same.
-// one batch buffer: rows (R), entry offsets (R+1), U's dinv (R), columns
-// (E) and values (E, plus the 4-byte rounding of the copied value range)
-template <typename FT, typename DT>
-struct LuBatchSmem {
-    size_t row, eptr, in, pci, pv, bytes;
-    static __host__ __device__ LuBatchSmem of(int R, int E)
-    {
-        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
-        LuBatchSmem m;
-        m.row = 0;
-        m.eptr = m.row + al((size_t)R * sizeof(int));
-        m.in = m.eptr + al((size_t)(R + 1) * sizeof(int));
-        m.pci = m.in + al((size_t)R * sizeof(DT));
-        m.pv = m.pci + al((size_t)E * sizeof(int));
-        m.bytes = m.pv + al((size_t)E * sizeof(FT) + 8);
-        return m;
-    }
-};
 
 __device__ __forceinline__ void named_sync(int id, int count)
 {
@@ -1466,8 +1487,10 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
     // the staged form when both triangles have level batches and the
     // solution vector plus two batches fit in shared memory
     const TrsvTuning &tu = trsv_tuning();
+    const int brows = std::max(L.lub_rows, U.lub_rows), bents = std::max(L.lub_entries, U.lub_entries);
+    const int nbuf = tu.lub_auto ? 2 : tu.lub_bufs;
     const size_t ssm = (((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15) +
-                       (size_t)tu.lub_bufs * LuBatchSmem<FT, DT>::of(tu.lub_rows, tu.lub_entries).bytes;
+                       (size_t)nbuf * LuBatchSmem<FT, DT>::of(brows, bents).bytes;
     if (L.nlub > 0 && U.nlub > 0 && ssm <= LU_SMEM_LIMIT && trsv_tuning().lu_staged) {
         static size_t sattr = 0;
         if (ssm > sattr) {
@@ -1483,8 +1506,7 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
         if (trsv_tuning().lu_staged_threads > 0) cw = std::min(16, trsv_tuning().lu_staged_threads / 32);
         k_lu_staged<VT, FT, DT><<<1, thr, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
                                                                   U.args<FT>(), U.lstart.p, U.lub.p, U.nlub, dinv, x,
-                                                                  z, done_flag, cw, tu.lub_rows, tu.lub_entries,
-                                                                  tu.lub_bufs);
+                                                                  z, done_flag, cw, brows, bents, nbuf);
         return;
     }
     static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
