@@ -147,17 +147,18 @@ TrsvTuning &trsv_tuning()
         if (const char *e = getenv("XS_SWEEP_FUSE")) t.fuse_sweeps = atoi(e) != 0;
         if (const char *e = getenv("XS_LU_STAGED")) t.lu_staged = atoi(e) != 0;
         if (const char *e = getenv("XS_SWEEP_BALANCED")) t.balanced_sweep_grid = atoi(e) != 0;
-        if (const char *e = getenv("XS_LU_BATCH")) {  // "rows,entries"
-            int r = 0, en = 0;
-            if (sscanf(e, "%d,%d", &r, &en) == 2 && r >= 32 && en >= 32) {
+        if (const char *e = getenv("XS_LU_BATCH")) {  // "rows,entries,buffers"
+            int r = 0, en = 0, b = 0;
+            if (sscanf(e, "%d,%d,%d", &r, &en, &b) == 3 && r >= 32 && en >= 32 && b >= 2 && b <= LUB_MAX_BUFS) {
                 t.lub_rows = r;
                 t.lub_entries = en;
+                t.lub_bufs = b;
                 t.lub_auto = 0;
             }
         }
         if (const char *e = getenv("XS_LU_STAGED_THREADS")) {
             const int v = atoi(e);
-            t.lu_staged_threads = v >= 32 && v <= LU_BLOCK_THREADS && v % 32 == 0 ? v : 0;  // whole warps
+            t.lu_staged_threads = v >= 32 && v <= LU_BLOCK_THREADS && v % 32 == 0 ? v : 0;
         }
         init = true;
     }
@@ -815,11 +816,11 @@ static void load_dinv(Handle &h, const double *vals, const long *diagsrc, bool n
 {
     const int g = geom().sms * 4;
     TriDev &U = h.M.U;
-    if (U.dinv64.n != (size_t)h.n) { U.dinv64.alloc(h.n, 4); U.dinv64_nat.alloc(h.n); }
+    if (U.dinv64.n != (size_t)h.n) { U.dinv64.alloc(h.n); U.dinv64_nat.alloc(h.n); }
     k_gather_dinv<double><<<g, 256, 0, h.s>>>(h.n, U.perm.p, diagsrc, vals, U.dinv64.p);
     k_gather_dinv<double><<<g, 256, 0, h.s>>>(h.n, nullptr, diagsrc, vals, U.dinv64_nat.p);
     if (need32) {
-        if (U.dinv32.n != (size_t)h.n) { U.dinv32.alloc(h.n, 4); U.dinv32_nat.alloc(h.n); }
+        if (U.dinv32.n != (size_t)h.n) { U.dinv32.alloc(h.n); U.dinv32_nat.alloc(h.n); }
         k_gather_dinv<float><<<g, 256, 0, h.s>>>(h.n, U.perm.p, diagsrc, vals, U.dinv32.p);
         k_gather_dinv<float><<<g, 256, 0, h.s>>>(h.n, nullptr, diagsrc, vals, U.dinv32_nat.p);
     }
@@ -1512,7 +1513,7 @@ static void adjoint_prepare(Handle &h)
                 k_gather_convert<double><<<g, 256, 0, h.s>>>(D->nnz, D->src_nat.p, vals, D->nv64.p);
             }
         }
-        T.U.dinv64.alloc(n, 4);
+        T.U.dinv64.alloc(n);
         T.U.dinv64_nat.alloc(n);
         k_gather_dinv<double><<<g, 256, 0, h.s>>>(n, T.U.perm.p, diagsrc, vals, T.U.dinv64.p);
         k_gather_dinv<double><<<g, 256, 0, h.s>>>(n, nullptr, diagsrc, vals, T.U.dinv64_nat.p);

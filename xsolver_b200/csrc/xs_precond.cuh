@@ -127,7 +127,7 @@ struct PrecondDev {
             const VT *dinv;
             if constexpr (std::is_same<VT, double>::value) dinv = U.dinv64.p;
             else dinv = U.dinv32.p;
-            launch_lu_block<VT, FT, VT>(L, U, dinv, x, z, done_flag, err, s);
+            launch_lu_block<VT, FT, VT>(L, U, dinv, x, z, done_flag, s);
             return;
         }
         exact_half<VT, FT>(0, x, z, done_flag, s);

@@ -38,32 +38,27 @@ namespace xs {
 constexpr int TRSV_THREADS = 128;
 constexpr int TRSV_CHUNK = 8;
 // single-CTA LU solve: the solution vector in shared memory (at most this
-// many bytes); the staged form also holds two level batches (sizes in
-// TrsvTuning), all within LU_SMEM_LIMIT
+// many bytes); the staged form also holds up to LUB_MAX_BUFS level batches
+// (sizes in TrsvTuning), all within LU_SMEM_LIMIT
 constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
+constexpr int LUB_MAX_BUFS = 4;
 constexpr size_t LU_SMEM_LIMIT = 227 * 1024;
 
-// one batch buffer, filled by 1-D bulk copies of 16-byte aligned ranges:
-// a header written by the issuing thread (the batch's code, last level + 1,
-// first position, first entry, and the element shift of each copied range
-// inside its region), the level starts (at most R+1), rows (R), entry
-// offsets (R+1), U's dinv (R), columns (E) and values (E); every region has
-// 16 bytes of slack for the rounding of its range
+// one batch buffer: rows (R), entry offsets (R+1), U's dinv (R), columns
+// (E) and values (E, plus the 4-byte rounding of the copied value range)
 template <typename FT, typename DT>
 struct LuBatchSmem {
-    size_t hdr, lvl, row, eptr, in, pci, pv, bytes;
+    size_t row, eptr, in, pci, pv, bytes;
     static __host__ __device__ LuBatchSmem of(int R, int E)
     {
-        auto al = [](size_t b) { return (b + 16 + 15) & ~(size_t)15; };
+        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
         LuBatchSmem m;
-        m.hdr = 0;
-        m.lvl = 64;
-        m.row = m.lvl + al((size_t)(R + 1) * sizeof(int));
+        m.row = 0;
         m.eptr = m.row + al((size_t)R * sizeof(int));
         m.in = m.eptr + al((size_t)(R + 1) * sizeof(int));
         m.pci = m.in + al((size_t)R * sizeof(DT));
         m.pv = m.pci + al((size_t)E * sizeof(int));
-        m.bytes = m.pv + al((size_t)E * sizeof(FT));
+        m.bytes = m.pv + al((size_t)E * sizeof(FT) + 8);
         return m;
     }
 };
@@ -125,15 +120,16 @@ struct TrsvTuning {
     // single-CTA solve with its level batches staged in shared memory (1) or
     // its row data loaded one level ahead from global memory (0)
     int lu_staged = 1;
-    // threads of the staged single-CTA solve (multiple of 32, at most 1024;
-    // 0: the widest level's rows rounded to whole warps, at least 128)
+    // walker threads of the staged single-CTA solve (multiple of 32, at most
+    // 512; 0: the widest level's rows rounded to whole warps)
     int lu_staged_threads = 0;
-    // its level batches: at most lub_rows rows and lub_entries entries in
-    // each of two shared-memory buffers; lub_auto sizes the buffers to fill
-    // the shared memory the solution vector leaves (fewer, larger batches
-    // measured faster: 2D 128^2 231 us with 768-row batches against 234 at
-    // 512, and 260-311 us with 3-4 smaller buffers)
-    int lub_rows = 512, lub_entries = 2048, lub_auto = 1;
+    // its level batches: at most lub_rows rows and lub_entries entries, in
+    // lub_bufs shared-memory buffers (copied up to lub_bufs - 1 batches
+    // ahead); lub_auto sizes two buffers to fill the shared memory the
+    // solution vector leaves (fewer, larger batches measured faster: 2D
+    // 128^2 231 us with 768-row batches against 234 at 512 and 260-311 with
+    // 3-4 smaller buffers)
+    int lub_rows = 512, lub_entries = 2048, lub_bufs = 2, lub_auto = 1;
     // Jacobi-sweep passes on a grid whose CTAs all take the same number of
     // row blocks (1) or on one full wave of CTAs (0)
     int balanced_sweep_grid = 0;
@@ -1089,15 +1085,14 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     } else if (!T.chunked) {
         level_analysis();
         T.nlevels = P.nlevels;
-        // padded: the staged single-CTA solve copies 16-byte aligned ranges
-        T.perm.alloc(n, 4); T.perm.upload(P.perm.data(), n, s);
-        T.prp.alloc(n + 1, 4); T.prp.upload(P.prp.data(), n + 1, s);
-        T.pci.alloc(m, 4);
+        T.perm.alloc(n); T.perm.upload(P.perm.data(), n, s);
+        T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
+        T.pci.alloc(m);
         T.src.alloc(m);
         k_pos_entries<<<g, 256, 0, s>>>(n, upper, T.perm.p, T.prp.p, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, T.pci.p,
                                         T.src.p);
         check_launch();
-        T.lstart.alloc(P.nlevels + 1, 4); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
+        T.lstart.alloc(P.nlevels + 1); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
         T.max_level_rows = 0;
         for (int l = 0; l < P.nlevels; l++) T.max_level_rows = std::max(T.max_level_rows, P.lstart[l + 1] - P.lstart[l]);
         // level batches of the staged single-CTA solve (systems it serves only)
@@ -1345,6 +1340,15 @@ __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_block(TrsvArgs<FT> L, c
 // in the L phase) and is overwritten level by level; row arithmetic and
 // entry order are those of trsv_row, so results are bitwise the same.
 
+__device__ __forceinline__ void named_sync(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int count)
+{
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 // first level of batch b of a triangle's batch list
 __device__ __forceinline__ int lub_first_level(const int *__restrict__ lub, int b)
 {
@@ -1352,85 +1356,57 @@ __device__ __forceinline__ int lub_first_level(const int *__restrict__ lub, int 
     return v < 0 ? -1 - v : v;
 }
 
-// Issue the bulk copies of batch b into buf (one thread): each array range
-// rounded out to 16-byte boundaries (the arrays are allocated with at least
-// 16 bytes of padding), the element shift of the range's start recorded in
-// the header; completion counted on bar.  A batch holding one level too
-// large to stage only arrives on bar.
+// copy batch b (rows, entry offsets, columns, values, U's dinv) into buf;
+// threads tid of T; nothing for a level too large to stage
 template <typename FT, typename DT, bool UPPER>
-__device__ __forceinline__ void lu_issue_batch(const TrsvArgs<FT> &P, const int *__restrict__ ls,
+__device__ __forceinline__ void lu_stage_batch(const TrsvArgs<FT> &P, const int *__restrict__ ls,
                                                const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
-                                               unsigned char *buf, const LuBatchSmem<FT, DT> &B, uint64_t *bar)
+                                               unsigned char *buf, const LuBatchSmem<FT, DT> &B, int tid, int T)
 {
-    int *hdr = (int *)(buf + B.hdr);
-    const int code = __ldg(lub + b);
-    hdr[0] = code;
-    if (code < 0) {
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-        return;
-    }
-    const int l0 = code, l1 = lub_first_level(lub, b + 1);
-    const int pa = __ldg(ls + l0), pb = __ldg(ls + l1);
+    if (__ldg(lub + b) < 0) return;
+    const int pa = __ldg(ls + lub_first_level(lub, b)), pb = __ldg(ls + lub_first_level(lub, b + 1));
     const int ea = __ldg(P.prp + pa), eb = __ldg(P.prp + pb);
-    hdr[1] = l1;
-    hdr[2] = pa;
-    hdr[3] = ea;
-    struct Range {
-        uintptr_t b0, b1;
-        size_t dst;
-    } r[6];
-    int nr = 0;
-    auto plan = [&](const void *base, long first, long count, int esz, size_t dst, int slot) {
-        const uintptr_t a0 = (uintptr_t)base + (uintptr_t)(first * esz);
-        const uintptr_t a1 = a0 + (uintptr_t)(count * esz);
-        const uintptr_t b0 = a0 & ~(uintptr_t)15, b1 = (a1 + 15) & ~(uintptr_t)15;
-        hdr[4 + slot] = (int)((a0 - b0) / (uintptr_t)esz);
-        if (b1 > b0) r[nr++] = Range{b0, b1, dst};
-    };
-    plan(ls, l0, l1 - l0 + 1, 4, B.lvl, 0);
-    plan(P.perm, pa, pb - pa, 4, B.row, 1);
-    plan(P.prp, pa, pb - pa + 1, 4, B.eptr, 2);
-    plan(P.pci, ea, eb - ea, 4, B.pci, 3);
-    plan(P.pv, ea, eb - ea, (int)sizeof(FT), B.pv, 4);
-    if (UPPER) plan(dinv, pa, pb - pa, (int)sizeof(DT), B.in, 5);
-    uint32_t total = 0;
-    for (int q = 0; q < nr; q++) total += (uint32_t)(r[q].b1 - r[q].b0);
-    mbar_expect_tx(bar, total);
-    for (int q = 0; q < nr; q++)
-        bulk_g2s(buf + r[q].dst, (const void *)r[q].b0, (uint32_t)(r[q].b1 - r[q].b0), bar);
+    int *s_row = (int *)(buf + B.row), *s_eptr = (int *)(buf + B.eptr), *s_pci = (int *)(buf + B.pci);
+    for (int i = tid; i < pb - pa; i += T) cp_async4(s_row + i, P.perm + pa + i);
+    for (int i = tid; i <= pb - pa; i += T) cp_async4(s_eptr + i, P.prp + pa + i);
+    for (int i = tid; i < eb - ea; i += T) cp_async4(s_pci + i, P.pci + ea + i);
+    const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L, vb1 = ((long)eb * (long)sizeof(FT) + 3) & ~3L;
+    const unsigned char *vsrc = (const unsigned char *)P.pv;
+    for (long w = tid; w < (vb1 - vb0) / 4; w += T) cp_async4(buf + B.pv + 4 * w, vsrc + vb0 + 4 * w);
+    if (UPPER)
+        for (int i = tid; i < pb - pa; i += T) cp_async_n<sizeof(DT)>((DT *)(buf + B.in) + i, dinv + pa + i);
 }
 
-// the levels of the batch in buf, by all threads of the CTA (a block
-// barrier after each level)
+// the levels of batch b by threads tid of T (a barrier of those T threads,
+// id level_bar, after each level)
 template <typename VT, typename FT, typename DT, bool UPPER>
-__device__ __forceinline__ void lu_walk_batch(const TrsvArgs<FT> &P, const int *__restrict__ ls,
-                                              const DT *__restrict__ dinv, VT *ys, const unsigned char *buf,
-                                              const LuBatchSmem<FT, DT> &B)
+__device__ __forceinline__ void lu_batch_levels(const TrsvArgs<FT> &P, const int *__restrict__ ls,
+                                                const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
+                                                VT *ys, const unsigned char *buf, const LuBatchSmem<FT, DT> &B, int tid,
+                                                int T, int level_bar)
 {
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int *hdr = (const int *)(buf + B.hdr);
-    const int code = hdr[0];
-    if (code >= 0) {
-        const int l0 = code, l1 = hdr[1], pa = hdr[2], ea = hdr[3];
-        const int *s_lvl = (const int *)(buf + B.lvl) + hdr[4];
-        const int *s_row = (const int *)(buf + B.row) + hdr[5];
-        const int *s_eptr = (const int *)(buf + B.eptr) + hdr[6];
-        const int *s_pci = (const int *)(buf + B.pci) + hdr[7];
-        const FT *s_pv = (const FT *)(buf + B.pv) + hdr[8];
-        const DT *s_in = (const DT *)(buf + B.in) + (UPPER ? hdr[9] : 0);
+    const int lb = __ldg(lub + b);
+    if (lb >= 0) {
+        const int l0 = lb, l1 = lub_first_level(lub, b + 1);
+        const int pa = __ldg(ls + l0), ea = __ldg(P.prp + pa);
+        const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L;
+        const int *s_row = (const int *)(buf + B.row), *s_eptr = (const int *)(buf + B.eptr);
+        const int *s_pci = (const int *)(buf + B.pci);
+        const DT *s_in = (const DT *)(buf + B.in);
+        const FT *pv = (const FT *)(buf + B.pv + ((long)ea * (long)sizeof(FT) - vb0));
         for (int l = l0; l < l1; l++) {
-            const int q0 = s_lvl[l - l0] - pa, q1 = s_lvl[l - l0 + 1] - pa;
+            const int q0 = __ldg(ls + l) - pa, q1 = __ldg(ls + l + 1) - pa;
             for (int i = q0 + tid; i < q1; i += T) {
                 const int row = s_row[i];
                 VT acc = UPPER ? (VT)(ys[row] * (VT)s_in[i]) : ys[row];
                 const int k1 = s_eptr[i + 1] - ea;
-                for (int k = s_eptr[i] - ea; k < k1; k++) acc = msub(acc, ys[s_pci[k]], (VT)FVal<FT>::cvt(s_pv[k]));
+                for (int k = s_eptr[i] - ea; k < k1; k++) acc = msub(acc, ys[s_pci[k]], (VT)FVal<FT>::cvt(pv[k]));
                 ys[row] = acc;
             }
-            __syncthreads();
+            named_sync(level_bar, T);
         }
     } else {  // one level too large to stage: its rows from global memory
-        const int l = -1 - code;
+        const int l = -1 - lb;
         for (int p = __ldg(ls + l) + tid; p < __ldg(ls + l + 1); p += T) {
             const int row = __ldg(P.perm + p);
             VT acc = UPPER ? (VT)(ys[row] * (VT)__ldg(dinv + p)) : ys[row];
@@ -1438,64 +1414,60 @@ __device__ __forceinline__ void lu_walk_batch(const TrsvArgs<FT> &P, const int *
                 acc = msub(acc, ys[__ldg(P.pci + k)], (VT)FVal<FT>::ld(P.pv, k));
             ys[row] = acc;
         }
-        __syncthreads();
+        named_sync(level_bar, T);
     }
 }
 
-// Staged single-CTA LU solve: the batches of L then U pass through two
-// shared-memory buffers, each filled by one thread's bulk copies (TMA,
-// completion on the buffer's mbarrier) one batch ahead of the walk; all
-// threads walk the levels with a block barrier between levels.  A waiting
-// thread gives up after a bounded time (DEV_TMA_TIMEOUT) and the CTA returns
-// once every thread has seen the outcome.
+// Warp-specialised: the first cw warps walk the levels (a barrier of those
+// warps only between levels), the other warps copy the batches, L's then
+// U's, into nbuf buffers up to nbuf - 1 batches ahead; named barriers
+// 1..nbuf ("batch in buffer k landed": the copiers arrive, the walkers wait)
+// and nbuf+1..2*nbuf ("buffer k free": the walkers arrive, the copiers wait
+// before reusing it) hand the buffers over; barrier 2*nbuf+1 is the walkers'.
 template <typename VT, typename FT, typename DT>
 __global__ void __launch_bounds__(LU_BLOCK_THREADS) k_lu_staged(TrsvArgs<FT> L, const int *__restrict__ lstart,
                                                                  const int *__restrict__ lubL, int nbL, TrsvArgs<FT> U,
                                                                  const int *__restrict__ ustart,
                                                                  const int *__restrict__ lubU, int nbU,
                                                                  const DT *__restrict__ dinv, const VT *__restrict__ x,
-                                                                 VT *__restrict__ z, const int *done_flag, int brows,
-                                                                 int bents, int *err)
+                                                                 VT *__restrict__ z, const int *done_flag, int cw,
+                                                                 int brows, int bents, int nbuf)
 {
     extern __shared__ __align__(16) unsigned char lus_smem[];
-    __shared__ __align__(8) uint64_t bars[2];
     if (done_flag && *done_flag) return;
     const LuBatchSmem<FT, DT> B = LuBatchSmem<FT, DT>::of(brows, bents);
     const size_t yb = ((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15;
     VT *ys = (VT *)lus_smem;
-    unsigned char *bufs[2] = {lus_smem + yb, lus_smem + yb + B.bytes};
-    const int nb = nbL + nbU;
-    auto issue = [&](int g) {
-        const int k = g & 1;
-        if (g < nbL) lu_issue_batch<FT, DT, false>(L, lstart, lubL, g, nullptr, bufs[k], B, &bars[k]);
-        else lu_issue_batch<FT, DT, true>(U, ustart, lubU, g - nbL, dinv, bufs[k], B, &bars[k]);
-    };
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        fence_mbar_init();
-    }
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) ys[i] = x[i];
     __syncthreads();
-    if (threadIdx.x == 0 && nb > 0) issue(0);
-    for (int g = 0; g < nb; g++) {
-        const int k = g & 1;
-        // every thread is past the walk of batch g - 1, whose buffer the
-        // copy of batch g + 1 overwrites
-        if (threadIdx.x == 0 && g + 1 < nb) {
-            fence_proxy_async();
-            issue(g + 1);
+    const int all = blockDim.x, ct = cw * 32, nb = nbL + nbU;
+    const int level_bar = 2 * nbuf + 1;
+    if ((int)threadIdx.x >= ct) {  // copiers
+        const int tid = threadIdx.x - ct, T = all - ct;
+        for (int g = 0; g < nb; g++) {
+            const int k = g % nbuf;
+            unsigned char *buf = lus_smem + yb + (size_t)k * B.bytes;
+            if (g >= nbuf) named_sync(1 + nbuf + k, all);  // the walkers are done with batch g - nbuf
+            if (g < nbL) lu_stage_batch<FT, DT, false>(L, lstart, lubL, g, nullptr, buf, B, tid, T);
+            else lu_stage_batch<FT, DT, true>(U, ustart, lubU, g - nbL, dinv, buf, B, tid, T);
+            cp_async_commit();
+            cp_async_wait<0>();
+            named_arrive(1 + k, all);
         }
-        const bool landed = mbar_wait_bounded(&bars[k], (uint32_t)((g >> 1) & 1), err);
-        if (!__syncthreads_and(landed)) {
-            // give the copy of batch g + 1 its bounded time to land before
-            // the shared memory goes away
-            if (threadIdx.x == 0 && g + 1 < nb) mbar_wait_bounded(&bars[k ^ 1], (uint32_t)(((g + 1) >> 1) & 1), err);
-            return;
+    } else {  // walkers
+        for (int g = 0; g < nb; g++) {
+            const int k = g % nbuf;
+            const unsigned char *buf = lus_smem + yb + (size_t)k * B.bytes;
+            named_sync(1 + k, all);  // batch g landed
+            if (g < nbL)
+                lu_batch_levels<VT, FT, DT, false>(L, lstart, lubL, g, nullptr, ys, buf, B, threadIdx.x, ct, level_bar);
+            else
+                lu_batch_levels<VT, FT, DT, true>(U, ustart, lubU, g - nbL, dinv, ys, buf, B, threadIdx.x, ct,
+                                                  level_bar);
+            if (g + nbuf < nb) named_arrive(1 + nbuf + k, all);  // buffer k free for batch g + nbuf
         }
-        if (g < nbL) lu_walk_batch<VT, FT, DT, false>(L, lstart, nullptr, ys, bufs[k], B);
-        else lu_walk_batch<VT, FT, DT, true>(U, ustart, dinv, ys, bufs[k], B);
     }
+    __syncthreads();
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) z[i] = ys[i];
 }
 
@@ -1510,12 +1482,15 @@ inline bool lu_block_ok(const TriDev &L, const TriDev &U)
 
 template <typename VT, typename FT, typename DT>
 inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, const VT *x, VT *z, const int *done_flag,
-                            int *err, cudaStream_t s)
+                            cudaStream_t s)
 {
     // the staged form when both triangles have level batches and the
-    // solution vector plus two batch buffers fit in shared memory
+    // solution vector plus two batches fit in shared memory
+    const TrsvTuning &tu = trsv_tuning();
     const int brows = std::max(L.lub_rows, U.lub_rows), bents = std::max(L.lub_entries, U.lub_entries);
-    const size_t ssm = (((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15) + 2 * LuBatchSmem<FT, DT>::of(brows, bents).bytes;
+    const int nbuf = tu.lub_auto ? 2 : tu.lub_bufs;
+    const size_t ssm = (((size_t)L.n * sizeof(VT) + 15) & ~(size_t)15) +
+                       (size_t)nbuf * LuBatchSmem<FT, DT>::of(brows, bents).bytes;
     if (L.nlub > 0 && U.nlub > 0 && ssm <= LU_SMEM_LIMIT && trsv_tuning().lu_staged) {
         static size_t sattr = 0;
         if (ssm > sattr) {
@@ -1523,14 +1498,15 @@ inline void launch_lu_block(const TriDev &L, const TriDev &U, const DT *dinv, co
                                          (int)ssm));
             sattr = ssm;
         }
-        // threads: the widest level's rows in whole warps (at least 4 warps),
-        // so a level takes one pass and its barrier waits for few warps
+        // 1024 threads: walker warps for the widest level's rows (at most 16),
+        // the rest copy
+        const int thr = LU_BLOCK_THREADS;
         const int wide = std::max(L.max_level_rows, U.max_level_rows);
-        int thr = std::min(LU_BLOCK_THREADS, std::max(128, (wide + 31) / 32 * 32));
-        if (trsv_tuning().lu_staged_threads > 0) thr = trsv_tuning().lu_staged_threads;
-        k_lu_staged<VT, FT, DT><<<1, thr, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub, U.args<FT>(),
-                                                    U.lstart.p, U.lub.p, U.nlub, dinv, x, z, done_flag, brows, bents,
-                                                    err);
+        int cw = std::max(1, std::min(16, (wide + 31) / 32));
+        if (trsv_tuning().lu_staged_threads > 0) cw = std::min(16, trsv_tuning().lu_staged_threads / 32);
+        k_lu_staged<VT, FT, DT><<<1, thr, ssm, s>>>(L.args<FT>(), L.lstart.p, L.lub.p, L.nlub,
+                                                                  U.args<FT>(), U.lstart.p, U.lub.p, U.nlub, dinv, x,
+                                                                  z, done_flag, cw, brows, bents, nbuf);
         return;
     }
     static size_t attr = 0;  // largest dynamic shared memory enabled so far for this instantiation
