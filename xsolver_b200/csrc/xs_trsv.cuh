@@ -44,16 +44,20 @@ constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
 constexpr int LUB_MAX_BUFS = 4;
 constexpr size_t LU_SMEM_LIMIT = 227 * 1024;
 
-// one batch buffer: rows (R), entry offsets (R+1), U's dinv (R), columns
-// (E) and values (E, plus the 4-byte rounding of the copied value range)
+// one batch buffer: a header (the batch's code, last level + 1, first
+// position, first entry), its level starts (at most R+1), rows (R), entry
+// offsets (R+1), U's dinv (R), columns (E) and values (E, plus the 4-byte
+// rounding of the copied value range)
 template <typename FT, typename DT>
 struct LuBatchSmem {
-    size_t row, eptr, in, pci, pv, bytes;
+    size_t hdr, lvl, row, eptr, in, pci, pv, bytes;
     static __host__ __device__ LuBatchSmem of(int R, int E)
     {
         auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
         LuBatchSmem m;
-        m.row = 0;
+        m.hdr = 0;
+        m.lvl = 16;
+        m.row = m.lvl + al((size_t)(R + 1) * sizeof(int));
         m.eptr = m.row + al((size_t)R * sizeof(int));
         m.in = m.eptr + al((size_t)(R + 1) * sizeof(int));
         m.pci = m.in + al((size_t)R * sizeof(DT));
@@ -1363,9 +1367,23 @@ __device__ __forceinline__ void lu_stage_batch(const TrsvArgs<FT> &P, const int 
                                                const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
                                                unsigned char *buf, const LuBatchSmem<FT, DT> &B, int tid, int T)
 {
-    if (__ldg(lub + b) < 0) return;
-    const int pa = __ldg(ls + lub_first_level(lub, b)), pb = __ldg(ls + lub_first_level(lub, b + 1));
+    int *hdr = (int *)(buf + B.hdr);
+    const int code = __ldg(lub + b);
+    if (code < 0) {
+        if (tid == 0) hdr[0] = code;
+        return;
+    }
+    const int l0 = code, l1 = lub_first_level(lub, b + 1);
+    const int pa = __ldg(ls + l0), pb = __ldg(ls + l1);
     const int ea = __ldg(P.prp + pa), eb = __ldg(P.prp + pb);
+    if (tid == 0) {
+        hdr[0] = l0;
+        hdr[1] = l1;
+        hdr[2] = pa;
+        hdr[3] = ea;
+    }
+    int *s_lvl = (int *)(buf + B.lvl);
+    for (int i = tid; i <= l1 - l0; i += T) cp_async4(s_lvl + i, ls + l0 + i);
     int *s_row = (int *)(buf + B.row), *s_eptr = (int *)(buf + B.eptr), *s_pci = (int *)(buf + B.pci);
     for (int i = tid; i < pb - pa; i += T) cp_async4(s_row + i, P.perm + pa + i);
     for (int i = tid; i <= pb - pa; i += T) cp_async4(s_eptr + i, P.prp + pa + i);
@@ -1385,17 +1403,20 @@ __device__ __forceinline__ void lu_batch_levels(const TrsvArgs<FT> &P, const int
                                                 VT *ys, const unsigned char *buf, const LuBatchSmem<FT, DT> &B, int tid,
                                                 int T, int level_bar)
 {
-    const int lb = __ldg(lub + b);
+    // the batch's header and level starts come from shared memory (the
+    // copiers wrote them), so a level step touches shared memory only
+    const int *hdr = (const int *)(buf + B.hdr);
+    const int lb = hdr[0];
     if (lb >= 0) {
-        const int l0 = lb, l1 = lub_first_level(lub, b + 1);
-        const int pa = __ldg(ls + l0), ea = __ldg(P.prp + pa);
+        const int l0 = lb, l1 = hdr[1], pa = hdr[2], ea = hdr[3];
         const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L;
+        const int *s_lvl = (const int *)(buf + B.lvl);
         const int *s_row = (const int *)(buf + B.row), *s_eptr = (const int *)(buf + B.eptr);
         const int *s_pci = (const int *)(buf + B.pci);
         const DT *s_in = (const DT *)(buf + B.in);
         const FT *pv = (const FT *)(buf + B.pv + ((long)ea * (long)sizeof(FT) - vb0));
         for (int l = l0; l < l1; l++) {
-            const int q0 = __ldg(ls + l) - pa, q1 = __ldg(ls + l + 1) - pa;
+            const int q0 = s_lvl[l - l0] - pa, q1 = s_lvl[l - l0 + 1] - pa;
             for (int i = q0 + tid; i < q1; i += T) {
                 const int row = s_row[i];
                 VT acc = UPPER ? (VT)(ys[row] * (VT)s_in[i]) : ys[row];
