@@ -816,11 +816,11 @@ static void load_dinv(Handle &h, const double *vals, const long *diagsrc, bool n
 {
     const int g = geom().sms * 4;
     TriDev &U = h.M.U;
-    if (U.dinv64.n != (size_t)h.n) { U.dinv64.alloc(h.n); U.dinv64_nat.alloc(h.n); }
+    if (U.dinv64.n != (size_t)h.n) { U.dinv64.alloc(h.n, 4); U.dinv64_nat.alloc(h.n); }
     k_gather_dinv<double><<<g, 256, 0, h.s>>>(h.n, U.perm.p, diagsrc, vals, U.dinv64.p);
     k_gather_dinv<double><<<g, 256, 0, h.s>>>(h.n, nullptr, diagsrc, vals, U.dinv64_nat.p);
     if (need32) {
-        if (U.dinv32.n != (size_t)h.n) { U.dinv32.alloc(h.n); U.dinv32_nat.alloc(h.n); }
+        if (U.dinv32.n != (size_t)h.n) { U.dinv32.alloc(h.n, 4); U.dinv32_nat.alloc(h.n); }
         k_gather_dinv<float><<<g, 256, 0, h.s>>>(h.n, U.perm.p, diagsrc, vals, U.dinv32.p);
         k_gather_dinv<float><<<g, 256, 0, h.s>>>(h.n, nullptr, diagsrc, vals, U.dinv32_nat.p);
     }
@@ -1513,7 +1513,7 @@ static void adjoint_prepare(Handle &h)
                 k_gather_convert<double><<<g, 256, 0, h.s>>>(D->nnz, D->src_nat.p, vals, D->nv64.p);
             }
         }
-        T.U.dinv64.alloc(n);
+        T.U.dinv64.alloc(n, 4);
         T.U.dinv64_nat.alloc(n);
         k_gather_dinv<double><<<g, 256, 0, h.s>>>(n, T.U.perm.p, diagsrc, vals, T.U.dinv64.p);
         k_gather_dinv<double><<<g, 256, 0, h.s>>>(n, nullptr, diagsrc, vals, T.U.dinv64_nat.p);

@@ -1041,11 +1041,11 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
     up(L, R.hlrp, R.hlci, R.lrp.p, R.lci.p, false, R.lv.p);
     up(U, R.hurp, R.huci, R.urp.p, R.uci.p, true, R.uv.p);
     const int g = geom().sms * 4;
-    U.dinv64.alloc(n); U.dinv64_nat.alloc(n);
+    U.dinv64.alloc(n, 4); U.dinv64_nat.alloc(n);
     k_gather_dinv<double><<<g, 256, 0, s>>>(n, U.perm.p, R.diag_ident.p, R.dinv.p, U.dinv64.p);
     k_gather_dinv<double><<<g, 256, 0, s>>>(n, nullptr, R.diag_ident.p, R.dinv.p, U.dinv64_nat.p);
     if (need32) {
-        U.dinv32.alloc(n); U.dinv32_nat.alloc(n);
+        U.dinv32.alloc(n, 4); U.dinv32_nat.alloc(n);
         k_gather_dinv<float><<<g, 256, 0, s>>>(n, U.perm.p, R.diag_ident.p, R.dinv.p, U.dinv32.p);
         k_gather_dinv<float><<<g, 256, 0, s>>>(n, nullptr, R.diag_ident.p, R.dinv.p, U.dinv32_nat.p);
     }

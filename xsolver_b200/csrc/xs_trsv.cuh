@@ -44,25 +44,27 @@ constexpr size_t LU_BLOCK_SMEM_MAX = 200 * 1024;
 constexpr int LUB_MAX_BUFS = 4;
 constexpr size_t LU_SMEM_LIMIT = 227 * 1024;
 
-// one batch buffer: a header (the batch's code, last level + 1, first
-// position, first entry), its level starts (at most R+1), rows (R), entry
-// offsets (R+1), U's dinv (R), columns (E) and values (E, plus the 4-byte
-// rounding of the copied value range)
+// one batch buffer, filled with 16-byte copies of 16-byte aligned ranges: a
+// header (the batch's code, last level + 1, first position, first entry,
+// and the element shift of each copied range inside its region), the level
+// starts (at most R+1), rows (R), entry offsets (R+1), U's dinv (R),
+// columns (E) and values (E); each region has 16 bytes of slack for the
+// rounding of its range
 template <typename FT, typename DT>
 struct LuBatchSmem {
     size_t hdr, lvl, row, eptr, in, pci, pv, bytes;
     static __host__ __device__ LuBatchSmem of(int R, int E)
     {
-        auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+        auto al = [](size_t b) { return (b + 16 + 15) & ~(size_t)15; };
         LuBatchSmem m;
         m.hdr = 0;
-        m.lvl = 16;
+        m.lvl = 64;
         m.row = m.lvl + al((size_t)(R + 1) * sizeof(int));
         m.eptr = m.row + al((size_t)R * sizeof(int));
         m.in = m.eptr + al((size_t)(R + 1) * sizeof(int));
         m.pci = m.in + al((size_t)R * sizeof(DT));
         m.pv = m.pci + al((size_t)E * sizeof(int));
-        m.bytes = m.pv + al((size_t)E * sizeof(FT) + 8);
+        m.bytes = m.pv + al((size_t)E * sizeof(FT));
         return m;
     }
 };
@@ -1089,14 +1091,15 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
     } else if (!T.chunked) {
         level_analysis();
         T.nlevels = P.nlevels;
-        T.perm.alloc(n); T.perm.upload(P.perm.data(), n, s);
-        T.prp.alloc(n + 1); T.prp.upload(P.prp.data(), n + 1, s);
-        T.pci.alloc(m);
+        // padded: the staged single-CTA solve copies 16-byte aligned ranges
+        T.perm.alloc(n, 4); T.perm.upload(P.perm.data(), n, s);
+        T.prp.alloc(n + 1, 4); T.prp.upload(P.prp.data(), n + 1, s);
+        T.pci.alloc(m, 4);
         T.src.alloc(m);
         k_pos_entries<<<g, 256, 0, s>>>(n, upper, T.perm.p, T.prp.p, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, T.pci.p,
                                         T.src.p);
         check_launch();
-        T.lstart.alloc(P.nlevels + 1); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
+        T.lstart.alloc(P.nlevels + 1, 4); T.lstart.upload(P.lstart.data(), P.nlevels + 1, s);
         T.max_level_rows = 0;
         for (int l = 0; l < P.nlevels; l++) T.max_level_rows = std::max(T.max_level_rows, P.lstart[l + 1] - P.lstart[l]);
         // level batches of the staged single-CTA solve (systems it serves only)
@@ -1360,8 +1363,11 @@ __device__ __forceinline__ int lub_first_level(const int *__restrict__ lub, int 
     return v < 0 ? -1 - v : v;
 }
 
-// copy batch b (rows, entry offsets, columns, values, U's dinv) into buf;
-// threads tid of T; nothing for a level too large to stage
+// copy batch b (level starts, rows, entry offsets, columns, values, U's
+// dinv) into buf with 16-byte copies, threads tid of T: each array range is
+// rounded out to 16-byte boundaries (the arrays are allocated with at least
+// 16 bytes of padding) and the element shift of its start goes into the
+// header; a level too large to stage only gets its code
 template <typename FT, typename DT, bool UPPER>
 __device__ __forceinline__ void lu_stage_batch(const TrsvArgs<FT> &P, const int *__restrict__ ls,
                                                const int *__restrict__ lub, int b, const DT *__restrict__ dinv,
@@ -1382,17 +1388,20 @@ __device__ __forceinline__ void lu_stage_batch(const TrsvArgs<FT> &P, const int 
         hdr[2] = pa;
         hdr[3] = ea;
     }
-    int *s_lvl = (int *)(buf + B.lvl);
-    for (int i = tid; i <= l1 - l0; i += T) cp_async4(s_lvl + i, ls + l0 + i);
-    int *s_row = (int *)(buf + B.row), *s_eptr = (int *)(buf + B.eptr), *s_pci = (int *)(buf + B.pci);
-    for (int i = tid; i < pb - pa; i += T) cp_async4(s_row + i, P.perm + pa + i);
-    for (int i = tid; i <= pb - pa; i += T) cp_async4(s_eptr + i, P.prp + pa + i);
-    for (int i = tid; i < eb - ea; i += T) cp_async4(s_pci + i, P.pci + ea + i);
-    const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L, vb1 = ((long)eb * (long)sizeof(FT) + 3) & ~3L;
-    const unsigned char *vsrc = (const unsigned char *)P.pv;
-    for (long w = tid; w < (vb1 - vb0) / 4; w += T) cp_async4(buf + B.pv + 4 * w, vsrc + vb0 + 4 * w);
-    if (UPPER)
-        for (int i = tid; i < pb - pa; i += T) cp_async_n<sizeof(DT)>((DT *)(buf + B.in) + i, dinv + pa + i);
+    auto copy = [&](const void *base, long first, long count, int esz, size_t dst, int slot) {
+        const uintptr_t a0 = (uintptr_t)base + (uintptr_t)(first * esz);
+        const uintptr_t b0 = a0 & ~(uintptr_t)15;
+        const uintptr_t b1 = (a0 + (uintptr_t)(count * esz) + 15) & ~(uintptr_t)15;
+        if (tid == 0) hdr[4 + slot] = (int)((a0 - b0) / (uintptr_t)esz);
+        const long chunks = (long)((b1 - b0) >> 4);
+        for (long c = tid; c < chunks; c += T) cp_async16(buf + dst + 16 * c, (const void *)(b0 + 16 * c));
+    };
+    copy(ls, l0, l1 - l0 + 1, 4, B.lvl, 0);
+    copy(P.perm, pa, pb - pa, 4, B.row, 1);
+    copy(P.prp, pa, pb - pa + 1, 4, B.eptr, 2);
+    copy(P.pci, ea, eb - ea, 4, B.pci, 3);
+    copy(P.pv, ea, eb - ea, (int)sizeof(FT), B.pv, 4);
+    if (UPPER) copy(dinv, pa, pb - pa, (int)sizeof(DT), B.in, 5);
 }
 
 // the levels of batch b by threads tid of T (a barrier of those T threads,
@@ -1409,12 +1418,12 @@ __device__ __forceinline__ void lu_batch_levels(const TrsvArgs<FT> &P, const int
     const int lb = hdr[0];
     if (lb >= 0) {
         const int l0 = lb, l1 = hdr[1], pa = hdr[2], ea = hdr[3];
-        const long vb0 = ((long)ea * (long)sizeof(FT)) & ~3L;
-        const int *s_lvl = (const int *)(buf + B.lvl);
-        const int *s_row = (const int *)(buf + B.row), *s_eptr = (const int *)(buf + B.eptr);
-        const int *s_pci = (const int *)(buf + B.pci);
-        const DT *s_in = (const DT *)(buf + B.in);
-        const FT *pv = (const FT *)(buf + B.pv + ((long)ea * (long)sizeof(FT) - vb0));
+        const int *s_lvl = (const int *)(buf + B.lvl) + hdr[4];
+        const int *s_row = (const int *)(buf + B.row) + hdr[5];
+        const int *s_eptr = (const int *)(buf + B.eptr) + hdr[6];
+        const int *s_pci = (const int *)(buf + B.pci) + hdr[7];
+        const FT *pv = (const FT *)(buf + B.pv) + hdr[8];
+        const DT *s_in = (const DT *)(buf + B.in) + (UPPER ? hdr[9] : 0);
         for (int l = l0; l < l1; l++) {
             const int q0 = s_lvl[l - l0] - pa, q1 = s_lvl[l - l0 + 1] - pa;
             for (int i = q0 + tid; i < q1; i += T) {

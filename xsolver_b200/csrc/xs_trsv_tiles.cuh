@@ -510,6 +510,12 @@ struct TileSmem {
     }
 };
 
+// 16 bytes global -> shared, bypassing L1 (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async4(void *dst, const void *src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
