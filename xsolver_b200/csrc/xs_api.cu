@@ -417,7 +417,7 @@ struct Handle {
     // box-scheduled exact ILU(0) on the L solve's boxes (k_ilu0_tiles: the
     // arrays of IluTileArgs); built with the pattern analysis when L has
     // boxes whose entries fit in shared memory
-    bool ilu_tiles = false;
+    bool ilu_tiles = false, ilu_tiles_built = false;
     size_t ilu_tiles_smem = 0;
     int ilu_max_entries = 0, ilu_max_lower = 0, ilu_max_rows = 0;
     DBuf<int> ilu_ebase, ilu_ent, ilu_roff, ilu_rdiag, ilu_lbase, ilu_loff, ilu_dep;
@@ -724,25 +724,48 @@ static void analyse_pattern(Handle &h)
     h.tpos.free();  // IC(0) transpose map of the previous pattern
     const int n = h.n;
     const int *rp = h.hrp.data(), *ci = h.hci.data();
+    // diagonal positions and the strict triangles' row counts (rows in
+    // parallel blocks), then the triangles as CSR with source indices into
+    // A's value array
     h.huptr.assign(n, -1);
-    for (int i = 0; i < n; i++)
-        for (int k = rp[i]; k < rp[i + 1]; k++)
-            if (ci[k] == i) h.huptr[i] = k;
+    std::vector<int> lrp(n + 1, 0), urp(n + 1, 0);
+    const long RB = 65536;
+    host_parallel_for((n + RB - 1) / RB, 1, [&](long b) {
+        const int i1 = (int)std::min<long>(n, (b + 1) * RB);
+        for (int i = (int)(b * RB); i < i1; i++) {
+            int nl = 0, nu = 0;
+            for (int k = rp[i]; k < rp[i + 1]; k++) {
+                if (ci[k] < i) nl++;
+                else if (ci[k] > i) nu++;
+                else h.huptr[i] = k;
+            }
+            lrp[i + 1] = nl;
+            urp[i + 1] = nu;
+        }
+    });
     for (int i = 0; i < n; i++)
         if (h.huptr[i] < 0) throw Status(XS_ERR_NO_DIAG);
-    // strict triangles as CSR with source indices into A's value array
-    std::vector<int> lrp(n + 1, 0), urp(n + 1, 0), lci, uci;
-    std::vector<long> lsrc, usrc;
-    lci.reserve(h.nnz / 2);
-    uci.reserve(h.nnz / 2);
     for (int i = 0; i < n; i++) {
-        for (int k = rp[i]; k < rp[i + 1]; k++) {
-            if (ci[k] < i) { lci.push_back(ci[k]); lsrc.push_back(k); }
-            else if (ci[k] > i) { uci.push_back(ci[k]); usrc.push_back(k); }
-        }
-        lrp[i + 1] = (int)lci.size();
-        urp[i + 1] = (int)uci.size();
+        lrp[i + 1] += lrp[i];
+        urp[i + 1] += urp[i];
     }
+    std::vector<int> lci(lrp[n]), uci(urp[n]);
+    std::vector<long> lsrc(lrp[n]), usrc(urp[n]);
+    host_parallel_for((n + RB - 1) / RB, 1, [&](long b) {
+        const int i1 = (int)std::min<long>(n, (b + 1) * RB);
+        for (int i = (int)(b * RB); i < i1; i++) {
+            int ol = lrp[i], ou = urp[i];
+            for (int k = rp[i]; k < rp[i + 1]; k++) {
+                if (ci[k] < i) {
+                    lci[ol] = ci[k];
+                    lsrc[ol++] = k;
+                } else if (ci[k] > i) {
+                    uci[ou] = ci[k];
+                    usrc[ou++] = k;
+                }
+            }
+        }
+    });
     build_tri_dev(h.M.L, n, lrp, lci, false, [&](int k) { return lsrc[k]; }, h.s);
     build_tri_dev(h.M.U, n, urp, uci, true, [&](int k) { return usrc[k]; }, h.s);
     h.uptr.alloc(n);
@@ -757,7 +780,8 @@ static void analyse_pattern(Handle &h)
     h.flags.alloc(n);
     h.ilu_epoch = 0;
     h.max_row_len = -1;
-    build_ilu_tiles(h);
+    h.ilu_tiles = false;
+    h.ilu_tiles_built = false;  // the box ILU(0)'s arrays: built on first use
     XS_CUDA(cudaStreamSynchronize(h.s));
     h.analysed = true;
 }
@@ -917,6 +941,10 @@ static void factor_ilu(Handle &h, int kind, int sweeps)
         const int wmax = h.max_row_len;
         int G = 4;
         while (G < wmax && G < 64) G <<= 1;
+        if (ilu_tiles_flag() && !h.ilu_tiles_built) {
+            build_ilu_tiles(h);
+            h.ilu_tiles_built = true;
+        }
         if (h.ilu_tiles && ilu_tiles_flag()) {
             // box schedule: CTAs per SM as the staged box area allows
             const TriDev &L = h.M.L;

@@ -1018,7 +1018,10 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         k_iota_long<<<g, 256, 0, s>>>(T.nnz, T.src_nat.p);
     } else {
         std::vector<long> ns(T.nnz);
-        for (long k = 0; k < T.nnz; k++) ns[k] = src_of((int)k);
+        host_parallel_for((T.nnz + 65535) / 65536, 1, [&](long b) {
+            const long k1 = std::min<long>(T.nnz, (b + 1) * 65536);
+            for (long k = b * 65536; k < k1; k++) ns[k] = src_of((int)k);
+        });
         if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
     }
     // box layout for patterns on a structured grid (large triangles only);
