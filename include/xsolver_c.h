@@ -51,7 +51,7 @@ enum xs_status {
     XS_ERR_NAN = 7,           /* non-finite input or residual                   */
     XS_ERR_ORDER = 8,         /* calls out of order (e.g. pc before ksp)        */
     XS_ERR_ELL_WIDTH = 9,     /* ELL width outside the supported range          */
-    XS_ERR_UNSUPPORTED = 10,  /* combination not provided (e.g. ict on GPU)     */
+    XS_ERR_UNSUPPORTED = 10,  /* combination not provided (e.g. CSC format)     */
     XS_ERR_CAPACITY = 11,     /* a fixed per-row capacity was exceeded          */
     XS_ERR_NO_GPU = 12        /* no CUDA device visible                         */
 };
