@@ -327,6 +327,10 @@ int xs_plan_lusolve_t(xs_plan_t p, const double *d_x, double *d_z);
 /* wait for the plan's stream; returns the device status word (e.g. a
  * sync-free timeout) */
 int xs_plan_sync(xs_plan_t p);
+/* the CUDA stream (cudaStream_t) the plan's work is ordered on: a caller
+ * that orders its own work on it (or waits on it with events) needs no
+ * xs_plan_sync between calls */
+int xs_plan_get_stream(xs_plan_t p, void **stream);
 /* Testing hook for the bounded waits: with enable != 0, the first dependency
  * of the L-solve row at `position` is redirected to the row itself, a value
  * that no thread ever publishes, so the next L solve waits out its limit

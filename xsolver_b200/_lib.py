@@ -90,6 +90,7 @@ def _declare(L):
         "xs_plan_lusolve_t": [C.c_void_p, _vp, _vp],
         "xs_plan_lusolve_batch": [C.c_void_p, C.c_int, _vp, _vp],
         "xs_plan_sync": [C.c_void_p],
+        "xs_plan_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
         "xs_plan_debug_break_dependency": [C.c_void_p, C.c_int, C.c_int],
         "xs_plan_levels": [C.c_void_p, _ip, _ip],
         "xs_plan_time_op": [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp],

@@ -351,6 +351,16 @@ class Plan:
         finally:
             self._pending.clear()
 
+    def stream(self):
+        """The plan's CUDA stream as a torch stream object: work ordered on it
+        (or made to wait on it with events) follows the plan's calls without
+        a sync()."""
+        import torch
+
+        s = C.c_void_p()
+        check(self._L.xs_plan_get_stream(self.p, C.byref(s)), "plan stream")
+        return torch.cuda.ExternalStream(s.value or 0, device=torch.device("cuda", torch.cuda.current_device()))
+
     def debug_break_dependency(self, position: int, enable: bool = True):
         check(self._L.xs_plan_debug_break_dependency(self.p, position, 1 if enable else 0), "debug_break_dependency")
 

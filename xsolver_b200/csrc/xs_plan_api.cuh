@@ -304,6 +304,13 @@ int xs_plan_debug_break_dependency(xs_plan_t p, int position, int enable)
         }
     });
 }
+int xs_plan_get_stream(xs_plan_t p, void **stream)
+{
+    return guarded([&] {
+        if (!p || !stream) throw Status(XS_ERR_INVALID);
+        *stream = (void *)p->h->s;
+    });
+}
 int xs_plan_sync(xs_plan_t p)
 {
     return guarded([&] {

@@ -26,6 +26,8 @@ pointwise Jacobi (JacobiPC, intel/HostMatrix.h:127-147).  The local work goes th
 with spmv(x_aug) -> y and precond(r) -> z on the rank's device;
 DeviceBackend uses this library's CUDA kernels.
 """
+import contextlib
+
 import numpy as np
 import torch
 import torch.distributed as dist
@@ -123,17 +125,44 @@ class DeviceBackend:
         self.P_blk = Plan(CSRMatrix(n, brp, ci[own].astype(np.int32), np.asarray(val)[own], "block")).factor("ilu0")
         self.n, self.nh, self.device = n, nh, device
         self._y = torch.zeros(n + nh, dtype=torch.float64, device=device)
+        self.stream = self.P_aug.stream()
+        self.s_blk = self.P_blk.stream()
+
+    # The solvers run their torch work on self.stream (the SpMV plan's
+    # stream); a call made from any other stream, and every block solve (its
+    # plan has a stream of its own), is ordered against the caller's stream
+    # with events in both directions: no host synchronisation per call.
+    # checkpoint() is the solvers' periodic host sync; it also releases the
+    # plans' references to the tensors of finished work.
+    @staticmethod
+    def _ordered(plan_stream, launch, *tensors):
+        cur = torch.cuda.current_stream()
+        if cur == plan_stream:
+            return launch()
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        plan_stream.wait_event(ev)
+        out = launch()
+        for t in tensors:
+            t.record_stream(plan_stream)
+        done = torch.cuda.Event()
+        done.record(plan_stream)
+        cur.wait_event(done)
+        return out
 
     def spmv(self, x_aug):
-        self.P_aug.spmv(x_aug, self._y)
-        self.P_aug.sync()
+        self._ordered(self.stream, lambda: self.P_aug.spmv(x_aug, self._y), x_aug, self._y)
         return self._y[: self.n].clone()
 
     def precond(self, r):
+        r = r.contiguous()
         z = torch.empty_like(r)
-        self.P_blk.lusolve(r.contiguous(), z)
-        self.P_blk.sync()
+        self._ordered(self.s_blk, lambda: self.P_blk.lusolve(r, z), r, z)
         return z
+
+    def checkpoint(self):
+        self.P_aug.sync()
+        self.P_blk.sync()
 
 
 class JacobiPC:
@@ -159,104 +188,156 @@ def _gdot(a, b):
     return float(t.item())
 
 
-def bicgstab(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000, pc=None):
+def _reduce(*dots):
+    """The local dot products summed over the ranks, in one reduction of a
+    device vector (NCCL orders it on the current stream: no host wait)."""
+    t = torch.stack(list(dots))
+    dist.all_reduce(t)
+    return t
+
+
+def _on_stream(backend):
+    s = getattr(backend, "stream", None)
+    return torch.cuda.stream(s) if s is not None else contextlib.nullcontext()
+
+
+def _checkpoint(backend):
+    f = getattr(backend, "checkpoint", None)
+    if f is not None:
+        f()
+
+
+def bicgstab(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000, pc=None, check_every=16):
     """The reference's BiCGSTAB (intel/mpisolver-C-v1.cpp:365-482) on the
     rank's rows; every rank calls it with its own pieces.  pc: an object
     with precond(r) (e.g. JacobiPC); default the backend's block Jacobi.
     Returns (x_local, resvec, usediter) in the reference's convention
     (resvec[k] = ||r_k|| / ||r_0||, usediter = index of the last
-    iteration)."""
+    iteration).
+
+    The scalars stay on the device and each iteration takes three
+    reductions ((u, r^), ((v, s), (v, v)), ((r, r), (r, r^)): the next
+    iteration's beta comes with this one's residual norm).  The host reads
+    the convergence flag every check_every iterations; an iteration after
+    convergence leaves the solution and the history as they were, so the
+    result is that of stopping at once.  The arithmetic is the reference
+    loop's, operation by operation."""
     M = pc if pc is not None else backend
     dev = plan.device
     n, nh = plan.n_local, plan.n_halo
     small = 1e-20
-    b = torch.as_tensor(b_local, dtype=torch.float64, device=dev)
-    aug = torch.zeros(n + nh, dtype=torch.float64, device=dev)
+    with _on_stream(backend):
+        b = torch.as_tensor(b_local, dtype=torch.float64, device=dev)
+        aug = torch.zeros(n + nh, dtype=torch.float64, device=dev)
 
-    def A(v):
-        aug[:n] = v
-        plan.exchange(aug)
-        return backend.spmv(aug)
+        def A(v):
+            aug[:n] = v
+            plan.exchange(aug)
+            return backend.spmv(aug)
 
-    phi = torch.zeros(n, dtype=torch.float64, device=dev) if x0_local is None else \
-        torch.as_tensor(x0_local, dtype=torch.float64, device=dev).clone()
-    res = b - A(phi)
-    res0 = _gdot(res, res) ** 0.5
-    reso = res.clone()
-    pk = torch.zeros_like(res)
-    uk = torch.zeros_like(res)
-    alpha, beto, gama = 1.0, 1.0, 1.0
-    resvec, used = [], 0
-    for it in range(maxiter):
-        used = it
-        beta = _gdot(res, reso)
-        omega = (beta * gama) / (alpha * beto + small)
-        beto = beta
-        pk = pk + (-alpha) * uk
-        pk = omega * pk
-        pk = pk + res
-        uk = A(M.precond(pk))
-        tmp = _gdot(uk, reso)
-        gama = beta / (tmp + small)
-        sk = res + (-gama) * uk
-        vk = A(M.precond(sk))
-        t = torch.stack([torch.dot(vk, sk), torch.dot(vk, vk)])
-        dist.all_reduce(t)
-        t0, t1 = float(t[0]), float(t[1])
-        alpha = t0 / (t1 + small)
-        phi = phi + gama * pk
-        phi = phi + alpha * sk
-        res = sk + (-alpha) * vk
-        rsm = _gdot(res, res) ** 0.5 / (res0 + small)
-        resvec.append(rsm)
-        if rsm < tol:
-            break
-    return M.precond(phi), np.asarray(resvec), used
+        phi = torch.zeros(n, dtype=torch.float64, device=dev) if x0_local is None else \
+            torch.as_tensor(x0_local, dtype=torch.float64, device=dev).clone()
+        res = b - A(phi)
+        reso = res.clone()
+        t = _reduce(torch.dot(res, res), torch.dot(res, reso))
+        res0 = torch.sqrt(t[0])
+        beta_next = t[1]
+        pk = torch.zeros_like(res)
+        uk = torch.zeros_like(res)
+        one = torch.ones((), dtype=torch.float64, device=dev)
+        alpha, beto, gama = one.clone(), one.clone(), one.clone()
+        hist = torch.zeros(max(maxiter, 1), dtype=torch.float64, device=dev)
+        live = torch.ones((), dtype=torch.bool, device=dev)
+        last = torch.zeros((), dtype=torch.int64, device=dev)
+        for it in range(maxiter):
+            beta = beta_next
+            omega = (beta * gama) / (alpha * beto + small)
+            beto = beta
+            pk = pk + (-alpha) * uk
+            pk = omega * pk
+            pk = pk + res
+            uk = A(M.precond(pk))
+            tmp = _reduce(torch.dot(uk, reso))[0]
+            gama = beta / (tmp + small)
+            sk = res + (-gama) * uk
+            vk = A(M.precond(sk))
+            t = _reduce(torch.dot(vk, sk), torch.dot(vk, vk))
+            alpha = t[0] / (t[1] + small)
+            phi_new = phi + gama * pk
+            phi_new = phi_new + alpha * sk
+            phi = torch.where(live, phi_new, phi)
+            res = sk + (-alpha) * vk
+            t = _reduce(torch.dot(res, res), torch.dot(res, reso))
+            rsm = torch.sqrt(t[0]) / (res0 + small)
+            beta_next = t[1]
+            hist[it] = torch.where(live, rsm, hist[it])
+            last = torch.where(live, torch.full_like(last, it), last)
+            live = live & ~(rsm < tol)
+            if (it + 1) % check_every == 0 or it + 1 == maxiter:
+                _checkpoint(backend)
+                if not bool(live):
+                    break
+        x = M.precond(phi)
+        used = int(last)
+        resvec = hist[: used + 1].cpu().numpy()
+        _checkpoint(backend)
+    return x, resvec, used
 
 
-def pcg(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000, pc=None):
+def pcg(backend, plan: HaloPlan, b_local, x0_local=None, tol=1e-8, maxiter=1000, pc=None, check_every=16):
     """The reference's standard PCG, "cgm" (intel/mpisolver-C-v1.cpp:193-272),
     on the rank's rows with reduced dot products; pc as for bicgstab.
-    Returns (x_local, resvec, usediter) in the reference's convention."""
+    Returns (x_local, resvec, usediter) in the reference's convention.
+    Device scalars and periodic convergence checks as in bicgstab; two
+    reductions per iteration ((p, Ap), ((r, z), (r, r)))."""
     M = pc if pc is not None else backend
     dev = plan.device
     n, nh = plan.n_local, plan.n_halo
     small = 1e-20
-    b = torch.as_tensor(b_local, dtype=torch.float64, device=dev)
-    aug = torch.zeros(n + nh, dtype=torch.float64, device=dev)
+    with _on_stream(backend):
+        b = torch.as_tensor(b_local, dtype=torch.float64, device=dev)
+        aug = torch.zeros(n + nh, dtype=torch.float64, device=dev)
 
-    def A(v):
-        aug[:n] = v
-        plan.exchange(aug)
-        return backend.spmv(aug)
+        def A(v):
+            aug[:n] = v
+            plan.exchange(aug)
+            return backend.spmv(aug)
 
-    phi = torch.zeros(n, dtype=torch.float64, device=dev) if x0_local is None else \
-        torch.as_tensor(x0_local, dtype=torch.float64, device=dev).clone()
-    res = b - A(phi)
-    zk = M.precond(res)
-    t = torch.stack([torch.dot(res, res), torch.dot(res, zk)])
-    dist.all_reduce(t)
-    res0, tao = float(t[0]) ** 0.5, float(t[1])
-    pk = zk.clone()
-    resvec, used = [], 0
-    for it in range(maxiter):
-        used = it
-        taoo = tao
-        apk = A(pk)
-        sigma = _gdot(pk, apk)
-        alpha = tao / (sigma + small)
-        phi = phi + alpha * pk
-        res = res + (-alpha) * apk
+        phi = torch.zeros(n, dtype=torch.float64, device=dev) if x0_local is None else \
+            torch.as_tensor(x0_local, dtype=torch.float64, device=dev).clone()
+        res = b - A(phi)
         zk = M.precond(res)
-        tao = _gdot(res, zk)
-        beta = tao / (taoo + small)
-        pk = beta * pk
-        pk = pk + zk
-        rsm = _gdot(res, res) ** 0.5 / (res0 + small)
-        resvec.append(rsm)
-        if rsm < tol:
-            break
-    return phi, np.asarray(resvec), used
+        t = _reduce(torch.dot(res, res), torch.dot(res, zk))
+        res0, tao = torch.sqrt(t[0]), t[1]
+        pk = zk.clone()
+        hist = torch.zeros(max(maxiter, 1), dtype=torch.float64, device=dev)
+        live = torch.ones((), dtype=torch.bool, device=dev)
+        last = torch.zeros((), dtype=torch.int64, device=dev)
+        for it in range(maxiter):
+            taoo = tao
+            apk = A(pk)
+            sigma = _reduce(torch.dot(pk, apk))[0]
+            alpha = tao / (sigma + small)
+            phi = torch.where(live, phi + alpha * pk, phi)
+            res = res + (-alpha) * apk
+            zk = M.precond(res)
+            t = _reduce(torch.dot(res, zk), torch.dot(res, res))
+            tao = t[0]
+            beta = tao / (taoo + small)
+            pk = beta * pk
+            pk = pk + zk
+            rsm = torch.sqrt(t[1]) / (res0 + small)
+            hist[it] = torch.where(live, rsm, hist[it])
+            last = torch.where(live, torch.full_like(last, it), last)
+            live = live & ~(rsm < tol)
+            if (it + 1) % check_every == 0 or it + 1 == maxiter:
+                _checkpoint(backend)
+                if not bool(live):
+                    break
+        used = int(last)
+        resvec = hist[: used + 1].cpu().numpy()
+        _checkpoint(backend)
+    return phi, resvec, used
 
 
 def _rotate(dx, dy, c, s):
