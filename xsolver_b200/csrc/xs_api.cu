@@ -766,8 +766,8 @@ static void analyse_pattern(Handle &h)
             }
         }
     });
-    build_tri_dev(h.M.L, n, lrp, lci, false, [&](int k) { return lsrc[k]; }, h.s);
-    build_tri_dev(h.M.U, n, urp, uci, true, [&](int k) { return usrc[k]; }, h.s);
+    host_both([&] { build_tri_dev(h.M.L, n, lrp, lci, false, [&](int k) { return lsrc[k]; }, h.s); },
+              [&] { build_tri_dev(h.M.U, n, urp, uci, true, [&](int k) { return usrc[k]; }, h.s); });
     h.uptr.alloc(n);
     h.uptr.upload(h.huptr.data(), n, h.s);
     h.rowof.free();  // row of each entry and U by columns: built when a factorisation needs them

@@ -991,6 +991,7 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, do
     k_plt_final_fill<<<G, 256, 0, s>>>(n, L.rp, L.ci, L.v, U.rp, U.ci, U.v, R.lrp, R.lci, R.lv, R.dinv, R.urp, R.uci,
                                        R.uv);
     check_launch();
+    Trace tr_dl("    pattern download", s);
     R.hlrp.resize(n + 1); R.hurp.resize(n + 1);
     R.hlci.resize(R.nnzL); R.huci.resize(R.nnzU);
     R.lrp.download(R.hlrp.data(), n + 1, s);
@@ -1038,8 +1039,8 @@ inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriD
         check_launch();
         XS_CUDA(cudaStreamSynchronize(s));
     };
-    up(L, R.hlrp, R.hlci, R.lrp.p, R.lci.p, false, R.lv.p);
-    up(U, R.hurp, R.huci, R.urp.p, R.uci.p, true, R.uv.p);
+    host_both([&] { up(L, R.hlrp, R.hlci, R.lrp.p, R.lci.p, false, R.lv.p); },
+              [&] { up(U, R.hurp, R.huci, R.urp.p, R.uci.p, true, R.uv.p); });
     const int g = geom().sms * 4;
     U.dinv64.alloc(n, 4); U.dinv64_nat.alloc(n);
     k_gather_dinv<double><<<g, 256, 0, s>>>(n, U.perm.p, R.diag_ident.p, R.dinv.p, U.dinv64.p);

@@ -28,6 +28,7 @@
 //   needed.  Each spin is bounded (DEV_TRSV_TIMEOUT recorded, kernel returns),
 //   and any thread seeing the error word set stops waiting.
 #pragma once
+#include <exception>
 #include <vector>
 #include <algorithm>
 #include "xs_internal.cuh"
@@ -976,6 +977,37 @@ __global__ void k_gather_dinv(int n, const int *__restrict__ perm, const long *_
 
 namespace xs {
 
+// a() on this host thread and b() on a second one, returning when both are
+// done; the second thread takes the caller's current device, and the first
+// exception either throws is rethrown.  Used to analyse a factor's two
+// triangles at once (independent host work, uploads on one stream).
+template <typename A, typename B>
+inline void host_both(A a, B b)
+{
+    int dev = 0;
+    XS_CUDA(cudaGetDevice(&dev));
+    (void)geom();  // lazily initialised process-wide settings: set before the second thread reads them
+    (void)trsv_tuning();
+    (void)tile_tuning();
+    std::exception_ptr ea, eb;
+    std::thread t([&] {
+        try {
+            XS_CUDA(cudaSetDevice(dev));
+            b();
+        } catch (...) {
+            eb = std::current_exception();
+        }
+    });
+    try {
+        a();
+    } catch (...) {
+        ea = std::current_exception();
+    }
+    t.join();
+    if (ea) std::rethrow_exception(ea);
+    if (eb) std::rethrow_exception(eb);
+}
+
 // Build the device plan of a strict triangle (natural CSR rp/ci, src_of maps
 // an entry to its index in the value array) in the layout the tuning selects,
 // plus the natural-order copy used by the Jacobi-sweep mode.
@@ -997,6 +1029,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         tri_analyse(n, rp.data(), ci.data(), upper, src_of, P, /*entries=*/false);
     };
     Trace tr_up("    upload + positions", s);
+    Trace tr_nat("      natural CSR + sources", s);
     T.n = n;
     T.nnz = rp[n];
     T.nlevels = -1;
@@ -1024,6 +1057,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         });
         if (T.nnz) T.src_nat.upload(ns.data(), T.nnz, s);
     }
+    tr_nat.stop();
     // box layout for patterns on a structured grid (large triangles only);
     // boxes shrink until the rows and halo of one fit in shared memory
     TileHostPlan TP;
@@ -1069,6 +1103,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         }
     }
     if (T.tiled) {
+        Trace tr_bu("      box uploads", s);
         T.ntiles = TP.ntiles;
         T.tile_elems = TP.max_rows + TP.max_halo;
         T.t_max_rows = TP.max_rows;
@@ -1084,6 +1119,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         T.t_hptr.alloc(TP.halo_ptr.size()); T.t_hptr.upload(TP.halo_ptr.data(), TP.halo_ptr.size(), s);
         T.t_hrow.alloc(std::max<size_t>(TP.halo_row.size(), 1));
         if (!TP.halo_row.empty()) T.t_hrow.upload(TP.halo_row.data(), TP.halo_row.size(), s);
+        tr_bu.stop();
         if (need_levels) {
             level_analysis();
             T.nlevels = P.nlevels;
