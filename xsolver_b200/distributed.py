@@ -131,11 +131,14 @@ class DeviceBackend:
     # The solvers run their torch work on self.stream (the SpMV plan's
     # stream); a call made from any other stream, and every block solve (its
     # plan has a stream of its own), is ordered against the caller's stream
-    # with events in both directions: no host synchronisation per call.
-    # checkpoint() is the solvers' periodic host sync; it also releases the
-    # plans' references to the tensors of finished work.
+    # with events in both directions: no host synchronisation per call.  The
+    # plans keep the tensors of their queued work referenced until their
+    # sync(), so no record_stream is used: that would make torch's allocator
+    # record events on a plan's stream when the tensor is freed, which can be
+    # after the plan has destroyed that stream.  checkpoint() is the solvers'
+    # periodic host sync; it also releases those references.
     @staticmethod
-    def _ordered(plan_stream, launch, *tensors):
+    def _ordered(plan_stream, launch):
         cur = torch.cuda.current_stream()
         if cur == plan_stream:
             return launch()
@@ -143,21 +146,19 @@ class DeviceBackend:
         ev.record(cur)
         plan_stream.wait_event(ev)
         out = launch()
-        for t in tensors:
-            t.record_stream(plan_stream)
         done = torch.cuda.Event()
         done.record(plan_stream)
         cur.wait_event(done)
         return out
 
     def spmv(self, x_aug):
-        self._ordered(self.stream, lambda: self.P_aug.spmv(x_aug, self._y), x_aug, self._y)
+        self._ordered(self.stream, lambda: self.P_aug.spmv(x_aug, self._y))
         return self._y[: self.n].clone()
 
     def precond(self, r):
         r = r.contiguous()
         z = torch.empty_like(r)
-        self._ordered(self.s_blk, lambda: self.P_blk.lusolve(r, z), r, z)
+        self._ordered(self.s_blk, lambda: self.P_blk.lusolve(r, z))
         return z
 
     def checkpoint(self):
