@@ -1019,8 +1019,8 @@ static void upload_host_factors(cudaStream_t s, int n, HostTriFactors &F, Parilu
     R.diag_ident.alloc(std::max(n, 1));
     if (n) R.diag_ident.upload(ident.data(), n, s);
     XS_CUDA(cudaStreamSynchronize(s));  // the host arrays are released by the caller
-    R.hlrp = std::move(F.lrp); R.hlci = std::move(F.lci);
-    R.hurp = std::move(F.urp); R.huci = std::move(F.uci);
+    R.hlrp.assign(F.lrp.begin(), F.lrp.end()); R.hlci.assign(F.lci.begin(), F.lci.end());
+    R.hurp.assign(F.urp.begin(), F.urp.end()); R.huci.assign(F.uci.begin(), F.uci.end());
 }
 
 // factors out to caller arrays (any of them may be NULL)
@@ -1495,7 +1495,8 @@ static void adjoint_prepare(Handle &h)
         DBuf<long> ident_diag;
         if (pc_own_pattern(M.type)) {
             ParilutResult &R = h.ilut;
-            lrp = R.hlrp; lci = R.hlci; urp = R.hurp; uci = R.huci;
+            lrp.assign(R.hlrp.begin(), R.hlrp.end()); lci.assign(R.hlci.begin(), R.hlci.end());
+            urp.assign(R.hurp.begin(), R.hurp.end()); uci.assign(R.huci.begin(), R.huci.end());
             lsrc.resize(lci.size()); usrc.resize(uci.size());
             for (size_t k = 0; k < lsrc.size(); k++) lsrc[k] = (long)k;
             for (size_t k = 0; k < usrc.size(); k++) usrc[k] = (long)(lci.size() + k);

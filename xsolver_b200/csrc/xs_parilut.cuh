@@ -49,7 +49,7 @@ struct ParilutResult {
     DBuf<int> lrp, lci, urp, uci;  // strict triangles (seqilu0 layout)
     DBuf<double> lv, uv, dinv;
     DBuf<long> diag_ident;
-    std::vector<int> hlrp, hlci, hurp, huci;
+    HostArray<int> hlrp, hlci, hurp, huci;  // the pattern on the host (box analysis)
 };
 
 constexpr int PLT_CAP = 2048;  // candidate columns gathered per row (with duplicates)
@@ -992,12 +992,20 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, do
                                        R.uv);
     check_launch();
     Trace tr_dl("    pattern download", s);
-    R.hlrp.resize(n + 1); R.hurp.resize(n + 1);
-    R.hlci.resize(R.nnzL); R.huci.resize(R.nnzU);
-    R.lrp.download(R.hlrp.data(), n + 1, s);
-    R.urp.download(R.hurp.data(), n + 1, s);
-    if (R.nnzL) R.lci.download(R.hlci.data(), R.nnzL, s);
-    if (R.nnzU) R.uci.download(R.huci.data(), R.nnzU, s);
+    // uninitialised host arrays whose pages are first touched by parallel
+    // threads (a zero-filling resize faults them in on one thread)
+    auto fetch = [&](HostArray<int> &h, const DBuf<int> &d, long cnt) {
+        h.resize(cnt);
+        host_parallel_for((cnt + 262143) / 262144, 1, [&](long b) {
+            const long k1 = std::min(cnt, (b + 1) * 262144L);
+            for (long k = b * 262144L; k < k1; k += 1024) h[k] = 0;
+        });
+        if (cnt) d.download(h.data(), cnt, s);
+    };
+    fetch(R.hlrp, R.lrp, n + 1);
+    fetch(R.hurp, R.urp, n + 1);
+    fetch(R.hlci, R.lci, R.nnzL);
+    fetch(R.huci, R.uci, R.nnzU);
     std::vector<long> ident(n);
     std::iota(ident.begin(), ident.end(), 0L);
     R.diag_ident.alloc(n);
@@ -1009,7 +1017,7 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, do
 inline void ilut_to_tri(cudaStream_t s, int n, ParilutResult &R, TriDev &L, TriDev &U, bool need32)
 {
     Trace tr_all("ilut_to_tri", s);
-    auto up = [&](TriDev &T, const std::vector<int> &nrp, const std::vector<int> &nci, const int *drp, const int *dci,
+    auto up = [&](TriDev &T, const HostArray<int> &nrp, const HostArray<int> &nci, const int *drp, const int *dci,
                   bool upper, const double *vals) {
         T = TriDev();
         {

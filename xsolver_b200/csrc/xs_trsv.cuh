@@ -1011,13 +1011,14 @@ inline void host_both(A a, B b)
 // Build the device plan of a strict triangle (natural CSR rp/ci, src_of maps
 // an entry to its index in the value array) in the layout the tuning selects,
 // plus the natural-order copy used by the Jacobi-sweep mode.
-template <typename SrcF>
+template <typename SrcF, typename IV>
+// rp/ci: std::vector<int> or HostArray<int>
 // identity_src: entry k's value is vals[k] (src_of is not called)
 // d_rp/d_ci: the same pattern already on the device (copied instead of uploaded)
 // need_levels: keep the level order of a triangle that gets boxes (the
 // level-ordered ILU(0)/IC(0) kernels read it); without it a boxed
 // triangle skips the level analysis (nlevels = -1)
-inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const std::vector<int> &ci, bool upper, SrcF src_of,
+inline void build_tri_dev(TriDev &T, int n, const IV &rp, const IV &ci, bool upper, SrcF src_of,
                           cudaStream_t s, bool identity_src = false, const int *d_rp = nullptr,
                           const int *d_ci = nullptr, bool need_levels = true)
 {
@@ -1091,7 +1092,7 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
             for (int attempt = 0; attempt < 6; attempt++) {
                 TP = TileHostPlan();
                 Trace tr_lay("      box layout", s);
-                if (!tile_layout(n, rp.data(), ci.data(), upper, src_of, G, tt, TP)) break;
+                if (!tile_layout(n, rp.data(), ci.data(), upper, src_of, G, tt, TP, /*entries=*/false)) break;
                 tr_lay.stop();
                 if (TileSmem::of<double, double, double>(TP.max_rows, TP.max_halo, TP.max_entries).total <=
                     TILE_SMEM_MAX) {
@@ -1111,14 +1112,26 @@ inline void build_tri_dev(TriDev &T, int n, const std::vector<int> &rp, const st
         T.t_max_entries = TP.max_entries;
         T.perm.alloc(n); T.perm.upload(TP.perm.data(), n, s);
         T.prp.alloc(n + 1); T.prp.upload(TP.prp.data(), n + 1, s);
-        T.pci.alloc(m); if (T.nnz) T.pci.upload(TP.pci.data(), T.nnz, s);
-        T.src.alloc(m); if (T.nnz) T.src.upload(TP.src.data(), T.nnz, s);
         T.t_pos.alloc(TP.tile_pos.size()); T.t_pos.upload(TP.tile_pos.data(), TP.tile_pos.size(), s);
         T.t_lvl.alloc(TP.tile_lvl.size()); T.t_lvl.upload(TP.tile_lvl.data(), TP.tile_lvl.size(), s);
         T.t_lptr.alloc(TP.lvl_ptr.size()); T.t_lptr.upload(TP.lvl_ptr.data(), TP.lvl_ptr.size(), s);
         T.t_hptr.alloc(TP.halo_ptr.size()); T.t_hptr.upload(TP.halo_ptr.data(), TP.halo_ptr.size(), s);
         T.t_hrow.alloc(std::max<size_t>(TP.halo_row.size(), 1));
         if (!TP.halo_row.empty()) T.t_hrow.upload(TP.halo_row.data(), TP.halo_row.size(), s);
+        // the entries (slot and value source of each) written on the device
+        // from the rows' boxes and positions
+        T.pci.alloc(m);
+        T.src.alloc(m);
+        if (T.nnz) {
+            DBuf<int> d_tile_of, d_pos_of;
+            d_tile_of.alloc(n); d_tile_of.upload(TP.tile_of.data(), n, s);
+            d_pos_of.alloc(n); d_pos_of.upload(TP.pos_of.data(), n, s);
+            auto kern = upper ? k_tile_entries<true> : k_tile_entries<false>;
+            kern<<<g, 256, 0, s>>>(n, T.perm.p, T.prp.p, T.rp_nat.p, T.ci_nat.p, T.src_nat.p, d_tile_of.p, d_pos_of.p,
+                                   T.t_pos.p, T.t_hptr.p, T.t_hrow.p, T.pci.p, T.src.p);
+            check_launch();
+            XS_CUDA(cudaStreamSynchronize(s));  // before the temporaries are freed
+        }
         tr_bu.stop();
         if (need_levels) {
             level_analysis();

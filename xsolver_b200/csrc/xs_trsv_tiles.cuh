@@ -118,8 +118,11 @@ struct TileHostPlan {
     int n = 0, ntiles = 0, max_rows = 0, max_halo = 0, max_entries = 0;
     int nx = 0, ny = 0, nz = 0, sa = 0, sb = 0, sc = 0;
     std::vector<int> perm, prp, tile_pos, tile_lvl, lvl_ptr, halo_ptr, halo_row;
-    HostArray<int> pci;   // every entry written by the layout
+    HostArray<int> pci;   // every entry written by the layout (entries = true)
     HostArray<long> src;
+    // entries = false: what a device pass needs to write pci/src itself
+    HostArray<int> tile_of;  // by logical index (row, or n-1-row for U): the row's box
+    std::vector<int> pos_of;  // by row: its position
 };
 
 // ---------------------------------------------------------------- grid fit
@@ -315,7 +318,7 @@ inline bool tile_detect(int n, const int *rp, const int *ci, bool upper, TileGri
 // Box layout of a strict triangle on a detected grid (the second half).
 template <typename SrcF>
 inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF src_of, const TileGrid &G,
-                        const TileTuning &tt, TileHostPlan &h)
+                        const TileTuning &tt, TileHostPlan &h, bool entries = true)
 {
     const long nnz = rp[n];
     auto logical = [&](int r) -> long { return upper ? (long)n - 1 - r : (long)r; };
@@ -418,8 +421,10 @@ inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF sr
         const int r = h.perm[p];
         h.prp[p + 1] = h.prp[p] + (rp[r + 1] - rp[r]);
     }
-    h.pci.resize(nnz);  // written in full below (each box its rows' entries)
-    h.src.resize(nnz);
+    if (entries) {
+        h.pci.resize(nnz);  // written in full below (each box its rows' entries)
+        h.src.resize(nnz);
+    }
     h.halo_ptr.assign(h.ntiles + 1, 0);
     std::vector<std::vector<int>> ext_of(h.ntiles);
     host_parallel_for(h.ntiles, 16, [&](long t) {
@@ -432,6 +437,7 @@ inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF sr
         }
         std::sort(ext.begin(), ext.end());
         ext.erase(std::unique(ext.begin(), ext.end()), ext.end());
+        if (!entries) return;
         for (int p = p0; p < p1; p++) {
             const int r = h.perm[p];
             int o = h.prp[p];
@@ -458,7 +464,53 @@ inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF sr
         if (!ext_of[t].empty())
             std::memcpy(h.halo_row.data() + h.halo_ptr[t], ext_of[t].data(), sizeof(int) * ext_of[t].size());
     });
+    if (!entries) {
+        h.tile_of = std::move(tile_of);
+        h.pos_of = std::move(pos_of);
+    }
     return true;
+}
+
+// The entries of a box layout in accumulation order, one thread per
+// position: the same slots tile_layout writes on the host (a dependency in
+// the row's own box: its position minus the box's first; otherwise the box's
+// row count plus its index in the box's sorted halo list) and each entry's
+// value source (src_nat of the natural entry).  Inputs from tile_layout with
+// entries = false; rp/ci/src_nat the natural CSR on the device.
+template <bool UPPER>
+__global__ void k_tile_entries(int n, const int *__restrict__ perm, const int *__restrict__ prp,
+                               const int *__restrict__ rp, const int *__restrict__ ci,
+                               const long *__restrict__ src_nat, const int *__restrict__ tile_of,
+                               const int *__restrict__ pos_of, const int *__restrict__ tile_pos,
+                               const int *__restrict__ halo_ptr, const int *__restrict__ halo_row, int *__restrict__ pci,
+                               long *__restrict__ src)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int r = perm[p];
+        const int t = tile_of[UPPER ? n - 1 - r : r];
+        const int p0 = tile_pos[t], rows = tile_pos[t + 1] - p0;
+        const int h0 = halo_ptr[t], nh = halo_ptr[t + 1] - h0;
+        const int e0 = rp[r], e1 = rp[r + 1];
+        long o = prp[p];
+        for (int j = 0; j < e1 - e0; j++, o++) {
+            const int e = UPPER ? e1 - 1 - j : e0 + j;
+            const int d = ci[e];
+            int slot;
+            if (tile_of[UPPER ? n - 1 - d : d] == t) {
+                slot = pos_of[d] - p0;
+            } else {  // first halo index whose row is >= d (the row is in the list)
+                int lo = 0, hi = nh;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (halo_row[h0 + mid] < d) lo = mid + 1;
+                    else hi = mid;
+                }
+                slot = rows + lo;
+            }
+            pci[o] = slot;
+            src[o] = src_nat[e];
+        }
+    }
 }
 
 // Tile layout of a strict triangle (both halves, the given box dimensions); false when the pattern fits no grid
