@@ -1112,7 +1112,10 @@ static void build_precond(Handle &h)
         }
         // factors in the seqilu0 layout on their own pattern
         ilut_to_tri(h.s, n, h.ilut, M.L, M.U, need32);
-        pool_trim(h.s);
+        {
+            Trace tr_trim("  scratch pool trim", h.s);
+            pool_trim(h.s);
+        }
         M.ensure_buffers64(h.s);
         if (need32) M.ensure_buffers32(h.s);
         if (h.trsv_mode > 0) M.ensure_sweep_buffers(need32);

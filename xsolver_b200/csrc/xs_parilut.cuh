@@ -420,16 +420,35 @@ __device__ __forceinline__ double plt_sweep_value(const int *arp, const int *aci
 constexpr int PLT_ROW_CAP = 256;
 constexpr int PLT_SW_WARPS = 4;
 // column -> pattern position of the row being swept: open addressing in
-// shared memory, key (column) and position packed in one 64-bit word, at most
-// half full (PLT_HASH >= 2 * PLT_ROW_CAP), linear probing; a lookup costs one
-// or two loads where a binary search over the sorted pattern costs eight
+// shared memory, at most half full (PLT_HASH >= 2 * PLT_ROW_CAP), linear
+// probing; a lookup costs one or two loads where a binary search over the
+// sorted pattern costs eight.  One 32-bit word per slot: the column's low 24
+// bits above the position (< PLT_ROW_CAP - 1 = 255, 8 bits), so a warp's table
+// is 2 KB and more rows are in flight per SM.  Columns below 2^24 - 1 are
+// told apart by their 24 bits alone; for larger systems a match of the low
+// bits is confirmed against the staged column (plt_hash_find).
 constexpr int PLT_HASH = 512;
-constexpr unsigned long long PLT_HASH_EMPTY = ~0ull;
+constexpr unsigned PLT_HASH_EMPTY = ~0u;
+__device__ __forceinline__ unsigned plt_hash_key(int j, int q) { return ((unsigned)j << 8) | (unsigned)q; }
+
 __device__ __forceinline__ unsigned plt_hash_slot(int j)
 {
     return ((unsigned)j * 2654435761u) >> (32 - 9);  // log2(PLT_HASH) = 9
 }
-static_assert(PLT_HASH == 512 && PLT_HASH >= 2 * PLT_ROW_CAP, "hash table size");
+static_assert(PLT_HASH == 512 && PLT_HASH >= 2 * PLT_ROW_CAP && PLT_ROW_CAP <= 256, "hash table size");
+// position of column j in the staged pattern (col), or -1
+__device__ __forceinline__ int plt_hash_find(const unsigned *ht, const int *col, bool wide, int j)
+{
+    const unsigned lo = (unsigned)j & 0xffffffu;
+    for (unsigned sl = plt_hash_slot(j);; sl = (sl + 1) & (PLT_HASH - 1)) {
+        const unsigned kv = ht[sl];
+        if (kv == PLT_HASH_EMPTY) return -1;
+        if ((kv >> 8) == lo) {
+            const int q = (int)(kv & 0xffu);
+            if (!wide || col[q] == j) return q;
+        }
+    }
+}
 
 static __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
     int n, int parts, const int *__restrict__ arp, const int *__restrict__ aci, const double *__restrict__ av,
@@ -439,19 +458,22 @@ static __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
 {
     __shared__ int s_col[PLT_SW_WARPS][PLT_ROW_CAP];
     __shared__ double s_t[PLT_SW_WARPS][PLT_ROW_CAP];
-    __shared__ unsigned long long s_h[PLT_SW_WARPS][PLT_HASH];
+    __shared__ unsigned s_h[PLT_SW_WARPS][PLT_HASH];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int *col = s_col[w];
     double *t = s_t[w];
-    unsigned long long *ht = s_h[w];
+    unsigned *ht = s_h[w];
+    const bool wide = n > 0xffffff;  // columns up to n - 1 may share their low 24 bits
     for (int i = blockIdx.x * PLT_SW_WARPS + w; i < n; i += gridDim.x * PLT_SW_WARPS) {
         const int l0 = lrp[i], l1 = lrp[i + 1];
         // L row i: strict entries first (ascending), the unit diagonal (col i) last
         const int nl = (l1 > l0 && lci[l1 - 1] >= i) ? l1 - l0 - 1 : l1 - l0;
         const int u0 = urp[i], nu = urp[i + 1] - u0;
         const int m = nl + nu;
-        if (m > PLT_ROW_CAP) {
-            // per-entry walk for an unusually long row
+        if (m >= PLT_ROW_CAP) {
+            // per-entry walk for an unusually long row (the table takes rows
+            // of up to PLT_ROW_CAP - 1 entries: positions below 255, so no
+            // key equals the empty word)
             if (parts & 1) {
                 for (int q = lane; q < l1 - l0; q += 32) {
                     const int k = l0 + q, j = lci[k];
@@ -473,7 +495,7 @@ static __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
             col[q] = j;
             const int pa = find_pos(aci, arp[i], arp[i + 1], j);
             t[q] = pa >= 0 ? av[pa] : 0.0;
-            const unsigned long long kv = ((unsigned long long)(unsigned)j << 32) | (unsigned)q;
+            const unsigned kv = plt_hash_key(j, q);
             for (unsigned sl = plt_hash_slot(j);; sl = (sl + 1) & (PLT_HASH - 1))
                 if (atomicCAS(ht + sl, PLT_HASH_EMPTY, kv) == PLT_HASH_EMPTY) break;
         }
@@ -504,15 +526,7 @@ static __global__ void __launch_bounds__(32 * PLT_SW_WARPS) k_plt_sweep_rows(
                     if (!(parts & 2) && j >= i) continue;
                     if (!(parts & 1) && j < i) continue;
                     // position of j in the row's pattern (hash lookup)
-                    int pos = -1;
-                    for (unsigned sl = plt_hash_slot(j);; sl = (sl + 1) & (PLT_HASH - 1)) {
-                        const unsigned long long kv = ht[sl];
-                        if (kv == PLT_HASH_EMPTY) break;
-                        if ((int)(kv >> 32) == j) {
-                            pos = (int)(unsigned)kv;
-                            break;
-                        }
-                    }
+                    const int pos = plt_hash_find(ht, col, wide, j);
                     if (pos >= 0) t[pos] = t[pos] - lk * uv[e];
                 }
                 __syncwarp();
@@ -774,6 +788,19 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_write(int n, 
     if (over) atomicOr(err, DEV_CAPACITY);
 }
 
+// Grid of a warp-per-row kernel: every block resident at once (the blocks
+// take rows grid-strided, so each gets the same share; a grid larger than
+// what fits would run its surplus as a partial second wave), at most one
+// warp per row.
+template <typename K>
+inline int plt_resident_grid(K kern, int warps, int n)
+{
+    int per_sm = 0;
+    XS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, 0));
+    const long rows_cap = ((long)n + warps - 1) / warps;
+    return (int)std::max(1L, std::min(rows_cap, (long)std::max(per_sm, 1) * geom().sms));
+}
+
 struct PltCtx {
     cudaStream_t s;
     int *err;
@@ -878,7 +905,7 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, do
         Trace tr_cand("  candidates", s);
         DCsr D;
         D.n = n;
-        const int cg = std::min((n + PLT_WARPS - 1) / PLT_WARPS, geom().sms * 16);
+        const int cg = plt_resident_grid(k_candidates, PLT_WARPS, n);
         k_candidates<<<cg, 32 * PLT_WARPS, 0, s>>>(n, A.rp, A.ci, L.rp, L.ci, U.rp, U.ci, 0, cnt, nullptr, nullptr, err);
         check_launch();
         D.nnz = scan_counts(c, cnt, D.rp);
@@ -888,7 +915,7 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, do
         check_launch();
         tr_cand.stop();
         Trace tr_val("  candidate values", s);
-        k_candidate_values<<<std::max(1, std::min((n + PLT_CV_WARPS - 1) / PLT_CV_WARPS, geom().sms * 16)),
+        k_candidate_values<<<plt_resident_grid(k_candidate_values, PLT_CV_WARPS, n),
                              32 * PLT_CV_WARPS, 0, s>>>(n, A.rp, A.ci, A.v, L.rp, L.ci, L.v, U.rp, U.ci, U.v, udiag,
                                                         D.rp, D.ci, D.v);
         check_launch();
@@ -916,7 +943,7 @@ inline void parilut_build(cudaStream_t s, int *err, int n, const Operator &A, do
         tr_split.stop();
         Trace tr_s1("  LU sweep", s);
         // LU sweep (synchronous): both parts from the old values
-        const int rg = std::max(1, std::min((n + PLT_SW_WARPS - 1) / PLT_SW_WARPS, geom().sms * 16));
+        const int rg = plt_resident_grid(k_plt_sweep_rows, PLT_SW_WARPS, n);
         {
             DBuf<double> lnew, unew;
             lnew.alloc(L2.nnz);
