@@ -329,7 +329,9 @@ int xs_plan_lusolve_t(xs_plan_t p, const double *d_x, double *d_z);
 int xs_plan_sync(xs_plan_t p);
 /* the CUDA stream (cudaStream_t) the plan's work is ordered on: a caller
  * that orders its own work on it (or waits on it with events) needs no
- * xs_plan_sync between calls */
+ * xs_plan_sync between calls.  The plan owns the stream: it stays valid
+ * until xs_plan_destroy, which synchronises and destroys it, so nothing may
+ * be recorded on it (events, allocator stream uses) after that call. */
 int xs_plan_get_stream(xs_plan_t p, void **stream);
 /* Testing hook for the bounded waits: with enable != 0, the first dependency
  * of the L-solve row at `position` is redirected to the row itself, a value

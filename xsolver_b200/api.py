@@ -354,7 +354,11 @@ class Plan:
     def stream(self):
         """The plan's CUDA stream as a torch stream object: work ordered on it
         (or made to wait on it with events) follows the plan's calls without
-        a sync()."""
+        a sync().  The plan owns the stream and destroys it in close(), so a
+        tensor must not be given to it with record_stream(): torch's
+        allocator would record an event on it when the tensor is freed,
+        which can be after the plan is gone.  The plan itself keeps the
+        tensors of its queued work referenced until sync()."""
         import torch
 
         s = C.c_void_p()
