@@ -441,7 +441,10 @@ int xs_set_persistent_iteration(int enable);
  * (default) uses them for triangles of at least min_rows rows (default
  * 65536, at least 8) whose pattern fits a grid, with boxes of tx*ty*tz
  * sheared grid steps (default 16*16*8, halved along the longest side until
- * a box's staged data fits in shared memory); 0 keeps the level-ordered
+ * a box's staged data fits in shared memory; triangles averaging at least 20
+ * entries per row, such as ParILUT fill of 27-point operators, start from
+ * 8*4*2 instead unless a box size was set here or by XS_TRSV_TILES, since a
+ * box size set either way applies to every triangle); 0 keeps the level-ordered
  * solve (the other arguments are then ignored).  Results are bitwise
  * identical either way.  Environment XS_TRSV_TILES ("0" or "tx,ty,tz") and
  * XS_TRSV_TILE_MIN_ROWS set it at first use.  Fixed when a preconditioner is

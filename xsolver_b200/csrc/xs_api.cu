@@ -126,7 +126,7 @@ TileTuning &tile_tuning()
             int a = 0, b = 0, c = 0;
             const int k = sscanf(e, "%d,%d,%d", &a, &b, &c);
             if (k == 1 && a == 0) t.enable = 0;
-            else if (k == 3 && a > 0 && b > 0 && c > 0) { t.enable = 1; t.tx = a; t.ty = b; t.tz = c; }
+            else if (k == 3 && a > 0 && b > 0 && c > 0) { t.enable = 1; t.tx = a; t.ty = b; t.tz = c; t.user_box = 1; }
         }
         if (const char *e = getenv("XS_TRSV_TILE_MIN_ROWS")) t.min_rows = std::max(8, atoi(e));
         if (const char *e = getenv("XS_TRSV_TILE_BLOCKS_PER_SM")) t.blocks_per_sm = std::max(1, atoi(e));
@@ -1985,6 +1985,7 @@ int xs_set_trsv_tiles(int enable, int tx, int ty, int tz, int min_rows)
             tile_tuning().ty = ty;
             tile_tuning().tz = tz;
             tile_tuning().min_rows = min_rows;
+            tile_tuning().user_box = 1;
         }
     });
 }

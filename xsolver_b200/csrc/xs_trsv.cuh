@@ -1082,6 +1082,11 @@ inline void build_tri_dev(TriDev &T, int n, const IV &rp, const IV &ci, bool upp
             // its halo a quarter of its rows: the smallest box the layout
             // could accept), then the layout's own sizes decide
             const double per_row = (double)T.nnz / n;
+            if (!tt.user_box && per_row >= TILE_DENSE_ROW) {
+                tt.tx = TILE_DENSE_BOX[0];
+                tt.ty = TILE_DENSE_BOX[1];
+                tt.tz = TILE_DENSE_BOX[2];
+            }
             for (;;) {
                 const int rows = tt.tx * tt.ty * tt.tz;
                 if (TileSmem::of<double, double, double>(rows, rows / 4, (int)(rows * per_row)).total <=

@@ -79,7 +79,18 @@ struct TileTuning {
     int tx = 16, ty = 16, tz = 8;
     int min_rows = 65536;
     int blocks_per_sm = 4;
+    int user_box = 0;  // tx/ty/tz set by the caller (xs_set_trsv_tiles, XS_TRSV_TILES): no dense-row default
 };
+// Triangles with at least this many entries per row on average start from
+// TILE_DENSE_BOX boxes instead of tx/ty/tz: small boxes, long along x, four
+// resident per SM.  Measured on the 160^3 27-point ParILUT factors (about
+// 27 entries per row): GMRES(30) solve 222 ms with 8x4x2 boxes against
+// 294 ms with the 8x8x8 boxes the size-only shrink reached; 8x2x2 239,
+// 8x4x4 243, 16x8x4 248, 16x4x2 275, 32x4x4 349, 4x8x8 407 ms.  Sparse
+// rows (7-point ILU(0), 3 per row) keep 16x16x8: 0.45 ms per triangle
+// against 0.51-0.57 ms with 8x8x8 or 16x8x8.
+constexpr double TILE_DENSE_ROW = 20.0;
+constexpr int TILE_DENSE_BOX[3] = {8, 4, 2};
 TileTuning &tile_tuning();
 
 constexpr int TILE_THREADS = 256;
