@@ -169,3 +169,66 @@ def test_wrapping_neighbour_is_refused_or_scheduled_safely():
     T = tiles(A.n, rp2, np.ascontiguousarray(c2), False, (4, 4, 4))
     if T is not None:
         check_schedule(A.n, rp2, np.ascontiguousarray(c2), False, T)
+
+
+def device_rule_slots(n, rp, ci, upper, T):
+    """The slots the device pass (`k_tile_entries`) writes, restated in
+    numpy from the per-row data alone: each row's box and position and each
+    box's sorted halo list.  A dependency d of the row at position p in box
+    t gets its position minus the box's first when d lies in box t, else the
+    box's row count plus the index of d in the box's halo list; entries in
+    the accumulation order (L: increasing column, U: decreasing)."""
+    perm, prp = T["perm"].astype(np.int64), T["prp"].astype(np.int64)
+    tile_pos, halo_ptr, halo_row = T["tile_pos"].astype(np.int64), T["halo_ptr"].astype(np.int64), T["halo_row"]
+    nt = len(tile_pos) - 1
+    pos_of = np.empty(n, np.int64)
+    pos_of[perm] = np.arange(n)
+    box_of_pos = np.repeat(np.arange(nt), np.diff(tile_pos))
+    box_of_row = np.empty(n, np.int64)
+    box_of_row[perm] = box_of_pos
+    m = int(prp[-1])
+    p = np.repeat(np.arange(n), np.diff(prp))  # position of each staged entry
+    j = np.arange(m) - prp[p]  # its index within the row
+    r = perm[p]
+    e = (rp[r + 1] - 1 - j) if upper else (rp[r] + j)
+    d = ci[e].astype(np.int64)
+    t = box_of_row[r]
+    p0 = tile_pos[t]
+    rows = tile_pos[t + 1] - p0
+    nh = int(halo_ptr[-1])
+    halo_box = np.repeat(np.arange(nt), np.diff(halo_ptr))
+    keys = halo_box * n + halo_row[:nh].astype(np.int64)  # sorted: boxes in order, each list sorted
+    same = box_of_row[d] == t
+    slot = np.where(same, pos_of[d] - p0, rows + np.searchsorted(keys, t * n + d) - halo_ptr[t])
+    return slot
+
+
+@pytest.mark.parametrize("upper", [False, True])
+@pytest.mark.parametrize("case", ["7pt", "27pt", "parilut"])
+def test_device_entry_rule_matches_host_layout(case, upper):
+    """The solve's per-entry slots are written on the device from per-row
+    data (the host layout keeps only each row's box and position and the
+    halo lists); that rule reproduces, entry for entry, the slots the host
+    layout writes itself, and every halo lookup finds its row."""
+    if case == "parilut":
+        import oracle
+
+        A = st.convdiff3d_27pt(16)
+        F = oracle.parilut(A, fill=2.0, sweeps=5, droptol=1e-4)
+        rp, ci = (F.urp, F.uci) if upper else (F.lrp, F.lci)
+        rp, ci = np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32)
+        n, box = A.n, (8, 4, 2)
+    else:
+        A = st.poisson3d_7pt(24) if case == "7pt" else st.convdiff3d_27pt(14)
+        rp, ci = _tri(A, upper)
+        n, box = A.n, (8, 8, 4)
+    T = tiles(n, rp, ci, upper, box)
+    assert T is not None
+    slot = device_rule_slots(n, rp.astype(np.int64), ci, upper, T)
+    assert np.array_equal(slot, T["pci"][:len(slot)].astype(np.int64))
+    # per entry: its box's row count and halo length; halo slots stay inside the list
+    nt = len(T["tile_pos"]) - 1
+    box_of_pos = np.repeat(np.arange(nt), np.diff(T["tile_pos"]))
+    box = box_of_pos[np.repeat(np.arange(n), np.diff(T["prp"]))]
+    rows, nh = np.diff(T["tile_pos"])[box], np.diff(T["halo_ptr"])[box]
+    assert np.all(slot < rows + nh)
