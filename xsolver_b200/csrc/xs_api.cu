@@ -749,8 +749,9 @@ static void analyse_pattern(Handle &h)
         lrp[i + 1] += lrp[i];
         urp[i + 1] += urp[i];
     }
-    std::vector<int> lci(lrp[n]), uci(urp[n]);
-    std::vector<long> lsrc(lrp[n]), usrc(urp[n]);
+    // written in full by the row blocks below: no serial zero fill
+    HostArray<int> lci(lrp[n]), uci(urp[n]);
+    HostArray<long> lsrc(lrp[n]), usrc(urp[n]);
     host_parallel_for((n + RB - 1) / RB, 1, [&](long b) {
         const int i1 = (int)std::min<long>(n, (b + 1) * RB);
         for (int i = (int)(b * RB); i < i1; i++) {

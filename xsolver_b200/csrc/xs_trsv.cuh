@@ -1011,14 +1011,14 @@ inline void host_both(A a, B b)
 // Build the device plan of a strict triangle (natural CSR rp/ci, src_of maps
 // an entry to its index in the value array) in the layout the tuning selects,
 // plus the natural-order copy used by the Jacobi-sweep mode.
-template <typename SrcF, typename IV>
+template <typename SrcF, typename RV, typename CV>
 // rp/ci: std::vector<int> or HostArray<int>
 // identity_src: entry k's value is vals[k] (src_of is not called)
 // d_rp/d_ci: the same pattern already on the device (copied instead of uploaded)
 // need_levels: keep the level order of a triangle that gets boxes (the
 // level-ordered ILU(0)/IC(0) kernels read it); without it a boxed
 // triangle skips the level analysis (nlevels = -1)
-inline void build_tri_dev(TriDev &T, int n, const IV &rp, const IV &ci, bool upper, SrcF src_of,
+inline void build_tri_dev(TriDev &T, int n, const RV &rp, const CV &ci, bool upper, SrcF src_of,
                           cudaStream_t s, bool identity_src = false, const int *d_rp = nullptr,
                           const int *d_ci = nullptr, bool need_levels = true)
 {
@@ -1051,7 +1051,7 @@ inline void build_tri_dev(TriDev &T, int n, const IV &rp, const IV &ci, bool upp
     if (identity_src) {
         k_iota_long<<<g, 256, 0, s>>>(T.nnz, T.src_nat.p);
     } else {
-        std::vector<long> ns(T.nnz);
+        HostArray<long> ns(T.nnz);  // written in full below
         host_parallel_for((T.nnz + 65535) / 65536, 1, [&](long b) {
             const long k1 = std::min<long>(T.nnz, (b + 1) * 65536);
             for (long k = b * 65536; k < k1; k++) ns[k] = src_of((int)k);
