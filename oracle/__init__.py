@@ -7,7 +7,9 @@ ctypes bindings for
   _ref/libxsref_intel.so    the reference's own intel/ CPU solver compiled from
   _ref/libxsref_ilu0.so     its sources, its hip ilu0_simple and ilutp_final,
   _ref/libxsref_ic0.so      IC(0) and
-  _ref/libxsref_ict.so      ICT (Makefile).
+  _ref/libxsref_ict.so      ICT (Makefile), and
+  liboracle_mt.so           the threaded BiCGSTAB + ILU(0) of the benchmark's
+                            CPU reference arm (xs_oracle_mt.cpp; timing only).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
 this package, as the checker or the timed CPU baseline.  The product path
@@ -23,6 +25,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
+_LIB_MT = None
 _REF_INTEL = None
 _REF_ILU0 = None
 _REF_MMIO = None
@@ -58,6 +61,37 @@ def lib():
             build(ref=False)
         _LIB = C.CDLL(path)
     return _LIB
+
+
+def lib_mt():
+    global _LIB_MT
+    if _LIB_MT is None:
+        path = os.path.join(HERE, "liboracle_mt.so")
+        if not os.path.exists(path):
+            build(ref=False)
+        L = C.CDLL(path)
+        L.orcmt_bicgstab.restype = C.c_int
+        _LIB_MT = L
+    return _LIB_MT
+
+
+def bicgstab_threads(A, b, F, tol=1e-10, maxiter=1000, threads=0, x0=None):
+    """The reference BiCGSTAB + ILU(0) loop (intel/mpisolver-C-v1.cpp:365-482,
+    LU apply hip/HostMatrix/HostMatrixCSR.cpp:385-409) with its SpMV and
+    vector operations on `threads` host threads (0: all) and the triangular
+    solves sequential; dot products in a fixed blocked order.  For timing
+    (the benchmark's CPU reference arm); parity tests use solve().
+    Returns (x, iterations, final relative residual)."""
+    n = A.n
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    rsm = C.c_double()
+    it = lib_mt().orcmt_bicgstab(n, _p(A.rowptr, np.int32), _p(A.colidx, np.int32), _p(A.val), _p(F.lrp, np.int32),
+                                 _p(F.lci, np.int32), _p(F.lv), _p(F.dinv), _p(F.urp, np.int32),
+                                 _p(F.uci, np.int32), _p(F.uv), _p(np.ascontiguousarray(b, np.float64)), _p(x),
+                                 C.c_double(tol), int(maxiter), int(threads), C.byref(rsm))
+    if it < 0:
+        raise ValueError("orcmt_bicgstab: bad arguments")
+    return x, it, rsm.value
 
 
 def ref_intel():

@@ -219,3 +219,25 @@ def test_ic0_restatement_bitwise_vs_compiled_reference():
     """IC(0) (hip/Precond/ic0.cpp, ic0_csr_A with the Precond_ic0 defaults)."""
     for A in (st.poisson2d_5pt(15), st.varcoef3d_7pt(7, 2), st.poisson3d_7pt(8), st.varcoef3d_7pt(5, 7)):
         assert np.array_equal(oracle.ic0_values(A), oracle.ref_ic0_values(A)), A.name
+
+
+def test_threaded_timing_variant_tracks_the_oracle():
+    """The CPU reference arm of the benchmark times a threaded variant of the
+    restated BiCGSTAB + ILU(0) (SpMV and vector operations on host threads,
+    triangular solves sequential, dot products in a fixed blocked order).
+    It must solve the same system as the oracle: residual below the
+    tolerance, iteration count within two of the oracle's, the same solution
+    to the accuracy the tolerance allows, and identical results for any
+    thread count."""
+    A = st.varcoef3d_7pt(20, 3)
+    b = st.rhs_uniform(A.n, 1)
+    F = oracle.ilu0(A)
+    xo, ho, uo = oracle.solve("bicgstab", A, b, tol=1e-10, maxiter=500, pc="lu", factors=F)
+    runs = [oracle.bicgstab_threads(A, b, F, tol=1e-10, maxiter=500, threads=t) for t in (1, 3, 8)]
+    x, it, rsm = runs[0]
+    for xt, itt, rt in runs[1:]:
+        assert np.array_equal(xt, x) and itt == it and rt == rsm
+    rel = np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)
+    assert rsm < 1e-10 and rel < 1e-9
+    assert abs(it - (uo + 1)) <= 2, (it, uo + 1)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7
