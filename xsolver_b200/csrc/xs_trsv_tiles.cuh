@@ -36,6 +36,7 @@
 // identical to the level-ordered solve and to the oracle.
 #pragma once
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cstring>
 #include <thread>
@@ -441,13 +442,31 @@ inline bool tile_layout(int n, const int *rp, const int *ci, bool upper, SrcF sr
     host_parallel_for(h.ntiles, 16, [&](long t) {
         const int p0 = h.tile_pos[t], p1 = h.tile_pos[t + 1], rows = p1 - p0;
         std::vector<int> &ext = ext_of[t];
+        int lo = INT_MAX, hi = -1;
         for (int p = p0; p < p1; p++) {
             const int r = h.perm[p];
             for (int e = rp[r]; e < rp[r + 1]; e++)
-                if (tile_of[logical(ci[e])] != t) ext.push_back(ci[e]);
+                if (tile_of[logical(ci[e])] != t) {
+                    ext.push_back(ci[e]);
+                    lo = std::min(lo, ci[e]);
+                    hi = std::max(hi, ci[e]);
+                }
         }
-        std::sort(ext.begin(), ext.end());
-        ext.erase(std::unique(ext.begin(), ext.end()), ext.end());
+        // sorted, without duplicates: through a bitmap over [lo, hi] when
+        // that window is narrow against the list, else by sorting
+        const long words = hi >= lo ? ((long)hi - lo) / 64 + 1 : 0;
+        if (words > 0 && words <= 8 * (long)ext.size() + 64) {
+            thread_local std::vector<unsigned long long> bm;
+            bm.assign(words, 0ull);
+            for (int d : ext) bm[(d - lo) >> 6] |= 1ull << ((d - lo) & 63);
+            ext.clear();
+            for (long w = 0; w < words; w++)
+                for (unsigned long long x = bm[w]; x; x &= x - 1)
+                    ext.push_back(lo + (int)(w * 64) + __builtin_ctzll(x));
+        } else {
+            std::sort(ext.begin(), ext.end());
+            ext.erase(std::unique(ext.begin(), ext.end()), ext.end());
+        }
         if (!entries) return;
         for (int p = p0; p < p1; p++) {
             const int r = h.perm[p];
