@@ -362,3 +362,35 @@ def test_one_directional_halo_exchange():
     assert (out[0][4], out[0][5]) == (2, 0)
     assert (out[1][4], out[1][5]) == (1, 1)
     assert (out[2][4], out[2][5]) == (0, 2)
+
+
+@pytest.mark.parametrize("method,name", [("bicgstab", "c3"), ("cgm", "p3")])
+def test_result_does_not_depend_on_the_check_interval(method, name):
+    """The decomposition solvers keep their scalars on the device and read
+    the convergence flag on the host only every check_every iterations;
+    iterations after convergence must leave the solution, the history and
+    the count as they were.  So every interval gives the same bits, down to
+    an interval longer than the iteration limit (which runs the loop to
+    maxiter on frozen state)."""
+    import torch.distributed as dist
+
+    from xsolver_b200 import distributed as dd
+
+    A, b = _problem(name)
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=30))
+    try:
+        bounds = dd.row_bounds(A.n, 1)
+        rp, ci, v = dd.local_rows(A, bounds, 0)
+        plan = dd.HaloPlan(rp, ci, bounds, 0, "cpu")
+        be = CpuBackend(plan, v)
+        solve = dd.pcg if method == "cgm" else dd.bicgstab
+        runs = [solve(be, plan, b, tol=1e-10, maxiter=300, check_every=k) for k in (1, 4, 16, 1000)]
+    finally:
+        dist.destroy_process_group()
+    x0, rv0, used0 = runs[0]
+    assert used0 < 299 and rv0[-1] < 1e-10
+    for x, rv, used in runs[1:]:
+        assert used == used0
+        assert np.array_equal(rv, rv0)
+        assert np.array_equal(x.numpy(), x0.numpy())
